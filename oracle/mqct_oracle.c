@@ -1,0 +1,1294 @@
+/*
+ * mqct_oracle.c -- CPU FP64 oracle for the MQCT hot paths.
+ *
+ * TEST INFRASTRUCTURE ONLY (see mqct_oracle.h).  Plain-C restatement of the
+ * reference Fortran (MarquetteQuantum/MQCT) written from the mathematics and
+ * the reference's algorithms; each routine names the file:line it follows.
+ * Parity is pinned by tests against the reference's own example outputs
+ * (EXAMPLES_IO) and closed-form known answers.
+ */
+#include "mqct_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Physical constants, SRC/iotest.f:19-25 and SRC/propagator.f:46. */
+#define ORC_AUTOEV 27.21113845
+#define ORC_EVTOWN 8065.5448
+#define ORC_PI 3.14159265358979323846
+
+/* ---------------------------------------------------------------------- */
+/* LOGFACT table: SRC/pot_comp.f:311-322 (INI_FACT), log(n!) by summation. */
+#define LOGFACT_N 400
+static double g_logfact[LOGFACT_N + 1];
+static int g_logfact_ready = 0;
+static void orc_init_logfact(void) {
+  if (g_logfact_ready) return;
+  g_logfact[0] = 0.0;
+  for (int i = 1; i <= LOGFACT_N; ++i) g_logfact[i] = g_logfact[i - 1] + log((double)i);
+  g_logfact_ready = 1;
+}
+__attribute__((constructor)) static void orc_ctor(void) { orc_init_logfact(); }
+
+/* C_N_K binomial via LOGFACT, SRC/pot_comp.f:324-331. */
+static double orc_cnk(int n, int k) {
+  return exp(g_logfact[n] - g_logfact[n - k] - g_logfact[k]);
+}
+
+static double orc_ipow(double x, int n) { /* Fortran x**n with integer n >= 0 */
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Gauss-Legendre nodes/weights on [-1,1]: SRC/suppl_routines.f:157-204 (gauleg):
+ * Newton iteration on P_n from z0 = cos(pi(i-1/4)/(n+1/2)), |dz| <= 3e-15. */
+void orc_gauleg(int n, double* x, double* w) {
+  const double eps = 3.0e-15;
+  int m = (n + 1) / 2;
+  for (int i = 1; i <= m; ++i) {
+    double z = cos(ORC_PI * (i - 0.25) / (n + 0.5));
+    double z1, pp;
+    for (;;) {
+      double p1 = 1.0, p2 = 0.0, p3;
+      for (int j = 1; j <= n; ++j) {
+        p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (!(fabs(z - z1) > eps)) break;
+    }
+    x[i - 1] = -z;
+    x[n - i] = z;
+    w[i - 1] = 2.0 / ((1.0 - z * z) * pp * pp);
+    w[n - i] = w[i - 1];
+  }
+}
+
+/* Associated Legendre P_l^m(x) with Condon-Shortley phase:
+ * SRC/suppl_routines.f:207-243 (plgndr). */
+double orc_plgndr(int l, int m, double x) {
+  double pmm = 1.0;
+  if (m > 0) {
+    double somx2 = sqrt((1.0 - x) * (1.0 + x));
+    double fact = 1.0;
+    for (int i = 1; i <= m; ++i) {
+      pmm = -pmm * fact * somx2;
+      fact += 2.0;
+    }
+  }
+  if (l == m) return pmm;
+  double pmmp1 = x * (2 * m + 1) * pmm;
+  if (l == m + 1) return pmmp1;
+  double pll = 0.0;
+  for (int ll = m + 2; ll <= l; ++ll) {
+    pll = (x * (2 * ll - 1) * pmmp1 - (ll + m - 1) * pmm) / (ll - m);
+    pmm = pmmp1;
+    pmmp1 = pll;
+  }
+  return pll;
+}
+
+/* Jacobi polynomials P_0..P_n^(a,b)(x), three-term recurrence:
+ * SRC/suppl_routines.f:1-148 (jacobi_poly). */
+void orc_jacobi_poly(int n, double a, double b, double x, double* cx) {
+  if (n < 0) return;
+  cx[0] = 1.0;
+  if (n == 0) return;
+  cx[1] = (1.0 + 0.5 * (a + b)) * x + 0.5 * (a - b);
+  for (int i = 2; i <= n; ++i) {
+    double r = (double)i;
+    double c1 = 2.0 * r * (r + a + b) * (2.0 * r - 2.0 + a + b);
+    double c2 = (2.0 * r - 1.0 + a + b) * (2.0 * r + a + b) * (2.0 * r - 2.0 + a + b);
+    double c3 = (2.0 * r - 1.0 + a + b) * (a + b) * (a - b);
+    double c4 = -2.0 * (r - 1.0 + a) * (r - 1.0 + b) * (2.0 * r + a + b);
+    cx[i] = ((c3 + c2 * x) * cx[i - 1] + c4 * cx[i - 2]) / c1;
+  }
+}
+
+/* Wigner 3j symbol, Racah sum with doubled arguments:
+ * SRC/suppl_routines.f:270-314 (W3JS). */
+double orc_w3js(int j1, int j2, int j3, int m1, int m2, int m3) {
+  if (m1 + m2 + m3 != 0) return 0.0;
+  int ia = j1 + j2;
+  if (j3 > ia) return 0.0;
+  int ib = j1 - j2;
+  if (j3 < abs(ib)) return 0.0;
+  int jsum = j3 + ia, ic = j1 - m1, id = j2 - m2;
+  if (jsum % 2 || ic % 2 || id % 2) return 0.0;
+  if (abs(m1) > j1 || abs(m2) > j2 || abs(m3) > j3) return 0.0;
+  int ie = j3 - j2 + m1, iff = j3 - j1 - m2;
+  int zmin = 0;
+  if (-ie > zmin) zmin = -ie;
+  if (-iff > zmin) zmin = -iff;
+  int ig = ia - j3, ih = j2 + m2;
+  int zmax = ig;
+  if (ih < zmax) zmax = ih;
+  if (ic < zmax) zmax = ic;
+  double cc = 0.0;
+  for (int z = zmin; z <= zmax; z += 2) {
+    double denom = exp(g_logfact[z / 2] + g_logfact[(ig - z) / 2] + g_logfact[(ic - z) / 2] +
+                       g_logfact[(ih - z) / 2] + g_logfact[(ie + z) / 2] + g_logfact[(iff + z) / 2]);
+    if (z % 4 != 0) denom = -denom;
+    cc += 1.0 / denom;
+  }
+  double cc1 = exp(g_logfact[ig / 2] + g_logfact[(j3 + ib) / 2] + g_logfact[(j3 - ib) / 2] -
+                   g_logfact[(jsum + 2) / 2]);
+  double cc2 = exp(g_logfact[(j1 + m1) / 2] + g_logfact[ic / 2] + g_logfact[ih / 2] +
+                   g_logfact[id / 2] + g_logfact[(j3 - m3) / 2] + g_logfact[(j3 + m3) / 2]);
+  cc = cc * sqrt(cc1 * cc2);
+  if ((ib - m3) % 4 != 0) cc = -cc;
+  return cc;
+}
+
+/* Clebsch-Gordan <j1 m1 j2 m2|j3 m3>: SRC/suppl_routines.f:246-252 (CG). */
+double orc_cg(int j1, int j2, int j3, int m1, int m2, int m3) {
+  int e = -j1 + j2 - m3;
+  double sgn = (e % 2 == 0) ? 1.0 : -1.0;
+  return orc_w3js(2 * j1, 2 * j2, 2 * j3, 2 * m1, 2 * m2, -2 * m3) * sqrt(2.0 * j3 + 1.0) * sgn;
+}
+
+/* Cubic spline second derivatives with end slopes yp1/ypn (natural if >.99e30):
+ * SRC/suppl_routines.f:914-965 (spline). */
+void orc_spline(const double* x, const double* y, int n, double yp1, double ypn, double* y2) {
+  double* u = (double*)malloc(sizeof(double) * (size_t)n);
+  if (yp1 > 0.99e30) {
+    y2[0] = 0.0;
+    u[0] = 0.0;
+  } else {
+    y2[0] = -0.5;
+    u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1);
+  }
+  for (int i = 1; i < n - 1; ++i) {
+    double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+    double p = sig * y2[i - 1] + 2.0;
+    y2[i] = (sig - 1.0) / p;
+    u[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])) /
+                (x[i + 1] - x[i - 1]) -
+            sig * u[i - 1]) /
+           p;
+  }
+  double qn, un;
+  if (ypn > 0.99e30) {
+    qn = 0.0;
+    un = 0.0;
+  } else {
+    qn = 0.5;
+    un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]));
+  }
+  y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0);
+  for (int k = n - 2; k >= 0; --k) y2[k] = y2[k] * y2[k + 1] + u[k];
+  free(u);
+}
+
+/* Spline evaluation with derivative, bisection bracket:
+ * SRC/suppl_routines.f:968-1002 (splint). */
+void orc_splint(const double* xa, const double* ya, const double* y2a, int n, double x,
+                double* y, double* yprime) {
+  int klo = 1, khi = n;
+  while (khi - klo > 1) {
+    int k = (khi + klo) / 2;
+    if (xa[k - 1] > x) khi = k;
+    else klo = k;
+  }
+  double h = xa[khi - 1] - xa[klo - 1];
+  double a = (xa[khi - 1] - x) / h;
+  double b = (x - xa[klo - 1]) / h;
+  *y = a * ya[klo - 1] + b * ya[khi - 1] +
+       ((a * a * a - a) * y2a[klo - 1] + (b * b * b - b) * y2a[khi - 1]) * (h * h) / 6.0;
+  *yprime = -ya[klo - 1] / h + ya[khi - 1] / h +
+            (-(3.0 * a * a - 1.0) * y2a[klo - 1] / h + (3.0 * b * b - 1.0) * y2a[khi - 1] / h) *
+                (h * h) / 6.0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Wigner D-function as used by the reference: d(beta) from the Jacobi form
+ * with the reference's (n, a, lambda) case selection, times
+ * (cos + i sin)(k*gamma + m*alpha).  SRC/pot_comp.f:256-309 (Djkm). */
+void orc_djkm(int j, int k, int m, double alpha, double beta, double gamma, double* re,
+              double* im) {
+  int n = j + k, a = 0, lambda = 0;
+  if (j - k < n) n = j - k;
+  if (j + m < n) n = j + m;
+  if (j - m < n) n = j - m;
+  if (n == j + m) { a = k - m; lambda = 0; }
+  if (n == j - m) { a = m - k; lambda = k - m; }
+  if (n == j + k) { a = m - k; lambda = k - m; }
+  if (n == j - k) { a = k - m; lambda = 0; }
+  int b = 2 * j - 2 * n - a;
+  double cx[2 * 64 + 2];
+  orc_jacobi_poly(n, (double)a, (double)b, cos(beta), cx);
+  double sgn = ((lambda % 2) == 0) ? 1.0 : -1.0;
+  double dkm = cx[n] * sgn * sqrt(orc_cnk(2 * j - n, n + a)) / sqrt(orc_cnk(n + b, b)) *
+               orc_ipow(sin(beta / 2.0), a) * orc_ipow(cos(beta / 2.0), b);
+  *re = dkm * cos(k * gamma + m * alpha);
+  *im = dkm * sin(k * gamma + m * alpha);
+}
+
+/* Normalised spherical harmonic of the rigid diatom:
+ * SRC/basis_wave_functions.f:153-175 (WF_DIAT_TOP). */
+void orc_wf_diat(int j, int m, double theta, double phi, double* re, double* im) {
+  int am = abs(m);
+  double pl = orc_plgndr(j, am, cos(theta));
+  double nrm = sqrt((2.0 * j + 1.0) / 4.0 / ORC_PI * exp(g_logfact[j - am] - g_logfact[j + am]));
+  double wr = pl * nrm * cos(m * phi);
+  double wi = pl * nrm * sin(m * phi);
+  if (m < 0 && (am % 2)) {
+    wr = -wr;
+    wi = -wi;
+  }
+  *re = wr;
+  *im = wi;
+}
+
+/* Asymmetric-top wavefunction sum_K c_K sqrt((2j+1)/8pi^2) D^j_{K m}:
+ * SRC/basis_wave_functions.f:83-116 (WF_ASYM_TOP). */
+void orc_wf_asym(int j, const double* coeff, int m, double alpha, double beta, double gamma,
+                 double* re, double* im) {
+  double wr = 0.0, wi = 0.0;
+  double nrm = sqrt((2.0 * j + 1.0) / 8.0 / (ORC_PI * ORC_PI));
+  for (int i = 1; i <= 2 * j + 1; ++i) {
+    int dk = i - j - 1;
+    double dwr, dwi;
+    orc_djkm(j, dk, m, alpha, beta, gamma, &dwr, &dwi);
+    dwr *= nrm;
+    dwi *= nrm;
+    wr += dwr * coeff[i - 1];
+    wi += dwi * coeff[i - 1];
+  }
+  *re = wr;
+  *im = wi;
+}
+
+/* Rigid-rotor Hamiltonian element in the symmetric-top basis, z = c axis:
+ * SRC/asym_top.f:103-137 (hamilt_kyro). */
+static double orc_hamilt(int j, int k1, int k2, double A, double B, double C) {
+  double jj = j * (j + 1.0);
+  if (k1 != k2) {
+    if (k1 == k2 - 2 || k1 == k2 + 2) {
+      int kav = (k1 + k2) / 2;
+      double jxy = sqrt((j + 1.0) * j - kav * k1) * sqrt((j + 1.0) * j - kav * k2) / 2.0;
+      return 0.5 * (A - B) * jxy;
+    }
+    return 0.0;
+  }
+  return 0.5 * (A + B) * jj + (C - 0.5 * (A + B)) * (double)(k1 * k1);
+}
+
+/* Cyclic Jacobi eigensolver for a small dense symmetric matrix (row-major a[n*n]);
+ * eigenvalues in w, eigenvectors as columns of v (row-major v[i*n+col]). */
+static void orc_jacobi_eig(int n, double* a, double* w, double* v) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) v[i * n + j] = (i == j) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int i = 0; i < n; ++i) {
+      diag += a[i * n + i] * a[i * n + i];
+      for (int j = i + 1; j < n; ++j) off += a[i * n + j] * a[i * n + j];
+    }
+    if (off <= 1e-32 * (diag + 1e-300)) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = a[p * n + q];
+        if (fabs(apq) < 1e-300) continue;
+        double app = a[p * n + p], aqq = a[q * n + q];
+        double theta = (aqq - app) / (2.0 * apq);
+        double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          double akp = a[k * n + p], akq = a[k * n + q];
+          a[k * n + p] = c * akp - s * akq;
+          a[k * n + q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double apk = a[p * n + k], aqk = a[q * n + k];
+          a[p * n + k] = c * apk - s * aqk;
+          a[q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          double vkp = v[k * n + p], vkq = v[k * n + q];
+          v[k * n + p] = c * vkp - s * vkq;
+          v[k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i) w[i] = a[i * n + i];
+}
+
+/* Level (j, ka, kc): ascending eigenvalue number j + (ka - kc), the labelling of
+ * SRC/asym_top.f:139-173 (STATE) used by EIGEN_VAL/EIGEN_VEC
+ * (SRC/asym_top.f:1-101, 280-388).  The eigenvector sign is fixed so that its
+ * first non-negligible component (lowest K) is positive. */
+int orc_asym_top(double A, double B, double C, int j, int ka, int kc, double* energy,
+                 double* vec) {
+  int n = 2 * j + 1;
+  if (j < 0 || ka < 0 || kc < 0 || ka > j || kc > j) return -1;
+  if (ka + kc != j && ka + kc != j + 1) return -2;
+  int tau = ka - kc;
+  if (tau < -j || tau > j) return -3;
+  /* STATE: K_A = [0,1,1,2,2,...], index i = j + tau + 1 must reproduce ka. */
+  int idx = j + tau + 1; /* 1-based */
+  int ka_chk = idx / 2;
+  if (ka_chk != ka) return -4;
+  double* h = (double*)malloc(sizeof(double) * n * n);
+  double* vv = (double*)malloc(sizeof(double) * n * n);
+  double* w = (double*)malloc(sizeof(double) * n);
+  int* ord = (int*)malloc(sizeof(int) * n);
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) h[a * n + b] = orc_hamilt(j, a - j, b - j, A, B, C);
+  orc_jacobi_eig(n, h, w, vv);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  for (int i = 1; i < n; ++i) { /* insertion sort ascending */
+    int t = ord[i], p = i - 1;
+    while (p >= 0 && w[ord[p]] > w[t]) { ord[p + 1] = ord[p]; --p; }
+    ord[p + 1] = t;
+  }
+  int col = ord[idx - 1];
+  *energy = w[col];
+  int first = -1;
+  for (int k = 0; k < n; ++k) {
+    vec[k] = vv[k * n + col];
+    if (first < 0 && fabs(vec[k]) > 1e-10) first = k;
+  }
+  if (first >= 0 && vec[first] < 0)
+    for (int k = 0; k < n; ++k) vec[k] = -vec[k];
+  free(h); free(vv); free(w); free(ord);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* States: SRC/matrix_ini.f:60-209 (count) and 261-544 (fill), distinguishable
+ * particles.  Types 1/4: m=-j..j per channel; types 8/0: j12=|j1-j2|..j1+j2, m12. */
+int orc_count_states(const orc_system* sys) {
+  int st = 0;
+  for (int i = 0; i < sys->n_channels; ++i) {
+    switch (sys->sys_type) {
+      case 1: case 4: st += 2 * sys->j1[i] + 1; break;
+      case 8: case 0: {
+        int a = sys->j1[i], b = sys->j2[i];
+        for (int js = abs(a - b); js <= a + b; ++js) st += 2 * js + 1;
+        break;
+      }
+      default: return -1;
+    }
+  }
+  return st;
+}
+
+int orc_enumerate_states(const orc_system* sys, int32_t* indx_chann, int32_t* j12, int32_t* m12,
+                         double* ej) {
+  int st = 0;
+  for (int i = 0; i < sys->n_channels; ++i) {
+    if (sys->sys_type == 1 || sys->sys_type == 4) {
+      int j = sys->j1[i];
+      for (int m = -j; m <= j; ++m) {
+        indx_chann[st] = i + 1; j12[st] = j; m12[st] = m; ej[st] = sys->e_ch[i]; ++st;
+      }
+    } else if (sys->sys_type == 8 || sys->sys_type == 0) {
+      int a = sys->j1[i], b = sys->j2[i];
+      for (int js = abs(a - b); js <= a + b; ++js)
+        for (int m = -js; m <= js; ++m) {
+          indx_chann[st] = i + 1; j12[st] = js; m12[st] = m; ej[st] = sys->e_ch[i]; ++st;
+        }
+    } else {
+      return -1;
+    }
+  }
+  return st;
+}
+
+/* ind_mat: all (st1, st2) with st2 <= st1 and equal m12, st1 outer:
+ * SRC/matrix_ini.f:553-627. */
+int64_t orc_count_pairs(int n, const int32_t* m12) {
+  int64_t p = 0;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (m12[a] == m12[b]) ++p;
+  return p;
+}
+int64_t orc_ind_mat(int n, const int32_t* m12, int32_t* ind) {
+  int64_t p = 0;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (m12[a] == m12[b]) {
+        ind[2 * p] = a + 1;
+        ind[2 * p + 1] = b + 1;
+        ++p;
+      }
+  return p;
+}
+
+/* R grid: equidistant (SRC/matrix_ini.f:976-980) or the 3-segment
+ * "optimized" grid (SRC/matrix_ini.f:957-973). */
+void orc_rgrid(int n, double rmin, double rmax, int equidistant, double* R) {
+  if (equidistant) {
+    double dr = (rmax - rmin) / (n - 1.0);
+    for (int i = 1; i <= n; ++i) R[i - 1] = rmin + dr * (i - 1.0);
+    return;
+  }
+  int n1 = n / 3, n2 = n / 2 + 1;
+  R[0] = rmin;
+  R[n - 1] = rmax;
+  double dr = (rmax - rmin) / (n - 1.0);
+  for (int i = 1; i <= n1; ++i) R[i - 1] = rmin + dr * (i - 1.0) / 3.0;
+  for (int i = n1 + 1; i <= n2; ++i) R[i - 1] = R[n1 - 1] + dr * (i - n1);
+  dr = (rmax - R[n2 - 1]) / (n - n2);
+  for (int i = n2; i <= n; ++i) R[i - 1] = R[n2 - 1] + dr * (i - n2);
+}
+
+/* ---------------------------------------------------------------------- */
+/* Synthetic PES family (stand-ins for the USER_DEFINED_PES plugin of PES_DIRECTORIES).
+ *  LEGENDRE: V(R,beta) = sum_l [A_l exp(-b_l R) - C_l/R^6] P_l(cos beta),
+ *            p = [A_0..A_{n-1}, b_0.., C_0..].
+ *  SITES1:   atom at R*(sin b cos g, sin b sin g, cos b) in the rotor frame
+ *            (b,g = PES beta/gamma arguments); per term
+ *            p = [site, D, a, re, C6, rd]:
+ *            D(e^{-2a(r-re)} - 2e^{-a(r-re)}) - C6 (1-e^{-(r/rd)^6}) / r^6.
+ *  SITES2:   rotor 1 at the origin with Euler (alpha=0?,beta,gamma), rotor 2 at
+ *            R*z with Euler (aalpha,bbeta,ggamma); p = [s1, s2, D, a, re, C6, rd].
+ */
+static void orc_euler_rot(double a, double b, double g, double* M) {
+  /* R = Rz(a) Ry(b) Rz(g), row-major */
+  double ca = cos(a), sa = sin(a), cb = cos(b), sb = sin(b), cg = cos(g), sg = sin(g);
+  M[0] = ca * cb * cg - sa * sg; M[1] = -ca * cb * sg - sa * cg; M[2] = ca * sb;
+  M[3] = sa * cb * cg + ca * sg; M[4] = -sa * cb * sg + ca * cg; M[5] = sa * sb;
+  M[6] = -sb * cg;               M[7] = sb * sg;                 M[8] = cb;
+}
+static double orc_site_term(double r, const double* t) {
+  double D = t[0], a = t[1], re = t[2], c6 = t[3], rd = t[4];
+  double e = exp(-a * (r - re));
+  double r2 = r * r, r6 = r2 * r2 * r2;
+  double x = r / rd, x2 = x * x, x6 = x2 * x2 * x2;
+  return D * (e * e - 2.0 * e) - c6 * (1.0 - exp(-x6)) / r6;
+}
+double orc_pes_eval(const orc_pes* pes, double R, double alpha, double beta, double gamma,
+                    double aalpha, double bbeta, double ggamma) {
+  int n = pes->n_terms;
+  const double* p = pes->p;
+  if (pes->kind == ORC_PES_LEGENDRE) {
+    double x = cos(beta), v = 0.0;
+    double r2 = R * R, r6 = r2 * r2 * r2;
+    for (int l = 0; l < n; ++l) {
+      double pl = orc_plgndr(l, 0, x);
+      v += (p[l] * exp(-p[n + l] * R) - p[2 * n + l] / r6) * pl;
+    }
+    return v;
+  }
+  if (pes->kind == ORC_PES_SITES1) {
+    double ux = sin(beta) * cos(gamma), uy = sin(beta) * sin(gamma), uz = cos(beta);
+    double ax = R * ux, ay = R * uy, az = R * uz;
+    double v = 0.0;
+    for (int t = 0; t < n; ++t) {
+      const double* q = p + 6 * t;
+      const double* s = pes->sites1 + 3 * (int)q[0];
+      double dx = ax - s[0], dy = ay - s[1], dz = az - s[2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      v += orc_site_term(r, q + 1);
+    }
+    return v;
+  }
+  if (pes->kind == ORC_PES_SITES2) {
+    double M1[9], M2[9];
+    orc_euler_rot(alpha, beta, gamma, M1);
+    orc_euler_rot(aalpha, bbeta, ggamma, M2);
+    double v = 0.0;
+    for (int t = 0; t < n; ++t) {
+      const double* q = p + 7 * t;
+      const double* s1 = pes->sites1 + 3 * (int)q[0];
+      const double* s2 = pes->sites2 + 3 * (int)q[1];
+      double x1[3], x2[3];
+      for (int c = 0; c < 3; ++c) {
+        x1[c] = M1[3 * c] * s1[0] + M1[3 * c + 1] * s1[1] + M1[3 * c + 2] * s1[2];
+        x2[c] = M2[3 * c] * s2[0] + M2[3 * c + 1] * s2[1] + M2[3 * c + 2] * s2[2];
+      }
+      x2[2] += R;
+      double dx = x2[0] - x1[0], dy = x2[1] - x1[1], dz = x2[2] - x1[2];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      v += orc_site_term(r, q + 2);
+    }
+    return v;
+  }
+  return NAN;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Angular grids of INI_POT_STORAGE.  Type 1: GL beta on [0,pi]
+ * (SRC/pot_comp.f:374-394).  Type 4: GL beta x gamma, gamma midpoint-equidistant
+ * on [0,2pi] with weight 2/n when EQ_ANG_GRID (default) else GL
+ * (SRC/pot_comp.f:586-635).  The optional alpha grid (type 4 with n_alpha>0)
+ * replaces the analytic 2*pi alpha factor by the same midpoint rule. */
+typedef struct {
+  int nb, ng, na;
+  double xbl, xgl, xal;       /* half-lengths */
+  double *bx, *bw, *gx, *gw, *ax, *aw;
+  /* type 0 extra axes */
+  int nbb, naa, ngg;
+  double xbbl, xaal, xggl;
+  double *bbx, *bbw, *aax, *aaw, *ggx, *ggw;
+} orc_agrid;
+
+static void orc_axis_gl(int n, double lo, double hi, double** x, double** w, double* half) {
+  double* t = (double*)malloc(sizeof(double) * n);
+  double* u = (double*)malloc(sizeof(double) * n);
+  orc_gauleg(n, t, u);
+  double xm = 0.5 * (hi + lo), xl = 0.5 * (hi - lo);
+  for (int i = 0; i < n; ++i) t[i] = xm + xl * t[i];
+  *x = t; *w = u; *half = xl;
+}
+static void orc_axis_mid(int n, double lo, double hi, double** x, double** w, double* half) {
+  double* t = (double*)malloc(sizeof(double) * n);
+  double* u = (double*)malloc(sizeof(double) * n);
+  double xl = 0.5 * (hi - lo);
+  for (int i = 1; i <= n; ++i) {
+    t[i - 1] = lo + (i - 0.50) * 2.0 * xl / n;
+    u[i - 1] = 2.0 / n;
+  }
+  *x = t; *w = u; *half = xl;
+}
+static void orc_make_agrid(int sys_type, const orc_grid* g, orc_agrid* a) {
+  memset(a, 0, sizeof(*a));
+  a->nb = g->n_beta;
+  orc_axis_gl(g->n_beta, 0.0, ORC_PI, &a->bx, &a->bw, &a->xbl);
+  if (sys_type == 4 || sys_type == 0) {
+    a->ng = g->n_gamma;
+    if (g->eq_gamma) orc_axis_mid(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
+    else orc_axis_gl(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
+  }
+  if (sys_type == 4 && g->n_alpha > 0) {
+    a->na = g->n_alpha;
+    orc_axis_mid(g->n_alpha, 0.0, 2 * ORC_PI, &a->ax, &a->aw, &a->xal);
+  }
+  if (sys_type == 0) {
+    a->nbb = g->n_beta2;
+    orc_axis_gl(g->n_beta2, 0.0, ORC_PI, &a->bbx, &a->bbw, &a->xbbl);
+    a->naa = g->n_alpha2;
+    a->ngg = g->n_gamma2;
+    if (g->eq_gamma) {
+      orc_axis_mid(g->n_alpha2, 0.0, 2 * ORC_PI, &a->aax, &a->aaw, &a->xaal);
+      orc_axis_mid(g->n_gamma2, 0.0, 2 * ORC_PI, &a->ggx, &a->ggw, &a->xggl);
+    } else {
+      orc_axis_gl(g->n_alpha2, 0.0, 2 * ORC_PI, &a->aax, &a->aaw, &a->xaal);
+      orc_axis_gl(g->n_gamma2, 0.0, 2 * ORC_PI, &a->ggx, &a->ggw, &a->xggl);
+    }
+  }
+}
+static void orc_free_agrid(orc_agrid* a) {
+  free(a->bx); free(a->bw); free(a->gx); free(a->gw); free(a->ax); free(a->aw);
+  free(a->bbx); free(a->bbw); free(a->aax); free(a->aaw); free(a->ggx); free(a->ggw);
+}
+static int64_t orc_agrid_size(int sys_type, const orc_agrid* a) {
+  if (sys_type == 1) return a->nb;
+  if (sys_type == 4) return (int64_t)a->nb * a->ng * (a->na > 0 ? a->na : 1);
+  if (sys_type == 0) return (int64_t)a->naa * a->nb * a->nbb * a->ng * a->ngg;
+  return -1;
+}
+
+/* Wavefunction of state st (0-based) at a grid point, dispatching on type:
+ * type 1 WF_DIAT_TOP(j,m,beta,0); type 4 WF_ASYM_TOP(...,alpha,beta,gamma);
+ * type 0 WF_ASYM_TOP_ASYM_TOP (SRC/basis_wave_functions.f:1-41). */
+static void orc_wf_state(const orc_system* sys, int ch, int j12, int m12, double al, double be,
+                         double ga, double aal, double bbe, double gga, double* re, double* im) {
+  if (sys->sys_type == 1) {
+    orc_wf_diat(sys->j1[ch], m12, be, 0.0, re, im);
+  } else if (sys->sys_type == 4) {
+    orc_wf_asym(sys->j1[ch], sys->vec1 + (size_t)ch * sys->ldv, m12, al, be, ga, re, im);
+  } else { /* type 0 */
+    int j1 = sys->j1[ch], j2 = sys->j2[ch];
+    double wr = 0.0, wi = 0.0;
+    for (int m1 = -j1; m1 <= j1; ++m1) {
+      int m2 = m12 - m1;
+      if (abs(m2) > j2) continue;
+      double dr1, di1, dr2, di2;
+      orc_wf_asym(j1, sys->vec1 + (size_t)ch * sys->ldv, m1, al, be, ga, &dr1, &di1);
+      orc_wf_asym(j2, sys->vec2 + (size_t)ch * sys->ldv, m2, aal, bbe, gga, &dr2, &di2);
+      double cg = orc_cg(j1, j2, j12, m1, m2, m12);
+      wr += cg * (dr1 * dr2 - di1 * di2);
+      wi += cg * (dr1 * di2 + di1 * dr2);
+    }
+    *re = wr;
+    *im = wi;
+  }
+}
+
+/* Grid point g -> angles and the product of weights/Jacobian of the reference
+ * integrand (SRC/pot_comp.f:1947-1952, 2535-2557, 3663-3721). */
+typedef struct { double al, be, ga, aal, bbe, gga, wt; } orc_gpt;
+static orc_gpt orc_grid_point(int sys_type, const orc_agrid* a, int64_t g) {
+  orc_gpt p;
+  memset(&p, 0, sizeof(p));
+  if (sys_type == 1) {
+    p.be = a->bx[g];
+    p.wt = a->bw[g] * sin(p.be) * a->xbl * 2.0 * ORC_PI;
+  } else if (sys_type == 4) {
+    int na = a->na > 0 ? a->na : 1;
+    int ia = (int)(g % na);
+    int64_t r = g / na;
+    int ig = (int)(r % a->ng), ib = (int)(r / a->ng);
+    p.be = a->bx[ib];
+    p.ga = a->gx[ig];
+    if (a->na > 0) {
+      p.al = a->ax[ia];
+      p.wt = a->bw[ib] * a->gw[ig] * a->aw[ia] * sin(p.be) * a->xbl * a->xgl * a->xal;
+    } else {
+      p.wt = a->bw[ib] * a->gw[ig] * sin(p.be) * a->xbl * a->xgl * 2.0 * ORC_PI;
+    }
+  } else {
+    /* loop order alpha2, beta1, beta2, gamma1, gamma2 (gamma2 fastest) */
+    int i6 = (int)(g % a->ngg);
+    int64_t r = g / a->ngg;
+    int i5 = (int)(r % a->ng); r /= a->ng;
+    int i4 = (int)(r % a->nbb); r /= a->nbb;
+    int i3 = (int)(r % a->nb); r /= a->nb;
+    int i2 = (int)r;
+    p.be = a->bx[i3]; p.bbe = a->bbx[i4]; p.ga = a->gx[i5]; p.aal = a->aax[i2]; p.gga = a->ggx[i6];
+    p.wt = a->bw[i3] * a->gw[i5] * sin(p.be) * a->aaw[i2] * a->bbw[i4] * a->ggw[i6] * sin(p.bbe) *
+           a->xbl * a->xgl * a->xaal * a->xbbl * a->xggl * 2.0 * ORC_PI;
+  }
+  return p;
+}
+
+/* PES at a grid point with the per-type argument mapping of SRC/pes_sys_type.f:
+ * type 1 (R,beta) :2-9; type 4 (-beta,-gamma) :32-37; type 0 (0,b,g,aa,bb,gg) :90-97. */
+static double orc_pes_at(int sys_type, const orc_pes* pes, double R, const orc_gpt* p,
+                         int iR, int64_t g, int64_t ng) {
+  if (pes->kind == ORC_PES_TABLE) return pes->table[(size_t)iR * ng + g];
+  if (sys_type == 1) return orc_pes_eval(pes, R, 0.0, p->be, 0.0, 0.0, 0.0, 0.0);
+  if (sys_type == 4) return orc_pes_eval(pes, R, 0.0, -p->be, -p->ga, 0.0, 0.0, 0.0);
+  return orc_pes_eval(pes, R, 0.0, p->be, p->ga, p->aal, p->bbe, p->gga);
+}
+
+#define ORC_CM_TO_HARTREE (1.0 / ORC_EVTOWN / ORC_AUTOEV)
+
+int orc_integrate_elements(const orc_system* sys, int n_states, const int32_t* indx_chann,
+                           const int32_t* j12, const int32_t* m12, int64_t P,
+                           const int32_t* ind_mat, int nR, const double* R,
+                           const orc_grid* grid, const orc_pes* pes, int literal,
+                           int64_t k_begin, int64_t k_end, int iR_begin, int iR_end,
+                           int n_threads, double* mat) {
+  (void)P;
+  orc_agrid a;
+  orc_make_agrid(sys->sys_type, grid, &a);
+  int64_t ng = orc_agrid_size(sys->sys_type, &a);
+  if (ng <= 0) { orc_free_agrid(&a); return -1; }
+  orc_gpt* pts = (orc_gpt*)malloc(sizeof(orc_gpt) * (size_t)ng);
+  for (int64_t g = 0; g < ng; ++g) pts[g] = orc_grid_point(sys->sys_type, &a, g);
+  /* V table over (R, grid): INI_POT_STORAGE */
+  double* V = (double*)malloc(sizeof(double) * (size_t)ng * (iR_end - iR_begin));
+  for (int iR = iR_begin; iR < iR_end; ++iR)
+    for (int64_t g = 0; g < ng; ++g)
+      V[(size_t)(iR - iR_begin) * ng + g] = orc_pes_at(sys->sys_type, pes, R[iR], &pts[g], iR, g, ng);
+  /* Optional tabulation of psi_s(g) (same per-point arithmetic as the literal form). */
+  double* wr = NULL;
+  double* wi = NULL;
+  if (!literal) {
+    wr = (double*)malloc(sizeof(double) * (size_t)ng * n_states);
+    wi = (double*)malloc(sizeof(double) * (size_t)ng * n_states);
+#pragma omp parallel for schedule(dynamic) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+    for (int s = 0; s < n_states; ++s)
+      for (int64_t g = 0; g < ng; ++g) {
+        const orc_gpt* p = &pts[g];
+        orc_wf_state(sys, indx_chann[s] - 1, j12[s], m12[s], p->al, p->be, p->ga, p->aal, p->bbe,
+                     p->gga, &wr[(size_t)s * ng + g], &wi[(size_t)s * ng + g]);
+      }
+  }
+#pragma omp parallel for schedule(dynamic) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+  for (int64_t k = k_begin; k < k_end; ++k) {
+    int s1 = ind_mat[2 * k] - 1, s2 = ind_mat[2 * k + 1] - 1;
+    for (int iR = iR_begin; iR < iR_end; ++iR) {
+      const double* Vr = V + (size_t)(iR - iR_begin) * ng;
+      double acc = 0.0;
+      for (int64_t g = 0; g < ng; ++g) {
+        const orc_gpt* p = &pts[g];
+        double dr1, di1, dr2, di2;
+        if (literal) {
+          orc_wf_state(sys, indx_chann[s1] - 1, j12[s1], m12[s1], p->al, p->be, p->ga, p->aal,
+                       p->bbe, p->gga, &dr1, &di1);
+          orc_wf_state(sys, indx_chann[s2] - 1, j12[s2], m12[s2], p->al, p->be, p->ga, p->aal,
+                       p->bbe, p->gga, &dr2, &di2);
+        } else {
+          dr1 = wr[(size_t)s1 * ng + g]; di1 = wi[(size_t)s1 * ng + g];
+          dr2 = wr[(size_t)s2 * ng + g]; di2 = wi[(size_t)s2 * ng + g];
+        }
+        acc += (dr1 * dr2 + di1 * di2) * p->wt * Vr[g];
+      }
+      mat[(size_t)k * nR + iR] = acc;
+    }
+  }
+  free(V); free(pts); free(wr); free(wi);
+  orc_free_agrid(&a);
+  return 0;
+}
+
+static int orc_nearest(int n, const double* R, double r) { /* first minloc |R-r| */
+  int best = 0;
+  double d = fabs(R[0] - r);
+  for (int i = 1; i < n; ++i)
+    if (fabs(R[i] - r) < d) { d = fabs(R[i] - r); best = i; }
+  return best;
+}
+
+/* MATRIX_MAKE direct-integration flow: quadrature -> Hartree
+ * (SRC/matrix_ini.f:1948-1955), MIJ_CUTOFF at R~r_cut1/r_cut2 (:1969-1997),
+ * clamped spline with finite-difference end slopes (:2005-2016). */
+int orc_build_matrix(const orc_system* sys, int n_states, const int32_t* indx_chann,
+                     const int32_t* j12, const int32_t* m12, int64_t P, const int32_t* ind_mat,
+                     int nR, const double* R, const orc_grid* grid, const orc_pes* pes,
+                     double mij_cut_cm, double r_cut1, double r_cut2, int literal,
+                     int64_t k_begin, int64_t k_end, int n_threads, double* mat, double* y2,
+                     int32_t* skipped) {
+  int rc = orc_integrate_elements(sys, n_states, indx_chann, j12, m12, P, ind_mat, nR, R, grid,
+                                  pes, literal, k_begin, k_end, 0, nR, n_threads, mat);
+  if (rc) return rc;
+  int ir1 = orc_nearest(nR, R, r_cut1), ir2 = orc_nearest(nR, R, r_cut2);
+  double cut = mij_cut_cm / ORC_EVTOWN / ORC_AUTOEV;
+  for (int64_t k = k_begin; k < k_end; ++k) {
+    double* col = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) col[i] *= ORC_CM_TO_HARTREE;
+    double mx = fabs(col[ir1]);
+    if (fabs(col[ir2]) > mx) mx = fabs(col[ir2]);
+    if (mx < cut) {
+      for (int i = 0; i < nR; ++i) { col[i] = 0.0; y2[(size_t)k * nR + i] = 0.0; }
+      skipped[k] = 1;
+      continue;
+    }
+    skipped[k] = 0;
+    double d0 = (col[1] - col[0]) / (R[1] - R[0]);
+    double d1 = (col[nR - 1] - col[nR - 2]) / (R[nR - 1] - R[nR - 2]);
+    orc_spline(R, col, nR, d0, d1, y2 + (size_t)k * nR);
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Fortran unformatted sequential records: int32 length markers around each
+ * WRITE.  Layout of PRINT_MIJ_USER, SRC/matrix_ini.f:6640-6770. */
+static void orc_rec(FILE* f, const void* data, int32_t nbytes) {
+  fwrite(&nbytes, 4, 1, f);
+  fwrite(data, 1, (size_t)nbytes, f);
+  fwrite(&nbytes, 4, 1, f);
+}
+int orc_write_mtrx_uf(const char* path, int coll_type, int n_channels, int n_states,
+                      const int32_t* state_rec, int state_rec_len, int64_t P,
+                      const int32_t* ind_mat, int nR, const double* R, const double* mat) {
+  FILE* f = fopen(path, "wb");
+  if (!f) return -1;
+  int32_t v;
+  v = coll_type; orc_rec(f, &v, 4);
+  v = n_channels; orc_rec(f, &v, 4);
+  v = n_states; orc_rec(f, &v, 4);
+  v = (int32_t)P; orc_rec(f, &v, 4);
+  v = nR; orc_rec(f, &v, 4);
+  for (int s = 0; s < n_states; ++s) orc_rec(f, state_rec + (size_t)s * state_rec_len, 4 * state_rec_len);
+  for (int64_t k = 0; k < P; ++k) {
+    int32_t t[3] = {(int32_t)(k + 1), ind_mat[2 * k], ind_mat[2 * k + 1]};
+    orc_rec(f, t, 12);
+  }
+  for (int i = 0; i < nR; ++i) {
+    unsigned char buf[12];
+    int32_t ii = i + 1;
+    memcpy(buf, &ii, 4);
+    memcpy(buf + 4, &R[i], 8);
+    orc_rec(f, buf, 12);
+  }
+  for (int64_t k = 0; k < P; ++k) {
+    int32_t kk = (int32_t)(k + 1);
+    orc_rec(f, &kk, 4);
+    orc_rec(f, mat + (size_t)k * nR, 8 * nR);
+  }
+  fclose(f);
+  return 0;
+}
+
+/* Formatted MTRX.DAT (PRINT_MIJ, SRC/matrix_ini.f:4692-4891): five "KEY= n"
+ * header lines, a states table, "MIJ_INDEX" pairs, "#iR" R values and
+ * "#k_matel #iR Mij" rows. */
+int orc_read_mtrx_dat_header(const char* path, int* coll_type, int* n_channels, int* n_states,
+                             int64_t* P, int* nR) {
+  FILE* f = fopen(path, "r");
+  if (!f) return -1;
+  char line[512];
+  long long pp = 0;
+  int ok = 0;
+  if (fgets(line, sizeof line, f) && sscanf(line, "COLLISION_TYPE= %d", coll_type) == 1) ++ok;
+  if (fgets(line, sizeof line, f) && sscanf(line, "NUMBER_OF_CHANLS= %d", n_channels) == 1) ++ok;
+  if (fgets(line, sizeof line, f) && sscanf(line, "NUMBER_OF_STATES= %d", n_states) == 1) ++ok;
+  if (fgets(line, sizeof line, f) && sscanf(line, "MATRIX_SIZE= %lld", &pp) == 1) ++ok;
+  if (fgets(line, sizeof line, f) && sscanf(line, "R_GRID_SIZE= %d", nR) == 1) ++ok;
+  fclose(f);
+  *P = pp;
+  return ok == 5 ? 0 : -2;
+}
+int orc_read_mtrx_dat(const char* path, int n_state_cols, int32_t* state_cols, int32_t* ind_mat,
+                      double* R, double* mat) {
+  int ct, nch, ns, nR;
+  int64_t P;
+  if (orc_read_mtrx_dat_header(path, &ct, &nch, &ns, &P, &nR)) return -1;
+  FILE* f = fopen(path, "r");
+  char line[1024];
+  for (int i = 0; i < 5; ++i) fgets(line, sizeof line, f);
+  fgets(line, sizeof line, f); /* states header */
+  for (int s = 0; s < ns; ++s) {
+    if (!fgets(line, sizeof line, f)) { fclose(f); return -3; }
+    char* p = line;
+    for (int c = 0; c < n_state_cols; ++c) state_cols[(size_t)s * n_state_cols + c] = (int32_t)strtol(p, &p, 10);
+  }
+  fgets(line, sizeof line, f); /* MIJ_INDEX header */
+  for (int64_t k = 0; k < P; ++k) {
+    long long kk; int a, b;
+    if (!fgets(line, sizeof line, f) || sscanf(line, "%lld %d %d", &kk, &a, &b) != 3) { fclose(f); return -4; }
+    ind_mat[2 * k] = a; ind_mat[2 * k + 1] = b;
+  }
+  fgets(line, sizeof line, f); /* #iR header */
+  for (int i = 0; i < nR; ++i) {
+    int ii; double r;
+    if (!fgets(line, sizeof line, f) || sscanf(line, "%d %lf", &ii, &r) != 2) { fclose(f); return -5; }
+    R[i] = r;
+  }
+  fgets(line, sizeof line, f); /* #k_matel header */
+  for (int64_t k = 0; k < P; ++k)
+    for (int i = 0; i < nR; ++i) {
+      long long kk; int ii; double v;
+      if (!fgets(line, sizeof line, f) || sscanf(line, "%lld %d %lf", &kk, &ii, &v) != 3) { fclose(f); return -6; }
+      mat[(size_t)(kk - 1) * nR + (ii - 1)] = v;
+    }
+  fclose(f);
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Propagation.  State vector q (0-based): q[0..N-1] Re a, q[N..2N-1] Im a,
+ * q[2N]=R, q[2N+1]=P_R, q[2N+2]=theta, q[2N+3]=P_theta, q[2N+4]=phi,
+ * q[2N+5]=P_phi, q[2N+6]=q[2N+7]=0 (zero sinks): SRC/mqct_eqtns.f:123,148-161. */
+typedef struct {
+  const orc_tables* tab;
+  int n_u;                 /* unique Delta E count */
+  double* du;              /* unique Delta E values */
+  int32_t* uidx;           /* per pair */
+  double* misc;            /* 4 per pair (Coriolis factors) */
+  double *m, *dm, *phi_amp, *sc;
+} orc_rhs_ws;
+
+/* resize: unique Delta E table (last match within 1e-12 in single precision wins)
+ * and the Coriolis factors misc_bk, SRC/mqct_eqtns.f:1-110. */
+static void orc_ws_init(orc_rhs_ws* w, const orc_tables* t) {
+  int64_t P = t->P;
+  w->tab = t;
+  w->du = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
+  w->uidx = (int32_t*)malloc(sizeof(int32_t) * (size_t)(P > 0 ? P : 1));
+  w->misc = (double*)malloc(sizeof(double) * 4 * (size_t)(P > 0 ? P : 1));
+  w->m = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
+  w->dm = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
+  w->phi_amp = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
+  w->sc = (double*)malloc(sizeof(double) * 2 * (size_t)(P > 0 ? P : 1));
+  const double tol = (double)(float)1.0e-12;
+  int n_u = 0;
+  for (int64_t k = 0; k < P; ++k) {
+    int i = t->ind_mat[2 * k] - 1, j = t->ind_mat[2 * k + 1] - 1;
+    double de = t->ej[j] - t->ej[i];
+    int hit = -1;
+    for (int u = 0; u < n_u; ++u)
+      if (fabs(de - w->du[u]) < tol) hit = u;
+    if (hit < 0) { w->du[n_u] = de; hit = n_u++; }
+    w->uidx[k] = hit;
+    double jj = t->j12[j], mi = t->m12[i];
+    double m1 = mi + 1.0, m0 = mi - 1.0;
+    w->misc[4 * k + 0] = sqrt(jj * (jj + 1.0) - m1 * (m1 - 1.0));
+    w->misc[4 * k + 1] = sqrt(jj * (jj + 1.0) - m0 * (m0 + 1.0));
+    double ji = t->j12[i], mj = t->m12[j];
+    m1 = mj + 1; m0 = mj - 1;
+    w->misc[4 * k + 2] = sqrt(ji * (ji + 1.0) - m1 * (m1 - 1.0));
+    w->misc[4 * k + 3] = sqrt(ji * (ji + 1.0) - m0 * (m0 + 1.0));
+  }
+  w->n_u = n_u;
+}
+static void orc_ws_free(orc_rhs_ws* w) {
+  free(w->du); free(w->uidx); free(w->misc); free(w->m); free(w->dm); free(w->phi_amp); free(w->sc);
+}
+
+/* potential_data_bk + splint_bk: linear extrapolation below R_1, zero above R_n,
+ * cubic spline with derivative in between.  SRC/mqct_eqtns.f:501-611. */
+static void orc_matrix_at(const orc_tables* t, double x, double* m, double* dm) {
+  int nR = t->nR;
+  const double* R = t->R;
+  int64_t P = t->P;
+  if (x < R[0]) {
+    for (int64_t k = 0; k < P; ++k) {
+      const double* c = t->mat + (size_t)k * nR;
+      dm[k] = (c[1] - c[0]) / (R[1] - R[0]);
+      m[k] = dm[k] * (x - R[0]) + c[0];
+    }
+    return;
+  }
+  if (x > R[nR - 1]) {
+    for (int64_t k = 0; k < P; ++k) { m[k] = 0.0; dm[k] = 0.0; }
+    return;
+  }
+  int klo = 1, khi = nR;
+  while (khi - klo > 1) {
+    int kk = (khi + klo) / 2;
+    if (R[kk - 1] > x) khi = kk;
+    else klo = kk;
+  }
+  double h = R[khi - 1] - R[klo - 1];
+  double aa = (R[khi - 1] - x) / h, bb = (x - R[klo - 1]) / h;
+  double cc1 = aa * aa * aa - aa, cc2 = bb * bb * bb - bb;
+  double cc3 = 3 * aa * aa - 1.0, cc4 = 3 * bb * bb - 1.0;
+  double cc5 = (h * h) / 6.0, cc6 = cc5 / h;
+  for (int64_t k = 0; k < P; ++k) {
+    const double* c = t->mat + (size_t)k * nR;
+    const double* y = t->y2 + (size_t)k * nR;
+    double mlo = c[klo - 1], mhi = c[khi - 1], ylo = y[klo - 1], yhi = y[khi - 1];
+    m[k] = aa * mlo + bb * mhi + (cc1 * ylo + cc2 * yhi) * cc5;
+    dm[k] = (mhi - mlo) / h + (-cc3 * ylo + cc4 * yhi) * cc6;
+  }
+}
+
+/* DERIVS_BK for distinguishable particles, full CC, planar motion
+ * (POLAR_ANGLE=NO): SRC/mqct_eqtns.f:112-499. */
+static void orc_derivs_ws(orc_rhs_ws* w, double t, const double* q, double* dq) {
+  const orc_tables* tb = w->tab;
+  int N = tb->n_states;
+  int64_t P = tb->P;
+  double mass = tb->mass_au;
+  for (int i = 0; i < 2 * N + 8; ++i) dq[i] = 0.0;
+  double Rrr = q[2 * N];
+  double tet = q[2 * N + 2];
+  double sin_tet = sin(tet);
+  double dPhidT = q[2 * N + 5] / q[2 * N] / q[2 * N] / mass / (sin_tet * sin_tet);
+  orc_matrix_at(tb, Rrr, w->m, w->dm);
+  for (int u = 0; u < w->n_u; ++u) {
+    w->sc[2 * u] = sin(t * w->du[u]);
+    w->sc[2 * u + 1] = cos(t * w->du[u]);
+  }
+  const int Z1 = 2 * N + 6, Z2 = 2 * N + 7; /* zero sinks */
+  for (int64_t k = 0; k < P; ++k) {
+    int i = tb->ind_mat[2 * k] - 1, j = tb->ind_mat[2 * k + 1] - 1;
+    double M = w->m[k], Md = w->dm[k];
+    double d_f = (i == j) ? 1.0 : 2.0;
+    double iphase = w->sc[2 * w->uidx[k]], rphase = w->sc[2 * w->uidx[k] + 1];
+    double rfp = -d_f * iphase, ifp = d_f * rphase;
+    dq[i] += (q[j] * rfp + q[j + N] * ifp) * M / 2.0;
+    dq[i + N] += (q[j + N] * rfp - q[j] * ifp) * M / 2.0;
+    dq[j] -= (q[i] * rfp - q[i + N] * ifp) * M / 2.0;
+    dq[j + N] -= (q[i + N] * rfp + q[i] * ifp) * M / 2.0;
+    dq[2 * N + 1] -= ((q[i] * q[j] + q[i + N] * q[j + N]) * rphase -
+                      (q[i + N] * q[j] - q[i] * q[j + N]) * iphase) * d_f * Md;
+    const double* mc = w->misc + 4 * k;
+    double amp = 0.0;
+    {
+      int jj = tb->j12[j], mm = tb->m12[i];
+      int s1, s11, s0, s00;
+      if (abs(mm + 1) <= jj) { s1 = j + 1; s11 = s1 + N; } else { s1 = Z1; s11 = Z2; }
+      if (abs(mm - 1) <= jj) { s0 = j - 1; s00 = s0 + N; } else { s0 = Z1; s00 = Z2; }
+      amp = amp - sin_tet * rfp / 2.0 *
+                      (mc[0] * (q[i] * q[s1] + q[i + N] * q[s11]) +
+                       mc[1] * (q[i] * q[s0] + q[i + N] * q[s00])) -
+            sin_tet * (-ifp) / 2.0 *
+                (mc[0] * (q[i + N] * q[s1] - q[i] * q[s11]) +
+                 mc[1] * (q[i + N] * q[s0] - q[i] * q[s00]));
+    }
+    {
+      int jj = tb->j12[i], mm = tb->m12[j];
+      int s1, s11, s0, s00;
+      if (abs(mm + 1) <= jj) { s1 = i + 1; s11 = s1 + N; } else { s1 = Z1; s11 = Z2; }
+      if (abs(mm - 1) <= jj) { s0 = i - 1; s00 = s0 + N; } else { s0 = Z1; s00 = Z2; }
+      amp = amp - sin_tet * (-rfp) / 2.0 *
+                      (mc[2] * (q[s1] * q[j] + q[s11] * q[j + N]) +
+                       mc[3] * (q[s0] * q[j] + q[s00] * q[j + N]));
+      amp = amp - sin_tet * (-ifp) / 2.0 *
+                      (mc[2] * (q[s1] * q[j + N] - q[s11] * q[j]) +
+                       mc[3] * (q[s0] * q[j + N] - q[s00] * q[j]));
+    }
+    w->phi_amp[k] = amp;
+  }
+  double dot = 0.0;
+  for (int64_t k = 0; k < P; ++k) dot += w->m[k] * w->phi_amp[k];
+  dq[2 * N + 5] = dot;
+  for (int i = 0; i < N; ++i) {
+    double jj = tb->j12[i], mm = tb->m12[i];
+    double m1 = mm + 1.0, m0 = mm - 1.0;
+    double sqrt1 = sqrt(jj * (jj + 1.0) - m0 * (m0 + 1.0));
+    double sqrt2 = sqrt(jj * (jj + 1.0) - m1 * (m1 - 1.0));
+    if (i > 0) {
+      dq[i] += dPhidT / 2.0 * sqrt1 * q[i - 1 + N];
+      dq[i + N] -= dPhidT / 2.0 * sqrt1 * q[i - 1];
+    }
+    if (i < N - 1) {
+      dq[i] += dPhidT / 2.0 * sqrt2 * q[i + 1 + N];
+      dq[i + N] -= dPhidT / 2.0 * sqrt2 * q[i + 1];
+    }
+  }
+  dq[2 * N] = q[2 * N + 1] / mass;
+  dq[2 * N + 4] = q[2 * N + 5] / q[2 * N] / q[2 * N] / mass / (sin_tet * sin_tet);
+  dq[2 * N + 1] = dq[2 * N + 1] + q[2 * N + 3] / q[2 * N] / q[2 * N] / mass * q[2 * N + 3] / q[2 * N] +
+                  q[2 * N + 5] / q[2 * N] / q[2 * N] / mass * q[2 * N + 5] / q[2 * N] / (sin_tet * sin_tet);
+}
+
+int orc_derivs(const orc_tables* tab, double t, const double* q, double* dqdt) {
+  orc_rhs_ws w;
+  orc_ws_init(&w, tab);
+  orc_derivs_ws(&w, t, q, dqdt);
+  orc_ws_free(&w);
+  return 0;
+}
+
+/* Classical RK4 step: SRC/suppl_routines.f:1076-1113 (rk4). */
+typedef void (*orc_rhs_fn)(void* ctx, double t, const double* y, double* dy);
+static void orc_rk4(int n, double* y, const double* dydx, double x, double h, orc_rhs_fn f,
+                    void* ctx, double* yt, double* dyt, double* dym) {
+  double hh = h * 0.5, h6 = h / 6.0, xh = x + hh;
+  for (int i = 0; i < n; ++i) yt[i] = y[i] + hh * dydx[i];
+  f(ctx, xh, yt, dyt);
+  for (int i = 0; i < n; ++i) yt[i] = y[i] + hh * dyt[i];
+  f(ctx, xh, yt, dym);
+  for (int i = 0; i < n; ++i) {
+    yt[i] = y[i] + h * dym[i];
+    dym[i] = dyt[i] + dym[i];
+  }
+  f(ctx, x + h, yt, dyt);
+  for (int i = 0; i < n; ++i) y[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
+}
+static void orc_rhs_std(void* ctx, double t, const double* y, double* dy) {
+  orc_derivs_ws((orc_rhs_ws*)ctx, t, y, dy);
+}
+
+/* Coupling energy sum_k d_f M_k Re(a_i* a_j e^{-i dE t}) (SRC/propagator.f:2725-2788). */
+static double orc_pot(orc_rhs_ws* w, double t, double R, const double* q) {
+  const orc_tables* tb = w->tab;
+  int N = tb->n_states;
+  orc_matrix_at(tb, R, w->m, w->dm);
+  double pot = 0.0;
+  for (int64_t k = 0; k < tb->P; ++k) {
+    int i = tb->ind_mat[2 * k] - 1, j = tb->ind_mat[2 * k + 1] - 1;
+    double d = (i == j) ? 1.0 : 2.0;
+    double du = w->du[w->uidx[k]];
+    double ip = sin(t * du), rp = cos(t * du);
+    pot += d * w->m[k] * ((q[i] * q[j] + q[i + N] * q[j + N]) * rp - (q[i + N] * q[j] - q[i] * q[j + N]) * ip);
+  }
+  return pot;
+}
+
+/* DOTRAJECT, standard MQCT with fixed-step RK4: initial conditions
+ * SRC/propagator.f:2435-2566, energies :2695-2810, loop :3205-4050,
+ * final bookkeeping :4182-4383. */
+int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                  double* diag) {
+  int N = tab->n_states;
+  int n = 2 * N + 8;
+  double mass = tab->mass_au;
+  double* q = (double*)calloc((size_t)n, sizeof(double));
+  double* dq = (double*)calloc((size_t)n, sizeof(double));
+  double* yt = (double*)calloc((size_t)n, sizeof(double));
+  double* dyt = (double*)calloc((size_t)n, sizeof(double));
+  double* dym = (double*)calloc((size_t)n, sizeof(double));
+  orc_rhs_ws w;
+  orc_ws_init(&w, tab);
+  double k_vec = sqrt(mass * 2.0 * tr->e_coll);
+  double l_orb = sqrt(tr->l_real * (tr->l_real + 1.0));
+  double R_st = tr->r_start;
+  int status = 0;
+  q[tr->s_st - 1] = 1.0;
+  double tcur = 0.0;
+  int64_t counter = 0;
+  int vib = 0, period = 0;
+  double pot_end = 0.0;
+  double eror = 0.0, norm_err = 0.0;
+  if (l_orb / k_vec > R_st) {
+    status = 2; /* not propagated: impact parameter beyond RMAX */
+    q[2 * N] = R_st;
+  } else {
+    q[2 * N] = R_st;
+    q[2 * N + 1] = -sqrt(k_vec * k_vec - l_orb * l_orb / (R_st * R_st));
+    q[2 * N + 2] = acos(0.0);
+    q[2 * N + 3] = l_orb * sin(0.0);
+    q[2 * N + 4] = 0.0;
+    q[2 * N + 5] = l_orb * cos(0.0);
+    double Eqi = 0.0;
+    for (int i = 0; i < N; ++i) Eqi += (q[i] * q[i] + q[i + N] * q[i + N]) * tab->ej[i];
+    Eqi += orc_pot(&w, tcur, q[2 * N], q);
+    double pr = q[2 * N + 1], l = q[2 * N + 3], ql = q[2 * N + 2], qphi = q[2 * N + 5], R = q[2 * N];
+    double Eki = pr * pr / 2.0 / mass + l * l / 2.0 / mass / (R * R) +
+                 qphi * qphi / 2.0 / mass / (R * R) / (sin(ql) * sin(ql));
+    double tmp_R1 = 0.0, tmp_R2 = 0.0;
+    int run = 1;
+    while (run) {
+      ++counter;
+      if (q[2 * N] != q[2 * N]) { status = 3; break; }
+      orc_derivs_ws(&w, tcur, q, dq);
+      orc_rk4(n, q, dq, tcur, tr->dt, orc_rhs_std, &w, yt, dyt, dym);
+      double uR = q[2 * N], uphi = q[2 * N + 4];
+      if (tcur > (0.0 + tr->dt) && counter > 2) {
+        if ((tmp_R2 - tmp_R1) < 0.0 && (tmp_R1 - uR) > 0.0) vib += 1;
+      }
+      tmp_R2 = tmp_R1;
+      tmp_R1 = uR;
+      tcur += tr->dt;
+      period = (int)(fabs(uphi) / 2.0 / ORC_PI);
+      if (tr->numb_orb_prds <= period) run = 0;
+      if (vib >= tr->numb_oscl_prds) run = 0;
+      if (tr->time_lim > 0 && tcur >= tr->time_lim) run = 0;
+      if (uR > tr->r_fin) run = 0;
+      if (tr->max_steps > 0 && counter >= tr->max_steps && run) { run = 0; status = 1; }
+    }
+    double Eqf = 0.0, Pt = 0.0;
+    for (int i = 0; i < N; ++i) {
+      double p = q[i] * q[i] + q[i + N] * q[i + N];
+      Eqf += p * tab->ej[i];
+      Pt += p;
+    }
+    pr = q[2 * N + 1]; l = q[2 * N + 3]; ql = q[2 * N + 2]; qphi = q[2 * N + 5]; R = q[2 * N];
+    double Ef = pr * pr / 2.0 / mass + l * l / 2.0 / mass / (R * R) +
+                qphi * qphi / 2.0 / mass / (R * R) / (sin(ql) * sin(ql));
+    pot_end = orc_pot(&w, tcur, R, q);
+    eror = fabs(Eqf + Ef + pot_end - Eki - Eqi);
+    norm_err = fabs(1.0 - Pt);
+  }
+  for (int i = 0; i < 2 * N; ++i) amp[i] = q[i];
+  for (int c = 0; c < 6; ++c) cls[c] = q[2 * N + c];
+  diag[0] = tcur; diag[1] = (double)counter; diag[2] = norm_err; diag[3] = eror;
+  diag[4] = status; diag[5] = period; diag[6] = vib; diag[7] = pot_end;
+  orc_ws_free(&w);
+  free(q); free(dq); free(yt); free(dyt); free(dym);
+  return 0;
+}
+
+int orc_propagate_batch(const orc_tables* tab, int n_traj, const orc_traj* trajs, int n_threads,
+                        double* amp, double* cls, double* diag) {
+  int N = tab->n_states;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(n_threads > 0 ? n_threads : omp_get_max_threads())
+  for (int t = 0; t < n_traj; ++t)
+    orc_dotraject(tab, &trajs[t], amp + (size_t)t * 2 * N, cls + (size_t)t * 6, diag + (size_t)t * 8);
+  return 0;
+}
+
+/* AT-MQCT second run: classical path from the saved trajectory splined over t
+ * (end slopes from finite differences), amplitudes by DERIVS_BK_adia with RK4;
+ * the last step is truncated to the final saved time.
+ * SRC/propagator.f:3094-3132, 3862-3881; SRC/mqct_eqtns.f:720-985. */
+typedef struct {
+  orc_rhs_ws* w;
+  int n_at;
+  const double* t;
+  double* col[4];   /* R, theta, P_theta, P_phi */
+  double* col2[4];
+} orc_at_ctx;
+static void orc_rhs_at(void* vctx, double t, const double* q, double* dq) {
+  orc_at_ctx* c = (orc_at_ctx*)vctx;
+  orc_rhs_ws* w = c->w;
+  const orc_tables* tb = w->tab;
+  int N = tb->n_states;
+  double v[4], yp;
+  for (int a = 0; a < 4; ++a) orc_splint(c->t, c->col[a], c->col2[a], c->n_at, t, &v[a], &yp);
+  double Rrr = v[0], tet = v[1], pphi = v[3];
+  double sin_tet = sin(tet);
+  double dPhidT = pphi / Rrr / Rrr / tb->mass_au / (sin_tet * sin_tet);
+  for (int i = 0; i < 2 * N; ++i) dq[i] = 0.0;
+  orc_matrix_at(tb, Rrr, w->m, w->dm);
+  for (int u = 0; u < w->n_u; ++u) {
+    w->sc[2 * u] = sin(t * w->du[u]);
+    w->sc[2 * u + 1] = cos(t * w->du[u]);
+  }
+  for (int64_t k = 0; k < tb->P; ++k) {
+    int i = tb->ind_mat[2 * k] - 1, j = tb->ind_mat[2 * k + 1] - 1;
+    double M = w->m[k];
+    double d_f = (i == j) ? 1.0 : 2.0;
+    double iphase = w->sc[2 * w->uidx[k]], rphase = w->sc[2 * w->uidx[k] + 1];
+    double rfp = -d_f * iphase, ifp = d_f * rphase;
+    dq[i] += (q[j] * rfp + q[j + N] * ifp) * M / 2.0;
+    dq[i + N] += (q[j + N] * rfp - q[j] * ifp) * M / 2.0;
+    dq[j] -= (q[i] * rfp - q[i + N] * ifp) * M / 2.0;
+    dq[j + N] -= (q[i + N] * rfp + q[i] * ifp) * M / 2.0;
+  }
+  for (int i = 0; i < N; ++i) {
+    double jj = tb->j12[i], mm = tb->m12[i];
+    double m1 = mm + 1.0, m0 = mm - 1.0;
+    double sqrt1 = sqrt(jj * (jj + 1.0) - m0 * (m0 + 1.0));
+    double sqrt2 = sqrt(jj * (jj + 1.0) - m1 * (m1 - 1.0));
+    if (i > 0) {
+      dq[i] += dPhidT / 2.0 * sqrt1 * q[i - 1 + N];
+      dq[i + N] -= dPhidT / 2.0 * sqrt1 * q[i - 1];
+    }
+    if (i < N - 1) {
+      dq[i] += dPhidT / 2.0 * sqrt2 * q[i + 1 + N];
+      dq[i + N] -= dPhidT / 2.0 * sqrt2 * q[i + 1];
+    }
+  }
+}
+int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const double* rec,
+                     double* amp, double* diag) {
+  int N = tab->n_states, n = 2 * N;
+  orc_rhs_ws w;
+  orc_ws_init(&w, tab);
+  orc_at_ctx c;
+  c.w = &w;
+  c.n_at = n_at;
+  double* t = (double*)malloc(sizeof(double) * n_at);
+  for (int i = 0; i < n_at; ++i) t[i] = rec[8 * i];
+  c.t = t;
+  const int cols[4] = {1, 3, 4, 6}; /* R, theta, P_theta, P_phi in the record */
+  for (int a = 0; a < 4; ++a) {
+    c.col[a] = (double*)malloc(sizeof(double) * n_at);
+    c.col2[a] = (double*)malloc(sizeof(double) * n_at);
+    for (int i = 0; i < n_at; ++i) c.col[a][i] = rec[8 * i + cols[a]];
+    double yp1 = (c.col[a][1] - c.col[a][0]) / (t[1] - t[0]);
+    double ypn = (c.col[a][n_at - 1] - c.col[a][n_at - 2]) / (t[n_at - 1] - t[n_at - 2]);
+    orc_spline(t, c.col[a], n_at, yp1, ypn, c.col2[a]);
+  }
+  double* q = (double*)calloc((size_t)n, sizeof(double));
+  double* dq = (double*)calloc((size_t)n, sizeof(double));
+  double* yt = (double*)calloc((size_t)n, sizeof(double));
+  double* dyt = (double*)calloc((size_t)n, sizeof(double));
+  double* dym = (double*)calloc((size_t)n, sizeof(double));
+  q[tr->s_st - 1] = 1.0;
+  double tcur = t[0], dt = tr->dt;
+  double t_end = t[n_at - 1];
+  int64_t counter = 0;
+  int run = 1;
+  while (run) {
+    ++counter;
+    if ((tcur + dt) >= t_end) {
+      dt = t_end - tcur;
+      run = 0;
+    }
+    orc_rhs_at(&c, tcur, q, dq);
+    orc_rk4(n, q, dq, tcur, dt, orc_rhs_at, &c, yt, dyt, dym);
+    tcur += dt;
+    if (tr->max_steps > 0 && counter >= tr->max_steps) break;
+  }
+  double Pt = 0.0;
+  for (int i = 0; i < N; ++i) Pt += q[i] * q[i] + q[i + N] * q[i + N];
+  for (int i = 0; i < n; ++i) amp[i] = q[i];
+  diag[0] = tcur; diag[1] = (double)counter; diag[2] = fabs(1.0 - Pt); diag[3] = 0.0;
+  diag[4] = 0; diag[5] = 0; diag[6] = 0; diag[7] = 0;
+  for (int a = 0; a < 4; ++a) { free(c.col[a]); free(c.col2[a]); }
+  free(t); free(q); free(dq); free(yt); free(dyt); free(dym);
+  orc_ws_free(&w);
+  return 0;
+}
+
+/* INELAST_CALC, SRC/propagator.f:4776-4841 with DL=1 (trajectory of l is
+ * index l - L_MIN): sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(l). */
+int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int n_traj,
+                const double* prob, double k_vec, double* sigma) {
+  for (int f = 0; f < n_channels; ++f) {
+    double s = 0.0;
+    for (int J = J_down; J <= J_up; ++J)
+      for (int l = abs(J - j_ini); l <= J + j_ini; ++l) {
+        int id = l - L_min;
+        if (id < 0 || id >= n_traj) continue;
+        s += prob[(size_t)id * n_channels + f] * (2.0 * J + 1.0) / (k_vec * k_vec) /
+             (2.0 * j_ini + 1) * ORC_PI;
+      }
+    sigma[f] = s;
+  }
+  return 0;
+}

@@ -1,0 +1,171 @@
+/*
+ * mqct_oracle.h -- CPU FP64 oracle for the MQCT matrix-build and propagation
+ * hot paths.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain-C restatement of the
+ * reference algorithm (MarquetteQuantum/MQCT, Fortran).  It is the checker
+ * that the CUDA product is compared against; only tests/, the smoke check
+ * and bench.py's CPU-baseline leg may load it.  The product never links it.
+ *
+ * Every routine cites the reference file:line it restates
+ * (paths relative to the MQCT repository; SRC = MQCT_SOURCE_CODES).
+ *
+ * Conventions: indices that cross this ABI in ind_mat / indx_chann are
+ * 1-based (as in the reference); matrices are stored R-fastest
+ * (mat[k*nR + iR]), i.e. the Fortran column-major Mat_el(n_r, P).
+ */
+#ifndef MQCT_ORACLE_H
+#define MQCT_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- numerics (SRC/suppl_routines.f) ---------------- */
+void   orc_gauleg(int n, double* x, double* w);
+double orc_plgndr(int l, int m, double x);
+void   orc_jacobi_poly(int n, double a, double b, double x, double* cx);
+double orc_w3js(int j1, int j2, int j3, int m1, int m2, int m3); /* doubled args */
+double orc_cg(int j1, int j2, int j3, int m1, int m2, int m3);
+void   orc_spline(const double* x, const double* y, int n, double yp1, double ypn, double* y2);
+void   orc_splint(const double* xa, const double* ya, const double* y2a, int n,
+                  double x, double* y, double* yprime);
+
+/* ---------------- rotor functions ---------------- */
+void orc_djkm(int j, int k, int m, double alpha, double beta, double gamma,
+              double* re, double* im);
+void orc_wf_diat(int j, int m, double theta, double phi, double* re, double* im);
+/* Rigid asymmetric-top level (j, ka, kc): energy (same units as A,B,C) and the
+ * (2j+1) symmetric-top coefficients ordered K=-j..j.  Returns 0 or <0. */
+int  orc_asym_top(double A, double B, double C, int j, int ka, int kc,
+                  double* energy, double* vec);
+void orc_wf_asym(int j, const double* coeff, int m, double alpha, double beta,
+                 double gamma, double* re, double* im);
+
+/* ---------------- system / states (SRC/matrix_ini.f) ---------------- */
+typedef struct orc_system {
+  int32_t sys_type;      /* 1 diatom+atom, 4 asym top+atom, 8 asym top+diatom, 0 asym+asym */
+  int32_t n_channels;
+  const int32_t* j1;     /* per channel: j (type 1,4) or j1 (type 8,0) */
+  const int32_t* ka1;
+  const int32_t* kc1;
+  const int32_t* j2;     /* type 8, 0 */
+  const int32_t* ka2;    /* type 0 */
+  const int32_t* kc2;
+  const double* e_ch;    /* channel energies, cm^-1 */
+  const double* vec1;    /* eigenvectors of rotor 1, per channel, stride ldv (K=-j..j) */
+  const double* vec2;    /* eigenvectors of rotor 2 (type 0) */
+  int32_t ldv;
+} orc_system;
+
+int orc_count_states(const orc_system* sys);
+/* Fills indx_chann (1-based), j12, m12, Ej (cm^-1) for n states. */
+int orc_enumerate_states(const orc_system* sys, int32_t* indx_chann, int32_t* j12,
+                         int32_t* m12, double* ej);
+int64_t orc_count_pairs(int n_states, const int32_t* m12);
+int64_t orc_ind_mat(int n_states, const int32_t* m12, int32_t* ind_mat /* 2*P */);
+
+void orc_rgrid(int n, double rmin, double rmax, int equidistant, double* R);
+
+/* ---------------- synthetic PES (the plugin USER_DEFINED_PES) ---------------- */
+enum { ORC_PES_LEGENDRE = 1, ORC_PES_SITES1 = 2, ORC_PES_SITES2 = 3, ORC_PES_TABLE = 0 };
+typedef struct orc_pes {
+  int32_t kind;
+  int32_t n_terms;
+  const double* p;       /* kind-specific parameter block, see oracle source */
+  int32_t n_sites1, n_sites2;
+  const double* sites1;  /* xyz per site, body frame of rotor 1 */
+  const double* sites2;
+  const double* table;   /* kind TABLE: V[iR][g] over the full angular grid */
+} orc_pes;
+/* USER_DEFINED_PES(V,R,rvib,rvib2,alpha,beta,gamma,aalpha,bbeta,ggamma) */
+double orc_pes_eval(const orc_pes* pes, double R, double alpha, double beta, double gamma,
+                    double aalpha, double bbeta, double ggamma);
+
+/* ---------------- matrix build (SRC/matrix_ini.f MATRIX_MAKE, SRC/pot_comp.f) ---- */
+typedef struct orc_grid {
+  int32_t n_beta, n_gamma, n_alpha;      /* type 1: n_beta; type 4: beta x gamma (x alpha) */
+  int32_t n_beta2, n_alpha2, n_gamma2;   /* type 0: beta1=n_beta, gamma1=n_gamma */
+  int32_t eq_gamma;                      /* EQ_ANG_GRID (default 1): midpoint gamma/alpha grids */
+} orc_grid;
+
+/* Full build: Mat_el (Hartree) and spline second derivatives, MIJ_CUTOFF
+ * truncation.  literal != 0 re-evaluates the rotor wavefunctions at every
+ * grid point for every (k, R) exactly as INTEGRATOR_TEMP does (the reference
+ * cost); literal == 0 tabulates them once (same arithmetic per point).
+ * k_begin/k_end restrict the elements computed (others left untouched).
+ * n_threads <= 0 uses all OpenMP threads.  Returns 0 or <0. */
+int orc_build_matrix(const orc_system* sys, int n_states, const int32_t* indx_chann,
+                     const int32_t* j12, const int32_t* m12, int64_t P,
+                     const int32_t* ind_mat, int nR, const double* R,
+                     const orc_grid* grid, const orc_pes* pes,
+                     double mij_cut_cm, double r_cut1, double r_cut2, int literal,
+                     int64_t k_begin, int64_t k_end, int n_threads,
+                     double* mat, double* y2, int32_t* skipped);
+/* Only the quadrature (no cutoff/spline), values in cm^-1, for timing samples. */
+int orc_integrate_elements(const orc_system* sys, int n_states, const int32_t* indx_chann,
+                           const int32_t* j12, const int32_t* m12, int64_t P,
+                           const int32_t* ind_mat, int nR, const double* R,
+                           const orc_grid* grid, const orc_pes* pes, int literal,
+                           int64_t k_begin, int64_t k_end, int iR_begin, int iR_end,
+                           int n_threads, double* mat);
+
+/* ---------------- MTRX_UF.DAT / MTRX.DAT (SRC/matrix_ini.f) ---------------- */
+int orc_write_mtrx_uf(const char* path, int coll_type, int n_channels, int n_states,
+                      const int32_t* state_rec, int state_rec_len, int64_t P,
+                      const int32_t* ind_mat, int nR, const double* R, const double* mat);
+/* Formatted MTRX.DAT reader (header counts first, then arrays). */
+int orc_read_mtrx_dat_header(const char* path, int* coll_type, int* n_channels,
+                             int* n_states, int64_t* P, int* nR);
+int orc_read_mtrx_dat(const char* path, int n_state_cols, int32_t* state_cols,
+                      int32_t* ind_mat, double* R, double* mat);
+
+/* ---------------- propagation (SRC/mqct_eqtns.f, SRC/propagator.f) ---------- */
+typedef struct orc_tables {
+  int32_t n_states;
+  const int32_t* j12;
+  const int32_t* m12;
+  const double* ej;        /* Hartree */
+  int64_t P;
+  const int32_t* ind_mat;  /* 2*P, 1-based, only the retained (non-truncated) pairs */
+  int32_t nR;
+  const double* R;
+  const double* mat;       /* P x nR (R fastest), Hartree */
+  const double* y2;        /* spline second derivatives, same layout */
+  double mass_au;          /* reduced mass, electron masses */
+} orc_tables;
+
+typedef struct orc_traj {
+  double e_coll;           /* Hartree */
+  double l_real;           /* orbital angular momentum quantum number (float) */
+  int32_t s_st;            /* initial state, 1-based */
+  double dt;               /* atomic units */
+  double r_start;          /* R at t=0 (RMAX) */
+  double r_fin;            /* stop when R > r_fin */
+  int32_t numb_orb_prds;   /* stop after this many orbits (default 1) */
+  int32_t numb_oscl_prds;  /* stop after this many R oscillations (default 1) */
+  double time_lim;         /* <=0: none */
+  int64_t max_steps;
+} orc_traj;
+
+/* Per-trajectory output: amp[2N] (Re, Im), cls[6] = (R,P_R,theta,P_theta,phi,P_phi),
+ * diag[8] = (t_end, steps, norm_err, energy_err, status, orbit_cnt, vib_cnt, pot_end). */
+int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                  double* diag);
+int orc_propagate_batch(const orc_tables* tab, int n_traj, const orc_traj* trajs,
+                        int n_threads, double* amp, double* cls, double* diag);
+/* AT-MQCT: classical path given as n_at records (t,R,P_R,theta,P_theta,phi,P_phi,pot). */
+int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at,
+                     const double* at_rec, double* amp, double* diag);
+/* One RHS evaluation of DERIVS_BK (for unit checks); q, dqdt have 2N+8 entries. */
+int orc_derivs(const orc_tables* tab, double t, const double* q, double* dqdt);
+
+/* INELAST_CALC for one initial (j, m) block with integer l = L_MIN..L_MAX step 1:
+ * prob[n_traj*n_channels] -> sigma_bohr2[n_channels] (pi/k^2 * sum (2J+1)/(2j+1) P). */
+int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int n_traj,
+                const double* prob, double k_vec, double* sigma);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,104 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference's own
+example outputs (EXAMPLES_IO of MarquetteQuantum/MQCT).
+
+Run where the reference tree is available:
+    python tests/golden/make_golden.py /path/to/MQCT
+The fixtures are small numpy archives; tests read only the archives, so they
+also run where the reference tree is absent.
+"""
+from __future__ import annotations
+
+import os
+import struct
+import sys
+
+import numpy as np
+
+
+def _read_mtrx_dat(path, n_cols):
+    with open(path) as f:
+        lines = f.read().splitlines()
+    hdr = [int(lines[i].split("=")[1]) for i in range(5)]
+    coll, nch, ns, P, nR = hdr
+    p = 6
+    states = np.array([[int(x) for x in lines[p + s].split()[:n_cols]] for s in range(ns)],
+                      dtype=np.int32)
+    p += ns + 1
+    ind = np.array([[int(x) for x in lines[p + k].split()[1:3]] for k in range(P)], dtype=np.int32)
+    p += P + 1
+    R = np.array([float(lines[p + i].split()[1]) for i in range(nR)])
+    p += nR + 1
+    mat = np.zeros((P, nR))
+    for q in range(P * nR):
+        t = lines[p + q].split()
+        mat[int(t[0]) - 1, int(t[1]) - 1] = float(t[2])
+    return coll, nch, states, ind, R, mat
+
+
+def _read_table(path, ncols, first_int=True):
+    rows = []
+    for line in open(path):
+        t = line.split()
+        if len(t) == ncols and t[0 if not first_int else 1].replace(".", "").isdigit():
+            try:
+                rows.append([float(x) for x in t])
+            except ValueError:
+                pass
+    return np.array(rows)
+
+
+def main(ref_root):
+    ex = os.path.join(ref_root, "EXAMPLES_IO")
+    out = os.path.dirname(os.path.abspath(__file__))
+
+    # G3: asymmetric top + diatom (SYS_TYPE 8), H2O+H2, matrix read -> dynamics.
+    d = os.path.join(ex, "SYS_TYPE_8", "H2O_H2_Dynamics")
+    coll, nch, states, ind, R, mat = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 8)
+    opac = _read_table(os.path.join(d, "OPACITY_FUNCTIONS_L.out"), 2 + nch)
+    defl = _read_table(os.path.join(d, "DEFLECTION_FUNCTION.out"), 9, first_int=False)
+    sig = []
+    for line in open(os.path.join(d, "CROSS_SECTIONS.out")):
+        t = line.split()
+        if len(t) == 5 and t[0].isdigit():
+            sig.append(float(t[2]))
+    np.savez_compressed(
+        os.path.join(out, "g3_h2o_h2_type8.npz"), coll=coll, states=states, ind_mat=ind, R=R,
+        mat=mat, opacity=opac, deflection=defl, sigma_U=np.array(sig),
+        # $BASIS/$SYSTEM of H2OH2.inp
+        A=27.88063134, B=9.277708381, C=14.52176959, BE=60.853, mass_red=1.812773730,
+        rmax=30.0, time_step=10.0, U=800.0, b_impct=25.0, time_lim=3.5e6,
+        channels=np.array([[0, 0, 0, 0], [1, 1, 1, 0], [2, 0, 2, 0], [2, 1, 1, 0], [1, 0, 1, 1],
+                           [1, 1, 0, 1], [2, 1, 2, 1], [2, 2, 1, 1], [3, 1, 2, 1], [3, 2, 1, 1]],
+                          dtype=np.int32),
+        # CHANNELS ENERGIES, CM-1 printed in USER_INPUT_CHECK.out (3 decimals)
+        e_ch_printed=np.array([0.000, 37.158, 70.133, 95.245, 145.505, 164.108, 201.219, 257.028,
+                               295.304, 334.334]))
+
+    # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
+    d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
+    coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)
+    np.savez_compressed(os.path.join(out, "g4_type4_layout.npz"), states=states4, ind_mat=ind4,
+                        R=R4, mat=mat4, A=0.6666525, B=0.1769383, C=0.2306476,
+                        channels=np.array([[0, 0, 0], [1, 0, 1], [1, 1, 1]], dtype=np.int32),
+                        e_ch_printed=np.array([0.000, 0.408, 0.844]))
+
+    # G1 AT trajectory record layout: Fortran unformatted, 8 float64 per record.
+    d = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_AT_Approximation", "AT_MQCT_2nd_Step",
+                     "AT_APPROX_TRAJS", "500.00000", "0", "0")
+    raw = open(os.path.join(d, "AT_0_0_9_0"), "rb").read()
+    cnt = struct.unpack("<iii", open(os.path.join(d, "n_AT_0_0_9_0"), "rb").read())[1]
+    recs = []
+    off = 0
+    while off < len(raw):
+        n = struct.unpack_from("<i", raw, off)[0]
+        recs.append(struct.unpack_from("<8d", raw, off + 4))
+        off += n + 8
+    recs = np.array(recs)
+    np.savez_compressed(os.path.join(out, "g1_at_traj_l9.npz"), n_records=cnt,
+                        head=recs[:8], tail=recs[-4:], n_file=len(recs),
+                        t_span=np.array([recs[0, 0], recs[-1, 0]]))
+    print("fixtures written to", out)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
