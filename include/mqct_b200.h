@@ -1,0 +1,252 @@
+/*
+ * mqct_b200.h -- C ABI of the B200-native MQCT hot paths.
+ *
+ * Two entry points replace the reference's two hot loops:
+ *   mqct_build_matrix    <- the DO k / DO i / CALL INTEGRATOR_TEMP loop and the
+ *                           spline loop of MATRIX_MAKE
+ *                           (MQCT_SOURCE_CODES/matrix_ini.f:1920-2016,
+ *                            integrand MQCT_SOURCE_CODES/pot_comp.f:1790-3737)
+ *   mqct_propagate_batch <- the DO itraject / CALL DOTRAJECT loop of PROPAGATE
+ *                           (MQCT_SOURCE_CODES/propagator.f:885-899, DOTRAJECT
+ *                            :2283-4645, RHS MQCT_SOURCE_CODES/mqct_eqtns.f:112-985)
+ * plus the matrix-file formats of the SAVE_MTRX/READ_MTRX flow
+ * (MTRX_UF.DAT: MQCT_SOURCE_CODES/matrix_ini.f:6640-6780 and :5794-6630).
+ *
+ * Conventions shared with the reference so a Fortran iso_c_binding shim can
+ * pass its arrays unchanged:
+ *   - ind_mat is the reference's ind_mat(2,P): pairs (st1, st2), 1-based,
+ *     st2 <= st1, equal m12 (MQCT_SOURCE_CODES/matrix_ini.f:553-627);
+ *   - Mat_el / Mat_el_der are column-major (n_R, P): element k at R index i is
+ *     mat[k*nR + i]; energies in Hartree, distances in bohr;
+ *   - all buffers are owned by the caller (host memory unless a function says
+ *     "device"); the library never frees caller memory;
+ *   - every function returns MQCT_OK (0) or a negative MQCT_E_* code and never
+ *     exits; mqct_last_error() gives a message for the calling thread.
+ * The library needs a CUDA device; there is no CPU fallback.
+ */
+#ifndef MQCT_B200_H
+#define MQCT_B200_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MQCT_OK 0
+#define MQCT_E_ARG (-1)       /* invalid argument / inconsistent sizes        */
+#define MQCT_E_CUDA (-2)      /* CUDA runtime error                           */
+#define MQCT_E_NODEV (-3)     /* no CUDA device / extension not usable        */
+#define MQCT_E_IO (-4)        /* file I/O or malformed matrix file            */
+#define MQCT_E_RANGE (-5)     /* size beyond a documented limit               */
+#define MQCT_E_DEVICE (-6)    /* a device-side check failed (status word set) */
+
+/* SYS_TYPE values handled (MQCT_SOURCE_CODES/iotest.f $BASIS SYS_TYPE). */
+#define MQCT_SYS_DIATOM_ATOM 1
+#define MQCT_SYS_ASYM_ATOM 4
+#define MQCT_SYS_ASYM_DIATOM 8
+#define MQCT_SYS_ASYM_ASYM 0
+
+/* Contraction precision of the matrix build. */
+#define MQCT_PREC_FP64 0      /* plain FP64 CUDA-core form                    */
+#define MQCT_PREC_BF16X3 1    /* tcgen05 kind::f16, BF16 hi/lo split, FP32 acc */
+
+/* Propagation arithmetic. */
+#define MQCT_PROP_FP64 0      /* FP64 amplitudes and tables                   */
+#define MQCT_PROP_FP32 1      /* FP32 amplitude RHS and tables, FP64 phases,
+                                 FP64 classical variables and RK4 state        */
+
+/* Propagation modes. */
+#define MQCT_MODE_STD 0       /* Ehrenfest MQCT: classical and quantum coupled */
+#define MQCT_MODE_AT 1        /* AT-MQCT: classical path given                 */
+
+const char* mqct_last_error(void);
+int mqct_version(void);                 /* MAJOR*10000 + MINOR*100 + PATCH */
+int mqct_device_count(void);
+
+/* Collision system after INI_ARRAYS (MQCT_SOURCE_CODES/matrix_ini.f:1-806). */
+typedef struct mqct_sys_t {
+  int32_t sys_type;          /* MQCT_SYS_*                                       */
+  int32_t n_channels;
+  const int32_t* j1;         /* per channel: j (types 1, 4) or j1 (types 8, 0)   */
+  const int32_t* ka1;
+  const int32_t* kc1;
+  const int32_t* j2;         /* types 8, 0                                       */
+  const int32_t* ka2;        /* type 0                                           */
+  const int32_t* kc2;
+  const double* vec1;        /* rotor-1 eigenvectors, channel-major, stride ldv,
+                                components K=-j..j (M_VECTORS of
+                                MQCT_SOURCE_CODES/pot_comp.f:121-175)            */
+  const double* vec2;        /* rotor-2 eigenvectors (type 0)                    */
+  int32_t ldv;
+  int32_t n_states;
+  const int32_t* indx_chann; /* per state, 1-based channel                       */
+  const int32_t* j12;
+  const int32_t* m12;
+} mqct_sys_t;
+
+/* Angular quadrature (INI_POT_STORAGE, MQCT_SOURCE_CODES/pot_comp.f:333-1788):
+ * GL beta grids on [0,pi]; gamma/alpha grids midpoint-equidistant on [0,2pi]
+ * when eq_gamma (EQ_ANG_GRID=YES, the default) else GL.  Type 4 with
+ * n_alpha = 0 integrates alpha analytically (factor 2*pi) as the reference
+ * does; n_alpha > 0 contracts an explicit alpha grid. */
+typedef struct mqct_grid_t {
+  int32_t n_beta, n_gamma, n_alpha;
+  int32_t n_beta2, n_alpha2, n_gamma2;   /* type 0 */
+  int32_t eq_gamma;
+} mqct_grid_t;
+
+/* Potential energy surface (the USER_DEFINED_PES plugin, called through the
+ * per-type wrappers of MQCT_SOURCE_CODES/pes_sys_type.f:2-97).  Values in
+ * cm^-1, R in bohr.
+ *   TABLE:    caller-evaluated V on the grid, table[iR*K + g] (K grid points in
+ *             the library's grid order: beta outer, gamma, alpha inner), the
+ *             analogue of the reference's VGRID_UF.DAT path;
+ *   LEGENDRE: V(R,beta) = sum_l [A_l e^{-b_l R} - C_l/R^6] P_l(cos beta),
+ *             params = [A_0..A_{n-1}, b_0.., C_0..];
+ *   SITES1:   rigid-rotor sites + atom, per term [site, D, a, re, C6, rd]:
+ *             D(e^{-2a(r-re)} - 2e^{-a(r-re)}) - C6 (1 - e^{-(r/rd)^6}) / r^6;
+ *   SITES2:   two rigid rotors, per term [site1, site2, D, a, re, C6, rd]. */
+#define MQCT_PES_TABLE 0
+#define MQCT_PES_LEGENDRE 1
+#define MQCT_PES_SITES1 2
+#define MQCT_PES_SITES2 3
+typedef struct mqct_pes_t {
+  int32_t kind;
+  int32_t n_terms;
+  const double* params;
+  int32_t n_sites1, n_sites2;
+  const double* sites1;      /* xyz per site, bohr */
+  const double* sites2;
+  const double* table;
+} mqct_pes_t;
+
+/* Accuracy report of a split-precision build against an FP64 build of sampled
+ * elements (optional, may be NULL). */
+typedef struct mqct_err_report_t {
+  int32_t n_sampled;         /* in: elements to sample (0 = none)              */
+  double max_abs_err;        /* out, Hartree                                   */
+  double max_rel_err;        /* out, |d|/max(|M|, 1e-8 max|M| of the element)  */
+  double rms_rel_err;        /* out                                            */
+} mqct_err_report_t;
+
+/* Matrix build: M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
+ * (MQCT_SOURCE_CODES/pot_comp.f:1947-1952, 2535-2557, 3709-3721), converted to
+ * Hartree, MIJ_CUTOFF truncation at R~r_cut1/r_cut2
+ * (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997, columns whose max |M| there is
+ * below mij_cutoff_cm are zeroed and flagged in skipped[k]) and clamped-spline
+ * second derivatives with finite-difference end slopes (:2005-2016).
+ * Mat_el, Mat_el_y2: host, nR*P doubles; skipped: host, P int32 (may be NULL). */
+int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                      const double* R, int32_t nR, const mqct_grid_t* grid,
+                      const mqct_pes_t* pes, int32_t precision, double mij_cutoff_cm,
+                      double r_cut1, double r_cut2, double* Mat_el, double* Mat_el_y2,
+                      int32_t* skipped, mqct_err_report_t* err);
+
+/* Device-resident form of the same build for callers that keep the matrix on
+ * the GPU: a plan uploads the system once; execute writes Mat_el and y2 into
+ * device buffers (nR*P doubles each, may be NULL for y2) on the plan's stream. */
+typedef struct mqct_matrix_plan mqct_matrix_plan;
+int mqct_matrix_plan_create(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                            const double* R, int32_t nR, const mqct_grid_t* grid,
+                            const mqct_pes_t* pes, int32_t precision, double mij_cutoff_cm,
+                            double r_cut1, double r_cut2, mqct_matrix_plan** plan);
+int mqct_matrix_plan_execute(mqct_matrix_plan* plan, double* d_mat, double* d_y2,
+                             int32_t* d_skipped);
+int mqct_matrix_plan_sync(mqct_matrix_plan* plan);
+/* Flops of the contraction actually executed per build (2*P*nR*K times the
+ * number of split-precision products). */
+double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
+void mqct_matrix_plan_destroy(mqct_matrix_plan* plan);
+
+/* Propagation tables after READ_MIJ / MATRIX_MAKE: the retained pairs only
+ * (elements dropped by MIJ_CUTOFF removed, MQCT_SOURCE_CODES/matrix_ini.f:4309-4378),
+ * Mat_el already shifted when MIJ_SHIFT is on (:4270-4273). */
+typedef struct mqct_tables_t {
+  int32_t n_states;
+  const int32_t* j12;
+  const int32_t* m12;
+  const double* ej;          /* Hartree, per state                              */
+  int64_t P;
+  const int32_t* ind_mat;    /* 2*P, 1-based                                    */
+  int32_t nR;
+  const double* R;
+  const double* mat;         /* P x nR, Hartree                                 */
+  const double* y2;          /* spline second derivatives, same layout          */
+  double mass_au;            /* reduced mass in electron masses                 */
+} mqct_tables_t;
+
+/* One trajectory (DOTRAJECT initial conditions MQCT_SOURCE_CODES/propagator.f:2435-2566
+ * and stop rules :4033-4050). */
+typedef struct mqct_traj_init_t {
+  double e_coll;             /* collision energy, Hartree                       */
+  double l_real;             /* orbital angular momentum quantum number         */
+  int32_t s_st;              /* initial state, 1-based                          */
+  double dt;                 /* RK4 step, a.u.                                  */
+  double r_start;            /* R at t=0 (RMAX)                                 */
+  double r_fin;              /* stop when R > r_fin                             */
+  int32_t numb_orb_prds;     /* stop after this many orbits (reference default 1) */
+  int32_t numb_oscl_prds;    /* stop after this many R oscillations (default 1) */
+  double time_lim;           /* <= 0: none                                      */
+  int64_t max_steps;         /* device step cap; reaching it sets status 1      */
+} mqct_traj_init_t;
+
+/* AT-MQCT classical paths: per trajectory n_rec[t] records of
+ * (t, R, P_R, theta, P_theta, phi, P_phi, pot), concatenated in rec with
+ * offsets rec_off[t] (in records). */
+typedef struct mqct_at_paths_t {
+  const int64_t* rec_off;
+  const int32_t* n_rec;
+  const double* rec;
+} mqct_at_paths_t;
+
+/* Batched propagation.  amp_out: n_traj x 2N (Re a, Im a); cls_out: n_traj x 6
+ * (R, P_R, theta, P_theta, phi, P_phi); diag_out: n_traj x 8 (t_end, steps,
+ * |1-norm|, |energy error| Hartree, status, orbits, oscillations, coupling
+ * energy at the end).  status: 0 finished, 1 step cap reached, 2 not
+ * propagated (impact parameter beyond RMAX), 3 non-finite state. */
+int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
+                         int64_t n_traj, int32_t mode, const mqct_at_paths_t* at,
+                         int32_t arith, double* amp_out, double* cls_out, double* diag_out);
+
+/* Device-resident propagation plan (tables uploaded once; trajectories given
+ * per call).  run() uses host trajectory/out buffers; run_device() takes device
+ * buffers for init (n_traj mqct_traj_init_t) and outputs. */
+typedef struct mqct_prop_plan mqct_prop_plan;
+int mqct_prop_plan_create(const mqct_tables_t* tab, int32_t arith, mqct_prop_plan** plan);
+int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,
+                       double* amp_out, double* cls_out, double* diag_out);
+int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_init,
+                              int64_t n_traj, double* d_amp, double* d_cls, double* d_diag);
+int mqct_prop_plan_sync(mqct_prop_plan* plan);
+/* Algorithmic table bytes per trajectory step (16 * P for FP32, 32 * P for FP64). */
+double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan);
+void mqct_prop_plan_destroy(mqct_prop_plan* plan);
+
+/* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
+int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,
+                        double* energy, double* vec);
+int mqct_count_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
+                      const int32_t* j2);
+int mqct_enumerate_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
+                          const int32_t* j2, int32_t* indx_chann, int32_t* j12, int32_t* m12);
+int64_t mqct_count_pairs(int32_t n_states, const int32_t* m12);
+int64_t mqct_fill_ind_mat(int32_t n_states, const int32_t* m12, int32_t* ind_mat);
+int mqct_r_grid(int32_t n, double rmin, double rmax, int32_t equidistant, double* R);
+
+/* MTRX_UF.DAT (Fortran unformatted sequential, 4-byte record markers):
+ * header (coll_type, n_channels, n_states, P, nR), n_states state records of
+ * state_rec_len int32, P records (k, st1, st2), nR records (i, R), then per k
+ * a record (k) and a record Mat_el(:,k). */
+int mqct_write_mtrx_uf(const char* path, int32_t coll_type, int32_t n_channels,
+                       int32_t n_states, const int32_t* state_rec, int32_t state_rec_len,
+                       int64_t P, const int32_t* ind_mat, int32_t nR, const double* R,
+                       const double* mat);
+int mqct_read_mtrx_uf_header(const char* path, int32_t* coll_type, int32_t* n_channels,
+                             int32_t* n_states, int64_t* P, int32_t* nR,
+                             int32_t* state_rec_len);
+int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_rec,
+                      int32_t* ind_mat, double* R, double* mat);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

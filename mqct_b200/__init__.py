@@ -1,0 +1,452 @@
+"""mqct_b200 -- B200-native matrix build and trajectory propagation for MQCT.
+
+Host API mirroring the reference's flow (MarquetteQuantum/MQCT):
+
+    $BASIS    -> CollisionSystem        (channels, levels, INI_ARRAYS states/pairs)
+    $POTENTIAL-> build_matrix / MatrixPlan (MATRIX_MAKE direct integration, CUDA)
+              -> write_mtrx_uf / read_mtrx_uf (SAVE_MTRX / READ_MTRX, MTRX_UF.DAT)
+    $SYSTEM   -> PropagationTables + trajectory_set + propagate (PROPAGATE/DOTRAJECT, CUDA)
+              -> cross_sections (INELAST_CALC + the Billing correction)
+
+All compute runs in libmqct_b200.so (include/mqct_b200.h); this module only
+prepares host arrays and calls the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
+                   check, lib, ptr)
+from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
+
+__all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
+           "PropagationPlan", "trajectory_set", "cross_sections", "write_mtrx_uf",
+           "read_mtrx_uf", "spline_y2", "MqctError", "PREC_FP64", "PREC_BF16X3", "PROP_FP32",
+           "PROP_FP64", "MODE_STD", "MODE_AT"]
+
+
+def asym_top_level(A, B, Cc, j, ka, kc):
+    """Energy and symmetric-top coefficients (K=-j..j) of level (j, ka, kc)."""
+    e = C.c_double()
+    v = np.zeros(2 * j + 1)
+    check(lib().mqct_asym_top_level(A, B, Cc, j, ka, kc, C.byref(e), v))
+    return e.value, v
+
+
+class CollisionSystem:
+    """Collision system after the $BASIS block and INI_ARRAYS.
+
+    sys_type 1: channels (j,), energy BE j(j+1) - DE (j(j+1))^2 (MQCT_SOURCE_CODES/iotest.f:5454);
+    sys_type 4: channels (j, ka, kc), energy EIGEN_VAL(A,B,C) (MQCT_SOURCE_CODES/iotest.f:6611-6618);
+    sys_type 8: channels (j1, ka1, kc1, j2), EIGEN_VAL + BE j2(j2+1) (MQCT_SOURCE_CODES/iotest.f:9069-9079);
+    sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..).
+    """
+
+    def __init__(self, sys_type, channels, A=0.0, B=0.0, C=0.0, BE=0.0, DE=0.0, A2=None,
+                 B2=None, C2=None, e_ch=None):
+        ch = np.asarray(channels, dtype=np.int32)
+        if ch.ndim == 1:
+            ch = ch[:, None]
+        self.sys_type = int(sys_type)
+        self.channels = ch
+        nch = len(ch)
+        self.n_channels = nch
+        z = np.zeros(nch, np.int32)
+        self.j1 = np.ascontiguousarray(ch[:, 0])
+        self.ka1 = self.kc1 = self.j2 = self.ka2 = self.kc2 = z
+        jmax = int(ch[:, 0].max()) if sys_type in (1, 4) else int(max(ch[:, 0].max(), ch[:, 3].max()))
+        self.ldv = 2 * jmax + 1
+        self.vec1 = np.zeros((nch, self.ldv))
+        self.vec2 = np.zeros((nch, self.ldv))
+        E = np.zeros(nch)
+        if sys_type == 1:
+            jj = self.j1 * (self.j1 + 1.0)
+            E = BE * jj - DE * jj ** 2
+            self.vec1[:, 0] = 1.0
+        elif sys_type in (4, 8):
+            self.ka1 = np.ascontiguousarray(ch[:, 1])
+            self.kc1 = np.ascontiguousarray(ch[:, 2])
+            for i in range(nch):
+                e, v = asym_top_level(A, B, C, int(ch[i, 0]), int(ch[i, 1]), int(ch[i, 2]))
+                E[i] = e
+                self.vec1[i, :len(v)] = v
+            if sys_type == 8:
+                self.j2 = np.ascontiguousarray(ch[:, 3])
+                jj = self.j2 * (self.j2 + 1.0)
+                E = E + BE * jj - DE * jj ** 2
+        elif sys_type == 0:
+            self.ka1, self.kc1 = np.ascontiguousarray(ch[:, 1]), np.ascontiguousarray(ch[:, 2])
+            self.j2, self.ka2, self.kc2 = (np.ascontiguousarray(ch[:, 3]),
+                                           np.ascontiguousarray(ch[:, 4]),
+                                           np.ascontiguousarray(ch[:, 5]))
+            A2 = A if A2 is None else A2
+            B2 = B if B2 is None else B2
+            C2 = C if C2 is None else C2
+            for i in range(nch):
+                e1, v1 = asym_top_level(A, B, C, *map(int, ch[i, 0:3]))
+                e2, v2 = asym_top_level(A2, B2, C2, *map(int, ch[i, 3:6]))
+                E[i] = e1 + e2
+                self.vec1[i, :len(v1)] = v1
+                self.vec2[i, :len(v2)] = v2
+        else:
+            raise ValueError(f"unsupported SYS_TYPE {sys_type}")
+        self.e_ch = np.asarray(E if e_ch is None else e_ch, dtype=np.float64)
+        L = lib()
+        j2p = ptr(self.j2) if sys_type in (8, 0) else None
+        n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
+        self.indx_chann = np.zeros(n, np.int32)
+        self.j12 = np.zeros(n, np.int32)
+        self.m12 = np.zeros(n, np.int32)
+        check(L.mqct_enumerate_states(self.sys_type, nch, self.j1, j2p, self.indx_chann,
+                                      self.j12, self.m12))
+        self.n_states = n
+        self.ej_cm = self.e_ch[self.indx_chann - 1]
+        P = check(L.mqct_count_pairs(n, self.m12))
+        ind = np.zeros(2 * P, np.int32)
+        check(L.mqct_fill_ind_mat(n, self.m12, ind))
+        self.ind_mat = ind.reshape(P, 2)
+        self.P = int(P)
+        self.vec1 = np.ascontiguousarray(self.vec1)
+        self.vec2 = np.ascontiguousarray(self.vec2)
+
+    def c_struct(self):
+        return _abi.Sys(self.sys_type, self.n_channels, ptr(self.j1), ptr(self.ka1), ptr(self.kc1),
+                        ptr(self.j2), ptr(self.ka2), ptr(self.kc2), ptr(self.vec1),
+                        ptr(self.vec2), self.ldv, self.n_states, ptr(self.indx_chann),
+                        ptr(self.j12), ptr(self.m12))
+
+    def state_records(self):
+        """Per-state records of MTRX_UF.DAT (MQCT_SOURCE_CODES/matrix_ini.f:6666-6757)."""
+        st = np.arange(1, self.n_states + 1, dtype=np.int32)
+        ic = self.indx_chann
+        cols = [st, ic, self.j12, self.m12]
+        if self.sys_type == 1:
+            cols += [self.j1[ic - 1]]
+        elif self.sys_type == 4:
+            cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1]]
+        elif self.sys_type == 8:
+            cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1]]
+        else:
+            cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1],
+                     self.ka2[ic - 1], self.kc2[ic - 1]]
+        return np.ascontiguousarray(np.stack(cols, axis=1).astype(np.int32))
+
+
+def r_grid(n, rmin, rmax, equidistant=True):
+    R = np.zeros(n)
+    check(lib().mqct_r_grid(n, rmin, rmax, 1 if equidistant else 0, R))
+    return R
+
+
+@dataclass
+class PesSpec:
+    kind: int
+    n_terms: int
+    params: np.ndarray
+    sites1: np.ndarray | None = None
+    sites2: np.ndarray | None = None
+    table: np.ndarray | None = None
+
+    @staticmethod
+    def from_dict(d):
+        return PesSpec(d["kind"], d["n_terms"], np.ascontiguousarray(d["params"], np.float64),
+                       None if d.get("sites1") is None else np.ascontiguousarray(d["sites1"], np.float64),
+                       None if d.get("sites2") is None else np.ascontiguousarray(d["sites2"], np.float64),
+                       None if d.get("table") is None else np.ascontiguousarray(d["table"], np.float64))
+
+    def c_struct(self):
+        return _abi.Pes(self.kind, self.n_terms, ptr(self.params),
+                        0 if self.sites1 is None else len(self.sites1) // 3,
+                        0 if self.sites2 is None else len(self.sites2) // 3,
+                        ptr(self.sites1), ptr(self.sites2), ptr(self.table))
+
+
+def _grid_struct(grid):
+    if isinstance(grid, _abi.Grid):
+        return grid
+    g = list(grid) + [0] * (7 - len(grid))
+    return _abi.Grid(*g)
+
+
+def build_matrix(system: CollisionSystem, R, grid, pes, precision=PREC_FP64, mij_cutoff=1e-12,
+                 r_cut1=6.0, r_cut2=8.0):
+    """MATRIX_MAKE direct integration on the GPU: returns Mat_el (P x nR, Hartree),
+    its spline second derivatives and the MIJ_CUTOFF flags."""
+    R = np.ascontiguousarray(R, np.float64)
+    pes = pes if isinstance(pes, PesSpec) else PesSpec.from_dict(pes)
+    P, nR = system.P, len(R)
+    mat = np.zeros(P * nR)
+    y2 = np.zeros(P * nR)
+    sk = np.zeros(P, np.int32)
+    s = system.c_struct()
+    g = _grid_struct(grid)
+    ps = pes.c_struct()
+    check(lib().mqct_build_matrix(C.byref(s), np.ascontiguousarray(system.ind_mat.reshape(-1)), P,
+                                  R, nR, C.byref(g), C.byref(ps), precision, mij_cutoff, r_cut1,
+                                  r_cut2, mat, ptr(y2), ptr(sk), None))
+    return mat.reshape(P, nR), y2.reshape(P, nR), sk
+
+
+class MatrixPlan:
+    """Device-resident matrix build (mqct_matrix_plan_*); outputs in caller device buffers."""
+
+    def __init__(self, system, R, grid, pes, precision=PREC_BF16X3, mij_cutoff=1e-12,
+                 r_cut1=6.0, r_cut2=8.0):
+        self.R = np.ascontiguousarray(R, np.float64)
+        self.pes = pes if isinstance(pes, PesSpec) else PesSpec.from_dict(pes)
+        self.system = system
+        self._s = system.c_struct()
+        self._g = _grid_struct(grid)
+        self._p = self.pes.c_struct()
+        self._ind = np.ascontiguousarray(system.ind_mat.reshape(-1))
+        h = _abi.vp()
+        check(lib().mqct_matrix_plan_create(C.byref(self._s), self._ind, system.P, self.R,
+                                            len(self.R), C.byref(self._g), C.byref(self._p),
+                                            precision, mij_cutoff, r_cut1, r_cut2, C.byref(h)))
+        self.h = h
+        self.flops = lib().mqct_matrix_plan_flops(h)
+
+    def execute(self, d_mat: int, d_y2: int = 0, d_skipped: int = 0):
+        check(lib().mqct_matrix_plan_execute(self.h, d_mat, d_y2 or None, d_skipped or None))
+
+    def sync(self):
+        check(lib().mqct_matrix_plan_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().mqct_matrix_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spline_y2(R, mat):
+    """Clamped cubic-spline second derivatives with finite-difference end slopes for
+    every row of mat (READ_MIJ re-splines on read, MQCT_SOURCE_CODES/matrix_ini.f:5746-5753),
+    the tridiagonal recurrence of MQCT_SOURCE_CODES/suppl_routines.f:914-965 vectorised
+    over elements."""
+    R = np.asarray(R, np.float64)
+    Y = np.asarray(mat, np.float64)
+    P, n = Y.shape
+    y2 = np.zeros_like(Y)
+    u = np.zeros_like(Y)
+    yp1 = (Y[:, 1] - Y[:, 0]) / (R[1] - R[0])
+    ypn = (Y[:, -1] - Y[:, -2]) / (R[-1] - R[-2])
+    y2[:, 0] = -0.5
+    u[:, 0] = (3.0 / (R[1] - R[0])) * ((Y[:, 1] - Y[:, 0]) / (R[1] - R[0]) - yp1)
+    for i in range(1, n - 1):
+        sig = (R[i] - R[i - 1]) / (R[i + 1] - R[i - 1])
+        p = sig * y2[:, i - 1] + 2.0
+        y2[:, i] = (sig - 1.0) / p
+        u[:, i] = (6.0 * ((Y[:, i + 1] - Y[:, i]) / (R[i + 1] - R[i]) -
+                          (Y[:, i] - Y[:, i - 1]) / (R[i] - R[i - 1])) / (R[i + 1] - R[i - 1]) -
+                   sig * u[:, i - 1]) / p
+    un = (3.0 / (R[-1] - R[-2])) * (ypn - (Y[:, -1] - Y[:, -2]) / (R[-1] - R[-2]))
+    y2[:, -1] = (un - 0.5 * u[:, -2]) / (0.5 * y2[:, -2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[:, k] = y2[:, k] * y2[:, k + 1] + u[:, k]
+    return y2
+
+
+class PropagationTables:
+    """Matrix tables as DOTRAJECT sees them: MIJ_SHIFT (M -= M(R_max), default on,
+    MQCT_SOURCE_CODES/iotest.f:3754, :matrix_ini.f:5739-5743), MIJ_CUTOFF exclusion of
+    elements below mij_cutoff cm^-1 at R~r_cut1 and r_cut2 (MQCT_SOURCE_CODES/matrix_ini.f:4288-4378)
+    and re-splined knots."""
+
+    def __init__(self, j12, m12, ej_hartree, ind_mat, R, mat, mass_amu, y2=None, mij_shift=True,
+                 mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
+        R = np.ascontiguousarray(R, np.float64)
+        mat = np.asarray(mat, np.float64)
+        if mij_shift:
+            mat = mat - mat[:, -1:]
+        ir1 = int(np.argmin(np.abs(R - r_cut1)))
+        ir2 = int(np.argmin(np.abs(R - r_cut2)))
+        keep = np.maximum(np.abs(mat[:, ir1]), np.abs(mat[:, ir2])) >= mij_cutoff * CM_TO_HARTREE
+        self.keep = keep
+        self.mat = np.ascontiguousarray(mat[keep])
+        self.y2 = np.ascontiguousarray(spline_y2(R, self.mat) if y2 is None else np.asarray(y2)[keep])
+        self.ind_mat = np.ascontiguousarray(np.asarray(ind_mat, np.int32)[keep])
+        self.R = R
+        self.j12 = np.ascontiguousarray(j12, np.int32)
+        self.m12 = np.ascontiguousarray(m12, np.int32)
+        self.ej = np.ascontiguousarray(ej_hartree, np.float64)
+        self.mass_au = float(mass_amu) * AMU_TO_AU
+        self.n_states = len(self.j12)
+        self.P = len(self.ind_mat)
+
+    @staticmethod
+    def from_system(system: CollisionSystem, R, mat, mass_amu, **kw):
+        return PropagationTables(system.j12, system.m12, system.ej_cm * CM_TO_HARTREE,
+                                 system.ind_mat, R, mat, mass_amu, **kw)
+
+    def c_struct(self):
+        self._ind_flat = np.ascontiguousarray(self.ind_mat.reshape(-1))
+        return _abi.Tables(self.n_states, ptr(self.j12), ptr(self.m12), ptr(self.ej), self.P,
+                           ptr(self._ind_flat), len(self.R), ptr(self.R), ptr(self.mat),
+                           ptr(self.y2), self.mass_au)
+
+
+@dataclass
+class Trajectory:
+    e_coll: float           # Hartree
+    l_real: float
+    s_st: int               # 1-based
+    dt: float
+    r_start: float
+    r_fin: float
+    numb_orb_prds: int = 1
+    numb_oscl_prds: int = 1
+    time_lim: float = 0.0
+    max_steps: int = 2_000_000
+
+    def c_struct(self):
+        return _abi.TrajInit(self.e_coll, self.l_real, self.s_st, self.dt, self.r_start,
+                             self.r_fin, self.numb_orb_prds, self.numb_oscl_prds, self.time_lim,
+                             self.max_steps)
+
+
+def trajectory_set(U_cm, b_max, mass_amu, s_st, time_step, rmax, j_max_ini=0, dl=1,
+                   time_lim=0.0, max_steps=2_000_000):
+    """Integer-l trajectory set of PROPAGATE (MQCT_SOURCE_CODES/propagator.f:419-495):
+    k = sqrt(2 mu E), J_max = int(b_max k) - j_max, l = L_MIN..L_MAX step DL;
+    dt = TIME_STEP / sqrt(U / 300) (MQCT_SOURCE_CODES/propagator.f:2436)."""
+    E = U_cm * CM_TO_HARTREE
+    mu = mass_amu * AMU_TO_AU
+    k = np.sqrt(mu * 2.0 * E)
+    J_max = int(b_max * k) - j_max_ini
+    L_max = J_max + j_max_ini
+    L_min = max(0, 0 if J_max >= j_max_ini else j_max_ini - J_max)
+    dt = time_step / np.sqrt(U_cm / 300.0)
+    trajs = [Trajectory(E, float(l), s_st, dt, rmax, rmax, time_lim=time_lim, max_steps=max_steps)
+             for l in range(L_min, L_max + 1, dl)]
+    return trajs, dict(k=k, J_down=0, J_up=J_max, L_min=L_min, E=E)
+
+
+def _traj_array(trajs):
+    arr = (_abi.TrajInit * len(trajs))(*[t.c_struct() for t in trajs])
+    return arr
+
+
+def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, at_paths=None):
+    """Batched DOTRAJECT on the GPU.  Returns (amp [n, 2N], cls [n, 6], diag [n, 8])."""
+    n = len(trajs)
+    N = tables.n_states
+    amp = np.zeros(n * 2 * N)
+    cls = np.zeros(n * 6)
+    diag = np.zeros(n * 8)
+    t = tables.c_struct()
+    arr = _traj_array(trajs)
+    at = None
+    if mode == MODE_AT:
+        recs = [np.ascontiguousarray(p, np.float64).reshape(-1, 8) for p in at_paths]
+        n_rec = np.array([len(r) for r in recs], np.int32)
+        off = np.concatenate([[0], np.cumsum(n_rec)[:-1]]).astype(np.int64)
+        flat = np.ascontiguousarray(np.concatenate(recs).reshape(-1))
+        at_keep = (n_rec, off, flat)
+        at = _abi.AtPaths(ptr(off), ptr(n_rec), ptr(flat))
+    check(lib().mqct_propagate_batch(C.byref(t), arr, n, mode, C.byref(at) if at else None,
+                                     arith, amp, cls, diag))
+    return amp.reshape(n, 2 * N), cls.reshape(n, 6), diag.reshape(n, 8)
+
+
+class PropagationPlan:
+    """Tables uploaded once (mqct_prop_plan_*); run() per trajectory batch."""
+
+    def __init__(self, tables: PropagationTables, arith=PROP_FP32):
+        self.tables = tables
+        self._t = tables.c_struct()
+        h = _abi.vp()
+        check(lib().mqct_prop_plan_create(C.byref(self._t), arith, C.byref(h)))
+        self.h = h
+        self.bytes_per_step = lib().mqct_prop_plan_bytes_per_step(h)
+
+    def run(self, trajs):
+        n = len(trajs)
+        N = self.tables.n_states
+        amp = np.zeros(n * 2 * N)
+        cls = np.zeros(n * 6)
+        diag = np.zeros(n * 8)
+        check(lib().mqct_prop_plan_run(self.h, _traj_array(trajs), n, amp, cls, diag))
+        return amp.reshape(n, 2 * N), cls.reshape(n, 6), diag.reshape(n, 8)
+
+    def run_device(self, d_init: int, n: int, d_amp: int, d_cls: int, d_diag: int):
+        check(lib().mqct_prop_plan_run_device(self.h, d_init, n, d_amp, d_cls, d_diag))
+
+    def sync(self):
+        check(lib().mqct_prop_plan_sync(self.h))
+
+    def close(self):
+        if self.h:
+            lib().mqct_prop_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def channel_probabilities(amp, indx_chann, n_channels):
+    """probab(channel) = sum of |a|^2 over the channel's states
+    (MQCT_SOURCE_CODES/propagator.f:4364-4380)."""
+    N = len(indx_chann)
+    p = amp[:, :N] ** 2 + amp[:, N:] ** 2
+    out = np.zeros((amp.shape[0], n_channels))
+    for c in range(n_channels):
+        out[:, c] = p[:, indx_chann == c + 1].sum(axis=1)
+    return out
+
+
+def cross_sections(prob, j_ini, J_down, J_up, L_min, k_vec, U_cm=None, e_ch=None, chann_ini=1):
+    """INELAST_CALC for DL=1 (MQCT_SOURCE_CODES/propagator.f:4776-4841):
+    sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(l), in Angstrom^2
+    (sigma(U) column of CROSS_SECTIONS.out).  With U_cm and e_ch also returns the
+    Billing-corrected sigma(E_coll) (MQCT_SOURCE_CODES/propagator.f:1207-1208, 276-286)."""
+    n_traj, nch = prob.shape
+    sig = np.zeros(nch)
+    for J in range(J_down, J_up + 1):
+        for l in range(abs(J - j_ini), J + j_ini + 1):
+            i = l - L_min
+            if 0 <= i < n_traj:
+                sig += prob[i] * (2.0 * J + 1.0) / k_vec ** 2 / (2.0 * j_ini + 1) * np.pi
+    sig_U = sig * A_BOHR ** 2
+    if U_cm is None:
+        return sig_U
+    dE = np.asarray(e_ch) - e_ch[chann_ini - 1]
+    e_bill = U_cm + dE / 2.0 + dE ** 2 / 16.0 / U_cm
+    return sig_U, sig_U * U_cm / e_bill, e_bill
+
+
+def write_mtrx_uf(path, system: CollisionSystem, R, mat):
+    rec = system.state_records()
+    check(lib().mqct_write_mtrx_uf(path.encode(), system.sys_type, system.n_channels,
+                                   system.n_states, np.ascontiguousarray(rec.reshape(-1)),
+                                   rec.shape[1], system.P,
+                                   np.ascontiguousarray(system.ind_mat.reshape(-1)), len(R),
+                                   np.ascontiguousarray(R, np.float64),
+                                   np.ascontiguousarray(mat, np.float64).reshape(-1)))
+
+
+def read_mtrx_uf(path):
+    L = lib()
+    ct, nch, ns, nR, srl = (C.c_int32() for _ in range(5))
+    P = C.c_int64()
+    check(L.mqct_read_mtrx_uf_header(path.encode(), C.byref(ct), C.byref(nch), C.byref(ns),
+                                     C.byref(P), C.byref(nR), C.byref(srl)))
+    st = np.zeros(ns.value * srl.value, np.int32)
+    ind = np.zeros(2 * P.value, np.int32)
+    R = np.zeros(nR.value)
+    mat = np.zeros(P.value * nR.value)
+    check(L.mqct_read_mtrx_uf(path.encode(), srl.value, st, ind, R, mat))
+    return dict(coll_type=ct.value, n_channels=nch.value, states=st.reshape(ns.value, srl.value),
+                ind_mat=ind.reshape(P.value, 2), R=R, mat=mat.reshape(P.value, nR.value))

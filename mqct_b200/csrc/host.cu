@@ -1,0 +1,384 @@
+// host.cu -- host-side parts of the C ABI: error state, quadrature axes, rigid
+// asymmetric-top levels, state/pair enumeration (INI_ARRAYS), the R grid and
+// the MTRX_UF.DAT matrix file.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace mqct {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+void gauss_legendre(int n, double* x, double* w) {
+  const double eps = 3.0e-15;
+  int m = (n + 1) / 2;
+  for (int i = 1; i <= m; ++i) {
+    double z = cos(kPi * (i - 0.25) / (n + 0.5)), z1 = 0.0, pp = 0.0;
+    do {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+    } while (fabs(z - z1) > eps);
+    x[i - 1] = -z;
+    x[n - i] = z;
+    w[i - 1] = w[n - i] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+// Gauss-Legendre axis on [lo, hi]: nodes xm + xl*x, weights as on [-1,1]; the
+// half-length xl multiplies the integral (MQCT_SOURCE_CODES/pot_comp.f:376-381).
+Axis axis_gl(int n, double lo, double hi) {
+  Axis a;
+  a.x.resize(n);
+  a.w.resize(n);
+  gauss_legendre(n, a.x.data(), a.w.data());
+  double xm = 0.5 * (hi + lo), xl = 0.5 * (hi - lo);
+  for (int i = 0; i < n; ++i) a.x[i] = xm + xl * a.x[i];
+  a.half = xl;
+  return a;
+}
+// Midpoint-equidistant axis with weight 2/n (EQ_ANG_GRID,
+// MQCT_SOURCE_CODES/pot_comp.f:601-611).
+Axis axis_mid(int n, double lo, double hi) {
+  Axis a;
+  a.x.resize(n);
+  a.w.assign(n, 2.0 / n);
+  double xl = 0.5 * (hi - lo);
+  for (int i = 1; i <= n; ++i) a.x[i - 1] = lo + (i - 0.50) * 2.0 * xl / n;
+  a.half = xl;
+  return a;
+}
+
+// Rigid-rotor Hamiltonian in the symmetric-top basis with z along c
+// (MQCT_SOURCE_CODES/asym_top.f:103-137): diagonal (A+B)/2 J(J+1) +
+// (C-(A+B)/2) K^2, K+-2 couplings (A-B)/4 sqrt(..)sqrt(..).
+static double rotor_h(int j, int k1, int k2, double A, double B, double C) {
+  if (k1 == k2) return 0.5 * (A + B) * j * (j + 1.0) + (C - 0.5 * (A + B)) * (double)(k1 * k1);
+  if (k1 == k2 - 2 || k1 == k2 + 2) {
+    int kav = (k1 + k2) / 2;
+    return 0.5 * (A - B) * sqrt((j + 1.0) * j - kav * k1) * sqrt((j + 1.0) * j - kav * k2) / 2.0;
+  }
+  return 0.0;
+}
+
+// Threshold Jacobi diagonalisation of a small symmetric matrix (column-major a).
+static void sym_eig(int n, std::vector<double>& a, std::vector<double>& w,
+                    std::vector<double>& v) {
+  v.assign(n * n, 0.0);
+  for (int i = 0; i < n; ++i) v[i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0, scale = 0.0;
+    for (int c = 0; c < n; ++c)
+      for (int r = 0; r < n; ++r) {
+        double x = a[c * n + r] * a[c * n + r];
+        if (r == c) scale += x;
+        else off += x;
+      }
+    if (off <= 1e-30 * scale || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = a[q * n + p];
+        if (apq == 0.0) continue;
+        double tau = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
+        double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          double xp = a[p * n + k], xq = a[q * n + k];
+          a[p * n + k] = c * xp - s * xq;
+          a[q * n + k] = s * xp + c * xq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          double xp = a[k * n + p], xq = a[k * n + q];
+          a[k * n + p] = c * xp - s * xq;
+          a[k * n + q] = s * xp + c * xq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double xp = v[p * n + k], xq = v[q * n + k];
+          v[p * n + k] = c * xp - s * xq;
+          v[q * n + k] = s * xp + c * xq;
+        }
+      }
+  }
+  w.resize(n);
+  for (int i = 0; i < n; ++i) w[i] = a[i * n + i];
+}
+
+// Level (j, ka, kc) is eigenvalue number j + ka - kc in ascending order, the
+// (Ka, Kc) labelling of MQCT_SOURCE_CODES/asym_top.f:139-173.  The eigenvector
+// (components K=-j..j) is signed so its first non-negligible component is > 0.
+int asym_top_level(double A, double B, double C, int j, int ka, int kc, double* energy,
+                   double* vec) {
+  if (j < 0 || ka < 0 || kc < 0 || ka > j || kc > j) return MQCT_E_ARG;
+  if (ka + kc != j && ka + kc != j + 1) return MQCT_E_ARG;
+  int pos = j + ka - kc;  // 0-based rank
+  if (pos < 0 || pos > 2 * j || (pos + 1) / 2 != ka) return MQCT_E_ARG;
+  int n = 2 * j + 1;
+  std::vector<double> a(n * n), w, v;
+  for (int c = 0; c < n; ++c)
+    for (int r = 0; r < n; ++r) a[c * n + r] = rotor_h(j, r - j, c - j, A, B, C);
+  sym_eig(n, a, w, v);
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  for (int i = 1; i < n; ++i)
+    for (int k = i; k > 0 && w[ord[k - 1]] > w[ord[k]]; --k) std::swap(ord[k - 1], ord[k]);
+  int col = ord[pos];
+  *energy = w[col];
+  int first = -1;
+  for (int k = 0; k < n; ++k) {
+    vec[k] = v[col * n + k];
+    if (first < 0 && fabs(vec[k]) > 1e-10) first = k;
+  }
+  if (first >= 0 && vec[first] < 0)
+    for (int k = 0; k < n; ++k) vec[k] = -vec[k];
+  return MQCT_OK;
+}
+
+}  // namespace mqct
+
+using namespace mqct;
+
+extern "C" {
+
+const char* mqct_last_error(void) { return g_err.c_str(); }
+int mqct_version(void) { return 10000; }
+int mqct_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,
+                        double* energy, double* vec) {
+  int rc = asym_top_level(A, B, C, j, ka, kc, energy, vec);
+  if (rc) set_error("invalid asymmetric-top level j=%d ka=%d kc=%d", j, ka, kc);
+  return rc;
+}
+
+// States per channel: m = -j..j (types 1, 4) or j12 = |j1-j2|..j1+j2 with its m
+// (types 8, 0), channel-major (MQCT_SOURCE_CODES/matrix_ini.f:261-544).
+int mqct_count_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
+                      const int32_t* j2) {
+  if (n_channels <= 0 || !j1) return MQCT_E_ARG;
+  int st = 0;
+  for (int i = 0; i < n_channels; ++i) {
+    if (sys_type == 1 || sys_type == 4) st += 2 * j1[i] + 1;
+    else if (sys_type == 8 || sys_type == 0) {
+      if (!j2) return MQCT_E_ARG;
+      for (int js = abs(j1[i] - j2[i]); js <= j1[i] + j2[i]; ++js) st += 2 * js + 1;
+    } else {
+      set_error("unsupported SYS_TYPE %d", sys_type);
+      return MQCT_E_ARG;
+    }
+  }
+  return st;
+}
+
+int mqct_enumerate_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
+                          const int32_t* j2, int32_t* indx_chann, int32_t* j12, int32_t* m12) {
+  int n = mqct_count_states(sys_type, n_channels, j1, j2);
+  if (n < 0) return n;
+  int st = 0;
+  for (int i = 0; i < n_channels; ++i) {
+    int lo = (sys_type == 1 || sys_type == 4) ? j1[i] : abs(j1[i] - j2[i]);
+    int hi = (sys_type == 1 || sys_type == 4) ? j1[i] : j1[i] + j2[i];
+    for (int js = lo; js <= hi; ++js)
+      for (int m = -js; m <= js; ++m) {
+        indx_chann[st] = i + 1;
+        j12[st] = js;
+        m12[st] = m;
+        ++st;
+      }
+  }
+  return st;
+}
+
+// ind_mat: st1 outer, st2 <= st1, equal m12 (MQCT_SOURCE_CODES/matrix_ini.f:553-627).
+int64_t mqct_count_pairs(int32_t n, const int32_t* m12) {
+  if (n <= 0 || !m12) return MQCT_E_ARG;
+  int mmax = 0;
+  for (int s = 0; s < n; ++s) mmax = std::max(mmax, abs(m12[s]));
+  std::vector<int64_t> cnt(2 * mmax + 1, 0);
+  int64_t p = 0;
+  for (int s = 0; s < n; ++s) p += ++cnt[m12[s] + mmax];
+  return p;
+}
+int64_t mqct_fill_ind_mat(int32_t n, const int32_t* m12, int32_t* ind) {
+  if (n <= 0 || !m12 || !ind) return MQCT_E_ARG;
+  int64_t p = 0;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (m12[a] == m12[b]) {
+        ind[2 * p] = a + 1;
+        ind[2 * p + 1] = b + 1;
+        ++p;
+      }
+  return p;
+}
+
+// R grid: equidistant or the 3-segment "optimized" grid
+// (MQCT_SOURCE_CODES/matrix_ini.f:954-981).
+int mqct_r_grid(int32_t n, double rmin, double rmax, int32_t equidistant, double* R) {
+  if (n < 2 || !(rmax > rmin) || !R) return MQCT_E_ARG;
+  double dr = (rmax - rmin) / (n - 1.0);
+  if (equidistant) {
+    for (int i = 1; i <= n; ++i) R[i - 1] = rmin + dr * (i - 1.0);
+    return MQCT_OK;
+  }
+  if (n < 3) {  // the third segment would divide by n - n2 = 0
+    set_error("the optimized R grid needs at least 3 points");
+    return MQCT_E_ARG;
+  }
+  int n1 = n / 3, n2 = n / 2 + 1;
+  R[0] = rmin;
+  R[n - 1] = rmax;
+  for (int i = 1; i <= n1; ++i) R[i - 1] = rmin + dr * (i - 1.0) / 3.0;
+  for (int i = n1 + 1; i <= n2; ++i) R[i - 1] = R[n1 - 1] + dr * (i - n1);
+  dr = (rmax - R[n2 - 1]) / (n - n2);
+  for (int i = n2; i <= n; ++i) R[i - 1] = R[n2 - 1] + dr * (i - n2);
+  return MQCT_OK;
+}
+
+// ---------------------------------------------------------------- MTRX_UF.DAT
+static bool put_rec(FILE* f, const void* d, int32_t nb) {
+  return fwrite(&nb, 4, 1, f) == 1 && fwrite(d, 1, (size_t)nb, f) == (size_t)nb &&
+         fwrite(&nb, 4, 1, f) == 1;
+}
+static bool get_rec(FILE* f, void* d, int32_t expect, int32_t* got = nullptr) {
+  int32_t a = 0, b = 0;
+  if (fread(&a, 4, 1, f) != 1) return false;
+  if (got) *got = a;
+  if (expect >= 0 && a != expect) return false;
+  if (a < 0 || a > (1 << 30)) return false;
+  if (d && fread(d, 1, (size_t)a, f) != (size_t)a) return false;
+  if (!d && fseek(f, a, SEEK_CUR) != 0) return false;
+  if (fread(&b, 4, 1, f) != 1 || b != a) return false;
+  return true;
+}
+
+int mqct_write_mtrx_uf(const char* path, int32_t coll_type, int32_t n_channels,
+                       int32_t n_states, const int32_t* state_rec, int32_t state_rec_len,
+                       int64_t P, const int32_t* ind_mat, int32_t nR, const double* R,
+                       const double* mat) {
+  MQCT_ARG_CHECK(path && state_rec && ind_mat && R && mat && P > 0 && nR > 1 &&
+                     P < (int64_t)1 << 31 && state_rec_len > 0,
+                 "mqct_write_mtrx_uf: bad arguments");
+  FILE* f = fopen(path, "wb");
+  if (!f) {
+    set_error("cannot open %s for writing", path);
+    return MQCT_E_IO;
+  }
+  bool ok = true;
+  int32_t hdr[5] = {coll_type, n_channels, n_states, (int32_t)P, nR};
+  for (int i = 0; i < 5 && ok; ++i) ok = put_rec(f, &hdr[i], 4);
+  for (int s = 0; s < n_states && ok; ++s)
+    ok = put_rec(f, state_rec + (size_t)s * state_rec_len, 4 * state_rec_len);
+  for (int64_t k = 0; k < P && ok; ++k) {
+    int32_t t[3] = {(int32_t)(k + 1), ind_mat[2 * k], ind_mat[2 * k + 1]};
+    ok = put_rec(f, t, 12);
+  }
+  for (int i = 0; i < nR && ok; ++i) {
+    unsigned char b[12];
+    int32_t ii = i + 1;
+    memcpy(b, &ii, 4);
+    memcpy(b + 4, &R[i], 8);
+    ok = put_rec(f, b, 12);
+  }
+  for (int64_t k = 0; k < P && ok; ++k) {
+    int32_t kk = (int32_t)(k + 1);
+    ok = put_rec(f, &kk, 4) && put_rec(f, mat + (size_t)k * nR, 8 * nR);
+  }
+  if (fclose(f) != 0) ok = false;
+  if (!ok) {
+    set_error("write error on %s", path);
+    return MQCT_E_IO;
+  }
+  return MQCT_OK;
+}
+
+int mqct_read_mtrx_uf_header(const char* path, int32_t* coll_type, int32_t* n_channels,
+                             int32_t* n_states, int64_t* P, int32_t* nR,
+                             int32_t* state_rec_len) {
+  MQCT_ARG_CHECK(path, "null path");
+  FILE* f = fopen(path, "rb");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return MQCT_E_IO;
+  }
+  int32_t h[5];
+  bool ok = true;
+  for (int i = 0; i < 5 && ok; ++i) ok = get_rec(f, &h[i], 4);
+  int32_t len = 0;
+  if (ok && h[2] > 0) ok = get_rec(f, nullptr, -1, &len);
+  fclose(f);
+  if (!ok || h[2] <= 0 || h[3] <= 0 || h[4] <= 1 || len <= 0 || len % 4) {
+    set_error("malformed MTRX_UF header in %s", path);
+    return MQCT_E_IO;
+  }
+  *coll_type = h[0];
+  *n_channels = h[1];
+  *n_states = h[2];
+  *P = h[3];
+  *nR = h[4];
+  *state_rec_len = len / 4;
+  return MQCT_OK;
+}
+
+int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_rec,
+                      int32_t* ind_mat, double* R, double* mat) {
+  int32_t ct, nch, ns, nR, srl;
+  int64_t P;
+  int rc = mqct_read_mtrx_uf_header(path, &ct, &nch, &ns, &P, &nR, &srl);
+  if (rc) return rc;
+  MQCT_ARG_CHECK(srl == state_rec_len && state_rec && ind_mat && R && mat,
+                 "state record length %d != %d", srl, state_rec_len);
+  FILE* f = fopen(path, "rb");
+  if (!f) return MQCT_E_IO;
+  bool ok = true;
+  for (int i = 0; i < 5 && ok; ++i) ok = get_rec(f, nullptr, 4);
+  for (int s = 0; s < ns && ok; ++s) ok = get_rec(f, state_rec + (size_t)s * srl, 4 * srl);
+  for (int64_t k = 0; k < P && ok; ++k) {
+    int32_t t[3];
+    ok = get_rec(f, t, 12) && t[0] == k + 1 && t[1] >= 1 && t[1] <= ns && t[2] >= 1 &&
+         t[2] <= ns;
+    ind_mat[2 * k] = t[1];
+    ind_mat[2 * k + 1] = t[2];
+  }
+  for (int i = 0; i < nR && ok; ++i) {
+    unsigned char b[12];
+    int32_t ii;
+    ok = get_rec(f, b, 12);
+    memcpy(&ii, b, 4);
+    memcpy(&R[i], b + 4, 8);
+    ok = ok && ii == i + 1;
+  }
+  for (int64_t k = 0; k < P && ok; ++k) {
+    int32_t kk;
+    ok = get_rec(f, &kk, 4) && kk == k + 1 && get_rec(f, mat + (size_t)k * nR, 8 * nR);
+  }
+  fclose(f);
+  if (!ok) {
+    set_error("malformed MTRX_UF body in %s", path);
+    return MQCT_E_IO;
+  }
+  return MQCT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,640 @@
+// matrix.cu -- the state-to-state matrix build (H1).
+//
+// The reference evaluates, for every element k = (st1, st2) and every radial
+// point R_i, the quadrature of INTEGRATOR_TEMP
+// (MQCT_SOURCE_CODES/pot_comp.f:1790-3737) re-computing both rotor
+// wavefunctions at every grid point.  Here the same sum is one GEMM over the
+// angular grid:
+//     M[k, i] = sum_g X[k, g] * W[g, i],
+//     X[k, g] = Re(psi_st1(g)^* psi_st2(g)),   W[g, i] = w_g V(R_i, g)
+// with the grid g = (beta, gamma) (type 4) or beta (type 1).  An explicit alpha
+// grid (type 4, n_alpha > 0) multiplies each wavefunction by e^{i m alpha}; it
+// is contracted as written (X recomputed per alpha point).
+//
+// Kernels (one build = K1 + K2 + K3 + K4):
+//   K1 basis_kernel        rotor wavefunctions on the grid, FP64, per m-block
+//   K2 pes_weight_kernel   PES on (grid x R) times the quadrature weights
+//   K3 contract_fp64_kernel / tcgen05 split-precision kernel (contract_tc.cu)
+//   K4 finalize_kernel     Hartree units, MIJ_CUTOFF, clamped spline y2
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "common.cuh"
+#include "matrix_plan.cuh"
+
+using namespace mqct;
+
+namespace mqct {
+
+__constant__ double c_logfact[128];
+
+static int upload_logfact() {
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && done[dev]) return MQCT_OK;
+  double lf[128];
+  lf[0] = 0.0;
+  for (int i = 1; i < 128; ++i) lf[i] = lf[i - 1] + log((double)i);
+  MQCT_CUDA_TRY(cudaMemcpyToSymbol(c_logfact, lf, sizeof lf));
+  if (dev < 64) done[dev] = true;
+  return MQCT_OK;
+}
+
+// ------------------------------------------------------------------ K1: basis
+// psi for block-local state s at 2-D grid point g2 (beta outer, gamma inner):
+// type 1: Y_jm(beta, 0) (WF_DIAT_TOP, MQCT_SOURCE_CODES/basis_wave_functions.f:153-175);
+// type 4: sum_K c_K sqrt((2j+1)/8pi^2) d^j_{Km}(beta) e^{iK gamma} at alpha = 0
+//         (WF_ASYM_TOP :83-116 with Djkm MQCT_SOURCE_CODES/pot_comp.f:256-309).
+// Output psi[(blk_off + s) * G2 + g2] as (re, im) FP64.
+__global__ void basis_kernel(int sys_type, int n_rows, const int* __restrict__ row_state,
+                             const int* __restrict__ st_chan, const int* __restrict__ st_m,
+                             const int* __restrict__ ch_j, const double* __restrict__ vec,
+                             int ldv, const double* __restrict__ beta,
+                             const double* __restrict__ gamma, int n_gamma, int G2,
+                             double2* __restrict__ psi) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n_rows * G2) return;
+  int r = (int)(idx / G2), g2 = (int)(idx % G2);
+  int st = row_state[r];
+  int ch = st_chan[st];
+  int j = ch_j[ch], m = st_m[st];
+  double re = 0.0, im = 0.0;
+  if (sys_type == 1) {
+    double b = beta[g2];
+    int am = m < 0 ? -m : m;
+    double pl = mqct_dev::plgndr(j, am, cos(b));
+    double nrm = sqrt((2.0 * j + 1.0) / 4.0 / kPi * exp(c_logfact[j - am] - c_logfact[j + am]));
+    re = pl * nrm;
+    if (m < 0 && (am & 1)) re = -re;
+  } else {
+    int ib = g2 / n_gamma, ig = g2 % n_gamma;
+    double b = beta[ib], g = gamma[ig];
+    double nrm = sqrt((2.0 * j + 1.0) / 8.0 / (kPi * kPi));
+    const double* c = vec + (size_t)ch * ldv;
+    for (int i = 0; i <= 2 * j; ++i) {
+      int K = i - j;
+      if (c[i] == 0.0) continue;
+      double d = mqct_dev::wigner_d(j, K, m, b, c_logfact) * nrm;
+      double s, co;
+      sincos(K * g, &s, &co);
+      re += d * co * c[i];
+      im += d * s * c[i];
+    }
+  }
+  psi[idx] = make_double2(re, im);
+}
+
+// ------------------------------------------------------------------ K2: PES x weights
+struct PesDev {
+  int kind, n_terms, n_sites1, n_sites2;
+  const double* p;
+  const double* s1;
+  const double* s2;
+  const double* table;
+};
+
+__device__ inline double site_term(double r, const double* t) {
+  double D = t[0], a = t[1], re = t[2], c6 = t[3], rd = t[4];
+  double e = exp(-a * (r - re));
+  double r2 = r * r, r6 = r2 * r2 * r2;
+  double x = r / rd, x2 = x * x, x6 = x2 * x2 * x2;
+  return D * (e * e - 2.0 * e) - c6 * (1.0 - exp(-x6)) / r6;
+}
+
+// USER_DEFINED_PES(V,R,..,alpha,beta,gamma,..) for the built-in families.
+__device__ inline double pes_eval(const PesDev& P, double R, double beta, double gamma) {
+  if (P.kind == MQCT_PES_LEGENDRE) {
+    double x = cos(beta), v = 0.0;
+    double r2 = R * R, r6 = r2 * r2 * r2;
+    int n = P.n_terms;
+    // P_l(x) by Bonnet's recurrence
+    double pm = 1.0, pc = x;
+    for (int l = 0; l < n; ++l) {
+      double pl;
+      if (l == 0) pl = 1.0;
+      else if (l == 1) pl = x;
+      else {
+        pl = ((2.0 * l - 1.0) * x * pc - (l - 1.0) * pm) / l;
+        pm = pc;
+        pc = pl;
+      }
+      v += (P.p[l] * exp(-P.p[n + l] * R) - P.p[2 * n + l] / r6) * pl;
+    }
+    return v;
+  }
+  if (P.kind == MQCT_PES_SITES1) {
+    double sb, cb, sg, cg;
+    sincos(beta, &sb, &cb);
+    sincos(gamma, &sg, &cg);
+    double ax = R * sb * cg, ay = R * sb * sg, az = R * cb, v = 0.0;
+    for (int t = 0; t < P.n_terms; ++t) {
+      const double* q = P.p + 6 * t;
+      const double* s = P.s1 + 3 * (int)q[0];
+      double dx = ax - s[0], dy = ay - s[1], dz = az - s[2];
+      v += site_term(sqrt(dx * dx + dy * dy + dz * dz), q + 1);
+    }
+    return v;
+  }
+  return nan("");
+}
+
+// W[g2 * ldw + i] = wt[g2] * V(R_i, angles(g2)) with the argument mapping of
+// MQCT_SOURCE_CODES/pes_sys_type.f: type 1 passes beta (:8), type 4 passes
+// (-beta, -gamma) (:36).
+__global__ void pes_weight_kernel(int sys_type, PesDev pes, int G2, int nR,
+                                  const double* __restrict__ R, const double* __restrict__ beta,
+                                  const double* __restrict__ gamma, int n_gamma,
+                                  const double* __restrict__ wt, double* __restrict__ W,
+                                  int ldw) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)G2 * nR) return;
+  int g2 = (int)(idx / nR), i = (int)(idx % nR);
+  double v;
+  if (pes.kind == MQCT_PES_TABLE) {
+    v = pes.table[(size_t)i * G2 + g2];
+  } else if (sys_type == 1) {
+    v = pes_eval(pes, R[i], beta[g2], 0.0);
+  } else {
+    int ib = g2 / n_gamma, ig = g2 % n_gamma;
+    v = pes_eval(pes, R[i], -beta[ib], -gamma[ig]);
+  }
+  W[(size_t)g2 * ldw + i] = wt[g2] * v;
+}
+
+// ------------------------------------------------------------------ K3: FP64 form
+// acc[row, i] = sum_alpha sum_g2 X_alpha[row, g2] W[g2, i], a 128 x 64 tile per
+// CTA, 256 threads, 8 x 4 outputs per thread, K-chunks of 16 grid points.
+constexpr int F_TM = 128, F_TN = 64, F_TK = 16;
+__global__ void __launch_bounds__(256)
+contract_fp64_kernel(int n_rows, int G2, int nR, const int* __restrict__ row_a,
+                     const int* __restrict__ row_b, const int* __restrict__ row_m,
+                     const double2* __restrict__ psi, const double* __restrict__ W, int ldw,
+                     int n_alpha, const double* __restrict__ alpha,
+                     const double* __restrict__ walpha, double* __restrict__ acc) {
+  __shared__ double Xs[F_TK][F_TM + 1];
+  __shared__ double Ws[F_TK][F_TN];
+  const int tid = threadIdx.x;
+  const int row0 = blockIdx.x * F_TM, col0 = blockIdx.y * F_TN;
+  const int tr = tid / 16, tc = tid % 16;  // 16 x 16 threads: 8 rows x 4 cols each
+  double c[8][4];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) c[a][b] = 0.0;
+  // this thread's X-generation rows: row = tid % 128, g offsets (tid / 128) + 2*q
+  const int xr = tid % F_TM, xg0 = tid / F_TM;
+  const int grow = row0 + xr;
+  int ia = -1, ib = -1, mm = 0;
+  if (grow < n_rows) {
+    ia = row_a[grow];
+    ib = row_b[grow];
+    mm = row_m[grow];
+  }
+  const int na = n_alpha > 0 ? n_alpha : 1;
+  for (int k0 = 0; k0 < G2; k0 += F_TK) {
+    __syncthreads();
+    for (int q = tid; q < F_TK * F_TN; q += 256) {
+      int kk = q / F_TN, cc = q % F_TN;
+      int g = k0 + kk, col = col0 + cc;
+      Ws[kk][cc] = (g < G2 && col < nR) ? W[(size_t)g * ldw + col] : 0.0;
+    }
+    for (int al = 0; al < na; ++al) {
+      double zr = 1.0, zi = 0.0, wa = 1.0;
+      if (n_alpha > 0) {
+        sincos(mm * alpha[al], &zi, &zr);
+        wa = walpha[al];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < F_TK / 2; ++q) {
+        int kk = xg0 + 2 * q, g = k0 + kk;
+        double x = 0.0;
+        if (ia >= 0 && g < G2) {
+          double2 pa = psi[(size_t)ia * G2 + g], pb = psi[(size_t)ib * G2 + g];
+          if (n_alpha > 0) {  // rotate by e^{i m alpha}
+            double ar = zr * pa.x - zi * pa.y, ai = zr * pa.y + zi * pa.x;
+            double br = zr * pb.x - zi * pb.y, bi = zr * pb.y + zi * pb.x;
+            x = wa * (ar * br + ai * bi);
+          } else {
+            x = pa.x * pb.x + pa.y * pb.y;
+          }
+        }
+        Xs[kk][xr] = x;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int kk = 0; kk < F_TK; ++kk) {
+        double xv[8], wv[4];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) xv[a] = Xs[kk][tr * 8 + a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) wv[b] = Ws[kk][tc * 4 + b];
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) c[a][b] = fma(xv[a], wv[b], c[a][b]);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    int row = row0 + tr * 8 + a;
+    if (row >= n_rows) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int col = col0 + tc * 4 + b;
+      if (col < nR) acc[(size_t)row * nR + col] = c[a][b];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ K4: finalize
+// Per reference element k: sum the contraction partials (FP64), convert to
+// Hartree, apply MIJ_CUTOFF (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997) and
+// build the clamped spline with finite-difference end slopes
+// (:2005-2016, NR spline MQCT_SOURCE_CODES/suppl_routines.f:914-965).
+// Partials: n_part slabs of (n_rows x ldp) FP64 or FP32 values.
+template <class TP>
+__global__ void finalize_kernel(int64_t P, int nR, const int* __restrict__ k_to_row,
+                                const TP* __restrict__ part, int n_part, int64_t part_stride,
+                                int ldp, double scale, const double* __restrict__ R, int ir1,
+                                int ir2, double cut, double* __restrict__ mat,
+                                double* __restrict__ y2, int* __restrict__ skipped,
+                                double* __restrict__ work) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= P) return;
+  int row = k_to_row[k];
+  double* col = mat + (size_t)k * nR;
+  for (int i = 0; i < nR; ++i) {
+    double s = 0.0;
+    for (int p = 0; p < n_part; ++p) s += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
+    col[i] = s * scale;
+  }
+  double mx = fmax(fabs(col[ir1]), fabs(col[ir2]));
+  double* yy = y2 ? y2 + (size_t)k * nR : nullptr;
+  if (mx < cut) {
+    for (int i = 0; i < nR; ++i) {
+      col[i] = 0.0;
+      if (yy) yy[i] = 0.0;
+    }
+    if (skipped) skipped[k] = 1;
+    return;
+  }
+  if (skipped) skipped[k] = 0;
+  if (!yy) return;
+  double* u = work + (size_t)k * nR;
+  double yp1 = (col[1] - col[0]) / (R[1] - R[0]);
+  double ypn = (col[nR - 1] - col[nR - 2]) / (R[nR - 1] - R[nR - 2]);
+  yy[0] = -0.5;
+  u[0] = (3.0 / (R[1] - R[0])) * ((col[1] - col[0]) / (R[1] - R[0]) - yp1);
+  for (int i = 1; i < nR - 1; ++i) {
+    double sig = (R[i] - R[i - 1]) / (R[i + 1] - R[i - 1]);
+    double p = sig * yy[i - 1] + 2.0;
+    yy[i] = (sig - 1.0) / p;
+    u[i] = (6.0 * ((col[i + 1] - col[i]) / (R[i + 1] - R[i]) - (col[i] - col[i - 1]) / (R[i] - R[i - 1])) /
+                (R[i + 1] - R[i - 1]) -
+            sig * u[i - 1]) /
+           p;
+  }
+  double qn = 0.5;
+  double un = (3.0 / (R[nR - 1] - R[nR - 2])) * (ypn - (col[nR - 1] - col[nR - 2]) / (R[nR - 1] - R[nR - 2]));
+  yy[nR - 1] = (un - qn * u[nR - 2]) / (qn * yy[nR - 2] + 1.0);
+  for (int i = nR - 2; i >= 0; --i) yy[i] = yy[i] * yy[i + 1] + u[i];
+}
+
+// ------------------------------------------------------------------ plan
+static int nearest_index(const std::vector<double>& R, double r) {
+  int best = 0;
+  double d = fabs(R[0] - r);
+  for (size_t i = 1; i < R.size(); ++i)
+    if (fabs(R[i] - r) < d) {
+      d = fabs(R[i] - r);
+      best = (int)i;
+    }
+  return best;
+}
+
+int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, const double* R,
+                     int32_t nR_, const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec,
+                     double mij_cut, double rc1, double rc2) {
+  MQCT_ARG_CHECK(sys && ind_mat && R && grid && pes, "null argument");
+  MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 4,
+                 "matrix build supports SYS_TYPE 1 and 4 (got %d)", sys->sys_type);
+  MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31), "P out of range");
+  MQCT_ARG_CHECK(nR_ >= 2, "nR must be >= 2");
+  MQCT_ARG_CHECK(prec == MQCT_PREC_FP64 || prec == MQCT_PREC_BF16X3, "unknown precision %d", prec);
+  MQCT_ARG_CHECK(sys->n_states > 0 && sys->indx_chann && sys->m12 && sys->j1,
+                 "system without states");
+  MQCT_ARG_CHECK(sys->sys_type == 1 || (sys->vec1 && sys->ldv > 0), "type 4 needs eigenvectors");
+  MQCT_ARG_CHECK(grid->n_beta > 0 && (sys->sys_type == 1 || grid->n_gamma > 0), "empty grid");
+  MQCT_ARG_CHECK(pes->kind == MQCT_PES_TABLE || pes->kind == MQCT_PES_LEGENDRE ||
+                     pes->kind == MQCT_PES_SITES1,
+                 "PES kind %d not usable for SYS_TYPE %d", pes->kind, sys->sys_type);
+  MQCT_ARG_CHECK(pes->kind != MQCT_PES_TABLE || pes->table, "TABLE PES without table");
+  for (int i = 0; i < nR_ - 1; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
+  int rc = upload_logfact();
+  if (rc) return rc;
+  sys_type = sys->sys_type;
+  precision = prec;
+  P = P_;
+  nR = nR_;
+  n_states = sys->n_states;
+  Rh.assign(R, R + nR);
+  ir1 = nearest_index(Rh, rc1);
+  ir2 = nearest_index(Rh, rc2);
+  cut = mij_cut * kCmToHartree;
+  MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+  // --- states -> m-blocks
+  std::map<int, std::vector<int>> by_m;
+  for (int s = 0; s < n_states; ++s) {
+    int ch = sys->indx_chann[s] - 1;
+    MQCT_ARG_CHECK(ch >= 0 && ch < sys->n_channels, "indx_chann out of range at state %d", s + 1);
+    int j = sys->j1[ch];
+    MQCT_ARG_CHECK(j >= 0 && j <= 40 && abs(sys->m12[s]) <= j, "bad (j, m) at state %d", s + 1);
+    MQCT_ARG_CHECK(sys->sys_type == 1 || 2 * j + 1 <= sys->ldv, "ldv too small for j=%d", j);
+    by_m[sys->m12[s]].push_back(s);
+  }
+  std::vector<int> state_block(n_states), state_local(n_states);
+  std::vector<int> row_state;  // basis rows (block-ordered states)
+  std::vector<int> block_row0;
+  for (auto& kv : by_m) {
+    block_row0.push_back((int)row_state.size());
+    for (size_t l = 0; l < kv.second.size(); ++l) {
+      state_block[kv.second[l]] = (int)block_row0.size() - 1;
+      state_local[kv.second[l]] = (int)l;
+      row_state.push_back(kv.second[l]);
+    }
+  }
+  n_basis_rows = (int)row_state.size();
+  // --- pairs in GEMM order: grouped by block, each block padded to 128 rows
+  std::vector<std::vector<int64_t>> ks(block_row0.size());
+  for (int64_t k = 0; k < P; ++k) {
+    int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
+    MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states,
+                   "ind_mat out of range at k=%lld", (long long)k + 1);
+    MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "ind_mat pair with different m12 at k=%lld",
+                   (long long)k + 1);
+    ks[state_block[a]].push_back(k);
+  }
+  std::vector<int> rowa, rowb, rowm, k2r(P);
+  std::vector<int> tile_block;
+  for (size_t blk = 0; blk < ks.size(); ++blk) {
+    if (ks[blk].empty()) continue;
+    size_t start = rowa.size();
+    for (int64_t k : ks[blk]) {
+      int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
+      k2r[k] = (int)rowa.size();
+      rowa.push_back(block_row0[blk] + state_local[a]);
+      rowb.push_back(block_row0[blk] + state_local[b]);
+      rowm.push_back(sys->m12[a]);
+    }
+    while ((rowa.size() - start) % 128) {  // pad with a zero-weight duplicate of row 0
+      rowa.push_back(rowa[start]);
+      rowb.push_back(rowb[start]);
+      rowm.push_back(rowm[start]);
+    }
+    for (size_t t = start; t < rowa.size(); t += 128) tile_block.push_back((int)blk);
+  }
+  n_rows = (int)rowa.size();
+  n_tiles = n_rows / 128;
+
+  // --- grids and weights
+  Axis ab = axis_gl(grid->n_beta, 0.0, kPi);
+  Axis ag, aa;
+  std::vector<double> wt;
+  if (sys_type == 1) {
+    G2 = grid->n_beta;
+    n_gamma = 1;
+    wt.resize(G2);
+    for (int i = 0; i < G2; ++i) wt[i] = ab.w[i] * sin(ab.x[i]) * ab.half * 2.0 * kPi;
+    ag.x.assign(1, 0.0);
+  } else {
+    ag = grid->eq_gamma ? axis_mid(grid->n_gamma, 0.0, 2.0 * kPi)
+                        : axis_gl(grid->n_gamma, 0.0, 2.0 * kPi);
+    n_gamma = grid->n_gamma;
+    G2 = grid->n_beta * grid->n_gamma;
+    wt.resize(G2);
+    double afac = (grid->n_alpha > 0) ? 1.0 : 2.0 * kPi;
+    for (int ib = 0; ib < grid->n_beta; ++ib)
+      for (int ig = 0; ig < n_gamma; ++ig)
+        wt[ib * n_gamma + ig] = ab.w[ib] * ag.w[ig] * sin(ab.x[ib]) * ab.half * ag.half * afac;
+    if (grid->n_alpha > 0) {
+      aa = axis_mid(grid->n_alpha, 0.0, 2.0 * kPi);
+      n_alpha = grid->n_alpha;
+      std::vector<double> wa(n_alpha);
+      for (int i = 0; i < n_alpha; ++i) wa[i] = aa.w[i] * aa.half;
+      MQCT_CUDA_TRY(d_alpha.upload(aa.x, stream));
+      MQCT_CUDA_TRY(d_walpha.upload(wa, stream));
+      h_alpha = aa.x;
+      h_walpha = wa;
+    }
+  }
+  h_beta = ab.x;
+  h_gamma = ag.x;
+  h_wt = wt;
+  MQCT_CUDA_TRY(d_beta.upload(ab.x, stream));
+  MQCT_CUDA_TRY(d_gamma.upload(ag.x, stream));
+  MQCT_CUDA_TRY(d_wt.upload(wt, stream));
+  MQCT_CUDA_TRY(d_R.upload(Rh, stream));
+
+  // --- system tables
+  std::vector<int> st_chan(n_states), st_m(n_states), ch_j(sys->n_channels);
+  for (int s = 0; s < n_states; ++s) {
+    st_chan[s] = sys->indx_chann[s] - 1;
+    st_m[s] = sys->m12[s];
+  }
+  for (int c = 0; c < sys->n_channels; ++c) ch_j[c] = sys->j1[c];
+  MQCT_CUDA_TRY(d_row_state.upload(row_state, stream));
+  MQCT_CUDA_TRY(d_st_chan.upload(st_chan, stream));
+  MQCT_CUDA_TRY(d_st_m.upload(st_m, stream));
+  MQCT_CUDA_TRY(d_ch_j.upload(ch_j, stream));
+  ldv = sys->ldv > 0 ? sys->ldv : 1;
+  if (sys_type == 4) {
+    MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)sys->n_channels * ldv, stream));
+  } else {
+    std::vector<double> one(sys->n_channels, 1.0);
+    MQCT_CUDA_TRY(d_vec.upload(one, stream));
+    ldv = 1;
+  }
+  MQCT_CUDA_TRY(d_rowa.upload(rowa, stream));
+  MQCT_CUDA_TRY(d_rowb.upload(rowb, stream));
+  MQCT_CUDA_TRY(d_rowm.upload(rowm, stream));
+  MQCT_CUDA_TRY(d_k2r.upload(k2r, stream));
+  h_rowa = rowa;
+  h_rowb = rowb;
+  h_tile_block = tile_block;
+  MQCT_CUDA_TRY(d_tile_block.upload(tile_block, stream));
+
+  // --- PES
+  pes_kind = pes->kind;
+  pes_n_terms = pes->n_terms;
+  if (pes->kind == MQCT_PES_TABLE) {
+    MQCT_CUDA_TRY(d_pes_table.upload(pes->table, (size_t)nR * G2, stream));
+  } else {
+    int per = pes->kind == MQCT_PES_LEGENDRE ? 3 : 6;
+    size_t np = pes->kind == MQCT_PES_LEGENDRE ? 3 * (size_t)pes->n_terms : (size_t)per * pes->n_terms;
+    MQCT_ARG_CHECK(pes->n_terms > 0 && pes->params, "PES without parameters");
+    MQCT_CUDA_TRY(d_pes_p.upload(pes->params, np, stream));
+    if (pes->kind == MQCT_PES_SITES1) {
+      MQCT_ARG_CHECK(pes->n_sites1 > 0 && pes->sites1, "SITES1 PES without sites");
+      for (int t = 0; t < pes->n_terms; ++t) {
+        int s = (int)pes->params[6 * t];
+        MQCT_ARG_CHECK(s >= 0 && s < pes->n_sites1, "PES term %d references site %d", t, s);
+      }
+      MQCT_CUDA_TRY(d_pes_s1.upload(pes->sites1, 3 * (size_t)pes->n_sites1, stream));
+      pes_n_sites1 = pes->n_sites1;
+    }
+  }
+
+  // --- work buffers
+  MQCT_CUDA_TRY(d_psi.alloc((size_t)n_basis_rows * G2));
+  ldw = nR;
+  MQCT_CUDA_TRY(d_W.alloc((size_t)G2 * ldw));
+  MQCT_CUDA_TRY(d_work.alloc((size_t)P * nR));
+  if (precision == MQCT_PREC_FP64) {
+    MQCT_CUDA_TRY(d_acc.alloc((size_t)n_rows * nR));
+  } else {
+    int rc2 = tc_init();
+    if (rc2) return rc2;
+  }
+  MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
+  return MQCT_OK;
+}
+
+int MatrixPlan::run_basis_and_pes() {
+  int threads = 256;
+  int64_t nb = (int64_t)n_basis_rows * G2;
+  basis_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, stream>>>(
+      sys_type, n_basis_rows, d_row_state.p, d_st_chan.p, d_st_m.p, d_ch_j.p, d_vec.p, ldv,
+      d_beta.p, d_gamma.p, n_gamma, G2, d_psi.p);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  PesDev pd{pes_kind, pes_n_terms, pes_n_sites1, 0, d_pes_p.p, d_pes_s1.p, nullptr, d_pes_table.p};
+  int64_t nw = (int64_t)G2 * nR;
+  pes_weight_kernel<<<(unsigned)((nw + threads - 1) / threads), threads, 0, stream>>>(
+      sys_type, pd, G2, nR, d_R.p, d_beta.p, d_gamma.p, n_gamma, d_wt.p, d_W.p, ldw);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  return MQCT_OK;
+}
+
+int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
+  int rc = run_basis_and_pes();
+  if (rc) return rc;
+  if (precision == MQCT_PREC_FP64) {
+    dim3 g((n_rows + F_TM - 1) / F_TM, (nR + F_TN - 1) / F_TN);
+    contract_fp64_kernel<<<g, 256, 0, stream>>>(n_rows, G2, nR, d_rowa.p, d_rowb.p, d_rowm.p,
+                                                d_psi.p, d_W.p, ldw, n_alpha, d_alpha.p,
+                                                d_walpha.p, d_acc.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    finalize_kernel<double><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
+        P, nR, d_k2r.p, d_acc.p, 1, 0, nR, kCmToHartree, d_R.p, ir1, ir2, cut, d_mat, d_y2,
+        d_skipped, d_work.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+  } else {
+    rc = tc_execute();
+    if (rc) return rc;
+    finalize_kernel<float><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
+        P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree,
+        d_R.p, ir1, ir2, cut, d_mat, d_y2, d_skipped, d_work.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+  }
+  return MQCT_OK;
+}
+
+double MatrixPlan::flops() const {
+  double k = (double)G2 * (n_alpha > 0 ? n_alpha : 1);
+  double prods = precision == MQCT_PREC_FP64 ? 1.0 : 3.0;
+  return 2.0 * (double)P * nR * k * prods;
+}
+
+MatrixPlan::~MatrixPlan() {
+  if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace mqct
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int mqct_matrix_plan_create(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                            const double* R, int32_t nR, const mqct_grid_t* grid,
+                            const mqct_pes_t* pes, int32_t precision, double mij_cutoff_cm,
+                            double r_cut1, double r_cut2, mqct_matrix_plan** plan) {
+  MQCT_ARG_CHECK(plan, "null plan pointer");
+  *plan = nullptr;
+  if (mqct_device_count() <= 0) {
+    set_error("no CUDA device available");
+    return MQCT_E_NODEV;
+  }
+  auto* p = new MatrixPlan();
+  int rc = p->init(sys, ind_mat, P, R, nR, grid, pes, precision, mij_cutoff_cm, r_cut1, r_cut2);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *plan = reinterpret_cast<mqct_matrix_plan*>(p);
+  return MQCT_OK;
+}
+
+int mqct_matrix_plan_execute(mqct_matrix_plan* plan, double* d_mat, double* d_y2,
+                             int32_t* d_skipped) {
+  MQCT_ARG_CHECK(plan && d_mat, "null argument");
+  return reinterpret_cast<MatrixPlan*>(plan)->execute(d_mat, d_y2, d_skipped);
+}
+
+int mqct_matrix_plan_sync(mqct_matrix_plan* plan) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MQCT_CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<MatrixPlan*>(plan)->stream));
+  return MQCT_OK;
+}
+
+double mqct_matrix_plan_flops(const mqct_matrix_plan* plan) {
+  return plan ? reinterpret_cast<const MatrixPlan*>(plan)->flops() : 0.0;
+}
+
+void mqct_matrix_plan_destroy(mqct_matrix_plan* plan) {
+  delete reinterpret_cast<MatrixPlan*>(plan);
+}
+
+int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, const double* R,
+                      int32_t nR, const mqct_grid_t* grid, const mqct_pes_t* pes,
+                      int32_t precision, double mij_cutoff_cm, double r_cut1, double r_cut2,
+                      double* Mat_el, double* Mat_el_y2, int32_t* skipped,
+                      mqct_err_report_t* err) {
+  MQCT_ARG_CHECK(Mat_el, "null Mat_el");
+  mqct_matrix_plan* h = nullptr;
+  int rc = mqct_matrix_plan_create(sys, ind_mat, P, R, nR, grid, pes, precision, mij_cutoff_cm,
+                                   r_cut1, r_cut2, &h);
+  if (rc) return rc;
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(h);
+  DevBuf<double> dm, dy;
+  DevBuf<int> ds;
+  cudaError_t e = dm.alloc((size_t)P * nR);
+  if (e == cudaSuccess) e = dy.alloc((size_t)P * nR);
+  if (e == cudaSuccess) e = ds.alloc((size_t)P);
+  if (e != cudaSuccess) {
+    set_error("device allocation failed: %s", cudaGetErrorString(e));
+    mqct_matrix_plan_destroy(h);
+    return MQCT_E_CUDA;
+  }
+  rc = p->execute(dm.p, dy.p, ds.p);
+  if (!rc && err && err->n_sampled > 0 && precision != MQCT_PREC_FP64) rc = p->error_report(dm.p, err);
+  if (!rc) {
+    cudaMemcpyAsync(Mat_el, dm.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, p->stream);
+    if (Mat_el_y2)
+      cudaMemcpyAsync(Mat_el_y2, dy.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, p->stream);
+    if (skipped) cudaMemcpyAsync(skipped, ds.p, sizeof(int) * P, cudaMemcpyDeviceToHost, p->stream);
+    e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) {
+      set_error("matrix build failed: %s", cudaGetErrorString(e));
+      rc = MQCT_E_CUDA;
+    }
+  }
+  mqct_matrix_plan_destroy(h);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// matrix_plan.cuh -- state of one matrix-build plan (uploaded system, grids,
+// GEMM row order) shared by the FP64 and tcgen05 contraction paths.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+
+namespace mqct {
+
+struct MatrixPlan {
+  // problem
+  int sys_type = 0, precision = 0;
+  int64_t P = 0;
+  int nR = 0, n_states = 0;
+  int G2 = 0;        // 2-D grid points (beta x gamma) or beta points (type 1)
+  int n_gamma = 1;
+  int n_alpha = 0;   // explicit alpha grid points (0: analytic 2*pi)
+  int ldv = 1;
+  int ir1 = 0, ir2 = 0;
+  double cut = 0.0;
+  int pes_kind = 0, pes_n_terms = 0, pes_n_sites1 = 0;
+  std::vector<double> Rh, h_beta, h_gamma, h_wt, h_alpha, h_walpha;
+  cudaStream_t stream = nullptr;
+
+  // GEMM rows: pairs grouped by m-block, each block padded to a multiple of 128
+  int n_rows = 0, n_tiles = 0, n_basis_rows = 0;
+  std::vector<int> h_rowa, h_rowb, h_tile_block;
+  DevBuf<int> d_rowa, d_rowb, d_rowm, d_k2r, d_tile_block;
+  DevBuf<int> d_row_state, d_st_chan, d_st_m, d_ch_j;
+  DevBuf<double> d_vec, d_beta, d_gamma, d_wt, d_alpha, d_walpha, d_R;
+  DevBuf<double> d_pes_p, d_pes_s1, d_pes_table;
+
+  // work
+  DevBuf<double2> d_psi;  // basis rows x G2, FP64
+  DevBuf<double> d_W;     // G2 x ldw, FP64
+  int ldw = 0;
+  DevBuf<double> d_acc;   // FP64 form: n_rows x nR
+  DevBuf<double> d_work;  // spline scratch P x nR
+
+  // tcgen05 split-precision path (contract_tc.cu)
+  int tc_splits = 1, tc_ldp = 0, tc_npad = 0, tc_nchunk = 0;
+  DevBuf<float> d_part;                 // tc_splits x n_rows x tc_ldp
+  DevBuf<unsigned short> d_bimg;        // pre-swizzled B (W) images, hi/lo planes
+  DevBuf<float2> d_psi32;               // basis in FP32, chunk-major per row
+  DevBuf<int> d_status;
+  int tc_init();
+  int tc_execute();
+  int error_report(const double* d_mat, mqct_err_report_t* err);
+
+  int init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, const double* R, int32_t nR,
+           const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec, double mij_cut,
+           double rc1, double rc2);
+  int run_basis_and_pes();
+  int execute(double* d_mat, double* d_y2, int32_t* d_skipped);
+  double flops() const;
+  ~MatrixPlan();
+};
+
+}  // namespace mqct

@@ -914,20 +914,15 @@ static void orc_ws_free(orc_rhs_ws* w) {
   free(w->du); free(w->uidx); free(w->misc); free(w->m); free(w->dm); free(w->phi_amp); free(w->sc);
 }
 
-/* potential_data_bk + splint_bk: linear extrapolation below R_1, zero above R_n,
- * cubic spline with derivative in between.  SRC/mqct_eqtns.f:501-611. */
+/* potential_data_bk + splint_bk, SRC/mqct_eqtns.f:501-611: zero above R_n,
+ * cubic spline with derivative otherwise.  Below R_1 the reference computes a
+ * linear extrapolation (:534-543) but does not return, so splint_bk overwrites
+ * it with the cubic of the first interval (bisection gives klo=1, khi=2); that
+ * effective behaviour is what is restated here. */
 static void orc_matrix_at(const orc_tables* t, double x, double* m, double* dm) {
   int nR = t->nR;
   const double* R = t->R;
   int64_t P = t->P;
-  if (x < R[0]) {
-    for (int64_t k = 0; k < P; ++k) {
-      const double* c = t->mat + (size_t)k * nR;
-      dm[k] = (c[1] - c[0]) / (R[1] - R[0]);
-      m[k] = dm[k] * (x - R[0]) + c[0];
-    }
-    return;
-  }
   if (x > R[nR - 1]) {
     for (int64_t k = 0; k < P; ++k) { m[k] = 0.0; dm[k] = 0.0; }
     return;
