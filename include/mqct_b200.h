@@ -97,8 +97,9 @@ typedef struct mqct_grid_t {
 /* Potential energy surface (the USER_DEFINED_PES plugin, called through the
  * per-type wrappers of MQCT_SOURCE_CODES/pes_sys_type.f:2-97).  Values in
  * cm^-1, R in bohr.
- *   TABLE:    caller-evaluated V on the grid, table[iR*K + g] (K grid points in
- *             the library's grid order: beta outer, gamma, alpha inner), the
+ *   TABLE:    caller-evaluated V on the (beta, gamma) grid, table[iR*G + g]
+ *             with g = i_beta*n_gamma + i_gamma (G = n_beta for type 1); the
+ *             surface of an atom + rigid rotor does not depend on alpha.  The
  *             analogue of the reference's VGRID_UF.DAT path;
  *   LEGENDRE: V(R,beta) = sum_l [A_l e^{-b_l R} - C_l/R^6] P_l(cos beta),
  *             params = [A_0..A_{n-1}, b_0.., C_0..];
@@ -155,6 +156,10 @@ int mqct_matrix_plan_sync(mqct_matrix_plan* plan);
 /* Flops of the contraction actually executed per build (2*P*nR*K times the
  * number of split-precision products). */
 double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
+/* CUDA-event timings (ms) of the last execute, recorded on the plan's stream:
+ * t3[0] basis + PES tables, t3[1] contraction, t3[2] finalize (units, cutoff,
+ * spline).  Waits for the execute to finish. */
+int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3);
 void mqct_matrix_plan_destroy(mqct_matrix_plan* plan);
 
 /* Propagation tables after READ_MIJ / MATRIX_MAKE: the retained pairs only
@@ -219,6 +224,8 @@ int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_in
 int mqct_prop_plan_sync(mqct_prop_plan* plan);
 /* Algorithmic table bytes per trajectory step (16 * P for FP32, 32 * P for FP64). */
 double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan);
+/* CUDA-event time (ms) of the last propagation kernel on the plan's stream. */
+int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms);
 void mqct_prop_plan_destroy(mqct_prop_plan* plan);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */

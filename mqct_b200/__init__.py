@@ -216,6 +216,12 @@ class MatrixPlan:
     def sync(self):
         check(lib().mqct_matrix_plan_sync(self.h))
 
+    def timing(self):
+        """(basis+PES, contraction, finalize) milliseconds of the last execute."""
+        t = (C.c_float * 3)()
+        check(lib().mqct_matrix_plan_timing(self.h, t))
+        return tuple(float(x) for x in t)
+
     def close(self):
         if self.h:
             lib().mqct_matrix_plan_destroy(self.h)
@@ -383,6 +389,12 @@ class PropagationPlan:
 
     def sync(self):
         check(lib().mqct_prop_plan_sync(self.h))
+
+    def timing(self):
+        """Kernel milliseconds of the last run."""
+        t = C.c_float()
+        check(lib().mqct_prop_plan_timing(self.h, C.byref(t)))
+        return float(t.value)
 
     def close(self):
         if self.h:

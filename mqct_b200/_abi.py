@@ -78,9 +78,10 @@ class AtPaths(C.Structure):
 EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
-    "mqct_matrix_plan_flops", "mqct_matrix_plan_destroy", "mqct_propagate_batch",
+    "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy", "mqct_propagate_batch",
     "mqct_prop_plan_create", "mqct_prop_plan_run", "mqct_prop_plan_run_device",
-    "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_destroy",
+    "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
+    "mqct_prop_plan_destroy",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
     "mqct_fill_ind_mat", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
     "mqct_read_mtrx_uf",
@@ -111,6 +112,8 @@ def lib():
     L.mqct_matrix_plan_sync.argtypes = [vp]
     L.mqct_matrix_plan_flops.argtypes = [vp]
     L.mqct_matrix_plan_flops.restype = C.c_double
+    L.mqct_matrix_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
+    L.mqct_prop_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
     L.mqct_matrix_plan_destroy.argtypes = [vp]
     L.mqct_matrix_plan_destroy.restype = None
     L.mqct_propagate_batch.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,

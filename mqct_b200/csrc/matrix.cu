@@ -347,6 +347,7 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
   ir2 = nearest_index(Rh, rc2);
   cut = mij_cut * kCmToHartree;
   MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (auto& e : ev) MQCT_CUDA_TRY(cudaEventCreate(&e));
 
   // --- states -> m-blocks
   std::map<int, std::vector<int>> by_m;
@@ -521,14 +522,17 @@ int MatrixPlan::run_basis_and_pes() {
 }
 
 int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
+  MQCT_CUDA_TRY(cudaEventRecord(ev[0], stream));
   int rc = run_basis_and_pes();
   if (rc) return rc;
+  MQCT_CUDA_TRY(cudaEventRecord(ev[1], stream));
   if (precision == MQCT_PREC_FP64) {
     dim3 g((n_rows + F_TM - 1) / F_TM, (nR + F_TN - 1) / F_TN);
     contract_fp64_kernel<<<g, 256, 0, stream>>>(n_rows, G2, nR, d_rowa.p, d_rowb.p, d_rowm.p,
                                                 d_psi.p, d_W.p, ldw, n_alpha, d_alpha.p,
                                                 d_walpha.p, d_acc.p);
     MQCT_CUDA_TRY(cudaGetLastError());
+    MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
     finalize_kernel<double><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
         P, nR, d_k2r.p, d_acc.p, 1, 0, nR, kCmToHartree, d_R.p, ir1, ir2, cut, d_mat, d_y2,
         d_skipped, d_work.p);
@@ -536,11 +540,13 @@ int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
   } else {
     rc = tc_execute();
     if (rc) return rc;
+    MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
     finalize_kernel<float><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
         P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree,
         d_R.p, ir1, ir2, cut, d_mat, d_y2, d_skipped, d_work.p);
     MQCT_CUDA_TRY(cudaGetLastError());
   }
+  MQCT_CUDA_TRY(cudaEventRecord(ev[3], stream));
   return MQCT_OK;
 }
 
@@ -551,6 +557,8 @@ double MatrixPlan::flops() const {
 }
 
 MatrixPlan::~MatrixPlan() {
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -588,6 +596,14 @@ int mqct_matrix_plan_execute(mqct_matrix_plan* plan, double* d_mat, double* d_y2
 int mqct_matrix_plan_sync(mqct_matrix_plan* plan) {
   MQCT_ARG_CHECK(plan, "null plan");
   MQCT_CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<MatrixPlan*>(plan)->stream));
+  return MQCT_OK;
+}
+
+int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3) {
+  MQCT_ARG_CHECK(plan && t3, "null argument");
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  MQCT_CUDA_TRY(cudaEventSynchronize(p->ev[3]));
+  for (int i = 0; i < 3; ++i) MQCT_CUDA_TRY(cudaEventElapsedTime(&t3[i], p->ev[i], p->ev[i + 1]));
   return MQCT_OK;
 }
 

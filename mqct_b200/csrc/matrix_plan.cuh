@@ -21,6 +21,7 @@ struct MatrixPlan {
   int pes_kind = 0, pes_n_terms = 0, pes_n_sites1 = 0;
   std::vector<double> Rh, h_beta, h_gamma, h_wt, h_alpha, h_walpha;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   // GEMM rows: pairs grouped by m-block, each block padded to a multiple of 128
   int n_rows = 0, n_tiles = 0, n_basis_rows = 0;

@@ -512,6 +512,7 @@ struct PropPlan {
   int N = 0, P = 0, nR = 0, n_blocks = 0, n_e = 0, nmax = 0;
   double mass = 0.0;
   cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<double> d_R, d_e_val, d_cplus, d_cminus;
   DevBuf<int> d_blk_off, d_blk_n, d_blk_s0, d_blk_states, d_pair_loc, d_st_e, d_queue;
   DevBuf<float2> d_knots32;
@@ -562,6 +563,8 @@ struct PropPlan {
     nR = tab->nR;
     mass = tab->mass_au;
     MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    MQCT_CUDA_TRY(cudaEventCreate(&ev0));
+    MQCT_CUDA_TRY(cudaEventCreate(&ev1));
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -687,7 +690,9 @@ struct PropPlan {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PT, sb);
     int grid = (int)std::min<int64_t>(n_traj, (int64_t)n_sm * std::max(per_sm, 1));
     void* args[] = {&d, (void*)&d_init_p, &n_traj_i, &d_queue.p, &o};
+    MQCT_CUDA_TRY(cudaEventRecord(ev0, stream));
     MQCT_CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(PT), args, sb, stream));
+    MQCT_CUDA_TRY(cudaEventRecord(ev1, stream));
     return MQCT_OK;
   }
 
@@ -739,6 +744,8 @@ struct PropPlan {
   }
 
   ~PropPlan() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -818,6 +825,14 @@ double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan) {
   if (!plan) return 0.0;
   const PropPlan* p = reinterpret_cast<const PropPlan*>(plan);
   return (p->arith == MQCT_PROP_FP32 ? 16.0 : 32.0) * p->P;
+}
+
+int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms) {
+  MQCT_ARG_CHECK(plan && ms, "null argument");
+  PropPlan* p = reinterpret_cast<PropPlan*>(plan);
+  MQCT_CUDA_TRY(cudaEventSynchronize(p->ev1));
+  MQCT_CUDA_TRY(cudaEventElapsedTime(ms, p->ev0, p->ev1));
+  return MQCT_OK;
 }
 
 void mqct_prop_plan_destroy(mqct_prop_plan* plan) { delete reinterpret_cast<PropPlan*>(plan); }

@@ -115,11 +115,15 @@ def test_at_mode_matches_oracle(mq, oracle, gpu_available):
     mass = tab.mass_au
     E = 500.0 * syn.CM_TO_HARTREE
     v = np.sqrt(2 * E / mass)
-    paths = [_straight_path(b, v, 20.0, mass) for b in (0.5, 3.0, 6.0)]
+    paths = [_straight_path(b, v, 20.0, mass) for b in (4.0, 6.0, 9.0)]
     trajs = [mq.Trajectory(E, 0.0, 1, 20.0, 20.0, 20.0) for _ in paths]
     amp, cls, diag = mq.propagate(tab, trajs, arith=mq.PROP_FP64, mode=mq.MODE_AT, at_paths=paths)
     for i, p in enumerate(paths):
         oamp, odiag = oracle.dotraject_at(otab, oracle.make_traj(E, 0.0, 1, 20.0, 20.0, 20.0), p)
         assert np.max(np.abs(amp[i] - oamp)) < 1e-9
         assert diag[i, 1] == odiag[1]
+        assert abs(diag[i, 0] - odiag[0]) < 1e-9 * odiag[0]
     assert np.all(np.abs(diag[:, 2]) < 1e-8)
+    # the path passes the coupling region: population leaves the initial state
+    p = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
+    assert p[0, 0] < 0.999
