@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark of the MQCT hot paths on B200.
+
+Headline (`value`): the state-to-state matrix build of the asymmetric top + atom
+workload (A, B, C = 27.9, 14.5, 9.3 cm^-1, j <= 8 all tau and m: 969 states,
+31 977 same-m pairs; 12-term site-site PES; angular grid 48 GL beta x 48 gamma x
+48 alpha as written; 300 R points 3-25 bohr), in matrix elements (pairs x R
+points) per second.  One step = one full build: rotor basis + PES tables +
+contraction + units/cutoff/spline, inputs resident on the device.
+
+Secondary (`propagation`): batched trajectory propagation on that matrix
+(trajectories with b ~ U(0,15) bohr, E log-uniform 50-2000 cm^-1, RK4 dt=5 a.u.
+until R > 25 bohr), trajectories per second, FP32 arithmetic, and the plain
+FP64 GPU form of both paths for the speed-up.
+
+`--impl reference` times the reference algorithm on the host cores instead: the
+CPU restatement of INTEGRATOR_TEMP (wavefunctions re-evaluated at every grid
+point for every element and R, as the reference does) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="mqct", choices=["mqct", "reference"])
+    p.add_argument("--precision", default="auto", choices=["auto", "bf16x3", "fp64"])
+    p.add_argument("--c3-traj", type=int, default=1024,
+                   help="trajectories of the propagation workload timed (4096 = full set)")
+    p.add_argument("--no-propagation", action="store_true")
+    p.add_argument("--no-fp64-form", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- workload
+def workload():
+    import mqct_b200 as mq
+    from mqct_b200 import synthetic as syn
+    c2 = syn.config_c2(alpha_grid=True)
+    s = mq.CollisionSystem(4, c2["channels"], A=c2["A"], B=c2["B"], C=c2["C"])
+    R = mq.r_grid(c2["nR"], c2["rmin"], c2["rmax"])
+    return c2, s, R
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU arm
+def _matrix_bench(mq, s, R, c2, precision, steps, warmup, torch, flush):
+    plan = mq.MatrixPlan(s, R, c2["grid"], c2["pes"], precision=precision)
+    n = s.P * len(R)
+    d_mat = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_y2 = torch.empty(n, dtype=torch.float64, device="cuda")
+    d_sk = torch.empty(s.P, dtype=torch.int32, device="cuda")
+    for _ in range(warmup):
+        plan.execute(d_mat.data_ptr(), d_y2.data_ptr(), d_sk.data_ptr())
+        plan.sync()
+    seg = []
+    for _ in range(steps):
+        flush()
+        torch.cuda.synchronize()
+        plan.execute(d_mat.data_ptr(), d_y2.data_ptr(), d_sk.data_ptr())
+        seg.append(plan.timing())
+    torch.cuda.synchronize()
+    return plan, d_mat, d_sk, np.array(seg)
+
+
+def run_gpu(a):
+    import torch
+    import mqct_b200 as mq
+    from mqct_b200 import synthetic as syn
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    c2, s, R = workload()
+    peaks, peak_src = _peaks()
+    prec = mq.PREC_BF16X3 if a.precision in ("auto", "bf16x3") else mq.PREC_FP64
+    if a.precision == "auto":
+        try:
+            mq.MatrixPlan(s, R[:4], (8, 8, 0, 0, 0, 0, 1), c2["pes"], precision=prec).close()
+        except mq.MqctError:
+            prec = mq.PREC_FP64
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def flush():  # write 256 MB (> 126 MB L2) between timed steps
+        flush_buf.fill_(1.0)
+
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0] or 0)
+    barrier()
+    with Clocks(gpu_index) as clk:
+        t0 = time.perf_counter()
+        plan, d_mat, d_sk, seg = _matrix_bench(mq, s, R, c2, prec, a.steps, a.warmup, torch, flush)
+        barrier()
+        wall = time.perf_counter() - t0
+    step_ms = seg.sum(axis=1)
+    ms = float(np.mean(step_ms))
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    n_el = s.P * len(R)
+    value = world * n_el / (ms / 1e3)
+    flops = plan.flops
+    contract_ms = float(np.mean(seg[:, 1]))
+    achieved_tf = flops / (contract_ms / 1e3) / 1e12
+    out = {}
+
+    # plain FP64 GPU form of the same build, and the accuracy of the split path
+    fp64 = None
+    acc = None
+    if not a.no_fp64_form and prec != mq.PREC_FP64:
+        plan64, d_mat64, d_sk64, seg64 = _matrix_bench(mq, s, R, c2, mq.PREC_FP64, 1, 1, torch, flush)
+        ms64 = float(seg64.sum(axis=1).mean())
+        fp64 = {"ms_per_step": ms64, "speedup": ms64 / ms}
+        m1 = d_mat.view(s.P, len(R)).double()
+        m0 = d_mat64.view(s.P, len(R)).double()
+        keep = (d_sk == 0) & (d_sk64 == 0)
+        rowmax = m0.abs().amax(dim=1, keepdim=True)
+        gmax = m0.abs().max()
+        d = (m1 - m0).abs()
+        rel_row = (d / rowmax.clamp_min(1e-300))[keep]
+        rel_floor = (d / torch.maximum(m0.abs(), 1e-8 * rowmax).clamp_min(1e-300))[keep]
+        acc = {"max_rel_err_vs_fp64_rowmax": float(rel_row.max()),
+               "p99_rel_err_vs_fp64_rowmax": float(torch.quantile(rel_row.flatten()[:2_000_000], 0.99)),
+               "max_rel_err_floor_1e-8": float(rel_floor.max()),
+               "max_abs_err_hartree": float(d.max()),
+               "skip_flags_equal": bool(torch.equal(d_sk, d_sk64))}
+        plan64.close()
+    plan.close()
+    del d_mat
+
+    # e2e through the C ABI with host buffers (H2D of the system, D2H of Mat_el, y2, flags)
+    e2e_ms = []
+    for i in range(max(1, min(a.steps, 3))):
+        flush()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        mat, y2, sk = mq.build_matrix(s, R, c2["grid"], c2["pes"], precision=prec)
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    h2d = (s.ind_mat.nbytes + R.nbytes + s.indx_chann.nbytes * 3 + s.vec1.nbytes +
+           c2["pes"]["params"].nbytes + c2["pes"]["sites1"].nbytes)
+    d2h = mat.nbytes + y2.nbytes + sk.nbytes
+
+    # propagation (secondary)
+    prop = None
+    if not a.no_propagation:
+        prop = run_propagation(mq, syn, s, R, mat, a, torch, world)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    cpu = cpu_baseline_matrix(s, R, c2, a.cpu_seconds)
+    tc = prec == mq.PREC_BF16X3
+    peak = peaks.get("bf16_tflops", 1590.0)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "matrix elements/s",
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16x3-fp32acc" if tc else "f64",
+        "data": "synthetic (seeded site-site PES; no dataset)",
+        "config": {"workload": "asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), "
+                               "grid 48 GL beta x 48 gamma x 48 alpha, 300 R 3-25 bohr",
+                   "precision": "BF16x3 tcgen05" if tc else "FP64 CUDA cores",
+                   "elements_per_step": n_el, "grid_points": 48 * 48 * 48,
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "parallelism": f"replicas x{world}"},
+        "segments_ms": {"basis_pes": float(seg[:, 0].mean()), "contraction": contract_ms,
+                        "finalize": float(seg[:, 2].mean())},
+        "roofline": {"bound": "tensor" if tc else "fp64", "achieved": achieved_tf,
+                     "peak": peak if tc else None, "unit": "TFLOP/s",
+                     "frac": achieved_tf / peak if tc else None, "traffic": None,
+                     "peak_source": f"bf16_tflops ({peak_src})",
+                     "flops_per_launch": flops, "kernel": "contraction"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n_el / (float(np.median(e2e_ms)) / 1e3), "unit": "matrix elements/s",
+                "ms": float(np.median(e2e_ms)), "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "clocks": clk.summary(),
+        "gpu_launches": int(a.steps * 4),
+        "fp64_form": fp64,
+        "accuracy": acc,
+        "propagation": prop,
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_propagation(mq, syn, s, R, mat, a, torch, world):
+    c3 = syn.config_c3()
+    tab = mq.PropagationTables.from_system(s, R, mat, syn.config_c2()["mass_amu"])
+    n = min(a.c3_traj, c3["n_traj"])
+    E = c3["E_cm"][:n] * syn.CM_TO_HARTREE
+    k = np.sqrt(2 * tab.mass_au * E)
+    b = c3["b"][:n]
+    l = np.sqrt(np.maximum((b * k) ** 2 + 0.25, 0.0)) - 0.5   # b = sqrt(l(l+1))/k
+    trajs = [mq.Trajectory(float(E[i]), float(l[i]), 1, c3["dt"], c3["r_fin"], c3["r_fin"],
+                           max_steps=400000) for i in range(n)]
+    res = {}
+    for name, arith, nt in (("fp32", mq.PROP_FP32, n), ("fp64", mq.PROP_FP64, min(n, 256))):
+        plan = mq.PropagationPlan(tab, arith)
+        plan.run(trajs[:min(8, nt)])  # warm-up
+        t0 = time.perf_counter()
+        amp, cls, diag = plan.run(trajs[:nt])
+        wall = time.perf_counter() - t0
+        ms = plan.timing()
+        steps = float(diag[:, 1].sum())
+        res[name] = {"n_traj": nt, "kernel_ms": ms, "wall_s": wall,
+                     "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
+                     "table_bytes_per_step": plan.bytes_per_step,
+                     "achieved_table_GBs": steps * plan.bytes_per_step / (ms / 1e3) / 1e9,
+                     "max_status": float(diag[:, 4].max())}
+        if name == "fp32":
+            res["prob_fp32"] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
+        else:
+            p64 = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
+            p32 = res.pop("prob_fp32")[:nt]
+            res["max_abs_prob_diff_fp32_vs_fp64"] = float(np.abs(p32 - p64).max())
+        plan.close()
+    res["speedup_fp32_vs_fp64_form"] = res["fp32"]["traj_per_s"] / res["fp64"]["traj_per_s"]
+    res["workload"] = (f"{n} of the 4096 trajectories (b~U(0,15), E log-uniform 50-2000 cm^-1, "
+                       "dt=5 a.u., R>25 stop), c2 matrix, retained pairs "
+                       f"{tab.P} of {s.P}")
+    return res
+
+
+# ---------------------------------------------------------------- CPU / reference arm
+def cpu_baseline_matrix(s, R, c2, seconds, n_threads=0):
+    """The reference algorithm (INTEGRATOR_TEMP restated, wavefunctions re-evaluated
+    at every grid point) on a bounded sample of elements at one R point."""
+    from oracle import pyoracle as po
+    po.build()
+    ch = s.channels
+    osys = po.OracleSystem(4, ch[:, 0], ch[:, 1], ch[:, 2], e_ch=s.e_ch,
+                           vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    states = osys.states()
+    pd = c2["pes"]
+    pes = po.OraclePes(pd["kind"], pd["n_terms"], pd["params"], sites1=pd["sites1"])
+    cores = n_threads or os.cpu_count()
+    n_el = cores
+    k0 = s.P // 2
+    t0 = time.perf_counter()
+    po.integrate_elements(osys, states, s.ind_mat, R, c2["grid"], pes, literal=True,
+                          k_range=(k0, k0 + n_el), r_range=(150, 151), n_threads=n_threads)
+    t1 = time.perf_counter() - t0
+    n2 = int(max(cores, min(s.P - k0, n_el * max(1.0, (seconds - t1) / max(t1, 1e-3)))))
+    n2 = (n2 // cores) * cores or cores
+    t0 = time.perf_counter()
+    po.integrate_elements(osys, states, s.ind_mat, R, c2["grid"], pes, literal=True,
+                          k_range=(k0, k0 + n2), r_range=(150, 151), n_threads=n_threads)
+    t2 = time.perf_counter() - t0
+    return {"value": n2 / t2, "unit": "matrix elements/s", "cores": cores, "kind": "port",
+            "sample": f"{n2} elements x 1 R point of the same build (literal INTEGRATOR_TEMP "
+                      f"restatement, {cores} OpenMP threads), {t2:.1f} s"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    c2, s, R = workload()
+    vals = []
+    for _ in range(a.warmup):
+        cpu_baseline_matrix(s, R, c2, 2.0)
+    t0 = time.perf_counter()
+    last = None
+    for _ in range(a.steps):
+        last = cpu_baseline_matrix(s, R, c2, a.cpu_seconds / 2)
+        vals.append(last["value"])
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "matrix elements/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": (time.perf_counter() - t0) / a.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded site-site PES; no dataset)",
+            "config": {"workload": "asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), "
+                                   "grid 48 GL beta x 48 gamma x 48 alpha, 300 R 3-25 bohr"},
+            "cpu_baseline": dict(last, value=v),
+            "e2e": {"value": v, "unit": "matrix elements/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_gpu(a)
+
+
+if __name__ == "__main__":
+    main()

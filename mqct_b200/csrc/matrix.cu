@@ -15,7 +15,8 @@
 //   K1 basis_kernel        rotor wavefunctions on the grid, FP64, per m-block
 //   K2 pes_weight_kernel   PES on (grid x R) times the quadrature weights
 //   K3 contract_fp64_kernel / tcgen05 split-precision kernel (contract_tc.cu)
-//   K4 finalize_kernel     Hartree units, MIJ_CUTOFF, clamped spline y2
+//   K4 reduce_kernel + spline_kernel: FP64 sum of partials, Hartree units,
+//                          MIJ_CUTOFF, clamped spline y2
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -252,57 +253,87 @@ contract_fp64_kernel(int n_rows, int G2, int nR, const int* __restrict__ row_a,
 }
 
 // ------------------------------------------------------------------ K4: finalize
-// Per reference element k: sum the contraction partials (FP64), convert to
-// Hartree, apply MIJ_CUTOFF (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997) and
-// build the clamped spline with finite-difference end slopes
-// (:2005-2016, NR spline MQCT_SOURCE_CODES/suppl_routines.f:914-965).
-// Partials: n_part slabs of (n_rows x ldp) FP64 or FP32 values.
+// (a) reduce_kernel: one CTA per reference element k: sum the contraction
+//     partials of its GEMM row in FP64, convert to Hartree, write Mat_el(:,k)
+//     (coalesced along R) and apply MIJ_CUTOFF at R~r_cut1/r_cut2
+//     (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997): the column is zeroed and
+//     flagged when max(|M(ir1)|, |M(ir2)|) < cut.
 template <class TP>
-__global__ void finalize_kernel(int64_t P, int nR, const int* __restrict__ k_to_row,
-                                const TP* __restrict__ part, int n_part, int64_t part_stride,
-                                int ldp, double scale, const double* __restrict__ R, int ir1,
-                                int ir2, double cut, double* __restrict__ mat,
-                                double* __restrict__ y2, int* __restrict__ skipped,
-                                double* __restrict__ work) {
-  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= P) return;
-  int row = k_to_row[k];
+__global__ void reduce_kernel(int64_t P, int nR, const int* __restrict__ k_to_row,
+                              const TP* __restrict__ part, int n_part, int64_t part_stride, int ldp,
+                              double scale, int ir1, int ir2, double cut, double* __restrict__ mat,
+                              int* __restrict__ skipped) {
+  __shared__ double cut_vals[2];
+  const int64_t k = blockIdx.x;
+  const int row = k_to_row[k];
   double* col = mat + (size_t)k * nR;
-  for (int i = 0; i < nR; ++i) {
+  for (int i = threadIdx.x; i < nR; i += blockDim.x) {
     double s = 0.0;
     for (int p = 0; p < n_part; ++p) s += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
-    col[i] = s * scale;
+    s *= scale;
+    col[i] = s;
+    if (i == ir1) cut_vals[0] = s;
+    if (i == ir2) cut_vals[1] = s;
   }
-  double mx = fmax(fabs(col[ir1]), fabs(col[ir2]));
-  double* yy = y2 ? y2 + (size_t)k * nR : nullptr;
-  if (mx < cut) {
-    for (int i = 0; i < nR; ++i) {
-      col[i] = 0.0;
-      if (yy) yy[i] = 0.0;
+  __syncthreads();
+  const bool drop = fmax(fabs(cut_vals[0]), fabs(cut_vals[1])) < cut;
+  if (drop)
+    for (int i = threadIdx.x; i < nR; i += blockDim.x) col[i] = 0.0;
+  if (threadIdx.x == 0 && skipped) skipped[k] = drop ? 1 : 0;
+}
+
+// (b) spline_kernel: clamped cubic spline with finite-difference end slopes
+//     (MQCT_SOURCE_CODES/matrix_ini.f:2005-2016; NR spline recurrence of
+//     MQCT_SOURCE_CODES/suppl_routines.f:914-965).  The grid-only coefficients
+//     (sig, the y2 recurrence factor and 1/p) are precomputed; 32 elements per
+//     CTA are staged through shared memory so that global reads and writes are
+//     coalesced along R.  Flagged columns get y2 = 0.
+constexpr int SPL_EL = 32;
+__global__ void spline_kernel(int64_t P, int nR, const double* __restrict__ R,
+                              const double* __restrict__ coef, const double* __restrict__ mat,
+                              const int* __restrict__ skipped, double* __restrict__ y2) {
+  extern __shared__ double spl_sm[];
+  const int ld = nR + 1;
+  double* tile = spl_sm;                    // SPL_EL x ld values, then reused for y2
+  double* uu = spl_sm + SPL_EL * ld;        // SPL_EL x ld scratch
+  const int64_t k0 = (int64_t)blockIdx.x * SPL_EL;
+  const int nel = (int)((P - k0) < SPL_EL ? (P - k0) : SPL_EL);
+  for (int q = threadIdx.x; q < nel * nR; q += blockDim.x) {
+    int e = q / nR, i = q % nR;
+    tile[e * ld + i] = mat[(size_t)(k0 + e) * nR + i];
+  }
+  __syncthreads();
+  const int e = threadIdx.x;
+  if (e < nel) {
+    double* y = tile + e * ld;
+    double* u = uu + e * ld;
+    const double* sig = coef;              // [nR]
+    const double* yc = coef + nR;          // y2 recurrence factor [nR]
+    const double* pinv = coef + 2 * nR;    // 1/p [nR]
+    const bool zero = skipped && skipped[k0 + e];
+    if (!zero) {
+      double yp1 = (y[1] - y[0]) / (R[1] - R[0]);
+      double ypn = (y[nR - 1] - y[nR - 2]) / (R[nR - 1] - R[nR - 2]);
+      u[0] = (3.0 / (R[1] - R[0])) * ((y[1] - y[0]) / (R[1] - R[0]) - yp1);
+      for (int i = 1; i < nR - 1; ++i)
+        u[i] = (6.0 * ((y[i + 1] - y[i]) / (R[i + 1] - R[i]) - (y[i] - y[i - 1]) / (R[i] - R[i - 1])) /
+                    (R[i + 1] - R[i - 1]) -
+                sig[i] * u[i - 1]) *
+               pinv[i];
+      double un = (3.0 / (R[nR - 1] - R[nR - 2])) *
+                  (ypn - (y[nR - 1] - y[nR - 2]) / (R[nR - 1] - R[nR - 2]));
+      double last = (un - 0.5 * u[nR - 2]) / (0.5 * yc[nR - 2] + 1.0);
+      y[nR - 1] = last;  // the values are no longer needed: reuse the row for y2
+      for (int i = nR - 2; i >= 0; --i) y[i] = yc[i] * y[i + 1] + u[i];
+    } else {
+      for (int i = 0; i < nR; ++i) y[i] = 0.0;
     }
-    if (skipped) skipped[k] = 1;
-    return;
   }
-  if (skipped) skipped[k] = 0;
-  if (!yy) return;
-  double* u = work + (size_t)k * nR;
-  double yp1 = (col[1] - col[0]) / (R[1] - R[0]);
-  double ypn = (col[nR - 1] - col[nR - 2]) / (R[nR - 1] - R[nR - 2]);
-  yy[0] = -0.5;
-  u[0] = (3.0 / (R[1] - R[0])) * ((col[1] - col[0]) / (R[1] - R[0]) - yp1);
-  for (int i = 1; i < nR - 1; ++i) {
-    double sig = (R[i] - R[i - 1]) / (R[i + 1] - R[i - 1]);
-    double p = sig * yy[i - 1] + 2.0;
-    yy[i] = (sig - 1.0) / p;
-    u[i] = (6.0 * ((col[i + 1] - col[i]) / (R[i + 1] - R[i]) - (col[i] - col[i - 1]) / (R[i] - R[i - 1])) /
-                (R[i + 1] - R[i - 1]) -
-            sig * u[i - 1]) /
-           p;
+  __syncthreads();
+  for (int q = threadIdx.x; q < nel * nR; q += blockDim.x) {
+    int e2 = q / nR, i = q % nR;
+    y2[(size_t)(k0 + e2) * nR + i] = tile[e2 * ld + i];
   }
-  double qn = 0.5;
-  double un = (3.0 / (R[nR - 1] - R[nR - 2])) * (ypn - (col[nR - 1] - col[nR - 2]) / (R[nR - 1] - R[nR - 2]));
-  yy[nR - 1] = (un - qn * u[nR - 2]) / (qn * yy[nR - 2] + 1.0);
-  for (int i = nR - 2; i >= 0; --i) yy[i] = yy[i] * yy[i + 1] + u[i];
 }
 
 // ------------------------------------------------------------------ plan
@@ -364,6 +395,9 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
   std::vector<int> block_row0;
   for (auto& kv : by_m) {
     block_row0.push_back((int)row_state.size());
+    h_block_row0.push_back((int)row_state.size());
+    h_block_n.push_back((int)kv.second.size());
+    h_block_m.push_back(kv.first);
     for (size_t l = 0; l < kv.second.size(); ++l) {
       state_block[kv.second[l]] = (int)block_row0.size() - 1;
       state_local[kv.second[l]] = (int)l;
@@ -393,7 +427,7 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
       rowb.push_back(block_row0[blk] + state_local[b]);
       rowm.push_back(sys->m12[a]);
     }
-    while ((rowa.size() - start) % 128) {  // pad with a zero-weight duplicate of row 0
+    while ((rowa.size() - start) % 128) {  // pad to whole tiles; padded rows are never read back
       rowa.push_back(rowa[start]);
       rowb.push_back(rowb[start]);
       rowm.push_back(rowm[start]);
@@ -491,11 +525,29 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
     }
   }
 
+  // --- spline coefficients that depend on the grid only
+  {
+    std::vector<double> coef(3 * (size_t)nR, 0.0);
+    double prev = -0.5;  // y2[0] of the clamped spline
+    coef[nR + 0] = prev;
+    for (int i = 1; i < nR - 1; ++i) {
+      double sig = (Rh[i] - Rh[i - 1]) / (Rh[i + 1] - Rh[i - 1]);
+      double p = sig * prev + 2.0;
+      prev = (sig - 1.0) / p;
+      coef[i] = sig;
+      coef[nR + i] = prev;
+      coef[2 * nR + i] = 1.0 / p;
+    }
+    MQCT_CUDA_TRY(d_spl_coef.upload(coef, stream));
+    spline_smem = sizeof(double) * 2 * 32 * (size_t)(nR + 1);
+    MQCT_ARG_CHECK(spline_smem <= 200 * 1024, "nR=%d too large for the spline kernel", nR);
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(spline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)spline_smem));
+  }
   // --- work buffers
   MQCT_CUDA_TRY(d_psi.alloc((size_t)n_basis_rows * G2));
   ldw = nR;
   MQCT_CUDA_TRY(d_W.alloc((size_t)G2 * ldw));
-  MQCT_CUDA_TRY(d_work.alloc((size_t)P * nR));
   if (precision == MQCT_PREC_FP64) {
     MQCT_CUDA_TRY(d_acc.alloc((size_t)n_rows * nR));
   } else {
@@ -533,17 +585,24 @@ int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
                                                 d_walpha.p, d_acc.p);
     MQCT_CUDA_TRY(cudaGetLastError());
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
-    finalize_kernel<double><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
-        P, nR, d_k2r.p, d_acc.p, 1, 0, nR, kCmToHartree, d_R.p, ir1, ir2, cut, d_mat, d_y2,
-        d_skipped, d_work.p);
+    reduce_kernel<double><<<(unsigned)P, 128, 0, stream>>>(P, nR, d_k2r.p, d_acc.p, 1, 0, nR,
+                                                           kCmToHartree, ir1, ir2, cut, d_mat,
+                                                           d_skipped);
     MQCT_CUDA_TRY(cudaGetLastError());
   } else {
     rc = tc_execute();
     if (rc) return rc;
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
-    finalize_kernel<float><<<(unsigned)((P + 127) / 128), 128, 0, stream>>>(
-        P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree,
-        d_R.p, ir1, ir2, cut, d_mat, d_y2, d_skipped, d_work.p);
+    reduce_kernel<float><<<(unsigned)P, 128, 0, stream>>>(
+        P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree, ir1,
+        ir2, cut, d_mat, d_skipped);
+    MQCT_CUDA_TRY(cudaGetLastError());
+  }
+  if (d_y2) {
+    // the spline needs the cutoff flags; use the caller's or the plan's buffer
+    const int* flags = d_skipped;
+    spline_kernel<<<(unsigned)((P + SPL_EL - 1) / SPL_EL), 128, spline_smem, stream>>>(
+        P, nR, d_R.p, d_spl_coef.p, d_mat, flags, d_y2);
     MQCT_CUDA_TRY(cudaGetLastError());
   }
   MQCT_CUDA_TRY(cudaEventRecord(ev[3], stream));
@@ -595,8 +654,9 @@ int mqct_matrix_plan_execute(mqct_matrix_plan* plan, double* d_mat, double* d_y2
 
 int mqct_matrix_plan_sync(mqct_matrix_plan* plan) {
   MQCT_ARG_CHECK(plan, "null plan");
-  MQCT_CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<MatrixPlan*>(plan)->stream));
-  return MQCT_OK;
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return p->tc_check_status();
 }
 
 int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3) {
@@ -648,6 +708,7 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, 
       set_error("matrix build failed: %s", cudaGetErrorString(e));
       rc = MQCT_E_CUDA;
     }
+    if (!rc) rc = p->tc_check_status();
   }
   mqct_matrix_plan_destroy(h);
   return rc;

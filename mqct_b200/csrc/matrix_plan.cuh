@@ -1,11 +1,22 @@
 // matrix_plan.cuh -- state of one matrix-build plan (uploaded system, grids,
 // GEMM row order) shared by the FP64 and tcgen05 contraction paths.
 #pragma once
+#include <memory>
 #include <vector>
 
 #include "common.cuh"
 
 namespace mqct {
+
+// Per-plan state of the tcgen05 path (contract_tc.cu).
+struct TcInfo {
+  int n_chunks = 0, chunks_per_split = 1, npad = 0, n0 = 0, n1 = 0, nbmax = 0, stages = 3;
+  int tmem_cols = 512, n_blocks = 0, n_sm = 148;
+  size_t smem = 0;
+  DevBuf<int> blk_row0, blk_n, blk_m;
+  DevBuf<int64_t> blk_img_off;
+  DevBuf<float> alpha, walpha;
+};
 
 struct MatrixPlan {
   // problem
@@ -26,6 +37,7 @@ struct MatrixPlan {
   // GEMM rows: pairs grouped by m-block, each block padded to a multiple of 128
   int n_rows = 0, n_tiles = 0, n_basis_rows = 0;
   std::vector<int> h_rowa, h_rowb, h_tile_block;
+  std::vector<int> h_block_row0, h_block_n, h_block_m;  // m-blocks of the basis rows
   DevBuf<int> d_rowa, d_rowb, d_rowm, d_k2r, d_tile_block;
   DevBuf<int> d_row_state, d_st_chan, d_st_m, d_ch_j;
   DevBuf<double> d_vec, d_beta, d_gamma, d_wt, d_alpha, d_walpha, d_R;
@@ -36,7 +48,8 @@ struct MatrixPlan {
   DevBuf<double> d_W;     // G2 x ldw, FP64
   int ldw = 0;
   DevBuf<double> d_acc;   // FP64 form: n_rows x nR
-  DevBuf<double> d_work;  // spline scratch P x nR
+  DevBuf<double> d_spl_coef;  // grid-only spline coefficients (sig, y2 factor, 1/p)
+  size_t spline_smem = 0;
 
   // tcgen05 split-precision path (contract_tc.cu)
   int tc_splits = 1, tc_ldp = 0, tc_npad = 0, tc_nchunk = 0;
@@ -44,8 +57,10 @@ struct MatrixPlan {
   DevBuf<unsigned short> d_bimg;        // pre-swizzled B (W) images, hi/lo planes
   DevBuf<float2> d_psi32;               // basis in FP32, chunk-major per row
   DevBuf<int> d_status;
+  std::unique_ptr<TcInfo> tc;
   int tc_init();
   int tc_execute();
+  int tc_check_status();
   int error_report(const double* d_mat, mqct_err_report_t* err);
 
   int init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, const double* R, int32_t nR,
