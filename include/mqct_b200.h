@@ -222,7 +222,9 @@ int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64
 int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_init,
                               int64_t n_traj, double* d_amp, double* d_cls, double* d_diag);
 int mqct_prop_plan_sync(mqct_prop_plan* plan);
-/* Algorithmic table bytes per trajectory step (16 * P for FP32, 32 * P for FP64). */
+/* Algorithmic table bytes of one RK4 step of one trajectory: 4 right-hand sides,
+ * each reading two knot rows of (M, y2) and the slot locations over S slots (the
+ * full lower triangle of every m-block): 4 * S * (4 * sizeof(T) + 4). */
 double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan);
 /* CUDA-event time (ms) of the last propagation kernel on the plan's stream. */
 int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms);

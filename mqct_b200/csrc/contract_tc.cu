@@ -25,6 +25,7 @@
 #include <cmath>
 
 #include "matrix_plan.cuh"
+#include "ptx.cuh"
 
 namespace mqct {
 
@@ -33,60 +34,8 @@ constexpr int TC_KC = 64;        // K elements per chunk (8 core-matrix columns 
 constexpr int TC_PSI_LD = 66;    // float2 per staged basis row (64 + pad)
 constexpr int TC_THREADS = 192;
 constexpr int TC_A_PLANE = TC_M * TC_KC * 2;      // bytes of one bf16 plane of an A stage
-constexpr uint32_t TC_SPIN_LIMIT = 1u << 26;      // bounded mbarrier waits
+constexpr uint32_t TC_SPIN_LIMIT = kSpinLimit;     // bounded mbarrier waits
 
-// ---------------------------------------------------------------- PTX helpers
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait; returns false (and raises the CTA abort flag) on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag,
-                                          int* status, int code) {
-  for (uint32_t it = 0; it < TC_SPIN_LIMIT; ++it) {
-    if (mbar_try_wait(b, parity)) return true;
-    if (*abort_flag) return false;
-  }
-  *abort_flag = 1;
-  atomicCAS(status, 0, code);
-  return false;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
 // Shared-memory matrix descriptor: K-major, SWIZZLE_NONE, version 1.
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;

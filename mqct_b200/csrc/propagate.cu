@@ -17,11 +17,26 @@
 //     da/dt = -i D y - i (dphi/dt / 2) u
 // which is algebraically identical to the reference's pair loop (the phase of
 // a pair factorises into per-state phases; its Coriolis dot product is the
-// quadratic form above).  M(R) and M'(R) come from the cubic spline on the
-// stored knots; each m-block is staged densely in shared memory and reduced
-// with warp shuffles (deterministic order).  The RK4 state and the classical
-// variables stay FP64; the table/mat-vec arithmetic T is float (FP32 mode) or
-// double (FP64 mode).
+// quadratic form above).
+//
+// Table layout: for every m-block (states of equal m12, kept contiguous in an
+// internal block-major state order) the full lower triangle of the block is
+// stored row-major ("slot" T(i)+j for local row i >= column j, T(i)=i(i+1)/2),
+// pairs dropped by the cut-off as zeros, each block padded to 4 slots.  A knot
+// row holds (M, y2) for every slot at one R.
+//
+// One right-hand side, for the spline interval [R_klo, R_klo+1]:
+//  phase A -- every thread takes slots tid, tid+PT, ... : coalesced loads of
+//    the two knot rows, M and M' by the cubic spline, M stored packed in shared
+//    memory, the force term Re(bt_i^* bt_j) M'_ij accumulated in registers;
+//  phase B -- every thread takes whole rows: y_i = sum_j M_ij bt_j over the
+//    packed triangle (row part j <= i, then column part j > i), fixed order,
+//    no atomics, deterministic.
+// When the packed triangles of all blocks do not fit in shared memory the
+// blocks are processed in several passes.  The RK4 amplitudes are FP64 in
+// registers; the classical variables are FP64 in shared memory, advanced by
+// thread 0; the table and mat-vec arithmetic T is float (FP32 mode) or double
+// (FP64 mode).
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -32,33 +47,42 @@ using namespace mqct;
 
 namespace mqct {
 
-constexpr int PT = 256;        // threads per CTA
-constexpr int MAX_NS = 16;     // states per thread (N <= PT * MAX_NS = 4096)
+constexpr int PT = 512;        // threads per CTA
+constexpr int MAX_NS = 8;      // states per thread (N <= PT * MAX_NS = 4096)
+constexpr int UNROLL = 4;      // slots per thread in flight in phase A
 
 template <class T> struct V2;
 template <> struct V2<float> { using t = float2; };
 template <> struct V2<double> { using t = double2; };
 
 struct PropDev {
-  int N, P, nR, n_blocks, n_e, nmax;
-  const double* R;          // nR
-  const int* blk_off;       // n_blocks+1 offsets into pairs
-  const int* blk_n;         // states per block
-  const int* blk_s0;        // offset into blk_states
-  const int* blk_states;    // global state index per (block, local)
-  const int* pair_loc;      // ia | ib << 16 (block-local)
-  const int* st_e;          // energy class per state
-  const double* e_val;      // energy per class, Hartree
-  const double* cplus;      // per state coefficient of a_{i+1}
-  const double* cminus;     // per state coefficient of a_{i-1}
-  const void* knots;        // nR x P of (M, y2) in T precision
+  int N, nR, n_e, n_pass;
+  int64_t S;                   // slots per knot row (all blocks, padded)
+  const double* R;             // nR
+  const int* pass_row0;        // first internal state of each pass (n_pass + 1)
+  const int64_t* pass_slot0;   // first slot of each pass (n_pass + 1)
+  const int* st_blk;           // block of each internal state
+  const int* blk_n;            // states per block
+  const int* blk_s0;           // first internal state of the block
+  const int* blk_mp;           // offset of the block's triangle inside its pass
+  const uint32_t* loc;         // per slot: internal (row | column << 16)
+  const int* st_e;             // energy class per internal state
+  const double* e_val;         // energy per class, Hartree
+  const int* nb_plus;          // internal index of the reference-order successor, or -1
+  const int* nb_minus;         // internal index of the reference-order predecessor, or -1
+  const double* cplus;         // coefficient of the successor's amplitude
+  const double* cminus;        // coefficient of the predecessor's amplitude
+  const int* perm;             // internal -> reference state index
+  const int* inv_perm;         // reference -> internal state index
+  const void* knots;           // nR x S of (M, y2) in T precision
   double mass;
-  int mode;                 // MQCT_MODE_*
+  int mode;                    // MQCT_MODE_*
+  int mp_cap;                  // packed slots that fit in shared memory
   // AT paths
   const int64_t* at_off;
   const int* at_n;
-  const double* at_rec;     // records of 8
-  const double* at_y2;      // per record 4 second derivatives (R, theta, P_theta, P_phi)
+  const double* at_rec;        // records of 8
+  const double* at_y2;         // per record 4 second derivatives (R, theta, P_theta, P_phi)
 };
 
 struct TrajOut {
@@ -67,17 +91,24 @@ struct TrajOut {
   double* diag;
 };
 
+// Classical variables (R, P_R, theta, P_theta, phi, P_phi).
+struct Cls {
+  double R, PR, th, Pth, phi, Pphi;
+};
+
 // Shared-memory layout of one CTA (dynamic).
 template <class T>
 struct Smem {
-  typename V2<T>::t* bt;     // N
-  typename V2<T>::t* u;      // N
-  typename V2<T>::t* y;      // N
-  typename V2<T>::t* ph;     // n_e
-  T* Md;                     // nmax^2
-  double2* a_in;             // N (RHS input)
-  double* red;               // reduction scratch
-  int* flag;
+  Cls* c;                      // [0] state, [1] trial point, [2..4] k1..k3 (k2+k3 after step 3)
+  double* red;                 // reduction scratch, 3 per warp
+  int* flag;                   // [0] next trajectory, [1] keep running
+  double* Rg;                  // nR grid
+  double2* a_in;               // N (RHS input amplitudes)
+  typename V2<T>::t* bt;       // N
+  typename V2<T>::t* u;        // N
+  typename V2<T>::t* y;        // N
+  typename V2<T>::t* ph;       // n_e
+  T* Mp;                       // packed triangles of one pass
 };
 
 __device__ inline double warp_sum(double v) {
@@ -85,35 +116,35 @@ __device__ inline double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ inline float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
-// Block-wide sum of two doubles; result broadcast to all threads.
-__device__ inline void block_sum2(double& a, double& b, double* red) {
+// Block-wide sums of three doubles, broadcast to all threads (fixed order).
+__device__ inline void block_sum3(double& a, double& b, double& c, double* red) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   a = warp_sum(a);
   b = warp_sum(b);
+  c = warp_sum(c);
   if (lane == 0) {
-    red[2 * w] = a;
-    red[2 * w + 1] = b;
+    red[3 * w] = a;
+    red[3 * w + 1] = b;
+    red[3 * w + 2] = c;
   }
   __syncthreads();
-  double sa = 0.0, sb = 0.0;
+  double sa = 0.0, sb = 0.0, sc = 0.0;
 #pragma unroll
   for (int i = 0; i < PT / 32; ++i) {
-    sa += red[2 * i];
-    sb += red[2 * i + 1];
+    sa += red[3 * i];
+    sb += red[3 * i + 1];
+    sc += red[3 * i + 2];
   }
   a = sa;
   b = sb;
+  c = sc;
   __syncthreads();
 }
 
 // Spline coefficients at R (splint_bk, MQCT_SOURCE_CODES/mqct_eqtns.f:555-611;
-// above R_n the matrix is zero, MQCT_SOURCE_CODES/mqct_eqtns.f:545-549).
+// above R_n the matrix is zero, MQCT_SOURCE_CODES/mqct_eqtns.f:545-549; below
+// R_1 the first interval's cubic, the net effect of :534-551).
 struct SplineAt {
   int klo;
   bool zero;
@@ -159,21 +190,23 @@ __device__ inline double at_splint(const double* rec, const double* y2, int n, i
              (h * h) / 6.0;
 }
 
-struct Cls {
-  double R, PR, th, Pth, phi, Pphi;
-};
+__device__ inline float2 ldg2(const float2* p) { return __ldg(p); }
+__device__ inline double2 ldg2(const double2* p) { return __ldg(p); }
 
-// One right-hand-side evaluation.  Input amplitudes in sm.a_in (all states);
-// outputs: da for this thread's states (registers), the classical derivative
-// (std mode), and pot = Re(bt^+ y) (coupling energy).
+// One right-hand-side evaluation at time t and classical point cin (shared
+// memory).  Input amplitudes in sm.a_in (internal order).  Outputs: da for this
+// thread's states, the classical derivative written to dc by thread 0 (std
+// mode), and pot = Re(bt^+ y) (coupling energy), identical in all threads.
 template <class T, int NS>
-__device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls& c, int ns,
-                    double2 (&da)[NS], Cls& dc, double& pot) {
+__device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* cin, int ns,
+                    double2 (&da)[NS], Cls* dc, double& pot) {
   using T2 = typename V2<T>::t;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const int N = d.N;
+  const Cls c = *cin;
   const double sin_t = sin(c.th);
   const double dphidt = c.Pphi / c.R / c.R / d.mass / (sin_t * sin_t);
+  const SplineAt sp = spline_at(sm.Rg, d.nR, c.R);
   // phases per energy class: (cos E t, -sin E t) = e^{-iEt}
   for (int e = tid; e < d.n_e; e += PT) {
     double s, co;
@@ -183,104 +216,164 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls& c,
   }
   __syncthreads();
   for (int i = tid; i < N; i += PT) {
-    double2 a = sm.a_in[i];
-    T2 p = sm.ph[d.st_e[i]];
-    T ar = (T)a.x, ai = (T)a.y;
+    const double2 a = sm.a_in[i];
+    const T2 p = sm.ph[__ldg(d.st_e + i)];
+    const T ar = (T)a.x, ai = (T)a.y;
     sm.bt[i].x = p.x * ar - p.y * ai;
     sm.bt[i].y = p.x * ai + p.y * ar;
     double ur = 0.0, ui = 0.0;
-    if (i + 1 < N) {
-      ur += d.cplus[i] * sm.a_in[i + 1].x;
-      ui += d.cplus[i] * sm.a_in[i + 1].y;
+    const int np_ = __ldg(d.nb_plus + i), nm = __ldg(d.nb_minus + i);
+    if (np_ >= 0) {
+      const double cp = __ldg(d.cplus + i);
+      ur += cp * sm.a_in[np_].x;
+      ui += cp * sm.a_in[np_].y;
     }
-    if (i > 0) {
-      ur += d.cminus[i] * sm.a_in[i - 1].x;
-      ui += d.cminus[i] * sm.a_in[i - 1].y;
+    if (nm >= 0) {
+      const double cm = __ldg(d.cminus + i);
+      ur += cm * sm.a_in[nm].x;
+      ui += cm * sm.a_in[nm].y;
     }
     sm.u[i].x = (T)ur;
     sm.u[i].y = (T)ui;
+    if (sp.zero) {
+      sm.y[i].x = (T)0;
+      sm.y[i].y = (T)0;
+    }
   }
-  const SplineAt sp = spline_at(d.R, d.nR, c.R);
-  const T2* K0 = reinterpret_cast<const T2*>(d.knots) + (size_t)sp.klo * d.P;
-  const T2* K1 = K0 + d.P;
-  const T aa = (T)sp.aa, bb = (T)sp.bb, cc1 = (T)sp.cc1, cc2 = (T)sp.cc2, cc3 = (T)sp.cc3,
-          cc4 = (T)sp.cc4, cc5 = (T)sp.cc5, cc6 = (T)sp.cc6, hinv = (T)(1.0 / sp.h);
   T force = (T)0;
   __syncthreads();
-  for (int b = 0; b < d.n_blocks; ++b) {
-    const int n = d.blk_n[b], p0 = d.blk_off[b], p1 = d.blk_off[b + 1];
-    const int* st = d.blk_states + d.blk_s0[b];
-    for (int q = tid; q < n * n; q += PT) sm.Md[q] = (T)0;
-    __syncthreads();
-    if (!sp.zero) {
-      for (int k = p0 + tid; k < p1; k += PT) {
-        T2 lo = K0[k], hi = K1[k];
-        T m = aa * lo.x + bb * hi.x + (cc1 * lo.y + cc2 * hi.y) * cc5;
-        T md = (hi.x - lo.x) * hinv + (-cc3 * lo.y + cc4 * hi.y) * cc6;
-        int loc = d.pair_loc[k];
-        int ia = loc & 0xffff, ib = loc >> 16;
-        sm.Md[ia * n + ib] = m;
-        sm.Md[ib * n + ia] = m;
-        T2 x = sm.bt[st[ia]], z = sm.bt[st[ib]];
-        T re = x.x * z.x + x.y * z.y;
-        force += (ia == ib ? (T)1 : (T)2) * md * re;
+  if (!sp.zero) {
+    // M = aa lo + bb hi + c1 lo'' + c2 hi'';  M' = (hi - lo)/h + d1 lo'' + d2 hi''
+    const T aa = (T)sp.aa, bb = (T)sp.bb, c1 = (T)(sp.cc1 * sp.cc5), c2 = (T)(sp.cc2 * sp.cc5);
+    const T hinv = (T)(1.0 / sp.h), d1 = (T)(-sp.cc3 * sp.cc6), d2 = (T)(sp.cc4 * sp.cc6);
+    const T2* K0 = reinterpret_cast<const T2*>(d.knots) + (int64_t)sp.klo * d.S;
+    const T2* K1 = K0 + d.S;
+    for (int p = 0; p < d.n_pass; ++p) {
+      const int s0 = (int)d.pass_slot0[p], s1 = (int)d.pass_slot0[p + 1];
+      // phase A: interpolate the pass's slots into Mp, force term
+      for (int kb = s0 + tid; kb < s1; kb += UNROLL * PT) {
+        T2 lo[UNROLL], hi[UNROLL];
+        uint32_t l[UNROLL];
+#pragma unroll
+        for (int q = 0; q < UNROLL; ++q) {
+          const int k = kb + q * PT;
+          if (k < s1) {
+            lo[q] = ldg2(K0 + k);
+            hi[q] = ldg2(K1 + k);
+            l[q] = __ldg(d.loc + k);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < UNROLL; ++q) {
+          const int k = kb + q * PT;
+          if (k < s1) {
+            const T m = aa * lo[q].x + bb * hi[q].x + c1 * lo[q].y + c2 * hi[q].y;
+            const T md = (hi[q].x - lo[q].x) * hinv + d1 * lo[q].y + d2 * hi[q].y;
+            sm.Mp[k - s0] = m;
+            const int ia = (int)(l[q] & 0xffffu), ib = (int)(l[q] >> 16);
+            const T2 x = sm.bt[ia], z = sm.bt[ib];
+            const T re = x.x * z.x + x.y * z.y;
+            force += (ia == ib ? md : (T)2 * md) * re;
+          }
+        }
       }
+      __syncthreads();
+      // phase B: rows of the pass, y_i = sum_j M_ij bt_j
+      const int r0 = d.pass_row0[p], r1 = d.pass_row0[p + 1];
+      for (int r = r0 + tid; r < r1; r += PT) {
+        const int b = __ldg(d.st_blk + r);
+        const int n = __ldg(d.blk_n + b), sb = __ldg(d.blk_s0 + b);
+        const int i = r - sb;
+        const T2* z = sm.bt + sb;
+        const T* Mb = sm.Mp + __ldg(d.blk_mp + b);
+        int addr = i * (i + 1) / 2;
+        T yr0 = (T)0, yi0 = (T)0, yr1 = (T)0, yi1 = (T)0;
+        int j = 0;
+        for (; j + 1 < n; j += 2) {
+          const T m0 = Mb[addr];
+          addr += (j < i) ? 1 : (j + 1);
+          const T m1 = Mb[addr];
+          addr += (j + 1 < i) ? 1 : (j + 2);
+          const T2 z0 = z[j], z1 = z[j + 1];
+          yr0 += m0 * z0.x;
+          yi0 += m0 * z0.y;
+          yr1 += m1 * z1.x;
+          yi1 += m1 * z1.y;
+        }
+        if (j < n) {
+          const T m0 = Mb[addr];
+          const T2 z0 = z[j];
+          yr0 += m0 * z0.x;
+          yi0 += m0 * z0.y;
+        }
+        sm.y[r].x = yr0 + yr1;
+        sm.y[r].y = yi0 + yi1;
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    for (int r = warp; r < n; r += PT / 32) {
-      T yr = (T)0, yi = (T)0;
-      for (int j = lane; j < n; j += 32) {
-        T m = sm.Md[r * n + j];
-        T2 z = sm.bt[st[j]];
-        yr += m * z.x;
-        yi += m * z.y;
-      }
-      yr = warp_sum(yr);
-      yi = warp_sum(yi);
-      if (lane == 0) {
-        sm.y[st[r]].x = yr;
-        sm.y[st[r]].y = yi;
-      }
-    }
-    __syncthreads();
   }
-  // quadratic forms: F = Re(bt^+ M' bt) (accumulated above), g = Im(ut^+ y),
-  // pot = Re(bt^+ y)
-  double g = 0.0, pt = 0.0;
+  // quadratic forms: F (accumulated above), g = Im((D^* u)^+ y), pot = Re(bt^+ y)
+  double g = 0.0, pt = 0.0, f = (double)force;
   for (int i = tid; i < N; i += PT) {
-    T2 p = sm.ph[d.st_e[i]];
-    T2 uu = sm.u[i], yy = sm.y[i], bb2 = sm.bt[i];
-    T utr = p.x * uu.x - p.y * uu.y, uti = p.x * uu.y + p.y * uu.x;  // D^* u
+    const T2 p = sm.ph[__ldg(d.st_e + i)];
+    const T2 uu = sm.u[i], yy = sm.y[i], b2 = sm.bt[i];
+    const T utr = p.x * uu.x - p.y * uu.y, uti = p.x * uu.y + p.y * uu.x;
     g += (double)(utr * yy.y - uti * yy.x);
-    pt += (double)(bb2.x * yy.x + bb2.y * yy.y);
+    pt += (double)(b2.x * yy.x + b2.y * yy.y);
   }
-  double f = (double)force;
-  block_sum2(g, pt, sm.red);
-  double dummy = 0.0;
-  block_sum2(f, dummy, sm.red);
+  block_sum3(g, pt, f, sm.red);
   pot = pt;
   // da_i = -i e^{iE t} y_i - i (dphi/2) u_i
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
     if (q >= ns) break;
-    int i = tid + q * PT;
-    T2 p = sm.ph[d.st_e[i]];
-    T2 yy = sm.y[i], uu = sm.u[i];
-    double er = (double)p.x, ei = -(double)p.y;  // e^{iEt}
-    double zr = er * yy.x - ei * yy.y, zi = er * yy.y + ei * yy.x;
-    double cr = zr + 0.5 * dphidt * (double)uu.x, ci = zi + 0.5 * dphidt * (double)uu.y;
+    const int i = tid + q * PT;
+    const T2 p = sm.ph[__ldg(d.st_e + i)];
+    const T2 yy = sm.y[i], uu = sm.u[i];
+    const double er = (double)p.x, ei = -(double)p.y;  // e^{iEt}
+    const double zr = er * yy.x - ei * yy.y, zi = er * yy.y + ei * yy.x;
+    const double cr = zr + 0.5 * dphidt * (double)uu.x, ci = zi + 0.5 * dphidt * (double)uu.y;
     da[q] = make_double2(ci, -cr);  // -i (cr + i ci)
   }
-  if (d.mode == MQCT_MODE_STD) {
-    double R = c.R, m = d.mass;
-    dc.R = c.PR / m;
-    dc.PR = -f + c.Pth / R / R / m * c.Pth / R + c.Pphi / R / R / m * c.Pphi / R / (sin_t * sin_t);
-    dc.th = 0.0;
-    dc.Pth = 0.0;
-    dc.phi = c.Pphi / R / R / m / (sin_t * sin_t);
-    dc.Pphi = sin_t * g;
+  if (tid == 0 && d.mode == MQCT_MODE_STD) {
+    const double R = c.R, m = d.mass;
+    dc->R = c.PR / m;
+    dc->PR = -f + c.Pth / R / R / m * c.Pth / R + c.Pphi / R / R / m * c.Pphi / R / (sin_t * sin_t);
+    dc->th = 0.0;
+    dc->Pth = 0.0;
+    dc->phi = c.Pphi / R / R / m / (sin_t * sin_t);
+    dc->Pphi = sin_t * g;
   }
 }
+
+__device__ inline Cls cls_axpy(const Cls& a, double h, const Cls& b) {
+  return Cls{a.R + h * b.R, a.PR + h * b.PR, a.th + h * b.th,
+             a.Pth + h * b.Pth, a.phi + h * b.phi, a.Pphi + h * b.Pphi};
+}
+
+__device__ inline double kinetic(const Cls& c, double mass) {
+  return c.PR * c.PR / 2.0 / mass + c.Pth * c.Pth / 2.0 / mass / (c.R * c.R) +
+         c.Pphi * c.Pphi / 2.0 / mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
+}
+
+// Classical point of an AT trajectory at time t (thread 0).
+__device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc) {
+  const double* rec = d.at_rec + 8 * d.at_off[tr];
+  const double* y2 = d.at_y2 + 4 * d.at_off[tr];
+  const int n = d.at_n[tr];
+  cc->R = at_splint(rec, y2, n, 1, 0, t);
+  cc->th = at_splint(rec, y2, n, 3, 1, t);
+  cc->Pth = at_splint(rec, y2, n, 4, 2, t);
+  cc->Pphi = at_splint(rec, y2, n, 6, 3, t);
+  cc->PR = 0.0;
+  cc->phi = 0.0;
+}
+
+// Per-trajectory bookkeeping of thread 0 (shared memory).
+struct Book {
+  double tmpR1, tmpR2, eki, eqi;
+  int status, vib, period, run;
+};
 
 template <class T, int NS>
 __global__ void __launch_bounds__(PT, 1)
@@ -290,231 +383,226 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = d.N, tid = threadIdx.x;
   Smem<T> sm;
+  Book* bk;
   {
     unsigned char* p = smem_raw;
-    sm.a_in = reinterpret_cast<double2*>(p);
-    p += sizeof(double2) * N;
-    sm.bt = reinterpret_cast<T2*>(p);
-    p += sizeof(T2) * N;
-    sm.u = reinterpret_cast<T2*>(p);
-    p += sizeof(T2) * N;
-    sm.y = reinterpret_cast<T2*>(p);
-    p += sizeof(T2) * N;
-    sm.ph = reinterpret_cast<T2*>(p);
-    p += sizeof(T2) * ((d.n_e + 1) & ~1);
-    sm.red = reinterpret_cast<double*>(p);
-    p += sizeof(double) * 2 * (PT / 32);
-    sm.flag = reinterpret_cast<int*>(p);
-    p += 16;
-    sm.Md = reinterpret_cast<T*>(p);
+    auto take = [&](size_t bytes) {
+      unsigned char* r = p;
+      p += (bytes + 15) & ~size_t(15);
+      return r;
+    };
+    sm.c = reinterpret_cast<Cls*>(take(sizeof(Cls) * 5));
+    bk = reinterpret_cast<Book*>(take(sizeof(Book)));
+    sm.red = reinterpret_cast<double*>(take(sizeof(double) * 3 * (PT / 32)));
+    sm.flag = reinterpret_cast<int*>(take(16));
+    sm.Rg = reinterpret_cast<double*>(take(sizeof(double) * d.nR));
+    sm.a_in = reinterpret_cast<double2*>(take(sizeof(double2) * N));
+    sm.bt = reinterpret_cast<T2*>(take(sizeof(T2) * N));
+    sm.u = reinterpret_cast<T2*>(take(sizeof(T2) * N));
+    sm.y = reinterpret_cast<T2*>(take(sizeof(T2) * N));
+    sm.ph = reinterpret_cast<T2*>(take(sizeof(T2) * d.n_e));
+    sm.Mp = reinterpret_cast<T*>(take(sizeof(T) * (size_t)d.mp_cap));
   }
+  for (int i = tid; i < d.nR; i += PT) sm.Rg[i] = d.R[i];
+  Cls* const C = sm.c;       // current state
+  Cls* const CT = sm.c + 1;  // classical point of the stage
+  Cls* const KC = sm.c + 2;  // classical derivative of the stage
+  Cls* const K1 = sm.c + 3;  // first-stage derivative
+  Cls* const K23 = sm.c + 4; // sum of the second and third stages
   const int ns = (N + PT - 1 - tid) / PT;  // states owned by this thread
+  const bool at = d.mode == MQCT_MODE_AT;
   for (;;) {
+    __syncthreads();
     if (tid == 0) sm.flag[0] = atomicAdd(queue, 1);
     __syncthreads();
     const int tr = sm.flag[0];
-    __syncthreads();
     if (tr >= n_traj) break;
-    const mqct_traj_init_t ti = init[tr];
-    double2 y[NS], dydx[NS], dyt[NS], dym[NS];
+    const mqct_traj_init_t* ti = init + tr;
+    double2 y[NS], k[NS], k1[NS], k23[NS];
+    const int s_int = d.inv_perm[ti->s_st - 1];
 #pragma unroll
-    for (int q = 0; q < NS; ++q) y[q] = make_double2(0.0, 0.0);
-    _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns)
-      if (tid + q * PT == ti.s_st - 1) y[q].x = 1.0;
-    Cls c{}, dcl{}, dct{}, dcm{}, ct{};
-    const double k_vec = sqrt(d.mass * 2.0 * ti.e_coll);
-    const double l_orb = sqrt(ti.l_real * (ti.l_real + 1.0));
-    int status = 0;
-    double tcur = 0.0, pot0 = 0.0, pot_end = 0.0, eki = 0.0, eqi = 0.0, eerr = 0.0;
+    for (int q = 0; q < NS; ++q)
+      y[q] = make_double2((q < ns && tid + q * PT == s_int) ? 1.0 : 0.0, 0.0);
+    double tcur = at ? d.at_rec[8 * d.at_off[tr]] : 0.0;
+    const double t_end = at ? d.at_rec[8 * (d.at_off[tr] + d.at_n[tr] - 1)] : 0.0;
+    double dt = ti->dt;
     long long counter = 0;
-    int vib = 0, period = 0;
-    const bool at = d.mode == MQCT_MODE_AT;
-    const double* arec = nullptr;
-    const double* ay2 = nullptr;
-    int an = 0;
-    if (at) {
-      arec = d.at_rec + 8 * d.at_off[tr];
-      ay2 = d.at_y2 + 4 * d.at_off[tr];
-      an = d.at_n[tr];
-      tcur = arec[0];
+    if (tid == 0) {
+      const double k_vec = sqrt(d.mass * 2.0 * ti->e_coll);
+      const double l_orb = sqrt(ti->l_real * (ti->l_real + 1.0));
+      *bk = Book{0.0, 0.0, 0.0, 0.0, 0, 0, 0, 1};
+      *C = Cls{};
+      if (!at && l_orb / k_vec > ti->r_start) {
+        bk->status = 2;  // impact parameter beyond the starting distance: not propagated
+        bk->run = 0;
+        C->R = ti->r_start;
+      } else if (!at) {  // initial conditions, MQCT_SOURCE_CODES/propagator.f:2531-2566
+        C->R = ti->r_start;
+        C->PR = -sqrt(k_vec * k_vec - l_orb * l_orb / (ti->r_start * ti->r_start));
+        C->th = acos(0.0);
+        C->Pth = l_orb * sin(0.0);
+        C->phi = 0.0;
+        C->Pphi = l_orb * cos(0.0);
+      }
     }
-    auto classical_at = [&](double t, Cls& cc) {
-      cc.R = at_splint(arec, ay2, an, 1, 0, t);
-      cc.th = at_splint(arec, ay2, an, 3, 1, t);
-      cc.Pth = at_splint(arec, ay2, an, 4, 2, t);
-      cc.Pphi = at_splint(arec, ay2, an, 6, 3, t);
-      cc.PR = 0.0;
-      cc.phi = 0.0;
-    };
-    auto load_in = [&](const double2 (&v)[NS]) {
+    __syncthreads();
+    const bool skipped = bk->run == 0;
+    while (bk->run) {
+      ++counter;
+      bool last = false;
+      if (at && tcur + dt >= t_end) {
+        dt = t_end - tcur;
+        last = true;
+      }
+      const double hh = dt * 0.5, h6 = dt / 6.0;
+      // RK4 (MQCT_SOURCE_CODES/suppl_routines.f:1076-1113): stage s evaluates
+      // at t + {0, h/2, h/2, h} and y + {0, h/2 k1, h/2 k2, h k3}
+      for (int st = 0; st < 4; ++st) {
+        const double cst = st == 0 ? 0.0 : (st == 3 ? dt : hh);
+        const double tst = tcur + cst;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+          if (q < ns)
+            sm.a_in[tid + q * PT] =
+                st == 0 ? y[q] : make_double2(y[q].x + cst * k[q].x, y[q].y + cst * k[q].y);
+        if (tid == 0) {
+          if (at) classical_at(d, tr, tst, CT);
+          else *CT = st == 0 ? *C : cls_axpy(*C, cst, *KC);
+        }
+        __syncthreads();
+        double potv;
+        rhs<T, NS>(d, sm, tst, CT, ns, k, KC, potv);
+        if (st == 0) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) k1[q] = k[q];
+          if (tid == 0) *K1 = *KC;
+          if (counter == 1 && !at) {  // initial energies, MQCT_SOURCE_CODES/propagator.f:2695-2810
+            double q0 = 0.0, z1 = 0.0, z2 = 0.0;
+#pragma unroll
+            for (int q = 0; q < NS; ++q)
+              if (q < ns) {
+                const int i = tid + q * PT;
+                q0 += (y[q].x * y[q].x + y[q].y * y[q].y) * d.e_val[d.st_e[i]];
+              }
+            block_sum3(q0, z1, z2, sm.red);
+            if (tid == 0) {
+              bk->eqi = q0 + potv;
+              bk->eki = kinetic(*C, d.mass);
+            }
+          }
+        } else if (st == 1) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) k23[q] = k[q];
+          if (tid == 0) *K23 = *KC;
+        } else if (st == 2) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q) k23[q] = make_double2(k23[q].x + k[q].x, k23[q].y + k[q].y);
+          if (tid == 0) *K23 = cls_axpy(*K23, 1.0, *KC);
+        }
+      }
 #pragma unroll
       for (int q = 0; q < NS; ++q)
-        if (q < ns) sm.a_in[tid + q * PT] = v[q];
-      __syncthreads();
-    };
-    if (!at && l_orb / k_vec > ti.r_start) {
-      status = 2;
-      c.R = ti.r_start;
-    } else {
-      if (!at) {
-        c.R = ti.r_start;
-        c.PR = -sqrt(k_vec * k_vec - l_orb * l_orb / (ti.r_start * ti.r_start));
-        c.th = acos(0.0);
-        c.Pth = l_orb * sin(0.0);
-        c.phi = 0.0;
-        c.Pphi = l_orb * cos(0.0);
-      }
-      double tmpR1 = 0.0, tmpR2 = 0.0;
-      bool run = true;
-      double dt = ti.dt;
-      const double t_end = at ? arec[8 * (an - 1)] : 0.0;
-      while (run) {
-        ++counter;
-        if (at && tcur + dt >= t_end) {
-          dt = t_end - tcur;
-          run = false;
-        }
-        const double hh = dt * 0.5, h6 = dt / 6.0, xh = tcur + hh;
-        // k1 at (t, y)
-        load_in(y);
-        Cls cin = c;
-        if (at) classical_at(tcur, cin);
-        double potv;
-        rhs<T, NS>(d, sm, tcur, cin, ns, dydx, dcl, potv);
-        if (counter == 1 && !at) {
-          pot0 = potv;
-          double q0 = 0.0, dummy = 0.0;
-          _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns) {
-            int i = tid + q * PT;
-            q0 += (y[q].x * y[q].x + y[q].y * y[q].y) * d.e_val[d.st_e[i]];
-          }
-          block_sum2(q0, dummy, sm.red);
-          eqi = q0 + pot0;
-          eki = c.PR * c.PR / 2.0 / d.mass + c.Pth * c.Pth / 2.0 / d.mass / (c.R * c.R) +
-                c.Pphi * c.Pphi / 2.0 / d.mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
-        }
-        // k2 at (t + h/2, y + h/2 k1)
-        double2 yt[NS];
-        _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns)
-          yt[q] = make_double2(y[q].x + hh * dydx[q].x, y[q].y + hh * dydx[q].y);
+        if (q < ns)
+          y[q] = make_double2(y[q].x + h6 * (k1[q].x + k[q].x + 2.0 * k23[q].x),
+                              y[q].y + h6 * (k1[q].y + k[q].y + 2.0 * k23[q].y));
+      tcur += dt;
+      if (tid == 0) {
+        bool run = !last;
         if (!at) {
-          ct = Cls{c.R + hh * dcl.R, c.PR + hh * dcl.PR, c.th + hh * dcl.th,
-                   c.Pth + hh * dcl.Pth, c.phi + hh * dcl.phi, c.Pphi + hh * dcl.Pphi};
-        } else {
-          classical_at(xh, ct);
-        }
-        load_in(yt);
-        rhs<T, NS>(d, sm, xh, ct, ns, dyt, dct, potv);
-        // k3 at (t + h/2, y + h/2 k2)
-        _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns)
-          yt[q] = make_double2(y[q].x + hh * dyt[q].x, y[q].y + hh * dyt[q].y);
-        if (!at) {
-          ct = Cls{c.R + hh * dct.R, c.PR + hh * dct.PR, c.th + hh * dct.th,
-                   c.Pth + hh * dct.Pth, c.phi + hh * dct.phi, c.Pphi + hh * dct.Pphi};
-        }
-        load_in(yt);
-        rhs<T, NS>(d, sm, xh, ct, ns, dym, dcm, potv);
-        // k4 at (t + h, y + h k3)
-        _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns) {
-          yt[q] = make_double2(y[q].x + dt * dym[q].x, y[q].y + dt * dym[q].y);
-          dym[q] = make_double2(dyt[q].x + dym[q].x, dyt[q].y + dym[q].y);
-        }
-        if (!at) {
-          ct = Cls{c.R + dt * dcm.R, c.PR + dt * dcm.PR, c.th + dt * dcm.th,
-                   c.Pth + dt * dcm.Pth, c.phi + dt * dcm.phi, c.Pphi + dt * dcm.Pphi};
-          dcm = Cls{dct.R + dcm.R, dct.PR + dcm.PR, dct.th + dcm.th, dct.Pth + dcm.Pth,
-                    dct.phi + dcm.phi, dct.Pphi + dcm.Pphi};
-        } else {
-          classical_at(tcur + dt, ct);
-        }
-        load_in(yt);
-        rhs<T, NS>(d, sm, tcur + dt, ct, ns, dyt, dct, potv);
-        _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns)
-          y[q] = make_double2(y[q].x + h6 * (dydx[q].x + dyt[q].x + 2.0 * dym[q].x),
-                              y[q].y + h6 * (dydx[q].y + dyt[q].y + 2.0 * dym[q].y));
-        if (!at) {
-          c.R += h6 * (dcl.R + dct.R + 2.0 * dcm.R);
-          c.PR += h6 * (dcl.PR + dct.PR + 2.0 * dcm.PR);
-          c.th += h6 * (dcl.th + dct.th + 2.0 * dcm.th);
-          c.Pth += h6 * (dcl.Pth + dct.Pth + 2.0 * dcm.Pth);
-          c.phi += h6 * (dcl.phi + dct.phi + 2.0 * dcm.phi);
-          c.Pphi += h6 * (dcl.Pphi + dct.Pphi + 2.0 * dcm.Pphi);
+          Cls& c = *C;
+          const Cls &a1 = *K1, &a23 = *K23, &a4 = *KC;
+          c.R += h6 * (a1.R + a4.R + 2.0 * a23.R);
+          c.PR += h6 * (a1.PR + a4.PR + 2.0 * a23.PR);
+          c.th += h6 * (a1.th + a4.th + 2.0 * a23.th);
+          c.Pth += h6 * (a1.Pth + a4.Pth + 2.0 * a23.Pth);
+          c.phi += h6 * (a1.phi + a4.phi + 2.0 * a23.phi);
+          c.Pphi += h6 * (a1.Pphi + a4.Pphi + 2.0 * a23.Pphi);
           // stop rules, MQCT_SOURCE_CODES/propagator.f:4011-4050
           const double uR = c.R;
-          if (tcur > dt && counter > 2) {
-            if ((tmpR2 - tmpR1) < 0.0 && (tmpR1 - uR) > 0.0) vib += 1;
+          if (tcur - dt > dt && counter > 2) {
+            if ((bk->tmpR2 - bk->tmpR1) < 0.0 && (bk->tmpR1 - uR) > 0.0) bk->vib += 1;
           }
-          tmpR2 = tmpR1;
-          tmpR1 = uR;
-          tcur += dt;
-          period = (int)(fabs(c.phi) / 2.0 / kPi);
-          if (ti.numb_orb_prds <= period) run = false;
-          if (vib >= ti.numb_oscl_prds) run = false;
-          if (ti.time_lim > 0 && tcur >= ti.time_lim) run = false;
-          if (uR > ti.r_fin) run = false;
+          bk->tmpR2 = bk->tmpR1;
+          bk->tmpR1 = uR;
+          bk->period = (int)(fabs(c.phi) / 2.0 / kPi);
+          if (ti->numb_orb_prds <= bk->period) run = false;
+          if (bk->vib >= ti->numb_oscl_prds) run = false;
+          if (ti->time_lim > 0 && tcur >= ti->time_lim) run = false;
+          if (uR > ti->r_fin) run = false;
           if (!(uR == uR)) {
             run = false;
-            status = 3;
+            bk->status = 3;
           }
-        } else {
-          tcur += dt;
         }
-        if (run && ti.max_steps > 0 && counter >= ti.max_steps) {
+        if (run && ti->max_steps > 0 && counter >= ti->max_steps) {
           run = false;
-          status = 1;
+          bk->status = 1;
         }
+        bk->run = run ? 1 : 0;
       }
-      if (!at) {  // final energy bookkeeping, MQCT_SOURCE_CODES/propagator.f:4182-4343
-        load_in(y);
-        double2 dd[NS];
-        Cls dcx;
-        rhs<T, NS>(d, sm, tcur, c, ns, dd, dcx, pot_end);
-        double eqf = 0.0, dummy = 0.0;
-        _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns) {
-          int i = tid + q * PT;
+      __syncthreads();
+    }
+    double pot_end = 0.0, eerr = 0.0;
+    if (!at && !skipped) {  // final energy bookkeeping, MQCT_SOURCE_CODES/propagator.f:4182-4343
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+        if (q < ns) sm.a_in[tid + q * PT] = y[q];
+      if (tid == 0) *CT = *C;
+      __syncthreads();
+      rhs<T, NS>(d, sm, tcur, CT, ns, k, KC, pot_end);
+      double eqf = 0.0, z1 = 0.0, z2 = 0.0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+        if (q < ns) {
+          const int i = tid + q * PT;
           eqf += (y[q].x * y[q].x + y[q].y * y[q].y) * d.e_val[d.st_e[i]];
         }
-        block_sum2(eqf, dummy, sm.red);
-        double ef = c.PR * c.PR / 2.0 / d.mass + c.Pth * c.Pth / 2.0 / d.mass / (c.R * c.R) +
-                    c.Pphi * c.Pphi / 2.0 / d.mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
-        eerr = fabs(eqf + ef + pot_end - eki - eqi);
-      }
+      block_sum3(eqf, z1, z2, sm.red);
+      eerr = fabs(eqf + kinetic(*C, d.mass) + pot_end - bk->eki - bk->eqi);
     }
-    double nrm = 0.0, dummy = 0.0;
-    _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns) nrm += y[q].x * y[q].x + y[q].y * y[q].y;
-    block_sum2(nrm, dummy, sm.red);
+    double nrm = 0.0, z1 = 0.0, z2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < NS; ++q)
+      if (q < ns) nrm += y[q].x * y[q].x + y[q].y * y[q].y;
+    block_sum3(nrm, z1, z2, sm.red);
     double* amp = out.amp + (size_t)tr * 2 * N;
-    _Pragma("unroll") for (int q = 0; q < NS; ++q) if (q < ns) {
-      int i = tid + q * PT;
-      amp[i] = y[q].x;
-      amp[N + i] = y[q].y;
-    }
+#pragma unroll
+    for (int q = 0; q < NS; ++q)
+      if (q < ns) {
+        const int i = d.perm[tid + q * PT];
+        amp[i] = y[q].x;
+        amp[N + i] = y[q].y;
+      }
     if (tid == 0) {
+      const Cls& c = *C;
       double* cl = out.cls + (size_t)tr * 6;
       cl[0] = c.R; cl[1] = c.PR; cl[2] = c.th; cl[3] = c.Pth; cl[4] = c.phi; cl[5] = c.Pphi;
       double* dg = out.diag + (size_t)tr * 8;
       dg[0] = tcur;
       dg[1] = (double)counter;
-      dg[2] = status == 2 ? 0.0 : fabs(1.0 - nrm);
+      dg[2] = bk->status == 2 ? 0.0 : fabs(1.0 - nrm);
       dg[3] = eerr;
-      dg[4] = status;
-      dg[5] = period;
-      dg[6] = vib;
+      dg[4] = bk->status;
+      dg[5] = bk->period;
+      dg[6] = bk->vib;
       dg[7] = pot_end;
     }
-    __syncthreads();
   }
 }
 
 // ------------------------------------------------------------------ plan
 struct PropPlan {
   int arith = MQCT_PROP_FP32;
-  int N = 0, P = 0, nR = 0, n_blocks = 0, n_e = 0, nmax = 0;
+  int N = 0, P = 0, nR = 0, n_blocks = 0, n_e = 0, n_pass = 0, mp_cap = 0;
+  int64_t S = 0;
   double mass = 0.0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<double> d_R, d_e_val, d_cplus, d_cminus;
-  DevBuf<int> d_blk_off, d_blk_n, d_blk_s0, d_blk_states, d_pair_loc, d_st_e, d_queue;
+  DevBuf<int> d_pass_row0, d_st_blk, d_blk_n, d_blk_s0, d_blk_mp, d_st_e, d_nbp, d_nbm, d_perm,
+      d_inv, d_queue, d_status;
+  DevBuf<int64_t> d_pass_slot0;
+  DevBuf<uint32_t> d_loc;
   DevBuf<float2> d_knots32;
   DevBuf<double2> d_knots64;
   DevBuf<mqct_traj_init_t> d_init;
@@ -532,20 +620,23 @@ struct PropPlan {
       case 1: return (const void*)propagate_kernel<T, 1>;
       case 2: return (const void*)propagate_kernel<T, 2>;
       case 4: return (const void*)propagate_kernel<T, 4>;
-      case 8: return (const void*)propagate_kernel<T, 8>;
-      default: return (const void*)propagate_kernel<T, 16>;
+      default: return (const void*)propagate_kernel<T, 8>;
     }
   }
   const void* kernel_ptr() const {
     return arith == MQCT_PROP_FP32 ? pick<float>(ns) : pick<double>(ns);
   }
+  size_t tsize() const { return arith == MQCT_PROP_FP32 ? 4 : 8; }
 
-  size_t smem_bytes() const {
-    size_t t = arith == MQCT_PROP_FP32 ? 8 : 16;
-    size_t b = sizeof(double2) * N + 3 * t * N + t * ((n_e + 1) & ~1) + 16 * (PT / 32) + 16;
-    b = (b + 15) & ~size_t(15);
-    return b + (t / 2) * (size_t)nmax * nmax;
+  // Shared memory without the packed-triangle area.
+  size_t smem_fixed() const {
+    const size_t t2 = 2 * tsize();
+    auto a = [](size_t x) { return (x + 15) & ~size_t(15); };
+    return a(sizeof(Cls) * 5) + a(sizeof(Book)) + a(sizeof(double) * 3 * (PT / 32)) + a(16) +
+           a(8 * (size_t)nR) +
+           a(16 * (size_t)N) + 3 * a(t2 * N) + a(t2 * n_e);
   }
+  size_t smem_bytes() const { return smem_fixed() + ((tsize() * (size_t)mp_cap + 15) & ~size_t(15)); }
 
   int init(const mqct_tables_t* tab, int32_t ar) {
     MQCT_ARG_CHECK(tab && tab->j12 && tab->m12 && tab->ej && tab->ind_mat && tab->R &&
@@ -556,7 +647,8 @@ struct PropPlan {
                    "n_states %d beyond the kernel limit %d", tab->n_states, PT * MAX_NS);
     MQCT_ARG_CHECK(tab->P > 0 && tab->P < (1 << 30) && tab->nR >= 2, "bad P/nR");
     MQCT_ARG_CHECK(tab->mass_au > 0, "mass must be positive");
-    for (int i = 0; i + 1 < tab->nR; ++i) MQCT_ARG_CHECK(tab->R[i + 1] > tab->R[i], "R grid must increase");
+    for (int i = 0; i + 1 < tab->nR; ++i)
+      MQCT_ARG_CHECK(tab->R[i + 1] > tab->R[i], "R grid must increase");
     arith = ar;
     N = tab->n_states;
     P = (int)tab->P;
@@ -565,117 +657,179 @@ struct PropPlan {
     MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     MQCT_CUDA_TRY(cudaEventCreate(&ev0));
     MQCT_CUDA_TRY(cudaEventCreate(&ev1));
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    // blocks by m
+    int dev = 0, dev_smem = 0;
+    MQCT_CUDA_TRY(cudaGetDevice(&dev));
+    MQCT_CUDA_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    MQCT_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // m-blocks; internal order = blocks in ascending m, reference order inside
     std::map<int, std::vector<int>> by_m;
     for (int s = 0; s < N; ++s) by_m[tab->m12[s]].push_back(s);
-    std::vector<int> local(N), blk_of(N), blk_n, blk_s0, blk_states;
+    std::vector<int> local(N), blk_of(N), blk_n, blk_s0, perm, inv(N), st_blk(N);
+    std::vector<int64_t> blk_slot0;
+    int64_t slots = 0;
     for (auto& kv : by_m) {
-      int b = (int)blk_n.size();
-      blk_n.push_back((int)kv.second.size());
-      blk_s0.push_back((int)blk_states.size());
-      for (size_t l = 0; l < kv.second.size(); ++l) {
-        local[kv.second[l]] = (int)l;
-        blk_of[kv.second[l]] = b;
-        blk_states.push_back(kv.second[l]);
+      const int b = (int)blk_n.size();
+      const int n = (int)kv.second.size();
+      blk_n.push_back(n);
+      blk_s0.push_back((int)perm.size());
+      blk_slot0.push_back(slots);
+      slots += (((int64_t)n * (n + 1) / 2) + 3) & ~int64_t(3);
+      for (int l = 0; l < n; ++l) {
+        const int s = kv.second[l];
+        local[s] = l;
+        blk_of[s] = b;
+        st_blk[perm.size()] = b;
+        inv[s] = (int)perm.size();
+        perm.push_back(s);
       }
-      nmax = std::max(nmax, (int)kv.second.size());
     }
     n_blocks = (int)blk_n.size();
-    MQCT_ARG_CHECK(nmax < 65536, "block too large");
-    std::vector<std::vector<int>> bk(n_blocks);
-    for (int k = 0; k < P; ++k) {
-      int i = tab->ind_mat[2 * k] - 1, j = tab->ind_mat[2 * k + 1] - 1;
-      MQCT_ARG_CHECK(i >= 0 && i < N && j >= 0 && j < N, "ind_mat out of range at k=%d", k + 1);
-      MQCT_ARG_CHECK(tab->m12[i] == tab->m12[j], "pair with different m12 at k=%d", k + 1);
-      bk[blk_of[i]].push_back(k);
-    }
-    std::vector<int> blk_off(n_blocks + 1, 0), pair_loc, order;
-    for (int b = 0; b < n_blocks; ++b) {
-      blk_off[b] = (int)order.size();
-      for (int k : bk[b]) {
-        int i = tab->ind_mat[2 * k] - 1, j = tab->ind_mat[2 * k + 1] - 1;
-        pair_loc.push_back(local[i] | (local[j] << 16));
-        order.push_back(k);
-      }
-    }
-    blk_off[n_blocks] = (int)order.size();
-    // knots (M, y2) per R, pairs in block order
-    if (arith == MQCT_PROP_FP32) {
-      std::vector<float2> kn((size_t)nR * P);
-      for (int r = 0; r < nR; ++r)
-        for (int q = 0; q < P; ++q) {
-          size_t src = (size_t)order[q] * nR + r;
-          kn[(size_t)r * P + q] = make_float2((float)tab->mat[src], (float)tab->y2[src]);
-        }
-      MQCT_CUDA_TRY(d_knots32.upload(kn, stream));
-      MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
-    } else {
-      std::vector<double2> kn((size_t)nR * P);
-      for (int r = 0; r < nR; ++r)
-        for (int q = 0; q < P; ++q) {
-          size_t src = (size_t)order[q] * nR + r;
-          kn[(size_t)r * P + q] = make_double2(tab->mat[src], tab->y2[src]);
-        }
-      MQCT_CUDA_TRY(d_knots64.upload(kn, stream));
-      MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
-    }
-    // energy classes and Coriolis coefficients
+    S = slots;
+    MQCT_ARG_CHECK(S < ((int64_t)1 << 30), "%lld table slots beyond the kernel limit", (long long)S);
+    // energy classes (needed for the shared-memory size)
     std::vector<double> e_val;
     std::vector<int> st_e(N);
-    for (int s = 0; s < N; ++s) {
+    for (int ii = 0; ii < N; ++ii) {
+      const int s = perm[ii];
       int c = -1;
       for (size_t q = 0; q < e_val.size(); ++q)
-        if (e_val[q] == tab->ej[s]) { c = (int)q; break; }
+        if (e_val[q] == tab->ej[s]) {
+          c = (int)q;
+          break;
+        }
       if (c < 0) {
         c = (int)e_val.size();
         e_val.push_back(tab->ej[s]);
       }
-      st_e[s] = c;
+      st_e[ii] = c;
     }
     n_e = (int)e_val.size();
+    // passes: consecutive blocks whose packed triangles fit the shared memory left
+    const size_t fixed = smem_fixed();
+    MQCT_ARG_CHECK(fixed + 1024 <= (size_t)dev_smem,
+                   "shared memory of the state vectors (%zu B) beyond the device limit %d", fixed,
+                   dev_smem);
+    const int64_t cap = (int64_t)(((size_t)dev_smem - fixed) / tsize()) & ~int64_t(3);
+    std::vector<int64_t> pass_slot0;
+    std::vector<int> pass_row0, blk_mp(n_blocks);
+    int64_t max_pass = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+      const int64_t bs = (b + 1 < n_blocks ? blk_slot0[b + 1] : S) - blk_slot0[b];
+      MQCT_ARG_CHECK(bs <= cap, "m-block of %d states does not fit in shared memory", blk_n[b]);
+      if (pass_slot0.empty() || blk_slot0[b] + bs - pass_slot0.back() > cap) {
+        pass_slot0.push_back(blk_slot0[b]);
+        pass_row0.push_back(blk_s0[b]);
+      }
+      blk_mp[b] = (int)(blk_slot0[b] - pass_slot0.back());
+      max_pass = std::max(max_pass, blk_slot0[b] + bs - pass_slot0.back());
+    }
+    n_pass = (int)pass_slot0.size();
+    pass_slot0.push_back(S);
+    pass_row0.push_back(N);
+    mp_cap = (int)max_pass;
+    // slots of the stored pairs; every other slot keeps zero knots
+    std::vector<int> slot_pair(S, -1);
+    std::vector<uint32_t> loc(S, 0u);
+    for (int b = 0; b < n_blocks; ++b)
+      for (int i = 0; i < blk_n[b]; ++i)
+        for (int j = 0; j <= i; ++j)
+          loc[blk_slot0[b] + (int64_t)i * (i + 1) / 2 + j] =
+              (uint32_t)(blk_s0[b] + i) | ((uint32_t)(blk_s0[b] + j) << 16);
+    for (int k = 0; k < P; ++k) {
+      const int s1 = tab->ind_mat[2 * k] - 1, s2 = tab->ind_mat[2 * k + 1] - 1;
+      MQCT_ARG_CHECK(s1 >= 0 && s1 < N && s2 >= 0 && s2 < N, "ind_mat out of range at k=%d", k + 1);
+      MQCT_ARG_CHECK(tab->m12[s1] == tab->m12[s2], "pair with different m12 at k=%d", k + 1);
+      const int b = blk_of[s1];
+      const int i = std::max(local[s1], local[s2]), j = std::min(local[s1], local[s2]);
+      const int64_t slot = blk_slot0[b] + (int64_t)i * (i + 1) / 2 + j;
+      MQCT_ARG_CHECK(slot_pair[slot] < 0, "pair %d repeats pair %d", k + 1, slot_pair[slot] + 1);
+      slot_pair[slot] = k;
+    }
+    if (arith == MQCT_PROP_FP32) {
+      std::vector<float2> kn((size_t)nR * S, make_float2(0.f, 0.f));
+      for (int64_t q = 0; q < S; ++q)
+        if (slot_pair[q] >= 0)
+          for (int r = 0; r < nR; ++r) {
+            const size_t src = (size_t)slot_pair[q] * nR + r;
+            kn[(size_t)r * S + q] = make_float2((float)tab->mat[src], (float)tab->y2[src]);
+          }
+      MQCT_CUDA_TRY(d_knots32.upload(kn, stream));
+      MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
+    } else {
+      std::vector<double2> kn((size_t)nR * S, make_double2(0.0, 0.0));
+      for (int64_t q = 0; q < S; ++q)
+        if (slot_pair[q] >= 0)
+          for (int r = 0; r < nR; ++r) {
+            const size_t src = (size_t)slot_pair[q] * nR + r;
+            kn[(size_t)r * S + q] = make_double2(tab->mat[src], tab->y2[src]);
+          }
+      MQCT_CUDA_TRY(d_knots64.upload(kn, stream));
+      MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
+    }
+    // Coriolis neighbours: the reference couples a state with its successor and
+    // predecessor in the reference state order (sqrt2 / sqrt1,
+    // MQCT_SOURCE_CODES/mqct_eqtns.f:447-464); the coefficient vanishes where
+    // the neighbour has another j12.
     std::vector<double> cp(N, 0.0), cm(N, 0.0);
-    for (int s = 0; s < N; ++s) {
-      double J = tab->j12[s], m = tab->m12[s];
-      // reference sqrt2 / sqrt1 (MQCT_SOURCE_CODES/mqct_eqtns.f:447-448)
-      if (s + 1 < N) cp[s] = sqrt(J * (J + 1.0) - (m + 1.0) * m);
-      if (s > 0) cm[s] = sqrt(J * (J + 1.0) - (m - 1.0) * m);
+    std::vector<int> nbp(N, -1), nbm(N, -1);
+    for (int ii = 0; ii < N; ++ii) {
+      const int s = perm[ii];
+      const double J = tab->j12[s], m = tab->m12[s];
+      if (s + 1 < N) {
+        nbp[ii] = inv[s + 1];
+        cp[ii] = sqrt(J * (J + 1.0) - (m + 1.0) * m);
+      }
+      if (s > 0) {
+        nbm[ii] = inv[s - 1];
+        cm[ii] = sqrt(J * (J + 1.0) - (m - 1.0) * m);
+      }
     }
     MQCT_CUDA_TRY(d_R.upload(tab->R, nR, stream));
     MQCT_CUDA_TRY(d_e_val.upload(e_val, stream));
     MQCT_CUDA_TRY(d_cplus.upload(cp, stream));
     MQCT_CUDA_TRY(d_cminus.upload(cm, stream));
-    MQCT_CUDA_TRY(d_blk_off.upload(blk_off, stream));
+    MQCT_CUDA_TRY(d_nbp.upload(nbp, stream));
+    MQCT_CUDA_TRY(d_nbm.upload(nbm, stream));
+    MQCT_CUDA_TRY(d_pass_row0.upload(pass_row0, stream));
+    MQCT_CUDA_TRY(d_pass_slot0.upload(pass_slot0, stream));
+    MQCT_CUDA_TRY(d_st_blk.upload(st_blk, stream));
     MQCT_CUDA_TRY(d_blk_n.upload(blk_n, stream));
     MQCT_CUDA_TRY(d_blk_s0.upload(blk_s0, stream));
-    MQCT_CUDA_TRY(d_blk_states.upload(blk_states, stream));
-    MQCT_CUDA_TRY(d_pair_loc.upload(pair_loc, stream));
+    MQCT_CUDA_TRY(d_blk_mp.upload(blk_mp, stream));
+    MQCT_CUDA_TRY(d_loc.upload(loc, stream));
     MQCT_CUDA_TRY(d_st_e.upload(st_e, stream));
+    MQCT_CUDA_TRY(d_perm.upload(perm, stream));
+    MQCT_CUDA_TRY(d_inv.upload(inv, stream));
     MQCT_CUDA_TRY(d_queue.alloc(1));
-    size_t sb = smem_bytes();
-    MQCT_ARG_CHECK(sb <= 227 * 1024, "shared memory %zu B beyond the 227 KB limit", sb);
+    MQCT_CUDA_TRY(d_status.alloc(1));
+    MQCT_CUDA_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
     ns = 1;
     while (ns * PT < N) ns *= 2;
-    const void* fn = kernel_ptr();
-    MQCT_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb));
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_bytes()));
     MQCT_CUDA_TRY(cudaStreamSynchronize(stream));
     return MQCT_OK;
   }
 
   PropDev dev_view(int mode) const {
     PropDev d{};
-    d.N = N; d.P = P; d.nR = nR; d.n_blocks = n_blocks; d.n_e = n_e; d.nmax = nmax;
-    d.R = d_R.p; d.blk_off = d_blk_off.p; d.blk_n = d_blk_n.p; d.blk_s0 = d_blk_s0.p;
-    d.blk_states = d_blk_states.p; d.pair_loc = d_pair_loc.p; d.st_e = d_st_e.p;
-    d.e_val = d_e_val.p; d.cplus = d_cplus.p; d.cminus = d_cminus.p;
+    d.N = N; d.nR = nR; d.n_e = n_e; d.n_pass = n_pass; d.S = S;
+    d.R = d_R.p; d.pass_row0 = d_pass_row0.p; d.pass_slot0 = d_pass_slot0.p;
+    d.st_blk = d_st_blk.p; d.blk_n = d_blk_n.p; d.blk_s0 = d_blk_s0.p; d.blk_mp = d_blk_mp.p;
+    d.loc = d_loc.p; d.st_e = d_st_e.p; d.e_val = d_e_val.p;
+    d.nb_plus = d_nbp.p; d.nb_minus = d_nbm.p; d.cplus = d_cplus.p; d.cminus = d_cminus.p;
+    d.perm = d_perm.p; d.inv_perm = d_inv.p;
     d.knots = arith == MQCT_PROP_FP32 ? (const void*)d_knots32.p : (const void*)d_knots64.p;
     d.mass = mass;
     d.mode = mode;
+    d.mp_cap = mp_cap;
     d.at_off = d_at_off.p; d.at_n = d_at_n.p; d.at_rec = d_at_rec.p; d.at_y2 = d_at_y2.p;
     return d;
   }
+
+  // Algorithmic table bytes of one RK4 step: 4 right-hand sides, each reading
+  // two knot rows and the slot locations.
+  double bytes_per_step() const { return 4.0 * (double)S * (4.0 * tsize() + 4.0); }
 
   int launch(const mqct_traj_init_t* d_init_p, int64_t n_traj, int mode, double* amp,
              double* cls, double* diag) {
@@ -684,11 +838,11 @@ struct PropPlan {
     PropDev d = dev_view(mode);
     TrajOut o{amp, cls, diag};
     int n_traj_i = (int)n_traj;
-    size_t sb = smem_bytes();
+    const size_t sb = smem_bytes();
     int per_sm = 1;
     const void* fn = kernel_ptr();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PT, sb);
-    int grid = (int)std::min<int64_t>(n_traj, (int64_t)n_sm * std::max(per_sm, 1));
+    MQCT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PT, sb));
+    const int grid = (int)std::min<int64_t>(n_traj, (int64_t)n_sm * std::max(per_sm, 1));
     void* args[] = {&d, (void*)&d_init_p, &n_traj_i, &d_queue.p, &o};
     MQCT_CUDA_TRY(cudaEventRecord(ev0, stream));
     MQCT_CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(PT), args, sb, stream));
@@ -709,7 +863,7 @@ struct PropPlan {
     const int cols[4] = {1, 3, 4, 6};
     for (int64_t t = 0; t < n_traj; ++t) {
       const double* r = at->rec + 8 * at->rec_off[t];
-      int n = at->n_rec[t];
+      const int n = at->n_rec[t];
       for (int i = 0; i + 1 < n; ++i)
         MQCT_ARG_CHECK(r[8 * (i + 1)] > r[8 * i], "AT path %lld: time not increasing", (long long)t);
       u.assign(n, 0.0);
@@ -717,20 +871,21 @@ struct PropPlan {
         double* yy = y2.data() + 4 * at->rec_off[t];
         auto X = [&](int i) { return r[8 * i]; };
         auto Y = [&](int i) { return r[8 * i + cols[a]]; };
-        double yp1 = (Y(1) - Y(0)) / (X(1) - X(0));
-        double ypn = (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2));
+        const double yp1 = (Y(1) - Y(0)) / (X(1) - X(0));
+        const double ypn = (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2));
         yy[a] = -0.5;
         u[0] = (3.0 / (X(1) - X(0))) * ((Y(1) - Y(0)) / (X(1) - X(0)) - yp1);
         for (int i = 1; i < n - 1; ++i) {
-          double sig = (X(i) - X(i - 1)) / (X(i + 1) - X(i - 1));
-          double p = sig * yy[4 * (i - 1) + a] + 2.0;
+          const double sig = (X(i) - X(i - 1)) / (X(i + 1) - X(i - 1));
+          const double p = sig * yy[4 * (i - 1) + a] + 2.0;
           yy[4 * i + a] = (sig - 1.0) / p;
           u[i] = (6.0 * ((Y(i + 1) - Y(i)) / (X(i + 1) - X(i)) - (Y(i) - Y(i - 1)) / (X(i) - X(i - 1))) /
                       (X(i + 1) - X(i - 1)) -
                   sig * u[i - 1]) /
                  p;
         }
-        double un = (3.0 / (X(n - 1) - X(n - 2))) * (ypn - (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2)));
+        const double un =
+            (3.0 / (X(n - 1) - X(n - 2))) * (ypn - (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2)));
         yy[4 * (n - 1) + a] = (un - 0.5 * u[n - 2]) / (0.5 * yy[4 * (n - 2) + a] + 1.0);
         for (int i = n - 2; i >= 0; --i) yy[4 * i + a] = yy[4 * i + a] * yy[4 * (i + 1) + a] + u[i];
       }
@@ -765,6 +920,27 @@ static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mod
   return MQCT_OK;
 }
 
+// Host-buffer run: upload the initial conditions, launch, copy the results back.
+static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, int mode,
+                    double* amp_out, double* cls_out, double* diag_out) {
+  int rc = validate_init(init, n_traj, p->N, mode);
+  if (rc) return rc;
+  MQCT_CUDA_TRY(p->d_init.upload(init, n_traj, p->stream));
+  MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
+  MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
+  MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
+  rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p);
+  if (rc) return rc;
+  MQCT_CUDA_TRY(cudaMemcpyAsync(amp_out, p->d_amp.p, sizeof(double) * n_traj * 2 * p->N,
+                                cudaMemcpyDeviceToHost, p->stream));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(cls_out, p->d_cls.p, sizeof(double) * n_traj * 6,
+                                cudaMemcpyDeviceToHost, p->stream));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(diag_out, p->d_diag.p, sizeof(double) * n_traj * 8,
+                                cudaMemcpyDeviceToHost, p->stream));
+  MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  return MQCT_OK;
+}
+
 }  // namespace mqct
 
 extern "C" {
@@ -796,23 +972,8 @@ int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_in
 int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,
                        double* amp_out, double* cls_out, double* diag_out) {
   MQCT_ARG_CHECK(plan && init && amp_out && cls_out && diag_out, "null argument");
-  PropPlan* p = reinterpret_cast<PropPlan*>(plan);
-  int rc = validate_init(init, n_traj, p->N, MQCT_MODE_STD);
-  if (rc) return rc;
-  MQCT_CUDA_TRY(p->d_init.upload(init, n_traj, p->stream));
-  MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
-  MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
-  MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
-  rc = p->launch(p->d_init.p, n_traj, MQCT_MODE_STD, p->d_amp.p, p->d_cls.p, p->d_diag.p);
-  if (rc) return rc;
-  MQCT_CUDA_TRY(cudaMemcpyAsync(amp_out, p->d_amp.p, sizeof(double) * n_traj * 2 * p->N,
-                                cudaMemcpyDeviceToHost, p->stream));
-  MQCT_CUDA_TRY(cudaMemcpyAsync(cls_out, p->d_cls.p, sizeof(double) * n_traj * 6,
-                                cudaMemcpyDeviceToHost, p->stream));
-  MQCT_CUDA_TRY(cudaMemcpyAsync(diag_out, p->d_diag.p, sizeof(double) * n_traj * 8,
-                                cudaMemcpyDeviceToHost, p->stream));
-  MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
-  return MQCT_OK;
+  return run_host(reinterpret_cast<PropPlan*>(plan), init, n_traj, MQCT_MODE_STD, amp_out,
+                  cls_out, diag_out);
 }
 
 int mqct_prop_plan_sync(mqct_prop_plan* plan) {
@@ -823,8 +984,7 @@ int mqct_prop_plan_sync(mqct_prop_plan* plan) {
 
 double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan) {
   if (!plan) return 0.0;
-  const PropPlan* p = reinterpret_cast<const PropPlan*>(plan);
-  return (p->arith == MQCT_PROP_FP32 ? 16.0 : 32.0) * p->P;
+  return reinterpret_cast<const PropPlan*>(plan)->bytes_per_step();
 }
 
 int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms) {
@@ -848,34 +1008,7 @@ int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
   PropPlan* p = reinterpret_cast<PropPlan*>(h);
   rc = validate_init(init, n_traj, p->N, mode);
   if (!rc && mode == MQCT_MODE_AT) rc = p->set_at(at, n_traj);
-  if (!rc) {
-    if (mode == MQCT_MODE_STD) {
-      rc = mqct_prop_plan_run(h, init, n_traj, amp_out, cls_out, diag_out);
-    } else {
-      cudaError_t e = p->d_init.upload(init, n_traj, p->stream);
-      if (e == cudaSuccess) e = p->d_amp.alloc((size_t)n_traj * 2 * p->N);
-      if (e == cudaSuccess) e = p->d_cls.alloc((size_t)n_traj * 6);
-      if (e == cudaSuccess) e = p->d_diag.alloc((size_t)n_traj * 8);
-      if (e != cudaSuccess) {
-        set_error("%s", cudaGetErrorString(e));
-        rc = MQCT_E_CUDA;
-      }
-      if (!rc) rc = p->launch(p->d_init.p, n_traj, MQCT_MODE_AT, p->d_amp.p, p->d_cls.p, p->d_diag.p);
-      if (!rc) {
-        cudaMemcpyAsync(amp_out, p->d_amp.p, sizeof(double) * n_traj * 2 * p->N,
-                        cudaMemcpyDeviceToHost, p->stream);
-        cudaMemcpyAsync(cls_out, p->d_cls.p, sizeof(double) * n_traj * 6, cudaMemcpyDeviceToHost,
-                        p->stream);
-        cudaMemcpyAsync(diag_out, p->d_diag.p, sizeof(double) * n_traj * 8,
-                        cudaMemcpyDeviceToHost, p->stream);
-        e = cudaStreamSynchronize(p->stream);
-        if (e != cudaSuccess) {
-          set_error("propagation failed: %s", cudaGetErrorString(e));
-          rc = MQCT_E_CUDA;
-        }
-      }
-    }
-  }
+  if (!rc) rc = run_host(p, init, n_traj, mode, amp_out, cls_out, diag_out);
   mqct_prop_plan_destroy(h);
   return rc;
 }
