@@ -162,6 +162,19 @@ double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
 int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3);
 void mqct_matrix_plan_destroy(mqct_matrix_plan* plan);
 
+/* Spline fit of device-resident matrix columns without any device allocation
+ * (this entry point has no counterpart in the reference, which fits its splines
+ * on the host).  d_R: nR grid points, d_mat: P x nR values (column k at
+ * k * nR), d_skipped: optional per-column flags (y2 = 0 where set), d_y2: P x nR
+ * output; all device pointers; stream: a cudaStream_t or NULL.  The grid-only
+ * coefficients live in a fixed device array of the library, so nR is limited
+ * to 399 (MQCT_E_RANGE beyond).  The first call on each device (with that
+ * device current) looks up the array's address; make that first call before
+ * any stream capture.  Calls that may overlap in time (other streams or host
+ * threads) share the array and race: the caller serialises them. */
+int mqct_spline_y2_noalloc(const double* d_R, int32_t nR, const double* d_mat,
+                           const int32_t* d_skipped, int64_t P, double* d_y2, void* stream);
+
 /* Propagation tables after READ_MIJ / MATRIX_MAKE: the retained pairs only
  * (elements dropped by MIJ_CUTOFF removed, MQCT_SOURCE_CODES/matrix_ini.f:4309-4378),
  * Mat_el already shifted when MIJ_SHIFT is on (:4270-4273). */

@@ -78,7 +78,8 @@ class AtPaths(C.Structure):
 EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
-    "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy", "mqct_propagate_batch",
+    "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
+    "mqct_spline_y2_noalloc", "mqct_propagate_batch",
     "mqct_prop_plan_create", "mqct_prop_plan_run", "mqct_prop_plan_run_device",
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
     "mqct_prop_plan_destroy",
@@ -115,6 +116,7 @@ def lib():
     L.mqct_matrix_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
     L.mqct_prop_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
     L.mqct_matrix_plan_destroy.argtypes = [vp]
+    L.mqct_spline_y2_noalloc.argtypes = [vp, C.c_int32, vp, vp, C.c_int64, vp, vp]
     L.mqct_matrix_plan_destroy.restype = None
     L.mqct_propagate_batch.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
                                        C.c_int32, C.POINTER(AtPaths), C.c_int32, f64p, f64p,

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 
 #include "common.cuh"
 #include "matrix_plan.cuh"
@@ -715,3 +716,80 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ no-allocation spline fit
+// mqct_spline_y2_noalloc: the spline fit of spline_kernel for callers that
+// must not allocate device memory inside the call -- a host code that fixes
+// its device-memory budget once at start-up (several MPI ranks sharing one
+// GPU, where a per-call allocation can fail or fragment the pool), or a
+// latency-critical caller, for which cudaFree (and often cudaMalloc)
+// synchronises the whole device and stalls its other streams.  The grid-only
+// coefficients that the allocating path uploads from the host live here in a
+// fixed file-scope device array; a small kernel fills them from the caller's
+// R grid before the fit.  Every coefficient the fit reads is written by that
+// kernel first, so nothing in the array has to start at zero.
+constexpr int kNoAllocMaxR = 399;  // spline_kernel stages 2 x 32 x (nR + 1) doubles: <= 200 KB
+static __device__ __align__(256) double g_spline_noalloc_coef[3 * (kNoAllocMaxR + 1)];
+
+// Grid-only coefficients of the clamped spline (the host loop of
+// MatrixPlan::init): sig_i, the y2 recurrence factor and 1/p_i.  One thread:
+// the recurrence is sequential and nR is small.
+__global__ void spline_coef_kernel(int nR, const double* __restrict__ R, double* __restrict__ coef) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int i = 0; i < 3 * nR; ++i) coef[i] = 0.0;
+  double prev = -0.5;
+  coef[nR] = prev;
+  for (int i = 1; i < nR - 1; ++i) {
+    const double sig = (R[i] - R[i - 1]) / (R[i + 1] - R[i - 1]);
+    const double p = sig * prev + 2.0;
+    prev = (sig - 1.0) / p;
+    coef[i] = sig;
+    coef[nR + i] = prev;
+    coef[2 * nR + i] = 1.0 / p;
+  }
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_coef_ptr[kMaxDevices] = {};
+}  // namespace
+
+extern "C" int mqct_spline_y2_noalloc(const double* d_R, int32_t nR, const double* d_mat,
+                                      const int32_t* d_skipped, int64_t P, double* d_y2,
+                                      void* stream) {
+  MQCT_ARG_CHECK(d_R && d_mat && d_y2, "null argument");
+  MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31), "P out of range");
+  MQCT_ARG_CHECK(nR >= 2, "nR must be >= 2");
+  if (nR > kNoAllocMaxR) {
+    set_error("mqct_spline_y2_noalloc: nR=%d beyond its fixed limit of %d points", nR, kNoAllocMaxR);
+    return MQCT_E_RANGE;
+  }
+  int dev = 0;
+  MQCT_CUDA_TRY(cudaGetDevice(&dev));
+  MQCT_ARG_CHECK(dev >= 0 && dev < kMaxDevices, "device %d beyond the supported range", dev);
+  double* coef = nullptr;
+  {
+    // set-up, once per device (with that device current): the address of the
+    // fixed coefficient array
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_coef_ptr[dev]) {
+      void* p = nullptr;
+      MQCT_CUDA_TRY(cudaGetSymbolAddress(&p, g_spline_noalloc_coef));
+      g_noalloc_coef_ptr[dev] = static_cast<double*>(p);
+    }
+    coef = g_noalloc_coef_ptr[dev];
+  }
+  const size_t smem = sizeof(double) * 2 * SPL_EL * (size_t)(nR + 1);
+  // the launch limit is a property of the kernel that an allocating plan may
+  // have set lower for its own grid: raise it for this call's nR
+  MQCT_CUDA_TRY(cudaFuncSetAttribute(spline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  spline_coef_kernel<<<1, 1, 0, s>>>(nR, d_R, coef);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  spline_kernel<<<(unsigned)((P + SPL_EL - 1) / SPL_EL), 128, smem, s>>>(P, nR, d_R, coef, d_mat,
+                                                                        d_skipped, d_y2);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  return MQCT_OK;
+}
