@@ -41,7 +41,7 @@ def _args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="mqct", choices=["mqct", "reference"])
-    p.add_argument("--precision", default="auto", choices=["auto", "bf16x3", "fp64"])
+    p.add_argument("--precision", default="auto", choices=["auto", "f16x3", "bf16x3", "fp64"])
     p.add_argument("--c3-traj", type=int, default=1024,
                    help="trajectories of the propagation workload timed (4096 = full set)")
     p.add_argument("--no-propagation", action="store_true")
@@ -58,6 +58,20 @@ def workload():
     s = mq.CollisionSystem(4, c2["channels"], A=c2["A"], B=c2["B"], C=c2["C"])
     R = mq.r_grid(c2["nR"], c2["rmin"], c2["rmax"])
     return c2, s, R
+
+
+TC_PROFILE = os.path.join(ROOT, "profiles", "tc_contract_kernel_asymtop_j8_48x48x48_R300.md")
+
+
+def _profiled_traffic(path):
+    """DRAM bytes per launch recorded by the committed ncu summary (None if absent)."""
+    try:
+        for ln in open(path):
+            if ln.strip().startswith("dram_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].strip().split()[0])
+    except OSError:
+        pass
+    return None
 
 
 def _peaks():
@@ -165,7 +179,8 @@ def run_gpu(a):
 
     c2, s, R = workload()
     peaks, peak_src = _peaks()
-    prec = mq.PREC_BF16X3 if a.precision in ("auto", "bf16x3") else mq.PREC_FP64
+    prec = {"auto": mq.PREC_F16X3, "f16x3": mq.PREC_F16X3, "bf16x3": mq.PREC_BF16X3,
+            "fp64": mq.PREC_FP64}[a.precision]
     if a.precision == "auto":
         try:
             mq.MatrixPlan(s, R[:4], (8, 8, 0, 0, 0, 0, 1), c2["pes"], precision=prec).close()
@@ -205,20 +220,27 @@ def run_gpu(a):
         fp64 = {"ms_per_step": ms64, "speedup": ms64 / ms}
         m1 = d_mat.view(s.P, len(R)).double()
         m0 = d_mat64.view(s.P, len(R)).double()
-        keep = (d_sk == 0) & (d_sk64 == 0)
-        rowmax = m0.abs().amax(dim=1, keepdim=True)
-        gmax = m0.abs().max()
-        d = (m1 - m0).abs()
-        rel_row = (d / rowmax.clamp_min(1e-300))[keep]
-        rel_floor = (d / torch.maximum(m0.abs(), 1e-8 * rowmax).clamp_min(1e-300))[keep]
-        acc = {"max_rel_err_vs_fp64_rowmax": float(rel_row.max()),
-               "p99_rel_err_vs_fp64_rowmax": float(torch.quantile(rel_row.flatten()[:2_000_000], 0.99)),
-               "max_rel_err_floor_1e-8": float(rel_floor.max()),
-               "max_abs_err_hartree": float(d.max()),
-               "skip_flags_equal": bool(torch.equal(d_sk, d_sk64))}
+        acc = matrix_accuracy(m1, m0, d_sk, d_sk64, torch)
         plan64.close()
     plan.close()
     del d_mat
+
+    # the reference's own 2-D form of the same build (alpha integrated analytically,
+    # K = 48 x 48 = 2304): time and accuracy of the split path against its FP64 form
+    ref_form = None
+    if not a.no_fp64_form and prec != mq.PREC_FP64:
+        c2d = dict(c2, grid=(48, 48, 0, 0, 0, 0, 1))
+        p2, dm2, ds2, sg2 = _matrix_bench(mq, s, R, c2d, prec, max(1, a.steps), 1, torch, flush)
+        p2b, dm2b, ds2b, sg2b = _matrix_bench(mq, s, R, c2d, mq.PREC_FP64, 1, 1, torch, flush)
+        ms2, ms2b = float(sg2.sum(axis=1).mean()), float(sg2b.sum(axis=1).mean())
+        ref_form = {"grid": "48 GL beta x 48 gamma, alpha analytic (K = 2304)",
+                    "ms_per_step": ms2, "value": n_el / (ms2 / 1e3), "fp64_ms_per_step": ms2b,
+                    "speedup_vs_fp64_form": ms2b / ms2,
+                    "accuracy": matrix_accuracy(dm2.view(s.P, len(R)).double(),
+                                                dm2b.view(s.P, len(R)).double(), ds2, ds2b, torch)}
+        p2.close()
+        p2b.close()
+        del dm2, dm2b
 
     # e2e through the C ABI with host buffers (H2D of the system, D2H of Mat_el, y2, flags)
     e2e_ms = []
@@ -242,7 +264,8 @@ def run_gpu(a):
             dist.destroy_process_group()
         return
     cpu = cpu_baseline_matrix(s, R, c2, a.cpu_seconds)
-    tc = prec == mq.PREC_BF16X3
+    tc = prec in (mq.PREC_BF16X3, mq.PREC_F16X3)
+    tc_name = "F16x3" if prec == mq.PREC_F16X3 else "BF16x3"
     peak = peaks.get("bf16_tflops", 1590.0)
     line = {
         "metric": METRIC,
@@ -255,11 +278,11 @@ def run_gpu(a):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "bf16x3-fp32acc" if tc else "f64",
+        "dtype": (tc_name.lower() + "-fp32acc") if tc else "f64",
         "data": "synthetic (seeded site-site PES; no dataset)",
         "config": {"workload": "asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), "
                                "grid 48 GL beta x 48 gamma x 48 alpha, 300 R 3-25 bohr",
-                   "precision": "BF16x3 tcgen05" if tc else "FP64 CUDA cores",
+                   "precision": (tc_name + " tcgen05") if tc else "FP64 CUDA cores",
                    "elements_per_step": n_el, "grid_points": 48 * 48 * 48,
                    "l2": "flushed (256 MB write) between timed steps",
                    "parallelism": f"replicas x{world}"},
@@ -267,23 +290,53 @@ def run_gpu(a):
                         "finalize": float(seg[:, 2].mean())},
         "roofline": {"bound": "tensor" if tc else "fp64", "achieved": achieved_tf,
                      "peak": peak if tc else None, "unit": "TFLOP/s",
-                     "frac": achieved_tf / peak if tc else None, "traffic": None,
-                     "peak_source": f"bf16_tflops ({peak_src})",
+                     "frac": achieved_tf / peak if tc else None,
+                     "traffic": _profiled_traffic(TC_PROFILE) if tc else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "launch, " + os.path.relpath(TC_PROFILE, ROOT),
+                     "peak_source": f"bf16_tflops ({peak_src}; dense FP16 and BF16 rates are equal)",
                      "flops_per_launch": flops, "kernel": "contraction"},
         "cpu_baseline": cpu,
         "e2e": {"value": n_el / (float(np.median(e2e_ms)) / 1e3), "unit": "matrix elements/s",
                 "ms": float(np.median(e2e_ms)), "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
-        "gpu_launches": int(a.steps * 4),
+        "gpu_launches": int(a.steps * (7 if tc else 5)),
         "fp64_form": fp64,
         "accuracy": acc,
+        "reference_2d_form": ref_form,
         "propagation": prop,
         "wall_s": wall,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def matrix_accuracy(m1, m0, sk1, sk0, torch):
+    """Error of the split-precision matrix against the FP64 form of the same build.
+    Pairs whose FP64 radial function stays below 1e-9 of the largest element vanish by
+    symmetry (rounding noise only) and are excluded; for the rest e_k = max_R |dM_k| /
+    max_R |M_k| (relative max-norm error of the radial function) and, per entry above
+    1e-3 of its row maximum, |dM| / |M|."""
+    rowmax = m0.abs().amax(dim=1)
+    gmax = rowmax.max()
+    sig = rowmax >= 1e-9 * gmax
+    d = (m1 - m0).abs()
+    e_k = (d.amax(dim=1)[sig] / rowmax[sig])
+    big = (m0.abs() >= 1e-3 * rowmax[:, None]) & sig[:, None]
+    rel = (d[big] / m0.abs()[big])
+    samp = rel[torch.randperm(rel.numel(), device=rel.device)[:4_000_000]] if rel.numel() > 4_000_000 else rel
+    flag_diff = (sk1 != sk0)
+    return {"pairs_compared": int(sig.sum()), "pairs_zero_by_symmetry": int((~sig).sum()),
+            "pair_maxnorm_rel_err": {"median": float(e_k.median()),
+                                     "p99": float(torch.quantile(e_k, 0.99)),
+                                     "max": float(e_k.max())},
+            "entry_rel_err_above_1e-3_rowmax": {"median": float(samp.median()),
+                                                "p99": float(torch.quantile(samp, 0.99))},
+            "max_abs_err_hartree": float(d.max()),
+            "cutoff_flags_differing": int(flag_diff.sum()),
+            "max_fp64_element_of_differing_flags": float(rowmax[flag_diff].max()) if bool(flag_diff.any()) else 0.0}
 
 
 def run_propagation(mq, syn, s, R, mat, a, torch, world):
@@ -309,6 +362,7 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world):
                      "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
                      "table_bytes_per_step": plan.bytes_per_step,
                      "achieved_table_GBs": steps * plan.bytes_per_step / (ms / 1e3) / 1e9,
+                     "frac_of_hbm_peak": steps * plan.bytes_per_step / (ms / 1e3) / 1e9 / _peaks()[0]["hbm_gbs"],
                      "max_status": float(diag[:, 4].max())}
         if name == "fp32":
             res["prob_fp32"] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
@@ -316,6 +370,15 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world):
             p64 = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
             p32 = res.pop("prob_fp32")[:nt]
             res["max_abs_prob_diff_fp32_vs_fp64"] = float(np.abs(p32 - p64).max())
+            # opacity-weighted sums sum_traj (2l+1) P_f (cross sections up to a common
+            # factor) of the FP32 and FP64 runs over the same trajectories
+            w = 2 * l[:nt] + 1
+            s32, s64 = (w[:, None] * p32).sum(0), (w[:, None] * p64).sum(0)
+            keep = s64 > 1e-4 * s64[1:].max()
+            keep[0] = False  # elastic channel
+            res["sigma_rel_diff_fp32_vs_fp64"] = {
+                "channels": int(keep.sum()),
+                "max": float(np.max(np.abs(s32[keep] - s64[keep]) / s64[keep]))}
         plan.close()
     res["speedup_fp32_vs_fp64_form"] = res["fp32"]["traj_per_s"] / res["fp64"]["traj_per_s"]
     res["workload"] = (f"{n} of the 4096 trajectories (b~U(0,15), E log-uniform 50-2000 cm^-1, "

@@ -48,6 +48,8 @@ extern "C" {
 /* Contraction precision of the matrix build. */
 #define MQCT_PREC_FP64 0      /* plain FP64 CUDA-core form                    */
 #define MQCT_PREC_BF16X3 1    /* tcgen05 kind::f16, BF16 hi/lo split, FP32 acc */
+#define MQCT_PREC_F16X3 2     /* tcgen05 kind::f16, FP16 hi/lo split with power-of-two
+                                 scaling, FP32 acc (~22 significant bits per operand) */
 
 /* Propagation arithmetic. */
 #define MQCT_PROP_FP64 0      /* FP64 amplitudes and tables                   */

@@ -19,13 +19,13 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
+from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
                    check, lib, ptr)
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
            "PropagationPlan", "trajectory_set", "cross_sections", "write_mtrx_uf",
-           "read_mtrx_uf", "spline_y2", "MqctError", "PREC_FP64", "PREC_BF16X3", "PROP_FP32",
+           "read_mtrx_uf", "spline_y2", "MqctError", "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32",
            "PROP_FP64", "MODE_STD", "MODE_AT"]
 
 

@@ -17,7 +17,7 @@ MQCT_OK = 0
 ERRORS = {-1: "MQCT_E_ARG", -2: "MQCT_E_CUDA", -3: "MQCT_E_NODEV", -4: "MQCT_E_IO",
           -5: "MQCT_E_RANGE", -6: "MQCT_E_DEVICE"}
 
-PREC_FP64, PREC_BF16X3 = 0, 1
+PREC_FP64, PREC_BF16X3, PREC_F16X3 = 0, 1, 2
 PROP_FP64, PROP_FP32 = 0, 1
 MODE_STD, MODE_AT = 0, 1
 PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3

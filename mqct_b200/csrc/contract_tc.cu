@@ -1,25 +1,35 @@
-// contract_tc.cu -- split-precision (BF16x3) tensor-core contraction of the
-// matrix build on sm_100a: tcgen05.mma kind::f16 with FP32 accumulators in TMEM.
+// contract_tc.cu -- split-precision tensor-core contraction of the matrix build
+// on sm_100a: tcgen05.mma kind::f16 with FP32 accumulators in TMEM.
 //
 //   M[row, i] = sum_{c, alpha} sum_{g in chunk c} X_alpha[row, g] W[g, i]
-//   X = X_hi + X_lo, W = W_hi + W_lo (bfloat16 parts),
+//   X = X_hi + X_lo, W = W_hi + W_lo (16-bit parts),
 //   D += X_hi W_hi + X_hi W_lo + X_lo W_hi          (FP32 accumulate)
 //
+// Two 16-bit formats: BF16x3 (8 significant bits per part, ~16 bits kept) and
+// F16x3 (11 bits per part, ~22 bits kept; the products of FP16 parts are exact
+// in FP32).  FP16's range is narrow, so in F16x3 X is scaled by 2^14 and every
+// radial column of W by the power of two that brings its largest entry to
+// [2^13, 2^14); the finalize multiplies each column by the exact inverse.
+//
 // CTA = one 128-row tile of pair rows (one m-block) x all nR radial points.
-// Warp roles (192 threads):
+// Warp roles (320 threads):
 //   warp 0      bulk-copy (TMA) producer: per K-chunk the pre-arranged W image
 //               (hi and lo planes, K-major core-matrix layout) and the block's
 //               rotor-basis slice, one cp.async.bulk each, mbarrier complete_tx;
 //   warp 1      TMEM allocator + single-thread MMA issuer;
-//   warps 2..5  X producers: X = w_alpha Re((z psi_a)^* (z psi_b)) in FP32 from
+//   warps 2..9  X producers: X = w_alpha Re((z psi_a)^* (z psi_b)) in FP32 from
 //               the staged basis (z = e^{i m alpha}), split to BF16 hi/lo and
-//               written in the core-matrix layout; afterwards the epilogue
-//               (tcgen05.ld of the accumulator, FP32 partials to global).
+//               written in the core-matrix layout, two threads per tile row
+//               (each half of the chunk's K groups); afterwards the epilogue
+//               (tcgen05.ld of the accumulator, FP32 partials to global; the
+//               two warps of a TMEM lane quarter take alternate 16-column
+//               slices).
 // The operand tiles use the K-major SWIZZLE_NONE canonical layout: 8 rows x
 // 16 B core matrices, K-adjacent core matrices LBO apart, 8-row groups SBO =
 // 128 B apart.  Every mbarrier wait is bounded; on timeout the CTA records an
 // error code, drains, frees its TMEM and returns.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -32,7 +42,8 @@ namespace mqct {
 constexpr int TC_M = 128;        // rows per tile
 constexpr int TC_KC = 64;        // K elements per chunk (8 core-matrix columns of 8 bf16)
 constexpr int TC_PSI_LD = 66;    // float2 per staged basis row (64 + pad)
-constexpr int TC_THREADS = 192;
+constexpr int TC_THREADS = 320;
+constexpr int TC_PRODUCERS = TC_THREADS - 64;  // X-producer / epilogue threads
 constexpr int TC_A_PLANE = TC_M * TC_KC * 2;      // bytes of one bf16 plane of an A stage
 constexpr uint32_t TC_SPIN_LIMIT = kSpinLimit;     // bounded mbarrier waits
 
@@ -46,9 +57,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
   return d;                // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
 }
 // Instruction descriptor, kind::f16: BF16 A/B, FP32 D, both K-major.
+// a/b format 1 = BF16, 0 = F16 (A and B always of the same type).
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
+}
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -81,11 +96,84 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<uint32_t*>(&h);
 }
+__device__ __forceinline__ uint32_t pack_f16(float a, float b) {
+  __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+// Split of 8 FP32 values into hi and lo 16-bit parts (packed pairs).
+template <bool kF16>
+__device__ __forceinline__ void split8(const float (&x)[8], uint4& h, uint4& l) {
+  float r[8];
+  if (kF16) {
+    h.x = pack_f16(x[0], x[1]);
+    h.y = pack_f16(x[2], x[3]);
+    h.z = pack_f16(x[4], x[5]);
+    h.w = pack_f16(x[6], x[7]);
+    const __half2* hb = reinterpret_cast<const __half2*>(&h);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float2 f = __half22float2(hb[e]);
+      r[2 * e] = x[2 * e] - f.x;
+      r[2 * e + 1] = x[2 * e + 1] - f.y;
+    }
+    l.x = pack_f16(r[0], r[1]);
+    l.y = pack_f16(r[2], r[3]);
+    l.z = pack_f16(r[4], r[5]);
+    l.w = pack_f16(r[6], r[7]);
+  } else {
+    h.x = pack_bf16(x[0], x[1]);
+    h.y = pack_bf16(x[2], x[3]);
+    h.z = pack_bf16(x[4], x[5]);
+    h.w = pack_bf16(x[6], x[7]);
+    const __nv_bfloat162* hb = reinterpret_cast<const __nv_bfloat162*>(&h);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float2 f = __bfloat1622float2(hb[e]);
+      r[2 * e] = x[2 * e] - f.x;
+      r[2 * e + 1] = x[2 * e + 1] - f.y;
+    }
+    l.x = pack_bf16(r[0], r[1]);
+    l.y = pack_bf16(r[2], r[3]);
+    l.z = pack_bf16(r[4], r[5]);
+    l.w = pack_bf16(r[6], r[7]);
+  }
+}
+
+// F16x3 column scaling: one CTA per radial column i finds max_g |W[g, i]| and
+// writes the exponent s_i with max * 2^s_i in [2^13, 2^14) and the finalize
+// factor 2^-(s_i + kXScaleExp).
+constexpr int kXScaleExp = 14;
+__global__ void tc_wscale_kernel(const double* __restrict__ W, int ldw, int G2,
+                                 int* __restrict__ wexp, double* __restrict__ col_scale) {
+  __shared__ double red[32];
+  const int i = blockIdx.x;
+  double m = 0.0;
+  for (int g = threadIdx.x; g < G2; g += blockDim.x) m = fmax(m, fabs(W[(size_t)g * ldw + i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    m = fmax(m, red[0]);
+    int e = 0;
+    int s = 0;
+    if (m > 0.0) {
+      frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
+      s = 14 - e;
+    }
+    wexp[i] = s;
+    col_scale[i] = ldexp(1.0, -(s + kXScaleExp));
+  }
+}
 
 // ---------------------------------------------------------------- operand images
-// W (FP64, [g][ldw]) -> per chunk c: [plane hi/lo][kg 0..7][ng 0..Npad/8-1][8 rows][8 bf16].
+// W (FP64, [g][ldw]) -> per chunk c: [plane hi/lo][kg 0..7][ng 0..Npad/8-1][8 rows][8 x 16 bit];
+// F16x3 scales column n by 2^wexp[n] first (exact).
+template <bool kF16>
 __global__ void tc_bimage_kernel(const double* __restrict__ W, int ldw, int G2, int nR, int Npad,
-                                 int n_chunks, __nv_bfloat16* __restrict__ img) {
+                                 int n_chunks, const int* __restrict__ wexp,
+                                 unsigned short* __restrict__ img) {
   int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t per_chunk = (int64_t)TC_KC * Npad;
   if (idx >= per_chunk * n_chunks) return;
@@ -94,8 +182,19 @@ __global__ void tc_bimage_kernel(const double* __restrict__ W, int ldw, int G2, 
   int n = rem / TC_KC, k = rem % TC_KC;
   int g = c * TC_KC + k;
   double w = (g < G2 && n < nR) ? W[(size_t)g * ldw + n] : 0.0;
-  __nv_bfloat16 hi = __double2bfloat16(w);
-  __nv_bfloat16 lo = __double2bfloat16(w - (double)__bfloat162float(hi));
+  unsigned short hi, lo;
+  if (kF16) {
+    if (n < nR) w = ldexp(w, wexp[n]);
+    __half h = __double2half(w);
+    __half l = __double2half(w - (double)__half2float(h));
+    hi = __half_as_ushort(h);
+    lo = __half_as_ushort(l);
+  } else {
+    __nv_bfloat16 h = __double2bfloat16(w);
+    __nv_bfloat16 l = __double2bfloat16(w - (double)__bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+  }
   int kg = k >> 3, e = k & 7, ng = n >> 3, r8 = n & 7;
   size_t plane = (size_t)TC_KC * Npad;
   size_t off = (size_t)c * 2 * plane + (((size_t)kg * (Npad / 8) + ng) * 8 + r8) * 8 + e;
@@ -135,7 +234,7 @@ struct TcArgs {
   const int* rowa;                // basis row of st1 / st2 per GEMM row
   const int* rowb;
   const float2* psi_img;
-  const __nv_bfloat16* b_img;
+  const unsigned short* b_img;    // hi/lo planes of W, BF16 or F16 bits
   const float* alpha;             // alpha nodes (n_alpha_it, or none)
   const float* walpha;            // alpha weights
   float* part;                    // n_splits x n_rows x Npad
@@ -143,6 +242,7 @@ struct TcArgs {
   int* status;
 };
 
+template <bool kF16>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // carve shared memory (1024-byte aligned regions)
@@ -169,15 +269,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.stages; ++s) {
-      mbar_init(&A_full[s], 128);
+      mbar_init(&A_full[s], TC_PRODUCERS);
       mbar_init(&A_empty[s], 1);
     }
     mbar_init(B_full, 1);
     mbar_init(B_empty, 1);
     mbar_init(P_full, 1);
-    mbar_init(P_empty, 128);
+    mbar_init(P_empty, TC_PRODUCERS);
     mbar_init(ACC_full, 1);
-    mbar_init(ACC_empty, 128);
+    mbar_init(ACC_empty, TC_PRODUCERS);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -241,8 +341,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       uint32_t af_phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       int stage = 0;
       bool first_unit = true;
-      const uint32_t idesc0 = idesc_bf16(TC_M, a.N0);
-      const uint32_t idesc1 = a.N1 > 0 ? idesc_bf16(TC_M, a.N1) : 0u;
+      const uint32_t idesc0 = kF16 ? idesc_f16(TC_M, a.N0) : idesc_bf16(TC_M, a.N0);
+      const uint32_t idesc1 = a.N1 > 0 ? (kF16 ? idesc_f16(TC_M, a.N1) : idesc_bf16(TC_M, a.N1)) : 0u;
       const uint32_t sA0 = smem_u32(sA), sB0 = smem_u32(sB);
       const uint32_t lbo_a = (TC_M / 8) * 128, lbo_b = (uint32_t)(a.Npad / 8) * 128;
       const uint32_t bplane = (uint32_t)TC_KC * a.Npad * 2;
@@ -290,8 +390,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       }
     }
   } else {
-    // ---------------- X producers (warps 2..5) and epilogue
-    const int p = threadIdx.x - 64;  // tile row generated by this thread
+    // ---------------- X producers (warps 2..9) and epilogue
+    const int p = (threadIdx.x - 64) & (TC_M - 1);  // tile row generated by this thread
+    const int kh = (threadIdx.x - 64) / TC_M;       // half of the chunk's K groups
     uint32_t pf_phase = 0, af_phase = 0;
     uint32_t ae_phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool a_used[8] = {false, false, false, false, false, false, false, false};
@@ -316,6 +417,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
             sincosf((float)m * a.alpha[al], &zi, &zr);
             wa = a.walpha[al];
           }
+          if (kF16) wa *= (float)(1 << kXScaleExp);  // exact power-of-two scaling
           if (a_used[stage]) {
             if (!mbar_wait(&A_empty[stage], ae_phase[stage], abort_flag, a.status, 32)) break;
             ae_phase[stage] ^= 1;
@@ -324,7 +426,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           unsigned char* hi = sA + stage * (2 * TC_A_PLANE);
           unsigned char* lo = hi + TC_A_PLANE;
 #pragma unroll 2
-          for (int kg = 0; kg < TC_KC / 8; ++kg) {
+          for (int kg = kh * (TC_KC / 16); kg < (kh + 1) * (TC_KC / 16); ++kg) {
             float x[8];
 #pragma unroll
             for (int e = 0; e < 8; e += 2) {
@@ -339,22 +441,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
               x[e + 1] = wa * (ar1 * br1 + ai1 * bi1);
             }
             uint4 h, l;
-            float r[8];
-            h.x = pack_bf16(x[0], x[1]);
-            h.y = pack_bf16(x[2], x[3]);
-            h.z = pack_bf16(x[4], x[5]);
-            h.w = pack_bf16(x[6], x[7]);
-            const __nv_bfloat162* hb = reinterpret_cast<const __nv_bfloat162*>(&h);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              float2 f = __bfloat1622float2(hb[e]);
-              r[2 * e] = x[2 * e] - f.x;
-              r[2 * e + 1] = x[2 * e + 1] - f.y;
-            }
-            l.x = pack_bf16(r[0], r[1]);
-            l.y = pack_bf16(r[2], r[3]);
-            l.z = pack_bf16(r[4], r[5]);
-            l.w = pack_bf16(r[6], r[7]);
+            split8<kF16>(x, h, l);
             const uint32_t off = (uint32_t)(kg * (TC_M / 8) + (p >> 3)) * 128u + (uint32_t)(p & 7) * 16u;
             *reinterpret_cast<uint4*>(hi + off) = h;
             *reinterpret_cast<uint4*>(lo + off) = l;
@@ -371,7 +458,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       tc_fence_after();
       const int orow = tile * TC_M + q * 32 + lane;
       float* dst = a.part + (int64_t)split * a.part_stride + (int64_t)orow * a.Npad;
-      for (int c16 = 0; c16 < a.Npad; c16 += 16) {
+      for (int c16 = 16 * ((warp - 2) >> 2); c16 < a.Npad; c16 += 32) {
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c16, v);
 #pragma unroll
@@ -482,17 +569,33 @@ int MatrixPlan::tc_init() {
   MQCT_CUDA_TRY(d_psi32.alloc((size_t)acc));
   MQCT_CUDA_TRY(d_status.alloc(1));
   MQCT_CUDA_TRY(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
-  MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)t.smem));
+  if (precision == MQCT_PREC_F16X3) {
+    MQCT_CUDA_TRY(t.wexp.alloc((size_t)nR));
+    MQCT_CUDA_TRY(d_col_scale.alloc((size_t)nR));
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+  } else {
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+  }
   return MQCT_OK;
 }
 
 int MatrixPlan::tc_execute() {
   TcInfo& t = *tc;
   const int thr = 256;
+  const bool f16 = precision == MQCT_PREC_F16X3;
   int64_t nb_img = (int64_t)t.n_chunks * TC_KC * t.npad;
-  tc_bimage_kernel<<<(unsigned)((nb_img + thr - 1) / thr), thr, 0, stream>>>(
-      d_W.p, ldw, G2, nR, t.npad, t.n_chunks, reinterpret_cast<__nv_bfloat16*>(d_bimg.p));
+  const unsigned nbb = (unsigned)((nb_img + thr - 1) / thr);
+  if (f16) {
+    tc_wscale_kernel<<<(unsigned)nR, 256, 0, stream>>>(d_W.p, ldw, G2, t.wexp.p, d_col_scale.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    tc_bimage_kernel<true><<<nbb, thr, 0, stream>>>(d_W.p, ldw, G2, nR, t.npad, t.n_chunks,
+                                                    t.wexp.p, d_bimg.p);
+  } else {
+    tc_bimage_kernel<false><<<nbb, thr, 0, stream>>>(d_W.p, ldw, G2, nR, t.npad, t.n_chunks,
+                                                     nullptr, d_bimg.p);
+  }
   MQCT_CUDA_TRY(cudaGetLastError());
   int64_t np_img = (int64_t)n_basis_rows * t.n_chunks * TC_PSI_LD;
   tc_psiimage_kernel<<<(unsigned)((np_img + thr - 1) / thr), thr, 0, stream>>>(
@@ -519,14 +622,15 @@ int MatrixPlan::tc_execute() {
   a.rowa = d_rowa.p;
   a.rowb = d_rowb.p;
   a.psi_img = d_psi32.p;
-  a.b_img = reinterpret_cast<const __nv_bfloat16*>(d_bimg.p);
+  a.b_img = d_bimg.p;
   a.alpha = n_alpha > 0 ? t.alpha.p : nullptr;
   a.walpha = n_alpha > 0 ? t.walpha.p : nullptr;
   a.part = d_part.p;
   a.part_stride = (int64_t)n_rows * tc_ldp;
   a.status = d_status.p;
   int grid = std::min(a.n_units, t.n_sm);
-  tc_contract_kernel<<<grid, TC_THREADS, t.smem, stream>>>(a);
+  if (f16) tc_contract_kernel<true><<<grid, TC_THREADS, t.smem, stream>>>(a);
+  else tc_contract_kernel<false><<<grid, TC_THREADS, t.smem, stream>>>(a);
   MQCT_CUDA_TRY(cudaGetLastError());
   return MQCT_OK;
 }

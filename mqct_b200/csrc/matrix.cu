@@ -15,8 +15,8 @@
 //   K1 basis_kernel        rotor wavefunctions on the grid, FP64, per m-block
 //   K2 pes_weight_kernel   PES on (grid x R) times the quadrature weights
 //   K3 contract_fp64_kernel / tcgen05 split-precision kernel (contract_tc.cu)
-//   K4 reduce_kernel + spline_kernel: FP64 sum of partials, Hartree units,
-//                          MIJ_CUTOFF, clamped spline y2
+//   K4 finalize_kernel: FP64 sum of partials, Hartree units, MIJ_CUTOFF,
+//                          clamped spline y2 (one kernel)
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -254,33 +254,80 @@ contract_fp64_kernel(int n_rows, int G2, int nR, const int* __restrict__ row_a,
 }
 
 // ------------------------------------------------------------------ K4: finalize
-// (a) reduce_kernel: one CTA per reference element k: sum the contraction
-//     partials of its GEMM row in FP64, convert to Hartree, write Mat_el(:,k)
-//     (coalesced along R) and apply MIJ_CUTOFF at R~r_cut1/r_cut2
-//     (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997): the column is zeroed and
-//     flagged when max(|M(ir1)|, |M(ir2)|) < cut.
+// finalize_kernel: one CTA per reference element k.
+//  (a) sum the contraction partials of its GEMM row in FP64 (fixed order),
+//      convert to Hartree (times the exact per-column factor of the F16x3
+//      scaling), write Mat_el(:,k) coalesced along R;
+//  (b) MIJ_CUTOFF at R~r_cut1/r_cut2 (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997):
+//      the column is zeroed and flagged when max(|M(ir1)|, |M(ir2)|) < cut;
+//  (c) the clamped cubic spline with finite-difference end slopes
+//      (MQCT_SOURCE_CODES/matrix_ini.f:2005-2016; recurrence of
+//      MQCT_SOURCE_CODES/suppl_routines.f:914-965).  With both end slopes equal
+//      to the end differences, u_0 = 0 and u_n = 0; the remaining recurrence
+//      u_i = t_i - s_i u_{i-1}, y2_i = f_i y2_{i+1} + u_i has grid-only s_i, f_i
+//      and data terms t_i = c_i (d_i - d_{i-1}), d_i = (y_{i+1} - y_i) / h_i,
+//      which all threads form in parallel; one thread runs the two first-order
+//      recurrences (one FMA per step).
+// Grid coefficients (5 x nR, see MatrixPlan::init): 1/h_i, c_i, s_i, f_i, and
+// in slot [4 nR] the factor of y2_{n-1} = -u_{n-2} / (2 (f_{n-2}/2 + 1)).
 template <class TP>
-__global__ void reduce_kernel(int64_t P, int nR, const int* __restrict__ k_to_row,
-                              const TP* __restrict__ part, int n_part, int64_t part_stride, int ldp,
-                              double scale, int ir1, int ir2, double cut, double* __restrict__ mat,
-                              int* __restrict__ skipped) {
+__global__ void __launch_bounds__(128)
+finalize_kernel(int64_t P, int nR, const int* __restrict__ k_to_row, const TP* __restrict__ part,
+                int n_part, int64_t part_stride, int ldp, double scale,
+                const double* __restrict__ col_scale, int ir1, int ir2, double cut,
+                const double* __restrict__ gc, double* __restrict__ mat,
+                int* __restrict__ skipped, double* __restrict__ y2) {
+  extern __shared__ double fin_sm[];
+  double* __restrict__ col = fin_sm;           // nR values
+  double* __restrict__ t = fin_sm + nR;        // nR recurrence terms, then u
   __shared__ double cut_vals[2];
   const int64_t k = blockIdx.x;
   const int row = k_to_row[k];
-  double* col = mat + (size_t)k * nR;
   for (int i = threadIdx.x; i < nR; i += blockDim.x) {
-    double s = 0.0;
-    for (int p = 0; p < n_part; ++p) s += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
-    s *= scale;
-    col[i] = s;
-    if (i == ir1) cut_vals[0] = s;
-    if (i == ir2) cut_vals[1] = s;
+    double v = 0.0;
+    for (int p = 0; p < n_part; ++p) v += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
+    v *= col_scale ? scale * col_scale[i] : scale;
+    col[i] = v;
+    if (i == ir1) cut_vals[0] = v;
+    if (i == ir2) cut_vals[1] = v;
   }
   __syncthreads();
   const bool drop = fmax(fabs(cut_vals[0]), fabs(cut_vals[1])) < cut;
-  if (drop)
-    for (int i = threadIdx.x; i < nR; i += blockDim.x) col[i] = 0.0;
+  double* out = mat + (size_t)k * nR;
+  for (int i = threadIdx.x; i < nR; i += blockDim.x) out[i] = drop ? 0.0 : col[i];
   if (threadIdx.x == 0 && skipped) skipped[k] = drop ? 1 : 0;
+  if (!y2) return;
+  double* oy = y2 + (size_t)k * nR;
+  if (drop || nR < 3) {
+    for (int i = threadIdx.x; i < nR; i += blockDim.x) oy[i] = 0.0;
+    return;
+  }
+  const double* invh = gc;
+  const double* cfac = gc + nR;
+  const double* sfac = gc + 2 * nR;
+  const double* ffac = gc + 3 * nR;
+  for (int i = 1 + threadIdx.x; i < nR - 1; i += blockDim.x) {
+    const double d1 = (col[i + 1] - col[i]) * invh[i];
+    const double d0 = (col[i] - col[i - 1]) * invh[i - 1];
+    t[i] = cfac[i] * (d1 - d0);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;  // u_0
+    for (int i = 1; i < nR - 1; ++i) {
+      u = fma(-sfac[i], u, t[i]);
+      t[i] = u;
+    }
+    double yv = gc[4 * nR] * u;  // y2_{n-1}
+    col[nR - 1] = yv;
+    for (int i = nR - 2; i >= 1; --i) {
+      yv = fma(ffac[i], yv, t[i]);
+      col[i] = yv;
+    }
+    col[0] = ffac[0] * yv;  // u_0 = 0
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nR; i += blockDim.x) oy[i] = col[i];
 }
 
 // (b) spline_kernel: clamped cubic spline with finite-difference end slopes
@@ -357,7 +404,9 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
                  "matrix build supports SYS_TYPE 1 and 4 (got %d)", sys->sys_type);
   MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31), "P out of range");
   MQCT_ARG_CHECK(nR_ >= 2, "nR must be >= 2");
-  MQCT_ARG_CHECK(prec == MQCT_PREC_FP64 || prec == MQCT_PREC_BF16X3, "unknown precision %d", prec);
+  MQCT_ARG_CHECK(nR_ <= 3072, "nR=%d beyond the finalize limit of 3072 points", nR_);
+  MQCT_ARG_CHECK(prec == MQCT_PREC_FP64 || prec == MQCT_PREC_BF16X3 || prec == MQCT_PREC_F16X3,
+                 "unknown precision %d", prec);
   MQCT_ARG_CHECK(sys->n_states > 0 && sys->indx_chann && sys->m12 && sys->j1,
                  "system without states");
   MQCT_ARG_CHECK(sys->sys_type == 1 || (sys->vec1 && sys->ldv > 0), "type 4 needs eigenvectors");
@@ -526,24 +575,22 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
     }
   }
 
-  // --- spline coefficients that depend on the grid only
+  // --- grid-only coefficients of the fused spline fit (finalize_kernel)
   {
-    std::vector<double> coef(3 * (size_t)nR, 0.0);
-    double prev = -0.5;  // y2[0] of the clamped spline
-    coef[nR + 0] = prev;
+    std::vector<double> gc(5 * (size_t)nR, 0.0);
+    double f = -0.5;  // y2 recurrence factor at i = 0
+    gc[3 * nR] = f;
+    for (int i = 0; i + 1 < nR; ++i) gc[i] = 1.0 / (Rh[i + 1] - Rh[i]);
     for (int i = 1; i < nR - 1; ++i) {
-      double sig = (Rh[i] - Rh[i - 1]) / (Rh[i + 1] - Rh[i - 1]);
-      double p = sig * prev + 2.0;
-      prev = (sig - 1.0) / p;
-      coef[i] = sig;
-      coef[nR + i] = prev;
-      coef[2 * nR + i] = 1.0 / p;
+      const double sig = (Rh[i] - Rh[i - 1]) / (Rh[i + 1] - Rh[i - 1]);
+      const double p = sig * f + 2.0;
+      f = (sig - 1.0) / p;
+      gc[nR + i] = 6.0 / (Rh[i + 1] - Rh[i - 1]) / p;
+      gc[2 * nR + i] = sig / p;
+      gc[3 * nR + i] = f;
     }
-    MQCT_CUDA_TRY(d_spl_coef.upload(coef, stream));
-    spline_smem = sizeof(double) * 2 * 32 * (size_t)(nR + 1);
-    MQCT_ARG_CHECK(spline_smem <= 200 * 1024, "nR=%d too large for the spline kernel", nR);
-    MQCT_CUDA_TRY(cudaFuncSetAttribute(spline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)spline_smem));
+    gc[4 * nR] = nR >= 3 ? -0.5 / (0.5 * gc[3 * nR + nR - 2] + 1.0) : 0.0;
+    MQCT_CUDA_TRY(d_spl_fin.upload(gc, stream));
   }
   // --- work buffers
   MQCT_CUDA_TRY(d_psi.alloc((size_t)n_basis_rows * G2));
@@ -579,6 +626,7 @@ int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
   int rc = run_basis_and_pes();
   if (rc) return rc;
   MQCT_CUDA_TRY(cudaEventRecord(ev[1], stream));
+  const size_t fin_smem = sizeof(double) * 2 * (size_t)nR;
   if (precision == MQCT_PREC_FP64) {
     dim3 g((n_rows + F_TM - 1) / F_TM, (nR + F_TN - 1) / F_TN);
     contract_fp64_kernel<<<g, 256, 0, stream>>>(n_rows, G2, nR, d_rowa.p, d_rowb.p, d_rowm.p,
@@ -586,24 +634,18 @@ int MatrixPlan::execute(double* d_mat, double* d_y2, int32_t* d_skipped) {
                                                 d_walpha.p, d_acc.p);
     MQCT_CUDA_TRY(cudaGetLastError());
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
-    reduce_kernel<double><<<(unsigned)P, 128, 0, stream>>>(P, nR, d_k2r.p, d_acc.p, 1, 0, nR,
-                                                           kCmToHartree, ir1, ir2, cut, d_mat,
-                                                           d_skipped);
+    finalize_kernel<double><<<(unsigned)P, 128, fin_smem, stream>>>(
+        P, nR, d_k2r.p, d_acc.p, 1, 0, nR, kCmToHartree, nullptr, ir1, ir2, cut, d_spl_fin.p,
+        d_mat, d_skipped, d_y2);
     MQCT_CUDA_TRY(cudaGetLastError());
   } else {
     rc = tc_execute();
     if (rc) return rc;
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], stream));
-    reduce_kernel<float><<<(unsigned)P, 128, 0, stream>>>(
-        P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree, ir1,
-        ir2, cut, d_mat, d_skipped);
-    MQCT_CUDA_TRY(cudaGetLastError());
-  }
-  if (d_y2) {
-    // the spline needs the cutoff flags; use the caller's or the plan's buffer
-    const int* flags = d_skipped;
-    spline_kernel<<<(unsigned)((P + SPL_EL - 1) / SPL_EL), 128, spline_smem, stream>>>(
-        P, nR, d_R.p, d_spl_coef.p, d_mat, flags, d_y2);
+    finalize_kernel<float><<<(unsigned)P, 128, fin_smem, stream>>>(
+        P, nR, d_k2r.p, d_part.p, tc_splits, (int64_t)n_rows * tc_ldp, tc_ldp, kCmToHartree,
+        precision == MQCT_PREC_F16X3 ? d_col_scale.p : nullptr, ir1, ir2, cut, d_spl_fin.p, d_mat,
+        d_skipped, d_y2);
     MQCT_CUDA_TRY(cudaGetLastError());
   }
   MQCT_CUDA_TRY(cudaEventRecord(ev[3], stream));

@@ -16,6 +16,7 @@ struct TcInfo {
   DevBuf<int> blk_row0, blk_n, blk_m;
   DevBuf<int64_t> blk_img_off;
   DevBuf<float> alpha, walpha;
+  DevBuf<int> wexp;  // F16x3: power-of-two exponent of each W column
 };
 
 struct MatrixPlan {
@@ -48,10 +49,10 @@ struct MatrixPlan {
   DevBuf<double> d_W;     // G2 x ldw, FP64
   int ldw = 0;
   DevBuf<double> d_acc;   // FP64 form: n_rows x nR
-  DevBuf<double> d_spl_coef;  // grid-only spline coefficients (sig, y2 factor, 1/p)
-  size_t spline_smem = 0;
+  DevBuf<double> d_spl_fin;   // grid-only coefficients of the fused spline fit
+  DevBuf<double> d_col_scale; // F16x3: exact per-column rescaling of the contraction
 
-  // tcgen05 split-precision path (contract_tc.cu)
+  // tcgen05 split-precision paths (contract_tc.cu)
   int tc_splits = 1, tc_ldp = 0, tc_npad = 0, tc_nchunk = 0;
   DevBuf<float> d_part;                 // tc_splits x n_rows x tc_ldp
   DevBuf<unsigned short> d_bimg;        // pre-swizzled B (W) images, hi/lo planes
