@@ -153,6 +153,7 @@ def _matrix_bench(mq, s, R, c2, precision, steps, warmup, torch, flush):
         torch.cuda.synchronize()
         plan.execute(d_mat.data_ptr(), d_y2.data_ptr(), d_sk.data_ptr())
         seg.append(plan.timing())
+    plan.sync()  # raises if a device-side wait of the timed builds ran out of rounds
     torch.cuda.synchronize()
     return plan, d_mat, d_sk, np.array(seg)
 
