@@ -161,6 +161,7 @@ def _matrix_bench(mq, s, R, c2, precision, steps, warmup, torch, flush):
 def run_gpu(a):
     import torch
     import mqct_b200 as mq
+    from mqct_b200 import replicas
     from mqct_b200 import synthetic as syn
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -200,11 +201,7 @@ def run_gpu(a):
         barrier()
         wall = time.perf_counter() - t0
     step_ms = seg.sum(axis=1)
-    ms = float(np.mean(step_ms))
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(float(np.mean(step_ms)), dist, device="cuda")
     n_el = s.P * len(R)
     value = world * n_el / (ms / 1e3)
     flops = plan.flops
@@ -258,7 +255,7 @@ def run_gpu(a):
     # propagation (secondary)
     prop = None
     if not a.no_propagation:
-        prop = run_propagation(mq, syn, s, R, mat, a, torch, world)
+        prop = run_propagation(mq, syn, s, R, mat, a, torch, world, dist)
 
     if rank != 0:
         if dist is not None:
@@ -340,7 +337,8 @@ def matrix_accuracy(m1, m0, sk1, sk0, torch):
             "max_fp64_element_of_differing_flags": float(rowmax[flag_diff].max()) if bool(flag_diff.any()) else 0.0}
 
 
-def run_propagation(mq, syn, s, R, mat, a, torch, world):
+def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
+    from mqct_b200 import replicas
     c3 = syn.config_c3()
     tab = mq.PropagationTables.from_system(s, R, mat, syn.config_c2()["mass_amu"])
     n = min(a.c3_traj, c3["n_traj"])
@@ -357,7 +355,7 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world):
         t0 = time.perf_counter()
         amp, cls, diag = plan.run(trajs[:nt])
         wall = time.perf_counter() - t0
-        ms = plan.timing()
+        ms = replicas.max_over_ranks(plan.timing(), dist, device="cuda")
         steps = float(diag[:, 1].sum())
         res[name] = {"n_traj": nt, "kernel_ms": ms, "wall_s": wall,
                      "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
