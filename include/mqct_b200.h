@@ -99,15 +99,20 @@ typedef struct mqct_grid_t {
 /* Potential energy surface (the USER_DEFINED_PES plugin, called through the
  * per-type wrappers of MQCT_SOURCE_CODES/pes_sys_type.f:2-97).  Values in
  * cm^-1, R in bohr.
- *   TABLE:    caller-evaluated V on the (beta, gamma) grid, table[iR*G + g]
- *             with g = i_beta*n_gamma + i_gamma (G = n_beta for type 1); the
- *             surface of an atom + rigid rotor does not depend on alpha.  The
- *             analogue of the reference's VGRID_UF.DAT path;
+ *   TABLE:    caller-evaluated V on the angular grid, table[iR*G + g] with
+ *             g = i_beta*n_gamma + i_gamma (type 4; the surface of an atom +
+ *             rigid rotor does not depend on alpha), g = i_beta (type 1, G =
+ *             n_beta) or, for type 0, the 5-D index over (alpha2, beta1, beta2,
+ *             gamma1, gamma2) with gamma2 fastest.  The analogue of the
+ *             reference's VGRID_UF.DAT path;
  *   LEGENDRE: V(R,beta) = sum_l [A_l e^{-b_l R} - C_l/R^6] P_l(cos beta),
  *             params = [A_0..A_{n-1}, b_0.., C_0..];
  *   SITES1:   rigid-rotor sites + atom, per term [site, D, a, re, C6, rd]:
  *             D(e^{-2a(r-re)} - 2e^{-a(r-re)}) - C6 (1 - e^{-(r/rd)^6}) / r^6;
- *   SITES2:   two rigid rotors, per term [site1, site2, D, a, re, C6, rd]. */
+ *   SITES2:   two rigid rotors (type 0): rotor 1 at the origin with Euler
+ *             angles (0, beta1, gamma1), rotor 2 at R z with (alpha2, beta2,
+ *             gamma2) (the argument mapping of MQCT_SOURCE_CODES/pes_sys_type.f:90-97),
+ *             per term [site1, site2, D, a, re, C6, rd]. */
 #define MQCT_PES_TABLE 0
 #define MQCT_PES_LEGENDRE 1
 #define MQCT_PES_SITES1 2
@@ -131,7 +136,7 @@ typedef struct mqct_err_report_t {
   double rms_rel_err;        /* out                                            */
 } mqct_err_report_t;
 
-/* Matrix build: M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
+/* Matrix build (SYS_TYPE 1, 4 and 0): M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
  * (MQCT_SOURCE_CODES/pot_comp.f:1947-1952, 2535-2557, 3709-3721), converted to
  * Hartree, MIJ_CUTOFF truncation at R~r_cut1/r_cut2
  * (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997, columns whose max |M| there is

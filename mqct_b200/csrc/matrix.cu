@@ -46,16 +46,64 @@ static int upload_logfact() {
 }
 
 // ------------------------------------------------------------------ K1: basis
-// psi for block-local state s at 2-D grid point g2 (beta outer, gamma inner):
+// Second rotor and 5-D grid of SYS_TYPE 0 (two asymmetric tops).  Grid order
+// (alpha2, beta1, beta2, gamma1, gamma2), gamma2 fastest; alpha1 = 0 with the
+// analytic factor 2 pi in the weights (MQCT_SOURCE_CODES/pot_comp.f:3663-3721).
+struct Type0Dev {
+  const int* ch_j2;        // per channel
+  const double* vec2;      // per channel, stride ldv
+  const double* cg;        // per state: CG(j1 m1 j2 m12-m1 | j12 m12) at [m1 + j1], stride cg_ld
+  int cg_ld;
+  const double* beta2;
+  const double* alpha2;
+  const double* gamma2;
+  int nb1, ng1, nbb, naa, ngg;
+};
+
+__device__ inline void t0_index(const Type0Dev& t, int64_t g, int& ia2, int& ib1, int& ib2,
+                                int& ig1, int& ig2) {
+  ig2 = (int)(g % t.ngg);
+  int64_t r = g / t.ngg;
+  ig1 = (int)(r % t.ng1);
+  r /= t.ng1;
+  ib2 = (int)(r % t.nbb);
+  r /= t.nbb;
+  ib1 = (int)(r % t.nb1);
+  ia2 = (int)(r / t.nb1);
+}
+
+// Asymmetric-top wavefunction sum_K c_K sqrt((2j+1)/8pi^2) D^j_{Km}(alpha, beta,
+// gamma), D = d^j_{Km}(beta) e^{i(K gamma + m alpha)} (WF_ASYM_TOP,
+// MQCT_SOURCE_CODES/basis_wave_functions.f:83-116; Djkm MQCT_SOURCE_CODES/pot_comp.f:256-309).
+__device__ inline double2 asym_wf(int j, int m, const double* c, double alpha, double beta,
+                                  double gamma) {
+  const double nrm = sqrt((2.0 * j + 1.0) / 8.0 / (kPi * kPi));
+  double re = 0.0, im = 0.0;
+  for (int i = 0; i <= 2 * j; ++i) {
+    const int K = i - j;
+    if (c[i] == 0.0) continue;
+    const double d = mqct_dev::wigner_d(j, K, m, beta, c_logfact) * nrm * c[i];
+    double s, co;
+    sincos(K * gamma + m * alpha, &s, &co);
+    re += d * co;
+    im += d * s;
+  }
+  return make_double2(re, im);
+}
+
+// psi for block-local state s at grid point g:
 // type 1: Y_jm(beta, 0) (WF_DIAT_TOP, MQCT_SOURCE_CODES/basis_wave_functions.f:153-175);
 // type 4: sum_K c_K sqrt((2j+1)/8pi^2) d^j_{Km}(beta) e^{iK gamma} at alpha = 0
-//         (WF_ASYM_TOP :83-116 with Djkm MQCT_SOURCE_CODES/pot_comp.f:256-309).
-// Output psi[(blk_off + s) * G2 + g2] as (re, im) FP64.
+//         (WF_ASYM_TOP :83-116 with Djkm MQCT_SOURCE_CODES/pot_comp.f:256-309); the
+//         2-D grid has beta outer, gamma inner;
+// type 0: sum_{m1} CG(j1 m1 j2 m2 | j12 m12) psi1_{m1}(0, beta1, gamma1)
+//         psi2_{m2}(alpha2, beta2, gamma2) (WF_ASYM_TOP_ASYM_TOP :1-41) on the 5-D grid.
+// Output psi[(blk_off + s) * G2 + g] as (re, im) FP64.
 __global__ void basis_kernel(int sys_type, int n_rows, const int* __restrict__ row_state,
                              const int* __restrict__ st_chan, const int* __restrict__ st_m,
                              const int* __restrict__ ch_j, const double* __restrict__ vec,
                              int ldv, const double* __restrict__ beta,
-                             const double* __restrict__ gamma, int n_gamma, int G2,
+                             const double* __restrict__ gamma, int n_gamma, int G2, Type0Dev t0,
                              double2* __restrict__ psi) {
   int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)n_rows * G2) return;
@@ -71,6 +119,22 @@ __global__ void basis_kernel(int sys_type, int n_rows, const int* __restrict__ r
     double nrm = sqrt((2.0 * j + 1.0) / 4.0 / kPi * exp(c_logfact[j - am] - c_logfact[j + am]));
     re = pl * nrm;
     if (m < 0 && (am & 1)) re = -re;
+  } else if (sys_type == 0) {
+    int ia2, ib1, ib2, ig1, ig2;
+    t0_index(t0, g2, ia2, ib1, ib2, ig1, ig2);
+    const int j2 = t0.ch_j2[ch];
+    const double* c1 = vec + (size_t)ch * ldv;
+    const double* c2 = t0.vec2 + (size_t)ch * ldv;
+    const double* cgs = t0.cg + (size_t)st * t0.cg_ld;
+    for (int m1 = -j; m1 <= j; ++m1) {
+      const int m2 = m - m1;
+      const double w = cgs[m1 + j];
+      if (m2 < -j2 || m2 > j2 || w == 0.0) continue;
+      const double2 p1 = asym_wf(j, m1, c1, 0.0, beta[ib1], gamma[ig1]);
+      const double2 p2 = asym_wf(j2, m2, c2, t0.alpha2[ia2], t0.beta2[ib2], t0.gamma2[ig2]);
+      re += w * (p1.x * p2.x - p1.y * p2.y);
+      im += w * (p1.x * p2.y + p1.y * p2.x);
+    }
   } else {
     int ib = g2 / n_gamma, ig = g2 % n_gamma;
     double b = beta[ib], g = gamma[ig];
@@ -104,6 +168,38 @@ __device__ inline double site_term(double r, const double* t) {
   double r2 = r * r, r6 = r2 * r2 * r2;
   double x = r / rd, x2 = x * x, x6 = x2 * x2 * x2;
   return D * (e * e - 2.0 * e) - c6 * (1.0 - exp(-x6)) / r6;
+}
+
+// Rotation Rz(a) Ry(b) Rz(g) applied to a site position.
+__device__ inline void euler_apply(double a, double b, double g, const double* s, double* x) {
+  double ca, sa, cb, sb, cg, sg;
+  sincos(a, &sa, &ca);
+  sincos(b, &sb, &cb);
+  sincos(g, &sg, &cg);
+  const double m00 = ca * cb * cg - sa * sg, m01 = -ca * cb * sg - sa * cg, m02 = ca * sb;
+  const double m10 = sa * cb * cg + ca * sg, m11 = -sa * cb * sg + ca * cg, m12 = sa * sb;
+  const double m20 = -sb * cg, m21 = sb * sg, m22 = cb;
+  x[0] = m00 * s[0] + m01 * s[1] + m02 * s[2];
+  x[1] = m10 * s[0] + m11 * s[1] + m12 * s[2];
+  x[2] = m20 * s[0] + m21 * s[1] + m22 * s[2];
+}
+
+// SITES2 family for two rigid rotors: rotor 1 at the origin with Euler angles
+// (alpha, beta, gamma), rotor 2 at R z with (aalpha, bbeta, ggamma); per term
+// [site1, site2, D, a, re, C6, rd].
+__device__ inline double pes_eval_sites2(const PesDev& P, double R, double alpha, double beta,
+                                         double gamma, double aalpha, double bbeta, double ggamma) {
+  double v = 0.0;
+  for (int t = 0; t < P.n_terms; ++t) {
+    const double* q = P.p + 7 * t;
+    double x1[3], x2[3];
+    euler_apply(alpha, beta, gamma, P.s1 + 3 * (int)q[0], x1);
+    euler_apply(aalpha, bbeta, ggamma, P.s2 + 3 * (int)q[1], x2);
+    x2[2] += R;
+    const double dx = x2[0] - x1[0], dy = x2[1] - x1[1], dz = x2[2] - x1[2];
+    v += site_term(sqrt(dx * dx + dy * dy + dz * dz), q + 2);
+  }
+  return v;
 }
 
 // USER_DEFINED_PES(V,R,..,alpha,beta,gamma,..) for the built-in families.
@@ -145,10 +241,11 @@ __device__ inline double pes_eval(const PesDev& P, double R, double beta, double
 
 // W[g2 * ldw + i] = wt[g2] * V(R_i, angles(g2)) with the argument mapping of
 // MQCT_SOURCE_CODES/pes_sys_type.f: type 1 passes beta (:8), type 4 passes
-// (-beta, -gamma) (:36).
+// (-beta, -gamma) (:36), type 0 passes (0, beta1, gamma1, alpha2, beta2, gamma2)
+// (:90-97).
 __global__ void pes_weight_kernel(int sys_type, PesDev pes, int G2, int nR,
                                   const double* __restrict__ R, const double* __restrict__ beta,
-                                  const double* __restrict__ gamma, int n_gamma,
+                                  const double* __restrict__ gamma, int n_gamma, Type0Dev t0,
                                   const double* __restrict__ wt, double* __restrict__ W,
                                   int ldw) {
   int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,6 +256,11 @@ __global__ void pes_weight_kernel(int sys_type, PesDev pes, int G2, int nR,
     v = pes.table[(size_t)i * G2 + g2];
   } else if (sys_type == 1) {
     v = pes_eval(pes, R[i], beta[g2], 0.0);
+  } else if (sys_type == 0) {
+    int ia2, ib1, ib2, ig1, ig2;
+    t0_index(t0, g2, ia2, ib1, ib2, ig1, ig2);
+    v = pes_eval_sites2(pes, R[i], 0.0, beta[ib1], gamma[ig1], t0.alpha2[ia2], t0.beta2[ib2],
+                        t0.gamma2[ig2]);
   } else {
     int ib = g2 / n_gamma, ig = g2 % n_gamma;
     v = pes_eval(pes, R[i], -beta[ib], -gamma[ig]);
@@ -385,6 +487,27 @@ __global__ void spline_kernel(int64_t P, int nR, const double* __restrict__ R,
 }
 
 // ------------------------------------------------------------------ plan
+// Clebsch-Gordan coefficient <j1 m1 j2 m2 | J M> for integer arguments (Racah's
+// closed form; the coupling of WF_ASYM_TOP_ASYM_TOP,
+// MQCT_SOURCE_CODES/basis_wave_functions.f:1-41).
+static double clebsch_gordan(int j1, int m1, int j2, int m2, int J, int M) {
+  if (m1 + m2 != M || J < abs(j1 - j2) || J > j1 + j2 || abs(m1) > j1 || abs(m2) > j2 ||
+      abs(M) > J)
+    return 0.0;
+  auto lf = [](int n) { return std::lgamma((double)n + 1.0); };
+  const double pre = 0.5 * (std::log(2.0 * J + 1.0) + lf(J + j1 - j2) + lf(J - j1 + j2) +
+                            lf(j1 + j2 - J) - lf(j1 + j2 + J + 1) + lf(J + M) + lf(J - M) +
+                            lf(j1 - m1) + lf(j1 + m1) + lf(j2 - m2) + lf(j2 + m2));
+  double sum = 0.0;
+  for (int k = 0; k <= j1 + j2 - J; ++k) {
+    const int a = j1 - m1 - k, b = j2 + m2 - k, c = J - j2 + m1 + k, d = J - j1 - m2 + k;
+    if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+    const double t = std::exp(pre - lf(k) - lf(j1 + j2 - J - k) - lf(a) - lf(b) - lf(c) - lf(d));
+    sum += (k & 1) ? -t : t;
+  }
+  return sum;
+}
+
 static int nearest_index(const std::vector<double>& R, double r) {
   int best = 0;
   double d = fabs(R[0] - r);
@@ -400,8 +523,8 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
                      int32_t nR_, const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec,
                      double mij_cut, double rc1, double rc2) {
   MQCT_ARG_CHECK(sys && ind_mat && R && grid && pes, "null argument");
-  MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 4,
-                 "matrix build supports SYS_TYPE 1 and 4 (got %d)", sys->sys_type);
+  MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 4 || sys->sys_type == 0,
+                 "matrix build supports SYS_TYPE 1, 4 and 0 (got %d)", sys->sys_type);
   MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31), "P out of range");
   MQCT_ARG_CHECK(nR_ >= 2, "nR must be >= 2");
   MQCT_ARG_CHECK(nR_ <= 3072, "nR=%d beyond the finalize limit of 3072 points", nR_);
@@ -409,11 +532,20 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
                  "unknown precision %d", prec);
   MQCT_ARG_CHECK(sys->n_states > 0 && sys->indx_chann && sys->m12 && sys->j1,
                  "system without states");
-  MQCT_ARG_CHECK(sys->sys_type == 1 || (sys->vec1 && sys->ldv > 0), "type 4 needs eigenvectors");
+  MQCT_ARG_CHECK(sys->sys_type == 1 || (sys->vec1 && sys->ldv > 0), "rotor eigenvectors missing");
   MQCT_ARG_CHECK(grid->n_beta > 0 && (sys->sys_type == 1 || grid->n_gamma > 0), "empty grid");
-  MQCT_ARG_CHECK(pes->kind == MQCT_PES_TABLE || pes->kind == MQCT_PES_LEGENDRE ||
-                     pes->kind == MQCT_PES_SITES1,
-                 "PES kind %d not usable for SYS_TYPE %d", pes->kind, sys->sys_type);
+  if (sys->sys_type == 0) {
+    MQCT_ARG_CHECK(sys->j2 && sys->vec2 && sys->j12, "SYS_TYPE 0 needs j2, vec2 and j12");
+    MQCT_ARG_CHECK(grid->n_beta2 > 0 && grid->n_alpha2 > 0 && grid->n_gamma2 > 0 &&
+                       grid->n_alpha == 0,
+                   "SYS_TYPE 0 needs n_beta2, n_alpha2, n_gamma2 > 0 and n_alpha = 0");
+    MQCT_ARG_CHECK(pes->kind == MQCT_PES_TABLE || pes->kind == MQCT_PES_SITES2,
+                   "PES kind %d not usable for SYS_TYPE 0", pes->kind);
+  } else {
+    MQCT_ARG_CHECK(pes->kind == MQCT_PES_TABLE || pes->kind == MQCT_PES_LEGENDRE ||
+                       pes->kind == MQCT_PES_SITES1,
+                   "PES kind %d not usable for SYS_TYPE %d", pes->kind, sys->sys_type);
+  }
   MQCT_ARG_CHECK(pes->kind != MQCT_PES_TABLE || pes->table, "TABLE PES without table");
   for (int i = 0; i < nR_ - 1; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
   int rc = upload_logfact();
@@ -436,7 +568,16 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
     int ch = sys->indx_chann[s] - 1;
     MQCT_ARG_CHECK(ch >= 0 && ch < sys->n_channels, "indx_chann out of range at state %d", s + 1);
     int j = sys->j1[ch];
-    MQCT_ARG_CHECK(j >= 0 && j <= 40 && abs(sys->m12[s]) <= j, "bad (j, m) at state %d", s + 1);
+    MQCT_ARG_CHECK(j >= 0 && j <= 40, "bad j at state %d", s + 1);
+    if (sys->sys_type == 0) {
+      const int j2 = sys->j2[ch], j12 = sys->j12[s];
+      MQCT_ARG_CHECK(j2 >= 0 && j2 <= 40 && j12 >= abs(j - j2) && j12 <= j + j2 &&
+                         abs(sys->m12[s]) <= j12,
+                     "bad (j1, j2, j12, m12) at state %d", s + 1);
+      MQCT_ARG_CHECK(2 * j2 + 1 <= sys->ldv, "ldv too small for j2=%d", j2);
+    } else {
+      MQCT_ARG_CHECK(abs(sys->m12[s]) <= j, "bad (j, m) at state %d", s + 1);
+    }
     MQCT_ARG_CHECK(sys->sys_type == 1 || 2 * j + 1 <= sys->ldv, "ldv too small for j=%d", j);
     by_m[sys->m12[s]].push_back(s);
   }
@@ -497,6 +638,34 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
     wt.resize(G2);
     for (int i = 0; i < G2; ++i) wt[i] = ab.w[i] * sin(ab.x[i]) * ab.half * 2.0 * kPi;
     ag.x.assign(1, 0.0);
+  } else if (sys_type == 0) {
+    // 5-D grid of INI_POT_STORAGE for two rotors (MQCT_SOURCE_CODES/pot_comp.f:1628-1700):
+    // GL in both beta, midpoint (EQ_ANG_GRID) or GL in alpha2, gamma1, gamma2
+    auto ang = [&](int n) {
+      return grid->eq_gamma ? axis_mid(n, 0.0, 2.0 * kPi) : axis_gl(n, 0.0, 2.0 * kPi);
+    };
+    ag = ang(grid->n_gamma);
+    Axis abb = axis_gl(grid->n_beta2, 0.0, kPi), aa2 = ang(grid->n_alpha2), agg = ang(grid->n_gamma2);
+    n_gamma = grid->n_gamma;
+    t0_nbb = grid->n_beta2;
+    t0_naa = grid->n_alpha2;
+    t0_ngg = grid->n_gamma2;
+    const int64_t g5 = (int64_t)t0_naa * grid->n_beta * t0_nbb * n_gamma * t0_ngg;
+    MQCT_ARG_CHECK(g5 < ((int64_t)1 << 31), "5-D grid of %lld points too large", (long long)g5);
+    G2 = (int)g5;
+    wt.resize(G2);
+    const double half = ab.half * ag.half * aa2.half * abb.half * agg.half * 2.0 * kPi;
+    int64_t g = 0;
+    for (int i2 = 0; i2 < t0_naa; ++i2)
+      for (int i3 = 0; i3 < grid->n_beta; ++i3)
+        for (int i4 = 0; i4 < t0_nbb; ++i4)
+          for (int i5 = 0; i5 < n_gamma; ++i5)
+            for (int i6 = 0; i6 < t0_ngg; ++i6)
+              wt[g++] = ab.w[i3] * ag.w[i5] * sin(ab.x[i3]) * aa2.w[i2] * abb.w[i4] * agg.w[i6] *
+                        sin(abb.x[i4]) * half;
+    MQCT_CUDA_TRY(d_beta2.upload(abb.x, stream));
+    MQCT_CUDA_TRY(d_alpha2.upload(aa2.x, stream));
+    MQCT_CUDA_TRY(d_gamma2.upload(agg.x, stream));
   } else {
     ag = grid->eq_gamma ? axis_mid(grid->n_gamma, 0.0, 2.0 * kPi)
                         : axis_gl(grid->n_gamma, 0.0, 2.0 * kPi);
@@ -538,7 +707,26 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
   MQCT_CUDA_TRY(d_st_m.upload(st_m, stream));
   MQCT_CUDA_TRY(d_ch_j.upload(ch_j, stream));
   ldv = sys->ldv > 0 ? sys->ldv : 1;
-  if (sys_type == 4) {
+  if (sys_type == 0) {
+    std::vector<int> ch_j2(sys->n_channels);
+    int j1max = 0;
+    for (int c = 0; c < sys->n_channels; ++c) {
+      ch_j2[c] = sys->j2[c];
+      j1max = std::max(j1max, sys->j1[c]);
+    }
+    cg_ld = 2 * j1max + 1;
+    std::vector<double> cg((size_t)n_states * cg_ld, 0.0);
+    for (int st = 0; st < n_states; ++st) {
+      const int ch = sys->indx_chann[st] - 1, j1 = sys->j1[ch], j2 = sys->j2[ch];
+      for (int m1 = -j1; m1 <= j1; ++m1)
+        cg[(size_t)st * cg_ld + m1 + j1] =
+            clebsch_gordan(j1, m1, j2, sys->m12[st] - m1, sys->j12[st], sys->m12[st]);
+    }
+    MQCT_CUDA_TRY(d_ch_j2.upload(ch_j2, stream));
+    MQCT_CUDA_TRY(d_cg.upload(cg, stream));
+    MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)sys->n_channels * ldv, stream));
+  }
+  if (sys_type == 4 || sys_type == 0) {
     MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)sys->n_channels * ldv, stream));
   } else {
     std::vector<double> one(sys->n_channels, 1.0);
@@ -560,10 +748,23 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
   if (pes->kind == MQCT_PES_TABLE) {
     MQCT_CUDA_TRY(d_pes_table.upload(pes->table, (size_t)nR * G2, stream));
   } else {
-    int per = pes->kind == MQCT_PES_LEGENDRE ? 3 : 6;
-    size_t np = pes->kind == MQCT_PES_LEGENDRE ? 3 * (size_t)pes->n_terms : (size_t)per * pes->n_terms;
+    const size_t per = pes->kind == MQCT_PES_LEGENDRE ? 3 : (pes->kind == MQCT_PES_SITES1 ? 6 : 7);
+    const size_t np = per * (size_t)pes->n_terms;
     MQCT_ARG_CHECK(pes->n_terms > 0 && pes->params, "PES without parameters");
     MQCT_CUDA_TRY(d_pes_p.upload(pes->params, np, stream));
+    if (pes->kind == MQCT_PES_SITES2) {
+      MQCT_ARG_CHECK(pes->n_sites1 > 0 && pes->sites1 && pes->n_sites2 > 0 && pes->sites2,
+                     "SITES2 PES without sites");
+      for (int t = 0; t < pes->n_terms; ++t) {
+        const int s1 = (int)pes->params[7 * t], s2 = (int)pes->params[7 * t + 1];
+        MQCT_ARG_CHECK(s1 >= 0 && s1 < pes->n_sites1 && s2 >= 0 && s2 < pes->n_sites2,
+                       "PES term %d references sites (%d, %d)", t, s1, s2);
+      }
+      MQCT_CUDA_TRY(d_pes_s1.upload(pes->sites1, 3 * (size_t)pes->n_sites1, stream));
+      MQCT_CUDA_TRY(d_pes_s2.upload(pes->sites2, 3 * (size_t)pes->n_sites2, stream));
+      pes_n_sites1 = pes->n_sites1;
+      pes_n_sites2 = pes->n_sites2;
+    }
     if (pes->kind == MQCT_PES_SITES1) {
       MQCT_ARG_CHECK(pes->n_sites1 > 0 && pes->sites1, "SITES1 PES without sites");
       for (int t = 0; t < pes->n_terms; ++t) {
@@ -609,14 +810,17 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
 int MatrixPlan::run_basis_and_pes() {
   int threads = 256;
   int64_t nb = (int64_t)n_basis_rows * G2;
+  const Type0Dev t0{d_ch_j2.p, d_vec2.p, d_cg.p, cg_ld, d_beta2.p, d_alpha2.p, d_gamma2.p,
+                    (int)h_beta.size(), n_gamma, t0_nbb, t0_naa, t0_ngg};
   basis_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, stream>>>(
       sys_type, n_basis_rows, d_row_state.p, d_st_chan.p, d_st_m.p, d_ch_j.p, d_vec.p, ldv,
-      d_beta.p, d_gamma.p, n_gamma, G2, d_psi.p);
+      d_beta.p, d_gamma.p, n_gamma, G2, t0, d_psi.p);
   MQCT_CUDA_TRY(cudaGetLastError());
-  PesDev pd{pes_kind, pes_n_terms, pes_n_sites1, 0, d_pes_p.p, d_pes_s1.p, nullptr, d_pes_table.p};
+  PesDev pd{pes_kind, pes_n_terms, pes_n_sites1, pes_n_sites2, d_pes_p.p, d_pes_s1.p, d_pes_s2.p,
+            d_pes_table.p};
   int64_t nw = (int64_t)G2 * nR;
   pes_weight_kernel<<<(unsigned)((nw + threads - 1) / threads), threads, 0, stream>>>(
-      sys_type, pd, G2, nR, d_R.p, d_beta.p, d_gamma.p, n_gamma, d_wt.p, d_W.p, ldw);
+      sys_type, pd, G2, nR, d_R.p, d_beta.p, d_gamma.p, n_gamma, t0, d_wt.p, d_W.p, ldw);
   MQCT_CUDA_TRY(cudaGetLastError());
   return MQCT_OK;
 }

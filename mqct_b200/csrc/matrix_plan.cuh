@@ -30,7 +30,7 @@ struct MatrixPlan {
   int ldv = 1;
   int ir1 = 0, ir2 = 0;
   double cut = 0.0;
-  int pes_kind = 0, pes_n_terms = 0, pes_n_sites1 = 0;
+  int pes_kind = 0, pes_n_terms = 0, pes_n_sites1 = 0, pes_n_sites2 = 0;
   std::vector<double> Rh, h_beta, h_gamma, h_wt, h_alpha, h_walpha;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -42,7 +42,11 @@ struct MatrixPlan {
   DevBuf<int> d_rowa, d_rowb, d_rowm, d_k2r, d_tile_block;
   DevBuf<int> d_row_state, d_st_chan, d_st_m, d_ch_j;
   DevBuf<double> d_vec, d_beta, d_gamma, d_wt, d_alpha, d_walpha, d_R;
-  DevBuf<double> d_pes_p, d_pes_s1, d_pes_table;
+  DevBuf<double> d_pes_p, d_pes_s1, d_pes_s2, d_pes_table;
+  // SYS_TYPE 0: second rotor, Clebsch-Gordan table, the extra grid axes
+  DevBuf<int> d_ch_j2;
+  DevBuf<double> d_vec2, d_cg, d_beta2, d_alpha2, d_gamma2;
+  int cg_ld = 1, t0_nbb = 1, t0_naa = 1, t0_ngg = 1;
 
   // work
   DevBuf<double2> d_psi;  // basis rows x G2, FP64

@@ -54,6 +54,49 @@ def site_pes(n_terms=12, seed=2, sites=TRIATOMIC_SITES):
                 sites1=np.ascontiguousarray(sites, dtype=np.float64).reshape(-1), sites2=None)
 
 
+def rotor_sites9(seed=5, sites=TRIATOMIC_SITES):
+    """Nine interaction sites of a rigid triatomic: its three atoms plus six seeded
+    off-atom sites within 1.5 bohr of the centre of the atoms, bohr."""
+    rng = np.random.default_rng(seed)
+    extra = rng.uniform(-1.5, 1.5, (6, 3)) + np.mean(sites, axis=0)
+    return np.concatenate([np.asarray(sites, np.float64), extra])
+
+
+def site_pes2(seed=4, sites1=None, sites2=None):
+    """Rotor + rotor site-site surface (SITES2): one Morse + damped-dispersion term
+    per pair of sites (9 x 9 = 81 terms for the nine-site rotors), D ~ U(20, 200)/9
+    cm^-1 (so the 81 terms add up to the depth of one rotor-atom well), a ~ U(0.8,
+    1.4) bohr^-1, r_e ~ U(5, 7) bohr, C6 ~ U(1e4, 1e5)/9 cm^-1 bohr^6, r_d = r_e.
+    Rotor 1 sits at the origin, rotor 2 at R along z."""
+    s1 = rotor_sites9() if sites1 is None else np.asarray(sites1, np.float64)
+    s2 = s1 if sites2 is None else np.asarray(sites2, np.float64)
+    rng = np.random.default_rng(seed)
+    n1, n2 = len(s1), len(s2)
+    n = n1 * n2
+    p = np.zeros((n, 7))
+    p[:, 0] = np.repeat(np.arange(n1), n2)
+    p[:, 1] = np.tile(np.arange(n2), n1)
+    p[:, 2] = rng.uniform(20.0, 200.0, n) / 9.0
+    p[:, 3] = rng.uniform(0.8, 1.4, n)
+    p[:, 4] = rng.uniform(5.0, 7.0, n)
+    p[:, 5] = rng.uniform(1e4, 1e5, n) / 9.0
+    p[:, 6] = p[:, 4]
+    return dict(kind=_abi.PES_SITES2, n_terms=n, params=p.reshape(-1),
+                sites1=np.ascontiguousarray(s1).reshape(-1),
+                sites2=np.ascontiguousarray(s2).reshape(-1))
+
+
+def asym_channels(jmax):
+    """(j, Ka, Kc) levels of an asymmetric top for j <= jmax in the JMIN/JMAX order
+    (MQCT_SOURCE_CODES/iotest.f:6603-6617, labels of MQCT_SOURCE_CODES/asym_top.f:139-173)."""
+    out = []
+    for j in range(jmax + 1):
+        ka = [0] + [i // 2 for i in range(2, 2 * j + 2)]
+        kc = ka[::-1]
+        out += [(j, ka[i], kc[i]) for i in range(2 * j + 1)]
+    return out
+
+
 # ---------------------------------------------------------------- configurations
 def config_c1():
     """Rigid diatom (B = 1.93 cm^-1) + atom, j = 0..10 all m (121 states),
@@ -81,6 +124,20 @@ def config_c2(alpha_grid=True):
     return dict(name="c2_asym_top_atom", sys_type=4, channels=chans, A=27.9, B=14.5, C=9.3,
                 grid=(48, 48, 48 if alpha_grid else 0, 0, 0, 0, 1), nR=300, rmin=3.0,
                 rmax=25.0, pes=site_pes(12, seed=2), mass_amu=3.7523705333)
+
+
+def config_c4(jmax=5, j12_sum_max=None, grid_n=24):
+    """Two asymmetric tops (A, B, C = 27.9, 14.5, 9.3 cm^-1 each), channel pairs with
+    j1, j2 <= jmax (and j1 + j2 <= j12_sum_max if given), 5-D grid grid_n^5 (GL in
+    both beta, midpoint in alpha2, gamma1, gamma2), 200 R points 4-25 bohr, the 81-term
+    SITES2 surface, reduced mass 9.00764 amu."""
+    lv = asym_channels(jmax)
+    chans = [(a + b) for a in lv for b in lv
+             if j12_sum_max is None or a[0] + b[0] <= j12_sum_max]
+    n = grid_n
+    return dict(name="c4_two_asym_tops", sys_type=0, channels=chans, A=27.9, B=14.5, C=9.3,
+                grid=(n, n, 0, n, n, n, 1), nR=200, rmin=4.0, rmax=25.0, pes=site_pes2(),
+                mass_amu=9.00764)
 
 
 def config_c3():
