@@ -17,10 +17,11 @@
 //               (hi and lo planes, K-major core-matrix layout) and the block's
 //               rotor-basis slice, one cp.async.bulk each, mbarrier complete_tx;
 //   warp 1      TMEM allocator + single-thread MMA issuer;
-//   warps 2..9  X producers: X = w_alpha Re((z psi_a)^* (z psi_b)) in FP32 from
-//               the staged basis (z = e^{i m alpha}), split to BF16 hi/lo and
-//               written in the core-matrix layout, two threads per tile row
-//               (each half of the chunk's K groups); afterwards the epilogue
+//   warps 2..9  X producers: X = w_alpha Re(psi_a^* psi_b) in FP32 from the
+//               staged basis (the e^{i m alpha} phases of a same-m pair cancel),
+//               split to 16-bit hi/lo and written in the core-matrix layout, two
+//               threads per tile row (each half of the chunk's K groups), one
+//               A stage per alpha point; afterwards the epilogue
 //               (tcgen05.ld of the accumulator, FP32 partials to global; the
 //               two warps of a TMEM lane quarter take alternate 16-column
 //               slices).
@@ -403,7 +404,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       const int blk = a.tile_block[tile];
       const int row = tile * TC_M + p;
       const int la = a.rowa[row] - a.blk_row0[blk], lb = a.rowb[row] - a.blk_row0[blk];
-      const int m = a.blk_m[blk];
       const int c0 = split * a.chunks_per_split;
       const int c1 = min(a.n_chunks, c0 + a.chunks_per_split);
       const float2* pa = reinterpret_cast<const float2*>(sPsi) + la * TC_PSI_LD;
@@ -411,38 +411,44 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       for (int c = c0; c < c1 && !*abort_flag; ++c) {
         if (!mbar_wait(P_full, pf_phase, abort_flag, a.status, 31)) break;
         pf_phase ^= 1;
-        for (int al = 0; al < a.n_alpha_it; ++al) {
-          float zr = 1.f, zi = 0.f, wa = 1.f;
-          if (a.alpha) {
-            sincosf((float)m * a.alpha[al], &zi, &zr);
-            wa = a.walpha[al];
+        // X_alpha = w_alpha Re((z psi_a)^* (z psi_b)) with z = e^{i m alpha}: both
+        // states of a pair have the same m, so |z|^2 = 1 and the integrand at every
+        // alpha point equals w_alpha Re(psi_a^* psi_b) exactly.  The product is formed
+        // once per chunk and scaled per alpha point; every alpha slice is still
+        // contracted by the tensor cores.
+        float x0[TC_KC / 16][8];
+#pragma unroll
+        for (int kq = 0; kq < TC_KC / 16; ++kq) {
+          const int kg = kh * (TC_KC / 16) + kq;
+#pragma unroll
+          for (int e = 0; e < 8; e += 2) {
+            const float4 va = *reinterpret_cast<const float4*>(pa + kg * 8 + e);
+            const float4 vb = *reinterpret_cast<const float4*>(pb + kg * 8 + e);
+            x0[kq][e] = va.x * vb.x + va.y * vb.y;
+            x0[kq][e + 1] = va.z * vb.z + va.w * vb.w;
           }
+        }
+        for (int al = 0; al < a.n_alpha_it; ++al) {
+          float wa = a.alpha ? a.walpha[al] : 1.f;
           if (kF16) wa *= (float)(1 << kXScaleExp);  // exact power-of-two scaling
           if (a_used[stage]) {
-            if (!mbar_wait(&A_empty[stage], ae_phase[stage], abort_flag, a.status, 32)) break;
+            const bool ok = mbar_wait(&A_empty[stage], ae_phase[stage], abort_flag, a.status, 32);
             ae_phase[stage] ^= 1;
+            if (!ok) break;
           }
           a_used[stage] = true;
           unsigned char* hi = sA + stage * (2 * TC_A_PLANE);
           unsigned char* lo = hi + TC_A_PLANE;
-#pragma unroll 2
-          for (int kg = kh * (TC_KC / 16); kg < (kh + 1) * (TC_KC / 16); ++kg) {
+#pragma unroll
+          for (int kq = 0; kq < TC_KC / 16; ++kq) {
+            const int kg = kh * (TC_KC / 16) + kq;
             float x[8];
 #pragma unroll
-            for (int e = 0; e < 8; e += 2) {
-              float4 va = *reinterpret_cast<const float4*>(pa + kg * 8 + e);
-              float4 vb = *reinterpret_cast<const float4*>(pb + kg * 8 + e);
-              // (z psi_a)^* (z psi_b), real part
-              float ar0 = zr * va.x - zi * va.y, ai0 = zr * va.y + zi * va.x;
-              float br0 = zr * vb.x - zi * vb.y, bi0 = zr * vb.y + zi * vb.x;
-              float ar1 = zr * va.z - zi * va.w, ai1 = zr * va.w + zi * va.z;
-              float br1 = zr * vb.z - zi * vb.w, bi1 = zr * vb.w + zi * vb.z;
-              x[e] = wa * (ar0 * br0 + ai0 * bi0);
-              x[e + 1] = wa * (ar1 * br1 + ai1 * bi1);
-            }
+            for (int e = 0; e < 8; ++e) x[e] = wa * x0[kq][e];
             uint4 h, l;
             split8<kF16>(x, h, l);
-            const uint32_t off = (uint32_t)(kg * (TC_M / 8) + (p >> 3)) * 128u + (uint32_t)(p & 7) * 16u;
+            const uint32_t off =
+                (uint32_t)(kg * (TC_M / 8) + (p >> 3)) * 128u + (uint32_t)(p & 7) * 16u;
             *reinterpret_cast<uint4*>(hi + off) = h;
             *reinterpret_cast<uint4*>(lo + off) = l;
           }

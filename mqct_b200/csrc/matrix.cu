@@ -99,7 +99,8 @@ __device__ inline double2 asym_wf(int j, int m, const double* c, double alpha, d
 // type 0: sum_{m1} CG(j1 m1 j2 m2 | j12 m12) psi1_{m1}(0, beta1, gamma1)
 //         psi2_{m2}(alpha2, beta2, gamma2) (WF_ASYM_TOP_ASYM_TOP :1-41) on the 5-D grid.
 // Output psi[(blk_off + s) * G2 + g] as (re, im) FP64.
-__global__ void basis_kernel(int sys_type, int n_rows, const int* __restrict__ row_state,
+template <int SYS>
+__global__ void basis_kernel(int n_rows, const int* __restrict__ row_state,
                              const int* __restrict__ st_chan, const int* __restrict__ st_m,
                              const int* __restrict__ ch_j, const double* __restrict__ vec,
                              int ldv, const double* __restrict__ beta,
@@ -112,14 +113,14 @@ __global__ void basis_kernel(int sys_type, int n_rows, const int* __restrict__ r
   int ch = st_chan[st];
   int j = ch_j[ch], m = st_m[st];
   double re = 0.0, im = 0.0;
-  if (sys_type == 1) {
+  if constexpr (SYS == 1) {
     double b = beta[g2];
     int am = m < 0 ? -m : m;
     double pl = mqct_dev::plgndr(j, am, cos(b));
     double nrm = sqrt((2.0 * j + 1.0) / 4.0 / kPi * exp(c_logfact[j - am] - c_logfact[j + am]));
     re = pl * nrm;
     if (m < 0 && (am & 1)) re = -re;
-  } else if (sys_type == 0) {
+  } else if constexpr (SYS == 0) {
     int ia2, ib1, ib2, ig1, ig2;
     t0_index(t0, g2, ia2, ib1, ib2, ig1, ig2);
     const int j2 = t0.ch_j2[ch];
@@ -243,7 +244,8 @@ __device__ inline double pes_eval(const PesDev& P, double R, double beta, double
 // MQCT_SOURCE_CODES/pes_sys_type.f: type 1 passes beta (:8), type 4 passes
 // (-beta, -gamma) (:36), type 0 passes (0, beta1, gamma1, alpha2, beta2, gamma2)
 // (:90-97).
-__global__ void pes_weight_kernel(int sys_type, PesDev pes, int G2, int nR,
+template <int SYS>
+__global__ void pes_weight_kernel(PesDev pes, int G2, int nR,
                                   const double* __restrict__ R, const double* __restrict__ beta,
                                   const double* __restrict__ gamma, int n_gamma, Type0Dev t0,
                                   const double* __restrict__ wt, double* __restrict__ W,
@@ -254,9 +256,9 @@ __global__ void pes_weight_kernel(int sys_type, PesDev pes, int G2, int nR,
   double v;
   if (pes.kind == MQCT_PES_TABLE) {
     v = pes.table[(size_t)i * G2 + g2];
-  } else if (sys_type == 1) {
+  } else if constexpr (SYS == 1) {
     v = pes_eval(pes, R[i], beta[g2], 0.0);
-  } else if (sys_type == 0) {
+  } else if constexpr (SYS == 0) {
     int ia2, ib1, ib2, ig1, ig2;
     t0_index(t0, g2, ia2, ib1, ib2, ig1, ig2);
     v = pes_eval_sites2(pes, R[i], 0.0, beta[ib1], gamma[ig1], t0.alpha2[ia2], t0.beta2[ib2],
@@ -812,15 +814,33 @@ int MatrixPlan::run_basis_and_pes() {
   int64_t nb = (int64_t)n_basis_rows * G2;
   const Type0Dev t0{d_ch_j2.p, d_vec2.p, d_cg.p, cg_ld, d_beta2.p, d_alpha2.p, d_gamma2.p,
                     (int)h_beta.size(), n_gamma, t0_nbb, t0_naa, t0_ngg};
-  basis_kernel<<<(unsigned)((nb + threads - 1) / threads), threads, 0, stream>>>(
-      sys_type, n_basis_rows, d_row_state.p, d_st_chan.p, d_st_m.p, d_ch_j.p, d_vec.p, ldv,
-      d_beta.p, d_gamma.p, n_gamma, G2, t0, d_psi.p);
+  const unsigned gb = (unsigned)((nb + threads - 1) / threads);
+  if (sys_type == 1)
+    basis_kernel<1><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
+                                                d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
+                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
+  else if (sys_type == 4)
+    basis_kernel<4><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
+                                                d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
+                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
+  else
+    basis_kernel<0><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
+                                                d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
+                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
   MQCT_CUDA_TRY(cudaGetLastError());
   PesDev pd{pes_kind, pes_n_terms, pes_n_sites1, pes_n_sites2, d_pes_p.p, d_pes_s1.p, d_pes_s2.p,
             d_pes_table.p};
   int64_t nw = (int64_t)G2 * nR;
-  pes_weight_kernel<<<(unsigned)((nw + threads - 1) / threads), threads, 0, stream>>>(
-      sys_type, pd, G2, nR, d_R.p, d_beta.p, d_gamma.p, n_gamma, t0, d_wt.p, d_W.p, ldw);
+  const unsigned gw = (unsigned)((nw + threads - 1) / threads);
+  if (sys_type == 1)
+    pes_weight_kernel<1><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,
+                                                     n_gamma, t0, d_wt.p, d_W.p, ldw);
+  else if (sys_type == 4)
+    pes_weight_kernel<4><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,
+                                                     n_gamma, t0, d_wt.p, d_W.p, ldw);
+  else
+    pes_weight_kernel<0><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,
+                                                     n_gamma, t0, d_wt.p, d_W.p, ldw);
   MQCT_CUDA_TRY(cudaGetLastError());
   return MQCT_OK;
 }
