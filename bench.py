@@ -299,7 +299,10 @@ def run_gpu(a):
                 "ms": float(np.median(e2e_ms)), "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
-        "gpu_launches": int(a.steps * (7 if tc else 5)),
+        # per build: rotor tables, basis, PES weights, [W column scaling (F16x3)], W image,
+        # basis image, contraction, finalize; the FP64 form: tables, basis, PES, contraction,
+        # finalize
+        "gpu_launches": int(a.steps * ((8 if prec == mq.PREC_F16X3 else 7) if tc else 5)),
         "fp64_form": fp64,
         "accuracy": acc,
         "reference_2d_form": ref_form,

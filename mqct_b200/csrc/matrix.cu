@@ -99,13 +99,44 @@ __device__ inline double2 asym_wf(int j, int m, const double* c, double alpha, d
 // type 0: sum_{m1} CG(j1 m1 j2 m2 | j12 m12) psi1_{m1}(0, beta1, gamma1)
 //         psi2_{m2}(alpha2, beta2, gamma2) (WF_ASYM_TOP_ASYM_TOP :1-41) on the 5-D grid.
 // Output psi[(blk_off + s) * G2 + g] as (re, im) FP64.
+// Rotor tables of the type-4 basis: dtab[(T(j) + (K+j)(2j+1) + (m+j)) * n_beta + ib]
+// = sqrt((2j+1)/8pi^2) d^j_{Km}(beta_ib) with T(j) = sum_{j'<j} (2j'+1)^2, and
+// phase[(K + jmax) * n_gamma + ig] = e^{i K gamma_ig}.  Both depend on the grid
+// only; psi is then a short sum over K of products of table entries.
+__device__ __host__ inline int dtab_off(int j) { return j * (2 * j - 1) * (2 * j + 1) / 3; }
+
+__global__ void rotor_tables_kernel(int jmax, int n_beta, const double* __restrict__ beta,
+                                    int n_gamma, const double* __restrict__ gamma,
+                                    double* __restrict__ dtab, double2* __restrict__ phase) {
+  const int n_d = dtab_off(jmax + 1) * n_beta;
+  const int n_p = (2 * jmax + 1) * n_gamma;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < n_d) {
+    const int ib = idx % n_beta;
+    int q = idx / n_beta;
+    int j = 0;
+    while (dtab_off(j + 1) <= q) ++j;
+    q -= dtab_off(j);
+    const int K = q / (2 * j + 1) - j, m = q % (2 * j + 1) - j;
+    dtab[idx] = mqct_dev::wigner_d(j, K, m, beta[ib], c_logfact) *
+                sqrt((2.0 * j + 1.0) / 8.0 / (kPi * kPi));
+  } else if (idx < n_d + n_p) {
+    const int q = idx - n_d;
+    const int K = q / n_gamma - jmax, ig = q % n_gamma;
+    double s, c;
+    sincos(K * gamma[ig], &s, &c);
+    phase[q] = make_double2(c, s);
+  }
+}
+
 template <int SYS>
 __global__ void basis_kernel(int n_rows, const int* __restrict__ row_state,
                              const int* __restrict__ st_chan, const int* __restrict__ st_m,
                              const int* __restrict__ ch_j, const double* __restrict__ vec,
                              int ldv, const double* __restrict__ beta,
                              const double* __restrict__ gamma, int n_gamma, int G2, Type0Dev t0,
-                             double2* __restrict__ psi) {
+                             const double* __restrict__ dtab, const double2* __restrict__ phase,
+                             int jmax, double2* __restrict__ psi) {
   int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)n_rows * G2) return;
   int r = (int)(idx / G2), g2 = (int)(idx % G2);
@@ -137,18 +168,18 @@ __global__ void basis_kernel(int n_rows, const int* __restrict__ row_state,
       im += w * (p1.x * p2.y + p1.y * p2.x);
     }
   } else {
-    int ib = g2 / n_gamma, ig = g2 % n_gamma;
-    double b = beta[ib], g = gamma[ig];
-    double nrm = sqrt((2.0 * j + 1.0) / 8.0 / (kPi * kPi));
+    const int ib = g2 / n_gamma, ig = g2 % n_gamma;
     const double* c = vec + (size_t)ch * ldv;
+    const int n_beta = G2 / n_gamma;
+    const double* dj = dtab + (size_t)(dtab_off(j) + (m + j)) * n_beta + ib;
+    const double2* pk = phase + (size_t)(jmax - j) * n_gamma + ig;
     for (int i = 0; i <= 2 * j; ++i) {
-      int K = i - j;
-      if (c[i] == 0.0) continue;
-      double d = mqct_dev::wigner_d(j, K, m, b, c_logfact) * nrm;
-      double s, co;
-      sincos(K * g, &s, &co);
-      re += d * co * c[i];
-      im += d * s * c[i];
+      const double ci = c[i];
+      if (ci == 0.0) continue;
+      const double d = ci * dj[(size_t)i * (2 * j + 1) * n_beta];
+      const double2 e = pk[(size_t)i * n_gamma];
+      re += d * e.x;
+      im += d * e.y;
     }
   }
   psi[idx] = make_double2(re, im);
@@ -704,6 +735,12 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
     st_m[s] = sys->m12[s];
   }
   for (int c = 0; c < sys->n_channels; ++c) ch_j[c] = sys->j1[c];
+  jmax_basis = 0;
+  for (int c = 0; c < sys->n_channels; ++c) jmax_basis = std::max(jmax_basis, (int)sys->j1[c]);
+  if (sys_type == 4) {
+    MQCT_CUDA_TRY(d_dtab.alloc((size_t)dtab_off(jmax_basis + 1) * grid->n_beta));
+    MQCT_CUDA_TRY(d_phase.alloc((size_t)(2 * jmax_basis + 1) * n_gamma));
+  }
   MQCT_CUDA_TRY(d_row_state.upload(row_state, stream));
   MQCT_CUDA_TRY(d_st_chan.upload(st_chan, stream));
   MQCT_CUDA_TRY(d_st_m.upload(st_m, stream));
@@ -815,18 +852,27 @@ int MatrixPlan::run_basis_and_pes() {
   const Type0Dev t0{d_ch_j2.p, d_vec2.p, d_cg.p, cg_ld, d_beta2.p, d_alpha2.p, d_gamma2.p,
                     (int)h_beta.size(), n_gamma, t0_nbb, t0_naa, t0_ngg};
   const unsigned gb = (unsigned)((nb + threads - 1) / threads);
+  if (sys_type == 4) {
+    const int n_tab = dtab_off(jmax_basis + 1) * (int)h_beta.size() + (2 * jmax_basis + 1) * n_gamma;
+    rotor_tables_kernel<<<(unsigned)((n_tab + threads - 1) / threads), threads, 0, stream>>>(
+        jmax_basis, (int)h_beta.size(), d_beta.p, n_gamma, d_gamma.p, d_dtab.p, d_phase.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+  }
   if (sys_type == 1)
     basis_kernel<1><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
                                                 d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
-                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
+                                                d_gamma.p, n_gamma, G2, t0, d_dtab.p, d_phase.p,
+                                                jmax_basis, d_psi.p);
   else if (sys_type == 4)
     basis_kernel<4><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
                                                 d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
-                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
+                                                d_gamma.p, n_gamma, G2, t0, d_dtab.p, d_phase.p,
+                                                jmax_basis, d_psi.p);
   else
     basis_kernel<0><<<gb, threads, 0, stream>>>(n_basis_rows, d_row_state.p, d_st_chan.p,
                                                 d_st_m.p, d_ch_j.p, d_vec.p, ldv, d_beta.p,
-                                                d_gamma.p, n_gamma, G2, t0, d_psi.p);
+                                                d_gamma.p, n_gamma, G2, t0, d_dtab.p, d_phase.p,
+                                                jmax_basis, d_psi.p);
   MQCT_CUDA_TRY(cudaGetLastError());
   PesDev pd{pes_kind, pes_n_terms, pes_n_sites1, pes_n_sites2, d_pes_p.p, d_pes_s1.p, d_pes_s2.p,
             d_pes_table.p};

@@ -47,6 +47,10 @@ struct MatrixPlan {
   DevBuf<int> d_ch_j2;
   DevBuf<double> d_vec2, d_cg, d_beta2, d_alpha2, d_gamma2;
   int cg_ld = 1, t0_nbb = 1, t0_naa = 1, t0_ngg = 1;
+  // type 4: rotor d-function and gamma-phase tables (rebuilt by every execute)
+  DevBuf<double> d_dtab;
+  DevBuf<double2> d_phase;
+  int jmax_basis = 0;
 
   // work
   DevBuf<double2> d_psi;  // basis rows x G2, FP64
