@@ -401,8 +401,8 @@ contract_fp64_kernel(int n_rows, int G2, int nR, const int* __restrict__ row_a,
 //      to the end differences, u_0 = 0 and u_n = 0; the remaining recurrence
 //      u_i = t_i - s_i u_{i-1}, y2_i = f_i y2_{i+1} + u_i has grid-only s_i, f_i
 //      and data terms t_i = c_i (d_i - d_{i-1}), d_i = (y_{i+1} - y_i) / h_i,
-//      which all threads form in parallel; one thread runs the two first-order
-//      recurrences (one FMA per step).
+//      which all threads form in parallel; one warp evaluates the two first-order
+//      recurrences as scans of affine maps (segments per lane + shuffle scan).
 // Grid coefficients (5 x nR, see MatrixPlan::init): 1/h_i, c_i, s_i, f_i, and
 // in slot [4 nR] the factor of y2_{n-1} = -u_{n-2} / (2 (f_{n-2}/2 + 1)).
 template <class TP>
@@ -418,13 +418,37 @@ finalize_kernel(int64_t P, int nR, const int* __restrict__ k_to_row, const TP* _
   __shared__ double cut_vals[2];
   const int64_t k = blockIdx.x;
   const int row = k_to_row[k];
-  for (int i = threadIdx.x; i < nR; i += blockDim.x) {
-    double v = 0.0;
-    for (int p = 0; p < n_part; ++p) v += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
-    v *= col_scale ? scale * col_scale[i] : scale;
-    col[i] = v;
-    if (i == ir1) cut_vals[0] = v;
-    if (i == ir2) cut_vals[1] = v;
+  if (sizeof(TP) == 4 && (ldp & 3) == 0 && (part_stride & 3) == 0) {
+    // FP32 partials: 16-byte loads, four radial points per thread
+    const float4* src = reinterpret_cast<const float4*>(part) + (size_t)row * (ldp >> 2);
+    for (int i4 = threadIdx.x; 4 * i4 < nR; i4 += blockDim.x) {
+      double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+#pragma unroll 4
+      for (int p = 0; p < n_part; ++p) {
+        const float4 f = __ldg(src + (size_t)p * (part_stride >> 2) + i4);
+        v0 += (double)f.x;
+        v1 += (double)f.y;
+        v2 += (double)f.z;
+        v3 += (double)f.w;
+      }
+      const double vv[4] = {v0, v1, v2, v3};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int i = 4 * i4 + e;
+        if (i < nR) col[i] = vv[e] * (col_scale ? scale * col_scale[i] : scale);
+      }
+    }
+  } else {
+    for (int i = threadIdx.x; i < nR; i += blockDim.x) {
+      double v = 0.0;
+      for (int p = 0; p < n_part; ++p) v += (double)part[(size_t)p * part_stride + (size_t)row * ldp + i];
+      col[i] = v * (col_scale ? scale * col_scale[i] : scale);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cut_vals[0] = col[ir1];
+    cut_vals[1] = col[ir2];
   }
   __syncthreads();
   const bool drop = fmax(fabs(cut_vals[0]), fabs(cut_vals[1])) < cut;
@@ -447,19 +471,65 @@ finalize_kernel(int64_t P, int nR, const int* __restrict__ k_to_row, const TP* _
     t[i] = cfac[i] * (d1 - d0);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double u = 0.0;  // u_0
-    for (int i = 1; i < nR - 1; ++i) {
+  if (threadIdx.x < 32) {
+    // Both recurrences are compositions of affine maps x -> a x + b, evaluated by
+    // one warp: each lane composes the maps of a contiguous segment, a shuffle
+    // scan composes the segments, and each lane replays its segment from the
+    // value entering it.
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x;
+    const int m = nR - 2;               // interior points 1 .. nR-2
+    const int L = (m + 31) / 32;
+    auto scan = [&](double& al, double& be) {  // exclusive prefix over lanes
+      for (int o = 1; o < 32; o <<= 1) {
+        const double pa = __shfl_up_sync(full, al, o), pb = __shfl_up_sync(full, be, o);
+        if (lane >= o) {
+          be = al * pb + be;
+          al = al * pa;
+        }
+      }
+      const double pa = __shfl_up_sync(full, al, 1), pb = __shfl_up_sync(full, be, 1);
+      al = lane ? pa : 1.0;
+      be = lane ? pb : 0.0;
+    };
+    // forward: u_i = t_i - s_i u_{i-1}, u_0 = 0
+    const int i0 = 1 + lane * L, i1 = min(1 + (lane + 1) * L, nR - 1);
+    double al = 1.0, be = 0.0;
+    for (int i = i0; i < i1; ++i) {
+      const double a = -sfac[i];
+      be = fma(a, be, t[i]);
+      al *= a;
+    }
+    scan(al, be);
+    double u = be;  // the prefix applied to u_0 = 0
+    for (int i = i0; i < i1; ++i) {
       u = fma(-sfac[i], u, t[i]);
       t[i] = u;
     }
-    double yv = gc[4 * nR] * u;  // y2_{n-1}
-    col[nR - 1] = yv;
-    for (int i = nR - 2; i >= 1; --i) {
+    __syncwarp();
+    const double ylast = gc[4 * nR] * t[nR - 2];  // y2_{n-1}
+    // backward: y2_i = f_i y2_{i+1} + u_i for i = n-2 .. 1 (k = n-2-i ascending)
+    const int k0 = lane * L, k1 = min((lane + 1) * L, m);
+    al = 1.0;
+    be = 0.0;
+    for (int k = k0; k < k1; ++k) {
+      const int i = nR - 2 - k;
+      const double f = ffac[i];
+      be = fma(f, be, t[i]);
+      al *= f;
+    }
+    scan(al, be);
+    double yv = fma(al, ylast, be);
+    for (int k = k0; k < k1; ++k) {
+      const int i = nR - 2 - k;
       yv = fma(ffac[i], yv, t[i]);
       col[i] = yv;
     }
-    col[0] = ffac[0] * yv;  // u_0 = 0
+    __syncwarp();
+    if (lane == 0) {
+      col[nR - 1] = ylast;
+      col[0] = ffac[0] * col[1];  // u_0 = 0
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nR; i += blockDim.x) oy[i] = col[i];
