@@ -251,29 +251,67 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     for (int p = 0; p < d.n_pass; ++p) {
       const int s0 = (int)d.pass_slot0[p], s1 = (int)d.pass_slot0[p + 1];
       // phase A: interpolate the pass's slots into Mp, force term
-      for (int kb = s0 + tid; kb < s1; kb += UNROLL * PT) {
-        T2 lo[UNROLL], hi[UNROLL];
-        uint32_t l[UNROLL];
+      if constexpr (sizeof(T) == 4) {
+        // two adjacent slots per load (16-byte knot loads, 8-byte location loads)
+        for (int kb = s0 + 2 * tid; kb < s1; kb += 2 * UNROLL * PT) {
+          float4 lo[UNROLL], hi[UNROLL];
+          uint2 l[UNROLL];
 #pragma unroll
-        for (int q = 0; q < UNROLL; ++q) {
-          const int k = kb + q * PT;
-          if (k < s1) {
-            lo[q] = ldg2(K0 + k);
-            hi[q] = ldg2(K1 + k);
-            l[q] = __ldg(d.loc + k);
+          for (int q = 0; q < UNROLL; ++q) {
+            const int k = kb + 2 * q * PT;
+            if (k < s1) {
+              lo[q] = __ldg(reinterpret_cast<const float4*>(K0 + k));
+              hi[q] = __ldg(reinterpret_cast<const float4*>(K1 + k));
+              l[q] = __ldg(reinterpret_cast<const uint2*>(d.loc + k));
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < UNROLL; ++q) {
+            const int k = kb + 2 * q * PT;
+            if (k < s1) {
+              const float m0 = aa * lo[q].x + bb * hi[q].x + c1 * lo[q].y + c2 * hi[q].y;
+              const float md0 = (hi[q].x - lo[q].x) * hinv + d1 * lo[q].y + d2 * hi[q].y;
+              const float m1 = aa * lo[q].z + bb * hi[q].z + c1 * lo[q].w + c2 * hi[q].w;
+              const float md1 = (hi[q].z - lo[q].z) * hinv + d1 * lo[q].w + d2 * hi[q].w;
+              *reinterpret_cast<float2*>(sm.Mp + (k - s0)) = make_float2(m0, m1);
+              {
+                const int ia = (int)(l[q].x & 0xffffu), ib = (int)(l[q].x >> 16);
+                const T2 x = sm.bt[ia], z = sm.bt[ib];
+                force += (ia == ib ? md0 : 2.f * md0) * (x.x * z.x + x.y * z.y);
+              }
+              {
+                const int ia = (int)(l[q].y & 0xffffu), ib = (int)(l[q].y >> 16);
+                const T2 x = sm.bt[ia], z = sm.bt[ib];
+                force += (ia == ib ? md1 : 2.f * md1) * (x.x * z.x + x.y * z.y);
+              }
+            }
           }
         }
+      } else {
+        for (int kb = s0 + tid; kb < s1; kb += UNROLL * PT) {
+          T2 lo[UNROLL], hi[UNROLL];
+          uint32_t l[UNROLL];
 #pragma unroll
-        for (int q = 0; q < UNROLL; ++q) {
-          const int k = kb + q * PT;
-          if (k < s1) {
-            const T m = aa * lo[q].x + bb * hi[q].x + c1 * lo[q].y + c2 * hi[q].y;
-            const T md = (hi[q].x - lo[q].x) * hinv + d1 * lo[q].y + d2 * hi[q].y;
-            sm.Mp[k - s0] = m;
-            const int ia = (int)(l[q] & 0xffffu), ib = (int)(l[q] >> 16);
-            const T2 x = sm.bt[ia], z = sm.bt[ib];
-            const T re = x.x * z.x + x.y * z.y;
-            force += (ia == ib ? md : (T)2 * md) * re;
+          for (int q = 0; q < UNROLL; ++q) {
+            const int k = kb + q * PT;
+            if (k < s1) {
+              lo[q] = ldg2(K0 + k);
+              hi[q] = ldg2(K1 + k);
+              l[q] = __ldg(d.loc + k);
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < UNROLL; ++q) {
+            const int k = kb + q * PT;
+            if (k < s1) {
+              const T m = aa * lo[q].x + bb * hi[q].x + c1 * lo[q].y + c2 * hi[q].y;
+              const T md = (hi[q].x - lo[q].x) * hinv + d1 * lo[q].y + d2 * hi[q].y;
+              sm.Mp[k - s0] = m;
+              const int ia = (int)(l[q] & 0xffffu), ib = (int)(l[q] >> 16);
+              const T2 x = sm.bt[ia], z = sm.bt[ib];
+              const T re = x.x * z.x + x.y * z.y;
+              force += (ia == ib ? md : (T)2 * md) * re;
+            }
           }
         }
       }
