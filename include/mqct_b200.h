@@ -169,6 +169,45 @@ double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
 int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3);
 void mqct_matrix_plan_destroy(mqct_matrix_plan* plan);
 
+/* Learned surrogate of an analytic PES (no counterpart in the reference, which
+ * evaluates its PES plugin at every grid point): a multilayer perceptron
+ * V(R, angles) with n_hidden_layers SiLU layers of `hidden` units on the
+ * features (R - c)/s and cos, sin of (beta1, gamma1, alpha2, beta2, gamma2),
+ * trained on the GPU (FP32, Adam, cosine-decayed learning rate) on n_samples
+ * seeded points of the PES with R uniform in [r_min, r_max] and the angles
+ * uniform on the grid's domain.  sys_type selects the angles used and the PES
+ * argument mapping (1: LEGENDRE or SITES1; 4: SITES1 or LEGENDRE; 0: SITES2).
+ * A surrogate is not re-entrant: one call at a time. */
+typedef struct mqct_surrogate mqct_surrogate;
+int mqct_surrogate_create(int32_t sys_type, const mqct_pes_t* pes, int32_t hidden,
+                          int32_t n_hidden_layers, uint64_t seed, double r_min, double r_max,
+                          mqct_surrogate** out);
+/* loss_per_epoch: epochs entries (MSE of the last batch, target units) or NULL;
+ * val_rmse: RMSE on a held-out seeded set (target units) or NULL. */
+int mqct_surrogate_train(mqct_surrogate* sur, int64_t n_samples, int32_t epochs, int32_t batch,
+                         double lr, double* loss_per_epoch, double* val_rmse);
+/* V (cm^-1) at n points args[6 i + (0..5)] = (R, beta1, gamma1, alpha2, beta2, gamma2). */
+int mqct_surrogate_predict(mqct_surrogate* sur, const double* args, int64_t n, double* v_out);
+int64_t mqct_surrogate_n_params(const mqct_surrogate* sur);
+/* Parameters, flat: per layer W (in x out, row-major) then b (out). */
+int mqct_surrogate_get_params(mqct_surrogate* sur, float* out);
+/* Mean squared error of the network on n feature rows X (n x 11) against targets
+ * y, and its gradient with respect to the flat parameters (the training step's
+ * backward pass). */
+int mqct_surrogate_loss_grad(mqct_surrogate* sur, const float* X, const float* y, int32_t n,
+                             double* loss, float* grad_out);
+void mqct_surrogate_destroy(mqct_surrogate* sur);
+/* Use a trained surrogate for the PES table of a plan's builds.  Every execute
+ * evaluates the network on the whole (grid x R) table, evaluates the exact PES on
+ * n_check grid points per radial point, and re-evaluates the whole grid exactly at
+ * every radial point where some checked |V_net - V| exceeds rel_bound |V| +
+ * abs_bound_cm.  The surrogate must outlive the plan's executes; NULL detaches. */
+int mqct_matrix_plan_set_surrogate(mqct_matrix_plan* plan, mqct_surrogate* sur, double rel_bound,
+                                   double abs_bound_cm, int32_t n_check);
+/* After an execute: radial points re-evaluated exactly, and the largest checked
+ * |V_net - V| / (rel_bound |V| + abs_bound_cm). */
+int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t* n_exact_r, double* max_ratio);
+
 /* Spline fit of device-resident matrix columns without any device allocation
  * (this entry point has no counterpart in the reference, which fits its splines
  * on the host).  d_R: nR grid points, d_mat: P x nR values (column k at

@@ -25,7 +25,7 @@ from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
            "PropagationPlan", "trajectory_set", "cross_sections", "write_mtrx_uf",
-           "read_mtrx_uf", "spline_y2", "MqctError", "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32",
+           "read_mtrx_uf", "spline_y2", "Surrogate", "MqctError", "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32",
            "PROP_FP64", "MODE_STD", "MODE_AT"]
 
 
@@ -136,6 +136,62 @@ class CollisionSystem:
         return np.ascontiguousarray(np.stack(cols, axis=1).astype(np.int32))
 
 
+class Surrogate:
+    """Learned PES surrogate (MLP on (R, cos/sin of the angles)) trained on the GPU
+    by the library's own kernels; see mqct_surrogate_* in include/mqct_b200.h."""
+
+    N_FEATURES = 11
+
+    def __init__(self, sys_type, pes, hidden=256, layers=4, seed=1, r_min=4.0, r_max=25.0):
+        self._pes = PesSpec.from_dict(pes) if isinstance(pes, dict) else pes
+        self._ps = self._pes.c_struct()
+        h = C.c_void_p()
+        check(lib().mqct_surrogate_create(int(sys_type), C.byref(self._ps), hidden, layers,
+                                          seed, r_min, r_max, C.byref(h)))
+        self.h = h
+        self.sys_type = int(sys_type)
+
+    def train(self, n_samples=2_000_000, epochs=10, batch=4096, lr=1e-3):
+        """Returns (last-batch loss per epoch, held-out RMSE), target units."""
+        loss = np.zeros(epochs)
+        val = C.c_double()
+        check(lib().mqct_surrogate_train(self.h, n_samples, epochs, batch, lr, ptr(loss),
+                                         C.byref(val)))
+        return loss, float(val.value)
+
+    def predict(self, args):
+        """V (cm^-1) at rows (R, beta1, gamma1, alpha2, beta2, gamma2)."""
+        a = np.ascontiguousarray(args, dtype=np.float64).reshape(-1, 6)
+        out = np.zeros(len(a))
+        check(lib().mqct_surrogate_predict(self.h, ptr(a), len(a), ptr(out)))
+        return out
+
+    def params(self):
+        n = lib().mqct_surrogate_n_params(self.h)
+        out = np.zeros(n, np.float32)
+        check(lib().mqct_surrogate_get_params(self.h, ptr(out)))
+        return out
+
+    def loss_grad(self, X, y):
+        X = np.ascontiguousarray(X, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(lib().mqct_surrogate_n_params(self.h), np.float32)
+        loss = C.c_double()
+        check(lib().mqct_surrogate_loss_grad(self.h, ptr(X), ptr(y), len(y), C.byref(loss), ptr(g)))
+        return float(loss.value), g
+
+    def close(self):
+        if self.h:
+            lib().mqct_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def r_grid(n, rmin, rmax, equidistant=True):
     R = np.zeros(n)
     check(lib().mqct_r_grid(n, rmin, rmax, 1 if equidistant else 0, R))
@@ -215,6 +271,20 @@ class MatrixPlan:
 
     def sync(self):
         check(lib().mqct_matrix_plan_sync(self.h))
+
+    def set_surrogate(self, sur, rel_bound=1e-2, abs_bound_cm=0.5, n_check=64):
+        """Evaluate the PES table with a trained Surrogate (None detaches)."""
+        check(lib().mqct_matrix_plan_set_surrogate(self.h, None if sur is None else sur.h,
+                                                   rel_bound, abs_bound_cm, n_check))
+        self._sur = sur
+
+    def surrogate_stats(self):
+        """(radial points re-evaluated exactly, largest checked residual ratio) of the
+        last execute."""
+        n = C.c_int32()
+        r = C.c_double()
+        check(lib().mqct_matrix_plan_surrogate_stats(self.h, C.byref(n), C.byref(r)))
+        return int(n.value), float(r.value)
 
     def timing(self):
         """(basis+PES, contraction, finalize) milliseconds of the last execute."""

@@ -80,6 +80,9 @@ EXPORTS = [
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_propagate_batch",
+    "mqct_surrogate_create", "mqct_surrogate_train", "mqct_surrogate_predict",
+    "mqct_surrogate_n_params", "mqct_surrogate_get_params", "mqct_surrogate_loss_grad",
+    "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
     "mqct_prop_plan_create", "mqct_prop_plan_run", "mqct_prop_plan_run_device",
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
     "mqct_prop_plan_destroy",
@@ -117,6 +120,18 @@ def lib():
     L.mqct_prop_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
     L.mqct_matrix_plan_destroy.argtypes = [vp]
     L.mqct_spline_y2_noalloc.argtypes = [vp, C.c_int32, vp, vp, C.c_int64, vp, vp]
+    L.mqct_surrogate_create.argtypes = [C.c_int32, C.POINTER(Pes), C.c_int32, C.c_int32,
+                                        C.c_uint64, C.c_double, C.c_double, C.POINTER(vp)]
+    L.mqct_surrogate_train.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_double, vp, vp]
+    L.mqct_surrogate_predict.argtypes = [vp, vp, C.c_int64, vp]
+    L.mqct_surrogate_n_params.argtypes = [vp]
+    L.mqct_surrogate_n_params.restype = C.c_int64
+    L.mqct_surrogate_get_params.argtypes = [vp, vp]
+    L.mqct_surrogate_loss_grad.argtypes = [vp, vp, vp, C.c_int32, vp, vp]
+    L.mqct_surrogate_destroy.argtypes = [vp]
+    L.mqct_surrogate_destroy.restype = None
+    L.mqct_matrix_plan_set_surrogate.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int32]
+    L.mqct_matrix_plan_surrogate_stats.argtypes = [vp, vp, vp]
     L.mqct_matrix_plan_destroy.restype = None
     L.mqct_propagate_batch.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
                                        C.c_int32, C.POINTER(AtPaths), C.c_int32, f64p, f64p,

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "matrix_plan.cuh"
+#include "pes.cuh"
 
 using namespace mqct;
 
@@ -186,91 +187,6 @@ __global__ void basis_kernel(int n_rows, const int* __restrict__ row_state,
 }
 
 // ------------------------------------------------------------------ K2: PES x weights
-struct PesDev {
-  int kind, n_terms, n_sites1, n_sites2;
-  const double* p;
-  const double* s1;
-  const double* s2;
-  const double* table;
-};
-
-__device__ inline double site_term(double r, const double* t) {
-  double D = t[0], a = t[1], re = t[2], c6 = t[3], rd = t[4];
-  double e = exp(-a * (r - re));
-  double r2 = r * r, r6 = r2 * r2 * r2;
-  double x = r / rd, x2 = x * x, x6 = x2 * x2 * x2;
-  return D * (e * e - 2.0 * e) - c6 * (1.0 - exp(-x6)) / r6;
-}
-
-// Rotation Rz(a) Ry(b) Rz(g) applied to a site position.
-__device__ inline void euler_apply(double a, double b, double g, const double* s, double* x) {
-  double ca, sa, cb, sb, cg, sg;
-  sincos(a, &sa, &ca);
-  sincos(b, &sb, &cb);
-  sincos(g, &sg, &cg);
-  const double m00 = ca * cb * cg - sa * sg, m01 = -ca * cb * sg - sa * cg, m02 = ca * sb;
-  const double m10 = sa * cb * cg + ca * sg, m11 = -sa * cb * sg + ca * cg, m12 = sa * sb;
-  const double m20 = -sb * cg, m21 = sb * sg, m22 = cb;
-  x[0] = m00 * s[0] + m01 * s[1] + m02 * s[2];
-  x[1] = m10 * s[0] + m11 * s[1] + m12 * s[2];
-  x[2] = m20 * s[0] + m21 * s[1] + m22 * s[2];
-}
-
-// SITES2 family for two rigid rotors: rotor 1 at the origin with Euler angles
-// (alpha, beta, gamma), rotor 2 at R z with (aalpha, bbeta, ggamma); per term
-// [site1, site2, D, a, re, C6, rd].
-__device__ inline double pes_eval_sites2(const PesDev& P, double R, double alpha, double beta,
-                                         double gamma, double aalpha, double bbeta, double ggamma) {
-  double v = 0.0;
-  for (int t = 0; t < P.n_terms; ++t) {
-    const double* q = P.p + 7 * t;
-    double x1[3], x2[3];
-    euler_apply(alpha, beta, gamma, P.s1 + 3 * (int)q[0], x1);
-    euler_apply(aalpha, bbeta, ggamma, P.s2 + 3 * (int)q[1], x2);
-    x2[2] += R;
-    const double dx = x2[0] - x1[0], dy = x2[1] - x1[1], dz = x2[2] - x1[2];
-    v += site_term(sqrt(dx * dx + dy * dy + dz * dz), q + 2);
-  }
-  return v;
-}
-
-// USER_DEFINED_PES(V,R,..,alpha,beta,gamma,..) for the built-in families.
-__device__ inline double pes_eval(const PesDev& P, double R, double beta, double gamma) {
-  if (P.kind == MQCT_PES_LEGENDRE) {
-    double x = cos(beta), v = 0.0;
-    double r2 = R * R, r6 = r2 * r2 * r2;
-    int n = P.n_terms;
-    // P_l(x) by Bonnet's recurrence
-    double pm = 1.0, pc = x;
-    for (int l = 0; l < n; ++l) {
-      double pl;
-      if (l == 0) pl = 1.0;
-      else if (l == 1) pl = x;
-      else {
-        pl = ((2.0 * l - 1.0) * x * pc - (l - 1.0) * pm) / l;
-        pm = pc;
-        pc = pl;
-      }
-      v += (P.p[l] * exp(-P.p[n + l] * R) - P.p[2 * n + l] / r6) * pl;
-    }
-    return v;
-  }
-  if (P.kind == MQCT_PES_SITES1) {
-    double sb, cb, sg, cg;
-    sincos(beta, &sb, &cb);
-    sincos(gamma, &sg, &cg);
-    double ax = R * sb * cg, ay = R * sb * sg, az = R * cb, v = 0.0;
-    for (int t = 0; t < P.n_terms; ++t) {
-      const double* q = P.p + 6 * t;
-      const double* s = P.s1 + 3 * (int)q[0];
-      double dx = ax - s[0], dy = ay - s[1], dz = az - s[2];
-      v += site_term(sqrt(dx * dx + dy * dy + dz * dz), q + 1);
-    }
-    return v;
-  }
-  return nan("");
-}
-
 // W[g2 * ldw + i] = wt[g2] * V(R_i, angles(g2)) with the argument mapping of
 // MQCT_SOURCE_CODES/pes_sys_type.f: type 1 passes beta (:8), type 4 passes
 // (-beta, -gamma) (:36), type 0 passes (0, beta1, gamma1, alpha2, beta2, gamma2)
@@ -297,6 +213,90 @@ __global__ void pes_weight_kernel(PesDev pes, int G2, int nR,
   } else {
     int ib = g2 / n_gamma, ig = g2 % n_gamma;
     v = pes_eval(pes, R[i], -beta[ib], -gamma[ig]);
+  }
+  W[(size_t)g2 * ldw + i] = wt[g2] * v;
+}
+
+// ------------------------------------------------------------------ K2': learned PES
+// Grid angles (beta1, gamma1, alpha2, beta2, gamma2) of grid point g2 (unused 0).
+template <int SYS>
+__device__ inline void grid_angles(int g2, const double* beta, const double* gamma, int n_gamma,
+                                   const Type0Dev& t0, double* ang) {
+  ang[0] = ang[1] = ang[2] = ang[3] = ang[4] = 0.0;
+  if constexpr (SYS == 1) {
+    ang[0] = beta[g2];
+  } else if constexpr (SYS == 4) {
+    ang[0] = beta[g2 / n_gamma];
+    ang[1] = gamma[g2 % n_gamma];
+  } else {
+    int ia2, ib1, ib2, ig1, ig2;
+    t0_index(t0, g2, ia2, ib1, ib2, ig1, ig2);
+    ang[0] = beta[ib1];
+    ang[1] = gamma[ig1];
+    ang[2] = t0.alpha2[ia2];
+    ang[3] = t0.beta2[ib2];
+    ang[4] = t0.gamma2[ig2];
+  }
+}
+
+// Surrogate features of every (grid point, R) of the W table, row g2 * nR + i.
+template <int SYS>
+__global__ void sur_features_kernel(int G2, int nR, const double* __restrict__ R,
+                                    const double* __restrict__ beta, const double* __restrict__ gamma,
+                                    int n_gamma, Type0Dev t0, double r_c, double r_s,
+                                    float* __restrict__ X) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)G2 * nR) return;
+  const int g2 = (int)(idx / nR), i = (int)(idx % nR);
+  double ang[5];
+  grid_angles<SYS>(g2, beta, gamma, n_gamma, t0, ang);
+  float* f = X + (size_t)idx * 11;
+  f[0] = (float)((R[i] - r_c) / r_s);
+  for (int a = 0; a < 5; ++a) {
+    double sn, cs;
+    sincos(ang[a], &sn, &cs);
+    f[1 + 2 * a] = (float)cs;
+    f[2 + 2 * a] = (float)sn;
+  }
+}
+
+// Residual check: n_check grid points per radial point, evaluated exactly;
+// ratio[i] = max |V_net - V| / (rel |V| + abs) (non-negative floats compare as
+// their bit patterns).
+template <int SYS>
+__global__ void sur_check_kernel(PesDev pes, int G2, int nR, const double* __restrict__ R,
+                                 const double* __restrict__ beta, const double* __restrict__ gamma,
+                                 int n_gamma, Type0Dev t0, const double* __restrict__ vnet,
+                                 int n_check, double rel, double abs_cm,
+                                 unsigned* __restrict__ ratio_bits) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_check * nR) return;
+  const int c = idx / nR, i = idx % nR;
+  const int g2 = (int)(((int64_t)c * G2 + G2 / 2) / n_check) % G2;
+  double ang[5];
+  grid_angles<SYS>(g2, beta, gamma, n_gamma, t0, ang);
+  const double v = pes_at(SYS, pes, R[i], ang);
+  const double r = fabs(vnet[(size_t)g2 * nR + i] - v) / (rel * fabs(v) + abs_cm);
+  atomicMax(ratio_bits + i, __float_as_uint((float)fmin(r, 3.0e38)));
+}
+
+// W from the network, or from the exact PES at the radial points that failed the check.
+template <int SYS>
+__global__ void sur_weight_kernel(PesDev pes, int G2, int nR, const double* __restrict__ R,
+                                  const double* __restrict__ beta, const double* __restrict__ gamma,
+                                  int n_gamma, Type0Dev t0, const double* __restrict__ vnet,
+                                  const unsigned* __restrict__ ratio_bits,
+                                  const double* __restrict__ wt, double* __restrict__ W, int ldw) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)G2 * nR) return;
+  const int g2 = (int)(idx / nR), i = (int)(idx % nR);
+  double v;
+  if (__uint_as_float(ratio_bits[i]) > 1.0f) {
+    double ang[5];
+    grid_angles<SYS>(g2, beta, gamma, n_gamma, t0, ang);
+    v = pes_at(SYS, pes, R[i], ang);
+  } else {
+    v = vnet[idx];
   }
   W[(size_t)g2 * ldw + i] = wt[g2] * v;
 }
@@ -948,6 +948,7 @@ int MatrixPlan::run_basis_and_pes() {
             d_pes_table.p};
   int64_t nw = (int64_t)G2 * nR;
   const unsigned gw = (unsigned)((nw + threads - 1) / threads);
+  if (sur) return run_surrogate_pes(pd, t0);
   if (sys_type == 1)
     pes_weight_kernel<1><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,
                                                      n_gamma, t0, d_wt.p, d_W.p, ldw);
@@ -958,6 +959,42 @@ int MatrixPlan::run_basis_and_pes() {
     pes_weight_kernel<0><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,
                                                      n_gamma, t0, d_wt.p, d_W.p, ldw);
   MQCT_CUDA_TRY(cudaGetLastError());
+  return MQCT_OK;
+}
+
+int MatrixPlan::run_surrogate_pes(const PesDev& pd, const Type0Dev& t0) {
+  const int threads = 256;
+  const int64_t nw = (int64_t)G2 * nR;
+  const unsigned gw = (unsigned)((nw + threads - 1) / threads);
+  const unsigned gc = (unsigned)(((int64_t)sur_check * nR + threads - 1) / threads);
+  int st = 0;
+  double r_c = 0.0, r_s = 1.0;
+  surrogate_feature_map(sur, &st, &r_c, &r_s);
+  MQCT_CUDA_TRY(cudaMemsetAsync(d_sur_ratio.p, 0, sizeof(unsigned) * nR, stream));
+#define MQCT_SUR_LAUNCH(SYS)                                                                     \
+  sur_features_kernel<SYS><<<gw, threads, 0, stream>>>(G2, nR, d_R.p, d_beta.p, d_gamma.p,     \
+                                                       n_gamma, t0, r_c, r_s, d_sur_x.p);      \
+  MQCT_CUDA_TRY(cudaGetLastError());                                                            \
+  {                                                                                             \
+    const int rc_ = surrogate_predict_on(sur, d_sur_x.p, nw, d_sur_v.p, stream);               \
+    if (rc_) return rc_;                                                                        \
+  }                                                                                             \
+  sur_check_kernel<SYS><<<gc, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,     \
+                                                    n_gamma, t0, d_sur_v.p, sur_check, sur_rel, \
+                                                    sur_abs, d_sur_ratio.p);                    \
+  MQCT_CUDA_TRY(cudaGetLastError());                                                            \
+  sur_weight_kernel<SYS><<<gw, threads, 0, stream>>>(pd, G2, nR, d_R.p, d_beta.p, d_gamma.p,    \
+                                                     n_gamma, t0, d_sur_v.p, d_sur_ratio.p,     \
+                                                     d_wt.p, d_W.p, ldw);                       \
+  MQCT_CUDA_TRY(cudaGetLastError());
+  if (sys_type == 1) {
+    MQCT_SUR_LAUNCH(1)
+  } else if (sys_type == 4) {
+    MQCT_SUR_LAUNCH(4)
+  } else {
+    MQCT_SUR_LAUNCH(0)
+  }
+#undef MQCT_SUR_LAUNCH
   return MQCT_OK;
 }
 
@@ -1173,5 +1210,57 @@ extern "C" int mqct_spline_y2_noalloc(const double* d_R, int32_t nR, const doubl
   spline_kernel<<<(unsigned)((P + SPL_EL - 1) / SPL_EL), 128, smem, s>>>(P, nR, d_R, coef, d_mat,
                                                                         d_skipped, d_y2);
   MQCT_CUDA_TRY(cudaGetLastError());
+  return MQCT_OK;
+}
+
+extern "C" int mqct_matrix_plan_set_surrogate(mqct_matrix_plan* plan, mqct_surrogate* sur,
+                                              double rel_bound, double abs_bound_cm,
+                                              int32_t n_check) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  if (!sur) {
+    p->sur = nullptr;
+    return MQCT_OK;
+  }
+  MQCT_ARG_CHECK(rel_bound >= 0.0 && abs_bound_cm > 0.0 && n_check >= 1,
+                 "bad surrogate residual bound or check count");
+  MQCT_ARG_CHECK(p->pes_kind != MQCT_PES_TABLE, "a surrogate needs an analytic PES to check against");
+  int st = -1;
+  double rc = 0.0, rs = 0.0;
+  surrogate_feature_map(sur, &st, &rc, &rs);
+  MQCT_ARG_CHECK(st == p->sys_type, "surrogate of SYS_TYPE %d for a SYS_TYPE %d plan", st,
+                 p->sys_type);
+  const int64_t nw = (int64_t)p->G2 * p->nR;
+  MQCT_ARG_CHECK(nw <= ((int64_t)1 << 28), "PES table of %lld points too large for the surrogate path",
+                 (long long)nw);
+  MQCT_CUDA_TRY(p->d_sur_x.alloc((size_t)nw * 11));
+  MQCT_CUDA_TRY(p->d_sur_v.alloc((size_t)nw));
+  MQCT_CUDA_TRY(p->d_sur_ratio.alloc((size_t)p->nR));
+  p->sur = sur;
+  p->sur_rel = rel_bound;
+  p->sur_abs = abs_bound_cm;
+  p->sur_check = std::min<int>(n_check, p->G2);
+  return MQCT_OK;
+}
+
+extern "C" int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t* n_exact_r,
+                                                double* max_ratio) {
+  MQCT_ARG_CHECK(plan && n_exact_r && max_ratio, "null argument");
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  MQCT_ARG_CHECK(p->sur, "plan has no surrogate");
+  std::vector<unsigned> bits(p->nR);
+  MQCT_CUDA_TRY(cudaMemcpyAsync(bits.data(), p->d_sur_ratio.p, sizeof(unsigned) * p->nR,
+                                cudaMemcpyDeviceToHost, p->stream));
+  MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  int n = 0;
+  double mx = 0.0;
+  for (unsigned b : bits) {
+    float f;
+    std::memcpy(&f, &b, sizeof f);
+    if (f > 1.0f) ++n;
+    mx = std::max(mx, (double)f);
+  }
+  *n_exact_r = n;
+  *max_ratio = mx;
   return MQCT_OK;
 }

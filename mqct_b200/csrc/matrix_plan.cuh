@@ -8,6 +8,10 @@
 
 namespace mqct {
 
+// Surrogate bridge (surrogate.cu).
+int surrogate_predict_on(void* sur, const float* X, int64_t n, double* v_out, cudaStream_t st);
+void surrogate_feature_map(const void* sur, int* sys_type, double* r_c, double* r_s);
+
 // Per-plan state of the tcgen05 path (contract_tc.cu).
 struct TcInfo {
   int n_chunks = 0, chunks_per_split = 1, npad = 0, n0 = 0, n1 = 0, nbmax = 0, stages = 3;
@@ -51,6 +55,13 @@ struct MatrixPlan {
   DevBuf<double> d_dtab;
   DevBuf<double2> d_phase;
   int jmax_basis = 0;
+  // learned PES (surrogate.cu): features, network values, per-R residual ratios
+  void* sur = nullptr;
+  double sur_rel = 0.0, sur_abs = 1.0;
+  int sur_check = 1;
+  DevBuf<float> d_sur_x;
+  DevBuf<double> d_sur_v;
+  DevBuf<unsigned> d_sur_ratio;
 
   // work
   DevBuf<double2> d_psi;  // basis rows x G2, FP64
@@ -76,6 +87,7 @@ struct MatrixPlan {
            const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec, double mij_cut,
            double rc1, double rc2);
   int run_basis_and_pes();
+  int run_surrogate_pes(const struct PesDev& pd, const struct Type0Dev& t0);
   int execute(double* d_mat, double* d_y2, int32_t* d_skipped);
   double flops() const;
   ~MatrixPlan();
