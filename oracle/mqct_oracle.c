@@ -1287,3 +1287,76 @@ int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int 
   }
   return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* SRC/pot_comp.f:7826-8058 (EXPANSION_MATRIX_ELEMENT, SYS_TYPE 8).  For the pair
+ * (p = stp, pp = stpp) with total m:
+ *   A_t = sqrt((2l1+1)(2l2+1))/(4 pi) <j2'' 0 l2 0|j2' 0> M1 M3,
+ *   M1  = sum over nju = nju1 and (if nju1 != 0) -nju1 with the phase
+ *         (-1)^(l1+l2+l+nju1) for the second, of
+ *         sum_{k1'} <j1'' k1'-nju l1 nju|j1' k1'> c'_{k1'} c''_{k1'-nju}   (:7948-7974),
+ *   M3  = sum_{m'} <j1' m' j2' m-m'|j12' m> sum_{me} <l1 me l2 -me|l 0>
+ *         <j1'' m'' j2'' m-m''|j12'' m> <j1'' m'' l1 me|j1' m'>
+ *         <j2'' m-m'' l2 -me|j2' m-m'>,  m'' = m' - me                    (:7982-8018),
+ *   M_k(R) = sqrt((2j1''+1)/(2j1'+1)) sqrt((2j2''+1)/(2j2'+1)) sum_t T_t(R) A_t
+ * with the triangle rules of :7923-7925. */
+static int orc_triangle(int a, int b, int c) { return c >= abs(a - b) && c <= a + b; }
+
+int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double* mat) {
+  if (sys->sys_type != 8 || !sys->j2 || !sys->vec1) return -1;
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t k = 0; k < P; ++k) {
+    const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+    const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
+    const int j1p = sys->j1[cp], j2p = sys->j2[cp], j1pp = sys->j1[cpp], j2pp = sys->j2[cpp];
+    const int j12p = j12[sp], j12pp = j12[spp], m = m12[sp];
+    const double* vp = sys->vec1 + (size_t)cp * sys->ldv;
+    const double* vpp = sys->vec1 + (size_t)cpp * sys->ldv;
+    const double coef12 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+    double* out = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) out[i] = 0.0;
+    for (int t = 0; t < n_terms; ++t) {
+      const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
+                l = labels[4 * t + 3];
+      if (!orc_triangle(j1pp, l1, j1p) || !orc_triangle(l1, l2, l) || !orc_triangle(j2pp, l2, j2p))
+        continue;
+      const double coef3 = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (4.0 * ORC_PI);
+      const double cg_j2 = orc_cg(j2pp, l2, j2p, 0, 0, 0);
+      double m1 = 0.0;
+      for (int planar = 0; planar < (nju1 == 0 ? 1 : 2); ++planar) {
+        const int nju = planar ? -nju1 : nju1;
+        const double phase = planar ? (((l1 + l2 + l + nju1) % 2) ? -1.0 : 1.0) : 1.0;
+        double s = 0.0;
+        for (int k1p = -j1p; k1p <= j1p; ++k1p) {
+          const int k1pp = k1p - nju;
+          if (abs(k1pp) > j1pp) continue;
+          s += orc_cg(j1pp, l1, j1p, k1pp, nju, k1p) * vp[j1p + k1p] * vpp[j1pp + k1pp];
+        }
+        m1 += phase * s;
+      }
+      double m3 = 0.0;
+      for (int mp = -j1p; mp <= j1p; ++mp) {
+        if (abs(m - mp) > j2p) continue;
+        const double cg_p = orc_cg(j1p, j2p, j12p, mp, m - mp, m);
+        double m2 = 0.0;
+        const int mx = l1 < l2 ? l1 : l2;
+        for (int me = -mx; me <= mx; ++me) {
+          const int mpp = mp - me;
+          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+          m2 += orc_cg(l1, l2, l, me, -me, 0) * orc_cg(j1pp, j2pp, j12pp, mpp, m - mpp, m) *
+                orc_cg(j1pp, l1, j1p, mpp, me, mp) * orc_cg(j2pp, l2, j2p, m - mpp, -me, m - mp);
+        }
+        m3 += m2 * cg_p;
+      }
+      const double a = coef3 * cg_j2 * m1 * m3;
+      if (a == 0.0) continue;
+      for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
+    }
+    for (int i = 0; i < nR; ++i) out[i] *= coef12 * ORC_CM_TO_HARTREE;
+  }
+  return 0;
+}

@@ -165,6 +165,16 @@ int orc_derivs(const orc_tables* tab, double t, const double* q, double* dqdt);
 int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int n_traj,
                 const double* prob, double k_vec, double* sigma);
 
+/* PES-expansion matrix elements of SYS_TYPE 8 (asymmetric top + diatom),
+ * SRC/pot_comp.f:7826-8058 (EXPANSION_MATRIX_ELEMENT, case 8): per stored pair k
+ * (stp = ind_mat[2k], stpp = ind_mat[2k+1]) and R point, the sum over terms t of
+ * terms[iR * n_terms + t] (cm^-1) times the R-independent angular coefficient of
+ * (l1, nju1, l2, l) = labels[4t .. 4t+3]; mat[k * nR + iR] in Hartree. */
+int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double* mat);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,9 @@ def lib():
         L.orc_w3js.argtypes = [C.c_int] * 6
         L.orc_cg.restype = C.c_double
         L.orc_cg.argtypes = [C.c_int] * 6
+        L.orc_expansion_matrix_type8.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
+                                                 C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_djkm.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_wf_diat.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double,
@@ -338,3 +341,19 @@ def inelast(n_channels, j_ini, J_down, J_up, L_min, prob, k_vec):
     p = np.ascontiguousarray(prob, np.float64)
     lib().orc_inelast(n_channels, j_ini, J_down, J_up, L_min, p.shape[0], p.reshape(-1), k_vec, sig)
     return sig
+
+
+def expansion_matrix_type8(osys, states, ind, labels, terms):
+    """SYS_TYPE 8 matrix (P x nR, Hartree) from PES expansion terms (nR x n_terms, cm^-1)."""
+    ic, j12, m12, _ = states
+    ind = np.ascontiguousarray(ind, np.int32)
+    labels = np.ascontiguousarray(labels, np.int32)
+    terms = np.ascontiguousarray(terms, np.float64)
+    P, nR = ind.shape[0], terms.shape[0]
+    mat = np.zeros(P * nR)
+    rc = lib().orc_expansion_matrix_type8(C.byref(osys.s), _ptr(ic), _ptr(j12), _ptr(m12), P,
+                                          _ptr(ind.reshape(-1)), labels.shape[0],
+                                          _ptr(labels.reshape(-1)), nR, _ptr(terms), _ptr(mat))
+    if rc:
+        raise RuntimeError(f"orc_expansion_matrix_type8 failed: {rc}")
+    return mat.reshape(P, nR)

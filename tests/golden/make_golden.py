@@ -74,6 +74,19 @@ def main(ref_root):
         e_ch_printed=np.array([0.000, 37.158, 70.133, 95.245, 145.505, 164.108, 201.219, 257.028,
                                295.304, 334.334]))
 
+    # G5: the PES expansion terms from which the reference built the G3 matrix
+    # (EXAMPLES_IO/SYS_TYPE_8/H2O_H2_MTRXCalculation: PES_EXPAN_TERMS.DAT -> MTRX.DAT,
+    # which is identical to the G3 MTRX.DAT).  Header "R_Bohr v_l1_nju1_l2_l ...",
+    # then one row per R (f6.2 R, e19.12 values, cm^-1).
+    d = os.path.join(ex, "SYS_TYPE_8", "H2O_H2_MTRXCalculation")
+    with open(os.path.join(d, "PES_EXPAN_TERMS.DAT")) as f:
+        head = f.readline().split()
+        rows = [[float(x) for x in ln.split()] for ln in f if ln.strip()]
+    labels = np.array([[int(x) for x in h.split("_")[1:]] for h in head[1:]], dtype=np.int32)
+    vals = np.array(rows)
+    np.savez_compressed(os.path.join(out, "g5_h2o_h2_expansion_terms.npz"), labels=labels,
+                        R=vals[:, 0], terms=vals[:, 1:])
+
     # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)
