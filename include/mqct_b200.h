@@ -149,6 +149,18 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
                       double r_cut1, double r_cut2, double* Mat_el, double* Mat_el_y2,
                       int32_t* skipped, mqct_err_report_t* err);
 
+/* Matrix build from PES expansion terms (the READ_EXPANSION path: READ_EXPANSION_TERMS
+ * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749),
+ * SYS_TYPE 8 (asymmetric top + diatom, case 8 at :7826-8058): labels[4t .. 4t+3] =
+ * (l1, nju1, l2, l) of term t (the TERMS list of $POTENTIAL), terms[iR * n_terms + t]
+ * the expansion coefficients in cm^-1 (the rows of PES_EXPAN_TERMS.DAT).  Output as
+ * mqct_build_matrix: Hartree, MIJ_CUTOFF, spline y2.  j1, j2 <= 30, l1, l2 <= 30, l <= 60. */
+int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                                const double* R, int32_t nR, int32_t n_terms,
+                                const int32_t* labels, const double* terms, double mij_cutoff_cm,
+                                double r_cut1, double r_cut2, double* Mat_el, double* Mat_el_y2,
+                                int32_t* skipped);
+
 /* Device-resident form of the same build for callers that keep the matrix on
  * the GPU: a plan uploads the system once; execute writes Mat_el and y2 into
  * device buffers (nR*P doubles each, may be NULL for y2) on the plan's stream. */

@@ -25,8 +25,9 @@ from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
            "PropagationPlan", "trajectory_set", "cross_sections", "write_mtrx_uf",
-           "read_mtrx_uf", "spline_y2", "Surrogate", "MqctError", "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32",
-           "PROP_FP64", "MODE_STD", "MODE_AT"]
+           "read_mtrx_uf", "spline_y2", "Surrogate", "build_matrix_expansion", "MqctError",
+           "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
+           "MODE_AT"]
 
 
 def asym_top_level(A, B, Cc, j, ka, kc):
@@ -244,6 +245,26 @@ def build_matrix(system: CollisionSystem, R, grid, pes, precision=PREC_FP64, mij
     check(lib().mqct_build_matrix(C.byref(s), np.ascontiguousarray(system.ind_mat.reshape(-1)), P,
                                   R, nR, C.byref(g), C.byref(ps), precision, mij_cutoff, r_cut1,
                                   r_cut2, mat, ptr(y2), ptr(sk), None))
+    return mat.reshape(P, nR), y2.reshape(P, nR), sk
+
+
+def build_matrix_expansion(system: CollisionSystem, R, labels, terms, mij_cutoff=1e-12, r_cut1=6.0,
+                           r_cut2=8.0):
+    """Matrix from PES expansion terms (READ_EXPANSION path, SYS_TYPE 8): labels (n_terms x 4:
+    l1, nju1, l2, l), terms (nR x n_terms, cm^-1).  Returns (Mat_el, y2, skipped) as
+    build_matrix."""
+    R = np.ascontiguousarray(R, np.float64)
+    labels = np.ascontiguousarray(labels, np.int32).reshape(-1, 4)
+    terms = np.ascontiguousarray(terms, np.float64).reshape(len(R), len(labels))
+    P, nR = system.P, len(R)
+    mat = np.zeros(P * nR)
+    y2 = np.zeros(P * nR)
+    sk = np.zeros(P, np.int32)
+    sd = system.c_struct()
+    ind = np.ascontiguousarray(system.ind_mat.reshape(-1))
+    check(lib().mqct_build_matrix_expansion(C.byref(sd), ind, P, R, nR, len(labels),
+                                            labels.reshape(-1), terms.reshape(-1), mij_cutoff,
+                                            r_cut1, r_cut2, mat, ptr(y2), ptr(sk)))
     return mat.reshape(P, nR), y2.reshape(P, nR), sk
 
 

@@ -79,7 +79,7 @@ EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
-    "mqct_spline_y2_noalloc", "mqct_propagate_batch",
+    "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
     "mqct_surrogate_create", "mqct_surrogate_train", "mqct_surrogate_predict",
     "mqct_surrogate_n_params", "mqct_surrogate_get_params", "mqct_surrogate_loss_grad",
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
@@ -120,6 +120,9 @@ def lib():
     L.mqct_prop_plan_timing.argtypes = [vp, C.POINTER(C.c_float)]
     L.mqct_matrix_plan_destroy.argtypes = [vp]
     L.mqct_spline_y2_noalloc.argtypes = [vp, C.c_int32, vp, vp, C.c_int64, vp, vp]
+    L.mqct_build_matrix_expansion.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
+                                              C.c_int32, i32p, f64p, C.c_double, C.c_double,
+                                              C.c_double, f64p, vp, vp]
     L.mqct_surrogate_create.argtypes = [C.c_int32, C.POINTER(Pes), C.c_int32, C.c_int32,
                                         C.c_uint64, C.c_double, C.c_double, C.POINTER(vp)]
     L.mqct_surrogate_train.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_double, vp, vp]

@@ -611,6 +611,25 @@ static double clebsch_gordan(int j1, int m1, int j2, int m2, int J, int M) {
   return sum;
 }
 
+// Grid-only coefficients of finalize_kernel's spline fit (5 x nR, see there).
+static std::vector<double> spline_grid_coefs(const std::vector<double>& Rh) {
+  const int nR = (int)Rh.size();
+  std::vector<double> gc(5 * (size_t)nR, 0.0);
+  double f = -0.5;  // y2 recurrence factor at i = 0
+  gc[3 * nR] = f;
+  for (int i = 0; i + 1 < nR; ++i) gc[i] = 1.0 / (Rh[i + 1] - Rh[i]);
+  for (int i = 1; i < nR - 1; ++i) {
+    const double sig = (Rh[i] - Rh[i - 1]) / (Rh[i + 1] - Rh[i - 1]);
+    const double p = sig * f + 2.0;
+    f = (sig - 1.0) / p;
+    gc[nR + i] = 6.0 / (Rh[i + 1] - Rh[i - 1]) / p;
+    gc[2 * nR + i] = sig / p;
+    gc[3 * nR + i] = f;
+  }
+  gc[4 * nR] = nR >= 3 ? -0.5 / (0.5 * gc[3 * nR + nR - 2] + 1.0) : 0.0;
+  return gc;
+}
+
 static int nearest_index(const std::vector<double>& R, double r) {
   int best = 0;
   double d = fabs(R[0] - r);
@@ -886,22 +905,7 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
   }
 
   // --- grid-only coefficients of the fused spline fit (finalize_kernel)
-  {
-    std::vector<double> gc(5 * (size_t)nR, 0.0);
-    double f = -0.5;  // y2 recurrence factor at i = 0
-    gc[3 * nR] = f;
-    for (int i = 0; i + 1 < nR; ++i) gc[i] = 1.0 / (Rh[i + 1] - Rh[i]);
-    for (int i = 1; i < nR - 1; ++i) {
-      const double sig = (Rh[i] - Rh[i - 1]) / (Rh[i + 1] - Rh[i - 1]);
-      const double p = sig * f + 2.0;
-      f = (sig - 1.0) / p;
-      gc[nR + i] = 6.0 / (Rh[i + 1] - Rh[i - 1]) / p;
-      gc[2 * nR + i] = sig / p;
-      gc[3 * nR + i] = f;
-    }
-    gc[4 * nR] = nR >= 3 ? -0.5 / (0.5 * gc[3 * nR + nR - 2] + 1.0) : 0.0;
-    MQCT_CUDA_TRY(d_spl_fin.upload(gc, stream));
-  }
+  MQCT_CUDA_TRY(d_spl_fin.upload(spline_grid_coefs(Rh), stream));
   // --- work buffers
   MQCT_CUDA_TRY(d_psi.alloc((size_t)n_basis_rows * G2));
   ldw = nR;
@@ -1262,5 +1266,210 @@ extern "C" int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t*
   }
   *n_exact_r = n;
   *max_ratio = mx;
+  return MQCT_OK;
+}
+
+// ------------------------------------------------------------------ PES-expansion path
+// Matrix elements from PES expansion terms (the READ_EXPANSION path of the
+// reference, EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6465-8749;
+// asymmetric top + diatom, case 8 at :7826-8058):
+//   M_k(R) = c_k sum_t T_t(R) A_{k,t}
+// with R-independent angular coefficients A (products of Clebsch-Gordan
+// coefficients and rotor eigenvectors, see expansion_angular_kernel) and
+// c_k = sqrt((2 j1''+1)/(2 j1'+1)) sqrt((2 j2''+1)/(2 j2'+1)).  A is formed on the
+// GPU (one thread per (pair, term)), the sum over terms is an FP64 contraction,
+// and the fused finalize converts to Hartree, applies MIJ_CUTOFF and fits the
+// spline.
+
+// <j1 m1 j2 m2 | J M> by Racah's closed form with the log-factorial table.
+__device__ inline double cg_dev(int j1, int m1, int j2, int m2, int J, int M) {
+  if (m1 + m2 != M || J < abs(j1 - j2) || J > j1 + j2 || abs(m1) > j1 || abs(m2) > j2 ||
+      abs(M) > J)
+    return 0.0;
+  const double* lf = c_logfact;
+  const double pre = 0.5 * (log(2.0 * J + 1.0) + lf[J + j1 - j2] + lf[J - j1 + j2] +
+                            lf[j1 + j2 - J] - lf[j1 + j2 + J + 1] + lf[J + M] + lf[J - M] +
+                            lf[j1 - m1] + lf[j1 + m1] + lf[j2 - m2] + lf[j2 + m2]);
+  double sum = 0.0;
+  for (int k = 0; k <= j1 + j2 - J; ++k) {
+    const int a = j1 - m1 - k, b = j2 + m2 - k, c = J - j2 + m1 + k, d = J - j1 - m2 + k;
+    if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+    const double t = exp(pre - lf[k] - lf[j1 + j2 - J - k] - lf[a] - lf[b] - lf[c] - lf[d]);
+    sum += (k & 1) ? -t : t;
+  }
+  return sum;
+}
+
+__device__ inline bool triangle_ok(int a, int b, int c) { return c >= abs(a - b) && c <= a + b; }
+
+// A[k * n_terms + t] (times c_k) for SYS_TYPE 8; p = ind_mat[2k] - 1, pp = ind_mat[2k+1] - 1.
+//   A = sqrt((2l1+1)(2l2+1))/(4 pi) <j2'' 0 l2 0|j2' 0> M1 M3, with
+//   M1 = sum over nju = nju1 and (nju1 != 0) -nju1, phase (-1)^(l1+l2+l+nju1) on the
+//        second, of sum_{k1'} <j1'' k1'-nju l1 nju|j1' k1'> c'_{k1'} c''_{k1'-nju},
+//   M3 = sum_{m'} <j1' m' j2' m-m'|j12' m> sum_{me} <l1 me l2 -me|l 0>
+//        <j1'' m'' j2'' m-m''|j12'' m> <j1'' m'' l1 me|j1' m'> <j2'' m-m'' l2 -me|j2' m-m'>,
+//        m'' = m' - me.
+__global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
+                                         const int* __restrict__ st_chan,
+                                         const int* __restrict__ st_j12,
+                                         const int* __restrict__ st_m, const int* __restrict__ ch_j1,
+                                         const int* __restrict__ ch_j2,
+                                         const double* __restrict__ vec, int ldv,
+                                         const int* __restrict__ labels, double* __restrict__ A) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * n_terms) return;
+  const int64_t k = idx / n_terms;
+  const int t = (int)(idx % n_terms);
+  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
+  const int j12p = st_j12[sp], j12pp = st_j12[spp], m = st_m[sp];
+  const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
+            l = labels[4 * t + 3];
+  double a = 0.0;
+  if (triangle_ok(j1pp, l1, j1p) && triangle_ok(l1, l2, l) && triangle_ok(j2pp, l2, j2p)) {
+    const double* vp = vec + (size_t)cp * ldv;
+    const double* vpp = vec + (size_t)cpp * ldv;
+    double m1 = 0.0;
+    for (int planar = 0; planar < (nju1 == 0 ? 1 : 2); ++planar) {
+      const int nju = planar ? -nju1 : nju1;
+      const double phase = planar ? (((l1 + l2 + l + nju1) & 1) ? -1.0 : 1.0) : 1.0;
+      double sum = 0.0;
+      for (int k1p = -j1p; k1p <= j1p; ++k1p) {
+        const int k1pp = k1p - nju;
+        if (abs(k1pp) > j1pp) continue;
+        sum += cg_dev(j1pp, k1pp, l1, nju, j1p, k1p) * vp[j1p + k1p] * vpp[j1pp + k1pp];
+      }
+      m1 += phase * sum;
+    }
+    double m3 = 0.0;
+    if (m1 != 0.0) {
+      const int mx = l1 < l2 ? l1 : l2;
+      for (int mp = -j1p; mp <= j1p; ++mp) {
+        if (abs(m - mp) > j2p) continue;
+        double m2 = 0.0;
+        for (int me = -mx; me <= mx; ++me) {
+          const int mpp = mp - me;
+          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+          m2 += cg_dev(l1, me, l2, -me, l, 0) * cg_dev(j1pp, mpp, j2pp, m - mpp, j12pp, m) *
+                cg_dev(j1pp, mpp, l1, me, j1p, mp) * cg_dev(j2pp, m - mpp, l2, -me, j2p, m - mp);
+        }
+        m3 += m2 * cg_dev(j1p, mp, j2p, m - mp, j12p, m);
+      }
+    }
+    a = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (4.0 * kPi) * cg_dev(j2pp, 0, l2, 0, j2p, 0) *
+        m1 * m3 * sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+        sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+  }
+  A[idx] = a;
+}
+
+// M[k * nR + i] = sum_t A[k, t] T[i, t] (fixed order); one CTA per pair.
+__global__ void expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
+                                          const double* __restrict__ T, double* __restrict__ M) {
+  const int64_t k = blockIdx.x;
+  const double* a = A + k * n_terms;
+  for (int i = threadIdx.x; i < nR; i += blockDim.x) {
+    const double* ti = T + (size_t)i * n_terms;
+    double s = 0.0;
+    for (int t = 0; t < n_terms; ++t) s = fma(a[t], ti[t], s);
+    M[k * nR + i] = s;
+  }
+}
+
+extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                                           const double* R, int32_t nR, int32_t n_terms,
+                                           const int32_t* labels, const double* terms,
+                                           double mij_cutoff_cm, double r_cut1, double r_cut2,
+                                           double* Mat_el, double* Mat_el_y2, int32_t* skipped) {
+  MQCT_ARG_CHECK(sys && ind_mat && R && labels && terms && Mat_el, "null argument");
+  MQCT_ARG_CHECK(sys->sys_type == 8, "the expansion path supports SYS_TYPE 8 (got %d)",
+                 sys->sys_type);
+  MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->vec1 && sys->ldv > 0 && sys->indx_chann && sys->j12 &&
+                     sys->m12 && sys->n_states > 0,
+                 "system arrays missing");
+  MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && nR >= 2 && nR <= 3072,
+                 "bad sizes");
+  for (int i = 0; i + 1 < nR; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
+  for (int t = 0; t < n_terms; ++t) {
+    const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
+              l = labels[4 * t + 3];
+    // the log-factorial table (128 entries) bounds every Clebsch-Gordan argument sum
+    MQCT_ARG_CHECK(l1 >= 0 && l2 >= 0 && l >= 0 && nju1 >= 0 && nju1 <= l1 && l1 <= 30 &&
+                       l2 <= 30 && l <= 60,
+                   "bad expansion term %d (%d, %d, %d, %d): nju1 in 0..l1, l1, l2 <= 30, l <= 60",
+                   t + 1, l1, nju1, l2, l);
+  }
+  const int n_states = sys->n_states;
+  std::vector<int> st_chan(n_states);
+  for (int s = 0; s < n_states; ++s) {
+    st_chan[s] = sys->indx_chann[s] - 1;
+    MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < sys->n_channels, "indx_chann out of range");
+    const int ch = st_chan[s];
+    MQCT_ARG_CHECK(sys->j1[ch] >= 0 && sys->j1[ch] <= 30 && sys->j2[ch] >= 0 &&
+                       sys->j2[ch] <= 30 && 2 * sys->j1[ch] + 1 <= sys->ldv,
+                   "bad channel %d (j1, j2 <= 30)", ch + 1);
+    MQCT_ARG_CHECK(sys->j12[s] >= abs(sys->j1[ch] - sys->j2[ch]) &&
+                       sys->j12[s] <= sys->j1[ch] + sys->j2[ch] && abs(sys->m12[s]) <= sys->j12[s],
+                   "bad (j12, m12) at state %d", s + 1);
+  }
+  for (int64_t k = 0; k < P; ++k) {
+    const int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
+    MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states, "ind_mat out of range");
+    MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
+                   (long long)k + 1);
+  }
+  if (mqct_device_count() <= 0) {
+    set_error("no CUDA device available");
+    return MQCT_E_NODEV;
+  }
+  int rc = upload_logfact();
+  if (rc) return rc;
+  cudaStream_t st = nullptr;
+  MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } guard{st};
+  std::vector<int> ch_j1(sys->j1, sys->j1 + sys->n_channels), ch_j2(sys->j2, sys->j2 + sys->n_channels);
+  DevBuf<int> d_ind, d_chan, d_j12, d_m, d_j1, d_j2, d_lab, d_k2r, d_sk;
+  DevBuf<double> d_vec, d_T, d_A, d_M, d_mat, d_y2, d_gc;
+  MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
+  MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
+  MQCT_CUDA_TRY(d_j12.upload(sys->j12, n_states, st));
+  MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
+  MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
+  MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
+  MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)sys->n_channels * sys->ldv, st));
+  MQCT_CUDA_TRY(d_lab.upload(labels, 4 * (size_t)n_terms, st));
+  MQCT_CUDA_TRY(d_T.upload(terms, (size_t)nR * n_terms, st));
+  std::vector<double> Rh(R, R + nR);
+  MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
+  std::vector<int> k2r(P);
+  for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
+  MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
+  MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
+  MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
+  MQCT_CUDA_TRY(d_mat.alloc((size_t)P * nR));
+  MQCT_CUDA_TRY(d_y2.alloc((size_t)P * nR));
+  MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
+  const int64_t n_at = P * n_terms;
+  expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
+      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec.p, sys->ldv, d_lab.p,
+      d_A.p);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  expansion_contract_kernel<<<(unsigned)P, 128, 0, st>>>(n_terms, nR, d_A.p, d_T.p, d_M.p);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  const int ir1 = nearest_index(Rh, r_cut1), ir2 = nearest_index(Rh, r_cut2);
+  finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
+      P, nR, d_k2r.p, d_M.p, 1, 0, nR, kCmToHartree, nullptr, ir1, ir2,
+      mij_cutoff_cm * kCmToHartree, d_gc.p, d_mat.p, d_sk.p, Mat_el_y2 ? d_y2.p : nullptr);
+  MQCT_CUDA_TRY(cudaGetLastError());
+  MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el, d_mat.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, st));
+  if (Mat_el_y2)
+    MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el_y2, d_y2.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, st));
+  if (skipped)
+    MQCT_CUDA_TRY(cudaMemcpyAsync(skipped, d_sk.p, sizeof(int32_t) * P, cudaMemcpyDeviceToHost, st));
+  MQCT_CUDA_TRY(cudaStreamSynchronize(st));
   return MQCT_OK;
 }

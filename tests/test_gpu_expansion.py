@@ -1,0 +1,43 @@
+"""GPU parity of the PES-expansion matrix build (SYS_TYPE 8): the reference's own
+H2O + H2 matrix (MTRX.DAT, built by the reference from PES_EXPAN_TERMS.DAT) is
+reproduced from the same expansion terms, up to the per-level eigenvector phase
+(see tests/test_oracle_expansion.py), and the GPU agrees with the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from test_oracle_expansion import level_gauge
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_expansion_matrix_matches_reference_and_oracle(mq, oracle, gpu_available):
+    g = np.load(os.path.join(GOLD, "g3_h2o_h2_type8.npz"))
+    g5 = np.load(os.path.join(GOLD, "g5_h2o_h2_expansion_terms.npz"))
+    s = mq.CollisionSystem(8, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           BE=float(g["BE"]))
+    m, y2, sk = mq.build_matrix_expansion(s, g5["R"], g5["labels"], g5["terms"], mij_cutoff=0.0)
+    ref = g["mat"]
+    gauge = level_gauge(s, m, ref)
+    assert np.max(np.abs(m - gauge[:, None] * ref)) <= 1e-10 * np.abs(ref).max()
+    ch = s.channels
+    osys = oracle.OracleSystem(8, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch,
+                               vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    mo = oracle.expansion_matrix_type8(osys, osys.states(), s.ind_mat, g5["labels"], g5["terms"])
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+    # spline of the columns: the host restatement of the reference's spline
+    y2ref = mq.spline_y2(g5["R"], m)
+    assert np.max(np.abs(y2 - y2ref)) <= 1e-10 * np.abs(y2ref).max()
+    assert not sk.any()
+
+
+def test_expansion_rejects_bad_terms(mq, gpu_available):
+    g = np.load(os.path.join(GOLD, "g3_h2o_h2_type8.npz"))
+    s = mq.CollisionSystem(8, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           BE=float(g["BE"]))
+    R = g["R"]
+    with pytest.raises(mq.MqctError):
+        mq.build_matrix_expansion(s, R, np.array([[1, 2, 0, 1]]), np.zeros((len(R), 1)))
