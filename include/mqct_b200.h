@@ -150,16 +150,23 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
                       int32_t* skipped, mqct_err_report_t* err);
 
 /* Matrix build from PES expansion terms (the READ_EXPANSION path: READ_EXPANSION_TERMS
- * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749),
- * SYS_TYPE 8 (asymmetric top + diatom, case 8 at :7826-8058): labels[4t .. 4t+3] =
- * (l1, nju1, l2, l) of term t (the TERMS list of $POTENTIAL), terms[iR * n_terms + t]
- * the expansion coefficients in cm^-1 (the rows of PES_EXPAN_TERMS.DAT).  Output as
- * mqct_build_matrix: Hartree, MIJ_CUTOFF, spline y2.  j1, j2 <= 30, l1, l2 <= 30, l <= 60. */
+ * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749), for
+ * SYS_TYPE 8 (asymmetric top + diatom, case 8 at :7826-8058) and SYS_TYPE 0 (two
+ * asymmetric tops, distinguishable partners, case 0 at :8257-8672).  The arrays are
+ * the reference's own:
+ *   a_top  A_TOP(5, nterms): per term 5 int32, (l1, nju1, l2, l, -) for SYS_TYPE 8,
+ *          (l1, nju1, l2, nju2, l) for SYS_TYPE 0 (:6322-6338);
+ *   terms  expansion_terms(n_r_coll, nterms): terms[t * nR + iR], R fastest, in the
+ *          energy unit of the PES_EXPAN_TERMS.DAT file;
+ *   e_unit conv_unit_e, the Hartree value of that unit (MQCT_SOURCE_CODES/matrix_ini.f:918-921:
+ *          1/eVtown/autoeV for CM-1, 1/kcal for KCAL, 1/autokelv/autoeV for K).
+ * Output as mqct_build_matrix: Mat_el in Hartree, MIJ_CUTOFF (mij_cutoff_cm, cm^-1)
+ * and the spline y2.  j1, j2 <= 30, l1, l2 <= 30, l <= 60, n_terms <= 4096. */
 int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
                                 const double* R, int32_t nR, int32_t n_terms,
-                                const int32_t* labels, const double* terms, double mij_cutoff_cm,
-                                double r_cut1, double r_cut2, double* Mat_el, double* Mat_el_y2,
-                                int32_t* skipped);
+                                const int32_t* a_top, const double* terms, double e_unit,
+                                double mij_cutoff_cm, double r_cut1, double r_cut2,
+                                double* Mat_el, double* Mat_el_y2, int32_t* skipped);
 
 /* Device-resident form of the same build for callers that keep the matrix on
  * the GPU: a plan uploads the system once; execute writes Mat_el and y2 into
@@ -286,6 +293,18 @@ int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
 /* Device-resident propagation plan (tables uploaded once; trajectories given
  * per call).  run() uses host trajectory/out buffers; run_device() takes device
  * buffers for init (n_traj mqct_traj_init_t) and outputs. */
+/* The same in standard mode with SAVE_TRAJECT = YES (the classical paths of the
+ * first AT-MQCT run, MQCT_SOURCE_CODES/propagator.f:2866-2880, 3458-3464, 4329-4337):
+ * rec_out (host, n_traj * max_rec * 8 doubles) receives per trajectory the records
+ * (t, R, P_R, theta, P_theta, phi, P_phi, pot) of the state at the top of every
+ * RK4 step, pot the coupling energy, then one record of the final state stamped
+ * t_final + dt; n_rec_out[t] = records produced (those past max_rec are counted,
+ * not written).  Record t of a trajectory is at rec_out[(t * max_rec + r) * 8]. */
+int mqct_propagate_batch_rec(const mqct_tables_t* tab, const mqct_traj_init_t* init,
+                             int64_t n_traj, int32_t arith, int64_t max_rec, double* amp_out,
+                             double* cls_out, double* diag_out, double* rec_out,
+                             int64_t* n_rec_out);
+
 typedef struct mqct_prop_plan mqct_prop_plan;
 int mqct_prop_plan_create(const mqct_tables_t* tab, int32_t arith, mqct_prop_plan** plan);
 int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,

@@ -24,8 +24,8 @@ from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_F
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
-           "PropagationPlan", "trajectory_set", "cross_sections", "write_mtrx_uf",
-           "read_mtrx_uf", "spline_y2", "Surrogate", "build_matrix_expansion", "MqctError",
+           "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections", "write_mtrx_uf",
+           "read_mtrx_uf", "spline_y2", "Surrogate", "build_matrix_expansion", "E_UNIT", "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
            "MODE_AT"]
 
@@ -248,22 +248,36 @@ def build_matrix(system: CollisionSystem, R, grid, pes, precision=PREC_FP64, mij
     return mat.reshape(P, nR), y2.reshape(P, nR), sk
 
 
-def build_matrix_expansion(system: CollisionSystem, R, labels, terms, mij_cutoff=1e-12, r_cut1=6.0,
-                           r_cut2=8.0):
-    """Matrix from PES expansion terms (READ_EXPANSION path, SYS_TYPE 8): labels (n_terms x 4:
-    l1, nju1, l2, l), terms (nR x n_terms, cm^-1).  Returns (Mat_el, y2, skipped) as
-    build_matrix."""
+# Hartree value of the PES_EXPAN_TERMS.DAT energy units (E_UNITS, conv_unit_e of
+# MQCT_SOURCE_CODES/matrix_ini.f:918-921 with the constants of iotest.f:20-24)
+E_UNIT = {"CM-1": CM_TO_HARTREE, "KCAL": 1.0 / 627.509469, "K": 1.0 / 1.1604519e4 / 27.21113845,
+          "AU": 1.0}
+
+
+def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",
+                           mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
+    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 8 and 0).
+
+    labels: the TERMS list, one row per term: (l1, nju1, l2, l) for SYS_TYPE 8,
+    (l1, nju1, l2, nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
+    PES_EXPAN_TERMS.DAT, in the unit e_unit (a key of E_UNIT or the Hartree value of
+    one unit).  Returns (Mat_el, y2, skipped) as build_matrix."""
     R = np.ascontiguousarray(R, np.float64)
-    labels = np.ascontiguousarray(labels, np.int32).reshape(-1, 4)
-    terms = np.ascontiguousarray(terms, np.float64).reshape(len(R), len(labels))
+    lab = np.asarray(labels, np.int32)
+    lab = lab.reshape(len(lab), -1)
+    a_top = np.zeros((len(lab), 5), np.int32)  # A_TOP(5, nterms)
+    a_top[:, :lab.shape[1]] = lab
+    # expansion_terms(n_r_coll, nterms): R fastest
+    T = np.ascontiguousarray(np.asarray(terms, np.float64).reshape(len(R), len(lab)).T)
+    eu = E_UNIT[e_unit.upper()] if isinstance(e_unit, str) else float(e_unit)
     P, nR = system.P, len(R)
     mat = np.zeros(P * nR)
     y2 = np.zeros(P * nR)
     sk = np.zeros(P, np.int32)
     sd = system.c_struct()
     ind = np.ascontiguousarray(system.ind_mat.reshape(-1))
-    check(lib().mqct_build_matrix_expansion(C.byref(sd), ind, P, R, nR, len(labels),
-                                            labels.reshape(-1), terms.reshape(-1), mij_cutoff,
+    check(lib().mqct_build_matrix_expansion(C.byref(sd), ind, P, R, nR, len(lab),
+                                            a_top.reshape(-1), T.reshape(-1), eu, mij_cutoff,
                                             r_cut1, r_cut2, mat, ptr(y2), ptr(sk)))
     return mat.reshape(P, nR), y2.reshape(P, nR), sk
 
@@ -414,8 +428,11 @@ class Trajectory:
 def trajectory_set(U_cm, b_max, mass_amu, s_st, time_step, rmax, j_max_ini=0, dl=1,
                    time_lim=0.0, max_steps=2_000_000):
     """Integer-l trajectory set of PROPAGATE (MQCT_SOURCE_CODES/propagator.f:419-495):
-    k = sqrt(2 mu E), J_max = int(b_max k) - j_max, l = L_MIN..L_MAX step DL;
-    dt = TIME_STEP / sqrt(U / 300) (MQCT_SOURCE_CODES/propagator.f:2436)."""
+    k = sqrt(2 mu E), J_max = int(b_max k) - j_max, (L_MAX - L_MIN)/DL + 1 trajectories
+    at the midpoints of their l bins, l = int((id - 1/2) DL + L_MIN) capped at L_MAX
+    (TRAJ_ORB, MQCT_SOURCE_CODES/propagator.f:5163-5167, 5195-5198; for DL = 1,
+    l = L_MIN, L_MIN + 1, ...); dt = TIME_STEP / sqrt(U / 300)
+    (MQCT_SOURCE_CODES/propagator.f:2436)."""
     E = U_cm * CM_TO_HARTREE
     mu = mass_amu * AMU_TO_AU
     k = np.sqrt(mu * 2.0 * E)
@@ -423,9 +440,11 @@ def trajectory_set(U_cm, b_max, mass_amu, s_st, time_step, rmax, j_max_ini=0, dl
     L_max = J_max + j_max_ini
     L_min = max(0, 0 if J_max >= j_max_ini else j_max_ini - J_max)
     dt = time_step / np.sqrt(U_cm / 300.0)
+    n_traj = (L_max - L_min) // dl + 1
+    ls = [min(int((i - 0.5) * dl + L_min), L_max) for i in range(1, n_traj + 1)]
     trajs = [Trajectory(E, float(l), s_st, dt, rmax, rmax, time_lim=time_lim, max_steps=max_steps)
-             for l in range(L_min, L_max + 1, dl)]
-    return trajs, dict(k=k, J_down=0, J_up=J_max, L_min=L_min, E=E)
+             for l in ls]
+    return trajs, dict(k=k, J_down=0, J_up=J_max, L_min=L_min, E=E, dl=dl)
 
 
 def _traj_array(trajs):
@@ -453,6 +472,27 @@ def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, 
     check(lib().mqct_propagate_batch(C.byref(t), arr, n, mode, C.byref(at) if at else None,
                                      arith, amp, cls, diag))
     return amp.reshape(n, 2 * N), cls.reshape(n, 6), diag.reshape(n, 8)
+
+
+def propagate_record(tables: PropagationTables, trajs, arith=PROP_FP64, max_rec=1 << 15):
+    """Standard-mode DOTRAJECT with SAVE_TRAJECT on the GPU: returns (amp, cls, diag,
+    paths), paths[t] the (n x 8) records (t, R, P_R, theta, P_theta, phi, P_phi, pot)
+    that an AT-MQCT run takes as at_paths."""
+    n = len(trajs)
+    N = tables.n_states
+    amp = np.zeros(n * 2 * N)
+    cls = np.zeros(n * 6)
+    diag = np.zeros(n * 8)
+    rec = np.zeros(n * max_rec * 8)
+    n_rec = np.zeros(n, np.int64)
+    t = tables.c_struct()
+    check(lib().mqct_propagate_batch_rec(C.byref(t), _traj_array(trajs), n, arith, max_rec, amp,
+                                         cls, diag, rec, n_rec))
+    if (n_rec > max_rec).any():
+        raise MqctError(-1, f"{int(n_rec.max())} records exceed max_rec={max_rec}")
+    rec = rec.reshape(n, max_rec, 8)
+    paths = [rec[i, :n_rec[i]].copy() for i in range(n)]
+    return amp.reshape(n, 2 * N), cls.reshape(n, 6), diag.reshape(n, 8), paths
 
 
 class PropagationPlan:
@@ -510,16 +550,19 @@ def channel_probabilities(amp, indx_chann, n_channels):
     return out
 
 
-def cross_sections(prob, j_ini, J_down, J_up, L_min, k_vec, U_cm=None, e_ch=None, chann_ini=1):
-    """INELAST_CALC for DL=1 (MQCT_SOURCE_CODES/propagator.f:4776-4841):
-    sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(l), in Angstrom^2
-    (sigma(U) column of CROSS_SECTIONS.out).  With U_cm and e_ch also returns the
-    Billing-corrected sigma(E_coll) (MQCT_SOURCE_CODES/propagator.f:1207-1208, 276-286)."""
+def cross_sections(prob, j_ini, J_down, J_up, L_min, k_vec, U_cm=None, e_ch=None, chann_ini=1,
+                   dl=1):
+    """INELAST_CALC (MQCT_SOURCE_CODES/propagator.f:4776-4841):
+    sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(traj(l)), in Angstrom^2
+    (sigma(U) column of CROSS_SECTIONS.out), traj(l) = (l - L_MIN) / DL the trajectory of
+    l's bin (TRAJ_ORB, MQCT_SOURCE_CODES/propagator.f:5127-5134).  With U_cm and e_ch also
+    returns the Billing-corrected sigma(E_coll) (MQCT_SOURCE_CODES/propagator.f:1207-1208,
+    276-286)."""
     n_traj, nch = prob.shape
     sig = np.zeros(nch)
     for J in range(J_down, J_up + 1):
         for l in range(abs(J - j_ini), J + j_ini + 1):
-            i = l - L_min
+            i = (l - L_min) // dl
             if 0 <= i < n_traj:
                 sig += prob[i] * (2.0 * J + 1.0) / k_vec ** 2 / (2.0 * j_ini + 1) * np.pi
     sig_U = sig * A_BOHR ** 2

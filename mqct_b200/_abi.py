@@ -80,6 +80,7 @@ EXPORTS = [
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
+    "mqct_propagate_batch_rec",
     "mqct_surrogate_create", "mqct_surrogate_train", "mqct_surrogate_predict",
     "mqct_surrogate_n_params", "mqct_surrogate_get_params", "mqct_surrogate_loss_grad",
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
@@ -122,7 +123,7 @@ def lib():
     L.mqct_spline_y2_noalloc.argtypes = [vp, C.c_int32, vp, vp, C.c_int64, vp, vp]
     L.mqct_build_matrix_expansion.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
                                               C.c_int32, i32p, f64p, C.c_double, C.c_double,
-                                              C.c_double, f64p, vp, vp]
+                                              C.c_double, C.c_double, f64p, vp, vp]
     L.mqct_surrogate_create.argtypes = [C.c_int32, C.POINTER(Pes), C.c_int32, C.c_int32,
                                         C.c_uint64, C.c_double, C.c_double, C.POINTER(vp)]
     L.mqct_surrogate_train.argtypes = [vp, C.c_int64, C.c_int32, C.c_int32, C.c_double, vp, vp]
@@ -139,6 +140,10 @@ def lib():
     L.mqct_propagate_batch.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
                                        C.c_int32, C.POINTER(AtPaths), C.c_int32, f64p, f64p,
                                        f64p]
+    L.mqct_propagate_batch_rec.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
+                                           C.c_int32, C.c_int64, f64p, f64p, f64p, f64p,
+                                           np.ctypeslib.ndpointer(dtype=np.int64,
+                                                                  flags="C_CONTIGUOUS")]
     L.mqct_prop_plan_create.argtypes = [C.POINTER(Tables), C.c_int32, C.POINTER(vp)]
     L.mqct_prop_plan_run.argtypes = [vp, C.POINTER(TrajInit), C.c_int64, f64p, f64p, f64p]
     L.mqct_prop_plan_run_device.argtypes = [vp, vp, C.c_int64, vp, vp, vp]

@@ -1271,15 +1271,14 @@ extern "C" int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t*
 
 // ------------------------------------------------------------------ PES-expansion path
 // Matrix elements from PES expansion terms (the READ_EXPANSION path of the
-// reference, EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6465-8749;
-// asymmetric top + diatom, case 8 at :7826-8058):
-//   M_k(R) = c_k sum_t T_t(R) A_{k,t}
+// reference, EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6465-8749):
+//   M_k(R) = e_unit c_k sum_t T_t(R) A_{k,t}
 // with R-independent angular coefficients A (products of Clebsch-Gordan
-// coefficients and rotor eigenvectors, see expansion_angular_kernel) and
-// c_k = sqrt((2 j1''+1)/(2 j1'+1)) sqrt((2 j2''+1)/(2 j2'+1)).  A is formed on the
-// GPU (one thread per (pair, term)), the sum over terms is an FP64 contraction,
-// and the fused finalize converts to Hartree, applies MIJ_CUTOFF and fits the
-// spline.
+// coefficients and rotor eigenvectors, see expansion_angular_kernel),
+// c_k = sqrt((2 j1''+1)/(2 j1'+1)) sqrt((2 j2''+1)/(2 j2'+1)) and e_unit the
+// Hartree value of the terms' energy unit.  A is formed on the GPU (one thread
+// per (pair, term)), the sum over terms is an FP64 contraction, and the fused
+// finalize applies MIJ_CUTOFF and fits the spline.
 
 // <j1 m1 j2 m2 | J M> by Racah's closed form with the log-factorial table.
 __device__ inline double cg_dev(int j1, int m1, int j2, int m2, int J, int M) {
@@ -1302,20 +1301,40 @@ __device__ inline double cg_dev(int j1, int m1, int j2, int m2, int J, int M) {
 
 __device__ inline bool triangle_ok(int a, int b, int c) { return c >= abs(a - b) && c <= a + b; }
 
-// A[k * n_terms + t] (times c_k) for SYS_TYPE 8; p = ind_mat[2k] - 1, pp = ind_mat[2k+1] - 1.
-//   A = sqrt((2l1+1)(2l2+1))/(4 pi) <j2'' 0 l2 0|j2' 0> M1 M3, with
-//   M1 = sum over nju = nju1 and (nju1 != 0) -nju1, phase (-1)^(l1+l2+l+nju1) on the
-//        second, of sum_{k1'} <j1'' k1'-nju l1 nju|j1' k1'> c'_{k1'} c''_{k1'-nju},
+// sum_{k'} <j'' k'-nju l nju|j' k'> c'_{k'} c''_{k'-nju}: one rotor's projection sum.
+__device__ inline double rotor_sum(int jpp, int l, int jp, int nju, const double* vp,
+                                   const double* vpp) {
+  double s = 0.0;
+  for (int kp = -jp; kp <= jp; ++kp) {
+    const int kpp = kp - nju;
+    if (abs(kpp) > jpp) continue;
+    s += cg_dev(jpp, kpp, l, nju, jp, kp) * vp[jp + kp] * vpp[jpp + kpp];
+  }
+  return s;
+}
+
+// A[k * n_terms + t] (times c_k) for term t = (l1, nju1, l2, nju2, l) = lab5[5t..5t+4];
+// p = ind_mat[2k] - 1 (stp), pp = ind_mat[2k+1] - 1 (stpp), m = m12(p).
+//   A = pref sqrt((2l1+1)(2l2+1)) K M3 with
+//   K  = sum over (nju1, nju2) and, unless both vanish, (-nju1, -nju2) with the
+//        phase (-1)^(l1+l2+l+nju1+nju2) on the second, of S1 S2,
+//        S1 = sum_{k1'} <j1'' k1'-nju1 l1 nju1|j1' k1'> c1'_{k1'} c1''_{k1'-nju1},
+//        S2 the same for rotor 2 with (l2, nju2),
 //   M3 = sum_{m'} <j1' m' j2' m-m'|j12' m> sum_{me} <l1 me l2 -me|l 0>
 //        <j1'' m'' j2'' m-m''|j12'' m> <j1'' m'' l1 me|j1' m'> <j2'' m-m'' l2 -me|j2' m-m'>,
 //        m'' = m' - me.
+// Two asymmetric tops (case 0, :8257-8672): pref = 1/(8 pi^2).  Asymmetric top +
+// diatom (case 8, :7826-8058): rotor 2's vector is the unit vector at K = 0 and
+// nju2 = 0, so S2 = <j2'' 0 l2 0|j2' 0> and pref = 1/(4 pi).
 __global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
                                          const int* __restrict__ st_chan,
                                          const int* __restrict__ st_j12,
                                          const int* __restrict__ st_m, const int* __restrict__ ch_j1,
                                          const int* __restrict__ ch_j2,
-                                         const double* __restrict__ vec, int ldv,
-                                         const int* __restrict__ labels, double* __restrict__ A) {
+                                         const double* __restrict__ vec1, int ldv1,
+                                         const double* __restrict__ vec2, int ldv2,
+                                         const int* __restrict__ lab5, double pref,
+                                         double* __restrict__ A) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= P * n_terms) return;
   const int64_t k = idx / n_terms;
@@ -1324,26 +1343,24 @@ __global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __re
   const int cp = st_chan[sp], cpp = st_chan[spp];
   const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
   const int j12p = st_j12[sp], j12pp = st_j12[spp], m = st_m[sp];
-  const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
-            l = labels[4 * t + 3];
+  const int l1 = lab5[5 * t], nju1 = lab5[5 * t + 1], l2 = lab5[5 * t + 2],
+            nju2 = lab5[5 * t + 3], l = lab5[5 * t + 4];
   double a = 0.0;
   if (triangle_ok(j1pp, l1, j1p) && triangle_ok(l1, l2, l) && triangle_ok(j2pp, l2, j2p)) {
-    const double* vp = vec + (size_t)cp * ldv;
-    const double* vpp = vec + (size_t)cpp * ldv;
-    double m1 = 0.0;
-    for (int planar = 0; planar < (nju1 == 0 ? 1 : 2); ++planar) {
-      const int nju = planar ? -nju1 : nju1;
-      const double phase = planar ? (((l1 + l2 + l + nju1) & 1) ? -1.0 : 1.0) : 1.0;
-      double sum = 0.0;
-      for (int k1p = -j1p; k1p <= j1p; ++k1p) {
-        const int k1pp = k1p - nju;
-        if (abs(k1pp) > j1pp) continue;
-        sum += cg_dev(j1pp, k1pp, l1, nju, j1p, k1p) * vp[j1p + k1p] * vpp[j1pp + k1pp];
-      }
-      m1 += phase * sum;
+    const double* v1p = vec1 + (size_t)cp * ldv1;
+    const double* v1pp = vec1 + (size_t)cpp * ldv1;
+    const double* v2p = vec2 + (size_t)cp * ldv2;
+    const double* v2pp = vec2 + (size_t)cpp * ldv2;
+    double kt = 0.0;
+    const int n_planar = (nju1 == 0 && nju2 == 0) ? 1 : 2;
+    for (int planar = 0; planar < n_planar; ++planar) {
+      const int n1 = planar ? -nju1 : nju1, n2 = planar ? -nju2 : nju2;
+      const double phase = planar ? (((l1 + l2 + l + nju1 + nju2) & 1) ? -1.0 : 1.0) : 1.0;
+      const double s1 = rotor_sum(j1pp, l1, j1p, n1, v1p, v1pp);
+      if (s1 != 0.0) kt += phase * s1 * rotor_sum(j2pp, l2, j2p, n2, v2p, v2pp);
     }
     double m3 = 0.0;
-    if (m1 != 0.0) {
+    if (kt != 0.0) {
       const int mx = l1 < l2 ? l1 : l2;
       for (int mp = -j1p; mp <= j1p; ++mp) {
         if (abs(m - mp) > j2p) continue;
@@ -1357,58 +1374,76 @@ __global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __re
         m3 += m2 * cg_dev(j1p, mp, j2p, m - mp, j12p, m);
       }
     }
-    a = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (4.0 * kPi) * cg_dev(j2pp, 0, l2, 0, j2p, 0) *
-        m1 * m3 * sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
-        sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+    a = pref * sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) * kt * m3 *
+        sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) * sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
   }
   A[idx] = a;
 }
 
-// M[k * nR + i] = sum_t A[k, t] T[i, t] (fixed order); one CTA per pair.
-__global__ void expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
-                                          const double* __restrict__ T, double* __restrict__ M) {
+// M[k * nR + i] = sum_t A[k, t] T[t * nR + i] (fixed order); one CTA per pair, the
+// pair's coefficients staged in shared memory, threads along R (coalesced T rows).
+__global__ void __launch_bounds__(128)
+expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
+                          const double* __restrict__ T, double* __restrict__ M) {
+  extern __shared__ double ex_a[];
   const int64_t k = blockIdx.x;
-  const double* a = A + k * n_terms;
+  for (int t = threadIdx.x; t < n_terms; t += blockDim.x) ex_a[t] = A[k * n_terms + t];
+  __syncthreads();
   for (int i = threadIdx.x; i < nR; i += blockDim.x) {
-    const double* ti = T + (size_t)i * n_terms;
     double s = 0.0;
-    for (int t = 0; t < n_terms; ++t) s = fma(a[t], ti[t], s);
+    for (int t = 0; t < n_terms; ++t) s = fma(ex_a[t], T[(size_t)t * nR + i], s);
     M[k * nR + i] = s;
   }
 }
 
 extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
                                            const double* R, int32_t nR, int32_t n_terms,
-                                           const int32_t* labels, const double* terms,
+                                           const int32_t* a_top, const double* terms, double e_unit,
                                            double mij_cutoff_cm, double r_cut1, double r_cut2,
                                            double* Mat_el, double* Mat_el_y2, int32_t* skipped) {
-  MQCT_ARG_CHECK(sys && ind_mat && R && labels && terms && Mat_el, "null argument");
-  MQCT_ARG_CHECK(sys->sys_type == 8, "the expansion path supports SYS_TYPE 8 (got %d)",
-                 sys->sys_type);
+  MQCT_ARG_CHECK(sys && ind_mat && R && a_top && terms && Mat_el, "null argument");
+  const int type = sys->sys_type;
+  MQCT_ARG_CHECK(type == 8 || type == 0,
+                 "the expansion path supports SYS_TYPE 8 and 0 (got %d)", type);
   MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->vec1 && sys->ldv > 0 && sys->indx_chann && sys->j12 &&
-                     sys->m12 && sys->n_states > 0,
+                     sys->m12 && sys->n_states > 0 && (type != 0 || sys->vec2),
                  "system arrays missing");
-  MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && nR >= 2 && nR <= 3072,
-                 "bad sizes");
+  MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && n_terms <= 4096 && nR >= 2 &&
+                     nR <= 3072,
+                 "bad sizes (n_terms <= 4096, 2 <= nR <= 3072)");
+  MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
   for (int i = 0; i + 1 < nR; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
+  // canonical labels (l1, nju1, l2, nju2, l); A_TOP columns: case 8 (l1, nju1, l2, l),
+  // case 0 (l1, nju1, l2, nju2, l) (MQCT_SOURCE_CODES/pot_comp.f:6322-6338)
+  std::vector<int> lab5(5 * (size_t)n_terms);
   for (int t = 0; t < n_terms; ++t) {
-    const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
-              l = labels[4 * t + 3];
-    // the log-factorial table (128 entries) bounds every Clebsch-Gordan argument sum
-    MQCT_ARG_CHECK(l1 >= 0 && l2 >= 0 && l >= 0 && nju1 >= 0 && nju1 <= l1 && l1 <= 30 &&
-                       l2 <= 30 && l <= 60,
-                   "bad expansion term %d (%d, %d, %d, %d): nju1 in 0..l1, l1, l2 <= 30, l <= 60",
-                   t + 1, l1, nju1, l2, l);
+    const int* c = a_top + 5 * t;
+    const int l1 = c[0], nju1 = c[1], l2 = c[2];
+    const int nju2 = type == 0 ? c[3] : 0, l = type == 0 ? c[4] : c[3];
+    // the log-factorial table (128 entries) bounds every Clebsch-Gordan argument sum;
+    // the sign rules are the reference's input checks (:7620-7633, :8288-8302)
+    MQCT_ARG_CHECK(l1 >= 0 && l2 >= 0 && l >= 0 && l1 <= 30 && l2 <= 30 && l <= 60 &&
+                       nju1 >= 0 && nju1 <= l1 && abs(nju2) <= l2 && !(nju1 == 0 && nju2 < 0),
+                   "bad expansion term %d (l1=%d nju1=%d l2=%d nju2=%d l=%d): l1, l2 <= 30, "
+                   "l <= 60, 0 <= nju1 <= l1, |nju2| <= l2, nju2 >= 0 when nju1 = 0",
+                   t + 1, l1, nju1, l2, nju2, l);
+    int* o = &lab5[5 * (size_t)t];
+    o[0] = l1; o[1] = nju1; o[2] = l2; o[3] = nju2; o[4] = l;
   }
-  const int n_states = sys->n_states;
+  const int n_states = sys->n_states, n_ch = sys->n_channels;
   std::vector<int> st_chan(n_states);
+  int j2max = 0;
+  for (int c = 0; c < n_ch; ++c) {
+    MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 && sys->j2[c] >= 0 && sys->j2[c] <= 30 &&
+                       2 * sys->j1[c] + 1 <= sys->ldv &&
+                       (type != 0 || 2 * sys->j2[c] + 1 <= sys->ldv),
+                   "bad channel %d (j1, j2 <= 30, 2j + 1 <= ldv)", c + 1);
+    j2max = std::max(j2max, sys->j2[c]);
+  }
   for (int s = 0; s < n_states; ++s) {
     st_chan[s] = sys->indx_chann[s] - 1;
-    MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < sys->n_channels, "indx_chann out of range");
+    MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < n_ch, "indx_chann out of range");
     const int ch = st_chan[s];
-    MQCT_ARG_CHECK(sys->j1[ch] >= 0 && sys->j1[ch] <= 30 && sys->j2[ch] >= 0 &&
-                       sys->j2[ch] <= 30 && 2 * sys->j1[ch] + 1 <= sys->ldv,
-                   "bad channel %d (j1, j2 <= 30)", ch + 1);
     MQCT_ARG_CHECK(sys->j12[s] >= abs(sys->j1[ch] - sys->j2[ch]) &&
                        sys->j12[s] <= sys->j1[ch] + sys->j2[ch] && abs(sys->m12[s]) <= sys->j12[s],
                    "bad (j12, m12) at state %d", s + 1);
@@ -1419,6 +1454,15 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
     MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
                    (long long)k + 1);
   }
+  // rotor 2: the asymmetric-top vectors (case 0) or the diatom's unit vector at K = 0
+  int ldv2 = sys->ldv;
+  std::vector<double> vec2_diatom;
+  if (type == 8) {
+    ldv2 = 2 * j2max + 1;
+    vec2_diatom.assign((size_t)n_ch * ldv2, 0.0);
+    for (int c = 0; c < n_ch; ++c) vec2_diatom[(size_t)c * ldv2 + sys->j2[c]] = 1.0;
+  }
+  const double pref = type == 0 ? 1.0 / (8.0 * kPi * kPi) : 1.0 / (4.0 * kPi);
   if (mqct_device_count() <= 0) {
     set_error("no CUDA device available");
     return MQCT_E_NODEV;
@@ -1431,17 +1475,19 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
     cudaStream_t s;
     ~StreamGuard() { cudaStreamDestroy(s); }
   } guard{st};
-  std::vector<int> ch_j1(sys->j1, sys->j1 + sys->n_channels), ch_j2(sys->j2, sys->j2 + sys->n_channels);
+  std::vector<int> ch_j1(sys->j1, sys->j1 + n_ch), ch_j2(sys->j2, sys->j2 + n_ch);
   DevBuf<int> d_ind, d_chan, d_j12, d_m, d_j1, d_j2, d_lab, d_k2r, d_sk;
-  DevBuf<double> d_vec, d_T, d_A, d_M, d_mat, d_y2, d_gc;
+  DevBuf<double> d_vec1, d_vec2, d_T, d_A, d_M, d_mat, d_y2, d_gc;
   MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
   MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
   MQCT_CUDA_TRY(d_j12.upload(sys->j12, n_states, st));
   MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
   MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
   MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
-  MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)sys->n_channels * sys->ldv, st));
-  MQCT_CUDA_TRY(d_lab.upload(labels, 4 * (size_t)n_terms, st));
+  MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * sys->ldv, st));
+  if (type == 8) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
+  else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));
+  MQCT_CUDA_TRY(d_lab.upload(lab5, st));
   MQCT_CUDA_TRY(d_T.upload(terms, (size_t)nR * n_terms, st));
   std::vector<double> Rh(R, R + nR);
   MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
@@ -1455,15 +1501,16 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
   MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
   const int64_t n_at = P * n_terms;
   expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
-      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec.p, sys->ldv, d_lab.p,
-      d_A.p);
+      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, sys->ldv, d_vec2.p,
+      ldv2, d_lab.p, pref, d_A.p);
   MQCT_CUDA_TRY(cudaGetLastError());
-  expansion_contract_kernel<<<(unsigned)P, 128, 0, st>>>(n_terms, nR, d_A.p, d_T.p, d_M.p);
+  expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
+      n_terms, nR, d_A.p, d_T.p, d_M.p);
   MQCT_CUDA_TRY(cudaGetLastError());
   const int ir1 = nearest_index(Rh, r_cut1), ir2 = nearest_index(Rh, r_cut2);
   finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
-      P, nR, d_k2r.p, d_M.p, 1, 0, nR, kCmToHartree, nullptr, ir1, ir2,
-      mij_cutoff_cm * kCmToHartree, d_gc.p, d_mat.p, d_sk.p, Mat_el_y2 ? d_y2.p : nullptr);
+      P, nR, d_k2r.p, d_M.p, 1, 0, nR, e_unit, nullptr, ir1, ir2, mij_cutoff_cm * kCmToHartree,
+      d_gc.p, d_mat.p, d_sk.p, Mat_el_y2 ? d_y2.p : nullptr);
   MQCT_CUDA_TRY(cudaGetLastError());
   MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el, d_mat.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, st));
   if (Mat_el_y2)

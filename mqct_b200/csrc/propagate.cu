@@ -85,16 +85,33 @@ struct PropDev {
   const double* at_y2;         // per record 4 second derivatives (R, theta, P_theta, P_phi)
 };
 
-struct TrajOut {
-  double* amp;
-  double* cls;
-  double* diag;
-};
-
 // Classical variables (R, P_R, theta, P_theta, phi, P_phi).
 struct Cls {
   double R, PR, th, Pth, phi, Pphi;
 };
+
+struct TrajOut {
+  double* amp;
+  double* cls;
+  double* diag;
+  // SAVE_TRAJECT records (standard mode; null: none): rec_cap records of 8 doubles per
+  // trajectory, n_rec the count produced (records past rec_cap are counted, not written)
+  double* rec;
+  int64_t rec_cap;
+  int64_t* n_rec;
+};
+
+// One SAVE_TRAJECT record (t, R, P_R, theta, P_theta, phi, P_phi, pot),
+// MQCT_SOURCE_CODES/propagator.f:3458-3464 and 4329-4337.
+__device__ inline void save_record(const TrajOut& o, int tr, int64_t& n, double t, const Cls& c,
+                                   double pot) {
+  if (n < o.rec_cap) {
+    double* r = o.rec + ((size_t)tr * o.rec_cap + n) * 8;
+    r[0] = t; r[1] = c.R; r[2] = c.PR; r[3] = c.th; r[4] = c.Pth; r[5] = c.phi; r[6] = c.Pphi;
+    r[7] = pot;
+  }
+  ++n;
+}
 
 // Shared-memory layout of one CTA (dynamic).
 template <class T>
@@ -410,6 +427,7 @@ __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc)
 // Per-trajectory bookkeeping of thread 0 (shared memory).
 struct Book {
   double tmpR1, tmpR2, eki, eqi;
+  int64_t n_rec;
   int status, vib, period, run;
 };
 
@@ -468,7 +486,7 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
     if (tid == 0) {
       const double k_vec = sqrt(d.mass * 2.0 * ti->e_coll);
       const double l_orb = sqrt(ti->l_real * (ti->l_real + 1.0));
-      *bk = Book{0.0, 0.0, 0.0, 0.0, 0, 0, 0, 1};
+      *bk = Book{0.0, 0.0, 0.0, 0.0, 0, 0, 0, 0, 1};
       *C = Cls{};
       if (!at && l_orb / k_vec > ti->r_start) {
         bk->status = 2;  // impact parameter beyond the starting distance: not propagated
@@ -513,7 +531,11 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
         if (st == 0) {
 #pragma unroll
           for (int q = 0; q < NS; ++q) k1[q] = k[q];
-          if (tid == 0) *K1 = *KC;
+          if (tid == 0) {
+            *K1 = *KC;
+            // the state before the step, with its coupling energy
+            if (out.rec && !at) save_record(out, tr, bk->n_rec, tcur, *C, potv);
+          }
           if (counter == 1 && !at) {  // initial energies, MQCT_SOURCE_CODES/propagator.f:2695-2810
             double q0 = 0.0, z1 = 0.0, z2 = 0.0;
 #pragma unroll
@@ -597,6 +619,8 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
         }
       block_sum3(eqf, z1, z2, sm.red);
       eerr = fabs(eqf + kinetic(*C, d.mass) + pot_end - bk->eki - bk->eqi);
+      // the closing record carries the final state stamped one step later
+      if (tid == 0 && out.rec) save_record(out, tr, bk->n_rec, tcur + dt, *C, pot_end);
     }
     double nrm = 0.0, z1 = 0.0, z2 = 0.0;
 #pragma unroll
@@ -624,6 +648,7 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
       dg[5] = bk->period;
       dg[6] = bk->vib;
       dg[7] = pot_end;
+      if (out.n_rec) out.n_rec[tr] = bk->n_rec;
     }
   }
 }
@@ -870,11 +895,12 @@ struct PropPlan {
   double bytes_per_step() const { return 4.0 * (double)S * (4.0 * tsize() + 4.0); }
 
   int launch(const mqct_traj_init_t* d_init_p, int64_t n_traj, int mode, double* amp,
-             double* cls, double* diag) {
+             double* cls, double* diag, double* rec = nullptr, int64_t rec_cap = 0,
+             int64_t* n_rec = nullptr) {
     MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 30), "n_traj out of range");
     MQCT_CUDA_TRY(cudaMemsetAsync(d_queue.p, 0, sizeof(int), stream));
     PropDev d = dev_view(mode);
-    TrajOut o{amp, cls, diag};
+    TrajOut o{amp, cls, diag, rec, rec_cap, n_rec};
     int n_traj_i = (int)n_traj;
     const size_t sb = smem_bytes();
     int per_sm = 1;
@@ -958,17 +984,32 @@ static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mod
   return MQCT_OK;
 }
 
-// Host-buffer run: upload the initial conditions, launch, copy the results back.
+// Host-buffer run: upload the initial conditions, launch, copy the results back
+// (and the SAVE_TRAJECT records when rec_out is given).
 static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, int mode,
-                    double* amp_out, double* cls_out, double* diag_out) {
+                    double* amp_out, double* cls_out, double* diag_out,
+                    double* rec_out = nullptr, int64_t rec_cap = 0, int64_t* n_rec_out = nullptr) {
   int rc = validate_init(init, n_traj, p->N, mode);
   if (rc) return rc;
   MQCT_CUDA_TRY(p->d_init.upload(init, n_traj, p->stream));
   MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
   MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
   MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
-  rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p);
+  DevBuf<double> d_rec;
+  DevBuf<int64_t> d_nrec;
+  if (rec_out) {
+    MQCT_CUDA_TRY(d_rec.alloc((size_t)n_traj * rec_cap * 8));
+    MQCT_CUDA_TRY(d_nrec.alloc((size_t)n_traj));
+  }
+  rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p, d_rec.p,
+                 rec_cap, d_nrec.p);
   if (rc) return rc;
+  if (rec_out) {
+    MQCT_CUDA_TRY(cudaMemcpyAsync(rec_out, d_rec.p, sizeof(double) * n_traj * rec_cap * 8,
+                                  cudaMemcpyDeviceToHost, p->stream));
+    MQCT_CUDA_TRY(cudaMemcpyAsync(n_rec_out, d_nrec.p, sizeof(int64_t) * n_traj,
+                                  cudaMemcpyDeviceToHost, p->stream));
+  }
   MQCT_CUDA_TRY(cudaMemcpyAsync(amp_out, p->d_amp.p, sizeof(double) * n_traj * 2 * p->N,
                                 cudaMemcpyDeviceToHost, p->stream));
   MQCT_CUDA_TRY(cudaMemcpyAsync(cls_out, p->d_cls.p, sizeof(double) * n_traj * 6,
@@ -1047,6 +1088,22 @@ int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
   rc = validate_init(init, n_traj, p->N, mode);
   if (!rc && mode == MQCT_MODE_AT) rc = p->set_at(at, n_traj);
   if (!rc) rc = run_host(p, init, n_traj, mode, amp_out, cls_out, diag_out);
+  mqct_prop_plan_destroy(h);
+  return rc;
+}
+
+int mqct_propagate_batch_rec(const mqct_tables_t* tab, const mqct_traj_init_t* init,
+                             int64_t n_traj, int32_t arith, int64_t max_rec, double* amp_out,
+                             double* cls_out, double* diag_out, double* rec_out,
+                             int64_t* n_rec_out) {
+  MQCT_ARG_CHECK(init && amp_out && cls_out && diag_out && rec_out && n_rec_out, "null argument");
+  MQCT_ARG_CHECK(max_rec > 0 && max_rec < ((int64_t)1 << 32), "max_rec out of range");
+  mqct_prop_plan* h = nullptr;
+  int rc = mqct_prop_plan_create(tab, arith, &h);
+  if (rc) return rc;
+  PropPlan* p = reinterpret_cast<PropPlan*>(h);
+  rc = run_host(p, init, n_traj, MQCT_MODE_STD, amp_out, cls_out, diag_out, rec_out, max_rec,
+                n_rec_out);
   mqct_prop_plan_destroy(h);
   return rc;
 }

@@ -1075,9 +1075,16 @@ static double orc_pot(orc_rhs_ws* w, double t, double R, const double* q) {
 /* DOTRAJECT, standard MQCT with fixed-step RK4: initial conditions
  * SRC/propagator.f:2435-2566, energies :2695-2810, loop :3205-4050,
  * final bookkeeping :4182-4383. */
-int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
-                  double* diag) {
+/* rec (optional, 8 doubles per record, max_rec records): the SAVE_TRAJECT
+ * records of the reference (SRC/propagator.f:3458-3464, 4329-4337): at the top
+ * of every step (t, R, P_R, theta, P_theta, phi, P_phi, pot) of the state before
+ * the step, pot the coupling energy; after the last step one more record of the
+ * final state stamped t_final + dt.  *n_rec receives the record count (the
+ * records past max_rec are counted but not written). */
+static int orc_dotraject_impl(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                              double* diag, double* rec, int64_t max_rec, int64_t* n_rec) {
   int N = tab->n_states;
+  int64_t nr = 0;
   int n = 2 * N + 8;
   double mass = tab->mass_au;
   double* q = (double*)calloc((size_t)n, sizeof(double));
@@ -1118,6 +1125,15 @@ int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double
     while (run) {
       ++counter;
       if (q[2 * N] != q[2 * N]) { status = 3; break; }
+      if (rec) {
+        if (nr < max_rec) {
+          double* r = rec + 8 * nr;
+          r[0] = tcur;
+          for (int c = 0; c < 6; ++c) r[1 + c] = q[2 * N + c];
+          r[7] = orc_pot(&w, tcur, q[2 * N], q);
+        }
+        ++nr;
+      }
       orc_derivs_ws(&w, tcur, q, dq);
       orc_rk4(n, q, dq, tcur, tr->dt, orc_rhs_std, &w, yt, dyt, dym);
       double uR = q[2 * N], uphi = q[2 * N + 4];
@@ -1146,7 +1162,17 @@ int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double
     pot_end = orc_pot(&w, tcur, R, q);
     eror = fabs(Eqf + Ef + pot_end - Eki - Eqi);
     norm_err = fabs(1.0 - Pt);
+    if (rec) {
+      if (nr < max_rec) {
+        double* r = rec + 8 * nr;
+        r[0] = tcur + tr->dt;
+        for (int c = 0; c < 6; ++c) r[1 + c] = q[2 * N + c];
+        r[7] = pot_end;
+      }
+      ++nr;
+    }
   }
+  if (n_rec) *n_rec = nr;
   for (int i = 0; i < 2 * N; ++i) amp[i] = q[i];
   for (int c = 0; c < 6; ++c) cls[c] = q[2 * N + c];
   diag[0] = tcur; diag[1] = (double)counter; diag[2] = norm_err; diag[3] = eror;
@@ -1154,6 +1180,15 @@ int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double
   orc_ws_free(&w);
   free(q); free(dq); free(yt); free(dyt); free(dym);
   return 0;
+}
+
+int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                  double* diag) {
+  return orc_dotraject_impl(tab, tr, amp, cls, diag, NULL, 0, NULL);
+}
+int orc_dotraject_rec(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                      double* diag, double* rec, int64_t max_rec, int64_t* n_rec) {
+  return orc_dotraject_impl(tab, tr, amp, cls, diag, rec, max_rec, n_rec);
 }
 
 int orc_propagate_batch(const orc_tables* tab, int n_traj, const orc_traj* trajs, int n_threads,
@@ -1274,11 +1309,19 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
  * index l - L_MIN): sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(l). */
 int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int n_traj,
                 const double* prob, double k_vec, double* sigma) {
+  return orc_inelast_dl(n_channels, j_ini, J_down, J_up, L_min, 1, n_traj, prob, k_vec, sigma);
+}
+/* With a step DL in l: trajectory id = (l - L_MIN) / DL (TRAJ_ORB flag 1,
+ * SRC/propagator.f:5127-5134), so every l of a bin takes the probability of the
+ * bin's trajectory, l = (id + 1/2) DL + L_MIN truncated (:5163-5167). */
+int orc_inelast_dl(int n_channels, int j_ini, int J_down, int J_up, int L_min, int dl,
+                   int n_traj, const double* prob, double k_vec, double* sigma) {
+  if (dl < 1) return -1;
   for (int f = 0; f < n_channels; ++f) {
     double s = 0.0;
     for (int J = J_down; J <= J_up; ++J)
       for (int l = abs(J - j_ini); l <= J + j_ini; ++l) {
-        int id = l - L_min;
+        int id = (l - L_min) / dl;
         if (id < 0 || id >= n_traj) continue;
         s += prob[(size_t)id * n_channels + f] * (2.0 * J + 1.0) / (k_vec * k_vec) /
              (2.0 * j_ini + 1) * ORC_PI;
@@ -1357,6 +1400,85 @@ int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
       for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
     }
     for (int i = 0; i < nR; ++i) out[i] *= coef12 * ORC_CM_TO_HARTREE;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* SRC/pot_comp.f:8257-8746 (EXPANSION_MATRIX_ELEMENT, SYS_TYPE 0, two asymmetric
+ * tops, partners distinguishable: the CG_jk_1 / M_coulp_1 branch).  For the pair
+ * (p = stp, pp = stpp) with total m and the term (l1, nju1, l2, nju2, l):
+ *   A_t = sqrt((2l1+1)(2l2+1))/(8 pi^2) K_t M3_t,
+ *   K_t = sum over (nju1, nju2) and, unless both vanish, (-nju1, -nju2) with the
+ *         phase (-1)^(l1+l2+l+nju1+nju2) for the second, of S1 S2 with
+ *         S1 = sum_{k1'} <j1'' k1'-nju1 l1 nju1|j1' k1'> c1'_{k1'} c1''_{k1'-nju1},
+ *         S2 = sum_{k2'} <j2'' k2'-nju2 l2 nju2|j2' k2'> c2'_{k2'} c2''_{k2'-nju2}
+ *         (:8388-8425, triangle rules of :8381-8382),
+ *   M3_t as for SYS_TYPE 8 (:8577-8650),
+ *   M_k(R) = e_unit sqrt((2j1''+1)/(2j1'+1)) sqrt((2j2''+1)/(2j2'+1)) sum_t T_t(R) A_t
+ * (:8653-8672; e_unit = conv_unit_e, SRC/matrix_ini.f:918-921). */
+int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double e_unit, double* mat) {
+  if (sys->sys_type != 0 || !sys->j2 || !sys->vec1 || !sys->vec2) return -1;
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t k = 0; k < P; ++k) {
+    const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+    const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
+    const int j1p = sys->j1[cp], j2p = sys->j2[cp], j1pp = sys->j1[cpp], j2pp = sys->j2[cpp];
+    const int j12p = j12[sp], j12pp = j12[spp], m = m12[sp];
+    const double* v1p = sys->vec1 + (size_t)cp * sys->ldv;
+    const double* v1pp = sys->vec1 + (size_t)cpp * sys->ldv;
+    const double* v2p = sys->vec2 + (size_t)cp * sys->ldv;
+    const double* v2pp = sys->vec2 + (size_t)cpp * sys->ldv;
+    const double coef12 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+    double* out = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) out[i] = 0.0;
+    for (int t = 0; t < n_terms; ++t) {
+      const int l1 = labels[5 * t], nju1 = labels[5 * t + 1], l2 = labels[5 * t + 2],
+                nju2 = labels[5 * t + 3], l = labels[5 * t + 4];
+      if (!orc_triangle(j1pp, l1, j1p) || !orc_triangle(j2pp, l2, j2p) || !orc_triangle(l1, l2, l))
+        continue;
+      const double coef3 = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (8.0 * ORC_PI * ORC_PI);
+      double kt = 0.0;
+      const int n_planar = (nju1 == 0 && nju2 == 0) ? 1 : 2;
+      for (int planar = 0; planar < n_planar; ++planar) {
+        const int n1 = planar ? -nju1 : nju1, n2 = planar ? -nju2 : nju2;
+        const double phase = planar ? (((l1 + l2 + l + nju1 + nju2) & 1) ? -1.0 : 1.0) : 1.0;
+        double s1 = 0.0, s2 = 0.0;
+        for (int k1p = -j1p; k1p <= j1p; ++k1p) {
+          const int k1pp = k1p - n1;
+          if (abs(k1pp) > j1pp) continue;
+          s1 += orc_cg(j1pp, l1, j1p, k1pp, n1, k1p) * v1p[j1p + k1p] * v1pp[j1pp + k1pp];
+        }
+        for (int k2p = -j2p; k2p <= j2p; ++k2p) {
+          const int k2pp = k2p - n2;
+          if (abs(k2pp) > j2pp) continue;
+          s2 += orc_cg(j2pp, l2, j2p, k2pp, n2, k2p) * v2p[j2p + k2p] * v2pp[j2pp + k2pp];
+        }
+        kt += phase * s1 * s2;
+      }
+      double m3 = 0.0;
+      for (int mp = -j1p; mp <= j1p; ++mp) {
+        if (abs(m - mp) > j2p) continue;
+        const double cg_p = orc_cg(j1p, j2p, j12p, mp, m - mp, m);
+        double m2 = 0.0;
+        const int mx = l1 < l2 ? l1 : l2;
+        for (int me = -mx; me <= mx; ++me) {
+          const int mpp = mp - me;
+          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+          m2 += orc_cg(l1, l2, l, me, -me, 0) * orc_cg(j1pp, j2pp, j12pp, mpp, m - mpp, m) *
+                orc_cg(j1pp, l1, j1p, mpp, me, mp) * orc_cg(j2pp, l2, j2p, m - mpp, -me, m - mp);
+        }
+        m3 += m2 * cg_p;
+      }
+      const double a = coef3 * kt * m3;
+      if (a == 0.0) continue;
+      for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
+    }
+    for (int i = 0; i < nR; ++i) out[i] *= coef12 * e_unit;
   }
   return 0;
 }

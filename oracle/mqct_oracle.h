@@ -154,6 +154,11 @@ int orc_dotraject(const orc_tables* tab, const orc_traj* tr, double* amp, double
                   double* diag);
 int orc_propagate_batch(const orc_tables* tab, int n_traj, const orc_traj* trajs,
                         int n_threads, double* amp, double* cls, double* diag);
+/* DOTRAJECT with the SAVE_TRAJECT records (8 doubles each: t, R, P_R, theta,
+ * P_theta, phi, P_phi, pot) of the state at the top of every step plus the final
+ * state stamped t_final + dt; *n_rec = records produced (written up to max_rec). */
+int orc_dotraject_rec(const orc_tables* tab, const orc_traj* tr, double* amp, double* cls,
+                      double* diag, double* rec, int64_t max_rec, int64_t* n_rec);
 /* AT-MQCT: classical path given as n_at records (t,R,P_R,theta,P_theta,phi,P_phi,pot). */
 int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at,
                      const double* at_rec, double* amp, double* diag);
@@ -164,6 +169,9 @@ int orc_derivs(const orc_tables* tab, double t, const double* q, double* dqdt);
  * prob[n_traj*n_channels] -> sigma_bohr2[n_channels] (pi/k^2 * sum (2J+1)/(2j+1) P). */
 int orc_inelast(int n_channels, int j_ini, int J_down, int J_up, int L_min, int n_traj,
                 const double* prob, double k_vec, double* sigma);
+/* The same with trajectories every dl values of l (trajectory id = (l - L_min)/dl). */
+int orc_inelast_dl(int n_channels, int j_ini, int J_down, int J_up, int L_min, int dl,
+                   int n_traj, const double* prob, double k_vec, double* sigma);
 
 /* PES-expansion matrix elements of SYS_TYPE 8 (asymmetric top + diatom),
  * SRC/pot_comp.f:7826-8058 (EXPANSION_MATRIX_ELEMENT, case 8): per stored pair k
@@ -174,6 +182,14 @@ int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
                                const int32_t* j12, const int32_t* m12, int64_t P,
                                const int32_t* ind_mat, int n_terms, const int32_t* labels,
                                int nR, const double* terms, double* mat);
+
+/* SYS_TYPE 0 (two asymmetric tops, distinguishable), SRC/pot_comp.f:8257-8746:
+ * labels[5t .. 5t+4] = (l1, nju1, l2, nju2, l) (the A_TOP columns), terms in the
+ * file's energy unit, e_unit = Hartree per that unit. */
+int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double e_unit, double* mat);
 
 #ifdef __cplusplus
 }

@@ -117,6 +117,14 @@ def lib():
                                        f64p]
         L.orc_inelast.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, f64p,
                                   C.c_double, f64p]
+        L.orc_inelast_dl.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_int, f64p, C.c_double, f64p]
+        L.orc_dotraject_rec.argtypes = [C.POINTER(Tables), C.POINTER(Traj), f64p, f64p, f64p,
+                                        f64p, C.c_int64, C.POINTER(C.c_int64)]
+        L.orc_expansion_matrix_type0.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
+                                                 C.c_void_p, C.c_int, C.c_void_p, C.c_double,
+                                                 C.c_void_p]
         _lib = L
     return _lib
 
@@ -336,11 +344,29 @@ def derivs(tables, t, q):
     return dq
 
 
-def inelast(n_channels, j_ini, J_down, J_up, L_min, prob, k_vec):
+def inelast(n_channels, j_ini, J_down, J_up, L_min, prob, k_vec, dl=1):
     sig = np.zeros(n_channels)
     p = np.ascontiguousarray(prob, np.float64)
-    lib().orc_inelast(n_channels, j_ini, J_down, J_up, L_min, p.shape[0], p.reshape(-1), k_vec, sig)
+    rc = lib().orc_inelast_dl(n_channels, j_ini, J_down, J_up, L_min, dl, p.shape[0],
+                              p.reshape(-1), k_vec, sig)
+    if rc:
+        raise RuntimeError(f"orc_inelast_dl failed: {rc}")
     return sig
+
+
+def dotraject_record(tables, traj, max_rec=1 << 20):
+    """DOTRAJECT with SAVE_TRAJECT: (amp, cls, diag, records n x 8)."""
+    N = len(tables.j12)
+    amp = np.zeros(2 * N)
+    cls = np.zeros(6)
+    diag = np.zeros(8)
+    rec = np.zeros(8 * max_rec)
+    n = C.c_int64(0)
+    lib().orc_dotraject_rec(C.byref(tables.s), C.byref(traj), amp, cls, diag, rec, max_rec,
+                            C.byref(n))
+    if n.value > max_rec:
+        raise RuntimeError(f"{n.value} records exceed max_rec={max_rec}")
+    return amp, cls, diag, rec[:8 * n.value].reshape(n.value, 8)
 
 
 def expansion_matrix_type8(osys, states, ind, labels, terms):
@@ -356,4 +382,22 @@ def expansion_matrix_type8(osys, states, ind, labels, terms):
                                           _ptr(labels.reshape(-1)), nR, _ptr(terms), _ptr(mat))
     if rc:
         raise RuntimeError(f"orc_expansion_matrix_type8 failed: {rc}")
+    return mat.reshape(P, nR)
+
+
+def expansion_matrix_type0(osys, states, ind, labels, terms, e_unit):
+    """SYS_TYPE 0 matrix (P x nR, Hartree) from PES expansion terms (nR x n_terms, in the
+    unit e_unit Hartree); labels n_terms x 5 (l1, nju1, l2, nju2, l)."""
+    ic, j12, m12, _ = states
+    ind = np.ascontiguousarray(ind, np.int32)
+    labels = np.ascontiguousarray(labels, np.int32).reshape(-1, 5)
+    terms = np.ascontiguousarray(terms, np.float64)
+    P, nR = ind.shape[0], terms.shape[0]
+    mat = np.zeros(P * nR)
+    rc = lib().orc_expansion_matrix_type0(C.byref(osys.s), _ptr(ic), _ptr(j12), _ptr(m12), P,
+                                          _ptr(ind.reshape(-1)), labels.shape[0],
+                                          _ptr(labels.reshape(-1)), nR, _ptr(terms), e_unit,
+                                          _ptr(mat))
+    if rc:
+        raise RuntimeError(f"orc_expansion_matrix_type0 failed: {rc}")
     return mat.reshape(P, nR)

@@ -9,6 +9,7 @@ also run where the reference tree is absent.
 from __future__ import annotations
 
 import os
+import re
 import struct
 import sys
 
@@ -110,6 +111,69 @@ def main(ref_root):
     np.savez_compressed(os.path.join(out, "g1_at_traj_l9.npz"), n_records=cnt,
                         head=recs[:8], tail=recs[-4:], n_file=len(recs),
                         t_span=np.array([recs[0, 0], recs[-1, 0]]))
+    # G1: two asymmetric tops (SYS_TYPE 0), H2O+H2O AT-MQCT in two runs
+    # (EXAMPLES_IO/SYS_TYPE_0/H2O_H2O_AT_Approximation).  Both runs build their
+    # matrix from the same PES_EXPAN_TERMS.DAT (empty header line, then one row per
+    # R: f6.2 R and 28 values in kcal/mol); the term labels (l1, nju1, l2, nju2, l)
+    # are the TERMS list of the input.  The 1st run (one channel, RK4 step 10)
+    # saves the classical paths (AT_APPROX_TRAJS, one file per l = 9, 28, ..., 256);
+    # the 2nd run (9 channels, AT_APPROX, step 100) propagates along them.  Kept:
+    # per path its record count and its first 4, middle 3 and last 3 records; the
+    # 2nd run's opacities, deflection table and cross sections.
+    base = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_AT_Approximation")
+    d1 = os.path.join(base, "AT_MQCT_1st_Step")
+    d2 = os.path.join(base, "AT_MQCT_2nd_Step")
+    inp = open(os.path.join(d2, "H2O_H2O_AT_MQCT_2nd_run.inp")).read()
+    tl = re.split(r"(?<![A-Z_])TERMS\s*=", inp)[1].split("$END")[0]
+    lab = np.array([int(x) for x in tl.replace(",", " ").split()], dtype=np.int32).reshape(-1, 5)
+    with open(os.path.join(d2, "PES_EXPAN_TERMS.DAT")) as f:
+        f.readline()
+        rows = np.array([[float(x) for x in ln.split()] for ln in f if ln.strip()])
+    tdir = os.path.join(d2, "AT_APPROX_TRAJS", "500.00000", "0", "0")
+    ls = np.arange(9, 257, 19)
+    n_rec, heads, mids, tails = [], [], [], []
+    for l in ls:
+        raw = open(os.path.join(tdir, f"AT_0_0_{l}_0"), "rb").read()
+        recs = []
+        off = 0
+        while off < len(raw):
+            n = struct.unpack_from("<i", raw, off)[0]
+            recs.append(struct.unpack_from("<8d", raw, off + 4))
+            off += n + 8
+        recs = np.array(recs)
+        n_rec.append(len(recs))
+        heads.append(recs[:4])
+        h = len(recs) // 2
+        mids.append(recs[h - 1:h + 2])
+        tails.append(recs[-3:])
+    sig2 = []
+    for line in open(os.path.join(d2, "CROSS_SECTIONS.out")):
+        t = line.split()
+        if len(t) == 5 and t[0].isdigit():
+            sig2.append(float(t[2]))
+    # M-resolved cross sections (channel 1 there is the probability sum of the
+    # initial channel; CROSS_SECTIONS.out reports ELAST_CALC's elastic value instead)
+    sig2m = []
+    for line in open(os.path.join(d2, "M_PROJ_CROSSECTIONS.out")):
+        t = line.split()
+        if len(t) == 2 and t[0].isdigit():
+            sig2m.append(float(t[1]))
+    np.savez_compressed(
+        os.path.join(out, "g1_h2o_h2o_at.npz"), labels=lab, R=rows[:, 0], terms=rows[:, 1:],
+        sigma2_mproj=np.array(sig2m),
+        l=ls, n_rec=np.array(n_rec), rec_head=np.array(heads), rec_mid=np.array(mids),
+        rec_tail=np.array(tails),
+        opacity2=_read_table(os.path.join(d2, "OPACITY_FUNCTIONS_L.out"), 11),
+        deflection1=_read_table(os.path.join(d1, "DEFLECTION_FUNCTION.out"), 9, first_int=False),
+        deflection2=_read_table(os.path.join(d2, "DEFLECTION_FUNCTION.out"), 9, first_int=False),
+        sigma2=np.array(sig2),
+        # $BASIS/$SYSTEM of the two inputs
+        A=27.87700, B=9.28500, C=14.51200, mass_red=9.00764, U=500.0, b_impct=30.0, rmax=30.0,
+        dl=19, time_step1=10.0, time_step2=100.0, time_lim=3.5e6,
+        channels=np.array([[0, 0, 0, 0, 0, 0], [0, 0, 0, 1, 1, 1], [0, 0, 0, 2, 0, 2],
+                           [1, 1, 1, 0, 0, 0], [1, 1, 1, 1, 1, 1], [1, 1, 1, 2, 0, 2],
+                           [2, 0, 2, 0, 0, 0], [2, 0, 2, 1, 1, 1], [2, 0, 2, 2, 0, 2]],
+                          dtype=np.int32))
     print("fixtures written to", out)
 
 
