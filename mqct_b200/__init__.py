@@ -43,6 +43,9 @@ class CollisionSystem:
 
     sys_type 1: channels (j,), energy BE j(j+1) - DE (j(j+1))^2 (MQCT_SOURCE_CODES/iotest.f:5454);
     sys_type 4: channels (j, ka, kc), energy EIGEN_VAL(A,B,C) (MQCT_SOURCE_CODES/iotest.f:6611-6618);
+    sys_type 7: channels (j1, k, eps, j2), A j1(j1+1) - (A-C) k^2 + BE j2(j2+1) - DE (j2(j2+1))^2
+    (MQCT_SOURCE_CODES/iotest.f:8311-8312); k and eps are kept in ka1 and kc1, and vec1 holds
+    the parity-adapted top (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) over K;
     sys_type 8: channels (j1, ka1, kc1, j2), EIGEN_VAL + BE j2(j2+1) (MQCT_SOURCE_CODES/iotest.f:9069-9079);
     sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..).
     """
@@ -79,6 +82,20 @@ class CollisionSystem:
                 self.j2 = np.ascontiguousarray(ch[:, 3])
                 jj = self.j2 * (self.j2 + 1.0)
                 E = E + BE * jj - DE * jj ** 2
+        elif sys_type == 7:
+            self.ka1 = np.ascontiguousarray(ch[:, 1])
+            self.kc1 = np.ascontiguousarray(ch[:, 2])
+            self.j2 = np.ascontiguousarray(ch[:, 3])
+            j1 = self.j1.astype(np.float64)
+            jj = self.j2 * (self.j2 + 1.0)
+            E = A * j1 * (j1 + 1.0) - (A - C) * self.ka1 ** 2.0 + BE * jj - DE * jj ** 2
+            for i in range(nch):
+                j, k, eps = int(ch[i, 0]), int(ch[i, 1]), int(ch[i, 2])
+                if not (0 <= k <= j and eps in (0, 1) and not (k == 0 and eps == 1)):
+                    raise ValueError(f"bad symmetric-top channel {tuple(ch[i])}")
+                a = 1.0 / np.sqrt(2.0 * (1.0 + (k == 0)))
+                self.vec1[i, j + k] += a
+                self.vec1[i, j - k] += -a if eps else a
         elif sys_type == 0:
             self.ka1, self.kc1 = np.ascontiguousarray(ch[:, 1]), np.ascontiguousarray(ch[:, 2])
             self.j2, self.ka2, self.kc2 = (np.ascontiguousarray(ch[:, 3]),
@@ -97,7 +114,7 @@ class CollisionSystem:
             raise ValueError(f"unsupported SYS_TYPE {sys_type}")
         self.e_ch = np.asarray(E if e_ch is None else e_ch, dtype=np.float64)
         L = lib()
-        j2p = ptr(self.j2) if sys_type in (8, 0) else None
+        j2p = ptr(self.j2) if sys_type in (7, 8, 0) else None
         n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
         self.indx_chann = np.zeros(n, np.int32)
         self.j12 = np.zeros(n, np.int32)
@@ -129,7 +146,7 @@ class CollisionSystem:
             cols += [self.j1[ic - 1]]
         elif self.sys_type == 4:
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1]]
-        elif self.sys_type == 8:
+        elif self.sys_type in (7, 8):
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1]]
         else:
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1],
@@ -256,9 +273,9 @@ E_UNIT = {"CM-1": CM_TO_HARTREE, "KCAL": 1.0 / 627.509469, "K": 1.0 / 1.1604519e
 
 def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",
                            mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
-    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 8 and 0).
+    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 7, 8 and 0).
 
-    labels: the TERMS list, one row per term: (l1, nju1, l2, l) for SYS_TYPE 8,
+    labels: the TERMS list, one row per term: (l1, nju1, l2, l) for SYS_TYPE 7 and 8,
     (l1, nju1, l2, nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
     PES_EXPAN_TERMS.DAT, in the unit e_unit (a key of E_UNIT or the Hartree value of
     one unit).  Returns (Mat_el, y2, skipped) as build_matrix."""

@@ -173,14 +173,14 @@ int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int
 }
 
 // States per channel: m = -j..j (types 1, 4) or j12 = |j1-j2|..j1+j2 with its m
-// (types 8, 0), channel-major (MQCT_SOURCE_CODES/matrix_ini.f:261-544).
+// (types 7, 8, 0), channel-major (MQCT_SOURCE_CODES/matrix_ini.f:148-173, 261-544).
 int mqct_count_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
                       const int32_t* j2) {
   if (n_channels <= 0 || !j1) return MQCT_E_ARG;
   int st = 0;
   for (int i = 0; i < n_channels; ++i) {
     if (sys_type == 1 || sys_type == 4) st += 2 * j1[i] + 1;
-    else if (sys_type == 8 || sys_type == 0) {
+    else if (sys_type == 7 || sys_type == 8 || sys_type == 0) {
       if (!j2) return MQCT_E_ARG;
       for (int js = abs(j1[i] - j2[i]); js <= j1[i] + j2[i]; ++js) st += 2 * js + 1;
     } else {

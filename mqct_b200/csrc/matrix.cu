@@ -1325,7 +1325,8 @@ __device__ inline double rotor_sum(int jpp, int l, int jp, int nju, const double
 //        m'' = m' - me.
 // Two asymmetric tops (case 0, :8257-8672): pref = 1/(8 pi^2).  Asymmetric top +
 // diatom (case 8, :7826-8058): rotor 2's vector is the unit vector at K = 0 and
-// nju2 = 0, so S2 = <j2'' 0 l2 0|j2' 0> and pref = 1/(4 pi).
+// nju2 = 0, so S2 = <j2'' 0 l2 0|j2' 0> and pref = 1/(4 pi).  Symmetric top + diatom
+// (case 7, :7593-7824): as case 8 with rotor 1's parity-adapted vector.
 __global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
                                          const int* __restrict__ st_chan,
                                          const int* __restrict__ st_j12,
@@ -1403,18 +1404,19 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
                                            double* Mat_el, double* Mat_el_y2, int32_t* skipped) {
   MQCT_ARG_CHECK(sys && ind_mat && R && a_top && terms && Mat_el, "null argument");
   const int type = sys->sys_type;
-  MQCT_ARG_CHECK(type == 8 || type == 0,
-                 "the expansion path supports SYS_TYPE 8 and 0 (got %d)", type);
-  MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->vec1 && sys->ldv > 0 && sys->indx_chann && sys->j12 &&
-                     sys->m12 && sys->n_states > 0 && (type != 0 || sys->vec2),
+  MQCT_ARG_CHECK(type == 7 || type == 8 || type == 0,
+                 "the expansion path supports SYS_TYPE 7, 8 and 0 (got %d)", type);
+  MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->indx_chann && sys->j12 && sys->m12 &&
+                     sys->n_states > 0 && (type == 7 || (sys->vec1 && sys->ldv > 0)) &&
+                     (type != 0 || sys->vec2) && (type != 7 || (sys->ka1 && sys->kc1)),
                  "system arrays missing");
   MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && n_terms <= 4096 && nR >= 2 &&
                      nR <= 3072,
                  "bad sizes (n_terms <= 4096, 2 <= nR <= 3072)");
   MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
   for (int i = 0; i + 1 < nR; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
-  // canonical labels (l1, nju1, l2, nju2, l); A_TOP columns: case 8 (l1, nju1, l2, l),
-  // case 0 (l1, nju1, l2, nju2, l) (MQCT_SOURCE_CODES/pot_comp.f:6322-6338)
+  // canonical labels (l1, nju1, l2, nju2, l); A_TOP columns: cases 7, 8 (l1, nju1, l2, l),
+  // case 0 (l1, nju1, l2, nju2, l) (MQCT_SOURCE_CODES/pot_comp.f:6317-6338)
   std::vector<int> lab5(5 * (size_t)n_terms);
   for (int t = 0; t < n_terms; ++t) {
     const int* c = a_top + 5 * t;
@@ -1432,12 +1434,20 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
   }
   const int n_states = sys->n_states, n_ch = sys->n_channels;
   std::vector<int> st_chan(n_states);
-  int j2max = 0;
+  int j1max = 0, j2max = 0;
   for (int c = 0; c < n_ch; ++c) {
     MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 && sys->j2[c] >= 0 && sys->j2[c] <= 30 &&
-                       2 * sys->j1[c] + 1 <= sys->ldv &&
+                       (type == 7 || 2 * sys->j1[c] + 1 <= sys->ldv) &&
                        (type != 0 || 2 * sys->j2[c] + 1 <= sys->ldv),
                    "bad channel %d (j1, j2 <= 30, 2j + 1 <= ldv)", c + 1);
+    if (type == 7)
+      MQCT_ARG_CHECK(sys->ka1[c] >= 0 && sys->ka1[c] <= sys->j1[c] &&
+                         (sys->kc1[c] == 0 || sys->kc1[c] == 1) &&
+                         !(sys->ka1[c] == 0 && sys->kc1[c] == 1),
+                     "bad symmetric-top channel %d (j=%d k=%d eps=%d): 0 <= k <= j, eps in {0, 1}, "
+                     "eps = 0 when k = 0",
+                     c + 1, sys->j1[c], sys->ka1[c], sys->kc1[c]);
+    j1max = std::max(j1max, sys->j1[c]);
     j2max = std::max(j2max, sys->j2[c]);
   }
   for (int s = 0; s < n_states; ++s) {
@@ -1454,10 +1464,25 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
     MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
                    (long long)k + 1);
   }
+  // rotor 1 of SYS_TYPE 7: the parity-adapted symmetric top
+  // (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) as a vector over K; with it
+  // the K-sum S1 is the four-term bracket of the reference (:7680-7707 with coef4)
+  int ldv1 = sys->ldv;
+  std::vector<double> vec1_sym;
+  if (type == 7) {
+    ldv1 = 2 * j1max + 1;
+    vec1_sym.assign((size_t)n_ch * ldv1, 0.0);
+    for (int c = 0; c < n_ch; ++c) {
+      const int j = sys->j1[c], kk = sys->ka1[c];
+      const double a = 1.0 / sqrt(2.0 * (1.0 + (kk == 0 ? 1.0 : 0.0)));
+      vec1_sym[(size_t)c * ldv1 + j + kk] += a;
+      vec1_sym[(size_t)c * ldv1 + j - kk] += (sys->kc1[c] & 1) ? -a : a;
+    }
+  }
   // rotor 2: the asymmetric-top vectors (case 0) or the diatom's unit vector at K = 0
   int ldv2 = sys->ldv;
   std::vector<double> vec2_diatom;
-  if (type == 8) {
+  if (type != 0) {
     ldv2 = 2 * j2max + 1;
     vec2_diatom.assign((size_t)n_ch * ldv2, 0.0);
     for (int c = 0; c < n_ch; ++c) vec2_diatom[(size_t)c * ldv2 + sys->j2[c]] = 1.0;
@@ -1484,8 +1509,9 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
   MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
   MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
   MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
-  MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * sys->ldv, st));
-  if (type == 8) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
+  if (type == 7) MQCT_CUDA_TRY(d_vec1.upload(vec1_sym, st));
+  else MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * ldv1, st));
+  if (type != 0) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
   else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));
   MQCT_CUDA_TRY(d_lab.upload(lab5, st));
   MQCT_CUDA_TRY(d_T.upload(terms, (size_t)nR * n_terms, st));
@@ -1501,7 +1527,7 @@ extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t*
   MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
   const int64_t n_at = P * n_terms;
   expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
-      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, sys->ldv, d_vec2.p,
+      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, ldv1, d_vec2.p,
       ldv2, d_lab.p, pref, d_A.p);
   MQCT_CUDA_TRY(cudaGetLastError());
   expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(

@@ -373,7 +373,7 @@ int orc_count_states(const orc_system* sys) {
   for (int i = 0; i < sys->n_channels; ++i) {
     switch (sys->sys_type) {
       case 1: case 4: st += 2 * sys->j1[i] + 1; break;
-      case 8: case 0: {
+      case 7: case 8: case 0: {
         int a = sys->j1[i], b = sys->j2[i];
         for (int js = abs(a - b); js <= a + b; ++js) st += 2 * js + 1;
         break;
@@ -393,7 +393,7 @@ int orc_enumerate_states(const orc_system* sys, int32_t* indx_chann, int32_t* j1
       for (int m = -j; m <= j; ++m) {
         indx_chann[st] = i + 1; j12[st] = j; m12[st] = m; ej[st] = sys->e_ch[i]; ++st;
       }
-    } else if (sys->sys_type == 8 || sys->sys_type == 0) {
+    } else if (sys->sys_type == 7 || sys->sys_type == 8 || sys->sys_type == 0) {
       int a = sys->j1[i], b = sys->j2[i];
       for (int js = abs(a - b); js <= a + b; ++js)
         for (int m = -js; m <= js; ++m) {
@@ -1475,6 +1475,78 @@ int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
         m3 += m2 * cg_p;
       }
       const double a = coef3 * kt * m3;
+      if (a == 0.0) continue;
+      for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
+    }
+    for (int i = 0; i < nR; ++i) out[i] *= coef12 * e_unit;
+  }
+  return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* SRC/pot_comp.f:7593-7824 (EXPANSION_MATRIX_ELEMENT, SYS_TYPE 7: symmetric top
+ * (j1, k, eps) + diatom j2, the parity-adapted top |j k eps> =
+ * (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0))).  For the pair (p, pp) and the
+ * term (l1, nju1, l2, l):
+ *   A_t = sqrt((2l1+1)(2l2+1))/(4 pi) coef4 <j2'' 0 l2 0|j2' 0> M1 M3,
+ *   coef4 = 1/sqrt(2(1+d_{k'0}) 2(1+d_{k''0})),
+ *   M1 = sum over nju = nju1 and (nju1 != 0) -nju1, phase (-1)^(l1+l2+l+nju1) on the
+ *        second, of <j1'' k'' l1 nju|j1' k'> + (-1)^eps' <j1'' k'' l1 nju|j1' -k'>
+ *        + (-1)^eps'' <j1'' -k'' l1 nju|j1' k'> + (-1)^(eps'+eps'') <j1'' -k'' l1 nju|j1' -k'>
+ *        (:7680-7707),
+ *   M3 as for SYS_TYPE 8 (:7712-7745),
+ *   M_k(R) = e_unit sqrt((2j1''+1)/(2j1'+1)) sqrt((2j2''+1)/(2j2'+1)) sum_t T_t(R) A_t.
+ * The channel's k is sys->ka1, its eps sys->kc1; labels 4 per term. */
+int orc_expansion_matrix_type7(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double e_unit, double* mat) {
+  if (sys->sys_type != 7 || !sys->j2 || !sys->ka1 || !sys->kc1) return -1;
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t k = 0; k < P; ++k) {
+    const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+    const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
+    const int j1p = sys->j1[cp], j2p = sys->j2[cp], j1pp = sys->j1[cpp], j2pp = sys->j2[cpp];
+    const int kp = sys->ka1[cp], kpp = sys->ka1[cpp];
+    const double sp_eps = (sys->kc1[cp] & 1) ? -1.0 : 1.0, spp_eps = (sys->kc1[cpp] & 1) ? -1.0 : 1.0;
+    const int j12p = j12[sp], j12pp = j12[spp], m = m12[sp];
+    const double coef12 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+    const double coef4 = 1.0 / sqrt(2.0 * (1.0 + (kp == 0)) * 2.0 * (1.0 + (kpp == 0)));
+    double* out = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) out[i] = 0.0;
+    for (int t = 0; t < n_terms; ++t) {
+      const int l1 = labels[4 * t], nju1 = labels[4 * t + 1], l2 = labels[4 * t + 2],
+                l = labels[4 * t + 3];
+      if (!orc_triangle(j1pp, l1, j1p) || !orc_triangle(l1, l2, l) || !orc_triangle(j2pp, l2, j2p))
+        continue;
+      const double coef3 = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (4.0 * ORC_PI);
+      const double cg_j2 = orc_cg(j2pp, l2, j2p, 0, 0, 0);
+      double m1 = 0.0;
+      for (int planar = 0; planar < (nju1 == 0 ? 1 : 2); ++planar) {
+        const int nju = planar ? -nju1 : nju1;
+        const double phase = planar ? (((l1 + l2 + l + nju1) % 2) ? -1.0 : 1.0) : 1.0;
+        const double cg_all = orc_cg(j1pp, l1, j1p, kpp, nju, kp) +
+                              orc_cg(j1pp, l1, j1p, kpp, nju, -kp) * sp_eps +
+                              orc_cg(j1pp, l1, j1p, -kpp, nju, kp) * spp_eps +
+                              orc_cg(j1pp, l1, j1p, -kpp, nju, -kp) * sp_eps * spp_eps;
+        m1 += phase * cg_all;
+      }
+      double m3 = 0.0;
+      for (int mp = -j1p; mp <= j1p; ++mp) {
+        if (abs(m - mp) > j2p) continue;
+        const double cg_p = orc_cg(j1p, j2p, j12p, mp, m - mp, m);
+        double m2 = 0.0;
+        const int mx = l1 < l2 ? l1 : l2;
+        for (int me = -mx; me <= mx; ++me) {
+          const int mpp = mp - me;
+          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+          m2 += orc_cg(l1, l2, l, me, -me, 0) * orc_cg(j1pp, j2pp, j12pp, mpp, m - mpp, m) *
+                orc_cg(j1pp, l1, j1p, mpp, me, mp) * orc_cg(j2pp, l2, j2p, m - mpp, -me, m - mp);
+        }
+        m3 += m2 * cg_p;
+      }
+      const double a = coef3 * coef4 * cg_j2 * m1 * m3;
       if (a == 0.0) continue;
       for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
     }

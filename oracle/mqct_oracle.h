@@ -44,11 +44,12 @@ void orc_wf_asym(int j, const double* coeff, int m, double alpha, double beta,
 
 /* ---------------- system / states (SRC/matrix_ini.f) ---------------- */
 typedef struct orc_system {
-  int32_t sys_type;      /* 1 diatom+atom, 4 asym top+atom, 8 asym top+diatom, 0 asym+asym */
+  int32_t sys_type;      /* 1 diatom+atom, 4 asym top+atom, 7 sym top+diatom,
+                            8 asym top+diatom, 0 asym+asym */
   int32_t n_channels;
   const int32_t* j1;     /* per channel: j (type 1,4) or j1 (type 8,0) */
-  const int32_t* ka1;
-  const int32_t* kc1;
+  const int32_t* ka1;    /* type 7: k of the symmetric top */
+  const int32_t* kc1;    /* type 7: eps (parity) */
   const int32_t* j2;     /* type 8, 0 */
   const int32_t* ka2;    /* type 0 */
   const int32_t* kc2;
@@ -187,6 +188,13 @@ int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
  * labels[5t .. 5t+4] = (l1, nju1, l2, nju2, l) (the A_TOP columns), terms in the
  * file's energy unit, e_unit = Hartree per that unit. */
 int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
+                               const int32_t* j12, const int32_t* m12, int64_t P,
+                               const int32_t* ind_mat, int n_terms, const int32_t* labels,
+                               int nR, const double* terms, double e_unit, double* mat);
+
+/* SYS_TYPE 7 (symmetric top + diatom), SRC/pot_comp.f:7593-7824: the channel's k in
+ * sys->ka1 and eps in sys->kc1; labels[4t .. 4t+3] = (l1, nju1, l2, l). */
+int orc_expansion_matrix_type7(const orc_system* sys, const int32_t* indx_chann,
                                const int32_t* j12, const int32_t* m12, int64_t P,
                                const int32_t* ind_mat, int n_terms, const int32_t* labels,
                                int nR, const double* terms, double e_unit, double* mat);

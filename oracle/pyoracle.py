@@ -121,6 +121,10 @@ def lib():
                                      C.c_int, f64p, C.c_double, f64p]
         L.orc_dotraject_rec.argtypes = [C.POINTER(Tables), C.POINTER(Traj), f64p, f64p, f64p,
                                         f64p, C.c_int64, C.POINTER(C.c_int64)]
+        L.orc_expansion_matrix_type7.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
+                                                 C.c_void_p, C.c_int, C.c_void_p, C.c_double,
+                                                 C.c_void_p]
         L.orc_expansion_matrix_type0.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
                                                  C.c_void_p, C.c_int, C.c_void_p, C.c_double,
@@ -400,4 +404,23 @@ def expansion_matrix_type0(osys, states, ind, labels, terms, e_unit):
                                           _ptr(mat))
     if rc:
         raise RuntimeError(f"orc_expansion_matrix_type0 failed: {rc}")
+    return mat.reshape(P, nR)
+
+
+def expansion_matrix_type7(osys, states, ind, labels, terms, e_unit):
+    """SYS_TYPE 7 matrix (P x nR, Hartree) from PES expansion terms (nR x n_terms, in the
+    unit e_unit Hartree); labels n_terms x 4 (l1, nju1, l2, l); the system's ka1 = k,
+    kc1 = eps."""
+    ic, j12, m12, _ = states
+    ind = np.ascontiguousarray(ind, np.int32)
+    labels = np.ascontiguousarray(labels, np.int32).reshape(-1, 4)
+    terms = np.ascontiguousarray(terms, np.float64)
+    P, nR = ind.shape[0], terms.shape[0]
+    mat = np.zeros(P * nR)
+    rc = lib().orc_expansion_matrix_type7(C.byref(osys.s), _ptr(ic), _ptr(j12), _ptr(m12), P,
+                                          _ptr(ind.reshape(-1)), labels.shape[0],
+                                          _ptr(labels.reshape(-1)), nR, _ptr(terms), e_unit,
+                                          _ptr(mat))
+    if rc:
+        raise RuntimeError(f"orc_expansion_matrix_type7 failed: {rc}")
     return mat.reshape(P, nR)

@@ -88,6 +88,32 @@ def main(ref_root):
     np.savez_compressed(os.path.join(out, "g5_h2o_h2_expansion_terms.npz"), labels=labels,
                         R=vals[:, 0], terms=vals[:, 1:])
 
+    # G5b: symmetric top + diatom (SYS_TYPE 7), ND3+D2
+    # (EXAMPLES_IO/SYS_TYPE_7/NH3_H2_MTRX_calculation: PES_EXPAN_TERMS.DAT, 377 terms
+    # (l1, nju1, l2, l) in cm^-1 -> MTRX.DAT, 80 states, 461 pairs, 86 R).  Every R
+    # point of the expansion is independent of the others, so 12 of the 86 R points
+    # are kept: the terms there and all 461 matrix columns.
+    d = os.path.join(ex, "SYS_TYPE_7", "NH3_H2_MTRX_calculation")
+    coll7, nch7, states7, ind7, R7, mat7 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 8)
+    with open(os.path.join(d, "PES_EXPAN_TERMS.DAT")) as f:
+        head = f.readline().split()
+        rows = np.array([[float(x) for x in ln.split()] for ln in f if ln.strip()])
+    labels7 = np.array([[int(x) for x in h.split("_")[1:]] for h in head[1:]], dtype=np.int32)
+    keep = np.linspace(0, len(R7) - 1, 12).round().astype(int)
+    assert np.allclose(rows[keep, 0], R7[keep], atol=5e-3)
+    np.savez_compressed(
+        os.path.join(out, "g5b_nd3_d2_type7.npz"), coll=coll7, states=states7, ind_mat=ind7,
+        r_index=keep, R=R7[keep], mat=mat7[:, keep], labels=labels7, terms=rows[keep, 1:],
+        # $BASIS of NH3H2.inp: A = B, C of the symmetric top, BE of the diatom
+        A=5.1432, C=3.1015, BE=30.443,
+        channels=np.array([[0, 0, 0, 0], [1, 0, 0, 0], [2, 0, 0, 0], [3, 0, 0, 0], [3, 3, 0, 0],
+                           [3, 3, 1, 0], [1, 1, 0, 0], [1, 1, 1, 0], [2, 1, 0, 0], [2, 1, 1, 0],
+                           [3, 1, 0, 0], [3, 1, 1, 0], [4, 1, 0, 0], [5, 1, 0, 0]],
+                          dtype=np.int32),
+        # CHANNELS ENERGIES, CM-1 of USER_INPUT_CHECK.out
+        e_ch_printed=np.array([0.0, 10.2864, 30.8592, 61.7184, 43.3431, 43.3431, 8.2447, 8.2447,
+                               28.8175, 28.8175, 59.6767, 59.6767, 100.8223, 152.2543]))
+
     # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)

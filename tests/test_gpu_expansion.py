@@ -41,3 +41,35 @@ def test_expansion_rejects_bad_terms(mq, gpu_available):
     R = g["R"]
     with pytest.raises(mq.MqctError):
         mq.build_matrix_expansion(s, R, np.array([[1, 2, 0, 1]]), np.zeros((len(R), 1)))
+
+
+def test_type7_expansion_matches_reference_and_oracle(mq, oracle, gpu_available):
+    g = np.load(os.path.join(GOLD, "g5b_nd3_d2_type7.npz"))
+    s = mq.CollisionSystem(7, g["channels"], A=float(g["A"]), C=float(g["C"]), BE=float(g["BE"]))
+    m, y2, sk = mq.build_matrix_expansion(s, g["R"], g["labels"], g["terms"], e_unit="CM-1",
+                                          mij_cutoff=0.0)
+    ref = g["mat"]
+    assert np.max(np.abs(m - ref)) <= 1e-11 * np.abs(ref).max()
+    ch = s.channels
+    osys = oracle.OracleSystem(7, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch, ldv=1)
+    mo = oracle.expansion_matrix_type7(osys, osys.states(), s.ind_mat, g["labels"], g["terms"],
+                                       mq.E_UNIT["CM-1"])
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+    assert not sk.any()
+
+
+def test_expansion_mij_cutoff_flags(mq, oracle, gpu_available):
+    """MIJ_CUTOFF on the expansion path: elements whose |M| at the R points nearest
+    r_cut1 and r_cut2 stays below the cut are zeroed and flagged, as in the
+    direct-integration build."""
+    g = np.load(os.path.join(GOLD, "g5b_nd3_d2_type7.npz"))
+    s = mq.CollisionSystem(7, g["channels"], A=float(g["A"]), C=float(g["C"]), BE=float(g["BE"]))
+    R = g["R"]
+    m0, _, _ = mq.build_matrix_expansion(s, R, g["labels"], g["terms"], mij_cutoff=0.0)
+    cut_cm = 5.0   # 220 symmetry zeros and 46 small elements fall below it
+    m, y2, sk = mq.build_matrix_expansion(s, R, g["labels"], g["terms"], mij_cutoff=cut_cm)
+    ir1, ir2 = np.argmin(np.abs(R - 6.0)), np.argmin(np.abs(R - 8.0))
+    expect = np.maximum(np.abs(m0[:, ir1]), np.abs(m0[:, ir2])) < cut_cm * mq.CM_TO_HARTREE
+    assert (expect & (np.abs(m0).max(axis=1) > 1e-12)).sum() > 20 and not expect.all()
+    assert np.array_equal(sk.astype(bool), expect)
+    assert np.all(m[expect] == 0.0) and np.array_equal(m[~expect], m0[~expect])

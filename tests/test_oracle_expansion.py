@@ -64,3 +64,46 @@ def test_expansion_reproduces_reference_matrix(mq, oracle):
     gauge = level_gauge(s, m, ref)
     assert (gauge < 0).any()  # the phase convention does differ for some levels
     assert np.max(np.abs(m - gauge[:, None] * ref)) <= 1e-10 * np.abs(ref).max()
+
+
+def _g5b():
+    return np.load(os.path.join(GOLD, "g5b_nd3_d2_type7.npz"))
+
+
+def test_type7_levels_states_and_pairs(mq):
+    """SYS_TYPE 7 (ND3 + D2): printed channel energies, the state table and the pair
+    order of the reference's MTRX.DAT."""
+    g = _g5b()
+    s = mq.CollisionSystem(7, g["channels"], A=float(g["A"]), C=float(g["C"]), BE=float(g["BE"]))
+    assert np.allclose(s.e_ch, g["e_ch_printed"], atol=1e-9)
+    st = g["states"]
+    assert s.n_states == 80 and s.P == 461
+    assert (s.indx_chann == st[:, 1]).all() and (s.j12 == st[:, 2]).all()
+    assert (s.m12 == st[:, 3]).all() and (s.ind_mat == g["ind_mat"]).all()
+    assert (s.state_records()[:, 4:] == st[:, 4:]).all()   # J1, K, EPS, J2 columns
+
+
+def test_type7_expansion_reproduces_reference_matrix(mq, oracle):
+    g = _g5b()
+    s = mq.CollisionSystem(7, g["channels"], A=float(g["A"]), C=float(g["C"]), BE=float(g["BE"]))
+    ch = s.channels
+    osys = oracle.OracleSystem(7, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch, ldv=1)
+    m = oracle.expansion_matrix_type7(osys, osys.states(), s.ind_mat, g["labels"], g["terms"],
+                                      mq.E_UNIT["CM-1"])
+    ref = g["mat"]
+    assert np.max(np.abs(m - ref)) <= 1e-11 * np.abs(ref).max()
+
+
+def test_type7_equals_type8_form_with_parity_adapted_vector(mq, oracle):
+    """The reduction the GPU kernel uses: the four-term symmetric-top bracket of
+    case 7 equals the K-sum of case 8 over the parity-adapted vector."""
+    g = _g5b()
+    s = mq.CollisionSystem(7, g["channels"], A=float(g["A"]), C=float(g["C"]), BE=float(g["BE"]))
+    ch = s.channels
+    o7 = oracle.OracleSystem(7, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch, ldv=1)
+    m7 = oracle.expansion_matrix_type7(o7, o7.states(), s.ind_mat, g["labels"], g["terms"], 1.0)
+    o8 = oracle.OracleSystem(8, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch,
+                             vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    # the type-8 restatement works in cm^-1 and converts to Hartree itself
+    m8 = oracle.expansion_matrix_type8(o8, o8.states(), s.ind_mat, g["labels"], g["terms"])
+    assert np.max(np.abs(m8 / mq.E_UNIT["CM-1"] - m7)) <= 1e-12 * np.abs(m7).max()
