@@ -346,6 +346,28 @@ int mqct_read_mtrx_uf_header(const char* path, int32_t* coll_type, int32_t* n_ch
 int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_rec,
                       int32_t* ind_mat, double* R, double* mat);
 
+/* Formatted MTRX.DAT (SAVE_MTRX / READ_MTRX with UNFORMAT = NO): PRINT_MIJ and READ_MIJ,
+ * MQCT_SOURCE_CODES/matrix_ini.f:4692-4877 and 5794-6630.  Five header counts, the
+ * state table (the columns of state_rec, SYS_TYPE 1, 4, 7, 8 or 0 for the writer), the
+ * pairs, the R grid (e19.12) and one line (k, iR, Mij) per element (e19.12).  The
+ * header reader returns the counts and the number of state columns. */
+int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
+                        int32_t n_states, const int32_t* state_rec, int32_t state_rec_len,
+                        int64_t P, const int32_t* ind_mat, int32_t nR, const double* R,
+                        const double* mat);
+int mqct_read_mtrx_dat_header(const char* path, int32_t* coll_type, int32_t* n_channels,
+                              int32_t* n_states, int64_t* P, int32_t* nR,
+                              int32_t* state_rec_len);
+int mqct_read_mtrx_dat(const char* path, int32_t state_rec_len, int32_t* state_rec,
+                       int32_t* ind_mat, double* R, double* mat);
+
+/* PES_EXPAN_TERMS.DAT (READ_EXPANSION_TERMS, MQCT_SOURCE_CODES/pot_comp.f:6344-6388): a
+ * header line, then per R point R and n_terms coefficients.  R[iR] and
+ * terms[t * nR + iR] (the expansion_terms(n_r_coll, nterms) layout that
+ * mqct_build_matrix_expansion takes); values in the file's energy unit. */
+int mqct_read_expansion_terms(const char* path, int32_t nR, int32_t n_terms, double* R,
+                              double* terms);
+
 #ifdef __cplusplus
 }
 #endif

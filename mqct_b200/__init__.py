@@ -25,7 +25,8 @@ from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
            "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections", "write_mtrx_uf",
-           "read_mtrx_uf", "spline_y2", "Surrogate", "build_matrix_expansion", "E_UNIT", "MqctError",
+           "read_mtrx_uf", "write_mtrx_dat", "read_mtrx_dat", "read_expansion_terms",
+           "spline_y2", "Surrogate", "build_matrix_expansion", "E_UNIT", "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
            "MODE_AT"]
 
@@ -613,3 +614,40 @@ def read_mtrx_uf(path):
     check(L.mqct_read_mtrx_uf(path.encode(), srl.value, st, ind, R, mat))
     return dict(coll_type=ct.value, n_channels=nch.value, states=st.reshape(ns.value, srl.value),
                 ind_mat=ind.reshape(P.value, 2), R=R, mat=mat.reshape(P.value, nR.value))
+
+
+def write_mtrx_dat(path, system: CollisionSystem, R, mat):
+    """Formatted MTRX.DAT as PRINT_MIJ writes it (MQCT_SOURCE_CODES/matrix_ini.f:4692-4877)."""
+    rec = system.state_records()
+    check(lib().mqct_write_mtrx_dat(path.encode(), system.sys_type, system.n_channels,
+                                    system.n_states, np.ascontiguousarray(rec.reshape(-1)),
+                                    rec.shape[1], system.P,
+                                    np.ascontiguousarray(system.ind_mat.reshape(-1)), len(R),
+                                    np.ascontiguousarray(R, np.float64),
+                                    np.ascontiguousarray(mat, np.float64).reshape(-1)))
+
+
+def read_mtrx_dat(path):
+    """Formatted MTRX.DAT (READ_MTRX with UNFORMAT = NO): coll_type, n_channels, the state
+    table, ind_mat, R and Mat_el (P x nR)."""
+    L = lib()
+    ct, nch, ns, nR, srl = (C.c_int32() for _ in range(5))
+    P = C.c_int64()
+    check(L.mqct_read_mtrx_dat_header(path.encode(), C.byref(ct), C.byref(nch), C.byref(ns),
+                                      C.byref(P), C.byref(nR), C.byref(srl)))
+    st = np.zeros(ns.value * srl.value, np.int32)
+    ind = np.zeros(2 * P.value, np.int32)
+    R = np.zeros(nR.value)
+    mat = np.zeros(P.value * nR.value)
+    check(L.mqct_read_mtrx_dat(path.encode(), srl.value, st, ind, R, mat))
+    return dict(coll_type=ct.value, n_channels=nch.value, states=st.reshape(ns.value, srl.value),
+                ind_mat=ind.reshape(P.value, 2), R=R, mat=mat.reshape(P.value, nR.value))
+
+
+def read_expansion_terms(path, nR, n_terms):
+    """PES_EXPAN_TERMS.DAT (READ_EXPANSION_TERMS): returns R (nR) and the terms as the
+    file's rows (nR x n_terms), ready for build_matrix_expansion."""
+    R = np.zeros(nR)
+    T = np.zeros(nR * n_terms)
+    check(lib().mqct_read_expansion_terms(path.encode(), nR, n_terms, R, T))
+    return R, np.ascontiguousarray(T.reshape(n_terms, nR).T)

@@ -89,7 +89,8 @@ EXPORTS = [
     "mqct_prop_plan_destroy",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
     "mqct_fill_ind_mat", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
-    "mqct_read_mtrx_uf",
+    "mqct_read_mtrx_uf", "mqct_write_mtrx_dat", "mqct_read_mtrx_dat_header",
+    "mqct_read_mtrx_dat", "mqct_read_expansion_terms",
 ]
 
 _lib = None
@@ -166,6 +167,10 @@ def lib():
     L.mqct_read_mtrx_uf_header.argtypes = [C.c_char_p] + [C.POINTER(C.c_int32)] * 3 + [
         C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.mqct_read_mtrx_uf.argtypes = [C.c_char_p, C.c_int32, i32p, i32p, f64p, f64p]
+    L.mqct_write_mtrx_dat.argtypes = L.mqct_write_mtrx_uf.argtypes
+    L.mqct_read_mtrx_dat_header.argtypes = L.mqct_read_mtrx_uf_header.argtypes
+    L.mqct_read_mtrx_dat.argtypes = L.mqct_read_mtrx_uf.argtypes
+    L.mqct_read_expansion_terms.argtypes = [C.c_char_p, C.c_int32, C.c_int32, f64p, f64p]
     _lib = L
     return L
 

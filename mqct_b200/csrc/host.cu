@@ -5,6 +5,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -378,6 +380,286 @@ int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_re
     set_error("malformed MTRX_UF body in %s", path);
     return MQCT_E_IO;
   }
+  return MQCT_OK;
+}
+
+// ---------------------------------------------------------------- MTRX.DAT (formatted)
+// The formatted matrix file of SAVE_MTRX / READ_MTRX with UNFORMAT = NO: PRINT_MIJ
+// (MQCT_SOURCE_CODES/matrix_ini.f:4692-4877) writes five header counts, the state
+// table, ind_mat, the R grid and one line (k, iR, Mij) per element; READ_MIJ reads it.
+
+// Fortran Ew.d output (0.ddd...E+ee, or 0.ddd...+eee for |exponent| > 99), right
+// justified in w columns; d significant digits, rounded to nearest.
+static std::string fortran_e(double v, int w, int d) {
+  char buf[64];
+  std::string body;
+  if (v == 0.0 || !std::isfinite(v)) {
+    if (!std::isfinite(v)) {
+      body = std::isnan(v) ? "NaN" : (v > 0 ? "Infinity" : "-Infinity");
+    } else {
+      body = "0.";
+      body.append(d, '0');
+      body += "E+00";
+    }
+  } else {
+    // d significant digits in C's d.ddd form, then shifted into 0.dddd form
+    snprintf(buf, sizeof buf, "%.*e", d - 1, std::fabs(v));
+    const char* e = strchr(buf, 'e');
+    std::string digits;
+    for (const char* c = buf; c < e; ++c)
+      if (*c >= '0' && *c <= '9') digits += *c;
+    const int ex = atoi(e + 1) + 1;
+    body = std::string(v < 0 ? "-" : "") + "0." + digits;
+    const int ax = ex < 0 ? -ex : ex;
+    if (ax <= 99) snprintf(buf, sizeof buf, "E%c%02d", ex < 0 ? '-' : '+', ax);
+    else snprintf(buf, sizeof buf, "%c%03d", ex < 0 ? '-' : '+', ax);
+    body += buf;
+  }
+  if ((int)body.size() >= w) return body;
+  return std::string(w - body.size(), ' ') + body;
+}
+
+// A Fortran real: also accepts the exponent form without the letter (0.1-100).
+static bool parse_fortran_real(const char*& p, double* out) {
+  while (*p == ' ' || *p == '\t') ++p;
+  if (!*p || *p == '\n' || *p == '\r') return false;
+  const char* start = p;
+  while (*p && *p != ' ' && *p != '\t' && *p != '\n' && *p != '\r') ++p;
+  std::string tok(start, p - start);
+  for (auto& c : tok)
+    if (c == 'D' || c == 'd') c = 'E';
+  // a sign after the first digit without an exponent letter starts the exponent
+  for (size_t i = 1; i < tok.size(); ++i)
+    if ((tok[i] == '-' || tok[i] == '+') && tok[i - 1] != 'E' && tok[i - 1] != 'e') {
+      tok.insert(i, "E");
+      break;
+    }
+  char* end = nullptr;
+  *out = strtod(tok.c_str(), &end);
+  return end && *end == '\0';
+}
+
+static const char* const* mtrx_dat_columns(int coll_type, int* n) {
+  static const char* c1[] = {"#STATE", "#CHANNEL", "J12", "M12", "J"};
+  static const char* c4[] = {"#STATE", "#CHANNEL", "J12", "M12", "J", "KA", "KC"};
+  static const char* c7[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K", "EPS", "J2"};
+  static const char* c8[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K1A", "K1C", "J2"};
+  static const char* c0[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "KA1", "KC1",
+                             "J2", "KA2", "KC2"};
+  switch (coll_type) {
+    case 1: *n = 5; return c1;
+    case 4: *n = 7; return c4;
+    case 7: *n = 8; return c7;
+    case 8: *n = 8; return c8;
+    case 0: *n = 10; return c0;
+    default: *n = 0; return nullptr;
+  }
+}
+
+int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
+                        int32_t n_states, const int32_t* state_rec, int32_t state_rec_len,
+                        int64_t P, const int32_t* ind_mat, int32_t nR, const double* R,
+                        const double* mat) {
+  int ncol = 0;
+  const char* const* cols = mtrx_dat_columns(coll_type, &ncol);
+  MQCT_ARG_CHECK(cols, "mqct_write_mtrx_dat: SYS_TYPE %d not supported (1, 4, 7, 8, 0)",
+                 coll_type);
+  MQCT_ARG_CHECK(path && state_rec && ind_mat && R && mat && P > 0 && nR > 1 && n_states > 0,
+                 "mqct_write_mtrx_dat: bad arguments");
+  MQCT_ARG_CHECK(state_rec_len == ncol, "SYS_TYPE %d state records have %d columns (got %d)",
+                 coll_type, ncol, state_rec_len);
+  FILE* f = fopen(path, "w");
+  if (!f) {
+    set_error("cannot open %s for writing", path);
+    return MQCT_E_IO;
+  }
+  fprintf(f, "COLLISION_TYPE= %1d\n", coll_type);
+  fprintf(f, "NUMBER_OF_CHANLS=%5d\n", n_channels);
+  fprintf(f, "NUMBER_OF_STATES= %6d\n", n_states);
+  fprintf(f, "MATRIX_SIZE= %9lld\n", (long long)P);
+  fprintf(f, "R_GRID_SIZE= %4d\n", nR);
+  for (int c = 0; c < ncol; ++c) fprintf(f, c ? " %8s" : "%8s", cols[c]);
+  fputc('\n', f);
+  for (int st = 0; st < n_states; ++st) {
+    for (int c = 0; c < ncol; ++c)
+      fprintf(f, c ? " %8d" : "%8d", state_rec[(size_t)st * ncol + c]);
+    fputc('\n', f);
+  }
+  fprintf(f, "%16s %8s %8s\n", "MIJ_INDEX", "ST_1", "ST_2");
+  for (int64_t k = 0; k < P; ++k)
+    fprintf(f, "%16lld %8d %8d\n", (long long)k + 1, ind_mat[2 * k], ind_mat[2 * k + 1]);
+  fprintf(f, "%5s %19s\n", "#iR", "R_COM(iR)");
+  for (int i = 0; i < nR; ++i) fprintf(f, "%5d %s\n", i + 1, fortran_e(R[i], 19, 12).c_str());
+  fprintf(f, "%16s %8s %19s\n", "#k_matel", "#iR", "Mij(iR,k_matel)");
+  for (int64_t k = 0; k < P; ++k)
+    for (int i = 0; i < nR; ++i)
+      fprintf(f, "%16lld %8d %s\n", (long long)k + 1, i + 1,
+              fortran_e(mat[(size_t)k * nR + i], 19, 12).c_str());
+  if (fclose(f) != 0) {
+    set_error("write error on %s", path);
+    return MQCT_E_IO;
+  }
+  return MQCT_OK;
+}
+
+static bool read_line(FILE* f, std::string& line) {
+  line.clear();
+  int c;
+  while ((c = fgetc(f)) != EOF && c != '\n') line += (char)c;
+  return !(c == EOF && line.empty());
+}
+
+static bool header_count(const std::string& line, const char* key, long long* v) {
+  const size_t n = strlen(key);
+  if (line.compare(0, n, key) != 0) return false;
+  char* end = nullptr;
+  *v = strtoll(line.c_str() + n, &end, 10);
+  return end != line.c_str() + n;
+}
+
+int mqct_read_mtrx_dat_header(const char* path, int32_t* coll_type, int32_t* n_channels,
+                              int32_t* n_states, int64_t* P, int32_t* nR,
+                              int32_t* state_rec_len) {
+  MQCT_ARG_CHECK(path && coll_type && n_channels && n_states && P && nR && state_rec_len,
+                 "null argument");
+  FILE* f = fopen(path, "r");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return MQCT_E_IO;
+  }
+  static const char* keys[5] = {"COLLISION_TYPE=", "NUMBER_OF_CHANLS=", "NUMBER_OF_STATES=",
+                                "MATRIX_SIZE=", "R_GRID_SIZE="};
+  long long h[5] = {0, 0, 0, 0, 0};
+  std::string line;
+  bool ok = true;
+  for (int i = 0; i < 5 && ok; ++i) ok = read_line(f, line) && header_count(line, keys[i], &h[i]);
+  int ncol = 0;
+  if (ok && read_line(f, line)) {
+    const char* p = line.c_str();
+    while (*p) {
+      while (*p == ' ' || *p == '\t' || *p == '\r') ++p;
+      if (!*p) break;
+      ++ncol;
+      while (*p && *p != ' ' && *p != '\t' && *p != '\r') ++p;
+    }
+  }
+  fclose(f);
+  if (!ok || h[2] <= 0 || h[3] <= 0 || h[3] >= ((long long)1 << 31) || h[4] <= 1 || ncol < 5) {
+    set_error("malformed MTRX.DAT header in %s", path);
+    return MQCT_E_IO;
+  }
+  *coll_type = (int32_t)h[0];
+  *n_channels = (int32_t)h[1];
+  *n_states = (int32_t)h[2];
+  *P = h[3];
+  *nR = (int32_t)h[4];
+  *state_rec_len = ncol;
+  return MQCT_OK;
+}
+
+int mqct_read_mtrx_dat(const char* path, int32_t state_rec_len, int32_t* state_rec,
+                       int32_t* ind_mat, double* R, double* mat) {
+  int32_t ct, nch, ns, nR, ncol;
+  int64_t P;
+  int rc = mqct_read_mtrx_dat_header(path, &ct, &nch, &ns, &P, &nR, &ncol);
+  if (rc) return rc;
+  MQCT_ARG_CHECK(state_rec && ind_mat && R && mat, "null argument");
+  MQCT_ARG_CHECK(state_rec_len == ncol, "%s has %d state columns (caller expects %d)", path, ncol,
+                 state_rec_len);
+  FILE* f = fopen(path, "r");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return MQCT_E_IO;
+  }
+  std::string line;
+  auto fail = [&](const char* what, long long at) {
+    fclose(f);
+    set_error("malformed MTRX.DAT %s (%s, entry %lld)", path, what, at);
+    return MQCT_E_IO;
+  };
+  for (int i = 0; i < 6; ++i)
+    if (!read_line(f, line)) return fail("header", i + 1);
+  for (int s = 0; s < ns; ++s) {
+    if (!read_line(f, line)) return fail("state table", s + 1);
+    const char* p = line.c_str();
+    for (int c = 0; c < ncol; ++c) {
+      char* end = nullptr;
+      const long v = strtol(p, &end, 10);
+      if (end == p) return fail("state table", s + 1);
+      state_rec[(size_t)s * ncol + c] = (int32_t)v;
+      p = end;
+    }
+  }
+  if (!read_line(f, line)) return fail("pair header", 0);
+  for (int64_t k = 0; k < P; ++k) {
+    long long kk;
+    int a, b;
+    if (!read_line(f, line) || sscanf(line.c_str(), "%lld %d %d", &kk, &a, &b) != 3 || kk != k + 1 ||
+        a < 1 || a > ns || b < 1 || b > ns)
+      return fail("ind_mat", k + 1);
+    ind_mat[2 * k] = a;
+    ind_mat[2 * k + 1] = b;
+  }
+  if (!read_line(f, line)) return fail("R header", 0);
+  for (int i = 0; i < nR; ++i) {
+    int ii;
+    char* end = nullptr;
+    if (!read_line(f, line)) return fail("R grid", i + 1);
+    ii = (int)strtol(line.c_str(), &end, 10);
+    const char* p = end;
+    if (ii != i + 1 || !parse_fortran_real(p, &R[i])) return fail("R grid", i + 1);
+  }
+  if (!read_line(f, line)) return fail("element header", 0);
+  std::vector<char> seen((size_t)P * nR, 0);
+  for (int64_t q = 0; q < P * (int64_t)nR; ++q) {
+    if (!read_line(f, line)) return fail("elements", q + 1);
+    char* end = nullptr;
+    const long long kk = strtoll(line.c_str(), &end, 10);
+    const char* p = end;
+    const long ii = strtol(p, &end, 10);
+    p = end;
+    double v;
+    if (kk < 1 || kk > P || ii < 1 || ii > nR || !parse_fortran_real(p, &v))
+      return fail("elements", q + 1);
+    const size_t at = (size_t)(kk - 1) * nR + (ii - 1);
+    if (seen[at]) return fail("repeated element", q + 1);
+    seen[at] = 1;
+    mat[at] = v;
+  }
+  fclose(f);
+  return MQCT_OK;
+}
+
+// ---------------------------------------------------------------- PES_EXPAN_TERMS.DAT
+// READ_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:6344-6388): one header line, then
+// per R point the value of R and the nterms expansion coefficients.  Output in the
+// reference's layout: R[iR], terms[t * nR + iR] (expansion_terms(n_r_coll, nterms)).
+int mqct_read_expansion_terms(const char* path, int32_t nR, int32_t n_terms, double* R,
+                              double* terms) {
+  MQCT_ARG_CHECK(path && R && terms && nR > 0 && n_terms > 0, "bad arguments");
+  FILE* f = fopen(path, "r");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return MQCT_E_IO;
+  }
+  std::string line;
+  if (!read_line(f, line)) {  // header
+    fclose(f);
+    set_error("%s is empty", path);
+    return MQCT_E_IO;
+  }
+  for (int i = 0; i < nR; ++i) {
+    bool ok = read_line(f, line);
+    const char* p = line.c_str();
+    ok = ok && parse_fortran_real(p, &R[i]);
+    for (int t = 0; t < n_terms && ok; ++t) ok = parse_fortran_real(p, &terms[(size_t)t * nR + i]);
+    if (!ok) {
+      fclose(f);
+      set_error("%s: R point %d has fewer than %d terms (or is missing)", path, i + 1, n_terms);
+      return MQCT_E_IO;
+    }
+  }
+  fclose(f);
   return MQCT_OK;
 }
 
