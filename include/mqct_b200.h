@@ -306,6 +306,33 @@ int mqct_propagate_batch_rec(const mqct_tables_t* tab, const mqct_traj_init_t* i
                              double* cls_out, double* diag_out, double* rec_out,
                              int64_t* n_rec_out);
 
+/* Time integrator of the propagation (PROPAGATOR = RK4 | ODEINT of $SYSTEM,
+ * MQCT_SOURCE_CODES/iotest.f:2628-2640, 2676-2681).  ODEINT is the reference's adaptive
+ * Cash-Karp scheme (rkqs / rkck / odeint, MQCT_SOURCE_CODES/suppl_routines.f:1229-1435):
+ * in standard mode every step dt of DOTRAJECT is covered by adaptive steps with
+ * relative accuracy eps (eps_odeint) and minimum step hmin (min_t_stp), the step
+ * size carried from one dt to the next (propagator.f:3933-3941); in AT mode one such
+ * call covers the whole saved path (propagator.f:3900-3908).  The stop rules, records
+ * and energy bookkeeping stay per step dt.  ODEINT requires MQCT_PROP_FP64: its error
+ * control resolves every amplitude to relative eps, below the FP32 rounding of the
+ * right-hand side, so FP32 steps would collapse (MQCT_E_ARG).  As in the reference,
+ * the error scale |y| + |h dy/dt| + 1e-30 also covers amplitudes at rounding level:
+ * with hmin = 0 the step can collapse where their rounding noise dominates, and a
+ * step at or below hmin is accepted without a new step proposal, so once the step
+ * reaches hmin it stays there; a small positive hmin bounds the cost. */
+#define MQCT_INTEG_RK4 0
+#define MQCT_INTEG_ODEINT 1
+typedef struct mqct_integrator_t {
+  int32_t method;   /* MQCT_INTEG_* */
+  double eps;       /* ODEINT accuracy (> 0) */
+  double hmin;      /* ODEINT minimum step, a.u. (>= 0) */
+} mqct_integrator_t;
+/* mqct_propagate_batch with an integrator other than RK4. */
+int mqct_propagate_batch_integ(const mqct_tables_t* tab, const mqct_traj_init_t* init,
+                               int64_t n_traj, int32_t mode, const mqct_at_paths_t* at,
+                               int32_t arith, const mqct_integrator_t* integ, double* amp_out,
+                               double* cls_out, double* diag_out);
+
 typedef struct mqct_prop_plan mqct_prop_plan;
 int mqct_prop_plan_create(const mqct_tables_t* tab, int32_t arith, mqct_prop_plan** plan);
 int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,
@@ -320,6 +347,8 @@ double mqct_prop_plan_bytes_per_step(const mqct_prop_plan* plan);
 /* CUDA-event time (ms) of the last propagation kernel on the plan's stream. */
 int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms);
 void mqct_prop_plan_destroy(mqct_prop_plan* plan);
+/* Select the plan's integrator for the following runs (default RK4). */
+int mqct_prop_plan_set_integrator(mqct_prop_plan* plan, const mqct_integrator_t* integ);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
 int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,

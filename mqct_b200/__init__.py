@@ -470,8 +470,21 @@ def _traj_array(trajs):
     return arr
 
 
-def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, at_paths=None):
-    """Batched DOTRAJECT on the GPU.  Returns (amp [n, 2N], cls [n, 6], diag [n, 8])."""
+def _integrator(integrator):
+    """None or "RK4": RK4 with the trajectories' dt; ("ODEINT", eps, hmin): the adaptive
+    Cash-Karp scheme (PROPAGATOR = ODEINT) with accuracy eps and minimum step hmin."""
+    if integrator is None or (isinstance(integrator, str) and integrator.upper() == "RK4"):
+        return None
+    name, eps, hmin = integrator
+    if name.upper() != "ODEINT":
+        raise ValueError(f"unknown integrator {name!r}")
+    return _abi.Integrator(_abi.INTEG_ODEINT, float(eps), float(hmin))
+
+
+def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, at_paths=None,
+              integrator=None):
+    """Batched DOTRAJECT on the GPU.  Returns (amp [n, 2N], cls [n, 6], diag [n, 8]).
+    integrator: None (RK4) or ("ODEINT", eps, hmin)."""
     n = len(trajs)
     N = tables.n_states
     amp = np.zeros(n * 2 * N)
@@ -487,8 +500,14 @@ def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, 
         flat = np.ascontiguousarray(np.concatenate(recs).reshape(-1))
         at_keep = (n_rec, off, flat)
         at = _abi.AtPaths(ptr(off), ptr(n_rec), ptr(flat))
-    check(lib().mqct_propagate_batch(C.byref(t), arr, n, mode, C.byref(at) if at else None,
-                                     arith, amp, cls, diag))
+    integ = _integrator(integrator)
+    if integ is None:
+        check(lib().mqct_propagate_batch(C.byref(t), arr, n, mode, C.byref(at) if at else None,
+                                         arith, amp, cls, diag))
+    else:
+        check(lib().mqct_propagate_batch_integ(C.byref(t), arr, n, mode,
+                                               C.byref(at) if at else None, arith,
+                                               C.byref(integ), amp, cls, diag))
     return amp.reshape(n, 2 * N), cls.reshape(n, 6), diag.reshape(n, 8)
 
 
@@ -535,6 +554,11 @@ class PropagationPlan:
 
     def run_device(self, d_init: int, n: int, d_amp: int, d_cls: int, d_diag: int):
         check(lib().mqct_prop_plan_run_device(self.h, d_init, n, d_amp, d_cls, d_diag))
+
+    def set_integrator(self, integrator=None):
+        """None or "RK4" (default), or ("ODEINT", eps, hmin) for the following runs."""
+        integ = _integrator(integrator) or _abi.Integrator(_abi.INTEG_RK4, 0.0, 0.0)
+        check(lib().mqct_prop_plan_set_integrator(self.h, C.byref(integ)))
 
     def sync(self):
         check(lib().mqct_prop_plan_sync(self.h))

@@ -20,6 +20,7 @@ ERRORS = {-1: "MQCT_E_ARG", -2: "MQCT_E_CUDA", -3: "MQCT_E_NODEV", -4: "MQCT_E_I
 PREC_FP64, PREC_BF16X3, PREC_F16X3 = 0, 1, 2
 PROP_FP64, PROP_FP32 = 0, 1
 MODE_STD, MODE_AT = 0, 1
+INTEG_RK4, INTEG_ODEINT = 0, 1
 PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3
 
 i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -74,13 +75,17 @@ class AtPaths(C.Structure):
     _fields_ = [("rec_off", vp), ("n_rec", vp), ("rec", vp)]
 
 
+class Integrator(C.Structure):
+    _fields_ = [("method", C.c_int32), ("eps", C.c_double), ("hmin", C.c_double)]
+
+
 # Every symbol declared in include/mqct_b200.h (checked by the ABI test).
 EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
-    "mqct_propagate_batch_rec",
+    "mqct_propagate_batch_rec", "mqct_propagate_batch_integ", "mqct_prop_plan_set_integrator",
     "mqct_surrogate_create", "mqct_surrogate_train", "mqct_surrogate_predict",
     "mqct_surrogate_n_params", "mqct_surrogate_get_params", "mqct_surrogate_loss_grad",
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
@@ -145,6 +150,10 @@ def lib():
                                            C.c_int32, C.c_int64, f64p, f64p, f64p, f64p,
                                            np.ctypeslib.ndpointer(dtype=np.int64,
                                                                   flags="C_CONTIGUOUS")]
+    L.mqct_propagate_batch_integ.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
+                                             C.c_int32, C.POINTER(AtPaths), C.c_int32,
+                                             C.POINTER(Integrator), f64p, f64p, f64p]
+    L.mqct_prop_plan_set_integrator.argtypes = [vp, C.POINTER(Integrator)]
     L.mqct_prop_plan_create.argtypes = [C.POINTER(Tables), C.c_int32, C.POINTER(vp)]
     L.mqct_prop_plan_run.argtypes = [vp, C.POINTER(TrajInit), C.c_int64, f64p, f64p, f64p]
     L.mqct_prop_plan_run_device.argtypes = [vp, vp, C.c_int64, vp, vp, vp]

@@ -78,6 +78,7 @@ struct PropDev {
   double mass;
   int mode;                    // MQCT_MODE_*
   int mp_cap;                  // packed slots that fit in shared memory
+  double ode_eps, ode_hmin;    // ODEINT accuracy and minimum step (adaptive kernel)
   // AT paths
   const int64_t* at_off;
   const int* at_n;
@@ -113,10 +114,14 @@ __device__ inline void save_record(const TrajOut& o, int tr, int64_t& n, double 
   ++n;
 }
 
+// Classical slots in shared memory: state, stage input, stage derivative, first-stage
+// derivative, RK4 middle-stage sum, Cash-Karp stages 2-5, Cash-Karp result and error.
+constexpr int kClsSlots = 11;
+
 // Shared-memory layout of one CTA (dynamic).
 template <class T>
 struct Smem {
-  Cls* c;                      // [0] state, [1] trial point, [2..4] k1..k3 (k2+k3 after step 3)
+  Cls* c;                      // kClsSlots classical slots (see above)
   double* red;                 // reduction scratch, 3 per warp
   int* flag;                   // [0] next trajectory, [1] keep running
   double* Rg;                  // nR grid
@@ -406,6 +411,48 @@ __device__ inline Cls cls_axpy(const Cls& a, double h, const Cls& b) {
              a.Pth + h * b.Pth, a.phi + h * b.phi, a.Pphi + h * b.Pphi};
 }
 
+// Component i of the classical variables (R, P_R, theta, P_theta, phi, P_phi).
+__device__ inline double& cls_ref(Cls& c, int i) {
+  switch (i) {
+    case 0: return c.R;
+    case 1: return c.PR;
+    case 2: return c.th;
+    case 3: return c.Pth;
+    case 4: return c.phi;
+    default: return c.Pphi;
+  }
+}
+__device__ inline double cls_get(const Cls& c, int i) { return cls_ref(const_cast<Cls&>(c), i); }
+
+// Block-wide maximum, broadcast to all threads.
+__device__ inline double block_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double m = red[0];
+#pragma unroll
+  for (int i = 1; i < PT / 32; ++i) m = fmax(m, red[i]);
+  __syncthreads();
+  return m;
+}
+
+// Cash-Karp 5(4) coefficients (MQCT_SOURCE_CODES/suppl_routines.f:1313-1329).  A4 is
+// written there as the default-real literal .6, so its value is 0.6 in single precision.
+constexpr double kCkB21 = .2, kCkB31 = 3.0 / 40.0, kCkB32 = 9.0 / 40.0, kCkB41 = .3,
+                 kCkB42 = -.9, kCkB43 = 1.2, kCkB51 = -11.0 / 54.0, kCkB52 = 2.5,
+                 kCkB53 = -70.0 / 27.0, kCkB54 = 35.0 / 27.0, kCkB61 = 1631.0 / 55296.0,
+                 kCkB62 = 175.0 / 512.0, kCkB63 = 575.0 / 13824.0, kCkB64 = 44275.0 / 110592.0,
+                 kCkB65 = 253.0 / 4096.0, kCkC1 = 37.0 / 378.0, kCkC3 = 250.0 / 621.0,
+                 kCkC4 = 125.0 / 594.0, kCkC6 = 512.0 / 1771.0,
+                 kCkDC1 = kCkC1 - 2825.0 / 27648.0, kCkDC3 = kCkC3 - 18575.0 / 48384.0,
+                 kCkDC4 = kCkC4 - 13525.0 / 55296.0, kCkDC5 = -277.0 / 14336.0,
+                 kCkDC6 = kCkC6 - .25;
+constexpr double kCkA4 = (double)0.6f;
+constexpr int kOdeMaxSteps = 10000;  // MAXSTP of odeint
+
 __device__ inline double kinetic(const Cls& c, double mass) {
   return c.PR * c.PR / 2.0 / mass + c.Pth * c.Pth / 2.0 / mass / (c.R * c.R) +
          c.Pphi * c.Pphi / 2.0 / mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
@@ -431,7 +478,9 @@ struct Book {
   int status, vib, period, run;
 };
 
-template <class T, int NS>
+// kAdaptive: PROPAGATOR = ODEINT (adaptive Cash-Karp steps inside every step dt, or
+// over the whole path in AT mode) in place of RK4 with step dt.
+template <class T, int NS, bool kAdaptive>
 __global__ void __launch_bounds__(PT, 1)
 propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_traj,
                  int* __restrict__ queue, TrajOut out) {
@@ -447,7 +496,7 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
       p += (bytes + 15) & ~size_t(15);
       return r;
     };
-    sm.c = reinterpret_cast<Cls*>(take(sizeof(Cls) * 5));
+    sm.c = reinterpret_cast<Cls*>(take(sizeof(Cls) * kClsSlots));
     bk = reinterpret_cast<Book*>(take(sizeof(Book)));
     sm.red = reinterpret_cast<double*>(take(sizeof(double) * 3 * (PT / 32)));
     sm.flag = reinterpret_cast<int*>(take(16));
@@ -465,6 +514,9 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
   Cls* const KC = sm.c + 2;  // classical derivative of the stage
   Cls* const K1 = sm.c + 3;  // first-stage derivative
   Cls* const K23 = sm.c + 4; // sum of the second and third stages
+  Cls* const KS = sm.c + 5;  // Cash-Karp stages 2..5 (KS[0..3])
+  Cls* const CO = sm.c + 9;  // Cash-Karp result
+  Cls* const CE = sm.c + 10; // Cash-Karp error estimate
   const int ns = (N + PT - 1 - tid) / PT;  // states owned by this thread
   const bool at = d.mode == MQCT_MODE_AT;
   for (;;) {
@@ -503,14 +555,202 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
     }
     __syncthreads();
     const bool skipped = bk->run == 0;
+    double dt_step = dt;  // ODEINT's carried step (dt_step / dt_corrected)
+    // hooks of the first right-hand side of a step: the SAVE_TRAJECT record and,
+    // on the first step, the initial energies (MQCT_SOURCE_CODES/propagator.f:2695-2810)
+    auto first_rhs = [&](double potv) {
+      if (tid == 0 && out.rec && !at) save_record(out, tr, bk->n_rec, tcur, *C, potv);
+      if (counter == 1 && !at) {
+        double q0 = 0.0, z1 = 0.0, z2 = 0.0;
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+          if (q < ns) {
+            const int i = tid + q * PT;
+            q0 += (y[q].x * y[q].x + y[q].y * y[q].y) * d.e_val[d.st_e[i]];
+          }
+        block_sum3(q0, z1, z2, sm.red);
+        if (tid == 0) {
+          bk->eqi = q0 + potv;
+          bk->eki = kinetic(*C, d.mass);
+        }
+      }
+    };
     while (bk->run) {
       ++counter;
       bool last = false;
+      double h6 = 0.0;
+      if constexpr (kAdaptive) {
+        // ---- ODEINT (MQCT_SOURCE_CODES/suppl_routines.f:1229-1435; called per step dt at
+        // propagator.f:3933, over the whole AT path at :3900).  All threads take the same
+        // control decisions from block-wide values.
+        const double x1 = tcur, x2 = at ? t_end : tcur + dt;
+        double x = x1, h = dt_step, hnext = dt_step;
+        double2 k2[NS], k3[NS], k4[NS], k5[NS], yo[NS], ye[NS];
+        // stage input: amplitudes y + h * (combination) into a_in, classical into CT
+        auto set_stage = [&](double ts, auto comb, auto ccomb) {
+#pragma unroll
+          for (int q = 0; q < NS; ++q)
+            if (q < ns) sm.a_in[tid + q * PT] = comb(q);
+          if (tid == 0) {
+            if (at) classical_at(d, tr, ts, CT);
+            else {
+              Cls c;
+              for (int i = 0; i < 6; ++i) cls_ref(c, i) = ccomb(i);
+              *CT = c;
+            }
+          }
+          __syncthreads();
+        };
+        for (int nstp = 1; nstp <= kOdeMaxSteps; ++nstp) {
+          double potv;
+          set_stage(x, [&](int q) { return y[q]; }, [&](int i) { return cls_get(*C, i); });
+          rhs<T, NS>(d, sm, x, CT, ns, k1, KC, potv);
+          if (tid == 0) *K1 = *KC;
+          if (nstp == 1) first_rhs(potv);
+          if (nstp == kOdeMaxSteps) {
+            // the last allowed step: RK4 over what remains (odeint's last_step branch)
+            const double hr = x2 - x, hh = hr * 0.5, h6r = hr / 6.0, xh = x + hh;
+            set_stage(xh, [&](int q) { return make_double2(y[q].x + hh * k1[q].x, y[q].y + hh * k1[q].y); },
+                      [&](int i) { return cls_get(*C, i) + hh * cls_get(*K1, i); });
+            rhs<T, NS>(d, sm, xh, CT, ns, k2, KC, potv);
+            if (tid == 0) KS[0] = *KC;
+            set_stage(xh, [&](int q) { return make_double2(y[q].x + hh * k2[q].x, y[q].y + hh * k2[q].y); },
+                      [&](int i) { return cls_get(*C, i) + hh * cls_get(KS[0], i); });
+            rhs<T, NS>(d, sm, xh, CT, ns, k3, KC, potv);
+            if (tid == 0) KS[1] = *KC;
+            set_stage(x + hr, [&](int q) { return make_double2(y[q].x + hr * k3[q].x, y[q].y + hr * k3[q].y); },
+                      [&](int i) { return cls_get(*C, i) + hr * cls_get(KS[1], i); });
+            rhs<T, NS>(d, sm, x + hr, CT, ns, k4, KC, potv);
+#pragma unroll
+            for (int q = 0; q < NS; ++q)
+              if (q < ns) {
+                const double2 m = make_double2(k2[q].x + k3[q].x, k2[q].y + k3[q].y);
+                y[q] = make_double2(y[q].x + h6r * (k1[q].x + k4[q].x + 2.0 * m.x),
+                                    y[q].y + h6r * (k1[q].y + k4[q].y + 2.0 * m.y));
+              }
+            if (tid == 0 && !at)
+              for (int i = 0; i < 6; ++i)
+                cls_ref(*C, i) += h6r * (cls_get(*K1, i) + cls_get(*KC, i) +
+                                         2.0 * (cls_get(KS[0], i) + cls_get(KS[1], i)));
+            __syncthreads();
+            x = x2;
+            break;
+          }
+          const double hs = h;  // the error scale uses the step before it is cut
+          if ((x + h - x2) * (x + h - x1) > 0.0) h = x2 - x;
+          for (;;) {  // rkqs: Cash-Karp trial steps until the error is within eps
+            set_stage(x + .2 * h,
+                      [&](int q) { return make_double2(y[q].x + kCkB21 * h * k1[q].x, y[q].y + kCkB21 * h * k1[q].y); },
+                      [&](int i) { return cls_get(*C, i) + kCkB21 * h * cls_get(*K1, i); });
+            rhs<T, NS>(d, sm, x + .2 * h, CT, ns, k2, KC, potv);
+            if (tid == 0) KS[0] = *KC;
+            set_stage(x + .3 * h,
+                      [&](int q) {
+                        return make_double2(y[q].x + h * (kCkB31 * k1[q].x + kCkB32 * k2[q].x),
+                                            y[q].y + h * (kCkB31 * k1[q].y + kCkB32 * k2[q].y));
+                      },
+                      [&](int i) {
+                        return cls_get(*C, i) + h * (kCkB31 * cls_get(*K1, i) + kCkB32 * cls_get(KS[0], i));
+                      });
+            rhs<T, NS>(d, sm, x + .3 * h, CT, ns, k3, KC, potv);
+            if (tid == 0) KS[1] = *KC;
+            set_stage(x + kCkA4 * h,
+                      [&](int q) {
+                        return make_double2(
+                            y[q].x + h * (kCkB41 * k1[q].x + kCkB42 * k2[q].x + kCkB43 * k3[q].x),
+                            y[q].y + h * (kCkB41 * k1[q].y + kCkB42 * k2[q].y + kCkB43 * k3[q].y));
+                      },
+                      [&](int i) {
+                        return cls_get(*C, i) + h * (kCkB41 * cls_get(*K1, i) + kCkB42 * cls_get(KS[0], i) +
+                                                     kCkB43 * cls_get(KS[1], i));
+                      });
+            rhs<T, NS>(d, sm, x + kCkA4 * h, CT, ns, k4, KC, potv);
+            if (tid == 0) KS[2] = *KC;
+            set_stage(x + 1.0 * h,
+                      [&](int q) {
+                        return make_double2(y[q].x + h * (kCkB51 * k1[q].x + kCkB52 * k2[q].x +
+                                                          kCkB53 * k3[q].x + kCkB54 * k4[q].x),
+                                            y[q].y + h * (kCkB51 * k1[q].y + kCkB52 * k2[q].y +
+                                                          kCkB53 * k3[q].y + kCkB54 * k4[q].y));
+                      },
+                      [&](int i) {
+                        return cls_get(*C, i) + h * (kCkB51 * cls_get(*K1, i) + kCkB52 * cls_get(KS[0], i) +
+                                                     kCkB53 * cls_get(KS[1], i) + kCkB54 * cls_get(KS[2], i));
+                      });
+            rhs<T, NS>(d, sm, x + 1.0 * h, CT, ns, k5, KC, potv);
+            if (tid == 0) KS[3] = *KC;
+            set_stage(x + .875 * h,
+                      [&](int q) {
+                        return make_double2(
+                            y[q].x + h * (kCkB61 * k1[q].x + kCkB62 * k2[q].x + kCkB63 * k3[q].x +
+                                          kCkB64 * k4[q].x + kCkB65 * k5[q].x),
+                            y[q].y + h * (kCkB61 * k1[q].y + kCkB62 * k2[q].y + kCkB63 * k3[q].y +
+                                          kCkB64 * k4[q].y + kCkB65 * k5[q].y));
+                      },
+                      [&](int i) {
+                        return cls_get(*C, i) + h * (kCkB61 * cls_get(*K1, i) + kCkB62 * cls_get(KS[0], i) +
+                                                     kCkB63 * cls_get(KS[1], i) + kCkB64 * cls_get(KS[2], i) +
+                                                     kCkB65 * cls_get(KS[3], i));
+                      });
+            rhs<T, NS>(d, sm, x + .875 * h, CT, ns, k, KC, potv);  // k = stage 6
+            double em = 0.0;
+#pragma unroll
+            for (int q = 0; q < NS; ++q)
+              if (q < ns) {
+                yo[q] = make_double2(
+                    y[q].x + h * (kCkC1 * k1[q].x + kCkC3 * k3[q].x + kCkC4 * k4[q].x + kCkC6 * k[q].x),
+                    y[q].y + h * (kCkC1 * k1[q].y + kCkC3 * k3[q].y + kCkC4 * k4[q].y + kCkC6 * k[q].y));
+                ye[q] = make_double2(h * (kCkDC1 * k1[q].x + kCkDC3 * k3[q].x + kCkDC4 * k4[q].x +
+                                          kCkDC5 * k5[q].x + kCkDC6 * k[q].x),
+                                     h * (kCkDC1 * k1[q].y + kCkDC3 * k3[q].y + kCkDC4 * k4[q].y +
+                                          kCkDC5 * k5[q].y + kCkDC6 * k[q].y));
+                em = fmax(em, fabs(ye[q].x / (fabs(y[q].x) + fabs(hs * k1[q].x) + 1e-30)));
+                em = fmax(em, fabs(ye[q].y / (fabs(y[q].y) + fabs(hs * k1[q].y) + 1e-30)));
+              }
+            if (tid == 0 && !at) {
+              Cls o, e;
+              for (int i = 0; i < 6; ++i) {
+                const double c1 = cls_get(*K1, i), c3 = cls_get(KS[1], i), c4 = cls_get(KS[2], i),
+                             c5 = cls_get(KS[3], i), c6 = cls_get(*KC, i), c0 = cls_get(*C, i);
+                cls_ref(o, i) = c0 + h * (kCkC1 * c1 + kCkC3 * c3 + kCkC4 * c4 + kCkC6 * c6);
+                cls_ref(e, i) = h * (kCkDC1 * c1 + kCkDC3 * c3 + kCkDC4 * c4 + kCkDC5 * c5 + kCkDC6 * c6);
+                em = fmax(em, fabs(cls_get(e, i) / (fabs(c0) + fabs(hs * c1) + 1e-30)));
+              }
+              *CO = o;
+              *CE = e;
+            }
+            if (h <= d.ode_hmin) break;  // at or below the minimum step: accepted as it is
+            em = block_max(em, sm.red) / d.ode_eps;
+            if (em > 1.0) {
+              const double htemp = 0.9 * h * pow(em, -0.25);
+              h = fmax(fabs(htemp), 0.1 * fabs(h));
+              continue;
+            }
+            hnext = em > 1.89e-4 ? 0.9 * h * pow(em, -0.2) : 5.0 * h;
+            break;
+          }
+          x = x + h;
+#pragma unroll
+          for (int q = 0; q < NS; ++q)
+            if (q < ns) y[q] = yo[q];
+          if (tid == 0 && !at) *C = *CO;
+          __syncthreads();
+          if ((x - x2) * (x2 - x1) >= 0.0) break;
+          if (fabs(hnext) < d.ode_hmin) hnext = d.ode_hmin;
+          h = hnext;
+        }
+        dt_step = hnext;
+        if (at) {
+          last = true;
+          dt = x2 - tcur;
+        }
+      } else {
       if (at && tcur + dt >= t_end) {
         dt = t_end - tcur;
         last = true;
       }
-      const double hh = dt * 0.5, h6 = dt / 6.0;
+      const double hh = dt * 0.5;
+      h6 = dt / 6.0;
       // RK4 (MQCT_SOURCE_CODES/suppl_routines.f:1076-1113): stage s evaluates
       // at t + {0, h/2, h/2, h} and y + {0, h/2 k1, h/2 k2, h k3}
       for (int st = 0; st < 4; ++st) {
@@ -531,25 +771,8 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
         if (st == 0) {
 #pragma unroll
           for (int q = 0; q < NS; ++q) k1[q] = k[q];
-          if (tid == 0) {
-            *K1 = *KC;
-            // the state before the step, with its coupling energy
-            if (out.rec && !at) save_record(out, tr, bk->n_rec, tcur, *C, potv);
-          }
-          if (counter == 1 && !at) {  // initial energies, MQCT_SOURCE_CODES/propagator.f:2695-2810
-            double q0 = 0.0, z1 = 0.0, z2 = 0.0;
-#pragma unroll
-            for (int q = 0; q < NS; ++q)
-              if (q < ns) {
-                const int i = tid + q * PT;
-                q0 += (y[q].x * y[q].x + y[q].y * y[q].y) * d.e_val[d.st_e[i]];
-              }
-            block_sum3(q0, z1, z2, sm.red);
-            if (tid == 0) {
-              bk->eqi = q0 + potv;
-              bk->eki = kinetic(*C, d.mass);
-            }
-          }
+          if (tid == 0) *K1 = *KC;
+          first_rhs(potv);  // record of the state before the step; initial energies
         } else if (st == 1) {
 #pragma unroll
           for (int q = 0; q < NS; ++q) k23[q] = k[q];
@@ -565,18 +788,22 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
         if (q < ns)
           y[q] = make_double2(y[q].x + h6 * (k1[q].x + k[q].x + 2.0 * k23[q].x),
                               y[q].y + h6 * (k1[q].y + k[q].y + 2.0 * k23[q].y));
-      tcur += dt;
+      }
+      if (kAdaptive && at) tcur = t_end;
+      else tcur += dt;
       if (tid == 0) {
         bool run = !last;
         if (!at) {
           Cls& c = *C;
-          const Cls &a1 = *K1, &a23 = *K23, &a4 = *KC;
-          c.R += h6 * (a1.R + a4.R + 2.0 * a23.R);
-          c.PR += h6 * (a1.PR + a4.PR + 2.0 * a23.PR);
-          c.th += h6 * (a1.th + a4.th + 2.0 * a23.th);
-          c.Pth += h6 * (a1.Pth + a4.Pth + 2.0 * a23.Pth);
-          c.phi += h6 * (a1.phi + a4.phi + 2.0 * a23.phi);
-          c.Pphi += h6 * (a1.Pphi + a4.Pphi + 2.0 * a23.Pphi);
+          if constexpr (!kAdaptive) {  // the RK4 step of the classical variables
+            const Cls &a1 = *K1, &a23 = *K23, &a4 = *KC;
+            c.R += h6 * (a1.R + a4.R + 2.0 * a23.R);
+            c.PR += h6 * (a1.PR + a4.PR + 2.0 * a23.PR);
+            c.th += h6 * (a1.th + a4.th + 2.0 * a23.th);
+            c.Pth += h6 * (a1.Pth + a4.Pth + 2.0 * a23.Pth);
+            c.phi += h6 * (a1.phi + a4.phi + 2.0 * a23.phi);
+            c.Pphi += h6 * (a1.Pphi + a4.Pphi + 2.0 * a23.Pphi);
+          }
           // stop rules, MQCT_SOURCE_CODES/propagator.f:4011-4050
           const double uR = c.R;
           if (tcur - dt > dt && counter > 2) {
@@ -677,17 +904,43 @@ struct PropPlan {
   int n_sm = 148;
   int ns = 1;  // states per thread, power of two
 
-  template <class T>
+  int method = MQCT_INTEG_RK4;
+  double ode_eps = 1e-6, ode_hmin = 0.0;
+
+  template <class T, bool A>
   static const void* pick(int ns) {
     switch (ns) {
-      case 1: return (const void*)propagate_kernel<T, 1>;
-      case 2: return (const void*)propagate_kernel<T, 2>;
-      case 4: return (const void*)propagate_kernel<T, 4>;
-      default: return (const void*)propagate_kernel<T, 8>;
+      case 1: return (const void*)propagate_kernel<T, 1, A>;
+      case 2: return (const void*)propagate_kernel<T, 2, A>;
+      case 4: return (const void*)propagate_kernel<T, 4, A>;
+      default: return (const void*)propagate_kernel<T, 8, A>;
     }
   }
   const void* kernel_ptr() const {
-    return arith == MQCT_PROP_FP32 ? pick<float>(ns) : pick<double>(ns);
+    if (method == MQCT_INTEG_ODEINT)
+      return arith == MQCT_PROP_FP32 ? pick<float, true>(ns) : pick<double, true>(ns);
+    return arith == MQCT_PROP_FP32 ? pick<float, false>(ns) : pick<double, false>(ns);
+  }
+
+  int set_integrator(const mqct_integrator_t* in) {
+    MQCT_ARG_CHECK(in, "null integrator");
+    MQCT_ARG_CHECK(in->method == MQCT_INTEG_RK4 || in->method == MQCT_INTEG_ODEINT,
+                   "unknown integrator %d", in->method);
+    if (in->method == MQCT_INTEG_ODEINT) {
+      MQCT_ARG_CHECK(in->eps > 0.0 && in->hmin >= 0.0, "ODEINT needs eps > 0 and hmin >= 0");
+      // the error control resolves every component to relative eps of |y| + |h dy/dt|;
+      // FP32 rounding of the right-hand side (matrix, phases) leaves an error estimate
+      // for small amplitudes that does not shrink with h, so the steps collapse
+      MQCT_ARG_CHECK(arith == MQCT_PROP_FP64,
+                     "ODEINT needs FP64 arithmetic (FP32 rounding of the right-hand side "
+                     "defeats its error control on small amplitudes)");
+    }
+    method = in->method;
+    ode_eps = in->eps;
+    ode_hmin = in->hmin;
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_bytes()));
+    return MQCT_OK;
   }
   size_t tsize() const { return arith == MQCT_PROP_FP32 ? 4 : 8; }
 
@@ -695,7 +948,7 @@ struct PropPlan {
   size_t smem_fixed() const {
     const size_t t2 = 2 * tsize();
     auto a = [](size_t x) { return (x + 15) & ~size_t(15); };
-    return a(sizeof(Cls) * 5) + a(sizeof(Book)) + a(sizeof(double) * 3 * (PT / 32)) + a(16) +
+    return a(sizeof(Cls) * kClsSlots) + a(sizeof(Book)) + a(sizeof(double) * 3 * (PT / 32)) + a(16) +
            a(8 * (size_t)nR) +
            a(16 * (size_t)N) + 3 * a(t2 * N) + a(t2 * n_e);
   }
@@ -886,6 +1139,8 @@ struct PropPlan {
     d.mass = mass;
     d.mode = mode;
     d.mp_cap = mp_cap;
+    d.ode_eps = ode_eps;
+    d.ode_hmin = ode_hmin;
     d.at_off = d_at_off.p; d.at_n = d_at_n.p; d.at_rec = d_at_rec.p; d.at_y2 = d_at_y2.p;
     return d;
   }
@@ -1075,6 +1330,29 @@ int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms) {
 }
 
 void mqct_prop_plan_destroy(mqct_prop_plan* plan) { delete reinterpret_cast<PropPlan*>(plan); }
+
+int mqct_prop_plan_set_integrator(mqct_prop_plan* plan, const mqct_integrator_t* integ) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  return reinterpret_cast<PropPlan*>(plan)->set_integrator(integ);
+}
+
+int mqct_propagate_batch_integ(const mqct_tables_t* tab, const mqct_traj_init_t* init,
+                               int64_t n_traj, int32_t mode, const mqct_at_paths_t* at,
+                               int32_t arith, const mqct_integrator_t* integ, double* amp_out,
+                               double* cls_out, double* diag_out) {
+  MQCT_ARG_CHECK(init && amp_out && cls_out && diag_out && integ, "null argument");
+  MQCT_ARG_CHECK(mode == MQCT_MODE_STD || mode == MQCT_MODE_AT, "unknown mode %d", mode);
+  mqct_prop_plan* h = nullptr;
+  int rc = mqct_prop_plan_create(tab, arith, &h);
+  if (rc) return rc;
+  PropPlan* p = reinterpret_cast<PropPlan*>(h);
+  rc = p->set_integrator(integ);
+  if (!rc) rc = validate_init(init, n_traj, p->N, mode);
+  if (!rc && mode == MQCT_MODE_AT) rc = p->set_at(at, n_traj);
+  if (!rc) rc = run_host(p, init, n_traj, mode, amp_out, cls_out, diag_out);
+  mqct_prop_plan_destroy(h);
+  return rc;
+}
 
 int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init, int64_t n_traj,
                          int32_t mode, const mqct_at_paths_t* at, int32_t arith,

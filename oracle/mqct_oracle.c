@@ -1052,6 +1052,94 @@ static void orc_rk4(int n, double* y, const double* dydx, double x, double h, or
   f(ctx, x + h, yt, dyt);
   for (int i = 0; i < n; ++i) y[i] = y[i] + h6 * (dydx[i] + dyt[i] + 2.0 * dym[i]);
 }
+/* Adaptive step-size control, SRC/suppl_routines.f:1229-1435 (rkqs, rkck, odeint as
+ * the reference modified them): Cash-Karp 5(4) steps, error max_i |yerr_i / yscal_i|
+ * / eps with yscal_i = |y_i| + |h dydx_i| + 1e-30, shrink 0.9 h err^-1/4 (at least
+ * h/10), grow 0.9 h err^-1/5 or 5 h below err 1.89e-4; a step at or below hmin is
+ * accepted as it is; the step is cut to land on x2; at most 10000 steps, the last
+ * one an RK4 step over the remainder. */
+static const double ORC_CK_A4 = (double)0.6f; /* A4 = .6 is a default-real literal there */
+static void orc_rkck(int n, const double* y, const double* dydx, double x, double h,
+                     orc_rhs_fn f, void* ctx, double* yout, double* yerr, double* ak,
+                     double* yt) {
+  const double B21 = .2, B31 = 3.0 / 40.0, B32 = 9.0 / 40.0, B41 = .3, B42 = -.9, B43 = 1.2,
+               B51 = -11.0 / 54.0, B52 = 2.5, B53 = -70.0 / 27.0, B54 = 35.0 / 27.0,
+               B61 = 1631.0 / 55296.0, B62 = 175.0 / 512.0, B63 = 575.0 / 13824.0,
+               B64 = 44275.0 / 110592.0, B65 = 253.0 / 4096.0, C1 = 37.0 / 378.0,
+               C3 = 250.0 / 621.0, C4 = 125.0 / 594.0, C6 = 512.0 / 1771.0,
+               DC1 = C1 - 2825.0 / 27648.0, DC3 = C3 - 18575.0 / 48384.0,
+               DC4 = C4 - 13525.0 / 55296.0, DC5 = -277.0 / 14336.0, DC6 = C6 - .25;
+  double *ak2 = ak, *ak3 = ak + n, *ak4 = ak + 2 * n, *ak5 = ak + 3 * n, *ak6 = ak + 4 * n;
+  for (int i = 0; i < n; ++i) yt[i] = y[i] + B21 * h * dydx[i];
+  f(ctx, x + .2 * h, yt, ak2);
+  for (int i = 0; i < n; ++i) yt[i] = y[i] + h * (B31 * dydx[i] + B32 * ak2[i]);
+  f(ctx, x + .3 * h, yt, ak3);
+  for (int i = 0; i < n; ++i) yt[i] = y[i] + h * (B41 * dydx[i] + B42 * ak2[i] + B43 * ak3[i]);
+  f(ctx, x + ORC_CK_A4 * h, yt, ak4);
+  for (int i = 0; i < n; ++i)
+    yt[i] = y[i] + h * (B51 * dydx[i] + B52 * ak2[i] + B53 * ak3[i] + B54 * ak4[i]);
+  f(ctx, x + 1.0 * h, yt, ak5);
+  for (int i = 0; i < n; ++i)
+    yt[i] = y[i] + h * (B61 * dydx[i] + B62 * ak2[i] + B63 * ak3[i] + B64 * ak4[i] + B65 * ak5[i]);
+  f(ctx, x + .875 * h, yt, ak6);
+  for (int i = 0; i < n; ++i) yout[i] = y[i] + h * (C1 * dydx[i] + C3 * ak3[i] + C4 * ak4[i] + C6 * ak6[i]);
+  for (int i = 0; i < n; ++i)
+    yerr[i] = h * (DC1 * dydx[i] + DC3 * ak3[i] + DC4 * ak4[i] + DC5 * ak5[i] + DC6 * ak6[i]);
+}
+static void orc_rkqs(int n, double* y, const double* dydx, double* x, double htry, double eps,
+                     const double* yscal, double* hnext, double hmin, orc_rhs_fn f, void* ctx,
+                     double* ytemp, double* yerr, double* ak, double* yt) {
+  double h = htry;
+  for (;;) {
+    orc_rkck(n, y, dydx, *x, h, f, ctx, ytemp, yerr, ak, yt);
+    if (h <= hmin) break; /* accepted as it is; hnext keeps its value */
+    double errmax = 0.0;
+    for (int i = 0; i < n; ++i) errmax = fmax(errmax, fabs(yerr[i] / yscal[i]));
+    errmax = errmax / eps;
+    if (errmax > 1.0) {
+      const double htemp = 0.9 * h * pow(errmax, -0.25);
+      h = copysign(fmax(fabs(htemp), 0.1 * fabs(h)), h);
+      continue;
+    }
+    *hnext = errmax > 1.89e-4 ? 0.9 * h * pow(errmax, -0.2) : 5.0 * h;
+    break;
+  }
+  *x = *x + h;
+  for (int i = 0; i < n; ++i) y[i] = ytemp[i];
+}
+static void orc_rk4(int n, double* y, const double* dydx, double x, double h, orc_rhs_fn f,
+                    void* ctx, double* yt, double* dyt, double* dym);
+/* ystart advanced from x1 to x2; h1 the first trial step, *hnext_io receives the last
+ * proposed step (dt_corrected); returns the number of steps taken. */
+static int orc_odeint(int n, double* ystart, double x1, double x2, double eps, double h1,
+                      double hmin, orc_rhs_fn f, void* ctx, double* hnext_io) {
+  const int MAXSTP = 10000;
+  double* w = (double*)calloc((size_t)n * 11, sizeof(double));
+  double *y = w, *dydx = w + n, *yscal = w + 2 * n, *ytemp = w + 3 * n, *yerr = w + 4 * n,
+         *yt = w + 5 * n, *ak = w + 6 * n;
+  double x = x1, h = copysign(h1, x2 - x1), hnext = h;
+  int nstp;
+  for (int i = 0; i < n; ++i) y[i] = ystart[i];
+  for (nstp = 1; nstp <= MAXSTP; ++nstp) {
+    f(ctx, x, y, dydx);
+    if (nstp < MAXSTP) {
+      for (int i = 0; i < n; ++i) yscal[i] = fabs(y[i]) + fabs(h * dydx[i]) + 1e-30;
+      if ((x + h - x2) * (x + h - x1) > 0.0) h = x2 - x;
+      orc_rkqs(n, y, dydx, &x, h, eps, yscal, &hnext, hmin, f, ctx, ytemp, yerr, ak, yt);
+    } else {  /* the last allowed step: RK4 over what remains */
+      orc_rk4(n, y, dydx, x, x2 - x, f, ctx, yt, ytemp, yerr);
+      x = x2 + copysign(1e-30, x2 - x1);
+    }
+    if ((x - x2) * (x2 - x1) >= 0.0) break;
+    if (fabs(hnext) < hmin) hnext = copysign(hmin, x2 - x1);
+    h = hnext;
+  }
+  for (int i = 0; i < n; ++i) ystart[i] = y[i];
+  *hnext_io = hnext;
+  free(w);
+  return nstp;
+}
+
 static void orc_rhs_std(void* ctx, double t, const double* y, double* dy) {
   orc_derivs_ws((orc_rhs_ws*)ctx, t, y, dy);
 }
@@ -1121,6 +1209,7 @@ static int orc_dotraject_impl(const orc_tables* tab, const orc_traj* tr, double*
     double Eki = pr * pr / 2.0 / mass + l * l / 2.0 / mass / (R * R) +
                  qphi * qphi / 2.0 / mass / (R * R) / (sin(ql) * sin(ql));
     double tmp_R1 = 0.0, tmp_R2 = 0.0;
+    double dt_step = tr->dt; /* ODEINT's carried step (dt_step / dt_corrected) */
     int run = 1;
     while (run) {
       ++counter;
@@ -1134,8 +1223,14 @@ static int orc_dotraject_impl(const orc_tables* tab, const orc_traj* tr, double*
         }
         ++nr;
       }
-      orc_derivs_ws(&w, tcur, q, dq);
-      orc_rk4(n, q, dq, tcur, tr->dt, orc_rhs_std, &w, yt, dyt, dym);
+      if (tr->method == 1) {  /* PROPAGATOR = ODEINT: adaptive steps over [t, t + dt] */
+        double hn;
+        orc_odeint(n, q, tcur, tcur + tr->dt, tr->eps, dt_step, tr->hmin, orc_rhs_std, &w, &hn);
+        dt_step = hn;
+      } else {
+        orc_derivs_ws(&w, tcur, q, dq);
+        orc_rk4(n, q, dq, tcur, tr->dt, orc_rhs_std, &w, yt, dyt, dym);
+      }
       double uR = q[2 * N], uphi = q[2 * N + 4];
       if (tcur > (0.0 + tr->dt) && counter > 2) {
         if ((tmp_R2 - tmp_R1) < 0.0 && (tmp_R1 - uR) > 0.0) vib += 1;
@@ -1283,6 +1378,13 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   double t_end = t[n_at - 1];
   int64_t counter = 0;
   int run = 1;
+  if (tr->method == 1) {  /* ODEINT: one adaptive call over the whole path (:3888-3905) */
+    double hn;
+    orc_odeint(n, q, tcur, t_end, tr->eps, dt, tr->hmin, orc_rhs_at, &c, &hn);
+    tcur = t_end;
+    counter = 1;
+    run = 0;
+  }
   while (run) {
     ++counter;
     if ((tcur + dt) >= t_end) {

@@ -147,6 +147,9 @@ typedef struct orc_traj {
   int32_t numb_oscl_prds;  /* stop after this many R oscillations (default 1) */
   double time_lim;         /* <=0: none */
   int64_t max_steps;
+  int32_t method;          /* 0: RK4 (PROPAGATOR = RK4), 1: adaptive Cash-Karp (ODEINT) */
+  double eps;              /* ODEINT accuracy (eps_odeint) */
+  double hmin;             /* ODEINT minimum step (min_t_stp) */
 } orc_traj;
 
 /* Per-trajectory output: amp[2N] (Re, Im), cls[6] = (R,P_R,theta,P_theta,phi,P_phi),

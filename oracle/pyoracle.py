@@ -51,7 +51,8 @@ class Traj(C.Structure):
     _fields_ = [("e_coll", C.c_double), ("l_real", C.c_double), ("s_st", C.c_int32),
                 ("dt", C.c_double), ("r_start", C.c_double), ("r_fin", C.c_double),
                 ("numb_orb_prds", C.c_int32), ("numb_oscl_prds", C.c_int32),
-                ("time_lim", C.c_double), ("max_steps", C.c_int64)]
+                ("time_lim", C.c_double), ("max_steps", C.c_int64), ("method", C.c_int32),
+                ("eps", C.c_double), ("hmin", C.c_double)]
 
 
 def build() -> str:
@@ -318,8 +319,11 @@ class OracleTables:
 
 
 def make_traj(e_coll, l_real, s_st, dt, r_start, r_fin, numb_orb=1, numb_oscl=1, time_lim=0.0,
-              max_steps=0):
-    return Traj(e_coll, l_real, s_st, dt, r_start, r_fin, numb_orb, numb_oscl, time_lim, max_steps)
+              max_steps=0, method=0, eps=1e-6, hmin=0.0):
+    """method 0: RK4 with step dt; 1: adaptive Cash-Karp (ODEINT) with accuracy eps and
+    minimum step hmin inside every interval dt."""
+    return Traj(e_coll, l_real, s_st, dt, r_start, r_fin, numb_orb, numb_oscl, time_lim, max_steps,
+                method, eps, hmin)
 
 
 def propagate_batch(tables, trajs, n_threads=0):

@@ -1,0 +1,66 @@
+"""The oracle's adaptive integrator (PROPAGATOR = ODEINT: Cash-Karp steps with error
+control, MQCT_SOURCE_CODES/suppl_routines.f:1229-1435) against the reference's own
+RK4 results.  No reference example runs ODEINT, so this checks the restatement
+through the physics: with a tight enough accuracy the adaptive runs reproduce the
+per-trajectory probabilities the reference printed for its RK4 runs (H2O + H2
+standard MQCT, G3; H2O + H2O AT-MQCT second run, G1)."""
+import numpy as np
+
+from test_oracle_g1 import AMU as AMU1, KCAL, _g1, _systems, _tables
+from test_oracle_golden import AMU, AUTOEV, EVTOWN, _g3, _g3_tables
+
+
+def test_odeint_standard_mode_matches_reference_rk4(oracle):
+    g = _g3()
+    tab, _, _ = _g3_tables(oracle, g)
+    U = float(g["U"])
+    E = U / EVTOWN / AUTOEV
+    dt = float(g["time_step"]) / np.sqrt(U / 300.0)
+    rmax = float(g["rmax"])
+    st = g["states"]
+    N = len(st)
+    ls = [40, 80, 110]
+    trajs = [oracle.make_traj(E, float(l), 1, dt, rmax, rmax, 1, 1, float(g["time_lim"]), 0,
+                              method=1, eps=1e-5, hmin=0.0) for l in ls]
+    amp, cls, diag = oracle.propagate_batch(tab, trajs)
+    p = amp[:, :N] ** 2 + amp[:, N:] ** 2
+    prob = np.zeros((len(ls), 10))
+    for s in range(N):
+        prob[:, st[s, 1] - 1] += p[:, s]
+    ref = g["opacity"][ls, 2:]
+    assert np.max(np.abs(prob - ref)) < 1e-6
+    # the outer steps dt and the stop rules are those of the RK4 run
+    assert np.allclose(diag[:, 0], g["deflection"][ls, 4], rtol=2e-8)
+    assert np.all(diag[:, 2] < 1e-8)       # norm conservation
+
+
+def test_odeint_at_mode_matches_reference_rk4(mq, oracle):
+    g = _g1()
+    R, lab, T = g["R"], g["labels"], g["terms"]
+    mass = float(g["mass_red"]) * AMU1
+    U = float(g["U"])
+    E = U / EVTOWN / AUTOEV
+    rmax = float(g["rmax"])
+    s1, o1 = _systems(mq, oracle, g, g["channels"][:1])
+    tab1 = _tables(oracle, s1, oracle.expansion_matrix_type0(o1, o1.states(), s1.ind_mat, lab, T,
+                                                             1.0 / KCAL), R, mass)
+    s9, o9 = _systems(mq, oracle, g, g["channels"])
+    tab9 = _tables(oracle, s9, oracle.expansion_matrix_type0(o9, o9.states(), s9.ind_mat, lab, T,
+                                                             1.0 / KCAL), R, mass)
+    dt1 = float(g["time_step1"]) / np.sqrt(U / 300.0)
+    dt2 = float(g["time_step2"]) / np.sqrt(U / 300.0)
+    N = s9.n_states
+    for l in (85, 199):
+        tr = oracle.make_traj(E, float(l), 1, dt1, rmax, rmax, 1, 1, float(g["time_lim"]))
+        path = oracle.dotraject_record(tab1, tr)[3]
+        # one adaptive call over the whole path; the minimum step keeps the step count
+        # within odeint's 10000 (with hmin = 0 the amplitudes that start at zero drive
+        # the step to nothing, in the reference's scheme as here)
+        tr2 = oracle.make_traj(E, float(l), 1, dt2, rmax, rmax, 1, 1, float(g["time_lim"]), 0,
+                               method=1, eps=1e-6, hmin=20.0)
+        amp, diag = oracle.dotraject_at(tab9, tr2, path)
+        prob = np.zeros(9)
+        np.add.at(prob, s9.indx_chann - 1, amp[:N] ** 2 + amp[N:] ** 2)
+        i = list(g["l"]).index(l)
+        assert np.max(np.abs(prob - g["opacity2"][i, 2:])) < 1e-6
+        assert diag[0] == path[-1, 0] and diag[2] < 1e-10
