@@ -333,6 +333,22 @@ int mqct_propagate_batch_integ(const mqct_tables_t* tab, const mqct_traj_init_t*
                                int32_t arith, const mqct_integrator_t* integ, double* amp_out,
                                double* cls_out, double* diag_out);
 
+/* INELAST_CALC on the device (MQCT_SOURCE_CODES/propagator.f:4752-4851) from device
+ * amplitudes d_amp (n_traj x 2 n_states, the layout of mqct_propagate_batch's amp_out;
+ * trajectory t covers the l bin [L_MIN + t DL, L_MIN + (t + 1) DL)): per trajectory the
+ * channel probabilities d_prob (n_traj x n_channels), the J-resolved cross sections
+ * d_partial ((J_up - J_down + 1) x n_channels, PARTIAL_CROSS_SECTIONS_J.out) and their
+ * sums d_sigma (n_channels, M_PROJ_CROSSECTIONS.out), all in Angstrom^2, for the initial
+ * j12 = j_ini; the l of partial wave J maps to trajectory (l - L_MIN) / DL (TRAJ_ORB,
+ * :5127-5134).  indx_chann (host, per state, 1-based) must be channel-major; at most
+ * 2048 channels.  Runs on `stream` (cudaStream_t, NULL: the default stream), allocates
+ * nothing and returns without synchronising. */
+int mqct_cross_sections_device(const double* d_amp, int64_t n_traj, int32_t n_states,
+                               const int32_t* indx_chann, int32_t n_channels, int32_t j_ini,
+                               int32_t J_down, int32_t J_up, int32_t L_min, int32_t dl,
+                               double k_vec, double* d_prob, double* d_partial, double* d_sigma,
+                               void* stream);
+
 typedef struct mqct_prop_plan mqct_prop_plan;
 int mqct_prop_plan_create(const mqct_tables_t* tab, int32_t arith, mqct_prop_plan** plan);
 int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,

@@ -24,7 +24,8 @@ from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_F
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
-           "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections", "write_mtrx_uf",
+           "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections",
+           "cross_sections_device", "write_mtrx_uf",
            "read_mtrx_uf", "write_mtrx_dat", "read_mtrx_dat", "read_expansion_terms",
            "spline_y2", "Surrogate", "build_matrix_expansion", "E_UNIT", "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
@@ -613,6 +614,29 @@ def cross_sections(prob, j_ini, J_down, J_up, L_min, k_vec, U_cm=None, e_ch=None
     dE = np.asarray(e_ch) - e_ch[chann_ini - 1]
     e_bill = U_cm + dE / 2.0 + dE ** 2 / 16.0 / U_cm
     return sig_U, sig_U * U_cm / e_bill, e_bill
+
+
+def cross_sections_device(d_amp, system: CollisionSystem, j_ini, J_down, J_up, L_min, k_vec,
+                          dl=1):
+    """INELAST_CALC on the GPU from device amplitudes (a CUDA float64 torch tensor, n_traj x
+    2N, as propagate returns them): returns CUDA tensors (prob [n_traj, n_channels],
+    partial [J_up - J_down + 1, n_channels], sigma [n_channels]), cross sections in
+    Angstrom^2, computed on torch's current stream."""
+    import torch
+    amp = d_amp.contiguous()
+    if amp.dtype != torch.float64 or not amp.is_cuda or amp.shape[1] != 2 * system.n_states:
+        raise ValueError("d_amp must be a CUDA float64 tensor of shape (n_traj, 2 n_states)")
+    n_traj, nch = amp.shape[0], system.n_channels
+    prob = torch.empty((n_traj, nch), dtype=torch.float64, device=amp.device)
+    partial = torch.empty((J_up - J_down + 1, nch), dtype=torch.float64, device=amp.device)
+    sigma = torch.empty(nch, dtype=torch.float64, device=amp.device)
+    stream = torch.cuda.current_stream(amp.device).cuda_stream
+    check(lib().mqct_cross_sections_device(amp.data_ptr(), n_traj, system.n_states,
+                                           np.ascontiguousarray(system.indx_chann, np.int32), nch,
+                                           j_ini, J_down, J_up, L_min, dl, k_vec,
+                                           prob.data_ptr(), partial.data_ptr(), sigma.data_ptr(),
+                                           stream))
+    return prob, partial, sigma
 
 
 def write_mtrx_uf(path, system: CollisionSystem, R, mat):

@@ -184,9 +184,13 @@ def main(ref_root):
         t = line.split()
         if len(t) == 2 and t[0].isdigit():
             sig2m.append(float(t[1]))
+    # J-resolved cross sections (Angstrom^2) of PARTIAL_CROSS_SECTIONS_J.out: J, 9 channels
+    part = np.array([[float(x) for x in ln.split()]
+                     for ln in open(os.path.join(d2, "PARTIAL_CROSS_SECTIONS_J.out"))
+                     if len(ln.split()) == 10 and ln.split()[0].isdigit()])
     np.savez_compressed(
         os.path.join(out, "g1_h2o_h2o_at.npz"), labels=lab, R=rows[:, 0], terms=rows[:, 1:],
-        sigma2_mproj=np.array(sig2m),
+        sigma2_mproj=np.array(sig2m), partial2=part,
         l=ls, n_rec=np.array(n_rec), rec_head=np.array(heads), rec_mid=np.array(mids),
         rec_tail=np.array(tails),
         opacity2=_read_table(os.path.join(d2, "OPACITY_FUNCTIONS_L.out"), 11),

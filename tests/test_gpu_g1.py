@@ -84,3 +84,26 @@ def test_at_run_matches_reference(mq, g1, arith):
         assert np.allclose(sig, g["sigma2_mproj"], rtol=1e-8, atol=0)
     else:
         assert np.allclose(sig, g["sigma2_mproj"], rtol=1e-3, atol=0)
+
+
+def test_cross_sections_on_the_device(mq, g1):
+    """INELAST_CALC on the GPU from device amplitudes: channel probabilities, the
+    J-resolved cross sections of PARTIAL_CROSS_SECTIONS_J.out and their sums."""
+    import torch
+    g, meta = g1["g"], g1["meta"]
+    amp, _, _ = mq.propagate(g1["tab9"], g1["trajs2"], arith=mq.PROP_FP64, mode=mq.MODE_AT,
+                             at_paths=g1["paths"])
+    s9 = g1["s9"][0]
+    d_amp = torch.from_numpy(amp).cuda()
+    prob, partial, sigma = mq.cross_sections_device(d_amp, s9, 0, meta["J_down"], meta["J_up"],
+                                                    meta["L_min"], meta["k"], dl=meta["dl"])
+    torch.cuda.synchronize()
+    p_host = mq.channel_probabilities(amp, s9.indx_chann, 9)
+    assert np.allclose(prob.cpu().numpy(), p_host, rtol=1e-14, atol=1e-16)
+    s_host = mq.cross_sections(p_host, 0, meta["J_down"], meta["J_up"], meta["L_min"], meta["k"],
+                               dl=meta["dl"])
+    assert np.allclose(sigma.cpu().numpy(), s_host, rtol=1e-13)
+    ref = g["partial2"][:, 1:]
+    assert partial.shape == ref.shape
+    assert np.max(np.abs(partial.cpu().numpy() - ref) / ref) < 2e-7
+    assert np.allclose(sigma.cpu().numpy(), g["sigma2_mproj"], rtol=1e-8)

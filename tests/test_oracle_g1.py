@@ -137,3 +137,15 @@ def test_host_trajectory_set_and_cross_sections_with_dl(mq, oracle, g1_run):
     ref = oracle.inelast(9, 0, 0, meta["J_up"], 0, g1_run["prob"], g1_run["k"], dl=19) * ABOHR ** 2
     assert np.allclose(sig, ref, rtol=1e-13)
     assert np.allclose(sig, g["sigma2_mproj"], rtol=2e-9)
+
+
+def test_partial_cross_sections_per_j(g1_run):
+    """PARTIAL_CROSS_SECTIONS_J.out of the second run: per total J the cross section
+    pi/k^2 (2J+1) P_f(traj(J)) (j_ini = 0, l = J) in Angstrom^2, traj(l) = (l - L_MIN)/DL."""
+    g, prob, k = g1_run["g"], g1_run["prob"], g1_run["k"]
+    ref = g["partial2"]
+    J = ref[:, 0].astype(int)
+    assert np.array_equal(J, np.arange(260))
+    mine = (2 * J + 1.0)[:, None] / k ** 2 * np.pi * prob[J // int(g["dl"])] * ABOHR ** 2
+    r = ref[:, 1:]
+    assert np.max(np.abs(mine - r) / r) < 2e-7   # 8 printed digits
