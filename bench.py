@@ -8,6 +8,10 @@ workload (A, B, C = 27.9, 14.5, 9.3 cm^-1, j <= 8 all tau and m: 969 states,
 points) per second.  One step = one full build: rotor basis + PES tables +
 contraction + units/cutoff/spline, inputs resident on the device.
 
+Secondary (`expansion`): the PES-expansion build through its C ABI on the inputs of
+two reference examples (with the reference's logged single-rank build times) and a
+larger synthetic system.
+
 Secondary (`propagation`): batched trajectory propagation on that matrix
 (trajectories with b ~ U(0,15) bohr, E log-uniform 50-2000 cm^-1, RK4 dt=5 a.u.
 until R > 25 bohr), trajectories per second, FP32 arithmetic, and the plain
@@ -46,6 +50,7 @@ def _args():
                    help="trajectories of the propagation workload timed (4096 = full set)")
     p.add_argument("--no-propagation", action="store_true")
     p.add_argument("--no-fp64-form", action="store_true")
+    p.add_argument("--no-expansion", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     return p.parse_args()
 
@@ -261,6 +266,7 @@ def run_gpu(a):
         if dist is not None:
             dist.destroy_process_group()
         return
+    expansion = None if a.no_expansion else run_expansion(mq, syn)
     cpu = cpu_baseline_matrix(s, R, c2, a.cpu_seconds)
     tc = prec in (mq.PREC_BF16X3, mq.PREC_F16X3)
     tc_name = "F16x3" if prec == mq.PREC_F16X3 else "BF16x3"
@@ -307,6 +313,7 @@ def run_gpu(a):
         "accuracy": acc,
         "reference_2d_form": ref_form,
         "propagation": prop,
+        "expansion": expansion,
         "wall_s": wall,
     }
     print(json.dumps(line), flush=True)
@@ -417,6 +424,91 @@ def cpu_baseline_matrix(s, R, c2, seconds, n_threads=0):
     return {"value": n2 / t2, "unit": "matrix elements/s", "cores": cores, "kind": "port",
             "sample": f"{n2} elements x 1 R point of the same build (literal INTEGRATOR_TEMP "
                       f"restatement, {cores} OpenMP threads), {t2:.1f} s"}
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def run_expansion(mq, syn):
+    """The PES-expansion build (EXPANSION_MATRIX_ELEMENT, MIJ_CUTOFF, spline) end to end
+    through mqct_build_matrix_expansion (host arrays in, Mat_el and y2 out; transfers and
+    set-up inside the time), on the inputs of two reference examples whose logs give the
+    reference's single-rank build time, and on a larger asymmetric top + diatom system
+    (j1 <= 6 all levels, j2 = 0, 2) with the same 83 terms.  The oracle's restatement of
+    the same formulas (OpenMP, all host threads) is timed beside it."""
+    from oracle import pyoracle as po
+    po.build()
+    g3 = np.load(os.path.join(GOLDEN, "g3_h2o_h2_type8.npz"))
+    g5 = np.load(os.path.join(GOLDEN, "g5_h2o_h2_expansion_terms.npz"))
+    g1 = np.load(os.path.join(GOLDEN, "g1_h2o_h2o_at.npz"))
+    s8 = mq.CollisionSystem(8, g3["channels"], A=float(g3["A"]), B=float(g3["B"]),
+                            C=float(g3["C"]), BE=float(g3["BE"]))
+    s0 = mq.CollisionSystem(0, g1["channels"], A=float(g1["A"]), B=float(g1["B"]),
+                            C=float(g1["C"]))
+    big = [c + (j2,) for j2 in (0, 2) for c in syn.asym_channels(6)]
+    sb = mq.CollisionSystem(8, big, A=float(g3["A"]), B=float(g3["B"]), C=float(g3["C"]),
+                            BE=float(g3["BE"]))
+    cases = [
+        ("h2o_h2_type8", "H2O+H2 example (EXAMPLES_IO/SYS_TYPE_8/H2O_H2_MTRXCalculation): "
+         "104 states, 891 pairs, 101 R, 83 terms", s8, g5, "CM-1", 127.174),
+        ("h2o_h2o_type0", "H2O+H2O AT example, 2nd run (EXAMPLES_IO/SYS_TYPE_0/"
+         "H2O_H2O_AT_Approximation): 81 states, 594 pairs, 171 R, 28 terms", s0, g1, "KCAL",
+         283.947),
+        ("asymtop_j6_diatom_j02", f"asym top j1<=6 + diatom j2=0,2: {sb.n_states} states, "
+         f"{sb.P} pairs, 101 R, the 83 terms of the H2O+H2 example", sb, g5, "CM-1", None),
+    ]
+    import torch
+    out = {}
+    for key, desc, s, g, unit, ref_s in cases:
+        R, lab, T = g["R"], g["labels"], g["terms"]
+        times = []
+        for i in range(6):
+            t0 = time.perf_counter()
+            mq.build_matrix_expansion(s, R, lab, T, e_unit=unit)
+            times.append(time.perf_counter() - t0)
+        ms = float(np.median(times[2:])) * 1e3
+        n_el = s.P * len(R)
+        # device times of the plan: the angular set-up, and one execute (contraction,
+        # cut-off, spline) from terms resident on the device
+        plan = mq.ExpansionPlan(s, R, lab)
+        dT = torch.from_numpy(np.ascontiguousarray(T.T)).cuda()
+        dm = torch.empty((s.P, len(R)), dtype=torch.float64, device="cuda")
+        dy = torch.empty_like(dm)
+        dk = torch.empty(s.P, dtype=torch.int32, device="cuda")
+        ex = []
+        for i in range(5):
+            plan.execute(dT, dm, dy, dk, e_unit=unit)
+            plan.sync()
+            ex.append(plan.timing()[1])
+        ang_ms = plan.timing()[0]
+        ex_ms = float(np.median(ex[2:]))
+        plan.close()
+        del dT, dm, dy, dk
+        # the oracle on a bounded sample of pairs (all of them for the small examples)
+        ch = s.channels
+        kp = min(s.P, 4000)
+        ind = np.ascontiguousarray(s.ind_mat[:kp])
+        t0 = time.perf_counter()
+        if s.sys_type == 0:
+            osys = po.OracleSystem(0, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], ch[:, 4], ch[:, 5],
+                                   e_ch=s.e_ch, vec1=s.vec1.reshape(-1),
+                                   vec2=s.vec2.reshape(-1), ldv=s.ldv)
+            po.expansion_matrix_type0(osys, osys.states(), ind, lab, T, mq.E_UNIT[unit])
+        else:
+            osys = po.OracleSystem(8, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch,
+                                   vec1=s.vec1.reshape(-1), ldv=s.ldv)
+            po.expansion_matrix_type8(osys, osys.states(), ind, lab, T)
+        tc = time.perf_counter() - t0
+        out[key] = {"workload": desc, "elements": n_el, "ms_per_build_e2e": ms,
+                    "elements_per_s_e2e": n_el / (ms / 1e3),
+                    "device_ms_angular_setup": ang_ms, "device_ms_execute": ex_ms,
+                    "elements_per_s_device": n_el / ((ang_ms + ex_ms) / 1e3),
+                    "cpu_port_elements_per_s": kp * len(R) / tc,
+                    "cpu_port_sample": f"{kp} pairs x {len(R)} R, {os.cpu_count()} OpenMP threads, "
+                                       f"{tc:.2f} s",
+                    "reference_log_single_rank_s": ref_s,
+                    "speedup_vs_reference_log": (ref_s / (ms / 1e3)) if ref_s else None}
+    return out
 
 
 def run_reference(a):

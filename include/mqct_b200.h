@@ -169,6 +169,25 @@ int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, i
                                 double mij_cutoff_cm, double r_cut1, double r_cut2,
                                 double* Mat_el, double* Mat_el_y2, int32_t* skipped);
 
+/* The expansion build as a plan: _create validates the system, uploads it and forms
+ * the R-independent angular coefficients (EXPANSION_MATRIX_ELEMENT's angular_part,
+ * one per pair and term) on the device; _execute then forms Mat_el from radial terms
+ * already on the device (d_terms[t * nR + iR] in units of e_unit Hartree), applies
+ * MIJ_CUTOFF and fits the spline into device buffers (d_mat, d_y2: nR * P doubles,
+ * d_y2 may be NULL; d_skipped: P int32), asynchronously on the plan's stream; _sync
+ * waits for it; _timing gives the device milliseconds of the angular set-up and of
+ * the last execute.  One plan serves any number of term sets on the same R grid. */
+typedef struct mqct_expansion_plan mqct_expansion_plan;
+int mqct_expansion_plan_create(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                               const double* R, int32_t nR, int32_t n_terms, const int32_t* a_top,
+                               double mij_cutoff_cm, double r_cut1, double r_cut2,
+                               mqct_expansion_plan** plan);
+int mqct_expansion_plan_execute(mqct_expansion_plan* plan, const double* d_terms, double e_unit,
+                                double* d_mat, double* d_y2, int32_t* d_skipped);
+int mqct_expansion_plan_sync(mqct_expansion_plan* plan);
+int mqct_expansion_plan_timing(mqct_expansion_plan* plan, float* ms_angular, float* ms_execute);
+void mqct_expansion_plan_destroy(mqct_expansion_plan* plan);
+
 /* Device-resident form of the same build for callers that keep the matrix on
  * the GPU: a plan uploads the system once; execute writes Mat_el and y2 into
  * device buffers (nR*P doubles each, may be NULL for y2) on the plan's stream. */

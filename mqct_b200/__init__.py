@@ -27,7 +27,8 @@ __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables",
            "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections",
            "cross_sections_device", "write_mtrx_uf",
            "read_mtrx_uf", "write_mtrx_dat", "read_mtrx_dat", "read_expansion_terms",
-           "spline_y2", "Surrogate", "build_matrix_expansion", "E_UNIT", "MqctError",
+           "spline_y2", "Surrogate", "build_matrix_expansion", "ExpansionPlan", "E_UNIT",
+           "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
            "MODE_AT"]
 
@@ -299,6 +300,57 @@ def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM
                                             a_top.reshape(-1), T.reshape(-1), eu, mij_cutoff,
                                             r_cut1, r_cut2, mat, ptr(y2), ptr(sk)))
     return mat.reshape(P, nR), y2.reshape(P, nR), sk
+
+
+class ExpansionPlan:
+    """The expansion build with the angular coefficients formed once (mqct_expansion_plan_*);
+    execute() turns radial terms on the device into Mat_el, y2 and the MIJ_CUTOFF flags in
+    device buffers (torch tensors or raw device pointers)."""
+
+    def __init__(self, system: CollisionSystem, R, labels, mij_cutoff=1e-12, r_cut1=6.0,
+                 r_cut2=8.0):
+        self.R = np.ascontiguousarray(R, np.float64)
+        lab = np.asarray(labels, np.int32)
+        lab = lab.reshape(len(lab), -1)
+        a_top = np.zeros((len(lab), 5), np.int32)
+        a_top[:, :lab.shape[1]] = lab
+        self.n_terms = len(lab)
+        self.P = system.P
+        self._sd = system.c_struct()
+        h = _abi.vp()
+        check(lib().mqct_expansion_plan_create(C.byref(self._sd),
+                                               np.ascontiguousarray(system.ind_mat.reshape(-1)),
+                                               self.P, self.R, len(self.R), self.n_terms,
+                                               a_top.reshape(-1), mij_cutoff, r_cut1, r_cut2,
+                                               C.byref(h)))
+        self.h = h
+
+    def execute(self, d_terms, d_mat, d_y2, d_skipped, e_unit="CM-1"):
+        """d_terms: device terms[t * nR + iR] (a CUDA tensor n_terms x nR, or a pointer);
+        outputs P x nR (float64) and P (int32) device buffers."""
+        eu = E_UNIT[e_unit.upper()] if isinstance(e_unit, str) else float(e_unit)
+        p = [x.data_ptr() if hasattr(x, "data_ptr") else x for x in (d_terms, d_mat, d_y2, d_skipped)]
+        check(lib().mqct_expansion_plan_execute(self.h, p[0], eu, p[1], p[2], p[3]))
+
+    def sync(self):
+        check(lib().mqct_expansion_plan_sync(self.h))
+
+    def timing(self):
+        """(angular set-up ms, last execute ms) on the device."""
+        a, e = C.c_float(), C.c_float()
+        check(lib().mqct_expansion_plan_timing(self.h, C.byref(a), C.byref(e)))
+        return float(a.value), float(e.value)
+
+    def close(self):
+        if self.h:
+            lib().mqct_expansion_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MatrixPlan:

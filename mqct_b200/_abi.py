@@ -86,7 +86,8 @@ EXPORTS = [
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
     "mqct_propagate_batch_rec", "mqct_propagate_batch_integ", "mqct_prop_plan_set_integrator",
-    "mqct_cross_sections_device",
+    "mqct_cross_sections_device", "mqct_expansion_plan_create", "mqct_expansion_plan_execute",
+    "mqct_expansion_plan_sync", "mqct_expansion_plan_timing", "mqct_expansion_plan_destroy",
     "mqct_surrogate_create", "mqct_surrogate_train", "mqct_surrogate_predict",
     "mqct_surrogate_n_params", "mqct_surrogate_get_params", "mqct_surrogate_loss_grad",
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
@@ -155,6 +156,14 @@ def lib():
                                              C.c_int32, C.POINTER(AtPaths), C.c_int32,
                                              C.POINTER(Integrator), f64p, f64p, f64p]
     L.mqct_prop_plan_set_integrator.argtypes = [vp, C.POINTER(Integrator)]
+    L.mqct_expansion_plan_create.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
+                                             C.c_int32, i32p, C.c_double, C.c_double, C.c_double,
+                                             C.POINTER(vp)]
+    L.mqct_expansion_plan_execute.argtypes = [vp, vp, C.c_double, vp, vp, vp]
+    L.mqct_expansion_plan_sync.argtypes = [vp]
+    L.mqct_expansion_plan_timing.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.mqct_expansion_plan_destroy.argtypes = [vp]
+    L.mqct_expansion_plan_destroy.restype = None
     L.mqct_cross_sections_device.argtypes = [vp, C.c_int64, C.c_int32, i32p, C.c_int32, C.c_int32,
                                              C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                              C.c_double, vp, vp, vp, vp]

@@ -1397,152 +1397,253 @@ expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
   }
 }
 
-extern "C" int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
-                                           const double* R, int32_t nR, int32_t n_terms,
-                                           const int32_t* a_top, const double* terms, double e_unit,
-                                           double mij_cutoff_cm, double r_cut1, double r_cut2,
-                                           double* Mat_el, double* Mat_el_y2, int32_t* skipped) {
-  MQCT_ARG_CHECK(sys && ind_mat && R && a_top && terms && Mat_el, "null argument");
-  const int type = sys->sys_type;
-  MQCT_ARG_CHECK(type == 7 || type == 8 || type == 0,
-                 "the expansion path supports SYS_TYPE 7, 8 and 0 (got %d)", type);
-  MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->indx_chann && sys->j12 && sys->m12 &&
-                     sys->n_states > 0 && (type == 7 || (sys->vec1 && sys->ldv > 0)) &&
-                     (type != 0 || sys->vec2) && (type != 7 || (sys->ka1 && sys->kc1)),
-                 "system arrays missing");
-  MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && n_terms <= 4096 && nR >= 2 &&
-                     nR <= 3072,
-                 "bad sizes (n_terms <= 4096, 2 <= nR <= 3072)");
-  MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
-  for (int i = 0; i + 1 < nR; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
-  // canonical labels (l1, nju1, l2, nju2, l); A_TOP columns: cases 7, 8 (l1, nju1, l2, l),
-  // case 0 (l1, nju1, l2, nju2, l) (MQCT_SOURCE_CODES/pot_comp.f:6317-6338)
-  std::vector<int> lab5(5 * (size_t)n_terms);
-  for (int t = 0; t < n_terms; ++t) {
-    const int* c = a_top + 5 * t;
-    const int l1 = c[0], nju1 = c[1], l2 = c[2];
-    const int nju2 = type == 0 ? c[3] : 0, l = type == 0 ? c[4] : c[3];
-    // the log-factorial table (128 entries) bounds every Clebsch-Gordan argument sum;
-    // the sign rules are the reference's input checks (:7620-7633, :8288-8302)
-    MQCT_ARG_CHECK(l1 >= 0 && l2 >= 0 && l >= 0 && l1 <= 30 && l2 <= 30 && l <= 60 &&
-                       nju1 >= 0 && nju1 <= l1 && abs(nju2) <= l2 && !(nju1 == 0 && nju2 < 0),
-                   "bad expansion term %d (l1=%d nju1=%d l2=%d nju2=%d l=%d): l1, l2 <= 30, "
-                   "l <= 60, 0 <= nju1 <= l1, |nju2| <= l2, nju2 >= 0 when nju1 = 0",
-                   t + 1, l1, nju1, l2, nju2, l);
-    int* o = &lab5[5 * (size_t)t];
-    o[0] = l1; o[1] = nju1; o[2] = l2; o[3] = nju2; o[4] = l;
-  }
-  const int n_states = sys->n_states, n_ch = sys->n_channels;
-  std::vector<int> st_chan(n_states);
-  int j1max = 0, j2max = 0;
-  for (int c = 0; c < n_ch; ++c) {
-    MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 && sys->j2[c] >= 0 && sys->j2[c] <= 30 &&
-                       (type == 7 || 2 * sys->j1[c] + 1 <= sys->ldv) &&
-                       (type != 0 || 2 * sys->j2[c] + 1 <= sys->ldv),
-                   "bad channel %d (j1, j2 <= 30, 2j + 1 <= ldv)", c + 1);
-    if (type == 7)
-      MQCT_ARG_CHECK(sys->ka1[c] >= 0 && sys->ka1[c] <= sys->j1[c] &&
-                         (sys->kc1[c] == 0 || sys->kc1[c] == 1) &&
-                         !(sys->ka1[c] == 0 && sys->kc1[c] == 1),
-                     "bad symmetric-top channel %d (j=%d k=%d eps=%d): 0 <= k <= j, eps in {0, 1}, "
-                     "eps = 0 when k = 0",
-                     c + 1, sys->j1[c], sys->ka1[c], sys->kc1[c]);
-    j1max = std::max(j1max, sys->j1[c]);
-    j2max = std::max(j2max, sys->j2[c]);
-  }
-  for (int s = 0; s < n_states; ++s) {
-    st_chan[s] = sys->indx_chann[s] - 1;
-    MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < n_ch, "indx_chann out of range");
-    const int ch = st_chan[s];
-    MQCT_ARG_CHECK(sys->j12[s] >= abs(sys->j1[ch] - sys->j2[ch]) &&
-                       sys->j12[s] <= sys->j1[ch] + sys->j2[ch] && abs(sys->m12[s]) <= sys->j12[s],
-                   "bad (j12, m12) at state %d", s + 1);
-  }
-  for (int64_t k = 0; k < P; ++k) {
-    const int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
-    MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states, "ind_mat out of range");
-    MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
-                   (long long)k + 1);
-  }
-  // rotor 1 of SYS_TYPE 7: the parity-adapted symmetric top
-  // (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) as a vector over K; with it
-  // the K-sum S1 is the four-term bracket of the reference (:7680-7707 with coef4)
-  int ldv1 = sys->ldv;
-  std::vector<double> vec1_sym;
-  if (type == 7) {
-    ldv1 = 2 * j1max + 1;
-    vec1_sym.assign((size_t)n_ch * ldv1, 0.0);
-    for (int c = 0; c < n_ch; ++c) {
-      const int j = sys->j1[c], kk = sys->ka1[c];
-      const double a = 1.0 / sqrt(2.0 * (1.0 + (kk == 0 ? 1.0 : 0.0)));
-      vec1_sym[(size_t)c * ldv1 + j + kk] += a;
-      vec1_sym[(size_t)c * ldv1 + j - kk] += (sys->kc1[c] & 1) ? -a : a;
-    }
-  }
-  // rotor 2: the asymmetric-top vectors (case 0) or the diatom's unit vector at K = 0
-  int ldv2 = sys->ldv;
-  std::vector<double> vec2_diatom;
-  if (type != 0) {
-    ldv2 = 2 * j2max + 1;
-    vec2_diatom.assign((size_t)n_ch * ldv2, 0.0);
-    for (int c = 0; c < n_ch; ++c) vec2_diatom[(size_t)c * ldv2 + sys->j2[c]] = 1.0;
-  }
-  const double pref = type == 0 ? 1.0 / (8.0 * kPi * kPi) : 1.0 / (4.0 * kPi);
-  if (mqct_device_count() <= 0) {
-    set_error("no CUDA device available");
-    return MQCT_E_NODEV;
-  }
-  int rc = upload_logfact();
-  if (rc) return rc;
+namespace {
+
+// The expansion build as a plan: set-up (validation, uploads) and the R-independent
+// angular coefficients once; then per set of radial terms the contraction, the cut-off
+// and the spline on device buffers.
+struct ExpansionPlan {
+  int64_t P = 0;
+  int nR = 0, n_terms = 0, ir1 = 0, ir2 = 0;
+  double cut_hartree = 0.0;
   cudaStream_t st = nullptr;
-  MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  struct StreamGuard {
-    cudaStream_t s;
-    ~StreamGuard() { cudaStreamDestroy(s); }
-  } guard{st};
-  std::vector<int> ch_j1(sys->j1, sys->j1 + n_ch), ch_j2(sys->j2, sys->j2 + n_ch);
-  DevBuf<int> d_ind, d_chan, d_j12, d_m, d_j1, d_j2, d_lab, d_k2r, d_sk;
-  DevBuf<double> d_vec1, d_vec2, d_T, d_A, d_M, d_mat, d_y2, d_gc;
-  MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
-  MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
-  MQCT_CUDA_TRY(d_j12.upload(sys->j12, n_states, st));
-  MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
-  MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
-  MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
-  if (type == 7) MQCT_CUDA_TRY(d_vec1.upload(vec1_sym, st));
-  else MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * ldv1, st));
-  if (type != 0) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
-  else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));
-  MQCT_CUDA_TRY(d_lab.upload(lab5, st));
-  MQCT_CUDA_TRY(d_T.upload(terms, (size_t)nR * n_terms, st));
-  std::vector<double> Rh(R, R + nR);
-  MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
-  std::vector<int> k2r(P);
-  for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
-  MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
-  MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
-  MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
-  MQCT_CUDA_TRY(d_mat.alloc((size_t)P * nR));
-  MQCT_CUDA_TRY(d_y2.alloc((size_t)P * nR));
-  MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
-  const int64_t n_at = P * n_terms;
-  expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
-      P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, ldv1, d_vec2.p,
-      ldv2, d_lab.p, pref, d_A.p);
-  MQCT_CUDA_TRY(cudaGetLastError());
-  expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
-      n_terms, nR, d_A.p, d_T.p, d_M.p);
-  MQCT_CUDA_TRY(cudaGetLastError());
-  const int ir1 = nearest_index(Rh, r_cut1), ir2 = nearest_index(Rh, r_cut2);
-  finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
-      P, nR, d_k2r.p, d_M.p, 1, 0, nR, e_unit, nullptr, ir1, ir2, mij_cutoff_cm * kCmToHartree,
-      d_gc.p, d_mat.p, d_sk.p, Mat_el_y2 ? d_y2.p : nullptr);
-  MQCT_CUDA_TRY(cudaGetLastError());
-  MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el, d_mat.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, st));
-  if (Mat_el_y2)
-    MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el_y2, d_y2.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, st));
-  if (skipped)
-    MQCT_CUDA_TRY(cudaMemcpyAsync(skipped, d_sk.p, sizeof(int32_t) * P, cudaMemcpyDeviceToHost, st));
-  MQCT_CUDA_TRY(cudaStreamSynchronize(st));
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  DevBuf<int> d_k2r;
+  DevBuf<double> d_A, d_M, d_gc;
+
+  ~ExpansionPlan() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+
+  int init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, const double* R,
+           int32_t nR_, int32_t n_terms_, const int32_t* a_top, double mij_cutoff_cm,
+           double r_cut1, double r_cut2) {
+    const int64_t P = P_;
+    const int32_t nR = nR_, n_terms = n_terms_;
+    MQCT_ARG_CHECK(sys && ind_mat && R && a_top, "null argument");
+    const int type = sys->sys_type;
+    MQCT_ARG_CHECK(type == 7 || type == 8 || type == 0,
+                   "the expansion path supports SYS_TYPE 7, 8 and 0 (got %d)", type);
+    MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->indx_chann && sys->j12 && sys->m12 &&
+                       sys->n_states > 0 && (type == 7 || (sys->vec1 && sys->ldv > 0)) &&
+                       (type != 0 || sys->vec2) && (type != 7 || (sys->ka1 && sys->kc1)),
+                   "system arrays missing");
+    MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && n_terms <= 4096 && nR >= 2 &&
+                       nR <= 3072,
+                   "bad sizes (n_terms <= 4096, 2 <= nR <= 3072)");
+    for (int i = 0; i + 1 < nR; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
+    // canonical labels (l1, nju1, l2, nju2, l); A_TOP columns: cases 7, 8 (l1, nju1, l2, l),
+    // case 0 (l1, nju1, l2, nju2, l) (MQCT_SOURCE_CODES/pot_comp.f:6317-6338)
+    std::vector<int> lab5(5 * (size_t)n_terms);
+    for (int t = 0; t < n_terms; ++t) {
+      const int* c = a_top + 5 * t;
+      const int l1 = c[0], nju1 = c[1], l2 = c[2];
+      const int nju2 = type == 0 ? c[3] : 0, l = type == 0 ? c[4] : c[3];
+      // the log-factorial table (128 entries) bounds every Clebsch-Gordan argument sum;
+      // the sign rules are the reference's input checks (:7620-7633, :8288-8302)
+      MQCT_ARG_CHECK(l1 >= 0 && l2 >= 0 && l >= 0 && l1 <= 30 && l2 <= 30 && l <= 60 &&
+                         nju1 >= 0 && nju1 <= l1 && abs(nju2) <= l2 && !(nju1 == 0 && nju2 < 0),
+                     "bad expansion term %d (l1=%d nju1=%d l2=%d nju2=%d l=%d): l1, l2 <= 30, "
+                     "l <= 60, 0 <= nju1 <= l1, |nju2| <= l2, nju2 >= 0 when nju1 = 0",
+                     t + 1, l1, nju1, l2, nju2, l);
+      int* o = &lab5[5 * (size_t)t];
+      o[0] = l1; o[1] = nju1; o[2] = l2; o[3] = nju2; o[4] = l;
+    }
+    const int n_states = sys->n_states, n_ch = sys->n_channels;
+    std::vector<int> st_chan(n_states);
+    int j1max = 0, j2max = 0;
+    for (int c = 0; c < n_ch; ++c) {
+      MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 && sys->j2[c] >= 0 && sys->j2[c] <= 30 &&
+                         (type == 7 || 2 * sys->j1[c] + 1 <= sys->ldv) &&
+                         (type != 0 || 2 * sys->j2[c] + 1 <= sys->ldv),
+                     "bad channel %d (j1, j2 <= 30, 2j + 1 <= ldv)", c + 1);
+      if (type == 7)
+        MQCT_ARG_CHECK(sys->ka1[c] >= 0 && sys->ka1[c] <= sys->j1[c] &&
+                           (sys->kc1[c] == 0 || sys->kc1[c] == 1) &&
+                           !(sys->ka1[c] == 0 && sys->kc1[c] == 1),
+                       "bad symmetric-top channel %d (j=%d k=%d eps=%d): 0 <= k <= j, eps in {0, 1}, "
+                       "eps = 0 when k = 0",
+                       c + 1, sys->j1[c], sys->ka1[c], sys->kc1[c]);
+      j1max = std::max(j1max, sys->j1[c]);
+      j2max = std::max(j2max, sys->j2[c]);
+    }
+    for (int s = 0; s < n_states; ++s) {
+      st_chan[s] = sys->indx_chann[s] - 1;
+      MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < n_ch, "indx_chann out of range");
+      const int ch = st_chan[s];
+      MQCT_ARG_CHECK(sys->j12[s] >= abs(sys->j1[ch] - sys->j2[ch]) &&
+                         sys->j12[s] <= sys->j1[ch] + sys->j2[ch] && abs(sys->m12[s]) <= sys->j12[s],
+                     "bad (j12, m12) at state %d", s + 1);
+    }
+    for (int64_t k = 0; k < P; ++k) {
+      const int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
+      MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states, "ind_mat out of range");
+      MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
+                     (long long)k + 1);
+    }
+    // rotor 1 of SYS_TYPE 7: the parity-adapted symmetric top
+    // (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) as a vector over K; with it
+    // the K-sum S1 is the four-term bracket of the reference (:7680-7707 with coef4)
+    int ldv1 = sys->ldv;
+    std::vector<double> vec1_sym;
+    if (type == 7) {
+      ldv1 = 2 * j1max + 1;
+      vec1_sym.assign((size_t)n_ch * ldv1, 0.0);
+      for (int c = 0; c < n_ch; ++c) {
+        const int j = sys->j1[c], kk = sys->ka1[c];
+        const double a = 1.0 / sqrt(2.0 * (1.0 + (kk == 0 ? 1.0 : 0.0)));
+        vec1_sym[(size_t)c * ldv1 + j + kk] += a;
+        vec1_sym[(size_t)c * ldv1 + j - kk] += (sys->kc1[c] & 1) ? -a : a;
+      }
+    }
+    // rotor 2: the asymmetric-top vectors (case 0) or the diatom's unit vector at K = 0
+    int ldv2 = sys->ldv;
+    std::vector<double> vec2_diatom;
+    if (type != 0) {
+      ldv2 = 2 * j2max + 1;
+      vec2_diatom.assign((size_t)n_ch * ldv2, 0.0);
+      for (int c = 0; c < n_ch; ++c) vec2_diatom[(size_t)c * ldv2 + sys->j2[c]] = 1.0;
+    }
+    const double pref = type == 0 ? 1.0 / (8.0 * kPi * kPi) : 1.0 / (4.0 * kPi);
+    if (mqct_device_count() <= 0) {
+      set_error("no CUDA device available");
+      return MQCT_E_NODEV;
+    }
+    int rc = upload_logfact();
+    if (rc) return rc;
+    MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : ev) MQCT_CUDA_TRY(cudaEventCreate(&e));
+    this->P = P;
+    this->nR = nR;
+    this->n_terms = n_terms;
+    std::vector<int> ch_j1(sys->j1, sys->j1 + n_ch), ch_j2(sys->j2, sys->j2 + n_ch);
+    DevBuf<int> d_ind, d_chan, d_j12, d_m, d_j1, d_j2, d_lab;
+    DevBuf<double> d_vec1, d_vec2;
+    MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
+    MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
+    MQCT_CUDA_TRY(d_j12.upload(sys->j12, n_states, st));
+    MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
+    MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
+    MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
+    if (type == 7) MQCT_CUDA_TRY(d_vec1.upload(vec1_sym, st));
+    else MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * ldv1, st));
+    if (type != 0) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
+    else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));
+    MQCT_CUDA_TRY(d_lab.upload(lab5, st));
+    std::vector<double> Rh(R, R + nR);
+    MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
+    std::vector<int> k2r(P);
+    for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
+    MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
+    MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
+    MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
+    ir1 = nearest_index(Rh, r_cut1);
+    ir2 = nearest_index(Rh, r_cut2);
+    cut_hartree = mij_cutoff_cm * kCmToHartree;
+    const int64_t n_at = P * n_terms;
+    MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
+    expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
+        P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, ldv1, d_vec2.p,
+        ldv2, d_lab.p, pref, d_A.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(st));  // the set-up buffers are released on return
+    return MQCT_OK;
+  }
+
+  // Mat_el (Hartree), y2 and the MIJ_CUTOFF flags from radial terms d_terms
+  // (device, terms[t * nR + iR], in units of e_unit Hartree); asynchronous on st.
+  int execute(const double* d_terms, double e_unit, double* d_mat, double* d_y2, int* d_sk) {
+    MQCT_ARG_CHECK(d_terms && d_mat && d_sk, "null argument");
+    MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
+    MQCT_CUDA_TRY(cudaEventRecord(ev[2], st));
+    expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
+        n_terms, nR, d_A.p, d_terms, d_M.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
+        P, nR, d_k2r.p, d_M.p, 1, 0, nR, e_unit, nullptr, ir1, ir2, cut_hartree, d_gc.p, d_mat,
+        d_sk, d_y2);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    MQCT_CUDA_TRY(cudaEventRecord(ev[3], st));
+    return MQCT_OK;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int mqct_expansion_plan_create(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                               const double* R, int32_t nR, int32_t n_terms, const int32_t* a_top,
+                               double mij_cutoff_cm, double r_cut1, double r_cut2,
+                               mqct_expansion_plan** plan) {
+  MQCT_ARG_CHECK(plan, "null plan pointer");
+  *plan = nullptr;
+  auto* p = new ExpansionPlan();
+  int rc = p->init(sys, ind_mat, P, R, nR, n_terms, a_top, mij_cutoff_cm, r_cut1, r_cut2);
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *plan = reinterpret_cast<mqct_expansion_plan*>(p);
   return MQCT_OK;
 }
+
+int mqct_expansion_plan_execute(mqct_expansion_plan* plan, const double* d_terms, double e_unit,
+                                double* d_mat, double* d_y2, int32_t* d_skipped) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  return reinterpret_cast<ExpansionPlan*>(plan)->execute(d_terms, e_unit, d_mat, d_y2, d_skipped);
+}
+
+int mqct_expansion_plan_sync(mqct_expansion_plan* plan) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MQCT_CUDA_TRY(cudaStreamSynchronize(reinterpret_cast<ExpansionPlan*>(plan)->st));
+  return MQCT_OK;
+}
+
+int mqct_expansion_plan_timing(mqct_expansion_plan* plan, float* ms_angular, float* ms_execute) {
+  MQCT_ARG_CHECK(plan && ms_angular && ms_execute, "null argument");
+  ExpansionPlan* p = reinterpret_cast<ExpansionPlan*>(plan);
+  MQCT_CUDA_TRY(cudaEventElapsedTime(ms_angular, p->ev[0], p->ev[1]));
+  MQCT_CUDA_TRY(cudaEventSynchronize(p->ev[3]));
+  MQCT_CUDA_TRY(cudaEventElapsedTime(ms_execute, p->ev[2], p->ev[3]));
+  return MQCT_OK;
+}
+
+void mqct_expansion_plan_destroy(mqct_expansion_plan* plan) {
+  delete reinterpret_cast<ExpansionPlan*>(plan);
+}
+
+int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
+                                const double* R, int32_t nR, int32_t n_terms,
+                                const int32_t* a_top, const double* terms, double e_unit,
+                                double mij_cutoff_cm, double r_cut1, double r_cut2,
+                                double* Mat_el, double* Mat_el_y2, int32_t* skipped) {
+  MQCT_ARG_CHECK(terms && Mat_el, "null argument");
+  MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
+  ExpansionPlan p;
+  int rc = p.init(sys, ind_mat, P, R, nR, n_terms, a_top, mij_cutoff_cm, r_cut1, r_cut2);
+  if (rc) return rc;
+  DevBuf<double> d_T, d_mat, d_y2;
+  DevBuf<int> d_sk;
+  MQCT_CUDA_TRY(d_T.upload(terms, (size_t)nR * n_terms, p.st));
+  MQCT_CUDA_TRY(d_mat.alloc((size_t)P * nR));
+  if (Mat_el_y2) MQCT_CUDA_TRY(d_y2.alloc((size_t)P * nR));
+  MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
+  rc = p.execute(d_T.p, e_unit, d_mat.p, Mat_el_y2 ? d_y2.p : nullptr, d_sk.p);
+  if (rc) return rc;
+  MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el, d_mat.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost,
+                                p.st));
+  if (Mat_el_y2)
+    MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el_y2, d_y2.p, sizeof(double) * P * nR,
+                                  cudaMemcpyDeviceToHost, p.st));
+  if (skipped)
+    MQCT_CUDA_TRY(cudaMemcpyAsync(skipped, d_sk.p, sizeof(int32_t) * P, cudaMemcpyDeviceToHost,
+                                  p.st));
+  MQCT_CUDA_TRY(cudaStreamSynchronize(p.st));
+  return MQCT_OK;
+}
+
+}  // extern "C"

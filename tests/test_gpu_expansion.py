@@ -73,3 +73,30 @@ def test_expansion_mij_cutoff_flags(mq, oracle, gpu_available):
     assert (expect & (np.abs(m0).max(axis=1) > 1e-12)).sum() > 20 and not expect.all()
     assert np.array_equal(sk.astype(bool), expect)
     assert np.all(m[expect] == 0.0) and np.array_equal(m[~expect], m0[~expect])
+
+
+def test_expansion_plan_reuse(mq, gpu_available):
+    """The plan forms the angular coefficients once: execute() with the example's terms
+    equals the one-shot build, and with the terms doubled gives exactly twice the
+    matrix and its spline (both linear in the terms; cut-off off)."""
+    import torch
+    g = np.load(os.path.join(GOLD, "g3_h2o_h2_type8.npz"))
+    g5 = np.load(os.path.join(GOLD, "g5_h2o_h2_expansion_terms.npz"))
+    s = mq.CollisionSystem(8, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           BE=float(g["BE"]))
+    R, lab, T = g5["R"], g5["labels"], g5["terms"]
+    m1, y1, _ = mq.build_matrix_expansion(s, R, lab, T, mij_cutoff=0.0)
+    plan = mq.ExpansionPlan(s, R, lab, mij_cutoff=0.0)
+    dT = torch.from_numpy(np.ascontiguousarray(T.T)).cuda()      # terms[t * nR + iR]
+    dm = torch.empty((s.P, len(R)), dtype=torch.float64, device="cuda")
+    dy = torch.empty_like(dm)
+    dk = torch.empty(s.P, dtype=torch.int32, device="cuda")
+    plan.execute(dT, dm, dy, dk)
+    plan.sync()
+    assert np.array_equal(dm.cpu().numpy(), m1) and np.array_equal(dy.cpu().numpy(), y1)
+    plan.execute(2.0 * dT, dm, dy, dk)
+    plan.sync()
+    assert np.array_equal(dm.cpu().numpy(), 2.0 * m1) and np.array_equal(dy.cpu().numpy(), 2.0 * y1)
+    ang, ex = plan.timing()
+    assert ang > 0.0 and ex > 0.0
+    plan.close()
