@@ -1313,46 +1313,46 @@ __device__ inline double rotor_sum(int jpp, int l, int jp, int nju, const double
   return s;
 }
 
-// A[k * n_terms + t] (times c_k) for term t = (l1, nju1, l2, nju2, l) = lab5[5t..5t+4];
-// p = ind_mat[2k] - 1 (stp), pp = ind_mat[2k+1] - 1 (stpp), m = m12(p).
-//   A = pref sqrt((2l1+1)(2l2+1)) K M3 with
+// The angular coefficient of pair k (p = ind_mat[2k] - 1 = stp, pp = ind_mat[2k+1] - 1
+// = stpp, m = m12(p)) and term t = (l1, nju1, l2, nju2, l):
+//   A = pref sqrt((2l1+1)(2l2+1)) K M3 c_k,
 //   K  = sum over (nju1, nju2) and, unless both vanish, (-nju1, -nju2) with the
 //        phase (-1)^(l1+l2+l+nju1+nju2) on the second, of S1 S2,
 //        S1 = sum_{k1'} <j1'' k1'-nju1 l1 nju1|j1' k1'> c1'_{k1'} c1''_{k1'-nju1},
 //        S2 the same for rotor 2 with (l2, nju2),
 //   M3 = sum_{m'} <j1' m' j2' m-m'|j12' m> sum_{me} <l1 me l2 -me|l 0>
 //        <j1'' m'' j2'' m-m''|j12'' m> <j1'' m'' l1 me|j1' m'> <j2'' m-m'' l2 -me|j2' m-m'>,
-//        m'' = m' - me.
+//        m'' = m' - me,
+// zero unless (j1'', l1, j1'), (l1, l2, l) and (j2'', l2, j2') obey the triangle rule.
 // Two asymmetric tops (case 0, :8257-8672): pref = 1/(8 pi^2).  Asymmetric top +
 // diatom (case 8, :7826-8058): rotor 2's vector is the unit vector at K = 0 and
 // nju2 = 0, so S2 = <j2'' 0 l2 0|j2' 0> and pref = 1/(4 pi).  Symmetric top + diatom
 // (case 7, :7593-7824): as case 8 with rotor 1's parity-adapted vector.
-__global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
-                                         const int* __restrict__ st_chan,
-                                         const int* __restrict__ st_j12,
-                                         const int* __restrict__ st_m, const int* __restrict__ ch_j1,
-                                         const int* __restrict__ ch_j2,
-                                         const double* __restrict__ vec1, int ldv1,
-                                         const double* __restrict__ vec2, int ldv2,
-                                         const int* __restrict__ lab5, double pref,
-                                         double* __restrict__ A) {
+//
+// K depends on the two channels and the term only, M3 on the pair and (l1, l2, l)
+// only: they are formed once per (channel pair, term) and per (pair, distinct
+// (l1, l2, l)), and A in the contraction, with the products in the order above.
+
+// K[(c' n_ch + c'') n_terms + t].
+__global__ void expansion_k_kernel(int n_ch, int n_terms, const int* __restrict__ ch_j1,
+                                   const int* __restrict__ ch_j2,
+                                   const double* __restrict__ vec1, int ldv1,
+                                   const double* __restrict__ vec2, int ldv2,
+                                   const int* __restrict__ lab5, double* __restrict__ K) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= P * n_terms) return;
-  const int64_t k = idx / n_terms;
+  if (idx >= (int64_t)n_ch * n_ch * n_terms) return;
   const int t = (int)(idx % n_terms);
-  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
-  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int64_t cc = idx / n_terms;
+  const int cp = (int)(cc / n_ch), cpp = (int)(cc % n_ch);
   const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
-  const int j12p = st_j12[sp], j12pp = st_j12[spp], m = st_m[sp];
   const int l1 = lab5[5 * t], nju1 = lab5[5 * t + 1], l2 = lab5[5 * t + 2],
             nju2 = lab5[5 * t + 3], l = lab5[5 * t + 4];
-  double a = 0.0;
+  double kt = 0.0;
   if (triangle_ok(j1pp, l1, j1p) && triangle_ok(l1, l2, l) && triangle_ok(j2pp, l2, j2p)) {
     const double* v1p = vec1 + (size_t)cp * ldv1;
     const double* v1pp = vec1 + (size_t)cpp * ldv1;
     const double* v2p = vec2 + (size_t)cp * ldv2;
     const double* v2pp = vec2 + (size_t)cpp * ldv2;
-    double kt = 0.0;
     const int n_planar = (nju1 == 0 && nju2 == 0) ? 1 : 2;
     for (int planar = 0; planar < n_planar; ++planar) {
       const int n1 = planar ? -nju1 : nju1, n2 = planar ? -nju2 : nju2;
@@ -1360,35 +1360,151 @@ __global__ void expansion_angular_kernel(int64_t P, int n_terms, const int* __re
       const double s1 = rotor_sum(j1pp, l1, j1p, n1, v1p, v1pp);
       if (s1 != 0.0) kt += phase * s1 * rotor_sum(j2pp, l2, j2p, n2, v2p, v2pp);
     }
-    double m3 = 0.0;
-    if (kt != 0.0) {
-      const int mx = l1 < l2 ? l1 : l2;
-      for (int mp = -j1p; mp <= j1p; ++mp) {
-        if (abs(m - mp) > j2p) continue;
-        double m2 = 0.0;
-        for (int me = -mx; me <= mx; ++me) {
-          const int mpp = mp - me;
-          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
-          m2 += cg_dev(l1, me, l2, -me, l, 0) * cg_dev(j1pp, mpp, j2pp, m - mpp, j12pp, m) *
-                cg_dev(j1pp, mpp, l1, me, j1p, mp) * cg_dev(j2pp, m - mpp, l2, -me, j2p, m - mp);
-        }
-        m3 += m2 * cg_dev(j1p, mp, j2p, m - mp, j12p, m);
-      }
-    }
-    a = pref * sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) * kt * m3 *
-        sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) * sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
   }
-  A[idx] = a;
+  K[idx] = kt;
 }
 
-// M[k * nR + i] = sum_t A[k, t] T[t * nR + i] (fixed order); one CTA per pair, the
-// pair's coefficients staged in shared memory, threads along R (coalesced T rows).
+// M3[k n_u + u] for the distinct (l1, l2, l) = lll[3u .. 3u+2].
+__global__ void expansion_m3_kernel(int64_t P, int n_u, const int* __restrict__ ind_mat,
+                                    const int* __restrict__ st_chan,
+                                    const int* __restrict__ st_j12, const int* __restrict__ st_m,
+                                    const int* __restrict__ ch_j1, const int* __restrict__ ch_j2,
+                                    const int* __restrict__ lll, double* __restrict__ M3) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * n_u) return;
+  const int64_t k = idx / n_u;
+  const int u = (int)(idx % n_u);
+  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
+  const int j12p = st_j12[sp], j12pp = st_j12[spp], m = st_m[sp];
+  const int l1 = lll[3 * u], l2 = lll[3 * u + 1], l = lll[3 * u + 2];
+  double m3 = 0.0;
+  if (triangle_ok(j1pp, l1, j1p) && triangle_ok(l1, l2, l) && triangle_ok(j2pp, l2, j2p)) {
+    const int mx = l1 < l2 ? l1 : l2;
+    for (int mp = -j1p; mp <= j1p; ++mp) {
+      if (abs(m - mp) > j2p) continue;
+      double m2 = 0.0;
+      for (int me = -mx; me <= mx; ++me) {
+        const int mpp = mp - me;
+        if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+        m2 += cg_dev(l1, me, l2, -me, l, 0) * cg_dev(j1pp, mpp, j2pp, m - mpp, j12pp, m) *
+              cg_dev(j1pp, mpp, l1, me, j1p, mp) * cg_dev(j2pp, m - mpp, l2, -me, j2p, m - mp);
+      }
+      m3 += m2 * cg_dev(j1p, mp, j2p, m - mp, j12p, m);
+    }
+  }
+  M3[idx] = m3;
+}
+
+// Clebsch-Gordan tables for expansion_m3_table_kernel, filled by cg_dev (the same
+// values the direct kernel computes):
+//   rotor-l table  G(ja, jc, lb, ma, mb) = <ja ma lb mb|jc ma+mb>, ja, jc <= Ja, lb <= Lb,
+//     at (((ja (Ja+1) + jc) (Lb+1) + lb) (2Ja+1) + ma + Ja) (2Lb+1) + mb + Lb;
+//   state table    S(s, mp) = <j1 mp j2 m-mp|j12 m> of state s, mp in -J1..J1;
+//   term table     L(u, me) = <l1 me l2 -me|l 0> of (l1, l2, l)_u, me in -Lm..Lm.
+__global__ void cg_rotor_table_kernel(int Ja, int Lb, double* __restrict__ G) {
+  const int64_t n = (int64_t)(Ja + 1) * (Ja + 1) * (Lb + 1) * (2 * Ja + 1) * (2 * Lb + 1);
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  int64_t r = idx;
+  const int mb = (int)(r % (2 * Lb + 1)) - Lb;
+  r /= 2 * Lb + 1;
+  const int ma = (int)(r % (2 * Ja + 1)) - Ja;
+  r /= 2 * Ja + 1;
+  const int lb = (int)(r % (Lb + 1));
+  r /= Lb + 1;
+  const int jc = (int)(r % (Ja + 1));
+  const int ja = (int)(r / (Ja + 1));
+  G[idx] = cg_dev(ja, ma, lb, mb, jc, ma + mb);
+}
+__global__ void cg_state_table_kernel(int n_states, int J1, const int* __restrict__ st_chan,
+                                      const int* __restrict__ st_j12,
+                                      const int* __restrict__ st_m,
+                                      const int* __restrict__ ch_j1,
+                                      const int* __restrict__ ch_j2, double* __restrict__ S) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n_states * (2 * J1 + 1)) return;
+  const int s = (int)(idx / (2 * J1 + 1)), mp = (int)(idx % (2 * J1 + 1)) - J1;
+  const int c = st_chan[s], m = st_m[s];
+  S[idx] = cg_dev(ch_j1[c], mp, ch_j2[c], m - mp, st_j12[s], m);
+}
+__global__ void cg_term_table_kernel(int n_u, int Lm, const int* __restrict__ lll,
+                                     double* __restrict__ L) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_u * (2 * Lm + 1)) return;
+  const int u = idx / (2 * Lm + 1), me = idx % (2 * Lm + 1) - Lm;
+  L[idx] = cg_dev(lll[3 * u], me, lll[3 * u + 1], -me, lll[3 * u + 2], 0);
+}
+
+// expansion_m3_kernel with the Clebsch-Gordan coefficients read from the tables;
+// the same products in the same order.  G1: rotor 1 (Ja = J1, Lb = L1), G2: rotor 2
+// (Ja = J2, Lb = L2).
+__global__ void expansion_m3_table_kernel(int64_t P, int n_u, const int* __restrict__ ind_mat,
+                                          const int* __restrict__ st_chan,
+                                          const int* __restrict__ st_m,
+                                          const int* __restrict__ ch_j1,
+                                          const int* __restrict__ ch_j2,
+                                          const int* __restrict__ lll, int J1, int L1, int J2,
+                                          int L2, int Lm, const double* __restrict__ G1,
+                                          const double* __restrict__ G2,
+                                          const double* __restrict__ S,
+                                          const double* __restrict__ L,
+                                          double* __restrict__ M3) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * n_u) return;
+  const int64_t k = idx / n_u;
+  const int u = (int)(idx % n_u);
+  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
+  const int m = st_m[sp];
+  const int l1 = lll[3 * u], l2 = lll[3 * u + 1], l = lll[3 * u + 2];
+  double m3 = 0.0;
+  if (triangle_ok(j1pp, l1, j1p) && triangle_ok(l1, l2, l) && triangle_ok(j2pp, l2, j2p)) {
+    const int mx = l1 < l2 ? l1 : l2;
+    const double* g1 = G1 + (((int64_t)j1pp * (J1 + 1) + j1p) * (L1 + 1) + l1) *
+                                (2 * J1 + 1) * (2 * L1 + 1);
+    const double* g2 = G2 + (((int64_t)j2pp * (J2 + 1) + j2p) * (L2 + 1) + l2) *
+                                (2 * J2 + 1) * (2 * L2 + 1);
+    const double* s_p = S + (int64_t)sp * (2 * J1 + 1) + J1;
+    const double* s_pp = S + (int64_t)spp * (2 * J1 + 1) + J1;
+    const double* lt = L + (int64_t)u * (2 * Lm + 1) + Lm;
+    for (int mp = -j1p; mp <= j1p; ++mp) {
+      if (abs(m - mp) > j2p) continue;
+      double m2 = 0.0;
+      for (int me = -mx; me <= mx; ++me) {
+        const int mpp = mp - me;
+        if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+        m2 += lt[me] * s_pp[mpp] * g1[(mpp + J1) * (2 * L1 + 1) + me + L1] *
+              g2[(m - mpp + J2) * (2 * L2 + 1) - me + L2];
+      }
+      m3 += m2 * s_p[mp];
+    }
+  }
+  M3[idx] = m3;
+}
+
+// M[k * nR + i] = sum_t A[k, t] T[t * nR + i] (fixed order); one CTA per pair: the
+// pair's coefficients A[k, t] = fac_t K M3 c_k into shared memory, then threads along R
+// (coalesced T rows).  fac_t = pref sqrt((2l1+1)(2l2+1)), u_t the term's (l1, l2, l).
 __global__ void __launch_bounds__(128)
-expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
-                          const double* __restrict__ T, double* __restrict__ M) {
+expansion_contract_kernel(int n_ch, int n_terms, int n_u, int nR, const int* __restrict__ ind_mat,
+                          const int* __restrict__ st_chan, const int* __restrict__ ch_j1,
+                          const int* __restrict__ ch_j2, const double* __restrict__ K,
+                          const double* __restrict__ M3, const double* __restrict__ fac,
+                          const int* __restrict__ term_u, const double* __restrict__ T,
+                          double* __restrict__ M) {
   extern __shared__ double ex_a[];
   const int64_t k = blockIdx.x;
-  for (int t = threadIdx.x; t < n_terms; t += blockDim.x) ex_a[t] = A[k * n_terms + t];
+  const int cp = st_chan[ind_mat[2 * k] - 1], cpp = st_chan[ind_mat[2 * k + 1] - 1];
+  const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
+  const double c1 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0));
+  const double c2 = sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+  const double* Kc = K + ((int64_t)cp * n_ch + cpp) * n_terms;
+  const double* Mk = M3 + k * n_u;
+  for (int t = threadIdx.x; t < n_terms; t += blockDim.x)
+    ex_a[t] = fac[t] * Kc[t] * Mk[term_u[t]] * c1 * c2;
   __syncthreads();
   for (int i = threadIdx.x; i < nR; i += blockDim.x) {
     double s = 0.0;
@@ -1399,6 +1515,10 @@ expansion_contract_kernel(int n_terms, int nR, const double* __restrict__ A,
 
 namespace {
 
+// Largest Clebsch-Gordan table (doubles) the angular set-up builds; larger j/l ranges
+// evaluate the coefficients directly.
+constexpr int64_t kCgTableMax = (int64_t)8 << 20;
+
 // The expansion build as a plan: set-up (validation, uploads) and the R-independent
 // angular coefficients once; then per set of radial terms the contraction, the cut-off
 // and the spline on device buffers.
@@ -1408,8 +1528,9 @@ struct ExpansionPlan {
   double cut_hartree = 0.0;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  DevBuf<int> d_k2r;
-  DevBuf<double> d_A, d_M, d_gc;
+  int n_ch = 0, n_u = 0;
+  DevBuf<int> d_k2r, d_ind, d_chan, d_j1, d_j2, d_term_u;
+  DevBuf<double> d_K, d_M3, d_fac, d_M, d_gc;
 
   ~ExpansionPlan() {
     for (auto& e : ev)
@@ -1519,8 +1640,23 @@ struct ExpansionPlan {
     this->nR = nR;
     this->n_terms = n_terms;
     std::vector<int> ch_j1(sys->j1, sys->j1 + n_ch), ch_j2(sys->j2, sys->j2 + n_ch);
-    DevBuf<int> d_ind, d_chan, d_j12, d_m, d_j1, d_j2, d_lab;
+    DevBuf<int> d_j12, d_m, d_lab, d_lll;
     DevBuf<double> d_vec1, d_vec2;
+    this->n_ch = n_ch;
+    // the distinct (l1, l2, l) of the terms, and per term pref sqrt((2l1+1)(2l2+1))
+    std::vector<int> lll, term_u(n_terms);
+    std::vector<double> fac(n_terms);
+    for (int t = 0; t < n_terms; ++t) {
+      const int l1 = lab5[5 * t], l2 = lab5[5 * t + 2], l = lab5[5 * t + 4];
+      int u = 0;
+      while (u < (int)lll.size() / 3 &&
+             !(lll[3 * u] == l1 && lll[3 * u + 1] == l2 && lll[3 * u + 2] == l))
+        ++u;
+      if (u == (int)lll.size() / 3) lll.insert(lll.end(), {l1, l2, l});
+      term_u[t] = u;
+      fac[t] = pref * sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0));
+    }
+    n_u = (int)lll.size() / 3;
     MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
     MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
     MQCT_CUDA_TRY(d_j12.upload(sys->j12, n_states, st));
@@ -1532,21 +1668,57 @@ struct ExpansionPlan {
     if (type != 0) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
     else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));
     MQCT_CUDA_TRY(d_lab.upload(lab5, st));
+    MQCT_CUDA_TRY(d_lll.upload(lll, st));
+    MQCT_CUDA_TRY(d_term_u.upload(term_u, st));
+    MQCT_CUDA_TRY(d_fac.upload(fac, st));
     std::vector<double> Rh(R, R + nR);
     MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
     std::vector<int> k2r(P);
     for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
     MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
-    MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
+    MQCT_CUDA_TRY(d_K.alloc((size_t)n_ch * n_ch * n_terms));
+    MQCT_CUDA_TRY(d_M3.alloc((size_t)P * n_u));
     MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
     ir1 = nearest_index(Rh, r_cut1);
     ir2 = nearest_index(Rh, r_cut2);
     cut_hartree = mij_cutoff_cm * kCmToHartree;
-    const int64_t n_at = P * n_terms;
+    const int64_t n_k = (int64_t)n_ch * n_ch * n_terms, n_m3 = P * n_u;
+    // table sizes from the actual j and l ranges
+    int L1 = 0, L2 = 0, Lm = 0;
+    for (int u = 0; u < n_u; ++u) {
+      L1 = std::max(L1, lll[3 * u]);
+      L2 = std::max(L2, lll[3 * u + 1]);
+      Lm = std::max(Lm, std::min(lll[3 * u], lll[3 * u + 1]));
+    }
+    const int J1 = j1max, J2 = j2max;
+    const int64_t n_g1 = (int64_t)(J1 + 1) * (J1 + 1) * (L1 + 1) * (2 * J1 + 1) * (2 * L1 + 1);
+    const int64_t n_g2 = (int64_t)(J2 + 1) * (J2 + 1) * (L2 + 1) * (2 * J2 + 1) * (2 * L2 + 1);
+    const bool tables = n_g1 <= kCgTableMax && n_g2 <= kCgTableMax;
+    DevBuf<double> d_tab;  // the four tables in one allocation
     MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
-    expansion_angular_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
-        P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_vec1.p, ldv1, d_vec2.p,
-        ldv2, d_lab.p, pref, d_A.p);
+    expansion_k_kernel<<<(unsigned)((n_k + 127) / 128), 128, 0, st>>>(
+        n_ch, n_terms, d_j1.p, d_j2.p, d_vec1.p, ldv1, d_vec2.p, ldv2, d_lab.p, d_K.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    if (tables) {
+      const int64_t n_st = (int64_t)n_states * (2 * J1 + 1), n_lt = (int64_t)n_u * (2 * Lm + 1);
+      MQCT_CUDA_TRY(d_tab.alloc((size_t)(n_g1 + n_g2 + n_st + n_lt)));
+      double* g1 = d_tab.p;
+      double* g2 = g1 + n_g1;
+      double* stab = g2 + n_g2;
+      double* ltab = stab + n_st;
+      cg_rotor_table_kernel<<<(unsigned)((n_g1 + 127) / 128), 128, 0, st>>>(J1, L1, g1);
+      cg_rotor_table_kernel<<<(unsigned)((n_g2 + 127) / 128), 128, 0, st>>>(J2, L2, g2);
+      cg_state_table_kernel<<<(unsigned)((n_st + 127) / 128), 128, 0, st>>>(
+          n_states, J1, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, stab);
+      cg_term_table_kernel<<<(unsigned)((n_lt + 127) / 128), 128, 0, st>>>(n_u, Lm, d_lll.p, ltab);
+      MQCT_CUDA_TRY(cudaGetLastError());
+      expansion_m3_table_kernel<<<(unsigned)((n_m3 + 127) / 128), 128, 0, st>>>(
+          P, n_u, d_ind.p, d_chan.p, d_m.p, d_j1.p, d_j2.p, d_lll.p, J1, L1, J2, L2, Lm, g1, g2,
+          stab, ltab, d_M3.p);
+    } else {
+      expansion_m3_kernel<<<(unsigned)((n_m3 + 127) / 128), 128, 0, st>>>(
+          P, n_u, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_j1.p, d_j2.p, d_lll.p, d_M3.p);
+    }
     MQCT_CUDA_TRY(cudaGetLastError());
     MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
     MQCT_CUDA_TRY(cudaStreamSynchronize(st));  // the set-up buffers are released on return
@@ -1560,7 +1732,8 @@ struct ExpansionPlan {
     MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], st));
     expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
-        n_terms, nR, d_A.p, d_terms, d_M.p);
+        n_ch, n_terms, n_u, nR, d_ind.p, d_chan.p, d_j1.p, d_j2.p, d_K.p, d_M3.p, d_fac.p,
+        d_term_u.p, d_terms, d_M.p);
     MQCT_CUDA_TRY(cudaGetLastError());
     finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
         P, nR, d_k2r.p, d_M.p, 1, 0, nR, e_unit, nullptr, ir1, ir2, cut_hartree, d_gc.p, d_mat,
