@@ -100,3 +100,25 @@ def test_expansion_plan_reuse(mq, gpu_available):
     ang, ex = plan.timing()
     assert ang > 0.0 and ex > 0.0
     plan.close()
+
+
+def test_expansion_high_j_direct_path(mq, oracle, gpu_available):
+    """j = 20 rotor levels with an l1 = 20 term: the Clebsch-Gordan table of the angular
+    set-up would exceed its size cap, so the coefficients are evaluated directly; the
+    result agrees with the oracle as on the table path."""
+    chans = [(20, 0, 20, 0), (19, 0, 19, 0), (20, 1, 20, 0)]
+    s = mq.CollisionSystem(8, chans, A=27.88, B=9.28, C=14.52, BE=60.85)
+    R = np.linspace(4.0, 12.0, 9)
+    labels = np.array([[20, 0, 0, 20], [2, 0, 0, 2], [19, 2, 0, 19]], np.int32)
+    rng = np.random.default_rng(3)
+    terms = rng.standard_normal((len(R), len(labels)))
+    m, _, _ = mq.build_matrix_expansion(s, R, labels, terms, mij_cutoff=0.0)
+    ch = s.channels
+    osys = oracle.OracleSystem(8, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], e_ch=s.e_ch,
+                               vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    mo = oracle.expansion_matrix_type8(osys, osys.states(), s.ind_mat, labels, terms)
+    assert np.abs(mo).max() > 0
+    # at j = 20 the alternating Racah sums of the coefficients cancel several digits, and
+    # the two evaluations (log-factorial exponentials here, the oracle's 3j routine there)
+    # lose different ones: 6e-12 of the largest element
+    assert np.max(np.abs(m - mo)) <= 1e-10 * np.abs(mo).max()
