@@ -1656,3 +1656,148 @@ int orc_expansion_matrix_type7(const orc_system* sys, const int32_t* indx_chann,
   }
   return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* Identical partners (IDENTICAL = YES with IDENTICAL_PES = YES), SYS_TYPE 0,
+ * SRC/pot_comp.f:8257-8746 (EXPANSION_MATRIX_ELEMENT, case 0, all four symmetry
+ * branches).  States carry the exchange parity par = parity_state (+-1,
+ * SRC/matrix_ini.f:482-530); the channel's inversion parity p_inv = p1 p2 with p_r the
+ * sign of c_K c_-K for the first K = -j.. with a non-zero product (SRC/pot_comp.f:
+ * 70-110) and kappa = (-1)^(k1 + k2), k_r the parity of Ka_r - Kc_r (SRC/matrix_ini.f:
+ * 9147-9190) give parity_state_bk = (-1)^j12 p_inv kappa (SRC/matrix_ini.f:504), except
+ * for a diagonal pair of a channel whose two rotors are in the same level, where it is
+ * (-1)^j12 (SRC/pot_comp.f:8500-8505).  Per pair and term (l1, nju1, l2, nju2, l):
+ *   sym1: (j1'',l1,j1'), (j2'',l2,j2') triangles -- the direct branch;
+ *   sym2: unless l1 = l2 and |nju1| = |nju2|, (j1'',l2,j1'), (j2'',l1,j2') -- l1 <-> l2;
+ *   sym3: (j1'',l1,j2'), (j2'',l2,j1') -- the molecules exchanged, times par' bk';
+ *   sym4: unless l1 = l2 and |nju1| = |nju2|, (j1'',l2,j2'), (j2'',l1,j1'), likewise,
+ * each a planar sum of products of rotor sums (K-sums), and a sum over m' (|m'| <= j1'
+ * for the direct branches, |m'| <= j2' for the exchanged ones) and m_e of Clebsch-Gordan
+ * products (:8577-8650; the source loops m' over -j1'..j1' for all four, but the
+ * reference's own output for this case, EXAMPLES_IO/SYS_TYPE_0/H2O_H2O_Identical/MTRX.DAT,
+ * has the exchanged branches summed over |m'| <= j2', which this follows); the element is divided by
+ * sqrt(1 + d(j1',j2') d_p) sqrt(1 + d(j1'',j2'') d_pp), d_p = 1 when the two rotors of
+ * the channel are in the same level (:8674-8684). */
+static double orc_ksum(int jpp, int l, int jp, int nju, const double* vp, const double* vpp) {
+  double s = 0.0;
+  for (int kp = -jp; kp <= jp; ++kp) {
+    const int kpp = kp - nju;
+    if (abs(kpp) > jpp) continue;
+    s += orc_cg(jpp, l, jp, kpp, nju, kp) * vp[jp + kp] * vpp[jpp + kpp];
+  }
+  return s;
+}
+int orc_parity_inversion(const double* v1, int j1, const double* v2, int j2) {
+  int par[2] = {1, 1};
+  const double* v[2] = {v1, v2};
+  const int jj[2] = {j1, j2};
+  for (int r = 0; r < 2; ++r)
+    for (int i = 0; i <= jj[r]; ++i) {  /* K = -j + i and -K */
+      const double d = v[r][i] * v[r][2 * jj[r] - i];
+      if (d == 0.0) continue;
+      par[r] = d > 0.0 ? 1 : -1;
+      break;
+    }
+  return par[0] * par[1];
+}
+int orc_expansion_matrix_type0_identical(const orc_system* sys, const int32_t* indx_chann,
+                                         const int32_t* j12, const int32_t* m12,
+                                         const int32_t* parity, int64_t P,
+                                         const int32_t* ind_mat, int n_terms,
+                                         const int32_t* labels, int nR, const double* terms,
+                                         double e_unit, double* mat) {
+  if (sys->sys_type != 0 || !sys->j2 || !sys->vec1 || !sys->vec2 || !sys->ka1 || !sys->kc1 ||
+      !sys->ka2 || !sys->kc2 || !parity)
+    return -1;
+  const int nch = sys->n_channels;
+  int* pinv = (int*)malloc(sizeof(int) * nch);
+  int* kap = (int*)malloc(sizeof(int) * nch);
+  int* same = (int*)malloc(sizeof(int) * nch);
+  for (int c = 0; c < nch; ++c) {
+    pinv[c] = orc_parity_inversion(sys->vec1 + (size_t)c * sys->ldv, sys->j1[c],
+                                   sys->vec2 + (size_t)c * sys->ldv, sys->j2[c]);
+    const int k1 = abs(sys->ka1[c] - sys->kc1[c]) % 2, k2 = abs(sys->ka2[c] - sys->kc2[c]) % 2;
+    kap[c] = ((k1 + k2) % 2) ? -1 : 1;
+    same[c] = sys->j1[c] == sys->j2[c] && sys->ka1[c] == sys->ka2[c] && sys->kc1[c] == sys->kc2[c];
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t k = 0; k < P; ++k) {
+    const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+    const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
+    const int j1p = sys->j1[cp], j2p = sys->j2[cp], j1pp = sys->j1[cpp], j2pp = sys->j2[cpp];
+    const int j12p = j12[sp], j12pp = j12[spp], m = m12[sp];
+    const double* v1p = sys->vec1 + (size_t)cp * sys->ldv;
+    const double* v1pp = sys->vec1 + (size_t)cpp * sys->ldv;
+    const double* v2p = sys->vec2 + (size_t)cp * sys->ldv;
+    const double* v2pp = sys->vec2 + (size_t)cpp * sys->ldv;
+    const double par_p = parity[sp];
+    double bk_par1 = ((j12p % 2) ? -1.0 : 1.0) * pinv[cp] * kap[cp];
+    if (sp == spp && same[cp]) bk_par1 = (j12p % 2) ? -1.0 : 1.0;
+    const double coef12 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+    double* out = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) out[i] = 0.0;
+    for (int t = 0; t < n_terms; ++t) {
+      const int l1 = labels[5 * t], nju1 = labels[5 * t + 1], l2 = labels[5 * t + 2],
+                nju2 = labels[5 * t + 3], l = labels[5 * t + 4];
+      if (!orc_triangle(l1, l2, l)) continue;
+      const double coef3 = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (8.0 * ORC_PI * ORC_PI);
+      const int n_planar = (nju1 == 0 && nju2 == 0) ? 1 : 2;
+      const int swap_ok = !(l1 == l2 && abs(nju1) == abs(nju2));
+      const int s1 = orc_triangle(j1pp, l1, j1p) && orc_triangle(j2pp, l2, j2p);
+      const int s2 = swap_ok && orc_triangle(j1pp, l2, j1p) && orc_triangle(j2pp, l1, j2p);
+      const int s3 = orc_triangle(j1pp, l1, j2p) && orc_triangle(j2pp, l2, j1p);
+      const int s4 = swap_ok && orc_triangle(j1pp, l2, j2p) && orc_triangle(j2pp, l1, j1p);
+      if (!s1 && !s2 && !s3 && !s4) continue;
+      double k1 = 0.0, k2 = 0.0, k3 = 0.0, k4 = 0.0;
+      for (int planar = 0; planar < n_planar; ++planar) {
+        const int n1 = planar ? -nju1 : nju1, n2 = planar ? -nju2 : nju2;
+        const double sg = planar ? (((l1 + l2 + l + nju1 + nju2) % 2) ? -1.0 : 1.0) : 1.0;
+        const double sx = ((l1 + l2) % 2) ? -1.0 : 1.0;
+        if (s1) k1 += orc_ksum(j1pp, l1, j1p, n1, v1p, v1pp) * orc_ksum(j2pp, l2, j2p, n2, v2p, v2pp) * sg;
+        if (s2)
+          k2 += orc_ksum(j1pp, l2, j1p, n2, v1p, v1pp) * orc_ksum(j2pp, l1, j2p, n1, v2p, v2pp) * (sg * sx);
+        if (s3)
+          k3 += orc_ksum(j1pp, l1, j2p, n1, v2p, v1pp) * orc_ksum(j2pp, l2, j1p, n2, v1p, v2pp) * sg *
+                par_p * bk_par1;
+        if (s4)
+          k4 += orc_ksum(j1pp, l2, j2p, n2, v2p, v1pp) * orc_ksum(j2pp, l1, j1p, n1, v1p, v2pp) *
+                (sg * sx) * par_p * bk_par1;
+      }
+      double m5 = 0.0;
+      const int mx = l1 < l2 ? l1 : l2;
+      const int jm = j1p > j2p ? j1p : j2p;  /* direct branches |m'| <= j1', exchanged <= j2' */
+      for (int mp = -jm; mp <= jm; ++mp) {
+        if (abs(m - mp) > j1p && abs(m - mp) > j2p) continue;
+        const double cg_p = orc_cg(j1p, j2p, j12p, mp, m - mp, m);   /* 0 when |m - mp| > j2' */
+        const double cg_x = orc_cg(j2p, j1p, j12p, mp, m - mp, m);
+        double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+        for (int me = -mx; me <= mx; ++me) {
+          const int mpp = mp - me;
+          if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+          const double c0 = orc_cg(l1, l2, l, me, -me, 0) * orc_cg(j1pp, j2pp, j12pp, mpp, m - mpp, m);
+          if (abs(mp) <= j1p) {
+            if (s1) a1 += c0 * orc_cg(j1pp, l1, j1p, mpp, me, mp) * orc_cg(j2pp, l2, j2p, m - mpp, -me, m - mp);
+            if (s2) a2 += c0 * orc_cg(j1pp, l2, j1p, mpp, me, mp) * orc_cg(j2pp, l1, j2p, m - mpp, -me, m - mp);
+          }
+          if (abs(mp) <= j2p) {
+            if (s3) a3 += c0 * orc_cg(j1pp, l1, j2p, mpp, me, mp) * orc_cg(j2pp, l2, j1p, m - mpp, -me, m - mp);
+            if (s4) a4 += c0 * orc_cg(j1pp, l2, j2p, mpp, me, mp) * orc_cg(j2pp, l1, j1p, m - mpp, -me, m - mp);
+          }
+        }
+        if (s1) m5 += a1 * cg_p * k1;
+        if (s2) m5 += a2 * cg_p * k2;
+        if (s3) m5 += a3 * cg_x * k3;
+        if (s4) m5 += a4 * cg_x * k4;
+      }
+      const double a = coef3 * m5;
+      if (a == 0.0) continue;
+      for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
+    }
+    const double dp = (j1p == j2p && same[cp]) ? 1.0 : 0.0, dpp = (j1pp == j2pp && same[cpp]) ? 1.0 : 0.0;
+    const double norm = coef12 / sqrt(1.0 + dp) / sqrt(1.0 + dpp);
+    for (int i = 0; i < nR; ++i) out[i] *= norm * e_unit;
+  }
+  free(pinv); free(kap); free(same);
+  return 0;
+}

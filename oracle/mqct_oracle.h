@@ -202,6 +202,18 @@ int orc_expansion_matrix_type7(const orc_system* sys, const int32_t* indx_chann,
                                const int32_t* ind_mat, int n_terms, const int32_t* labels,
                                int nR, const double* terms, double e_unit, double* mat);
 
+/* SYS_TYPE 0 with identical partners (IDENTICAL = YES, IDENTICAL_PES = YES),
+ * SRC/pot_comp.f:8257-8746: parity[s] = the exchange parity of state s (+1/-1); the
+ * system needs ka1, kc1, ka2, kc2, vec1 and vec2. */
+int orc_expansion_matrix_type0_identical(const orc_system* sys, const int32_t* indx_chann,
+                                         const int32_t* j12, const int32_t* m12,
+                                         const int32_t* parity, int64_t P,
+                                         const int32_t* ind_mat, int n_terms,
+                                         const int32_t* labels, int nR, const double* terms,
+                                         double e_unit, double* mat);
+/* Inversion parity p1 p2 of a channel from its rotor vectors (SRC/pot_comp.f:70-110). */
+int orc_parity_inversion(const double* v1, int j1, const double* v2, int j2);
+
 #ifdef __cplusplus
 }
 #endif

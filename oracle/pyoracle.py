@@ -122,6 +122,11 @@ def lib():
                                      C.c_int, f64p, C.c_double, f64p]
         L.orc_dotraject_rec.argtypes = [C.POINTER(Tables), C.POINTER(Traj), f64p, f64p, f64p,
                                         f64p, C.c_int64, C.POINTER(C.c_int64)]
+        L.orc_expansion_matrix_type0_identical.argtypes = [C.POINTER(System), C.c_void_p,
+                                                          C.c_void_p, C.c_void_p, C.c_void_p,
+                                                          C.c_int64, C.c_void_p, C.c_int,
+                                                          C.c_void_p, C.c_int, C.c_void_p,
+                                                          C.c_double, C.c_void_p]
         L.orc_expansion_matrix_type7.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
                                                  C.c_void_p, C.c_int, C.c_void_p, C.c_double,
@@ -427,4 +432,24 @@ def expansion_matrix_type7(osys, states, ind, labels, terms, e_unit):
                                           _ptr(mat))
     if rc:
         raise RuntimeError(f"orc_expansion_matrix_type7 failed: {rc}")
+    return mat.reshape(P, nR)
+
+
+def expansion_matrix_type0_identical(osys, states, parity, ind, labels, terms, e_unit):
+    """SYS_TYPE 0 matrix for identical partners (P x nR, Hartree); parity: exchange parity
+    per state; labels n_terms x 5."""
+    ic, j12, m12, _ = states
+    par = np.ascontiguousarray(parity, np.int32)
+    ind = np.ascontiguousarray(ind, np.int32)
+    labels = np.ascontiguousarray(labels, np.int32).reshape(-1, 5)
+    terms = np.ascontiguousarray(terms, np.float64)
+    P, nR = ind.shape[0], terms.shape[0]
+    mat = np.zeros(P * nR)
+    rc = lib().orc_expansion_matrix_type0_identical(
+        C.byref(osys.s), _ptr(np.ascontiguousarray(ic, np.int32)),
+        _ptr(np.ascontiguousarray(j12, np.int32)), _ptr(np.ascontiguousarray(m12, np.int32)),
+        _ptr(par), P, _ptr(ind.reshape(-1)), labels.shape[0], _ptr(labels.reshape(-1)), nR,
+        _ptr(terms), e_unit, _ptr(mat))
+    if rc:
+        raise RuntimeError(f"orc_expansion_matrix_type0_identical failed: {rc}")
     return mat.reshape(P, nR)

@@ -114,6 +114,25 @@ def main(ref_root):
         e_ch_printed=np.array([0.0, 10.2864, 30.8592, 61.7184, 43.3431, 43.3431, 8.2447, 8.2447,
                                28.8175, 28.8175, 59.6767, 59.6767, 100.8223, 152.2543]))
 
+    # G5c: two identical asymmetric tops (SYS_TYPE 0, IDENTICAL = YES, IDENTICAL_PES = YES),
+    # H2O+H2O (EXAMPLES_IO/SYS_TYPE_0/H2O_H2O_Identical): 152 terms (kcal/mol) at 2 R
+    # points -> MTRX.DAT (81 parity-adapted states with their exchange parity P, 322 pairs).
+    d = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_Identical")
+    coll0, nch0, states0, ind0, R0, mat0 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 11)
+    inp = open(os.path.join(d, "H2O_H2O_Identical.inp")).read()
+    tl = re.split(r"(?<![A-Z_])TERMS\s*=", inp)[1].split("$END")[0]
+    lab0 = np.array([int(x) for x in tl.replace(",", " ").split()], dtype=np.int32).reshape(-1, 5)
+    with open(os.path.join(d, "PES_EXPAN_TERMS.DAT")) as f:
+        f.readline()
+        rows0 = np.array([[float(x) for x in ln.split()] for ln in f if ln.strip()])
+    np.savez_compressed(
+        os.path.join(out, "g5c_h2o_h2o_identical.npz"), coll=coll0, states=states0, ind_mat=ind0,
+        R=R0, mat=mat0, labels=lab0, terms=rows0[:, 1:], R_terms=rows0[:, 0],
+        A=27.87700, B=9.28500, C=14.51200,
+        channels=np.array([[0, 0, 0, 0, 0, 0], [0, 0, 0, 1, 1, 1], [0, 0, 0, 2, 0, 2],
+                           [1, 1, 1, 1, 1, 1], [1, 1, 1, 2, 0, 2], [2, 0, 2, 2, 0, 2]],
+                          dtype=np.int32))
+
     # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)
