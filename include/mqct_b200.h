@@ -83,6 +83,10 @@ typedef struct mqct_sys_t {
   const int32_t* indx_chann; /* per state, 1-based channel                       */
   const int32_t* j12;
   const int32_t* m12;
+  const int32_t* parity;     /* per state exchange parity parity_state (+1/-1) of
+                                identical partners (IDENTICAL = YES, SYS_TYPE 0),
+                                MQCT_SOURCE_CODES/matrix_ini.f:482-530; NULL when the
+                                partners are distinguishable                      */
 } mqct_sys_t;
 
 /* Angular quadrature (INI_POT_STORAGE, MQCT_SOURCE_CODES/pot_comp.f:333-1788):
@@ -394,6 +398,21 @@ int mqct_enumerate_states(int32_t sys_type, int32_t n_channels, const int32_t* j
                           const int32_t* j2, int32_t* indx_chann, int32_t* j12, int32_t* m12);
 int64_t mqct_count_pairs(int32_t n_states, const int32_t* m12);
 int64_t mqct_fill_ind_mat(int32_t n_states, const int32_t* m12, int32_t* ind_mat);
+/* Identical partners (SYS_TYPE 0, IDENTICAL = YES; MQCT_SOURCE_CODES/matrix_ini.f:482-530,
+ * 553-627): per channel, for p = 1 and (unless both rotors are in the same level) p = 2,
+ * the states (j12, m12) with exchange parity (-1)^(p-1), -1 for odd j12 of a same-level
+ * channel; pairs only between states of equal parity.  Same argument conventions as
+ * above; parity receives +1/-1 per state. */
+int mqct_count_states_identical(int32_t n_channels, const int32_t* j1, const int32_t* ka1,
+                                const int32_t* kc1, const int32_t* j2, const int32_t* ka2,
+                                const int32_t* kc2);
+int mqct_enumerate_states_identical(int32_t n_channels, const int32_t* j1, const int32_t* ka1,
+                                    const int32_t* kc1, const int32_t* j2, const int32_t* ka2,
+                                    const int32_t* kc2, int32_t* indx_chann, int32_t* j12,
+                                    int32_t* m12, int32_t* parity);
+int64_t mqct_count_pairs_identical(int32_t n_states, const int32_t* m12, const int32_t* parity);
+int64_t mqct_fill_ind_mat_identical(int32_t n_states, const int32_t* m12, const int32_t* parity,
+                                    int32_t* ind_mat);
 int mqct_r_grid(int32_t n, double rmin, double rmax, int32_t equidistant, double* R);
 
 /* MTRX_UF.DAT (Fortran unformatted sequential, 4-byte record markers):

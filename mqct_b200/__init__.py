@@ -50,11 +50,13 @@ class CollisionSystem:
     (MQCT_SOURCE_CODES/iotest.f:8311-8312); k and eps are kept in ka1 and kc1, and vec1 holds
     the parity-adapted top (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) over K;
     sys_type 8: channels (j1, ka1, kc1, j2), EIGEN_VAL + BE j2(j2+1) (MQCT_SOURCE_CODES/iotest.f:9069-9079);
-    sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..).
+    sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..);
+    identical=True (IDENTICAL = YES): parity-adapted states with their exchange parity
+    (self.parity), pairs only between equal parities (MQCT_SOURCE_CODES/matrix_ini.f:482-627).
     """
 
     def __init__(self, sys_type, channels, A=0.0, B=0.0, C=0.0, BE=0.0, DE=0.0, A2=None,
-                 B2=None, C2=None, e_ch=None):
+                 B2=None, C2=None, e_ch=None, identical=False):
         ch = np.asarray(channels, dtype=np.int32)
         if ch.ndim == 1:
             ch = ch[:, None]
@@ -117,18 +119,37 @@ class CollisionSystem:
             raise ValueError(f"unsupported SYS_TYPE {sys_type}")
         self.e_ch = np.asarray(E if e_ch is None else e_ch, dtype=np.float64)
         L = lib()
-        j2p = ptr(self.j2) if sys_type in (7, 8, 0) else None
-        n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
-        self.indx_chann = np.zeros(n, np.int32)
-        self.j12 = np.zeros(n, np.int32)
-        self.m12 = np.zeros(n, np.int32)
-        check(L.mqct_enumerate_states(self.sys_type, nch, self.j1, j2p, self.indx_chann,
-                                      self.j12, self.m12))
+        self.identical = bool(identical)
+        self.parity = None
+        if self.identical:
+            # IDENTICAL = YES: states carry the exchange parity, pairs join equal parities
+            if sys_type != 0:
+                raise ValueError("identical partners are supported for SYS_TYPE 0")
+            rot = [np.ascontiguousarray(x, np.int32) for x in
+                   (self.j1, self.ka1, self.kc1, self.j2, self.ka2, self.kc2)]
+            n = check(L.mqct_count_states_identical(nch, *rot))
+            self.indx_chann = np.zeros(n, np.int32)
+            self.j12 = np.zeros(n, np.int32)
+            self.m12 = np.zeros(n, np.int32)
+            self.parity = np.zeros(n, np.int32)
+            check(L.mqct_enumerate_states_identical(nch, *rot, self.indx_chann, self.j12,
+                                                    self.m12, self.parity))
+            P = check(L.mqct_count_pairs_identical(n, self.m12, self.parity))
+            ind = np.zeros(2 * P, np.int32)
+            check(L.mqct_fill_ind_mat_identical(n, self.m12, self.parity, ind))
+        else:
+            j2p = ptr(self.j2) if sys_type in (7, 8, 0) else None
+            n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
+            self.indx_chann = np.zeros(n, np.int32)
+            self.j12 = np.zeros(n, np.int32)
+            self.m12 = np.zeros(n, np.int32)
+            check(L.mqct_enumerate_states(self.sys_type, nch, self.j1, j2p, self.indx_chann,
+                                          self.j12, self.m12))
+            P = check(L.mqct_count_pairs(n, self.m12))
+            ind = np.zeros(2 * P, np.int32)
+            check(L.mqct_fill_ind_mat(n, self.m12, ind))
         self.n_states = n
         self.ej_cm = self.e_ch[self.indx_chann - 1]
-        P = check(L.mqct_count_pairs(n, self.m12))
-        ind = np.zeros(2 * P, np.int32)
-        check(L.mqct_fill_ind_mat(n, self.m12, ind))
         self.ind_mat = ind.reshape(P, 2)
         self.P = int(P)
         self.vec1 = np.ascontiguousarray(self.vec1)
@@ -138,7 +159,7 @@ class CollisionSystem:
         return _abi.Sys(self.sys_type, self.n_channels, ptr(self.j1), ptr(self.ka1), ptr(self.kc1),
                         ptr(self.j2), ptr(self.ka2), ptr(self.kc2), ptr(self.vec1),
                         ptr(self.vec2), self.ldv, self.n_states, ptr(self.indx_chann),
-                        ptr(self.j12), ptr(self.m12))
+                        ptr(self.j12), ptr(self.m12), ptr(self.parity))
 
     def state_records(self):
         """Per-state records of MTRX_UF.DAT (MQCT_SOURCE_CODES/matrix_ini.f:6666-6757)."""
@@ -154,6 +175,8 @@ class CollisionSystem:
         else:
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1],
                      self.ka2[ic - 1], self.kc2[ic - 1]]
+            if self.identical:
+                cols += [self.parity]       # the P column (matrix_ini.f:4846-4857)
         return np.ascontiguousarray(np.stack(cols, axis=1).astype(np.int32))
 
 

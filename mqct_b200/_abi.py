@@ -38,7 +38,7 @@ class Sys(C.Structure):
     _fields_ = [("sys_type", C.c_int32), ("n_channels", C.c_int32), ("j1", vp), ("ka1", vp),
                 ("kc1", vp), ("j2", vp), ("ka2", vp), ("kc2", vp), ("vec1", vp), ("vec2", vp),
                 ("ldv", C.c_int32), ("n_states", C.c_int32), ("indx_chann", vp), ("j12", vp),
-                ("m12", vp)]
+                ("m12", vp), ("parity", vp)]
 
 
 class Grid(C.Structure):
@@ -95,7 +95,8 @@ EXPORTS = [
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
     "mqct_prop_plan_destroy",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
-    "mqct_fill_ind_mat", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
+    "mqct_fill_ind_mat", "mqct_count_states_identical", "mqct_enumerate_states_identical",
+    "mqct_count_pairs_identical", "mqct_fill_ind_mat_identical", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
     "mqct_read_mtrx_uf", "mqct_write_mtrx_dat", "mqct_read_mtrx_dat_header",
     "mqct_read_mtrx_dat", "mqct_read_expansion_terms",
 ]
@@ -183,6 +184,12 @@ def lib():
     L.mqct_count_pairs.restype = C.c_int64
     L.mqct_fill_ind_mat.argtypes = [C.c_int32, i32p, i32p]
     L.mqct_fill_ind_mat.restype = C.c_int64
+    L.mqct_count_states_identical.argtypes = [C.c_int32] + [i32p] * 6
+    L.mqct_enumerate_states_identical.argtypes = [C.c_int32] + [i32p] * 10
+    L.mqct_count_pairs_identical.argtypes = [C.c_int32, i32p, i32p]
+    L.mqct_count_pairs_identical.restype = C.c_int64
+    L.mqct_fill_ind_mat_identical.argtypes = [C.c_int32, i32p, i32p, i32p]
+    L.mqct_fill_ind_mat_identical.restype = C.c_int64
     L.mqct_r_grid.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_int32, f64p]
     L.mqct_write_mtrx_uf.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, i32p, C.c_int32,
                                      C.c_int64, i32p, C.c_int32, f64p, f64p]

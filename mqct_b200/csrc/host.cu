@@ -212,6 +212,68 @@ int mqct_enumerate_states(int32_t sys_type, int32_t n_channels, const int32_t* j
   return st;
 }
 
+// Identical partners: per channel p = 1 and, unless both rotors are in the same level,
+// p = 2, each with all (j12, m12); parity (-1)^(p-1), -1 for odd j12 of a same-level
+// channel (MQCT_SOURCE_CODES/matrix_ini.f:482-530).
+static bool same_level(int c, const int32_t* j1, const int32_t* ka1, const int32_t* kc1,
+                       const int32_t* j2, const int32_t* ka2, const int32_t* kc2) {
+  return j1[c] == j2[c] && ka1[c] == ka2[c] && kc1[c] == kc2[c];
+}
+int mqct_count_states_identical(int32_t n_channels, const int32_t* j1, const int32_t* ka1,
+                                const int32_t* kc1, const int32_t* j2, const int32_t* ka2,
+                                const int32_t* kc2) {
+  if (n_channels <= 0 || !j1 || !ka1 || !kc1 || !j2 || !ka2 || !kc2) return MQCT_E_ARG;
+  int st = 0;
+  for (int c = 0; c < n_channels; ++c) {
+    const int np = same_level(c, j1, ka1, kc1, j2, ka2, kc2) ? 1 : 2;
+    for (int js = abs(j1[c] - j2[c]); js <= j1[c] + j2[c]; ++js) st += np * (2 * js + 1);
+  }
+  return st;
+}
+int mqct_enumerate_states_identical(int32_t n_channels, const int32_t* j1, const int32_t* ka1,
+                                    const int32_t* kc1, const int32_t* j2, const int32_t* ka2,
+                                    const int32_t* kc2, int32_t* indx_chann, int32_t* j12,
+                                    int32_t* m12, int32_t* parity) {
+  const int n = mqct_count_states_identical(n_channels, j1, ka1, kc1, j2, ka2, kc2);
+  if (n < 0) return n;
+  if (!indx_chann || !j12 || !m12 || !parity) return MQCT_E_ARG;
+  int st = 0;
+  for (int c = 0; c < n_channels; ++c) {
+    const bool same = same_level(c, j1, ka1, kc1, j2, ka2, kc2);
+    for (int p = 1; p <= (same ? 1 : 2); ++p)
+      for (int js = abs(j1[c] - j2[c]); js <= j1[c] + j2[c]; ++js)
+        for (int m = -js; m <= js; ++m) {
+          indx_chann[st] = c + 1;
+          j12[st] = js;
+          m12[st] = m;
+          parity[st] = (same && (js & 1)) ? -1 : (p == 1 ? 1 : -1);
+          ++st;
+        }
+  }
+  return st;
+}
+int64_t mqct_count_pairs_identical(int32_t n, const int32_t* m12, const int32_t* parity) {
+  if (n <= 0 || !m12 || !parity) return MQCT_E_ARG;
+  int64_t p = 0;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (m12[a] == m12[b] && parity[a] == parity[b]) ++p;
+  return p;
+}
+int64_t mqct_fill_ind_mat_identical(int32_t n, const int32_t* m12, const int32_t* parity,
+                                    int32_t* ind) {
+  if (n <= 0 || !m12 || !parity || !ind) return MQCT_E_ARG;
+  int64_t p = 0;
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (m12[a] == m12[b] && parity[a] == parity[b]) {
+        ind[2 * p] = a + 1;
+        ind[2 * p + 1] = b + 1;
+        ++p;
+      }
+  return p;
+}
+
 // ind_mat: st1 outer, st2 <= st1, equal m12 (MQCT_SOURCE_CODES/matrix_ini.f:553-627).
 int64_t mqct_count_pairs(int32_t n, const int32_t* m12) {
   if (n <= 0 || !m12) return MQCT_E_ARG;
@@ -445,13 +507,13 @@ static const char* const* mtrx_dat_columns(int coll_type, int* n) {
   static const char* c7[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K", "EPS", "J2"};
   static const char* c8[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K1A", "K1C", "J2"};
   static const char* c0[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "KA1", "KC1",
-                             "J2", "KA2", "KC2"};
+                             "J2", "KA2", "KC2", "P"};
   switch (coll_type) {
     case 1: *n = 5; return c1;
     case 4: *n = 7; return c4;
     case 7: *n = 8; return c7;
     case 8: *n = 8; return c8;
-    case 0: *n = 10; return c0;
+    case 0: *n = 10; return c0;  // 11 with the exchange parity of identical partners
     default: *n = 0; return nullptr;
   }
 }
@@ -466,6 +528,7 @@ int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
                  coll_type);
   MQCT_ARG_CHECK(path && state_rec && ind_mat && R && mat && P > 0 && nR > 1 && n_states > 0,
                  "mqct_write_mtrx_dat: bad arguments");
+  if (coll_type == 0 && state_rec_len == 11) ncol = 11;  // identical partners: P column
   MQCT_ARG_CHECK(state_rec_len == ncol, "SYS_TYPE %d state records have %d columns (got %d)",
                  coll_type, ncol, state_rec_len);
   FILE* f = fopen(path, "w");
@@ -478,11 +541,12 @@ int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
   fprintf(f, "NUMBER_OF_STATES= %6d\n", n_states);
   fprintf(f, "MATRIX_SIZE= %9lld\n", (long long)P);
   fprintf(f, "R_GRID_SIZE= %4d\n", nR);
-  for (int c = 0; c < ncol; ++c) fprintf(f, c ? " %8s" : "%8s", cols[c]);
+  // the P column of identical partners is a2 / i2 (matrix_ini.f:4846-4857)
+  for (int c = 0; c < ncol; ++c) fprintf(f, c == 0 ? "%8s" : (c == 10 ? " %2s" : " %8s"), cols[c]);
   fputc('\n', f);
   for (int st = 0; st < n_states; ++st) {
     for (int c = 0; c < ncol; ++c)
-      fprintf(f, c ? " %8d" : "%8d", state_rec[(size_t)st * ncol + c]);
+      fprintf(f, c == 0 ? "%8d" : (c == 10 ? " %2d" : " %8d"), state_rec[(size_t)st * ncol + c]);
     fputc('\n', f);
   }
   fprintf(f, "%16s %8s %8s\n", "MIJ_INDEX", "ST_1", "ST_2");

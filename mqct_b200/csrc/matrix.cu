@@ -1397,6 +1397,116 @@ __global__ void expansion_m3_kernel(int64_t P, int n_u, const int* __restrict__ 
   M3[idx] = m3;
 }
 
+// Identical partners (IDENTICAL = YES with IDENTICAL_PES = YES, SYS_TYPE 0;
+// MQCT_SOURCE_CODES/pot_comp.f:8257-8746): A[k * n_terms + t] with the four symmetry
+// branches -- sym1 direct, sym2 l1 <-> l2 (unless l1 = l2 and |nju1| = |nju2|), sym3 and
+// sym4 the same with the molecules exchanged, weighted by par' bk', bk' = (-1)^j12'
+// p_inv kappa of the channel ((-1)^j12' for a diagonal pair of a same-level channel) --
+// summed over m' (|m'| <= j1' direct, |m'| <= j2' exchanged: the reference's own output
+// for this case) and m_e, times sqrt((2j1''+1)/(2j1'+1)) sqrt((2j2''+1)/(2j2'+1)) and
+// 1/sqrt(1 + d_p) sqrt(1 + d_pp) (d_p = 1 for a same-level channel with j1' = j2').
+// One thread per (pair, term).
+__global__ void expansion_identical_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
+                                           const int* __restrict__ st_chan,
+                                           const int* __restrict__ st_j12,
+                                           const int* __restrict__ st_m,
+                                           const int* __restrict__ st_par,
+                                           const int* __restrict__ ch_j1,
+                                           const int* __restrict__ ch_j2,
+                                           const int* __restrict__ ch_pk,
+                                           const int* __restrict__ ch_same,
+                                           const double* __restrict__ vec1,
+                                           const double* __restrict__ vec2, int ldv,
+                                           const int* __restrict__ lab5, double* __restrict__ A) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * n_terms) return;
+  const int64_t k = idx / n_terms;
+  const int t = (int)(idx % n_terms);
+  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int j1p = ch_j1[cp], j2p = ch_j2[cp], j1pp = ch_j1[cpp], j2pp = ch_j2[cpp];
+  const int j12p = st_j12[sp], j12pp = st_j12[spp], m = st_m[sp];
+  const int l1 = lab5[5 * t], nju1 = lab5[5 * t + 1], l2 = lab5[5 * t + 2],
+            nju2 = lab5[5 * t + 3], l = lab5[5 * t + 4];
+  double a = 0.0;
+  const bool swap_ok = !(l1 == l2 && abs(nju1) == abs(nju2));
+  const bool s1 = triangle_ok(j1pp, l1, j1p) && triangle_ok(j2pp, l2, j2p);
+  const bool s2 = swap_ok && triangle_ok(j1pp, l2, j1p) && triangle_ok(j2pp, l1, j2p);
+  const bool s3 = triangle_ok(j1pp, l1, j2p) && triangle_ok(j2pp, l2, j1p);
+  const bool s4 = swap_ok && triangle_ok(j1pp, l2, j2p) && triangle_ok(j2pp, l1, j1p);
+  if (triangle_ok(l1, l2, l) && (s1 || s2 || s3 || s4)) {
+    const double* v1p = vec1 + (size_t)cp * ldv;
+    const double* v1pp = vec1 + (size_t)cpp * ldv;
+    const double* v2p = vec2 + (size_t)cp * ldv;
+    const double* v2pp = vec2 + (size_t)cpp * ldv;
+    const double par_p = st_par[sp];
+    const double bk_par1 = ((j12p & 1) ? -1.0 : 1.0) * ((sp == spp && ch_same[cp]) ? 1 : ch_pk[cp]);
+    const double coef3 = sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (8.0 * kPi * kPi);
+    const int n_planar = (nju1 == 0 && nju2 == 0) ? 1 : 2;
+    double k1 = 0.0, k2 = 0.0, k3 = 0.0, k4 = 0.0;
+    for (int planar = 0; planar < n_planar; ++planar) {
+      const int n1 = planar ? -nju1 : nju1, n2 = planar ? -nju2 : nju2;
+      const double sg = planar ? (((l1 + l2 + l + nju1 + nju2) & 1) ? -1.0 : 1.0) : 1.0;
+      const double sx = ((l1 + l2) & 1) ? -1.0 : 1.0;
+      if (s1) k1 += rotor_sum(j1pp, l1, j1p, n1, v1p, v1pp) * rotor_sum(j2pp, l2, j2p, n2, v2p, v2pp) * sg;
+      if (s2)
+        k2 += rotor_sum(j1pp, l2, j1p, n2, v1p, v1pp) * rotor_sum(j2pp, l1, j2p, n1, v2p, v2pp) * (sg * sx);
+      if (s3)
+        k3 += rotor_sum(j1pp, l1, j2p, n1, v2p, v1pp) * rotor_sum(j2pp, l2, j1p, n2, v1p, v2pp) * sg *
+              par_p * bk_par1;
+      if (s4)
+        k4 += rotor_sum(j1pp, l2, j2p, n2, v2p, v1pp) * rotor_sum(j2pp, l1, j1p, n1, v1p, v2pp) *
+              (sg * sx) * par_p * bk_par1;
+    }
+    double m5 = 0.0;
+    const int mx = l1 < l2 ? l1 : l2;
+    const int jm = j1p > j2p ? j1p : j2p;
+    for (int mp = -jm; mp <= jm; ++mp) {
+      if (abs(m - mp) > j1p && abs(m - mp) > j2p) continue;
+      const double cg_p = cg_dev(j1p, mp, j2p, m - mp, j12p, m);
+      const double cg_x = cg_dev(j2p, mp, j1p, m - mp, j12p, m);
+      double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+      for (int me = -mx; me <= mx; ++me) {
+        const int mpp = mp - me;
+        if (abs(mpp) > j1pp || abs(m - mpp) > j2pp) continue;
+        const double c0 = cg_dev(l1, me, l2, -me, l, 0) * cg_dev(j1pp, mpp, j2pp, m - mpp, j12pp, m);
+        if (abs(mp) <= j1p) {
+          if (s1) a1 += c0 * cg_dev(j1pp, mpp, l1, me, j1p, mp) * cg_dev(j2pp, m - mpp, l2, -me, j2p, m - mp);
+          if (s2) a2 += c0 * cg_dev(j1pp, mpp, l2, me, j1p, mp) * cg_dev(j2pp, m - mpp, l1, -me, j2p, m - mp);
+        }
+        if (abs(mp) <= j2p) {
+          if (s3) a3 += c0 * cg_dev(j1pp, mpp, l1, me, j2p, mp) * cg_dev(j2pp, m - mpp, l2, -me, j1p, m - mp);
+          if (s4) a4 += c0 * cg_dev(j1pp, mpp, l2, me, j2p, mp) * cg_dev(j2pp, m - mpp, l1, -me, j1p, m - mp);
+        }
+      }
+      if (s1) m5 += a1 * cg_p * k1;
+      if (s2) m5 += a2 * cg_p * k2;
+      if (s3) m5 += a3 * cg_x * k3;
+      if (s4) m5 += a4 * cg_x * k4;
+    }
+    const double dp = (j1p == j2p && ch_same[cp]) ? 1.0 : 0.0;
+    const double dpp = (j1pp == j2pp && ch_same[cpp]) ? 1.0 : 0.0;
+    a = coef3 * m5 * sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
+        sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0)) / sqrt(1.0 + dp) / sqrt(1.0 + dpp);
+  }
+  A[idx] = a;
+}
+
+// M[k * nR + i] = sum_t A[k * n_terms + t] T[t * nR + i] from stored coefficients.
+__global__ void __launch_bounds__(128)
+expansion_contract_a_kernel(int n_terms, int nR, const double* __restrict__ A,
+                            const double* __restrict__ T, double* __restrict__ M) {
+  extern __shared__ double ex_a[];
+  const int64_t k = blockIdx.x;
+  for (int t = threadIdx.x; t < n_terms; t += blockDim.x) ex_a[t] = A[k * n_terms + t];
+  __syncthreads();
+  for (int i = threadIdx.x; i < nR; i += blockDim.x) {
+    double s = 0.0;
+    for (int t = 0; t < n_terms; ++t) s = fma(ex_a[t], T[(size_t)t * nR + i], s);
+    M[k * nR + i] = s;
+  }
+}
+
 // Clebsch-Gordan tables for expansion_m3_table_kernel, filled by cg_dev (the same
 // values the direct kernel computes):
 //   rotor-l table  G(ja, jc, lb, ma, mb) = <ja ma lb mb|jc ma+mb>, ja, jc <= Ja, lb <= Lb,
@@ -1529,8 +1639,9 @@ struct ExpansionPlan {
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_ch = 0, n_u = 0;
+  bool identical = false;  // coefficients stored whole in d_A (identical partners)
   DevBuf<int> d_k2r, d_ind, d_chan, d_j1, d_j2, d_term_u;
-  DevBuf<double> d_K, d_M3, d_fac, d_M, d_gc;
+  DevBuf<double> d_K, d_M3, d_fac, d_M, d_gc, d_A;
 
   ~ExpansionPlan() {
     for (auto& e : ev)
@@ -1572,6 +1683,18 @@ struct ExpansionPlan {
       int* o = &lab5[5 * (size_t)t];
       o[0] = l1; o[1] = nju1; o[2] = l2; o[3] = nju2; o[4] = l;
     }
+    const bool ident = sys->parity != nullptr;
+    if (ident) {
+      MQCT_ARG_CHECK(type == 0 && sys->ka1 && sys->kc1 && sys->ka2 && sys->kc2,
+                     "identical partners need SYS_TYPE 0 with ka1, kc1, ka2, kc2");
+      // the reference's checks of an identical-partner term list (pot_comp.f:8303-8318)
+      for (int t = 0; t < n_terms; ++t) {
+        const int* o = &lab5[5 * (size_t)t];
+        MQCT_ARG_CHECK(o[0] >= o[2] && !(o[0] == o[2] && abs(o[1]) < abs(o[3])),
+                       "identical partners: term %d needs l1 >= l2 and, for l1 = l2, "
+                       "|nju1| >= |nju2|", t + 1);
+      }
+    }
     const int n_states = sys->n_states, n_ch = sys->n_channels;
     std::vector<int> st_chan(n_states);
     int j1max = 0, j2max = 0;
@@ -1593,6 +1716,9 @@ struct ExpansionPlan {
     for (int s = 0; s < n_states; ++s) {
       st_chan[s] = sys->indx_chann[s] - 1;
       MQCT_ARG_CHECK(st_chan[s] >= 0 && st_chan[s] < n_ch, "indx_chann out of range");
+      if (ident)
+        MQCT_ARG_CHECK(sys->parity[s] == 1 || sys->parity[s] == -1, "parity of state %d must be +-1",
+                       s + 1);
       const int ch = st_chan[s];
       MQCT_ARG_CHECK(sys->j12[s] >= abs(sys->j1[ch] - sys->j2[ch]) &&
                          sys->j12[s] <= sys->j1[ch] + sys->j2[ch] && abs(sys->m12[s]) <= sys->j12[s],
@@ -1603,6 +1729,9 @@ struct ExpansionPlan {
       MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states, "ind_mat out of range");
       MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
                      (long long)k + 1);
+      if (ident)
+        MQCT_ARG_CHECK(sys->parity[a] == sys->parity[b], "pair with different parity at k=%lld",
+                       (long long)k + 1);
     }
     // rotor 1 of SYS_TYPE 7: the parity-adapted symmetric top
     // (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) as a vector over K; with it
@@ -1676,12 +1805,49 @@ struct ExpansionPlan {
     std::vector<int> k2r(P);
     for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
     MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
-    MQCT_CUDA_TRY(d_K.alloc((size_t)n_ch * n_ch * n_terms));
-    MQCT_CUDA_TRY(d_M3.alloc((size_t)P * n_u));
     MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
+    if (!ident) {
+      MQCT_CUDA_TRY(d_K.alloc((size_t)n_ch * n_ch * n_terms));
+      MQCT_CUDA_TRY(d_M3.alloc((size_t)P * n_u));
+    }
     ir1 = nearest_index(Rh, r_cut1);
     ir2 = nearest_index(Rh, r_cut2);
     cut_hartree = mij_cutoff_cm * kCmToHartree;
+    if (ident) {
+      // per channel: p_inv kappa (pot_comp.f:70-110, matrix_ini.f:9147-9190) and whether the
+      // two rotors are in the same level
+      identical = true;
+      std::vector<int> pk(n_ch), same(n_ch);
+      for (int c = 0; c < n_ch; ++c) {
+        int par[2] = {1, 1};
+        const double* v[2] = {sys->vec1 + (size_t)c * ldv1, sys->vec2 + (size_t)c * ldv2};
+        const int jj[2] = {sys->j1[c], sys->j2[c]};
+        for (int r = 0; r < 2; ++r)
+          for (int i = 0; i <= jj[r]; ++i) {
+            const double d = v[r][i] * v[r][2 * jj[r] - i];
+            if (d == 0.0) continue;
+            par[r] = d > 0.0 ? 1 : -1;
+            break;
+          }
+        const int k1 = abs(sys->ka1[c] - sys->kc1[c]) % 2, k2 = abs(sys->ka2[c] - sys->kc2[c]) % 2;
+        pk[c] = par[0] * par[1] * (((k1 + k2) % 2) ? -1 : 1);
+        same[c] = sys->j1[c] == sys->j2[c] && sys->ka1[c] == sys->ka2[c] && sys->kc1[c] == sys->kc2[c];
+      }
+      DevBuf<int> d_par, d_pk, d_same;
+      MQCT_CUDA_TRY(d_par.upload(sys->parity, n_states, st));
+      MQCT_CUDA_TRY(d_pk.upload(pk, st));
+      MQCT_CUDA_TRY(d_same.upload(same, st));
+      MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
+      const int64_t n_at = P * n_terms;
+      MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
+      expansion_identical_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
+          P, n_terms, d_ind.p, d_chan.p, d_j12.p, d_m.p, d_par.p, d_j1.p, d_j2.p, d_pk.p, d_same.p,
+          d_vec1.p, d_vec2.p, ldv1, d_lab.p, d_A.p);
+      MQCT_CUDA_TRY(cudaGetLastError());
+      MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
+      MQCT_CUDA_TRY(cudaStreamSynchronize(st));
+      return MQCT_OK;
+    }
     const int64_t n_k = (int64_t)n_ch * n_ch * n_terms, n_m3 = P * n_u;
     // table sizes from the actual j and l ranges
     int L1 = 0, L2 = 0, Lm = 0;
@@ -1731,9 +1897,13 @@ struct ExpansionPlan {
     MQCT_ARG_CHECK(d_terms && d_mat && d_sk, "null argument");
     MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], st));
-    expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
-        n_ch, n_terms, n_u, nR, d_ind.p, d_chan.p, d_j1.p, d_j2.p, d_K.p, d_M3.p, d_fac.p,
-        d_term_u.p, d_terms, d_M.p);
+    if (identical)
+      expansion_contract_a_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
+          n_terms, nR, d_A.p, d_terms, d_M.p);
+    else
+      expansion_contract_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
+          n_ch, n_terms, n_u, nR, d_ind.p, d_chan.p, d_j1.p, d_j2.p, d_K.p, d_M3.p, d_fac.p,
+          d_term_u.p, d_terms, d_M.p);
     MQCT_CUDA_TRY(cudaGetLastError());
     finalize_kernel<double><<<(unsigned)P, 128, sizeof(double) * 2 * (size_t)nR, st>>>(
         P, nR, d_k2r.p, d_M.p, 1, 0, nR, e_unit, nullptr, ir1, ir2, cut_hartree, d_gc.p, d_mat,

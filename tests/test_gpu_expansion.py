@@ -122,3 +122,25 @@ def test_expansion_high_j_direct_path(mq, oracle, gpu_available):
     # the two evaluations (log-factorial exponentials here, the oracle's 3j routine there)
     # lose different ones: 6e-12 of the largest element
     assert np.max(np.abs(m - mo)) <= 1e-10 * np.abs(mo).max()
+
+
+def test_identical_expansion_matches_reference_and_oracle(mq, oracle, gpu_available):
+    from test_oracle_expansion import identical_gauge
+    g = np.load(os.path.join(GOLD, "g5c_h2o_h2o_identical.npz"))
+    s = mq.CollisionSystem(0, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           identical=True)
+    m, y2, sk = mq.build_matrix_expansion(s, g["R"], g["labels"], g["terms"], e_unit="KCAL",
+                                          mij_cutoff=0.0)
+    gauge, err = identical_gauge(s, m, g["mat"])
+    assert err <= 1e-10
+    ch = s.channels
+    osys = oracle.OracleSystem(0, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], ch[:, 4], ch[:, 5],
+                               e_ch=s.e_ch, vec1=s.vec1.reshape(-1), vec2=s.vec2.reshape(-1),
+                               ldv=s.ldv)
+    mo = oracle.expansion_matrix_type0_identical(osys, (s.indx_chann, s.j12, s.m12, None),
+                                                s.parity, s.ind_mat,
+                                                 g["labels"], g["terms"], mq.E_UNIT["KCAL"])
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+    # the term-list rule of identical partners (l1 >= l2) is enforced
+    with pytest.raises(mq.MqctError):
+        mq.build_matrix_expansion(s, g["R"], [[0, 0, 1, 0, 1]], np.zeros((2, 1)), e_unit="KCAL")

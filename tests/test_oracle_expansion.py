@@ -107,3 +107,73 @@ def test_type7_equals_type8_form_with_parity_adapted_vector(mq, oracle):
     # the type-8 restatement works in cm^-1 and converts to Hartree itself
     m8 = oracle.expansion_matrix_type8(o8, o8.states(), s.ind_mat, g["labels"], g["terms"])
     assert np.max(np.abs(m8 / mq.E_UNIT["CM-1"] - m7)) <= 1e-12 * np.abs(m7).max()
+
+
+def _g5c():
+    return np.load(os.path.join(GOLD, "g5c_h2o_h2o_identical.npz"))
+
+
+def identical_gauge(system, mat, ref):
+    """Per-pair sign from one sign per rotor level (the eigenvector phase, LAPACK's in the
+    reference, a fixed rule here), found over all level-sign choices; returns (gauge,
+    max deviation relative to the largest element)."""
+    import itertools
+    ch = system.channels
+    levels = sorted({tuple(c[:3]) for c in ch} | {tuple(c[3:]) for c in ch})
+    ic, ind = system.indx_chann, system.ind_mat
+    best = None
+    for signs in itertools.product((1, -1), repeat=len(levels)):
+        sg = dict(zip(levels, signs))
+        cs = np.array([sg[tuple(c[:3])] * sg[tuple(c[3:])] for c in ch])
+        gauge = cs[ic[ind[:, 0] - 1] - 1] * cs[ic[ind[:, 1] - 1] - 1]
+        e = np.max(np.abs(mat - gauge[:, None] * ref)) / np.abs(ref).max()
+        if best is None or e < best[1]:
+            best = (gauge, e)
+    return best
+
+
+def test_identical_states_and_pairs(mq):
+    """IDENTICAL = YES: the 81 parity-adapted states (with their exchange parity) and the
+    322 equal-parity pairs of the reference's H2O + H2O MTRX.DAT."""
+    g = _g5c()
+    s = mq.CollisionSystem(0, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           identical=True)
+    st = g["states"]
+    assert s.n_states == 81 and s.P == 322
+    assert np.array_equal(s.state_records(), st)
+    assert np.array_equal(s.ind_mat, g["ind_mat"])
+
+
+def test_identical_expansion_reproduces_reference_matrix(mq, oracle):
+    g = _g5c()
+    s = mq.CollisionSystem(0, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           identical=True)
+    ch = s.channels
+    osys = oracle.OracleSystem(0, ch[:, 0], ch[:, 1], ch[:, 2], ch[:, 3], ch[:, 4], ch[:, 5],
+                               e_ch=s.e_ch, vec1=s.vec1.reshape(-1), vec2=s.vec2.reshape(-1),
+                               ldv=s.ldv)
+    m = oracle.expansion_matrix_type0_identical(osys, (s.indx_chann, s.j12, s.m12, None),
+                                                s.parity, s.ind_mat,
+                                                g["labels"], g["terms"], mq.E_UNIT["KCAL"])
+    gauge, err = identical_gauge(s, m, g["mat"])
+    assert (gauge < 0).any()   # LAPACK's phases differ from the fixed rule for some levels
+    assert err <= 1e-10
+
+
+def test_identical_mtrx_dat_layout(mq, tmp_path):
+    g = _g5c()
+    s = mq.CollisionSystem(0, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           identical=True)
+    path = str(tmp_path / "MTRX.DAT")
+    mq.write_mtrx_dat(path, s, g["R"], g["mat"])
+    lines = open(path).read().splitlines()
+    # lines of EXAMPLES_IO/SYS_TYPE_0/H2O_H2O_Identical/MTRX.DAT
+    assert lines[:7] == ["COLLISION_TYPE= 0", "NUMBER_OF_CHANLS=    6",
+                         "NUMBER_OF_STATES=     81", "MATRIX_SIZE=       322",
+                         "R_GRID_SIZE=    2",
+                         "  #STATE #CHANNEL      J12      M12       J1      KA1      KC1       J2"
+                         "      KA2      KC2  P",
+                         "       1        1        0        0        0        0        0        0"
+                         "        0        0  1"]
+    d = mq.read_mtrx_dat(path)
+    assert np.array_equal(d["states"], g["states"]) and np.array_equal(d["mat"], g["mat"])
