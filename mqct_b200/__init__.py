@@ -28,6 +28,7 @@ __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables",
            "cross_sections_device", "write_mtrx_uf",
            "read_mtrx_uf", "write_mtrx_dat", "read_mtrx_dat", "read_expansion_terms",
            "spline_y2", "Surrogate", "build_matrix_expansion", "ExpansionPlan", "E_UNIT",
+           "expansion_terms_list", "write_expansion_terms_list",
            "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
            "MODE_AT"]
@@ -295,6 +296,36 @@ def build_matrix(system: CollisionSystem, R, grid, pes, precision=PREC_FP64, mij
 # MQCT_SOURCE_CODES/matrix_ini.f:918-921 with the constants of iotest.f:20-24)
 E_UNIT = {"CM-1": CM_TO_HARTREE, "KCAL": 1.0 / 627.509469, "K": 1.0 / 1.1604519e4 / 27.21113845,
           "AU": 1.0}
+
+
+def expansion_terms_list(sys_type, l1_max, l2_max, l1_min=0, l2_min=0, nju1_max=-1, l_max=-1,
+                         axl_sym1=1, equ_sym1=1, equ_sym2=1, odd_l1l2l=False):
+    """The term list CALC_EXPANSION generates for SYS_TYPE 7, 8 and 9 from the $POTENTIAL
+    keywords L1_MIN/L1_MAX, L2_MIN/L2_MAX, M1_MAX (nju1_max), L_MAX, AXL_SYM1, EQU_SYM1,
+    EQU_SYM2 and ODD_L1L2L (MQCT_SOURCE_CODES/pot_comp.f:4237-4262, 4314-4339): l1 in steps
+    of EQU_SYM1, nju1 = 0..min(l1, M1_MAX) in steps of AXL_SYM1, l2 in steps of EQU_SYM2,
+    l = |l1-l2|..min(l1+l2, L_MAX), without odd l1+l2+l unless ODD_L1L2L.  Returns an
+    (n, 4) array of (l1, nju1, l2, l), the rows of EXPANSION_TERMS_LIST.DAT."""
+    if sys_type not in (7, 8, 9):
+        raise ValueError("term lists are generated here for SYS_TYPE 7, 8 and 9")
+    nju1_max = l1_max if nju1_max < 0 else nju1_max
+    l_max = l1_max + l2_max if l_max < 0 else l_max
+    out = []
+    for l1 in range(l1_min, l1_max + 1, equ_sym1):
+        for nju1 in range(0, min(l1, nju1_max) + 1, axl_sym1):
+            for l2 in range(l2_min, l2_max + 1, equ_sym2):
+                for l in range(abs(l1 - l2), min(l1 + l2, l_max) + 1):
+                    if not odd_l1l2l and (l1 + l2 + l) % 2:
+                        continue
+                    out.append((l1, nju1, l2, l))
+    return np.array(out, dtype=np.int32).reshape(-1, 4)
+
+
+def write_expansion_terms_list(path, labels):
+    """EXPANSION_TERMS_LIST.DAT: one term per line, 'l1,nju1,l2,l,' (pot_comp.f:4250)."""
+    with open(path, "w") as f:
+        for row in np.asarray(labels, np.int32):
+            f.write("".join(f"{int(v)}," for v in row) + "\n")
 
 
 def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",

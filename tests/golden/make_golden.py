@@ -133,6 +133,18 @@ def main(ref_root):
                            [1, 1, 1, 1, 1, 1], [1, 1, 1, 2, 0, 2], [2, 0, 2, 2, 0, 2]],
                           dtype=np.int32))
 
+    # G6: the term lists CALC_EXPANSION generated from the $POTENTIAL limits
+    # (EXPANSION_TERMS_LIST.DAT of EXAMPLES_IO/SYS_TYPE_8/H2O_H2_GeneratingTerms:
+    # L1 0-4, L2 0-4, M1_MAX 4, AXL_SYM1 2, EQU_SYM2 2, ODD_L1L2L YES; and of
+    # EXAMPLES_IO/SYS_TYPE_7/NH3_H2_Generation_of_Terms: L1 0-4, L2 0-2, M1_MAX 3).
+    lists = {}
+    for key, sub in (("h2o_h2_type8", ("SYS_TYPE_8", "H2O_H2_GeneratingTerms")),
+                     ("nh3_h2_type7", ("SYS_TYPE_7", "NH3_H2_Generation_of_Terms"))):
+        txt = open(os.path.join(ex, *sub, "EXPANSION_TERMS_LIST.DAT")).read().split()
+        lists[key] = np.array([[int(x) for x in t.strip(",").split(",")] for t in txt],
+                              dtype=np.int32)
+    np.savez_compressed(os.path.join(out, "g6_expansion_term_lists.npz"), **lists)
+
     # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)

@@ -99,3 +99,17 @@ def test_malformed_mtrx_dat_is_rejected(mq, tmp_path):
     open(bad, "w").write("\n".join(["NUMBER_OF_CHANLS=   10"] + lines[1:]) + "\n")
     with pytest.raises(mq.MqctError):
         mq.read_mtrx_dat(bad)
+
+
+def test_expansion_term_lists_match_the_reference(mq, tmp_path):
+    """CALC_EXPANSION's term lists for the two generating examples, and the file layout."""
+    g = np.load(os.path.join(GOLD, "g6_expansion_term_lists.npz"))
+    t8 = mq.expansion_terms_list(8, 4, 4, nju1_max=4, axl_sym1=2, equ_sym2=2, odd_l1l2l=True)
+    assert np.array_equal(t8, g["h2o_h2_type8"])
+    t7 = mq.expansion_terms_list(7, 4, 2, nju1_max=3)
+    assert np.array_equal(t7, g["nh3_h2_type7"])
+    path = str(tmp_path / "EXPANSION_TERMS_LIST.DAT")
+    mq.write_expansion_terms_list(path, t7)
+    lines = open(path).read().splitlines()
+    assert lines[:2] == ["0,0,0,0,", "0,0,1,1,"] and lines[-1] == "4,3,2,6,"
+    assert len(lines) == 79
