@@ -267,6 +267,7 @@ def run_gpu(a):
             dist.destroy_process_group()
         return
     expansion = None if a.no_expansion else run_expansion(mq, syn)
+    projection = None if a.no_expansion else run_projection(mq, peaks)
     cpu = cpu_baseline_matrix(s, R, c2, a.cpu_seconds)
     tc = prec in (mq.PREC_BF16X3, mq.PREC_F16X3)
     tc_name = "F16x3" if prec == mq.PREC_F16X3 else "BF16x3"
@@ -314,6 +315,7 @@ def run_gpu(a):
         "reference_2d_form": ref_form,
         "propagation": prop,
         "expansion": expansion,
+        "projection": projection,
         "wall_s": wall,
     }
     print(json.dumps(line), flush=True)
@@ -511,6 +513,78 @@ def run_expansion(mq, syn):
                     "reference_log_single_rank_s": ref_s,
                     "speedup_vs_reference_log": (ref_s / (ms / 1e3)) if ref_s else None}
     return out
+
+
+def run_projection(mq, peaks):
+    """CALC_EXPANSION_TERMS at the size of the reference's CALC_EXPANSION example for
+    ND3+D2 (EXAMPLES_IO/SYS_TYPE_7/NH3_H2_CalcExpansion: 377 terms, GRD_R = 86,
+    GRD_ANG1 = 40,40 (alpha2 40), GRD_ANG2 = 20,20 (beta1, beta2 20), GRD_ANG3 = 40,40
+    (gamma1 40)), on a seeded PES table of that shape (the example's PES is a user
+    Fortran routine).  Device times of the three contractions with V resident (V larger
+    than L2, so every execute reads it from HBM), the end-to-end one-shot call on host
+    buffers (V up, terms and terms_im down), and the oracle restatement on a bounded
+    sample of (term, R) pairs, scaled to the full workload."""
+    import torch
+
+    from oracle import pyoracle as po
+    labels = np.load(os.path.join(GOLDEN, "g5b_nd3_d2_type7.npz"))["labels"]
+    shape = (40, 20, 20, 40)
+    nR = 86
+    rng = np.random.default_rng(7)
+    V = (rng.standard_normal((nR,) + shape) * 500.0).astype(np.float64)
+    G = int(np.prod(shape))
+    nt = len(labels)
+    pp = mq.ProjectionPlan(7, labels, shape)
+    dV = torch.from_numpy(V).cuda()
+    dT = torch.empty((nt, nR), dtype=torch.float64, device="cuda")
+    dI = torch.empty_like(dT)
+    torch.cuda.synchronize()
+    seg = []
+    for i in range(8):
+        pp.execute(dV, nR, dT, dI)
+        pp.sync()
+        seg.append(pp.timing())
+    seg = np.array(seg[3:])
+    ga, al, te = (float(np.median(seg[:, k])) for k in range(3))
+    pp.close()
+    del dV, dT, dI
+    n_out = nt * nR
+    # end to end: host V (pinned) in, both term arrays out; plan set-up inside the time
+    Vp = torch.from_numpy(V).pin_memory()
+    Vh = Vp.numpy()
+    e2e = []
+    for i in range(6):
+        t0 = time.perf_counter()
+        mq.project_terms(7, labels, Vh)
+        e2e.append(time.perf_counter() - t0)
+    e2e_ms = float(np.median(e2e[2:])) * 1e3
+    # the oracle on a sample: 4 terms (one per nju1 and the largest l) at 2 R points
+    pick = [0, int(np.argmax(labels[:, 1] == 3)), int(np.argmax(labels[:, 1] == 6)),
+            int(np.argmax(labels[:, 0] + labels[:, 2]))]
+    t0 = time.perf_counter()
+    po.project_terms(7, labels[pick], V[:2])
+    tc = time.perf_counter() - t0
+    per_pair_s = tc / (len(pick) * 2)
+    # algorithmic HBM bytes of the gamma contraction: V read once, F written once
+    n_pairs = len(set(int(x) for x in labels[:, 1]))
+    f_bytes = nR * shape[0] * shape[1] * shape[2] * n_pairs * 16
+    alg = V.nbytes + f_bytes
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    return {"workload": "ND3+D2 CALC_EXPANSION size (SYS_TYPE 7): 377 terms, 86 R, grid "
+                        "alpha2 40 x beta1 20 x beta2 20 x gamma1 40 (640000 points), "
+                        "seeded PES table",
+            "V_bytes": int(V.nbytes), "terms_per_call": n_out,
+            "device_ms": {"gamma": ga, "alpha2": al, "beta_terms": te, "total": ga + al + te},
+            "terms_per_s_device": n_out / ((ga + al + te) / 1e3),
+            "e2e": {"ms": e2e_ms, "terms_per_s": n_out / (e2e_ms / 1e3),
+                    "h2d_bytes": int(V.nbytes), "d2h_bytes": int(2 * n_out * 8)},
+            "roofline_gamma": {"bound": "hbm", "algorithmic_bytes": int(alg),
+                               "achieved_gbs": alg / (ga / 1e3) / 1e9, "peak_gbs": hbm,
+                               "frac": alg / (ga / 1e3) / 1e9 / hbm},
+            "cpu_port": {"terms_per_s": 1.0 / per_pair_s,
+                         "sample": f"{len(pick)} terms x 2 R (each a sum over the 640000 grid "
+                                   f"points), {os.cpu_count()} OpenMP threads, {tc:.2f} s",
+                         "full_workload_s_estimate": per_pair_s * n_out}}
 
 
 def run_reference(a):

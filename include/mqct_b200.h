@@ -450,6 +450,49 @@ int mqct_read_mtrx_dat(const char* path, int32_t state_rec_len, int32_t* state_r
  * mqct_build_matrix_expansion takes); values in the file's energy unit. */
 int mqct_read_expansion_terms(const char* path, int32_t nR, int32_t n_terms, double* R,
                               double* terms);
+/* The PES_EXPAN_TERMS.DAT writer of CALC_EXPANSION_TERMS
+ * (MQCT_SOURCE_CODES/pot_comp.f:5918-6270), SYS_TYPE 7, 8 and 0: appends R[iR] and
+ * terms[t * nR + iR] to path, the header line first when the file holds at most one
+ * line (runs over consecutive R ranges, IR_BGN / IR_FIN, share one file). */
+int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_terms,
+                               const int32_t* a_top, int32_t nR, const double* R,
+                               const double* terms);
+
+/* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
+ * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 7, 8 and 0: the
+ * quadrature projection of the PES tabulated on the angular grid onto the expansion
+ * terms,
+ *   terms[t * nR + iR]    = sum_g V Re(EXPANSION_TERM_t) w(g)    (intgrlr)
+ *   terms_im[t * nR + iR] = sum_g V Im(EXPANSION_TERM_t) w(g)    (intgrli)
+ * with the weights and grids of INI_POT_STORAGE: grid->n_beta = beta1 and
+ * grid->n_beta2 = beta2 (Gauss-Legendre on [0, pi]); grid->n_alpha2 = alpha2,
+ * grid->n_gamma = gamma1 and, for SYS_TYPE 0, grid->n_gamma2 = gamma2 (on [0, 2 pi],
+ * midpoint-equidistant when eq_gamma, else Gauss-Legendre); grid->n_alpha unused.
+ * V in the reference's V_3_2 / V_TRANSFER order, V[iR][alpha2][beta1][beta2][gamma1]
+ * (SYS_TYPE 7, 8) or V[iR][alpha2][beta1][beta2][gamma1][gamma2] (SYS_TYPE 0), in the
+ * unit the terms are wanted in.  a_top: A_TOP(5, nterms), (l1, nju1, l2, l, -) for 7
+ * and 8, (l1, nju1, l2, nju2, l) for 0, checked as the reference checks a term list
+ * (triangle rule, nju1 >= 0, nju2 >= 0 when nju1 = 0, no term twice up to the sign of
+ * the nju's; with identical != 0, SYS_TYPE 0 only, also l1 >= l2, |nju1| >= |nju2|
+ * when l1 = l2 and no term twice up to the exchange of the partners): MQCT_E_ARG
+ * otherwise.  The plan forms the per-term tables once; _execute projects device V
+ * (d_V) into device d_terms and d_terms_im (may be NULL) on the plan's stream,
+ * asynchronously; _timing gives the device milliseconds of the three contractions
+ * (gamma, alpha2, beta) of the last single-pass execute.  mqct_project_terms is the
+ * one-shot form on host buffers. */
+typedef struct mqct_projection_plan mqct_projection_plan;
+int mqct_projection_plan_create(int32_t sys_type, int32_t n_terms, const int32_t* a_top,
+                                const mqct_grid_t* grid, int32_t identical,
+                                mqct_projection_plan** plan);
+int mqct_projection_plan_execute(mqct_projection_plan* plan, const double* d_V, int32_t nR,
+                                 double* d_terms, double* d_terms_im);
+int mqct_projection_plan_sync(mqct_projection_plan* plan);
+int mqct_projection_plan_timing(mqct_projection_plan* plan, float* ms_gamma, float* ms_alpha,
+                                float* ms_terms);
+void mqct_projection_plan_destroy(mqct_projection_plan* plan);
+int mqct_project_terms(int32_t sys_type, int32_t n_terms, const int32_t* a_top,
+                       const mqct_grid_t* grid, int32_t identical, int32_t nR, const double* V,
+                       double* terms, double* terms_im);
 
 #ifdef __cplusplus
 }

@@ -805,3 +805,91 @@ def read_expansion_terms(path, nR, n_terms):
     T = np.zeros(nR * n_terms)
     check(lib().mqct_read_expansion_terms(path.encode(), nR, n_terms, R, T))
     return R, np.ascontiguousarray(T.reshape(n_terms, nR).T)
+
+
+def write_expansion_terms(path, sys_type, labels, R, terms):
+    """Append R and the terms (nR x n_terms, the rows of the file) to PES_EXPAN_TERMS.DAT
+    as CALC_EXPANSION_TERMS writes it, the header first when the file holds at most one
+    line."""
+    a_top = _a_top(labels)
+    R = np.ascontiguousarray(R, np.float64)
+    T = np.ascontiguousarray(np.asarray(terms, np.float64).reshape(len(R), len(a_top)).T)
+    check(lib().mqct_write_expansion_terms(path.encode(), int(sys_type), len(a_top),
+                                           a_top.reshape(-1), len(R), R, T.reshape(-1)))
+
+
+def _a_top(labels):
+    lab = np.asarray(labels, np.int32)
+    lab = lab.reshape(len(lab), -1)
+    a_top = np.zeros((len(lab), 5), np.int32)  # A_TOP(5, nterms)
+    a_top[:, :lab.shape[1]] = lab
+    return a_top
+
+
+def _projection_grid(V, sys_type, eq_gamma):
+    nR, n2, n3, n4, n5 = V.shape[:5]
+    n6 = V.shape[5] if sys_type == 0 else 0
+    if sys_type == 0 and V.ndim != 6 or sys_type != 0 and V.ndim != 5:
+        raise ValueError("V must be (nR, n_alpha2, n_beta1, n_beta2, n_gamma1[, n_gamma2])")
+    return _abi.Grid(n3, n5, 0, n4, n2, n6, 1 if eq_gamma else 0)
+
+
+def project_terms(sys_type, labels, V, eq_gamma=True, identical=False):
+    """CALC_EXPANSION_TERMS on the GPU: project V, tabulated on the angular grid as
+    (nR, n_alpha2, n_beta1, n_beta2, n_gamma1) for SYS_TYPE 7 and 8 or with a trailing
+    n_gamma2 axis for SYS_TYPE 0, onto the terms (rows (l1, nju1, l2, l) or
+    (l1, nju1, l2, nju2, l)).  Returns (terms, terms_im), nR x n_terms each, the rows of
+    PES_EXPAN_TERMS.DAT in the unit of V."""
+    a_top = _a_top(labels)
+    V = np.ascontiguousarray(V, np.float64)
+    g = _projection_grid(V, sys_type, eq_gamma)
+    nR, nt = V.shape[0], len(a_top)
+    T = np.zeros(nt * nR)
+    Ti = np.zeros(nt * nR)
+    check(lib().mqct_project_terms(int(sys_type), nt, a_top.reshape(-1), C.byref(g),
+                                   1 if identical else 0, nR, V.reshape(-1), T,
+                                   Ti.ctypes.data))
+    return T.reshape(nt, nR).T.copy(), Ti.reshape(nt, nR).T.copy()
+
+
+class ProjectionPlan:
+    """CALC_EXPANSION_TERMS with the per-term tables formed once (mqct_projection_plan_*);
+    execute() projects V on the device into device terms[t * nR + iR] (the layout that
+    ExpansionPlan.execute takes)."""
+
+    def __init__(self, sys_type, labels, grid_shape, eq_gamma=True, identical=False):
+        """grid_shape: (n_alpha2, n_beta1, n_beta2, n_gamma1[, n_gamma2])."""
+        a_top = _a_top(labels)
+        self.n_terms = len(a_top)
+        gs = tuple(grid_shape) + ((0,) if len(grid_shape) == 4 else ())
+        self.grid = _abi.Grid(gs[1], gs[3], 0, gs[2], gs[0], gs[4], 1 if eq_gamma else 0)
+        h = _abi.vp()
+        check(lib().mqct_projection_plan_create(int(sys_type), self.n_terms, a_top.reshape(-1),
+                                                C.byref(self.grid), 1 if identical else 0,
+                                                C.byref(h)))
+        self.h = h
+
+    def execute(self, d_V, nR, d_terms, d_terms_im=None):
+        p = [x.data_ptr() if hasattr(x, "data_ptr") else x for x in (d_V, d_terms, d_terms_im)]
+        check(lib().mqct_projection_plan_execute(self.h, p[0], int(nR), p[1], p[2]))
+
+    def sync(self):
+        check(lib().mqct_projection_plan_sync(self.h))
+
+    def timing(self):
+        """(gamma, alpha2, beta contraction ms) of the last execute, on the device."""
+        a, b, c = C.c_float(), C.c_float(), C.c_float()
+        check(lib().mqct_projection_plan_timing(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return float(a.value), float(b.value), float(c.value)
+
+    def close(self):
+        if self.h:
+            lib().mqct_projection_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -98,7 +98,9 @@ EXPORTS = [
     "mqct_fill_ind_mat", "mqct_count_states_identical", "mqct_enumerate_states_identical",
     "mqct_count_pairs_identical", "mqct_fill_ind_mat_identical", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
     "mqct_read_mtrx_uf", "mqct_write_mtrx_dat", "mqct_read_mtrx_dat_header",
-    "mqct_read_mtrx_dat", "mqct_read_expansion_terms",
+    "mqct_read_mtrx_dat", "mqct_read_expansion_terms", "mqct_write_expansion_terms",
+    "mqct_projection_plan_create", "mqct_projection_plan_execute", "mqct_projection_plan_sync",
+    "mqct_projection_plan_timing", "mqct_projection_plan_destroy", "mqct_project_terms",
 ]
 
 _lib = None
@@ -200,6 +202,17 @@ def lib():
     L.mqct_read_mtrx_dat_header.argtypes = L.mqct_read_mtrx_uf_header.argtypes
     L.mqct_read_mtrx_dat.argtypes = L.mqct_read_mtrx_uf.argtypes
     L.mqct_read_expansion_terms.argtypes = [C.c_char_p, C.c_int32, C.c_int32, f64p, f64p]
+    L.mqct_write_expansion_terms.argtypes = [C.c_char_p, C.c_int32, C.c_int32, i32p, C.c_int32,
+                                             f64p, f64p]
+    L.mqct_projection_plan_create.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(Grid),
+                                              C.c_int32, C.POINTER(vp)]
+    L.mqct_projection_plan_execute.argtypes = [vp, vp, C.c_int32, vp, vp]
+    L.mqct_projection_plan_sync.argtypes = [vp]
+    L.mqct_projection_plan_timing.argtypes = [vp] + [C.POINTER(C.c_float)] * 3
+    L.mqct_projection_plan_destroy.argtypes = [vp]
+    L.mqct_projection_plan_destroy.restype = None
+    L.mqct_project_terms.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(Grid), C.c_int32,
+                                     C.c_int32, f64p, f64p, vp]
     _lib = L
     return L
 

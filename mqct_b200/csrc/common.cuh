@@ -172,4 +172,24 @@ __host__ __device__ inline double plgndr(int l, int m, double x) {
   return pll;
 }
 
+// <j1 m1 j2 m2 | J M> by Racah's closed form from log factorials lf[n] = ln n!
+// (the coefficient of CG, MQCT_SOURCE_CODES/suppl_routines.f:246-252).
+__host__ __device__ inline double clebsch_gordan(int j1, int m1, int j2, int m2, int J, int M,
+                                                 const double* lf) {
+  if (m1 + m2 != M || J < abs(j1 - j2) || J > j1 + j2 || abs(m1) > j1 || abs(m2) > j2 ||
+      abs(M) > J)
+    return 0.0;
+  const double pre = 0.5 * (log(2.0 * J + 1.0) + lf[J + j1 - j2] + lf[J - j1 + j2] +
+                            lf[j1 + j2 - J] - lf[j1 + j2 + J + 1] + lf[J + M] + lf[J - M] +
+                            lf[j1 - m1] + lf[j1 + m1] + lf[j2 - m2] + lf[j2 + m2]);
+  double sum = 0.0;
+  for (int k = 0; k <= j1 + j2 - J; ++k) {
+    const int a = j1 - m1 - k, b = j2 + m2 - k, c = J - j2 + m1 + k, d = J - j1 - m2 + k;
+    if (a < 0 || b < 0 || c < 0 || d < 0) continue;
+    const double t = exp(pre - lf[k] - lf[j1 + j2 - J - k] - lf[a] - lf[b] - lf[c] - lf[d]);
+    sum += (k & 1) ? -t : t;
+  }
+  return sum;
+}
+
 }  // namespace mqct_dev

@@ -727,4 +727,50 @@ int mqct_read_expansion_terms(const char* path, int32_t nR, int32_t n_terms, dou
   return MQCT_OK;
 }
 
+// The writer of CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:5918-6270): appends
+// to the file; the header line ("R_Bohr" then one a19 label v_l1_nju1_l2_l, or
+// v_l1_nju1_l2_nju2_l for SYS_TYPE 0, per term, 3 blanks after each) only when the file
+// holds at most one line, then per R point f6.2, 1x and e19.12 with 3 blanks per term.
+int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_terms,
+                               const int32_t* a_top, int32_t nR, const double* R,
+                               const double* terms) {
+  MQCT_ARG_CHECK(path && a_top && R && terms && nR > 0 && n_terms > 0, "bad arguments");
+  MQCT_ARG_CHECK(sys_type == 7 || sys_type == 8 || sys_type == 0,
+                 "PES_EXPAN_TERMS.DAT is written here for SYS_TYPE 7, 8 and 0");
+  int lines = 0;
+  if (FILE* in = fopen(path, "r")) {
+    std::string line;
+    while (read_line(in, line)) ++lines;
+    fclose(in);
+  }
+  FILE* f = fopen(path, "a");
+  if (!f) {
+    set_error("cannot open %s", path);
+    return MQCT_E_IO;
+  }
+  if (lines <= 1) {
+    for (int t = 0; t < n_terms; ++t) {
+      const int32_t* q = a_top + 5 * t;
+      char lab[96];
+      if (sys_type == 0) snprintf(lab, sizeof lab, "v_%d_%d_%d_%d_%d", q[0], q[1], q[2], q[3], q[4]);
+      else snprintf(lab, sizeof lab, "v_%d_%d_%d_%d", q[0], q[1], q[2], q[3]);
+      lab[19] = 0;  // a19 keeps the leftmost 19 characters
+      if (t == 0) fprintf(f, "%-6s ", "R_Bohr");
+      fprintf(f, "%19s   ", lab);
+    }
+    fprintf(f, "\n");
+  }
+  for (int i = 0; i < nR; ++i) {
+    fprintf(f, "%6.2f ", R[i]);
+    for (int t = 0; t < n_terms; ++t)
+      fprintf(f, "%s   ", fortran_e(terms[(size_t)t * nR + i], 19, 12).c_str());
+    fprintf(f, "\n");
+  }
+  if (fclose(f) != 0) {
+    set_error("write to %s failed", path);
+    return MQCT_E_IO;
+  }
+  return MQCT_OK;
+}
+
 }  // extern "C"

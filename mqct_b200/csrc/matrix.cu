@@ -1282,21 +1282,7 @@ extern "C" int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t*
 
 // <j1 m1 j2 m2 | J M> by Racah's closed form with the log-factorial table.
 __device__ inline double cg_dev(int j1, int m1, int j2, int m2, int J, int M) {
-  if (m1 + m2 != M || J < abs(j1 - j2) || J > j1 + j2 || abs(m1) > j1 || abs(m2) > j2 ||
-      abs(M) > J)
-    return 0.0;
-  const double* lf = c_logfact;
-  const double pre = 0.5 * (log(2.0 * J + 1.0) + lf[J + j1 - j2] + lf[J - j1 + j2] +
-                            lf[j1 + j2 - J] - lf[j1 + j2 + J + 1] + lf[J + M] + lf[J - M] +
-                            lf[j1 - m1] + lf[j1 + m1] + lf[j2 - m2] + lf[j2 + m2]);
-  double sum = 0.0;
-  for (int k = 0; k <= j1 + j2 - J; ++k) {
-    const int a = j1 - m1 - k, b = j2 + m2 - k, c = J - j2 + m1 + k, d = J - j1 - m2 + k;
-    if (a < 0 || b < 0 || c < 0 || d < 0) continue;
-    const double t = exp(pre - lf[k] - lf[j1 + j2 - J - k] - lf[a] - lf[b] - lf[c] - lf[d]);
-    sum += (k & 1) ? -t : t;
-  }
-  return sum;
+  return mqct_dev::clebsch_gordan(j1, m1, j2, m2, J, M, c_logfact);
 }
 
 __device__ inline bool triangle_ok(int a, int b, int c) { return c >= abs(a - b) && c <= a + b; }

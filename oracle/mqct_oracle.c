@@ -1801,3 +1801,129 @@ int orc_expansion_matrix_type0_identical(const orc_system* sys, const int32_t* i
   free(pinv); free(kap); free(same);
   return 0;
 }
+
+/* ---------------------------------------------------------------------- */
+/* EXPANSION_TERM (SRC/pot_comp.f:3739-3896) for SYS_TYPE 7 and 8 (the same function,
+ * :3796-3824) and 0 (:3873-3895): the angular function of a PES expansion term at the
+ * grid angles (beta1, gamma1) of molecule 1 (alpha1 = 0) and (alpha2, beta2, gamma2) of
+ * molecule 2,
+ *   7, 8: sqrt((2l1+1)/4pi) sum_{m=-l2..l2, |m|<=l1} <l1 m l2 -m|l 0>
+ *         Djkm(l1, nju1, m; 0, beta1, gamma1) WF_DIAT_TOP(l2, -m; beta2, alpha2)
+ *   0:    sum_{|m|<=min(l1,l2)} <l1 m l2 -m|l 0> N1 Djkm(l1, nju1, m; 0, beta1, gamma1)
+ *         N2 Djkm(l2, nju2, -m; alpha2, beta2, gamma2),  N = sqrt((2l+1)/8pi^2). */
+void orc_expansion_term(int sys_type, int l, int l1, int l2, int nju1, int nju2, double beta1,
+                        double gamma1, double alpha2, double beta2, double gamma2, double* wfr,
+                        double* wfi) {
+  double wr = 0.0, wi = 0.0;
+  if (sys_type == 0) {
+    const int mm = l1 < l2 ? l1 : l2;
+    for (int m = -mm; m <= mm; ++m) {
+      double dr1, di1, dr2, di2;
+      orc_djkm(l1, nju1, m, 0.0, beta1, gamma1, &dr1, &di1);
+      const double n1 = sqrt((2.0 * l1 + 1.0) / 8.0 / (ORC_PI * ORC_PI));
+      dr1 *= n1;
+      di1 *= n1;
+      orc_djkm(l2, nju2, -m, alpha2, beta2, gamma2, &dr2, &di2);
+      const double n2 = sqrt((2.0 * l2 + 1.0) / 8.0 / (ORC_PI * ORC_PI));
+      dr2 *= n2;
+      di2 *= n2;
+      const double cg = orc_cg(l1, l2, l, m, -m, 0);
+      wr += cg * (dr1 * dr2 - di1 * di2);
+      wi += cg * (dr1 * di2 + dr2 * di1);
+    }
+    *wfr = wr;
+    *wfi = wi;
+    return;
+  }
+  for (int m = -l2; m <= l2; ++m) {
+    if (abs(m) > l1) continue;
+    double dr1, di1, dr2, di2;
+    orc_djkm(l1, nju1, m, 0.0, beta1, gamma1, &dr1, &di1);
+    orc_wf_diat(l2, -m, beta2, alpha2, &dr2, &di2);
+    const double cg = orc_cg(l1, l2, l, m, -m, 0);
+    wr += cg * (dr1 * dr2 - di1 * di2);
+    wi += cg * (dr1 * di2 + dr2 * di1);
+  }
+  const double f = sqrt((2.0 * l1 + 1.0) / 4.0 / ORC_PI);
+  *wfr = wr * f;
+  *wfi = wi * f;
+}
+
+/* CALC_EXPANSION_TERMS (SRC/pot_comp.f:5174-5417 for SYS_TYPE 7 and 8, :5557-5765 for
+ * 0; the grids of INI_POT_STORAGE, :1310-1370 and :1628-1700): the quadrature
+ * projection of V on the angular grid onto each term,
+ *   terms[t * nR + iR] = sum_g V Re(EXPANSION_TERM) wb wg sin(beta1) waa wbb sin(beta2)
+ *                        [wgg] xbl xgl xaal xbbl [xggl 2 pi]   (terms_im: Im)
+ * the bracketed factors for SYS_TYPE 0 only; beta1, beta2 Gauss-Legendre on [0, pi];
+ * alpha2, gamma1, gamma2 on [0, 2 pi] midpoint-equidistant with weight 2/n (eq_gamma) or
+ * Gauss-Legendre.  V[iR][alpha2][beta1][beta2][gamma1][gamma2] (V_3_2 / V_TRANSFER with
+ * gamma2, then gamma1, fastest; n_gamma2 = 1 for SYS_TYPE 7 and 8).  a_top: 5 per term,
+ * (l1, nju1, l2, l, -) for 7 and 8, (l1, nju1, l2, nju2, l) for 0. */
+int orc_project_terms(int sys_type, int n_terms, const int32_t* a_top, int n_alpha2,
+                      int n_beta1, int n_beta2, int n_gamma1, int n_gamma2, int eq_gamma, int nR,
+                      const double* V, double* terms, double* terms_im) {
+  if (sys_type != 0) n_gamma2 = 1;
+  double* xb = (double*)malloc(sizeof(double) * n_beta1);
+  double* wb = (double*)malloc(sizeof(double) * n_beta1);
+  double* xbb = (double*)malloc(sizeof(double) * n_beta2);
+  double* wbb = (double*)malloc(sizeof(double) * n_beta2);
+  double* xg = (double*)malloc(sizeof(double) * n_gamma1);
+  double* wg = (double*)malloc(sizeof(double) * n_gamma1);
+  double* xgg = (double*)malloc(sizeof(double) * n_gamma2);
+  double* wgg = (double*)malloc(sizeof(double) * n_gamma2);
+  double* xaa = (double*)malloc(sizeof(double) * n_alpha2);
+  double* waa = (double*)malloc(sizeof(double) * n_alpha2);
+  orc_gauleg(n_beta1, xb, wb);
+  orc_gauleg(n_beta2, xbb, wbb);
+  const double xbm = 0.5 * ORC_PI, xbl = 0.5 * ORC_PI, xgm = ORC_PI, xgl = ORC_PI;
+  const int nax[3] = {n_gamma1, n_gamma2, n_alpha2};
+  double* ax[3] = {xg, xgg, xaa};
+  double* aw[3] = {wg, wgg, waa};
+  for (int a = 0; a < 3; ++a) {
+    if (eq_gamma) {
+      for (int i = 0; i < nax[a]; ++i) {
+        ax[a][i] = (i + 0.5) * 2.0 * xgl / nax[a];
+        aw[a][i] = 2.0 / nax[a];
+      }
+    } else {
+      orc_gauleg(nax[a], ax[a], aw[a]);
+      for (int i = 0; i < nax[a]; ++i) ax[a][i] = xgm + xgl * ax[a][i];
+    }
+  }
+  if (sys_type != 0) {
+    xgg[0] = 0.0;
+    wgg[0] = 1.0;
+  }
+  const double tail = sys_type == 0 ? xbl * xgl * xgl * xbl * xgl * 2.0 * ORC_PI
+                                    : xbl * xgl * xgl * xbl;
+  const size_t G = (size_t)n_alpha2 * n_beta1 * n_beta2 * n_gamma1 * n_gamma2;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+  for (int t = 0; t < n_terms; ++t)
+    for (int iR = 0; iR < nR; ++iR) {
+      const int32_t* lab = a_top + 5 * t;
+      const int l1 = lab[0], nju1 = lab[1], l2 = lab[2];
+      const int nju2 = sys_type == 0 ? lab[3] : 0, l = sys_type == 0 ? lab[4] : lab[3];
+      const double* v = V + (size_t)iR * G;
+      double ir = 0.0, ii = 0.0;
+      size_t g = 0;
+      for (int i2 = 0; i2 < n_alpha2; ++i2)
+        for (int i3 = 0; i3 < n_beta1; ++i3)
+          for (int i4 = 0; i4 < n_beta2; ++i4)
+            for (int i5 = 0; i5 < n_gamma1; ++i5)
+              for (int i6 = 0; i6 < n_gamma2; ++i6, ++g) {
+                const double beta = xbm + xbl * xb[i3], bbeta = xbm + xbl * xbb[i4];
+                double wfr, wfi;
+                orc_expansion_term(sys_type, l, l1, l2, nju1, nju2, beta, xg[i5], xaa[i2], bbeta,
+                                   xgg[i6], &wfr, &wfi);
+                const double w = wb[i3] * wg[i5] * sin(beta) * waa[i2] * wbb[i4] * wgg[i6] *
+                                 sin(bbeta);
+                ir += v[g] * wfr * w * tail;
+                ii += v[g] * wfi * w * tail;
+              }
+      terms[(size_t)t * nR + iR] = ir;
+      if (terms_im) terms_im[(size_t)t * nR + iR] = ii;
+    }
+  free(xb); free(wb); free(xbb); free(wbb); free(xg); free(wg); free(xgg); free(wgg);
+  free(xaa); free(waa);
+  return 0;
+}

@@ -214,6 +214,17 @@ int orc_expansion_matrix_type0_identical(const orc_system* sys, const int32_t* i
 /* Inversion parity p1 p2 of a channel from its rotor vectors (SRC/pot_comp.f:70-110). */
 int orc_parity_inversion(const double* v1, int j1, const double* v2, int j2);
 
+/* EXPANSION_TERM and CALC_EXPANSION_TERMS for SYS_TYPE 7, 8 and 0
+ * (SRC/pot_comp.f:3739-3896, 4695-6274): the term's angular function, and the
+ * quadrature projection of V[iR][alpha2][beta1][beta2][gamma1][gamma2] onto the terms
+ * (a_top 5 per term), terms[t * nR + iR]. */
+void orc_expansion_term(int sys_type, int l, int l1, int l2, int nju1, int nju2, double beta1,
+                        double gamma1, double alpha2, double beta2, double gamma2, double* wfr,
+                        double* wfi);
+int orc_project_terms(int sys_type, int n_terms, const int32_t* a_top, int n_alpha2,
+                      int n_beta1, int n_beta2, int n_gamma1, int n_gamma2, int eq_gamma, int nR,
+                      const double* V, double* terms, double* terms_im);
+
 #ifdef __cplusplus
 }
 #endif

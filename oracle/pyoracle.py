@@ -127,6 +127,10 @@ def lib():
                                                           C.c_int64, C.c_void_p, C.c_int,
                                                           C.c_void_p, C.c_int, C.c_void_p,
                                                           C.c_double, C.c_void_p]
+        L.orc_expansion_term.argtypes = [C.c_int] * 6 + [C.c_double] * 5 + [
+            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_project_terms.argtypes = [C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 7 + [
+            C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_expansion_matrix_type7.argtypes = [C.POINTER(System), C.c_void_p, C.c_void_p,
                                                  C.c_void_p, C.c_int64, C.c_void_p, C.c_int,
                                                  C.c_void_p, C.c_int, C.c_void_p, C.c_double,
@@ -453,3 +457,27 @@ def expansion_matrix_type0_identical(osys, states, parity, ind, labels, terms, e
     if rc:
         raise RuntimeError(f"orc_expansion_matrix_type0_identical failed: {rc}")
     return mat.reshape(P, nR)
+
+
+def expansion_term(sys_type, l, l1, l2, nju1, nju2, beta1, gamma1, alpha2, beta2, gamma2=0.0):
+    r, i = C.c_double(), C.c_double()
+    lib().orc_expansion_term(sys_type, l, l1, l2, nju1, nju2, beta1, gamma1, alpha2, beta2, gamma2,
+                             C.byref(r), C.byref(i))
+    return r.value, i.value
+
+
+def project_terms(sys_type, labels, V, eq_gamma=True):
+    """CALC_EXPANSION_TERMS for SYS_TYPE 7, 8 and 0.  labels: one row per term, (l1, nju1,
+    l2, l) for 7 and 8 or (l1, nju1, l2, nju2, l) for 0; V: (nR, n_alpha2, n_beta1,
+    n_beta2, n_gamma1[, n_gamma2]).  Returns (terms, terms_im), each n_terms x nR."""
+    lab = np.asarray(labels, np.int32).reshape(len(labels), -1)
+    a_top = np.zeros((len(lab), 5), np.int32)
+    a_top[:, :lab.shape[1]] = lab
+    V = np.ascontiguousarray(V, np.float64)
+    nR, n2, n3, n4, n5 = V.shape[:5]
+    n6 = V.shape[5] if V.ndim == 6 else 1
+    T = np.zeros(nR * len(lab))
+    Ti = np.zeros(nR * len(lab))
+    lib().orc_project_terms(sys_type, len(lab), _ptr(a_top.reshape(-1)), n2, n3, n4, n5, n6,
+                            1 if eq_gamma else 0, nR, _ptr(V), _ptr(T), _ptr(Ti))
+    return T.reshape(len(lab), nR), Ti.reshape(len(lab), nR)

@@ -145,6 +145,18 @@ def main(ref_root):
                               dtype=np.int32)
     np.savez_compressed(os.path.join(out, "g6_expansion_term_lists.npz"), **lists)
 
+    # G7: PES_EXPAN_TERMS.DAT as CALC_EXPANSION_TERMS wrote it over two R ranges
+    # (EXAMPLES_IO/SYS_TYPE_7/NH3_H2_IR_BGN_FIN, IR_BGN/IR_FIN = 1-20 and 21-40; 37 terms,
+    # ND3+D2): the exact text lines of both files and the term labels.
+    d = os.path.join(ex, "SYS_TYPE_7", "NH3_H2_IR_BGN_FIN")
+    texts = {}
+    for key, sub in (("lines_1_20", "GRD_R_1_20"), ("lines_21_40", "GRD_R_21_40")):
+        with open(os.path.join(d, sub, "PES_EXPAN_TERMS.DAT")) as f:
+            texts[key] = np.array(f.read().split("\n"))
+    head = str(texts["lines_1_20"][0]).split()
+    labels_ir = np.array([[int(x) for x in h.split("_")[1:]] for h in head[1:]], dtype=np.int32)
+    np.savez_compressed(os.path.join(out, "g7_expan_terms_files.npz"), labels=labels_ir, **texts)
+
     # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)

@@ -91,10 +91,13 @@ def test_expansion_plan_reuse(mq, gpu_available):
     dm = torch.empty((s.P, len(R)), dtype=torch.float64, device="cuda")
     dy = torch.empty_like(dm)
     dk = torch.empty(s.P, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()  # the plan runs on its own stream
     plan.execute(dT, dm, dy, dk)
     plan.sync()
     assert np.array_equal(dm.cpu().numpy(), m1) and np.array_equal(dy.cpu().numpy(), y1)
-    plan.execute(2.0 * dT, dm, dy, dk)
+    dT2 = 2.0 * dT
+    torch.cuda.synchronize()
+    plan.execute(dT2, dm, dy, dk)
     plan.sync()
     assert np.array_equal(dm.cpu().numpy(), 2.0 * m1) and np.array_equal(dy.cpu().numpy(), 2.0 * y1)
     ang, ex = plan.timing()
