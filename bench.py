@@ -52,6 +52,9 @@ def _args():
     p.add_argument("--no-fp64-form", action="store_true")
     p.add_argument("--no-expansion", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--only-projection", type=int, default=0, metavar="NR",
+                   help="run the CALC_EXPANSION_TERMS block alone on NR R points and print "
+                        "it (a small case for profiling)")
     return p.parse_args()
 
 
@@ -66,13 +69,15 @@ def workload():
 
 
 TC_PROFILE = os.path.join(ROOT, "profiles", "tc_contract_kernel_asymtop_j8_48x48x48_R300.md")
+PROJ_PROFILE = os.path.join(ROOT, "profiles", "proj_kernels_nd3d2_calcexp_R32.md")
 
 
-def _profiled_traffic(path):
-    """DRAM bytes per launch recorded by the committed ncu summary (None if absent)."""
+def _profiled_traffic(path, key="dram_bytes_per_launch"):
+    """DRAM bytes per launch (or per unit) recorded by the committed ncu summary (None if
+    absent)."""
     try:
         for ln in open(path):
-            if ln.strip().startswith("dram_bytes_per_launch:"):
+            if ln.strip().startswith(key + ":"):
                 return float(ln.split(":", 1)[1].strip().split()[0])
     except OSError:
         pass
@@ -515,7 +520,7 @@ def run_expansion(mq, syn):
     return out
 
 
-def run_projection(mq, peaks):
+def run_projection(mq, peaks, nR=86):
     """CALC_EXPANSION_TERMS at the size of the reference's CALC_EXPANSION example for
     ND3+D2 (EXAMPLES_IO/SYS_TYPE_7/NH3_H2_CalcExpansion: 377 terms, GRD_R = 86,
     GRD_ANG1 = 40,40 (alpha2 40), GRD_ANG2 = 20,20 (beta1, beta2 20), GRD_ANG3 = 40,40
@@ -529,7 +534,6 @@ def run_projection(mq, peaks):
     from oracle import pyoracle as po
     labels = np.load(os.path.join(GOLDEN, "g5b_nd3_d2_type7.npz"))["labels"]
     shape = (40, 20, 20, 40)
-    nR = 86
     rng = np.random.default_rng(7)
     V = (rng.standard_normal((nR,) + shape) * 500.0).astype(np.float64)
     G = int(np.prod(shape))
@@ -579,6 +583,14 @@ def run_projection(mq, peaks):
             "e2e": {"ms": e2e_ms, "terms_per_s": n_out / (e2e_ms / 1e3),
                     "h2d_bytes": int(V.nbytes), "d2h_bytes": int(2 * n_out * 8)},
             "roofline_gamma": {"bound": "hbm", "algorithmic_bytes": int(alg),
+                               "traffic": (None if _profiled_traffic(PROJ_PROFILE,
+                                                                     "dram_bytes_per_R_point")
+                                           is None else
+                                           _profiled_traffic(PROJ_PROFILE,
+                                                             "dram_bytes_per_R_point") * nR),
+                               "traffic_source": "ncu DRAM bytes of the gamma kernel at 32 R "
+                                                 "points, scaled by R points, "
+                                                 + os.path.relpath(PROJ_PROFILE, ROOT),
                                "achieved_gbs": alg / (ga / 1e3) / 1e9, "peak_gbs": hbm,
                                "frac": alg / (ga / 1e3) / 1e9 / hbm},
             "cpu_port": {"terms_per_s": 1.0 / per_pair_s,
@@ -616,6 +628,10 @@ def run_reference(a):
 
 def main():
     a = _args()
+    if a.only_projection:
+        import mqct_b200 as mq
+        print(json.dumps(run_projection(mq, _peaks()[0], nR=a.only_projection)), flush=True)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:

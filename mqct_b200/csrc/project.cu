@@ -7,14 +7,18 @@
 //   Y_t(g) = sum_m K_t c_tm a_tm(beta1) b_tm(beta2) e^{i(nju1 gamma1 + nju2 gamma2)} e^{-i m alpha2},
 // with c_tm = <l1 m l2 -m|l 0>, a = d^{l1}_{nju1 m} and b = the diatom's normalised
 // Legendre function of order -m (types 7, 8) or d^{l2}_{nju2,-m} (type 0), so the sum
-// over the grid runs as three contractions, one per group of axes:
-//   F[R][a2][p][b] = sum_{g1,g2} V[R][a2][b][g1,g2] E_p(g1,g2)       (gamma, per (nju1, nju2) pair p)
-//   H[R][p][m][b]  = sum_{a2} F[R][a2][p][b] e^{-i m alpha2} w       (alpha2, per m)
-//   S_t(R)         = sum_m sum_b A_tm(b1) B_tm(b2) H[R][p_t][m][b]    (beta1 x beta2 = b)
+// over the grid runs as four contractions, one per axis group:
+//   F[R][a2][p][b]      = sum_{g1,g2} V[R][a2][b][g1,g2] E_p(g1,g2)   (gamma, per pair p = (nju1, nju2))
+//   H[R][p][m][b]       = sum_{a2} F[R][a2][p][b] e^{-i m alpha2} w   (alpha2, per m)
+//   K[R][p][m][l2][b1]  = sum_{b2} B_{p,l2,m}(b2) H[R][p][m][b1,b2]    (beta2, per l2)
+//   S_t(R)              = sum_m sum_{b1} A_tm(b1) K[R][p_t][m][l2_t][b1]   (beta1, per term)
 // with every quadrature weight folded into the tables E, A and B; terms = Re S,
 // terms_im = Im S (the reference's intgrlr and intgrli).  The first contraction reads V
-// once and carries the bandwidth; the other two run on arrays a few times smaller.
-// FP64 throughout; every sum in a fixed order, so results are reproducible.
+// once and carries the bandwidth; the others run on arrays 6x to 100x smaller.  The
+// gamma and alpha contractions are real GEMMs with a small constant operand, issued as
+// FP64 tensor-core MMAs (mma.sync m8n8k4 f64, 256 FMAs per warp instruction) so that the
+// kernel stays bound by reading V rather than by instruction issue.  FP64 throughout;
+// every sum in a fixed order, so results are reproducible.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,107 +34,189 @@ namespace {
 
 constexpr int kMaxL = 40;          // largest l1, l2, l of a term (log factorials to 127)
 constexpr int kThreads = 256;
-constexpr int kMBlock = 4;         // m values per thread of the alpha contraction
+constexpr int kKSteps = 16;        // k-steps of 4 columns whose V values a lane loads at once
 
 struct TermDev {
   int pair;     // index of the term's (nju1, nju2) in the pair list
+  int l2;
   int m_lo, m_hi;
 };
 
-// F[(blk * P + p) * J + j] for row = blk * J + j, blk = R * n_a2 + i_a2,
-// j = i_b1 * n_b2 + i_b2: one CTA stages kRows consecutive rows of V (each L = n_g1 * n_g2
-// doubles, contiguous in V) in shared memory, threads then run over (p, row).
-__global__ void proj_gamma_kernel(const double* __restrict__ V, int64_t n_rows, int L,
-                                  int L_pad, int rows_per_cta, int P, int J,
-                                  const double2* __restrict__ E, double2* __restrict__ F) {
-  extern __shared__ double vs[];
-  const int64_t row0 = (int64_t)blockIdx.x * rows_per_cta;
-  const int64_t left = n_rows - row0;
-  const int nr = left < rows_per_cta ? (int)left : rows_per_cta;
-  const double* src = V + row0 * L;
-  for (int i = threadIdx.x; i < nr * L; i += blockDim.x) {
-    const int r = i / L, k = i - r * L;
-    vs[r * L_pad + k] = __ldg(src + i);
-  }
-  __syncthreads();
-  for (int w = threadIdx.x; w < nr * P; w += blockDim.x) {
-    const int p = w / nr, r = w - p * nr;
-    const double* v = vs + r * L_pad;
-    double re = 0.0, im = 0.0;
-    for (int k = 0; k < L; ++k) {
-      const double2 e = __ldg(E + (size_t)k * P + p);
-      re = fma(v[k], e.x, re);
-      im = fma(v[k], e.y, im);
-    }
-    const int64_t row = row0 + r;
-    const int64_t blk = row / J;
-    const int j = (int)(row - blk * J);
-    F[(blk * P + p) * J + j] = make_double2(re, im);
-  }
+// D (8x8) += A (8x4, row) * B (4x8, col) in FP64: lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2 (l%4)], D[l/4][2 (l%4) + 1].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
 }
 
-// H[((R * P + p) * n_m + mi) * J + j] = sum_{a2} E2[mi][a2] F[R][a2][p][j]; each thread
-// forms kMBlock consecutive m values of one (R, p, j).
-__global__ void proj_alpha_kernel(const double2* __restrict__ F, int nR, int n_a2, int P, int J,
-                                  int n_m, const double2* __restrict__ E2,
-                                  double2* __restrict__ H) {
-  const int n_mb = (n_m + kMBlock - 1) / kMBlock;
-  const int64_t total = (int64_t)nR * P * n_mb * J;
-  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int j = (int)(idx % J);
-    int64_t q = idx / J;
-    const int mb = (int)(q % n_mb);
-    q /= n_mb;
-    const int p = (int)(q % P);
-    const int R = (int)(q / P);
-    const int m0 = mb * kMBlock;
-    double2 acc[kMBlock];
+// Gamma contraction as the GEMM F(rows x 8 NT) = V(rows x L) Eb(L x 8 NT): V read as the
+// row-major matrix of its rows (row = blk * J + j, blk = R * n_a2 + i_a2,
+// j = i_b1 * n_b2 + i_b2, L = n_g1 * n_g2 contiguous doubles), Eb the packed table of
+// column n = 2 q + part (Re / Im of E for pair 4 tile + q), Lp = L rounded up to 4,
+// Eb[(tile * Lp + k) * 8 + n].  A warp takes 8 rows at a time: each lane loads the
+// kKSteps values of its (row, column) slots at once (8 rows x 32 bytes per load
+// instruction), then the MMAs run over the k-steps for the NT pair tiles.
+// F[(blk * P + p) * J + j] (complex).
+template <int NT>
+__global__ void __launch_bounds__(kThreads)
+    proj_gamma_kernel(const double* __restrict__ V, int64_t n_rows, int L, int Lp, int P,
+                      int tile0, int J, const double* __restrict__ Eb, double2* __restrict__ F) {
+  const int lane = threadIdx.x & 31, kq = lane & 3, rq = lane >> 2;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t tile = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile * 8 < n_rows;
+       tile += nwarps) {
+    const int64_t row = tile * 8 + rq;
+    const bool ok = row < n_rows;
+    const double* src = V + (ok ? row : 0) * L;
+    double c[NT][2];
 #pragma unroll
-    for (int u = 0; u < kMBlock; ++u) acc[u] = make_double2(0.0, 0.0);
-    for (int a = 0; a < n_a2; ++a) {
-      const double2 f = F[(((int64_t)R * n_a2 + a) * P + p) * J + j];
+    for (int nt = 0; nt < NT; ++nt) c[nt][0] = c[nt][1] = 0.0;
+    for (int k0 = 0; k0 < Lp; k0 += 4 * kKSteps) {
+      double a[kKSteps];
 #pragma unroll
-      for (int u = 0; u < kMBlock; ++u) {
-        if (m0 + u >= n_m) break;
-        const double2 e = __ldg(E2 + (size_t)(m0 + u) * n_a2 + a);
-        acc[u].x = fma(f.x, e.x, fma(-f.y, e.y, acc[u].x));
-        acc[u].y = fma(f.x, e.y, fma(f.y, e.x, acc[u].y));
+      for (int s = 0; s < kKSteps; ++s) {
+        const int k = k0 + 4 * s + kq;
+        a[s] = (ok && k < L) ? __ldg(src + k) : 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < kKSteps; ++s) {
+        const int kk = k0 + 4 * s;
+        if (kk >= Lp) break;  // the same for the whole warp
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const double b = __ldg(Eb + ((size_t)(tile0 + nt) * Lp + kk + kq) * 8 + rq);
+          dmma(c[nt][0], c[nt][1], a[s], b);
+        }
       }
     }
+    if (ok) {
+      const int64_t blk = row / J;
+      const int j = (int)(row - blk * J);
 #pragma unroll
-    for (int u = 0; u < kMBlock; ++u) {
-      if (m0 + u >= n_m) break;
-      H[(((int64_t)R * P + p) * n_m + m0 + u) * J + j] = acc[u];
+      for (int nt = 0; nt < NT; ++nt) {
+        const int p = 4 * (tile0 + nt) + kq;
+        if (p < P) F[(blk * P + p) * J + j] = make_double2(c[nt][0], c[nt][1]);
+      }
     }
   }
 }
 
-// One warp per (term, R): lanes run over the beta1 x beta2 points, then a fixed
-// shuffle tree.  A[t][mi][b1], B[t][mi][b2] hold K_t c_tm a_tm w and b_tm w.
-__global__ void proj_terms_kernel(const double2* __restrict__ H, int nR, int r0, int nR_all,
-                                  int P, int J, int n_b2, int n_b1, int n_m,
+// Alpha contraction, per (R, p): H(m, j) = sum_{a2} E2(m, a2) F(a2, j) in complex numbers,
+// as the real GEMM of the rows 2 mi + part_out and the columns 2 a + part_in:
+//   Ab[(mt * K2p + k) * 8 + r] = A[8 mt + r][k],  A = [[E2r, -E2i], [E2i, E2r]] interleaved,
+// K2p = 2 n_a2 rounded up to 4.  A warp takes (R, p) and 8 consecutive j; MT m-tiles
+// starting at mt0.  H[((R * P + p) * n_m + mi) * J + j] (complex).
+template <int MT>
+__global__ void __launch_bounds__(kThreads)
+    proj_alpha_kernel(const double2* __restrict__ F, int nR, int n_a2, int P, int J, int n_m,
+                      int K2p, int mt0, const double* __restrict__ Ab, double2* __restrict__ H) {
+  const int lane = threadIdx.x & 31, kq = lane & 3, rq = lane >> 2;
+  const int n_jt = (J + 7) / 8;
+  const int64_t n_tasks = (int64_t)nR * P * n_jt;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const double* Fd = reinterpret_cast<const double*>(F);
+  double* Hd = reinterpret_cast<double*>(H);
+  for (int64_t task = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; task < n_tasks;
+       task += nwarps) {
+    const int jt = (int)(task % n_jt);
+    const int64_t rp = task / n_jt;  // R * P + p
+    const int p = (int)(rp % P);
+    const int R = (int)(rp / P);
+    const int jb = jt * 8 + rq;  // this lane's column of B
+    double c[MT][2];
+#pragma unroll
+    for (int t = 0; t < MT; ++t) c[t][0] = c[t][1] = 0.0;
+    const double* fcol = Fd + (((int64_t)R * n_a2 * P + p) * J + jb) * 2;
+    const int64_t fstride = (int64_t)P * J * 2;  // next alpha2
+    for (int c0 = 0; c0 < K2p; c0 += 4 * kKSteps) {
+      double b[kKSteps];  // this lane's B values of kKSteps k-steps, loaded at once
+#pragma unroll
+      for (int s = 0; s < kKSteps; ++s) {
+        const int k = c0 + 4 * s + kq, a = k >> 1;
+        b[s] = (a < n_a2 && jb < J) ? fcol[a * fstride + (k & 1)] : 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < kKSteps; ++s) {
+        const int k0 = c0 + 4 * s;
+        if (k0 >= K2p) break;  // the same for the whole warp
+#pragma unroll
+        for (int t = 0; t < MT; ++t) {
+          const double av = __ldg(Ab + ((size_t)(mt0 + t) * K2p + k0 + kq) * 8 + rq);
+          dmma(c[t][0], c[t][1], av, b[s]);
+        }
+      }
+    }
+    // D[r][n]: row 8 (mt0 + t) + rq = 2 mi + part, column j = 8 jt + 2 kq + i
+#pragma unroll
+    for (int t = 0; t < MT; ++t) {
+      const int row = 8 * (mt0 + t) + rq, mi = row >> 1, part = row & 1;
+      if (mi >= n_m) continue;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int j = jt * 8 + 2 * kq + i;
+        if (j < J) Hd[((rp * n_m + mi) * J + j) * 2 + part] = c[t][i];
+      }
+    }
+  }
+}
+
+// K[((((R * P + p) * n_m + mi) * n_l2 + l2) * n_b1 + i1] = sum_{b2} Bt[p][l2][mi][b2]
+// H[R][p][mi][i1 * n_b2 + b2]; zero where |m| > l2.
+__global__ void proj_beta2_kernel(const double2* __restrict__ H, int nR, int P, int n_m,
+                                  int n_l2, int n_b1, int n_b2, const double* __restrict__ Bt,
+                                  double2* __restrict__ K) {
+  const int64_t total = (int64_t)nR * P * n_m * n_l2 * n_b1;
+  const int m_max = (n_m - 1) / 2;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int i1 = (int)(idx % n_b1);
+    int64_t q = idx / n_b1;
+    const int l2 = (int)(q % n_l2);
+    q /= n_l2;
+    const int mi = (int)(q % n_m);
+    q /= n_m;
+    const int p = (int)(q % P);
+    const int R = (int)(q / P);
+    double re = 0.0, im = 0.0;
+    if (abs(mi - m_max) <= l2) {
+      const double* b = Bt + (((size_t)p * n_l2 + l2) * n_m + mi) * n_b2;
+      const double2* h = H + ((((int64_t)R * P + p) * n_m + mi) * n_b1 + i1) * n_b2;
+      for (int i2 = 0; i2 < n_b2; ++i2) {
+        const double w = __ldg(b + i2);
+        const double2 v = h[i2];
+        re = fma(w, v.x, re);
+        im = fma(w, v.y, im);
+      }
+    }
+    K[idx] = make_double2(re, im);
+  }
+}
+
+// One warp per (term, R): lanes over the (m, beta1) points of the term, then a fixed
+// shuffle tree.  S_t(R) = sum_m sum_{b1} A[t][mi][b1] K[R][p_t][mi][l2_t][b1].
+__global__ void proj_terms_kernel(const double2* __restrict__ K, int nR, int r0, int nR_all,
+                                  int P, int n_m, int n_l2, int n_b1,
                                   const TermDev* __restrict__ terms, int n_terms,
-                                  const double* __restrict__ A, const double* __restrict__ B,
-                                  double* __restrict__ out_re, double* __restrict__ out_im) {
+                                  const double* __restrict__ A, double* __restrict__ out_re,
+                                  double* __restrict__ out_im) {
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (wid >= (int64_t)n_terms * nR) return;
   const int t = (int)(wid / nR), R = (int)(wid % nR);
   const TermDev td = terms[t];
+  const int m_max = (n_m - 1) / 2;
+  const int n = (td.m_hi - td.m_lo + 1) * n_b1;
+  const double* a = A + ((size_t)t * n_m + td.m_lo + m_max) * n_b1;
+  const double2* kb = K + (((int64_t)R * P + td.pair) * n_m + td.m_lo + m_max) * n_l2 * n_b1 +
+                      (int64_t)td.l2 * n_b1;
   double re = 0.0, im = 0.0;
-  for (int m = td.m_lo; m <= td.m_hi; ++m) {
-    const int mi = m + (n_m - 1) / 2;
-    const double2* h = H + (((int64_t)R * P + td.pair) * n_m + mi) * J;
-    const double* a = A + ((size_t)t * n_m + mi) * n_b1;
-    const double* b = B + ((size_t)t * n_m + mi) * n_b2;
-    for (int j = lane; j < J; j += 32) {
-      const int i1 = j / n_b2, i2 = j - i1 * n_b2;
-      const double w = __ldg(a + i1) * __ldg(b + i2);
-      const double2 v = h[j];
-      re = fma(w, v.x, re);
-      im = fma(w, v.y, im);
-    }
+  for (int i = lane; i < n; i += 32) {
+    const int mo = i / n_b1, i1 = i - mo * n_b1;
+    const double w = __ldg(a + i);
+    const double2 v = kb[(int64_t)mo * n_l2 * n_b1 + i1];
+    re = fma(w, v.x, re);
+    im = fma(w, v.y, im);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -208,15 +294,14 @@ using namespace mqct;
 struct mqct_projection_plan {
   int sys_type = 8, n_terms = 0;
   int n_a2 = 0, n_b1 = 0, n_b2 = 0, n_g1 = 0, n_g2 = 1;
-  int P = 0, n_m = 0, J = 0, L = 0;
-  DevBuf<double2> E, E2;
+  int P = 0, n_m = 0, n_l2 = 0, J = 0, L = 0;
+  int Lp = 0, n_pt = 0, K2p = 0, n_mt = 0;  // padded GEMM sizes of the gamma and alpha steps
+  DevBuf<double> Eb, Ab;
   DevBuf<double> A, B;
   DevBuf<TermDev> terms;
-  DevBuf<double2> F, H;
-  int chunk_R = 0;
+  DevBuf<double2> F, H, K;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  float ms[3] = {0.f, 0.f, 0.f};
   bool timed = false;
 
   ~mqct_projection_plan() {
@@ -246,14 +331,16 @@ struct mqct_projection_plan {
     if (rc != MQCT_OK) return rc;
     J = n_b1 * n_b2;
     L = n_g1 * n_g2;
-    MQCT_ARG_CHECK((int64_t)L * 8 <= 40 * 1024, "n_gamma1 * n_gamma2 = %d exceeds 5120", L);
+    MQCT_ARG_CHECK((int64_t)J <= (1 << 24), "n_beta1 * n_beta2 = %d too large", J);
     if (mqct_device_count() <= 0) {
       set_error("no CUDA device available");
       return MQCT_E_NODEV;
     }
     // axes as INI_POT_STORAGE sets them (pot_comp.f:1310-1370, 1628-1700)
     const Axis b1 = axis_gl(n_b1, 0.0, kPi), b2 = axis_gl(n_b2, 0.0, kPi);
-    auto ang = [&](int n) { return g.eq_gamma ? axis_mid(n, 0.0, 2.0 * kPi) : axis_gl(n, 0.0, 2.0 * kPi); };
+    auto ang = [&](int n) {
+      return g.eq_gamma ? axis_mid(n, 0.0, 2.0 * kPi) : axis_gl(n, 0.0, 2.0 * kPi);
+    };
     const Axis a2 = ang(n_a2), g1 = ang(n_g1);
     Axis g2 = ang(n_g2);
     if (sys != 0) {  // no second gamma: one point, unit weight
@@ -265,10 +352,10 @@ struct mqct_projection_plan {
     std::vector<double> lf(128);
     lf[0] = 0.0;
     for (int i = 1; i < 128; ++i) lf[i] = lf[i - 1] + std::log((double)i);
-    // (nju1, nju2) pairs and the m range
+    // (nju1, nju2) pairs, the m range and the l2 values
     std::vector<std::pair<int, int>> pairs;
     std::vector<TermDev> td(nt);
-    int m_max = 0;
+    int m_max = 0, l2_max = 0;
     for (int t = 0; t < nt; ++t) {
       const int32_t* q = a_top + 5 * t;
       const int l1 = q[0], n1 = q[1], l2 = q[2], n2 = sys == 0 ? q[3] : 0;
@@ -276,61 +363,93 @@ struct mqct_projection_plan {
       auto it = std::find(pairs.begin(), pairs.end(), pr);
       td[t].pair = (int)(it - pairs.begin());
       if (it == pairs.end()) pairs.push_back(pr);
+      td[t].l2 = l2;
       const int mm = std::min(l1, l2);
       td[t].m_lo = -mm;
       td[t].m_hi = mm;
       m_max = std::max(m_max, mm);
+      l2_max = std::max(l2_max, l2);
     }
     P = (int)pairs.size();
     n_m = 2 * m_max + 1;
-    // E[k][p], k = i_g1 * n_g2 + i_g2
-    std::vector<double2> e((size_t)L * P), e2((size_t)n_m * n_a2);
+    n_l2 = l2_max + 1;
+    // Eb: B operand of the gamma GEMM, Eb[(tile * Lp + k) * 8 + 2 q + part] = Re / Im of
+    // e^{i(nju1 gamma1 + nju2 gamma2)} w for pair 4 tile + q at k = i_g1 * n_g2 + i_g2
+    Lp = (L + 3) / 4 * 4;
+    n_pt = (P + 3) / 4;
+    // (tiles padded with zeros to a multiple of 4: a pass covers up to 4 tiles)
+    std::vector<double> eb((size_t)(n_pt + 3) / 4 * 4 * Lp * 8, 0.0);
     for (int i5 = 0; i5 < n_g1; ++i5)
       for (int i6 = 0; i6 < n_g2; ++i6)
         for (int p = 0; p < P; ++p) {
           const double ph = pairs[p].first * g1.x[i5] + pairs[p].second * g2.x[i6];
           const double w = g1.w[i5] * g1.half * g2.w[i6] * g2.half * tail2;
-          e[((size_t)i5 * n_g2 + i6) * P + p] = make_double2(std::cos(ph) * w, std::sin(ph) * w);
+          const size_t k = (size_t)i5 * n_g2 + i6;
+          double* d = &eb[((size_t)(p / 4) * Lp + k) * 8 + 2 * (p % 4)];
+          d[0] = std::cos(ph) * w;
+          d[1] = std::sin(ph) * w;
         }
+    // Ab: A operand of the alpha GEMM, rows 2 mi + part_out, columns 2 a + part_in of
+    // [[E2r, -E2i], [E2i, E2r]], E2 = e^{-i m alpha2} w; Ab[(mt * K2p + k) * 8 + r]
+    K2p = (2 * n_a2 + 3) / 4 * 4;
+    n_mt = (2 * n_m + 7) / 8;
+    // (tiles padded with zeros to a multiple of 8: a pass covers up to 8 tiles)
+    std::vector<double> ab((size_t)(n_mt + 7) / 8 * 8 * K2p * 8, 0.0);
     for (int mi = 0; mi < n_m; ++mi)
       for (int i2 = 0; i2 < n_a2; ++i2) {
         const double ph = -(double)(mi - m_max) * a2.x[i2];
         const double w = a2.w[i2] * a2.half;
-        e2[(size_t)mi * n_a2 + i2] = make_double2(std::cos(ph) * w, std::sin(ph) * w);
+        const double er = std::cos(ph) * w, ei = std::sin(ph) * w;
+        for (int po = 0; po < 2; ++po)
+          for (int pi = 0; pi < 2; ++pi) {
+            const int row = 2 * mi + po, col = 2 * i2 + pi;
+            const double v = po == pi ? er : (po == 0 ? -ei : ei);
+            ab[((size_t)(row / 8) * K2p + col) * 8 + row % 8] = v;
+          }
       }
-    // A[t][mi][b1] = K_t c_tm d^{l1}_{nju1 m}(beta1) w, B[t][mi][b2] = b_tm(beta2) w
-    std::vector<double> ta((size_t)nt * n_m * n_b1, 0.0), tb((size_t)nt * n_m * n_b2, 0.0);
+    // A[t][mi][b1] = K_t c_tm d^{l1}_{nju1 m}(beta1) w; B[p][l2][mi][b2] = b(beta2) w with
+    // b = WF_DIAT_TOP(l2, -m, beta2, .) without its phase (types 7, 8) or
+    // d^{l2}_{nju2(p), -m}(beta2) (type 0)
+    std::vector<double> ta((size_t)nt * n_m * n_b1, 0.0);
+    std::vector<double> tb((size_t)P * n_l2 * n_m * n_b2, 0.0);
     for (int t = 0; t < nt; ++t) {
       const int32_t* q = a_top + 5 * t;
       const int l1 = q[0], n1 = q[1], l2 = q[2];
-      const int n2 = sys == 0 ? q[3] : 0, l = sys == 0 ? q[4] : q[3];
-      const double K = sys == 0 ? std::sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (8.0 * kPi * kPi)
-                                : std::sqrt((2.0 * l1 + 1.0) / 4.0 / kPi);
+      const int l = sys == 0 ? q[4] : q[3];
+      const double Kt = sys == 0 ? std::sqrt((2.0 * l1 + 1.0) * (2.0 * l2 + 1.0)) / (8.0 * kPi * kPi)
+                                 : std::sqrt((2.0 * l1 + 1.0) / 4.0 / kPi);
       for (int m = td[t].m_lo; m <= td[t].m_hi; ++m) {
         const int mi = m + m_max;
         const double c = mqct_dev::clebsch_gordan(l1, m, l2, -m, l, 0, lf.data());
         for (int i = 0; i < n_b1; ++i)
           ta[((size_t)t * n_m + mi) * n_b1 + i] =
-              K * c * mqct_dev::wigner_d(l1, n1, m, b1.x[i], lf.data()) * b1.w[i] *
+              Kt * c * mqct_dev::wigner_d(l1, n1, m, b1.x[i], lf.data()) * b1.w[i] *
               std::sin(b1.x[i]) * b1.half;
-        for (int i = 0; i < n_b2; ++i) {
-          double bv;
-          if (sys == 0) {
-            bv = mqct_dev::wigner_d(l2, n2, -m, b2.x[i], lf.data());
-          } else {  // WF_DIAT_TOP(l2, -m, beta2, .) without its phase
-            const int am = std::abs(m);
-            bv = mqct_dev::plgndr(l2, am, std::cos(b2.x[i])) *
-                 std::sqrt((2.0 * l2 + 1.0) / 4.0 / kPi * std::exp(lf[l2 - am] - lf[l2 + am]));
-            if (m > 0 && (am & 1)) bv = -bv;
-          }
-          tb[((size_t)t * n_m + mi) * n_b2 + i] = bv * b2.w[i] * std::sin(b2.x[i]) * b2.half;
-        }
       }
     }
+    for (int p = 0; p < P; ++p)
+      for (int l2 = 0; l2 < n_l2; ++l2)
+        for (int m = -std::min(l2, m_max); m <= std::min(l2, m_max); ++m) {
+          const int mi = m + m_max;
+          if (sys == 0 && std::abs(pairs[p].second) > l2) continue;
+          for (int i = 0; i < n_b2; ++i) {
+            double bv;
+            if (sys == 0) {
+              bv = mqct_dev::wigner_d(l2, pairs[p].second, -m, b2.x[i], lf.data());
+            } else {
+              const int am = std::abs(m);
+              bv = mqct_dev::plgndr(l2, am, std::cos(b2.x[i])) *
+                   std::sqrt((2.0 * l2 + 1.0) / 4.0 / kPi * std::exp(lf[l2 - am] - lf[l2 + am]));
+              if (m > 0 && (am & 1)) bv = -bv;
+            }
+            tb[(((size_t)p * n_l2 + l2) * n_m + mi) * n_b2 + i] =
+                bv * b2.w[i] * std::sin(b2.x[i]) * b2.half;
+          }
+        }
     MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     for (auto& x : ev) MQCT_CUDA_TRY(cudaEventCreate(&x));
-    MQCT_CUDA_TRY(E.upload(e, st));
-    MQCT_CUDA_TRY(E2.upload(e2, st));
+    MQCT_CUDA_TRY(Eb.upload(eb, st));
+    MQCT_CUDA_TRY(Ab.upload(ab, st));
     MQCT_CUDA_TRY(A.upload(ta, st));
     MQCT_CUDA_TRY(B.upload(tb, st));
     MQCT_CUDA_TRY(terms.upload(td, st));
@@ -338,11 +457,36 @@ struct mqct_projection_plan {
     return MQCT_OK;
   }
 
-  // R points per pass so that F and H stay within 4 GiB.
+  // R points per pass so that F, H and K stay within 4 GiB.
   int pass_R(int nR) const {
-    const size_t per_R = ((size_t)n_a2 * P * J + (size_t)P * n_m * J) * sizeof(double2);
+    const size_t per_R = ((size_t)n_a2 * P * J + (size_t)P * n_m * J +
+                          (size_t)P * n_m * n_l2 * n_b1) *
+                         sizeof(double2);
     const size_t cap = (size_t)4 << 30;
     return (int)std::max<size_t>(1, std::min<size_t>(nR, cap / per_R));
+  }
+
+  // Warps for n_tasks warp tasks, as whole CTAs, at most 16 CTAs per SM (grid-stride).
+  static unsigned ctas(int64_t n_tasks) {
+    const int64_t w = kThreads / 32;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_tasks + w - 1) / w, 148 * 16));
+  }
+
+  template <int NT>
+  int launch_gamma(const double* V, int64_t n_rows, int tile0) {
+    proj_gamma_kernel<NT><<<ctas((n_rows + 7) / 8), kThreads, 0, st>>>(V, n_rows, L, Lp, P,
+                                                                       tile0, J, Eb.p, F.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    return MQCT_OK;
+  }
+
+  template <int MT>
+  int launch_alpha(int nr, int mt0) {
+    const int64_t tasks = (int64_t)nr * P * ((J + 7) / 8);
+    proj_alpha_kernel<MT><<<ctas(tasks), kThreads, 0, st>>>(F.p, nr, n_a2, P, J, n_m, K2p, mt0,
+                                                           Ab.p, H.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    return MQCT_OK;
   }
 
   int execute(const double* d_V, int nR, double* d_terms, double* d_terms_im) {
@@ -350,29 +494,40 @@ struct mqct_projection_plan {
     const int rc_R = pass_R(nR);
     if (F.n < (size_t)rc_R * n_a2 * P * J) MQCT_CUDA_TRY(F.alloc((size_t)rc_R * n_a2 * P * J));
     if (H.n < (size_t)rc_R * P * n_m * J) MQCT_CUDA_TRY(H.alloc((size_t)rc_R * P * n_m * J));
-    const int L_pad = L | 1;
-    const int rows_per_cta = std::max(1, std::min(64, (40 * 1024 / 8) / L_pad));
-    const size_t smem = (size_t)rows_per_cta * L_pad * sizeof(double);
+    const size_t nK = (size_t)rc_R * P * n_m * n_l2 * n_b1;
+    if (K.n < nK) MQCT_CUDA_TRY(K.alloc(nK));
     const size_t G = (size_t)n_a2 * J * L;
     bool first = true;
     for (int r0 = 0; r0 < nR; r0 += rc_R) {
       const int nr = std::min(rc_R, nR - r0);
       const int64_t n_rows = (int64_t)nr * n_a2 * J;
+      const double* V = d_V + (size_t)r0 * G;
       if (first) MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
-      const int64_t nb = (n_rows + rows_per_cta - 1) / rows_per_cta;
-      proj_gamma_kernel<<<(unsigned)nb, kThreads, smem, st>>>(d_V + (size_t)r0 * G, n_rows, L,
-                                                              L_pad, rows_per_cta, P, J, E.p, F.p);
-      MQCT_CUDA_TRY(cudaGetLastError());
+      for (int t0 = 0; t0 < n_pt; t0 += 4) {  // up to 4 pair tiles (16 pairs) per pass over V
+        const int nt = std::min(4, n_pt - t0);
+        const int rc = nt == 1   ? launch_gamma<1>(V, n_rows, t0)
+                       : nt == 2 ? launch_gamma<2>(V, n_rows, t0)
+                                 : launch_gamma<4>(V, n_rows, t0);
+        if (rc != MQCT_OK) return rc;
+      }
       if (first) MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
-      const int64_t na = (int64_t)nr * P * ((n_m + kMBlock - 1) / kMBlock) * J;
-      const int64_t ba = std::min<int64_t>((na + kThreads - 1) / kThreads, 148 * 64);
-      proj_alpha_kernel<<<(unsigned)ba, kThreads, 0, st>>>(F.p, nr, n_a2, P, J, n_m, E2.p, H.p);
-      MQCT_CUDA_TRY(cudaGetLastError());
+      for (int m0 = 0; m0 < n_mt; m0 += 8) {  // up to 8 m tiles (32 m values) per pass
+        const int mt = std::min(8, n_mt - m0);
+        const int rc = mt == 1   ? launch_alpha<1>(nr, m0)
+                       : mt == 2 ? launch_alpha<2>(nr, m0)
+                       : mt <= 4 ? launch_alpha<4>(nr, m0)
+                                 : launch_alpha<8>(nr, m0);
+        if (rc != MQCT_OK) return rc;
+      }
       if (first) MQCT_CUDA_TRY(cudaEventRecord(ev[2], st));
-      const int64_t warps = (int64_t)n_terms * nr;
-      proj_terms_kernel<<<(unsigned)((warps * 32 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
-          H.p, nr, r0, nR, P, J, n_b2, n_b1, n_m, terms.p, n_terms, A.p, B.p, d_terms,
-          d_terms_im);
+      const int64_t nk = (int64_t)nr * P * n_m * n_l2 * n_b1;
+      const int64_t bk = std::min<int64_t>((nk + kThreads - 1) / kThreads, 148 * 64);
+      proj_beta2_kernel<<<(unsigned)bk, kThreads, 0, st>>>(H.p, nr, P, n_m, n_l2, n_b1, n_b2,
+                                                           B.p, K.p);
+      MQCT_CUDA_TRY(cudaGetLastError());
+      const int64_t nt = (int64_t)n_terms * nr;
+      proj_terms_kernel<<<(unsigned)((nt * 32 + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+          K.p, nr, r0, nR, P, n_m, n_l2, n_b1, terms.p, n_terms, A.p, d_terms, d_terms_im);
       MQCT_CUDA_TRY(cudaGetLastError());
       if (first) MQCT_CUDA_TRY(cudaEventRecord(ev[3], st));
       first = false;

@@ -119,3 +119,15 @@ def test_projection_plan_reuse(mq, gpu_available):
     pp.sync()
     assert np.array_equal(dT2.cpu().numpy(), 2.0 * T1[:2].T)
     pp.close()
+
+
+def test_projection_many_pairs_and_long_gamma_rows(mq, oracle, gpu_available):
+    """Type 0 with 41 (nju1, nju2) pairs (three register passes of the gamma contraction)
+    and n_gamma1 x n_gamma2 = 72 points per row (two staged chunks)."""
+    labels = [(4, n1, 4, n2, 4) for n1 in range(5) for n2 in range(-4, 5) if n1 > 0 or n2 >= 0]
+    assert len(labels) == 41
+    V = np.random.default_rng(4).normal(size=(2, 4, 6, 5, 9, 8)) * 300.0
+    T, Ti = mq.project_terms(0, labels, V, eq_gamma=False)
+    To, Tio = oracle.project_terms(0, labels, V, eq_gamma=False)
+    assert np.max(np.abs(T - To.T)) <= _bound(V)
+    assert np.max(np.abs(Ti - Tio.T)) <= _bound(V)
