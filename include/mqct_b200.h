@@ -59,6 +59,11 @@ extern "C" {
 /* Propagation modes. */
 #define MQCT_MODE_STD 0       /* Ehrenfest MQCT: classical and quantum coupled */
 #define MQCT_MODE_AT 1        /* AT-MQCT: classical path given                 */
+#define MQCT_MODE_CS 2        /* flag, OR-ed with either mode: the coupled-states
+                                 approximation (CS_APPROX = YES): no Coriolis
+                                 coupling of m12 blocks, no Coriolis torque
+                                 (MQCT_SOURCE_CODES/mqct_eqtns.f:208-210, 270,
+                                 362, 787, 845)                                */
 
 const char* mqct_last_error(void);
 int mqct_version(void);                 /* MAJOR*10000 + MINOR*100 + PATCH */
@@ -309,7 +314,10 @@ typedef struct mqct_at_paths_t {
  * (R, P_R, theta, P_theta, phi, P_phi); diag_out: n_traj x 8 (t_end, steps,
  * |1-norm|, |energy error| Hartree, status, orbits, oscillations, coupling
  * energy at the end).  status: 0 finished, 1 step cap reached, 2 not
- * propagated (impact parameter beyond RMAX), 3 non-finite state. */
+ * propagated (impact parameter beyond RMAX), 3 non-finite state.  mode:
+ * MQCT_MODE_STD or MQCT_MODE_AT, either OR-ed with MQCT_MODE_CS for the
+ * coupled-states approximation (states of other m12 than the initial state's keep
+ * zero amplitude, as the reference's skipped pairs leave them). */
 int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
                          int64_t n_traj, int32_t mode, const mqct_at_paths_t* at,
                          int32_t arith, double* amp_out, double* cls_out, double* diag_out);
@@ -388,6 +396,9 @@ int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms);
 void mqct_prop_plan_destroy(mqct_prop_plan* plan);
 /* Select the plan's integrator for the following runs (default RK4). */
 int mqct_prop_plan_set_integrator(mqct_prop_plan* plan, const mqct_integrator_t* integ);
+/* CS_APPROX for the following runs of the plan (cs != 0), as MQCT_MODE_CS does for
+ * one batch call. */
+int mqct_prop_plan_set_coupled_states(mqct_prop_plan* plan, int32_t cs);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
 int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,

@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (MODE_AT, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
+from ._abi import (MODE_AT, MODE_CS, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
                    check, lib, ptr)
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
@@ -31,7 +31,7 @@ __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables",
            "expansion_terms_list", "write_expansion_terms_list",
            "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
-           "MODE_AT"]
+           "MODE_AT", "MODE_CS"]
 
 
 def asym_top_level(A, B, Cc, j, ka, kc):
@@ -589,9 +589,10 @@ def _integrator(integrator):
 
 
 def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, at_paths=None,
-              integrator=None):
+              integrator=None, coupled_states=False):
     """Batched DOTRAJECT on the GPU.  Returns (amp [n, 2N], cls [n, 6], diag [n, 8]).
-    integrator: None (RK4) or ("ODEINT", eps, hmin)."""
+    integrator: None (RK4) or ("ODEINT", eps, hmin); coupled_states: CS_APPROX = YES
+    (no Coriolis coupling between m12 blocks, no Coriolis torque)."""
     n = len(trajs)
     N = tables.n_states
     amp = np.zeros(n * 2 * N)
@@ -600,7 +601,7 @@ def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, 
     t = tables.c_struct()
     arr = _traj_array(trajs)
     at = None
-    if mode == MODE_AT:
+    if mode & MODE_AT:
         recs = [np.ascontiguousarray(p, np.float64).reshape(-1, 8) for p in at_paths]
         n_rec = np.array([len(r) for r in recs], np.int32)
         off = np.concatenate([[0], np.cumsum(n_rec)[:-1]]).astype(np.int64)
@@ -608,6 +609,8 @@ def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, 
         at_keep = (n_rec, off, flat)
         at = _abi.AtPaths(ptr(off), ptr(n_rec), ptr(flat))
     integ = _integrator(integrator)
+    if coupled_states:
+        mode = mode | MODE_CS
     if integ is None:
         check(lib().mqct_propagate_batch(C.byref(t), arr, n, mode, C.byref(at) if at else None,
                                          arith, amp, cls, diag))
@@ -666,6 +669,10 @@ class PropagationPlan:
         """None or "RK4" (default), or ("ODEINT", eps, hmin) for the following runs."""
         integ = _integrator(integrator) or _abi.Integrator(_abi.INTEG_RK4, 0.0, 0.0)
         check(lib().mqct_prop_plan_set_integrator(self.h, C.byref(integ)))
+
+    def set_coupled_states(self, cs=True):
+        """CS_APPROX for the following runs."""
+        check(lib().mqct_prop_plan_set_coupled_states(self.h, 1 if cs else 0))
 
     def sync(self):
         check(lib().mqct_prop_plan_sync(self.h))

@@ -19,7 +19,7 @@ ERRORS = {-1: "MQCT_E_ARG", -2: "MQCT_E_CUDA", -3: "MQCT_E_NODEV", -4: "MQCT_E_I
 
 PREC_FP64, PREC_BF16X3, PREC_F16X3 = 0, 1, 2
 PROP_FP64, PROP_FP32 = 0, 1
-MODE_STD, MODE_AT = 0, 1
+MODE_STD, MODE_AT, MODE_CS = 0, 1, 2
 INTEG_RK4, INTEG_ODEINT = 0, 1
 PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3
 
@@ -93,7 +93,7 @@ EXPORTS = [
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
     "mqct_prop_plan_create", "mqct_prop_plan_run", "mqct_prop_plan_run_device",
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
-    "mqct_prop_plan_destroy",
+    "mqct_prop_plan_destroy", "mqct_prop_plan_set_coupled_states",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
     "mqct_fill_ind_mat", "mqct_count_states_identical", "mqct_enumerate_states_identical",
     "mqct_count_pairs_identical", "mqct_fill_ind_mat_identical", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
@@ -158,6 +158,7 @@ def lib():
     L.mqct_propagate_batch_integ.argtypes = [C.POINTER(Tables), C.POINTER(TrajInit), C.c_int64,
                                              C.c_int32, C.POINTER(AtPaths), C.c_int32,
                                              C.POINTER(Integrator), f64p, f64p, f64p]
+    L.mqct_prop_plan_set_coupled_states.argtypes = [vp, C.c_int32]
     L.mqct_prop_plan_set_integrator.argtypes = [vp, C.POINTER(Integrator)]
     L.mqct_expansion_plan_create.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
                                              C.c_int32, i32p, C.c_double, C.c_double, C.c_double,

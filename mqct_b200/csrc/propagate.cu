@@ -76,7 +76,8 @@ struct PropDev {
   const int* inv_perm;         // reference -> internal state index
   const void* knots;           // nR x S of (M, y2) in T precision
   double mass;
-  int mode;                    // MQCT_MODE_*
+  int mode;                    // MQCT_MODE_STD or MQCT_MODE_AT
+  int cs;                      // coupled-states approximation: no Coriolis terms
   int mp_cap;                  // packed slots that fit in shared memory
   double ode_eps, ode_hmin;    // ODEINT accuracy and minimum step (adaptive kernel)
   // AT paths
@@ -244,7 +245,9 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     sm.bt[i].x = p.x * ar - p.y * ai;
     sm.bt[i].y = p.x * ai + p.y * ar;
     double ur = 0.0, ui = 0.0;
-    const int np_ = __ldg(d.nb_plus + i), nm = __ldg(d.nb_minus + i);
+    // u = (J_+ + J_-) a; none with CS_APPROX (MQCT_SOURCE_CODES/mqct_eqtns.f:270, 362,
+    // 845), which also keeps dP_phi/dt = sin(theta) Im((D^* u)^+ y) at zero
+    const int np_ = d.cs ? -1 : __ldg(d.nb_plus + i), nm = d.cs ? -1 : __ldg(d.nb_minus + i);
     if (np_ >= 0) {
       const double cp = __ldg(d.cplus + i);
       ur += cp * sm.a_in[np_].x;
@@ -906,6 +909,7 @@ struct PropPlan {
 
   int method = MQCT_INTEG_RK4;
   double ode_eps = 1e-6, ode_hmin = 0.0;
+  bool cs = false;  // CS_APPROX for every run of the plan
 
   template <class T, bool A>
   static const void* pick(int ns) {
@@ -1137,7 +1141,8 @@ struct PropPlan {
     d.perm = d_perm.p; d.inv_perm = d_inv.p;
     d.knots = arith == MQCT_PROP_FP32 ? (const void*)d_knots32.p : (const void*)d_knots64.p;
     d.mass = mass;
-    d.mode = mode;
+    d.mode = mode & MQCT_MODE_AT;
+    d.cs = ((mode & MQCT_MODE_CS) != 0) || cs;
     d.mp_cap = mp_cap;
     d.ode_eps = ode_eps;
     d.ode_hmin = ode_hmin;
@@ -1225,6 +1230,7 @@ struct PropPlan {
 };
 
 static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mode) {
+  mode &= MQCT_MODE_AT;
   for (int64_t t = 0; t < n; ++t) {
     const mqct_traj_init_t& a = init[t];
     MQCT_ARG_CHECK(a.s_st >= 1 && a.s_st <= N, "trajectory %lld: s_st out of range", (long long)t);
@@ -1331,6 +1337,12 @@ int mqct_prop_plan_timing(mqct_prop_plan* plan, float* ms) {
 
 void mqct_prop_plan_destroy(mqct_prop_plan* plan) { delete reinterpret_cast<PropPlan*>(plan); }
 
+int mqct_prop_plan_set_coupled_states(mqct_prop_plan* plan, int32_t cs) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  reinterpret_cast<PropPlan*>(plan)->cs = cs != 0;
+  return MQCT_OK;
+}
+
 int mqct_prop_plan_set_integrator(mqct_prop_plan* plan, const mqct_integrator_t* integ) {
   MQCT_ARG_CHECK(plan, "null plan");
   return reinterpret_cast<PropPlan*>(plan)->set_integrator(integ);
@@ -1341,14 +1353,15 @@ int mqct_propagate_batch_integ(const mqct_tables_t* tab, const mqct_traj_init_t*
                                int32_t arith, const mqct_integrator_t* integ, double* amp_out,
                                double* cls_out, double* diag_out) {
   MQCT_ARG_CHECK(init && amp_out && cls_out && diag_out && integ, "null argument");
-  MQCT_ARG_CHECK(mode == MQCT_MODE_STD || mode == MQCT_MODE_AT, "unknown mode %d", mode);
+  MQCT_ARG_CHECK((mode & ~MQCT_MODE_CS) == MQCT_MODE_STD || (mode & ~MQCT_MODE_CS) == MQCT_MODE_AT,
+                 "unknown mode %d", mode);
   mqct_prop_plan* h = nullptr;
   int rc = mqct_prop_plan_create(tab, arith, &h);
   if (rc) return rc;
   PropPlan* p = reinterpret_cast<PropPlan*>(h);
   rc = p->set_integrator(integ);
   if (!rc) rc = validate_init(init, n_traj, p->N, mode);
-  if (!rc && mode == MQCT_MODE_AT) rc = p->set_at(at, n_traj);
+  if (!rc && (mode & MQCT_MODE_AT)) rc = p->set_at(at, n_traj);
   if (!rc) rc = run_host(p, init, n_traj, mode, amp_out, cls_out, diag_out);
   mqct_prop_plan_destroy(h);
   return rc;
@@ -1358,13 +1371,14 @@ int mqct_propagate_batch(const mqct_tables_t* tab, const mqct_traj_init_t* init,
                          int32_t mode, const mqct_at_paths_t* at, int32_t arith,
                          double* amp_out, double* cls_out, double* diag_out) {
   MQCT_ARG_CHECK(init && amp_out && cls_out && diag_out, "null argument");
-  MQCT_ARG_CHECK(mode == MQCT_MODE_STD || mode == MQCT_MODE_AT, "unknown mode %d", mode);
+  MQCT_ARG_CHECK((mode & ~MQCT_MODE_CS) == MQCT_MODE_STD || (mode & ~MQCT_MODE_CS) == MQCT_MODE_AT,
+                 "unknown mode %d", mode);
   mqct_prop_plan* h = nullptr;
   int rc = mqct_prop_plan_create(tab, arith, &h);
   if (rc) return rc;
   PropPlan* p = reinterpret_cast<PropPlan*>(h);
   rc = validate_init(init, n_traj, p->N, mode);
-  if (!rc && mode == MQCT_MODE_AT) rc = p->set_at(at, n_traj);
+  if (!rc && (mode & MQCT_MODE_AT)) rc = p->set_at(at, n_traj);
   if (!rc) rc = run_host(p, init, n_traj, mode, amp_out, cls_out, diag_out);
   mqct_prop_plan_destroy(h);
   return rc;

@@ -875,6 +875,8 @@ typedef struct {
   int32_t* uidx;           /* per pair */
   double* misc;            /* 4 per pair (Coriolis factors) */
   double *m, *dm, *phi_amp, *sc;
+  int cs;                  /* coupled states: only pairs of the initial m12, no Coriolis */
+  int cs_m;                /* m12 of the initial state */
 } orc_rhs_ws;
 
 /* resize: unique Delta E table (last match within 1e-12 in single precision wins)
@@ -889,6 +891,8 @@ static void orc_ws_init(orc_rhs_ws* w, const orc_tables* t) {
   w->dm = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
   w->phi_amp = (double*)malloc(sizeof(double) * (size_t)(P > 0 ? P : 1));
   w->sc = (double*)malloc(sizeof(double) * 2 * (size_t)(P > 0 ? P : 1));
+  w->cs = 0;
+  w->cs_m = 0;
   const double tol = (double)(float)1.0e-12;
   int n_u = 0;
   for (int64_t k = 0; k < P; ++k) {
@@ -948,7 +952,9 @@ static void orc_matrix_at(const orc_tables* t, double x, double* m, double* dm) 
 }
 
 /* DERIVS_BK for distinguishable particles, full CC, planar motion
- * (POLAR_ANGLE=NO): SRC/mqct_eqtns.f:112-499. */
+ * (POLAR_ANGLE=NO): SRC/mqct_eqtns.f:112-499.  With CS_APPROX (coupled states) the
+ * pairs whose m12 differs from the initial state's are skipped (:208-210) and so are
+ * the Coriolis terms of P_phi and of the amplitudes (:270, :362, :845). */
 static void orc_derivs_ws(orc_rhs_ws* w, double t, const double* q, double* dq) {
   const orc_tables* tb = w->tab;
   int N = tb->n_states;
@@ -967,6 +973,8 @@ static void orc_derivs_ws(orc_rhs_ws* w, double t, const double* q, double* dq) 
   const int Z1 = 2 * N + 6, Z2 = 2 * N + 7; /* zero sinks */
   for (int64_t k = 0; k < P; ++k) {
     int i = tb->ind_mat[2 * k] - 1, j = tb->ind_mat[2 * k + 1] - 1;
+    w->phi_amp[k] = 0.0;
+    if (w->cs && tb->m12[i] != w->cs_m) continue;
     double M = w->m[k], Md = w->dm[k];
     double d_f = (i == j) ? 1.0 : 2.0;
     double iphase = w->sc[2 * w->uidx[k]], rphase = w->sc[2 * w->uidx[k] + 1];
@@ -977,6 +985,7 @@ static void orc_derivs_ws(orc_rhs_ws* w, double t, const double* q, double* dq) 
     dq[j + N] -= (q[i + N] * rfp + q[i] * ifp) * M / 2.0;
     dq[2 * N + 1] -= ((q[i] * q[j] + q[i + N] * q[j + N]) * rphase -
                       (q[i + N] * q[j] - q[i] * q[j + N]) * iphase) * d_f * Md;
+    if (w->cs) continue;
     const double* mc = w->misc + 4 * k;
     double amp = 0.0;
     {
@@ -1007,8 +1016,8 @@ static void orc_derivs_ws(orc_rhs_ws* w, double t, const double* q, double* dq) 
   }
   double dot = 0.0;
   for (int64_t k = 0; k < P; ++k) dot += w->m[k] * w->phi_amp[k];
-  dq[2 * N + 5] = dot;
-  for (int i = 0; i < N; ++i) {
+  dq[2 * N + 5] = w->cs ? 0.0 : dot;
+  for (int i = 0; i < N && !w->cs; ++i) {
     double jj = tb->j12[i], mm = tb->m12[i];
     double m1 = mm + 1.0, m0 = mm - 1.0;
     double sqrt1 = sqrt(jj * (jj + 1.0) - m0 * (m0 + 1.0));
@@ -1182,6 +1191,8 @@ static int orc_dotraject_impl(const orc_tables* tab, const orc_traj* tr, double*
   double* dym = (double*)calloc((size_t)n, sizeof(double));
   orc_rhs_ws w;
   orc_ws_init(&w, tab);
+  w.cs = tr->cs;
+  w.cs_m = tab->m12[tr->s_st - 1];
   double k_vec = sqrt(mass * 2.0 * tr->e_coll);
   double l_orb = sqrt(tr->l_real * (tr->l_real + 1.0));
   double R_st = tr->r_start;
@@ -1324,6 +1335,7 @@ static void orc_rhs_at(void* vctx, double t, const double* q, double* dq) {
   }
   for (int64_t k = 0; k < tb->P; ++k) {
     int i = tb->ind_mat[2 * k] - 1, j = tb->ind_mat[2 * k + 1] - 1;
+    if (w->cs && tb->m12[i] != w->cs_m) continue; /* SRC/mqct_eqtns.f:787-789 */
     double M = w->m[k];
     double d_f = (i == j) ? 1.0 : 2.0;
     double iphase = w->sc[2 * w->uidx[k]], rphase = w->sc[2 * w->uidx[k] + 1];
@@ -1333,7 +1345,7 @@ static void orc_rhs_at(void* vctx, double t, const double* q, double* dq) {
     dq[j] -= (q[i] * rfp - q[i + N] * ifp) * M / 2.0;
     dq[j + N] -= (q[i + N] * rfp + q[i] * ifp) * M / 2.0;
   }
-  for (int i = 0; i < N; ++i) {
+  for (int i = 0; i < N && !w->cs; ++i) { /* no Coriolis with CS_APPROX (:845) */
     double jj = tb->j12[i], mm = tb->m12[i];
     double m1 = mm + 1.0, m0 = mm - 1.0;
     double sqrt1 = sqrt(jj * (jj + 1.0) - m0 * (m0 + 1.0));
@@ -1353,6 +1365,8 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   int N = tab->n_states, n = 2 * N;
   orc_rhs_ws w;
   orc_ws_init(&w, tab);
+  w.cs = tr->cs;
+  w.cs_m = tab->m12[tr->s_st - 1];
   orc_at_ctx c;
   c.w = &w;
   c.n_at = n_at;

@@ -150,6 +150,7 @@ typedef struct orc_traj {
   int32_t method;          /* 0: RK4 (PROPAGATOR = RK4), 1: adaptive Cash-Karp (ODEINT) */
   double eps;              /* ODEINT accuracy (eps_odeint) */
   double hmin;             /* ODEINT minimum step (min_t_stp) */
+  int32_t cs;              /* CS_APPROX = YES: coupled-states approximation */
 } orc_traj;
 
 /* Per-trajectory output: amp[2N] (Re, Im), cls[6] = (R,P_R,theta,P_theta,phi,P_phi),

@@ -52,7 +52,7 @@ class Traj(C.Structure):
                 ("dt", C.c_double), ("r_start", C.c_double), ("r_fin", C.c_double),
                 ("numb_orb_prds", C.c_int32), ("numb_oscl_prds", C.c_int32),
                 ("time_lim", C.c_double), ("max_steps", C.c_int64), ("method", C.c_int32),
-                ("eps", C.c_double), ("hmin", C.c_double)]
+                ("eps", C.c_double), ("hmin", C.c_double), ("cs", C.c_int32)]
 
 
 def build() -> str:
@@ -328,11 +328,12 @@ class OracleTables:
 
 
 def make_traj(e_coll, l_real, s_st, dt, r_start, r_fin, numb_orb=1, numb_oscl=1, time_lim=0.0,
-              max_steps=0, method=0, eps=1e-6, hmin=0.0):
+              max_steps=0, method=0, eps=1e-6, hmin=0.0, cs=False):
     """method 0: RK4 with step dt; 1: adaptive Cash-Karp (ODEINT) with accuracy eps and
-    minimum step hmin inside every interval dt."""
+    minimum step hmin inside every interval dt.  cs: the coupled-states approximation
+    (CS_APPROX = YES)."""
     return Traj(e_coll, l_real, s_st, dt, r_start, r_fin, numb_orb, numb_oscl, time_lim, max_steps,
-                method, eps, hmin)
+                method, eps, hmin, 1 if cs else 0)
 
 
 def propagate_batch(tables, trajs, n_threads=0):

@@ -157,13 +157,26 @@ def main(ref_root):
     labels_ir = np.array([[int(x) for x in h.split("_")[1:]] for h in head[1:]], dtype=np.int32)
     np.savez_compressed(os.path.join(out, "g7_expan_terms_files.npz"), labels=labels_ir, **texts)
 
-    # G4: asymmetric top + atom (SYS_TYPE 4), MF_He: state ordering and levels.
+    # G4: asymmetric top + atom (SYS_TYPE 4), MF_He with CS_APPROX = YES: state ordering,
+    # levels, and the coupled-states dynamics on the reference's own matrix
+    # (OPACITY_FUNCTIONS_L.out, DEFLECTION_FUNCTION.out finish times, CROSS_SECTIONS.out).
     d = os.path.join(ex, "SYS_TYPE_4", "MF_He_CS_MQCT")
     coll, nch, states4, ind4, R4, mat4 = _read_mtrx_dat(os.path.join(d, "MTRX.DAT"), 7)
+    opac4 = _read_table(os.path.join(d, "OPACITY_FUNCTIONS_L.out"), 2 + nch)
+    defl4 = _read_table(os.path.join(d, "DEFLECTION_FUNCTION.out"), 9, first_int=False)
+    sig4 = []
+    for line in open(os.path.join(d, "CROSS_SECTIONS.out")):
+        t = line.split()
+        if len(t) == 5 and t[0].isdigit():
+            sig4.append(float(t[2]))
     np.savez_compressed(os.path.join(out, "g4_type4_layout.npz"), states=states4, ind_mat=ind4,
                         R=R4, mat=mat4, A=0.6666525, B=0.1769383, C=0.2306476,
                         channels=np.array([[0, 0, 0], [1, 0, 1], [1, 1, 1]], dtype=np.int32),
-                        e_ch_printed=np.array([0.000, 0.408, 0.844]))
+                        e_ch_printed=np.array([0.000, 0.408, 0.844]),
+                        opacity=opac4, deflection=defl4, sigma_U=np.array(sig4),
+                        # $SYSTEM of MF_He_CS_MQCT.inp (R_COM in bohr whatever R_UNITS)
+                        mass_red=3.7523705333, rmax=42.40, U=50.0, b_impct=20.0,
+                        time_step=10.0, time_lim=3.5e6)
 
     # G1 AT trajectory record layout: Fortran unformatted, 8 float64 per record.
     d = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_AT_Approximation", "AT_MQCT_2nd_Step",
