@@ -397,6 +397,17 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
                 "max": float(np.max(np.abs(s32[keep] - s64[keep]) / s64[keep]))}
         plan.close()
     res["speedup_fp32_vs_fp64_form"] = res["fp32"]["traj_per_s"] / res["fp64"]["traj_per_s"]
+    # the coupled-states approximation (CS_APPROX) on the same trajectories: only the
+    # m-block of the initial state is streamed and propagated
+    plan = mq.PropagationPlan(tab, mq.PROP_FP32)
+    plan.set_coupled_states(True)
+    plan.run(trajs[:8])
+    amp, cls, diag = plan.run(trajs)
+    ms = replicas.max_over_ranks(plan.timing(), dist, device="cuda")
+    res["fp32_cs"] = {"n_traj": n, "kernel_ms": ms, "traj_per_s": world * n / (ms / 1e3),
+                      "traj_steps": float(diag[:, 1].sum()),
+                      "max_status": float(diag[:, 4].max())}
+    plan.close()
     res["workload"] = (f"{n} of the 4096 trajectories (b~U(0,15), E log-uniform 50-2000 cm^-1, "
                        "dt=5 a.u., R>25 stop), c2 matrix, retained pairs "
                        f"{tab.P} of {s.P}")

@@ -65,6 +65,8 @@ struct PropDev {
   const int* blk_n;            // states per block
   const int* blk_s0;           // first internal state of the block
   const int* blk_mp;           // offset of the block's triangle inside its pass
+  const int64_t* blk_slot0;    // first slot of each block (n_blocks + 1)
+  const int* blk_pass;         // pass holding each block
   const uint32_t* loc;         // per slot: internal (row | column << 16)
   const int* st_e;             // energy class per internal state
   const double* e_val;         // energy per class, Hartree
@@ -124,7 +126,7 @@ template <class T>
 struct Smem {
   Cls* c;                      // kClsSlots classical slots (see above)
   double* red;                 // reduction scratch, 3 per warp
-  int* flag;                   // [0] next trajectory, [1] keep running
+  int* flag;                   // [0] next trajectory, [1] keep running, [2] CS m-block or -1
   double* Rg;                  // nR grid
   double2* a_in;               // N (RHS input amplitudes)
   typename V2<T>::t* bt;       // N
@@ -230,6 +232,12 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
   const double sin_t = sin(c.th);
   const double dphidt = c.Pphi / c.R / c.R / d.mass / (sin_t * sin_t);
   const SplineAt sp = spline_at(sm.Rg, d.nR, c.R);
+  // coupled states: only the m-block of the initial state carries amplitude, so only
+  // its slots are read and only its rows formed; bt, u and y of the other rows were
+  // zeroed when the trajectory started and stay zero
+  const int cs_blk = sm.flag[2];
+  const int cs_r0 = cs_blk >= 0 ? __ldg(d.blk_s0 + cs_blk) : 0;
+  const int cs_r1 = cs_blk >= 0 ? cs_r0 + __ldg(d.blk_n + cs_blk) : N;
   // phases per energy class: (cos E t, -sin E t) = e^{-iEt}
   for (int e = tid; e < d.n_e; e += PT) {
     double s, co;
@@ -238,7 +246,7 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     sm.ph[e].y = (T)(-s);
   }
   __syncthreads();
-  for (int i = tid; i < N; i += PT) {
+  for (int i = cs_r0 + tid; i < cs_r1; i += PT) {
     const double2 a = sm.a_in[i];
     const T2 p = sm.ph[__ldg(d.st_e + i)];
     const T ar = (T)a.x, ai = (T)a.y;
@@ -273,12 +281,17 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     const T hinv = (T)(1.0 / sp.h), d1 = (T)(-sp.cc3 * sp.cc6), d2 = (T)(sp.cc4 * sp.cc6);
     const T2* K0 = reinterpret_cast<const T2*>(d.knots) + (int64_t)sp.klo * d.S;
     const T2* K1 = K0 + d.S;
-    for (int p = 0; p < d.n_pass; ++p) {
-      const int s0 = (int)d.pass_slot0[p], s1 = (int)d.pass_slot0[p + 1];
+    const int p_lo = cs_blk >= 0 ? __ldg(d.blk_pass + cs_blk) : 0;
+    const int p_hi = cs_blk >= 0 ? p_lo + 1 : d.n_pass;
+    for (int p = p_lo; p < p_hi; ++p) {
+      // s0: the pass's first slot (shared-memory base); [k0, s1): the slots read
+      const int s0 = (int)d.pass_slot0[p];
+      const int k0 = cs_blk >= 0 ? (int)d.blk_slot0[cs_blk] : s0;
+      const int s1 = cs_blk >= 0 ? (int)d.blk_slot0[cs_blk + 1] : (int)d.pass_slot0[p + 1];
       // phase A: interpolate the pass's slots into Mp, force term
       if constexpr (sizeof(T) == 4) {
         // two adjacent slots per load (16-byte knot loads, 8-byte location loads)
-        for (int kb = s0 + 2 * tid; kb < s1; kb += 2 * UNROLL * PT) {
+        for (int kb = k0 + 2 * tid; kb < s1; kb += 2 * UNROLL * PT) {
           float4 lo[UNROLL], hi[UNROLL];
           uint2 l[UNROLL];
 #pragma unroll
@@ -313,7 +326,7 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
           }
         }
       } else {
-        for (int kb = s0 + tid; kb < s1; kb += UNROLL * PT) {
+        for (int kb = k0 + tid; kb < s1; kb += UNROLL * PT) {
           T2 lo[UNROLL], hi[UNROLL];
           uint32_t l[UNROLL];
 #pragma unroll
@@ -342,7 +355,8 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
       }
       __syncthreads();
       // phase B: rows of the pass, y_i = sum_j M_ij bt_j
-      const int r0 = d.pass_row0[p], r1 = d.pass_row0[p + 1];
+      const int r0 = cs_blk >= 0 ? cs_r0 : d.pass_row0[p];
+      const int r1 = cs_blk >= 0 ? cs_r1 : d.pass_row0[p + 1];
       for (int r = r0 + tid; r < r1; r += PT) {
         const int b = __ldg(d.st_blk + r);
         const int n = __ldg(d.blk_n + b), sb = __ldg(d.blk_s0 + b);
@@ -377,7 +391,7 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
   }
   // quadratic forms: F (accumulated above), g = Im((D^* u)^+ y), pot = Re(bt^+ y)
   double g = 0.0, pt = 0.0, f = (double)force;
-  for (int i = tid; i < N; i += PT) {
+  for (int i = cs_r0 + tid; i < cs_r1; i += PT) {
     const T2 p = sm.ph[__ldg(d.st_e + i)];
     const T2 uu = sm.u[i], yy = sm.y[i], b2 = sm.bt[i];
     const T utr = p.x * uu.x - p.y * uu.y, uti = p.x * uu.y + p.y * uu.x;
@@ -543,6 +557,7 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
       const double l_orb = sqrt(ti->l_real * (ti->l_real + 1.0));
       *bk = Book{0.0, 0.0, 0.0, 0.0, 0, 0, 0, 0, 1};
       *C = Cls{};
+      sm.flag[2] = d.cs ? d.st_blk[s_int] : -1;
       if (!at && l_orb / k_vec > ti->r_start) {
         bk->status = 2;  // impact parameter beyond the starting distance: not propagated
         bk->run = 0;
@@ -557,6 +572,12 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
       }
     }
     __syncthreads();
+    if (d.cs)
+      for (int i = tid; i < N; i += PT) {
+        sm.bt[i] = T2{(T)0, (T)0};
+        sm.u[i] = T2{(T)0, (T)0};
+        sm.y[i] = T2{(T)0, (T)0};
+      }
     const bool skipped = bk->run == 0;
     double dt_step = dt;  // ODEINT's carried step (dt_step / dt_corrected)
     // hooks of the first right-hand side of a step: the SAVE_TRAJECT record and,
@@ -894,7 +915,8 @@ struct PropPlan {
   DevBuf<double> d_R, d_e_val, d_cplus, d_cminus;
   DevBuf<int> d_pass_row0, d_st_blk, d_blk_n, d_blk_s0, d_blk_mp, d_st_e, d_nbp, d_nbm, d_perm,
       d_inv, d_queue, d_status;
-  DevBuf<int64_t> d_pass_slot0;
+  DevBuf<int64_t> d_pass_slot0, d_blk_slot0;
+  DevBuf<int> d_blk_pass;
   DevBuf<uint32_t> d_loc;
   DevBuf<float2> d_knots32;
   DevBuf<double2> d_knots64;
@@ -1031,7 +1053,7 @@ struct PropPlan {
                    dev_smem);
     const int64_t cap = (int64_t)(((size_t)dev_smem - fixed) / tsize()) & ~int64_t(3);
     std::vector<int64_t> pass_slot0;
-    std::vector<int> pass_row0, blk_mp(n_blocks);
+    std::vector<int> pass_row0, blk_mp(n_blocks), blk_pass(n_blocks);
     int64_t max_pass = 0;
     for (int b = 0; b < n_blocks; ++b) {
       const int64_t bs = (b + 1 < n_blocks ? blk_slot0[b + 1] : S) - blk_slot0[b];
@@ -1041,6 +1063,7 @@ struct PropPlan {
         pass_row0.push_back(blk_s0[b]);
       }
       blk_mp[b] = (int)(blk_slot0[b] - pass_slot0.back());
+      blk_pass[b] = (int)pass_slot0.size() - 1;
       max_pass = std::max(max_pass, blk_slot0[b] + bs - pass_slot0.back());
     }
     n_pass = (int)pass_slot0.size();
@@ -1116,6 +1139,12 @@ struct PropPlan {
     MQCT_CUDA_TRY(d_blk_n.upload(blk_n, stream));
     MQCT_CUDA_TRY(d_blk_s0.upload(blk_s0, stream));
     MQCT_CUDA_TRY(d_blk_mp.upload(blk_mp, stream));
+    MQCT_CUDA_TRY(d_blk_pass.upload(blk_pass, stream));
+    {
+      std::vector<int64_t> bs0(blk_slot0);
+      bs0.push_back(S);
+      MQCT_CUDA_TRY(d_blk_slot0.upload(bs0, stream));
+    }
     MQCT_CUDA_TRY(d_loc.upload(loc, stream));
     MQCT_CUDA_TRY(d_st_e.upload(st_e, stream));
     MQCT_CUDA_TRY(d_perm.upload(perm, stream));
@@ -1136,6 +1165,7 @@ struct PropPlan {
     d.N = N; d.nR = nR; d.n_e = n_e; d.n_pass = n_pass; d.S = S;
     d.R = d_R.p; d.pass_row0 = d_pass_row0.p; d.pass_slot0 = d_pass_slot0.p;
     d.st_blk = d_st_blk.p; d.blk_n = d_blk_n.p; d.blk_s0 = d_blk_s0.p; d.blk_mp = d_blk_mp.p;
+    d.blk_slot0 = d_blk_slot0.p; d.blk_pass = d_blk_pass.p;
     d.loc = d_loc.p; d.st_e = d_st_e.p; d.e_val = d_e_val.p;
     d.nb_plus = d_nbp.p; d.nb_minus = d_nbm.p; d.cplus = d_cplus.p; d.cminus = d_cminus.p;
     d.perm = d_perm.p; d.inv_perm = d_inv.p;
@@ -1246,13 +1276,32 @@ static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mod
 }
 
 // Host-buffer run: upload the initial conditions, launch, copy the results back
-// (and the SAVE_TRAJECT records when rec_out is given).
+// (and the SAVE_TRAJECT records when rec_out is given).  In standard mode the
+// trajectories go to the device queue longest first (estimated steps
+// 2 r_start / (v dt), v the initial speed), so that the CTAs finish together instead
+// of waiting for a slow trajectory taken last; the results return in the caller's
+// order and do not depend on the order (one trajectory per CTA, no shared state).
 static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, int mode,
                     double* amp_out, double* cls_out, double* diag_out,
                     double* rec_out = nullptr, int64_t rec_cap = 0, int64_t* n_rec_out = nullptr) {
   int rc = validate_init(init, n_traj, p->N, mode);
   if (rc) return rc;
-  MQCT_CUDA_TRY(p->d_init.upload(init, n_traj, p->stream));
+  std::vector<int64_t> order(n_traj);
+  for (int64_t t = 0; t < n_traj; ++t) order[t] = t;
+  const bool reorder = (mode & MQCT_MODE_AT) == 0 && n_traj > 1;
+  if (reorder) {
+    std::vector<double> est(n_traj);
+    for (int64_t t = 0; t < n_traj; ++t) {
+      const mqct_traj_init_t& a = init[t];
+      const double v = std::sqrt(2.0 * a.e_coll / p->mass);
+      est[t] = 2.0 * a.r_start / (v * a.dt);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t x, int64_t y) { return est[x] > est[y]; });
+  }
+  std::vector<mqct_traj_init_t> sorted(n_traj);
+  for (int64_t t = 0; t < n_traj; ++t) sorted[t] = init[order[t]];
+  MQCT_CUDA_TRY(p->d_init.upload(sorted.data(), n_traj, p->stream));
   MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
   MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
   MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
@@ -1265,19 +1314,41 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
   rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p, d_rec.p,
                  rec_cap, d_nrec.p);
   if (rc) return rc;
+  const size_t na = (size_t)2 * p->N;
+  std::vector<double> amp(reorder ? (size_t)n_traj * na : 0), cls(reorder ? n_traj * 6 : 0),
+      diag(reorder ? n_traj * 8 : 0), rec(reorder && rec_out ? (size_t)n_traj * rec_cap * 8 : 0);
+  std::vector<int64_t> nrec(reorder && rec_out ? n_traj : 0);
+  double* h_amp = reorder ? amp.data() : amp_out;
+  double* h_cls = reorder ? cls.data() : cls_out;
+  double* h_diag = reorder ? diag.data() : diag_out;
+  double* h_rec = reorder ? rec.data() : rec_out;
+  int64_t* h_nrec = reorder ? nrec.data() : n_rec_out;
   if (rec_out) {
-    MQCT_CUDA_TRY(cudaMemcpyAsync(rec_out, d_rec.p, sizeof(double) * n_traj * rec_cap * 8,
+    MQCT_CUDA_TRY(cudaMemcpyAsync(h_rec, d_rec.p, sizeof(double) * n_traj * rec_cap * 8,
                                   cudaMemcpyDeviceToHost, p->stream));
-    MQCT_CUDA_TRY(cudaMemcpyAsync(n_rec_out, d_nrec.p, sizeof(int64_t) * n_traj,
+    MQCT_CUDA_TRY(cudaMemcpyAsync(h_nrec, d_nrec.p, sizeof(int64_t) * n_traj,
                                   cudaMemcpyDeviceToHost, p->stream));
   }
-  MQCT_CUDA_TRY(cudaMemcpyAsync(amp_out, p->d_amp.p, sizeof(double) * n_traj * 2 * p->N,
+  MQCT_CUDA_TRY(cudaMemcpyAsync(h_amp, p->d_amp.p, sizeof(double) * n_traj * na,
                                 cudaMemcpyDeviceToHost, p->stream));
-  MQCT_CUDA_TRY(cudaMemcpyAsync(cls_out, p->d_cls.p, sizeof(double) * n_traj * 6,
+  MQCT_CUDA_TRY(cudaMemcpyAsync(h_cls, p->d_cls.p, sizeof(double) * n_traj * 6,
                                 cudaMemcpyDeviceToHost, p->stream));
-  MQCT_CUDA_TRY(cudaMemcpyAsync(diag_out, p->d_diag.p, sizeof(double) * n_traj * 8,
+  MQCT_CUDA_TRY(cudaMemcpyAsync(h_diag, p->d_diag.p, sizeof(double) * n_traj * 8,
                                 cudaMemcpyDeviceToHost, p->stream));
   MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+  if (reorder) {
+    for (int64_t t = 0; t < n_traj; ++t) {
+      const int64_t o = order[t];
+      std::copy(amp.begin() + t * na, amp.begin() + (t + 1) * na, amp_out + o * na);
+      std::copy(cls.begin() + t * 6, cls.begin() + (t + 1) * 6, cls_out + o * 6);
+      std::copy(diag.begin() + t * 8, diag.begin() + (t + 1) * 8, diag_out + o * 8);
+      if (rec_out) {
+        const size_t rn = (size_t)rec_cap * 8;
+        std::copy(rec.begin() + t * rn, rec.begin() + (t + 1) * rn, rec_out + o * rn);
+        n_rec_out[o] = nrec[t];
+      }
+    }
+  }
   return MQCT_OK;
 }
 
