@@ -330,10 +330,10 @@ def write_expansion_terms_list(path, labels):
 
 def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",
                            mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
-    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 7, 8 and 0).
+    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 1, 4, 7, 8 and 0).
 
-    labels: the TERMS list, one row per term: (l1, nju1, l2, l) for SYS_TYPE 7 and 8,
-    (l1, nju1, l2, nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
+    labels: the TERMS list, one row per term: (l,) for SYS_TYPE 1, (l, nju) for SYS_TYPE
+    4, (l1, nju1, l2, l) for SYS_TYPE 7 and 8, (l1, nju1, l2, nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
     PES_EXPAN_TERMS.DAT, in the unit e_unit (a key of E_UNIT or the Hartree value of
     one unit).  Returns (Mat_el, y2, skipped) as build_matrix."""
     R = np.ascontiguousarray(R, np.float64)

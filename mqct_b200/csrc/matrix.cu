@@ -1479,6 +1479,49 @@ __global__ void expansion_identical_kernel(int64_t P, int n_terms, const int* __
 }
 
 // M[k * nR + i] = sum_t A[k * n_terms + t] T[t * nR + i] from stored coefficients.
+// Coefficients of a rotor and an atom (EXPANSION_MATRIX_ELEMENT, SYS_TYPE 1 and 4,
+// MQCT_SOURCE_CODES/pot_comp.f:6551-6622 and 6955-7075), one thread per (pair, term):
+//   A = sqrt((2j'+1)/(2j''+1)) sqrt((2l+1)/4pi) <j' m l 0|j'' m> S,
+//   S = sum over +nju (factor (-1)^nju) and, for nju > 0, -nju (factor 1) of
+//       sum_K <j' K l nju|j'' K+nju> c'_K c''_{K+nju},
+// with c the rotor vector over K (the unit vector at K = 0 for the diatom of type 1,
+// where S = <j' 0 l 0|j'' 0>).  lab5 holds (l, nju) per term.
+__global__ void expansion_atom_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
+                                      const int* __restrict__ st_chan,
+                                      const int* __restrict__ st_m,
+                                      const int* __restrict__ ch_j,
+                                      const double* __restrict__ vec, int ldv,
+                                      const int* __restrict__ lab5, double* __restrict__ A) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P * n_terms) return;
+  const int64_t k = idx / n_terms;
+  const int t = (int)(idx % n_terms);
+  const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+  const int cp = st_chan[sp], cpp = st_chan[spp];
+  const int jp = ch_j[cp], jpp = ch_j[cpp], m = st_m[sp];
+  const int l = lab5[5 * t], nju0 = lab5[5 * t + 1];
+  double a = 0.0;
+  if (triangle_ok(jpp, l, jp)) {
+    const double* vp = vec + (size_t)cp * ldv;
+    const double* vpp = vec + (size_t)cpp * ldv;
+    double S = 0.0;
+    for (int planar = 0; planar < (nju0 == 0 ? 1 : 2); ++planar) {
+      const int nju = planar ? -nju0 : nju0;
+      const double f = (planar == 0 && (nju0 & 1)) ? -1.0 : 1.0;
+      double b = 0.0;
+      for (int kp = -jp; kp <= jp; ++kp) {
+        const int kpp = kp + nju;
+        if (kpp < -jpp || kpp > jpp) continue;
+        b += cg_dev(jp, kp, l, nju, jpp, kpp) * vp[jp + kp] * vpp[jpp + kpp];
+      }
+      S += f * b;
+    }
+    a = sqrt((2.0 * jp + 1.0) / (2.0 * jpp + 1.0)) * sqrt((2.0 * l + 1.0) / (4.0 * kPi)) *
+        cg_dev(jp, m, l, 0, jpp, m) * S;
+  }
+  A[idx] = a;
+}
+
 __global__ void __launch_bounds__(128)
 expansion_contract_a_kernel(int n_terms, int nR, const double* __restrict__ A,
                             const double* __restrict__ T, double* __restrict__ M) {
@@ -1625,7 +1668,7 @@ struct ExpansionPlan {
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_ch = 0, n_u = 0;
-  bool identical = false;  // coefficients stored whole in d_A (identical partners)
+  bool a_stored = false;  // coefficients stored whole in d_A (identical partners, types 1 and 4)
   DevBuf<int> d_k2r, d_ind, d_chan, d_j1, d_j2, d_term_u;
   DevBuf<double> d_K, d_M3, d_fac, d_M, d_gc, d_A;
 
@@ -1635,6 +1678,108 @@ struct ExpansionPlan {
     if (st) cudaStreamDestroy(st);
   }
 
+  // The grid, cut-off and spline state shared by every system type.
+  int init_common(const int32_t* ind_mat, int64_t P_, const double* R, int32_t nR_,
+                  int32_t n_terms_, double mij_cutoff_cm, double r_cut1, double r_cut2) {
+    if (mqct_device_count() <= 0) {
+      set_error("no CUDA device available");
+      return MQCT_E_NODEV;
+    }
+    int rc = upload_logfact();
+    if (rc) return rc;
+    MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : ev) MQCT_CUDA_TRY(cudaEventCreate(&e));
+    P = P_;
+    nR = nR_;
+    n_terms = n_terms_;
+    MQCT_CUDA_TRY(d_ind.upload(ind_mat, 2 * (size_t)P, st));
+    std::vector<double> Rh(R, R + nR);
+    MQCT_CUDA_TRY(d_gc.upload(spline_grid_coefs(Rh), st));
+    std::vector<int> k2r(P);
+    for (int64_t k = 0; k < P; ++k) k2r[k] = (int)k;
+    MQCT_CUDA_TRY(d_k2r.upload(k2r, st));
+    MQCT_CUDA_TRY(d_M.alloc((size_t)P * nR));
+    ir1 = nearest_index(Rh, r_cut1);
+    ir2 = nearest_index(Rh, r_cut2);
+    cut_hartree = mij_cutoff_cm * kCmToHartree;
+    return MQCT_OK;
+  }
+
+  // SYS_TYPE 1 (diatom + atom) and 4 (asymmetric top + atom): the coefficients of every
+  // (pair, term) stored whole and contracted as for identical partners.  A_TOP columns:
+  // (l) for type 1, (l, nju) for type 4 (pot_comp.f:6276-6316).
+  int init_atom(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, const double* R,
+                int32_t nR_, int32_t n_terms_, const int32_t* a_top, double mij_cutoff_cm,
+                double r_cut1, double r_cut2) {
+    const int type = sys->sys_type;
+    MQCT_ARG_CHECK(sys->j1 && sys->indx_chann && sys->j12 && sys->m12 && sys->n_states > 0 &&
+                       (type == 1 || (sys->vec1 && sys->ldv > 0)),
+                   "system arrays missing");
+    MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31) && n_terms_ > 0 && n_terms_ <= 4096 &&
+                       nR_ >= 2 && nR_ <= 3072,
+                   "bad sizes (n_terms <= 4096, 2 <= nR <= 3072)");
+    for (int i = 0; i + 1 < nR_; ++i) MQCT_ARG_CHECK(R[i + 1] > R[i], "R grid must increase");
+    MQCT_ARG_CHECK(sys->parity == nullptr, "identical partners are SYS_TYPE 0");
+    std::vector<int> lab5(5 * (size_t)n_terms_, 0);
+    for (int t = 0; t < n_terms_; ++t) {
+      const int l = a_top[5 * t], nju = type == 4 ? a_top[5 * t + 1] : 0;
+      // the reference's check of nju (pot_comp.f:6985-6998); l bounded by the log factorials
+      MQCT_ARG_CHECK(l >= 0 && l <= 60 && nju >= 0 && nju <= l,
+                     "bad expansion term %d (l=%d nju=%d): 0 <= nju <= l <= 60", t + 1, l, nju);
+      lab5[5 * t] = l;
+      lab5[5 * t + 1] = nju;
+    }
+    const int n_states = sys->n_states, n_ch = sys->n_channels;
+    int jmax = 0;
+    for (int c = 0; c < n_ch; ++c) {
+      MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 &&
+                         (type == 1 || 2 * sys->j1[c] + 1 <= sys->ldv),
+                     "bad channel %d (j <= 30, 2j + 1 <= ldv)", c + 1);
+      jmax = std::max(jmax, sys->j1[c]);
+    }
+    std::vector<int> st_chan(n_states);
+    for (int s2 = 0; s2 < n_states; ++s2) {
+      st_chan[s2] = sys->indx_chann[s2] - 1;
+      MQCT_ARG_CHECK(st_chan[s2] >= 0 && st_chan[s2] < n_ch, "indx_chann out of range");
+      MQCT_ARG_CHECK(sys->j12[s2] == sys->j1[st_chan[s2]] && abs(sys->m12[s2]) <= sys->j12[s2],
+                     "bad (j12, m12) at state %d", s2 + 1);
+    }
+    for (int64_t k = 0; k < P_; ++k) {
+      const int a = ind_mat[2 * k] - 1, b = ind_mat[2 * k + 1] - 1;
+      MQCT_ARG_CHECK(a >= 0 && a < n_states && b >= 0 && b < n_states, "ind_mat out of range");
+      MQCT_ARG_CHECK(sys->m12[a] == sys->m12[b], "pair with different m12 at k=%lld",
+                     (long long)k + 1);
+    }
+    int ldv = sys->ldv;
+    std::vector<double> unit;
+    if (type == 1) {  // the diatom: one component, K = 0
+      ldv = 2 * jmax + 1;
+      unit.assign((size_t)n_ch * ldv, 0.0);
+      for (int c = 0; c < n_ch; ++c) unit[(size_t)c * ldv + sys->j1[c]] = 1.0;
+    }
+    int rc = init_common(ind_mat, P_, R, nR_, n_terms_, mij_cutoff_cm, r_cut1, r_cut2);
+    if (rc) return rc;
+    this->n_ch = n_ch;
+    DevBuf<int> d_m, d_lab;
+    DevBuf<double> d_vec;
+    MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
+    MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
+    MQCT_CUDA_TRY(d_j1.upload(sys->j1, n_ch, st));
+    if (type == 1) MQCT_CUDA_TRY(d_vec.upload(unit, st));
+    else MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)n_ch * ldv, st));
+    MQCT_CUDA_TRY(d_lab.upload(lab5, st));
+    MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
+    a_stored = true;
+    const int64_t n_at = P * n_terms;
+    MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
+    expansion_atom_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
+        P, n_terms, d_ind.p, d_chan.p, d_m.p, d_j1.p, d_vec.p, ldv, d_lab.p, d_A.p);
+    MQCT_CUDA_TRY(cudaGetLastError());
+    MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(st));
+    return MQCT_OK;
+  }
+
   int init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, const double* R,
            int32_t nR_, int32_t n_terms_, const int32_t* a_top, double mij_cutoff_cm,
            double r_cut1, double r_cut2) {
@@ -1642,8 +1787,10 @@ struct ExpansionPlan {
     const int32_t nR = nR_, n_terms = n_terms_;
     MQCT_ARG_CHECK(sys && ind_mat && R && a_top, "null argument");
     const int type = sys->sys_type;
-    MQCT_ARG_CHECK(type == 7 || type == 8 || type == 0,
-                   "the expansion path supports SYS_TYPE 7, 8 and 0 (got %d)", type);
+    MQCT_ARG_CHECK(type == 1 || type == 4 || type == 7 || type == 8 || type == 0,
+                   "the expansion path supports SYS_TYPE 1, 4, 7, 8 and 0 (got %d)", type);
+    if (type == 1 || type == 4)
+      return init_atom(sys, ind_mat, P_, R, nR_, n_terms_, a_top, mij_cutoff_cm, r_cut1, r_cut2);
     MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->indx_chann && sys->j12 && sys->m12 &&
                        sys->n_states > 0 && (type == 7 || (sys->vec1 && sys->ldv > 0)) &&
                        (type != 0 || sys->vec2) && (type != 7 || (sys->ka1 && sys->kc1)),
@@ -1802,7 +1949,7 @@ struct ExpansionPlan {
     if (ident) {
       // per channel: p_inv kappa (pot_comp.f:70-110, matrix_ini.f:9147-9190) and whether the
       // two rotors are in the same level
-      identical = true;
+      a_stored = true;
       std::vector<int> pk(n_ch), same(n_ch);
       for (int c = 0; c < n_ch; ++c) {
         int par[2] = {1, 1};
@@ -1883,7 +2030,7 @@ struct ExpansionPlan {
     MQCT_ARG_CHECK(d_terms && d_mat && d_sk, "null argument");
     MQCT_ARG_CHECK(e_unit > 0.0, "e_unit must be positive");
     MQCT_CUDA_TRY(cudaEventRecord(ev[2], st));
-    if (identical)
+    if (a_stored)
       expansion_contract_a_kernel<<<(unsigned)P, 128, sizeof(double) * (size_t)n_terms, st>>>(
           n_terms, nR, d_A.p, d_terms, d_M.p);
     else

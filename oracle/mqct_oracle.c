@@ -1520,6 +1520,82 @@ int orc_expansion_matrix_type8(const orc_system* sys, const int32_t* indx_chann,
   return 0;
 }
 
+/* EXPANSION_MATRIX_ELEMENT for a rotor and an atom (SRC/pot_comp.f:6551-6622 SYS_TYPE 1,
+ * :6846-6954 SYS_TYPE 3, :6955-7075 SYS_TYPE 4): for the pair (st', st''), j', j'' the
+ * rotor levels and m the pair's m12,
+ *   M = e_unit sqrt((2j'+1)/(2j''+1)) sum_t T_t(R) sqrt((2l+1)/4pi) <j' m l 0|j'' m> S_t
+ * with S_t = <j' 0 l 0|j'' 0> (type 1), the K-sum over the rotor vectors
+ * sum_{+-nju} phase (-1)^nju sum_K <j' K l nju|j'' K+nju> c'_K c''_{K+nju} (type 4: phase 1
+ * for +nju, (-1)^nju for -nju) or the same over the parity-adapted symmetric-top
+ * components with 1/sqrt(2(1+d_k'0) 2(1+d_k''0)) (type 3, whose -nju branch carries the
+ * factor (-1)**(-1)**nju = -1 as written there).  Terms nR x n_terms, labels 5 per term
+ * (l, nju, ...). */
+int orc_expansion_matrix_atom(const orc_system* sys, const int32_t* indx_chann,
+                              const int32_t* j12, const int32_t* m12, int64_t P,
+                              const int32_t* ind_mat, int n_terms, const int32_t* a_top, int nR,
+                              const double* terms, double e_unit, double* mat) {
+  const int type = sys->sys_type;
+  if (type != 1 && type != 3 && type != 4) return -1;
+  if (type == 4 && !sys->vec1) return -1;
+  if (type == 3 && (!sys->ka1 || !sys->kc1)) return -1;
+  (void)j12;
+#pragma omp parallel for schedule(dynamic)
+  for (int64_t k = 0; k < P; ++k) {
+    const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
+    const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
+    const int jp = sys->j1[cp], jpp = sys->j1[cpp], m = m12[sp];
+    const double coef1 = sqrt((2.0 * jp + 1.0) / (2.0 * jpp + 1.0));
+    double* out = mat + (size_t)k * nR;
+    for (int i = 0; i < nR; ++i) out[i] = 0.0;
+    for (int t = 0; t < n_terms; ++t) {
+      const int l = a_top[5 * t], nju0 = type == 1 ? 0 : a_top[5 * t + 1];
+      if (!orc_triangle(jpp, l, jp)) continue;
+      const double coef2 = sqrt((2.0 * l + 1.0) / (4.0 * ORC_PI));
+      const double cg_m = orc_cg(jp, l, jpp, m, 0, m);
+      double S = 0.0;
+      if (type == 1) {
+        S = orc_cg(jp, l, jpp, 0, 0, 0);
+      } else if (type == 4) {
+        const double* vp = sys->vec1 + (size_t)cp * sys->ldv;
+        const double* vpp = sys->vec1 + (size_t)cpp * sys->ldv;
+        for (int planar = 0; planar < (nju0 == 0 ? 1 : 2); ++planar) {
+          const double phase = planar ? ((nju0 % 2) ? -1.0 : 1.0) : 1.0;
+          const int nju = planar ? -nju0 : nju0;
+          const double sg = (abs(nju) % 2) ? -1.0 : 1.0;
+          for (int kp = -jp; kp <= jp; ++kp) {
+            const int kpp = kp + nju;
+            if (abs(kpp) > jpp) continue;
+            S += phase * sg * orc_cg(jp, l, jpp, kp, nju, kpp) * vp[jp + kp] * vpp[jpp + kpp];
+          }
+        }
+      } else {  /* type 3: channel (j, k, eps) */
+        const int kc_p = sys->ka1[cp], kc_pp = sys->ka1[cpp];
+        const int ep = sys->kc1[cp], epp = sys->kc1[cpp];
+        const double norm = 1.0 / sqrt(2.0 * (1.0 + (kc_p == 0)) * 2.0 * (1.0 + (kc_pp == 0)));
+        for (int planar = 0; planar < (nju0 == 0 ? 1 : 2); ++planar) {
+          const double phase = planar ? -1.0 : 1.0;
+          const int nju = planar ? -nju0 : nju0;
+          const double sg = (abs(nju) % 2) ? -1.0 : 1.0;
+          for (int par_p = 0; par_p < 2; ++par_p)
+            for (int par_pp = 0; par_pp < 2; ++par_pp) {
+              const int kp = par_p ? -kc_p : kc_p, kpp = par_pp ? -kc_pp : kc_pp;
+              if (kpp != kp + nju) continue;
+              const double sp_ = (par_p && (ep % 2)) ? -1.0 : 1.0;
+              const double spp_ = (par_pp && (epp % 2)) ? -1.0 : 1.0;
+              S += phase * sg * orc_cg(jp, l, jpp, kp, nju, kpp) * sp_ * spp_;
+            }
+        }
+        S *= norm;
+      }
+      const double a = coef2 * cg_m * S;
+      if (a == 0.0) continue;
+      for (int i = 0; i < nR; ++i) out[i] += terms[(size_t)i * n_terms + t] * a;
+    }
+    for (int i = 0; i < nR; ++i) out[i] *= coef1 * e_unit;
+  }
+  return 0;
+}
+
 /* ---------------------------------------------------------------------- */
 /* SRC/pot_comp.f:8257-8746 (EXPANSION_MATRIX_ELEMENT, SYS_TYPE 0, two asymmetric
  * tops, partners distinguishable: the CG_jk_1 / M_coulp_1 branch).  For the pair

@@ -215,6 +215,14 @@ int orc_expansion_matrix_type0_identical(const orc_system* sys, const int32_t* i
 /* Inversion parity p1 p2 of a channel from its rotor vectors (SRC/pot_comp.f:70-110). */
 int orc_parity_inversion(const double* v1, int j1, const double* v2, int j2);
 
+/* EXPANSION_MATRIX_ELEMENT for a rotor and an atom, SYS_TYPE 1, 3 and 4
+ * (SRC/pot_comp.f:6551-7075); terms nR x n_terms in units of e_unit Hartree, a_top 5
+ * per term (l, nju, ...). */
+int orc_expansion_matrix_atom(const orc_system* sys, const int32_t* indx_chann,
+                              const int32_t* j12, const int32_t* m12, int64_t P,
+                              const int32_t* ind_mat, int n_terms, const int32_t* a_top, int nR,
+                              const double* terms, double e_unit, double* mat);
+
 /* EXPANSION_TERM and CALC_EXPANSION_TERMS for SYS_TYPE 7, 8 and 0
  * (SRC/pot_comp.f:3739-3896, 4695-6274): the term's angular function, and the
  * quadrature projection of V[iR][alpha2][beta1][beta2][gamma1][gamma2] onto the terms

@@ -127,6 +127,9 @@ def lib():
                                                           C.c_int64, C.c_void_p, C.c_int,
                                                           C.c_void_p, C.c_int, C.c_void_p,
                                                           C.c_double, C.c_void_p]
+        L.orc_expansion_matrix_atom.argtypes = [C.POINTER(System)] + [C.c_void_p] * 3 + [C.c_int64, C.c_void_p, C.c_int,
+                                                C.c_void_p, C.c_int, C.c_void_p, C.c_double,
+                                                C.c_void_p]
         L.orc_expansion_term.argtypes = [C.c_int] * 6 + [C.c_double] * 5 + [
             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_project_terms.argtypes = [C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 7 + [
@@ -400,6 +403,25 @@ def expansion_matrix_type8(osys, states, ind, labels, terms):
                                           _ptr(labels.reshape(-1)), nR, _ptr(terms), _ptr(mat))
     if rc:
         raise RuntimeError(f"orc_expansion_matrix_type8 failed: {rc}")
+    return mat.reshape(P, nR)
+
+
+def expansion_matrix_atom(osys, states, ind, labels, terms, e_unit):
+    """SYS_TYPE 1, 3 or 4 matrix (P x nR, Hartree) from PES expansion terms (nR x n_terms in
+    the unit e_unit Hartree); labels: one row per term, (l,) or (l, nju)."""
+    ic, j12, m12, _ = states
+    ind = np.ascontiguousarray(ind, np.int32)
+    lab = np.asarray(labels, np.int32).reshape(len(labels), -1)
+    a_top = np.zeros((len(lab), 5), np.int32)
+    a_top[:, :lab.shape[1]] = lab
+    terms = np.ascontiguousarray(terms, np.float64)
+    P, nR = ind.shape[0], terms.shape[0]
+    mat = np.zeros(P * nR)
+    rc = lib().orc_expansion_matrix_atom(C.byref(osys.s), _ptr(ic), _ptr(j12), _ptr(m12), P,
+                                         _ptr(ind.reshape(-1)), len(lab), _ptr(a_top.reshape(-1)),
+                                         nR, _ptr(terms), e_unit, _ptr(mat))
+    if rc:
+        raise RuntimeError(f"orc_expansion_matrix_atom failed: {rc}")
     return mat.reshape(P, nR)
 
 

@@ -1,0 +1,55 @@
+"""GPU parity of the rotor + atom expansion build (SYS_TYPE 1 and 4,
+mqct_build_matrix_expansion) with the oracle restatement, and the cross-path check of
+tests/test_oracle_expansion_atom.py through the GPU's direct build (FP64) and expansion
+build: both within 1e-10 of the largest element."""
+import numpy as np
+import pytest
+
+from mqct_b200 import synthetic as syn
+from test_oracle_expansion_atom import CASES, CM, oracle_system, term_table
+
+pytestmark = pytest.mark.gpu
+
+
+def test_type4_expansion_matches_oracle(mq, oracle, gpu_available):
+    chans = [c for c in syn.config_c2()["channels"] if c[0] <= 6]
+    s = mq.CollisionSystem(4, chans, A=27.9, B=14.5, C=9.3)
+    ch = s.channels
+    osys = oracle.OracleSystem(4, ch[:, 0], ch[:, 1], ch[:, 2], e_ch=s.e_ch,
+                               vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    labels = [(l, nu) for l in range(7) for nu in range(l + 1)]
+    R = mq.r_grid(40, 3.0, 20.0)
+    rng = np.random.default_rng(8)
+    T = rng.normal(size=(len(R), len(labels))) * np.exp(-R)[:, None] * 1e4
+    m, y2, sk = mq.build_matrix_expansion(s, R, labels, T, mij_cutoff=0.0)
+    mo = oracle.expansion_matrix_atom(osys, osys.states(), s.ind_mat, labels, T, CM)
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+    assert not sk.any()
+
+
+def test_type1_expansion_matches_oracle(mq, oracle, gpu_available):
+    c1 = syn.config_c1()
+    s = mq.CollisionSystem(1, c1["channels"], BE=c1["BE"])
+    osys = oracle.OracleSystem(1, s.channels[:, 0], e_ch=s.e_ch)
+    labels = [(l,) for l in range(9)]
+    R = mq.r_grid(60, 3.0, 20.0)
+    T = np.random.default_rng(1).normal(size=(len(R), len(labels))) * 100.0
+    m, _, _ = mq.build_matrix_expansion(s, R, labels, T, mij_cutoff=0.0)
+    mo = oracle.expansion_matrix_atom(osys, osys.states(), s.ind_mat, labels, T, CM)
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+
+
+@pytest.mark.parametrize("sys_type", [4, 1])
+def test_direct_and_expansion_builds_agree_on_gpu(mq, oracle, gpu_available, sys_type):
+    case = CASES[sys_type]
+    s, _ = oracle_system(mq, oracle, sys_type, case)
+    W = term_table(oracle, case["labels"], case["grid"], sys_type)
+    R = np.array([5.0, 6.0, 7.0])
+    v = np.random.default_rng(2).normal(size=(len(case["labels"]), len(R))) * 100
+    V = np.einsum("tr,t...->r...", v, W)
+    nb, ng = case["grid"]
+    grid = (nb, ng, 0, 0, 0, 0, 1) if sys_type == 4 else (nb, 0, 0, 0, 0, 0, 1)
+    pes = dict(kind=mq._abi.PES_TABLE, n_terms=0, params=np.zeros(1), table=V.reshape(-1))
+    direct, _, _ = mq.build_matrix(s, R, grid, pes, precision=mq.PREC_FP64, mij_cutoff=0.0)
+    expan, _, _ = mq.build_matrix_expansion(s, R, case["labels"], v.T, mij_cutoff=0.0)
+    assert np.max(np.abs(direct - expan)) <= 1e-10 * np.abs(direct).max()
