@@ -834,6 +834,11 @@ def _a_top(labels):
 
 
 def _projection_grid(V, sys_type, eq_gamma):
+    if sys_type in (1, 4):
+        if V.ndim != (2 if sys_type == 1 else 3):
+            raise ValueError("V must be (nR, n_beta) for SYS_TYPE 1, (nR, n_beta, n_gamma) for 4")
+        return _abi.Grid(V.shape[1], V.shape[2] if sys_type == 4 else 0, 0, 0, 0, 0,
+                         1 if eq_gamma else 0)
     nR, n2, n3, n4, n5 = V.shape[:5]
     n6 = V.shape[5] if sys_type == 0 else 0
     if sys_type == 0 and V.ndim != 6 or sys_type != 0 and V.ndim != 5:
@@ -843,9 +848,9 @@ def _projection_grid(V, sys_type, eq_gamma):
 
 def project_terms(sys_type, labels, V, eq_gamma=True, identical=False):
     """CALC_EXPANSION_TERMS on the GPU: project V, tabulated on the angular grid as
-    (nR, n_alpha2, n_beta1, n_beta2, n_gamma1) for SYS_TYPE 7 and 8 or with a trailing
-    n_gamma2 axis for SYS_TYPE 0, onto the terms (rows (l1, nju1, l2, l) or
-    (l1, nju1, l2, nju2, l)).  Returns (terms, terms_im), nR x n_terms each, the rows of
+    (nR, n_beta) for SYS_TYPE 1, (nR, n_beta, n_gamma) for 4, (nR, n_alpha2, n_beta1,
+    n_beta2, n_gamma1) for 7 and 8 or with a trailing n_gamma2 axis for 0, onto the terms
+    (rows (l,), (l, nju), (l1, nju1, l2, l) or (l1, nju1, l2, nju2, l)).  Returns (terms, terms_im), nR x n_terms each, the rows of
     PES_EXPAN_TERMS.DAT in the unit of V."""
     a_top = _a_top(labels)
     V = np.ascontiguousarray(V, np.float64)
@@ -865,11 +870,17 @@ class ProjectionPlan:
     ExpansionPlan.execute takes)."""
 
     def __init__(self, sys_type, labels, grid_shape, eq_gamma=True, identical=False):
-        """grid_shape: (n_alpha2, n_beta1, n_beta2, n_gamma1[, n_gamma2])."""
+        """grid_shape: (n_beta,) for SYS_TYPE 1, (n_beta, n_gamma) for 4, (n_alpha2,
+        n_beta1, n_beta2, n_gamma1[, n_gamma2]) for 7, 8 and 0."""
         a_top = _a_top(labels)
         self.n_terms = len(a_top)
-        gs = tuple(grid_shape) + ((0,) if len(grid_shape) == 4 else ())
-        self.grid = _abi.Grid(gs[1], gs[3], 0, gs[2], gs[0], gs[4], 1 if eq_gamma else 0)
+        if sys_type in (1, 4):
+            gs = tuple(grid_shape) + (0,)
+            self.grid = _abi.Grid(gs[0], gs[1] if sys_type == 4 else 0, 0, 0, 0, 0,
+                                  1 if eq_gamma else 0)
+        else:
+            gs = tuple(grid_shape) + ((0,) if len(grid_shape) == 4 else ())
+            self.grid = _abi.Grid(gs[1], gs[3], 0, gs[2], gs[0], gs[4], 1 if eq_gamma else 0)
         h = _abi.vp()
         check(lib().mqct_projection_plan_create(int(sys_type), self.n_terms, a_top.reshape(-1),
                                                 C.byref(self.grid), 1 if identical else 0,

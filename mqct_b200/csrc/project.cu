@@ -236,6 +236,15 @@ __global__ void proj_terms_kernel(const double2* __restrict__ K, int nR, int r0,
 // when l1 = l2, and the exchange (l1, nju1) <-> (l2, nju2) counting as the same.  Beyond
 // the reference: |nju| <= l (the D function is undefined otherwise) and l <= kMaxL.
 int check_terms(int sys_type, int n_terms, const int32_t* a_top, int identical) {
+  if (sys_type == 1 || sys_type == 4) {  // (l) or (l, nju): nju >= 0 (pot_comp.f:5061-5066)
+    for (int t = 0; t < n_terms; ++t) {
+      const int l = a_top[5 * t], nju = sys_type == 4 ? a_top[5 * t + 1] : 0;
+      MQCT_ARG_CHECK(l >= 0 && l <= kMaxL, "term %d: l must be in 0..%d", t + 1, kMaxL);
+      MQCT_ARG_CHECK(nju >= 0, "term %d: the values of M1 should be always positive", t + 1);
+      MQCT_ARG_CHECK(nju <= l, "term %d: |nju| exceeds its l", t + 1);
+    }
+    return MQCT_OK;
+  }
   struct Lab {
     int l1, n1, l2, n2, l;
   };
@@ -310,11 +319,95 @@ struct mqct_projection_plan {
     if (st) cudaStreamDestroy(st);
   }
 
+  int upload_tables(const std::vector<double>& eb, const std::vector<double>& ab,
+                    const std::vector<double>& ta, const std::vector<double>& tb,
+                    const std::vector<TermDev>& td) {
+    MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& x : ev) MQCT_CUDA_TRY(cudaEventCreate(&x));
+    MQCT_CUDA_TRY(Eb.upload(eb, st));
+    MQCT_CUDA_TRY(Ab.upload(ab, st));
+    MQCT_CUDA_TRY(A.upload(ta, st));
+    MQCT_CUDA_TRY(B.upload(tb, st));
+    MQCT_CUDA_TRY(terms.upload(td, st));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(st));
+    return MQCT_OK;
+  }
+
+  // SYS_TYPE 1 (diatom + atom, V_2_1(n_beta, n_r)) and 4 (top + atom, V_3_1(n_gamma,
+  // n_beta, n_r)), CALC_EXPANSION_TERMS cases 1 and 4 (pot_comp.f:4973-4999, 5054-5104):
+  //   type 1: terms = sum_beta WF_DIAT_TOP(l, 0; beta) V wb sin(beta) xbl 2 pi
+  //   type 4: terms = sum_{beta,gamma} Re((-1)^nju WF_DIAT_TOP(l, nju; beta, gamma)) V wb wg
+  //           sin(beta) xbl xgl
+  // in the same contractions with the alpha2 and beta2 axes of one point and m = l2 = 0.
+  int init_atom(int sys, int nt, const int32_t* a_top, const mqct_grid_t& g) {
+    n_b1 = g.n_beta;
+    n_g1 = sys == 4 ? g.n_gamma : 1;
+    n_a2 = n_b2 = n_g2 = 1;
+    MQCT_ARG_CHECK(n_b1 > 0 && n_b1 <= 4096 && n_g1 > 0 && n_g1 <= 4096,
+                   "grid sizes must be in 1..4096 (beta %d, gamma %d)", n_b1, n_g1);
+    int rc = check_terms(sys, nt, a_top, 0);
+    if (rc != MQCT_OK) return rc;
+    J = n_b1;
+    L = n_g1;
+    if (mqct_device_count() <= 0) {
+      set_error("no CUDA device available");
+      return MQCT_E_NODEV;
+    }
+    const Axis b1 = axis_gl(n_b1, 0.0, kPi);
+    const Axis g1 = g.eq_gamma ? axis_mid(n_g1, 0.0, 2.0 * kPi) : axis_gl(n_g1, 0.0, 2.0 * kPi);
+    std::vector<double> lf(128);
+    lf[0] = 0.0;
+    for (int i = 1; i < 128; ++i) lf[i] = lf[i - 1] + std::log((double)i);
+    std::vector<int> nus;
+    std::vector<TermDev> td(nt);
+    for (int t = 0; t < nt; ++t) {
+      const int nju = sys == 4 ? a_top[5 * t + 1] : 0;
+      auto it = std::find(nus.begin(), nus.end(), nju);
+      td[t].pair = (int)(it - nus.begin());
+      if (it == nus.end()) nus.push_back(nju);
+      td[t].l2 = 0;
+      td[t].m_lo = td[t].m_hi = 0;
+    }
+    P = (int)nus.size();
+    n_m = 1;
+    n_l2 = 1;
+    Lp = (L + 3) / 4 * 4;
+    n_pt = (P + 3) / 4;
+    std::vector<double> eb((size_t)(n_pt + 3) / 4 * 4 * Lp * 8, 0.0);
+    for (int i = 0; i < n_g1; ++i)
+      for (int p = 0; p < P; ++p) {
+        const double w = sys == 4 ? g1.w[i] * g1.half : 1.0;
+        const double ph = sys == 4 ? nus[p] * g1.x[i] : 0.0;
+        double* d = &eb[((size_t)(p / 4) * Lp + i) * 8 + 2 * (p % 4)];
+        d[0] = std::cos(ph) * w;
+        d[1] = std::sin(ph) * w;
+      }
+    K2p = 4;  // one alpha2 point of unit weight: H = F
+    n_mt = 1;
+    std::vector<double> ab((size_t)8 * K2p * 8, 0.0);
+    ab[(size_t)0 * 8 + 0] = 1.0;  // row 0 (Re), column 0 (Re)
+    ab[(size_t)1 * 8 + 1] = 1.0;  // row 1 (Im), column 1 (Im)
+    std::vector<double> ta((size_t)nt * n_b1), tb((size_t)P, 1.0);
+    for (int t = 0; t < nt; ++t) {
+      const int l = a_top[5 * t], nju = sys == 4 ? a_top[5 * t + 1] : 0;
+      const double nrm = std::sqrt((2.0 * l + 1.0) / 4.0 / kPi * std::exp(lf[l - nju] - lf[l + nju]));
+      const double sg = (sys == 4 && (nju & 1)) ? -1.0 : 1.0;
+      const double tail = sys == 1 ? 2.0 * kPi : 1.0;
+      for (int i = 0; i < n_b1; ++i)
+        ta[(size_t)t * n_b1 + i] = sg * mqct_dev::plgndr(l, nju, std::cos(b1.x[i])) * nrm *
+                                   b1.w[i] * std::sin(b1.x[i]) * b1.half * tail;
+    }
+    return upload_tables(eb, ab, ta, tb, td);
+  }
+
   int init(int sys, int nt, const int32_t* a_top, const mqct_grid_t& g, int identical) {
-    MQCT_ARG_CHECK(sys == 7 || sys == 8 || sys == 0,
-                   "the projection is built for SYS_TYPE 7, 8 and 0 (got %d)", sys);
+    MQCT_ARG_CHECK(sys == 1 || sys == 4 || sys == 7 || sys == 8 || sys == 0,
+                   "the projection is built for SYS_TYPE 1, 4, 7, 8 and 0 (got %d)", sys);
     MQCT_ARG_CHECK(nt > 0 && a_top, "no terms");
     MQCT_ARG_CHECK(!identical || sys == 0, "identical partners are SYS_TYPE 0");
+    sys_type = sys;
+    n_terms = nt;
+    if (sys == 1 || sys == 4) return init_atom(sys, nt, a_top, g);
     sys_type = sys;
     n_terms = nt;
     n_a2 = g.n_alpha2;
@@ -446,15 +539,7 @@ struct mqct_projection_plan {
                 bv * b2.w[i] * std::sin(b2.x[i]) * b2.half;
           }
         }
-    MQCT_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    for (auto& x : ev) MQCT_CUDA_TRY(cudaEventCreate(&x));
-    MQCT_CUDA_TRY(Eb.upload(eb, st));
-    MQCT_CUDA_TRY(Ab.upload(ab, st));
-    MQCT_CUDA_TRY(A.upload(ta, st));
-    MQCT_CUDA_TRY(B.upload(tb, st));
-    MQCT_CUDA_TRY(terms.upload(td, st));
-    MQCT_CUDA_TRY(cudaStreamSynchronize(st));
-    return MQCT_OK;
+    return upload_tables(eb, ab, ta, tb, td);
   }
 
   // R points per pass so that F, H and K stay within 4 GiB.

@@ -2017,3 +2017,56 @@ int orc_project_terms(int sys_type, int n_terms, const int32_t* a_top, int n_alp
   free(xaa); free(waa);
   return 0;
 }
+
+/* CALC_EXPANSION_TERMS for a rotor and an atom (SRC/pot_comp.f:4973-4999 SYS_TYPE 1,
+ * 5054-5104 SYS_TYPE 4; EXPANSION_TERM :3756-3768): V[iR][beta] (V_2_1) or
+ * V[iR][beta][gamma] (V_3_1), terms[t * nR + iR] the real part as the reference sums it,
+ * terms_im the imaginary part. */
+int orc_project_terms_atom(int sys_type, int n_terms, const int32_t* a_top, int n_beta,
+                           int n_gamma, int eq_gamma, int nR, const double* V, double* terms,
+                           double* terms_im) {
+  if (sys_type != 1 && sys_type != 4) return -1;
+  if (sys_type == 1) n_gamma = 1;
+  double* xb = (double*)malloc(sizeof(double) * n_beta);
+  double* wb = (double*)malloc(sizeof(double) * n_beta);
+  double* xg = (double*)malloc(sizeof(double) * n_gamma);
+  double* wg = (double*)malloc(sizeof(double) * n_gamma);
+  orc_gauleg(n_beta, xb, wb);
+  const double xbm = 0.5 * ORC_PI, xbl = 0.5 * ORC_PI, xgm = ORC_PI, xgl = ORC_PI;
+  if (eq_gamma) {
+    for (int i = 0; i < n_gamma; ++i) { xg[i] = (i + 0.5) * 2.0 * xgl / n_gamma; wg[i] = 2.0 / n_gamma; }
+  } else {
+    orc_gauleg(n_gamma, xg, wg);
+    for (int i = 0; i < n_gamma; ++i) xg[i] = xgm + xgl * xg[i];
+  }
+#pragma omp parallel for collapse(2) schedule(dynamic)
+  for (int t = 0; t < n_terms; ++t)
+    for (int iR = 0; iR < nR; ++iR) {
+      const int l = a_top[5 * t], nju = sys_type == 4 ? a_top[5 * t + 1] : 0;
+      double ir = 0.0, ii = 0.0;
+      for (int i2 = 0; i2 < n_beta; ++i2) {
+        const double beta = xbm + xbl * xb[i2];
+        if (sys_type == 1) {
+          double wfr, wfi;
+          orc_wf_diat(l, 0, beta, 0.0, &wfr, &wfi);
+          const double v = V[(size_t)iR * n_beta + i2];
+          ir += (wfr * v) * wb[i2] * sin(beta) * xbl * 2.0 * ORC_PI;
+          ii += (wfi * v) * wb[i2] * sin(beta) * xbl * 2.0 * ORC_PI;
+          continue;
+        }
+        for (int i3 = 0; i3 < n_gamma; ++i3) {
+          double dwr, dwi;
+          orc_wf_diat(l, nju, beta, xg[i3], &dwr, &dwi);
+          const double sg = (nju % 2) ? -1.0 : 1.0;
+          const double v = V[((size_t)iR * n_beta + i2) * n_gamma + i3];
+          ir += dwr * sg * v * wb[i2] * wg[i3] * sin(beta) * xbl * xgl;
+          ii += dwi * sg * v * wb[i2] * wg[i3] * sin(beta) * xbl * xgl;
+        }
+      }
+      terms[(size_t)t * nR + iR] = ir;
+      if (terms_im) terms_im[(size_t)t * nR + iR] = ii;
+    }
+  free(xb); free(wb); free(xg); free(wg);
+  return 0;
+}
+

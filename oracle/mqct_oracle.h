@@ -234,6 +234,12 @@ int orc_project_terms(int sys_type, int n_terms, const int32_t* a_top, int n_alp
                       int n_beta1, int n_beta2, int n_gamma1, int n_gamma2, int eq_gamma, int nR,
                       const double* V, double* terms, double* terms_im);
 
+/* CALC_EXPANSION_TERMS for SYS_TYPE 1 (V[iR][beta]) and 4 (V[iR][beta][gamma])
+ * (SRC/pot_comp.f:4973-4999, 5054-5104); terms[t * nR + iR]. */
+int orc_project_terms_atom(int sys_type, int n_terms, const int32_t* a_top, int n_beta,
+                           int n_gamma, int eq_gamma, int nR, const double* V, double* terms,
+                           double* terms_im);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,6 +130,8 @@ def lib():
         L.orc_expansion_matrix_atom.argtypes = [C.POINTER(System)] + [C.c_void_p] * 3 + [C.c_int64, C.c_void_p, C.c_int,
                                                 C.c_void_p, C.c_int, C.c_void_p, C.c_double,
                                                 C.c_void_p]
+        L.orc_project_terms_atom.argtypes = [C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 4 + [
+            C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_expansion_term.argtypes = [C.c_int] * 6 + [C.c_double] * 5 + [
             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_project_terms.argtypes = [C.c_int, C.c_int, C.c_void_p] + [C.c_int] * 7 + [
@@ -487,6 +489,24 @@ def expansion_term(sys_type, l, l1, l2, nju1, nju2, beta1, gamma1, alpha2, beta2
     lib().orc_expansion_term(sys_type, l, l1, l2, nju1, nju2, beta1, gamma1, alpha2, beta2, gamma2,
                              C.byref(r), C.byref(i))
     return r.value, i.value
+
+
+def project_terms_atom(sys_type, labels, V, eq_gamma=True):
+    """CALC_EXPANSION_TERMS for SYS_TYPE 1 (V: nR x n_beta) and 4 (V: nR x n_beta x
+    n_gamma); labels (l,) or (l, nju).  Returns (terms, terms_im), n_terms x nR."""
+    lab = np.asarray(labels, np.int32).reshape(len(labels), -1)
+    a_top = np.zeros((len(lab), 5), np.int32)
+    a_top[:, :lab.shape[1]] = lab
+    V = np.ascontiguousarray(V, np.float64)
+    nR, nb = V.shape[:2]
+    ng = V.shape[2] if V.ndim == 3 else 1
+    T = np.zeros(nR * len(lab))
+    Ti = np.zeros(nR * len(lab))
+    rc = lib().orc_project_terms_atom(sys_type, len(lab), _ptr(a_top.reshape(-1)), nb, ng,
+                                      1 if eq_gamma else 0, nR, _ptr(V), _ptr(T), _ptr(Ti))
+    if rc:
+        raise RuntimeError(f"orc_project_terms_atom failed: {rc}")
+    return T.reshape(len(lab), nR), Ti.reshape(len(lab), nR)
 
 
 def project_terms(sys_type, labels, V, eq_gamma=True):

@@ -53,3 +53,37 @@ def test_direct_and_expansion_builds_agree_on_gpu(mq, oracle, gpu_available, sys
     direct, _, _ = mq.build_matrix(s, R, grid, pes, precision=mq.PREC_FP64, mij_cutoff=0.0)
     expan, _, _ = mq.build_matrix_expansion(s, R, case["labels"], v.T, mij_cutoff=0.0)
     assert np.max(np.abs(direct - expan)) <= 1e-10 * np.abs(direct).max()
+
+
+@pytest.mark.parametrize("sys_type,shape,eq", [(4, (3, 20, 16), True), (4, (2, 12, 9), False),
+                                               (1, (4, 30), True)])
+def test_atom_projection_matches_oracle(mq, oracle, gpu_available, sys_type, shape, eq):
+    labels = CASES[sys_type]["labels"]
+    V = np.random.default_rng(9).normal(size=shape) * 1e3 + 20.0
+    T, Ti = mq.project_terms(sys_type, labels, V, eq_gamma=eq)
+    To, Tio = oracle.project_terms_atom(sys_type, labels, V, eq_gamma=eq)
+    bound = 1e-12 * np.abs(V).max() * 4 * np.pi
+    assert np.max(np.abs(T - To.T)) <= bound and np.max(np.abs(Ti - Tio.T)) <= bound
+
+
+@pytest.mark.parametrize("sys_type", [4, 1])
+def test_atom_projection_to_matrix_pipeline(mq, oracle, gpu_available, sys_type):
+    """PES table -> projected terms -> expansion matrix, all on the GPU, against the
+    direct build of the same table: equal for type 1; for type 4 after reversing the
+    sign of the odd-nju terms (the projection's (-1)^nju, see the oracle tests)."""
+    case = CASES[sys_type]
+    s, _ = oracle_system(mq, oracle, sys_type, case)
+    W = term_table(oracle, case["labels"], case["grid"], sys_type)
+    R = np.array([5.0, 7.0])
+    v = np.random.default_rng(2).normal(size=(len(case["labels"]), len(R))) * 100
+    V = np.einsum("tr,t...->r...", v, W)
+    T, _ = mq.project_terms(sys_type, case["labels"], V)
+    if sys_type == 4:
+        T = T * np.array([(-1.0) ** lab[1] for lab in case["labels"]])[None, :]
+    assert np.allclose(T, v.T, rtol=0, atol=1e-10 * np.abs(v).max())
+    nb, ng = case["grid"]
+    grid = (nb, ng, 0, 0, 0, 0, 1) if sys_type == 4 else (nb, 0, 0, 0, 0, 0, 1)
+    pes = dict(kind=mq._abi.PES_TABLE, n_terms=0, params=np.zeros(1), table=V.reshape(-1))
+    direct, _, _ = mq.build_matrix(s, R, grid, pes, precision=mq.PREC_FP64, mij_cutoff=0.0)
+    expan, _, _ = mq.build_matrix_expansion(s, R, case["labels"], T, mij_cutoff=0.0)
+    assert np.max(np.abs(direct - expan)) <= 1e-10 * np.abs(direct).max()

@@ -87,3 +87,20 @@ def test_type1_term_is_the_gaunt_coefficient(mq, oracle):
         want = (np.sqrt(5 / (4 * np.pi)) * np.sqrt((2 * jp + 1) / (2 * jpp + 1)) *
                 oracle.cg(jp, 2, jpp, mm, 0, mm) * oracle.cg(jp, 2, jpp, 0, 0, 0))
         assert abs(m[k, 0] - want) < 1e-14
+
+
+@pytest.mark.parametrize("sys_type", [4, 1])
+def test_projection_recovers_the_coefficients(oracle, sys_type):
+    """CALC_EXPANSION_TERMS cases 1 and 4: a PES built from the projection's own functions,
+    V = sum_t v_t W'_t with W'_t = Re((-1)^nju Y), doubled for nju != 0 (type 4), or Y
+    (type 1), projects back onto v_t: the functions are orthonormal on the sphere (case 1
+    supplies the azimuthal 2 pi of its beta-only grid)."""
+    case = CASES[sys_type]
+    W = term_table(oracle, case["labels"], case["grid"], sys_type)
+    if sys_type == 4:
+        sg = np.array([(-1.0) ** lab[1] for lab in case["labels"]])
+        W = W * sg[:, None, None]
+    v = np.random.default_rng(4).normal(size=(len(case["labels"]), 2)) * 50
+    V = np.einsum("tr,t...->r...", v, W)
+    T, _ = oracle.project_terms_atom(sys_type, case["labels"], V)
+    assert np.max(np.abs(T - v)) <= 1e-10 * np.abs(v).max()
