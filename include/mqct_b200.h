@@ -471,6 +471,33 @@ int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_ter
                                const int32_t* a_top, int32_t nR, const double* R,
                                const double* terms);
 
+/* The per-energy result files, appended block by block as the reference appends them:
+ *   mqct_write_opacity: OPACITY_FUNCTIONS_L.out and (path_total, may be NULL)
+ *     TOTAL_PROBABILITIES_L.out (MQCT_SOURCE_CODES/propagator.f:5837-5896): per trajectory
+ *     l / k_vec, l and the channel probabilities prob[t * n_ch + c]; the totals file the
+ *     sum over channels and the sum without chann_ini (1-based);
+ *   mqct_write_partial_j: PARTIAL_CROSS_SECTIONS_J.out (:4845-4868), per total J the
+ *     J-resolved cross sections partial[i * n_ch + c] in Angstrom^2;
+ *   mqct_write_m_proj: M_PROJ_CROSSECTIONS.out (:4870-4880), the cross sections of one
+ *     initial state without the Billing correction, Angstrom^2;
+ *   mqct_write_cross_sections: one energy block of CROSS_SECTIONS.out
+ *     (MQCT_SOURCE_CODES/print_output.f:46-101): sigma(U) = sigma_f / U * E_bill, E_bill
+ *     and sigma_f for the channels with exists[c] != 0 (all when exists is NULL), the
+ *     probability and, with with_e_err, energy conservation errors in percent;
+ *     mqct_write_cross_sections_footer: the closing trajectory count (:117-118). */
+int mqct_write_opacity(const char* path, const char* path_total, int32_t s_st, int32_t j12,
+                       int32_t m12, int32_t i_ener, double U_cm, int32_t n_traj, const int32_t* l,
+                       double k_vec, int32_t n_ch, const double* prob, int32_t chann_ini);
+int mqct_write_partial_j(const char* path, int32_t s_st, int32_t j12, int32_t m12,
+                         int32_t i_ener, double U_cm, int32_t n_J, const int32_t* J, int32_t n_ch,
+                         const double* partial);
+int mqct_write_m_proj(const char* path, int32_t s_st, int32_t i_ener, int32_t j12, int32_t m12,
+                      int32_t n_ch, const double* sigma);
+int mqct_write_cross_sections(const char* path, double U_cm, int32_t chann_ini, int32_t n_ch,
+                              const int32_t* exists, const double* sigma_f, const double* E_bill,
+                              double p_err_pct, int32_t with_e_err, double e_err_pct);
+int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
+
 /* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
  * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 7, 8 and 0: the
  * quadrature projection of the PES tabulated on the angular grid onto the expansion

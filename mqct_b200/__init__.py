@@ -911,3 +911,48 @@ class ProjectionPlan:
         except Exception:
             pass
 
+
+def write_opacity(path, s_st, j12, m12, i_ener, U_cm, l, k_vec, prob, path_total=None,
+                  chann_ini=1):
+    """Append one block to OPACITY_FUNCTIONS_L.out (and TOTAL_PROBABILITIES_L.out when
+    path_total is given): prob is n_traj x n_channels, l the trajectories' l."""
+    prob = np.ascontiguousarray(prob, np.float64)
+    li = np.ascontiguousarray(l, np.int32)
+    check(lib().mqct_write_opacity(path.encode(), path_total.encode() if path_total else None,
+                                   int(s_st), int(j12), int(m12), int(i_ener), float(U_cm),
+                                   len(li), li, float(k_vec), prob.shape[1], prob.reshape(-1),
+                                   int(chann_ini)))
+
+
+def write_partial_j(path, s_st, j12, m12, i_ener, U_cm, J, partial):
+    """Append one block to PARTIAL_CROSS_SECTIONS_J.out (partial: n_J x n_channels, A^2)."""
+    partial = np.ascontiguousarray(partial, np.float64)
+    Ji = np.ascontiguousarray(J, np.int32)
+    check(lib().mqct_write_partial_j(path.encode(), int(s_st), int(j12), int(m12), int(i_ener),
+                                     float(U_cm), len(Ji), Ji, partial.shape[1],
+                                     partial.reshape(-1)))
+
+
+def write_m_proj(path, s_st, i_ener, j12, m12, sigma):
+    """Append one block to M_PROJ_CROSSECTIONS.out (sigma per channel, A^2)."""
+    sigma = np.ascontiguousarray(sigma, np.float64)
+    check(lib().mqct_write_m_proj(path.encode(), int(s_st), int(i_ener), int(j12), int(m12),
+                                  len(sigma), sigma))
+
+
+def write_cross_sections(path, U_cm, chann_ini, sigma_f, E_bill, p_err_pct, e_err_pct=None,
+                         exists=None):
+    """Append one energy block to CROSS_SECTIONS.out."""
+    sigma_f = np.ascontiguousarray(sigma_f, np.float64)
+    E_bill = np.ascontiguousarray(E_bill, np.float64)
+    ex = None if exists is None else np.ascontiguousarray(exists, np.int32)
+    check(lib().mqct_write_cross_sections(path.encode(), float(U_cm), int(chann_ini),
+                                          len(sigma_f), None if ex is None else ex.ctypes.data,
+                                          sigma_f, E_bill, float(p_err_pct),
+                                          0 if e_err_pct is None else 1,
+                                          0.0 if e_err_pct is None else float(e_err_pct)))
+
+
+def write_cross_sections_footer(path, n_traj_total):
+    check(lib().mqct_write_cross_sections_footer(path.encode(), int(n_traj_total)))
+

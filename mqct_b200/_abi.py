@@ -101,6 +101,8 @@ EXPORTS = [
     "mqct_read_mtrx_dat", "mqct_read_expansion_terms", "mqct_write_expansion_terms",
     "mqct_projection_plan_create", "mqct_projection_plan_execute", "mqct_projection_plan_sync",
     "mqct_projection_plan_timing", "mqct_projection_plan_destroy", "mqct_project_terms",
+    "mqct_write_opacity", "mqct_write_partial_j", "mqct_write_m_proj",
+    "mqct_write_cross_sections", "mqct_write_cross_sections_footer",
 ]
 
 _lib = None
@@ -212,6 +214,14 @@ def lib():
     L.mqct_projection_plan_timing.argtypes = [vp] + [C.POINTER(C.c_float)] * 3
     L.mqct_projection_plan_destroy.argtypes = [vp]
     L.mqct_projection_plan_destroy.restype = None
+    L.mqct_write_opacity.argtypes = [C.c_char_p, C.c_char_p] + [C.c_int32] * 4 + [
+        C.c_double, C.c_int32, i32p, C.c_double, C.c_int32, f64p, C.c_int32]
+    L.mqct_write_partial_j.argtypes = [C.c_char_p] + [C.c_int32] * 4 + [
+        C.c_double, C.c_int32, i32p, C.c_int32, f64p]
+    L.mqct_write_m_proj.argtypes = [C.c_char_p] + [C.c_int32] * 5 + [f64p]
+    L.mqct_write_cross_sections.argtypes = [C.c_char_p, C.c_double, C.c_int32, C.c_int32, vp,
+                                            f64p, f64p, C.c_double, C.c_int32, C.c_double]
+    L.mqct_write_cross_sections_footer.argtypes = [C.c_char_p, C.c_int32]
     L.mqct_project_terms.argtypes = [C.c_int32, C.c_int32, i32p, C.POINTER(Grid), C.c_int32,
                                      C.c_int32, f64p, f64p, vp]
     _lib = L

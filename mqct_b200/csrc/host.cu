@@ -773,4 +773,148 @@ int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_ter
   return MQCT_OK;
 }
 
+// ---------------------------------------------------------------- result files
+// The reference's per-energy output files (MQCT_SOURCE_CODES/propagator.f:4843-4880,
+// 5830-5896; print_output.f:46-101), appended block by block as the reference appends.
+static FILE* open_append(const char* path) {
+  FILE* f = fopen(path, "a");
+  if (!f) set_error("cannot open %s", path);
+  return f;
+}
+
+static int close_checked(FILE* f, const char* path) {
+  if (fclose(f) != 0) {
+    set_error("write to %s failed", path);
+    return MQCT_E_IO;
+  }
+  return MQCT_OK;
+}
+
+// Fortran F0.3 of a value >= 0 as gfortran writes it.
+static std::string fortran_f0_3(double v) {
+  char buf[64];
+  snprintf(buf, sizeof buf, "%.3f", v);
+  return buf;
+}
+
+static void state_header(FILE* f, int32_t s_st, int32_t j12, int32_t m12, int32_t i_ener,
+                         double U_cm) {
+  fprintf(f, "STATE= %d\nj12= %d\nm12= %d\nENERGY#%d, U(i)= %s cm^-1\n", s_st, j12, m12, i_ener,
+          fortran_f0_3(U_cm).c_str());
+}
+
+// OPACITY_FUNCTIONS_L.out and TOTAL_PROBABILITIES_L.out (propagator.f:5837-5896): per
+// trajectory l / k, l and the channel probabilities; the totals file (path_total may be
+// NULL) the sum and the sum without the initial channel (chann_ini, 1-based).
+int mqct_write_opacity(const char* path, const char* path_total, int32_t s_st, int32_t j12,
+                       int32_t m12, int32_t i_ener, double U_cm, int32_t n_traj, const int32_t* l,
+                       double k_vec, int32_t n_ch, const double* prob, int32_t chann_ini) {
+  MQCT_ARG_CHECK(path && l && prob && n_traj > 0 && n_ch > 0 && k_vec > 0.0, "bad arguments");
+  MQCT_ARG_CHECK(!path_total || (chann_ini >= 1 && chann_ini <= n_ch), "chann_ini out of range");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  state_header(f, s_st, j12, m12, i_ener, U_cm);
+  for (int c = 1; c <= n_ch; ++c) {
+    if (c == 1) fprintf(f, "    %-8s   %-7s  ", "B_IMPACT", "     L ");
+    fprintf(f, "CHANNEL=%6d  ", c);
+  }
+  fprintf(f, "\n");
+  for (int t = 0; t < n_traj; ++t) {
+    fprintf(f, "%s %6d ", fortran_e(l[t] / k_vec, 15, 8).c_str(), l[t]);
+    for (int c = 0; c < n_ch; ++c)
+      fprintf(f, "%s ", fortran_e(prob[(size_t)t * n_ch + c], 15, 8).c_str());
+    fprintf(f, "\n");
+  }
+  fprintf(f, " \n");
+  int rc = close_checked(f, path);
+  if (rc || !path_total) return rc;
+  f = open_append(path_total);
+  if (!f) return MQCT_E_IO;
+  state_header(f, s_st, j12, m12, i_ener, U_cm);
+  fprintf(f, "B_IMPACT       %-7s %15s %16s\n", "     L ", "TOT_ELAST_PROB", "TOT_INELAST_PROB");
+  for (int t = 0; t < n_traj; ++t) {
+    double sum = 0.0;
+    for (int c = 0; c < n_ch; ++c) sum += prob[(size_t)t * n_ch + c];
+    fprintf(f, "%s %6d %s %s\n", fortran_e(l[t] / k_vec, 15, 8).c_str(), l[t],
+            fortran_e(sum, 15, 8).c_str(),
+            fortran_e(sum - prob[(size_t)t * n_ch + chann_ini - 1], 15, 8).c_str());
+  }
+  fprintf(f, " \n");
+  return close_checked(f, path_total);
+}
+
+// PARTIAL_CROSS_SECTIONS_J.out (propagator.f:4845-4868): per total J the J-resolved
+// cross sections of every channel, Angstrom^2.
+int mqct_write_partial_j(const char* path, int32_t s_st, int32_t j12, int32_t m12,
+                         int32_t i_ener, double U_cm, int32_t n_J, const int32_t* J, int32_t n_ch,
+                         const double* partial) {
+  MQCT_ARG_CHECK(path && J && partial && n_J > 0 && n_ch > 0, "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  state_header(f, s_st, j12, m12, i_ener, U_cm);
+  for (int c = 1; c <= n_ch; ++c) {
+    if (c == 1) fprintf(f, "%-7s  ", "J_TOTAL");
+    fprintf(f, "CHANNEL=%6d  ", c);
+  }
+  fprintf(f, "\n");
+  for (int i = 0; i < n_J; ++i) {
+    fprintf(f, "%5d   ", J[i]);
+    for (int c = 0; c < n_ch; ++c)
+      fprintf(f, "%s ", fortran_e(partial[(size_t)i * n_ch + c], 15, 8).c_str());
+    fprintf(f, "\n");
+  }
+  return close_checked(f, path);
+}
+
+// M_PROJ_CROSSECTIONS.out (propagator.f:4870-4880): the cross sections of one initial
+// state without the Billing correction, Angstrom^2.
+int mqct_write_m_proj(const char* path, int32_t s_st, int32_t i_ener, int32_t j12, int32_t m12,
+                      int32_t n_ch, const double* sigma) {
+  MQCT_ARG_CHECK(path && sigma && n_ch > 0, "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  fprintf(f, " M RESOLVED CROSSECTIONS WITHOUT BILLING CORRECTION\n");
+  fprintf(f, "%10s %4d\n%10s %4d\n", "INI_STATE#", s_st, "ENERGY#", i_ener);
+  fprintf(f, " j12=%12d\n m12=%12d\n", j12, m12);
+  fprintf(f, "%-8s %19s\n", "CHANNEL#", "CROSSSECTIONS,ANG^2");
+  for (int c = 0; c < n_ch; ++c) fprintf(f, "%4d      %s\n", c + 1, fortran_e(sigma[c], 18, 11).c_str());
+  return close_checked(f, path);
+}
+
+// One energy block of CROSS_SECTIONS.out (print_output.f:46-101): per final channel with
+// a Billing energy (exists[c] != 0, or every channel when exists is NULL) the initial and
+// final channel, sigma(U) = sigma_f / U * E_bill, E_bill and sigma_f (Angstrom^2, cm^-1);
+// then the probability conservation error and, when with_e_err, the energy conservation
+// error (percent), and a blank record.  mqct_write_cross_sections_footer appends the
+// closing trajectory count.
+int mqct_write_cross_sections(const char* path, double U_cm, int32_t chann_ini, int32_t n_ch,
+                              const int32_t* exists, const double* sigma_f, const double* E_bill,
+                              double p_err_pct, int32_t with_e_err, double e_err_pct) {
+  MQCT_ARG_CHECK(path && sigma_f && E_bill && n_ch > 0 && U_cm > 0.0, "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  fprintf(f, "U= %14.6f cm^-1\n", U_cm);
+  fprintf(f, "%6s  %6s  %19s  %14s  %19s\n", "ilv", "flv", "sigma(U),ANG^2", "E_coll,cm^-1",
+          "sigma(E_coll),ANG^2");
+  for (int c = 0; c < n_ch; ++c) {
+    if (exists && !exists[c]) continue;
+    fprintf(f, "%6d  %6d  %s  %14.6f  %s\n", chann_ini, c + 1,
+            fortran_e(sigma_f[c] / U_cm * E_bill[c], 19, 10).c_str(), E_bill[c],
+            fortran_e(sigma_f[c], 19, 10).c_str());
+  }
+  fprintf(f, "%-28s %s\n", "TOTAL P CONSERVATION ERROR,%", fortran_e(p_err_pct, 12, 5).c_str());
+  if (with_e_err)
+    fprintf(f, "%-28s %s\n", "TOTAL E CONSERVATION ERROR,%", fortran_e(e_err_pct, 12, 5).c_str());
+  fprintf(f, " \n");
+  return close_checked(f, path);
+}
+
+int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total) {
+  MQCT_ARG_CHECK(path, "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  fprintf(f, "TOTAL NUMBER OF TRAJECTORIES = %3d\n", n_traj_total);
+  return close_checked(f, path);
+}
+
 }  // extern "C"

@@ -174,6 +174,12 @@ def main(ref_root):
                         channels=np.array([[0, 0, 0], [1, 0, 1], [1, 1, 1]], dtype=np.int32),
                         e_ch_printed=np.array([0.000, 0.408, 0.844]),
                         opacity=opac4, deflection=defl4, sigma_U=np.array(sig4),
+                        # the result files as written (for the writers' byte-for-byte tests)
+                        **{"text_" + name.split(".")[0].lower(): np.array(
+                            open(os.path.join(d, name)).read())
+                           for name in ("OPACITY_FUNCTIONS_L.out", "TOTAL_PROBABILITIES_L.out",
+                                        "PARTIAL_CROSS_SECTIONS_J.out", "M_PROJ_CROSSECTIONS.out",
+                                        "CROSS_SECTIONS.out")},
                         # $SYSTEM of MF_He_CS_MQCT.inp (R_COM in bohr whatever R_UNITS)
                         mass_red=3.7523705333, rmax=42.40, U=50.0, b_impct=20.0,
                         time_step=10.0, time_lim=3.5e6)
