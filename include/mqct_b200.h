@@ -161,12 +161,13 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
 /* Matrix build from PES expansion terms (the READ_EXPANSION path: READ_EXPANSION_TERMS
  * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749), for
  * SYS_TYPE 1 (diatom + atom, case 1 at :6551-6622), SYS_TYPE 4 (asymmetric top + atom,
- * case 4 at :6955-7075), SYS_TYPE 7 (symmetric top + diatom, case 7 at :7593-7824; the channel's k in
+ * case 4 at :6955-7075), SYS_TYPE 5 (two diatoms, distinguishable partners, case 5 at
+ * :7076-7386; j2 per channel in sys->j2, vec1 unused), SYS_TYPE 7 (symmetric top + diatom, case 7 at :7593-7824; the channel's k in
  * sys->ka1, its parity eps in sys->kc1, vec1 unused), SYS_TYPE 8 (asymmetric top +
  * diatom, case 8 at :7826-8058) and SYS_TYPE 0 (two asymmetric tops, distinguishable
  * partners, case 0 at :8257-8672).  The arrays are the reference's own:
  *   a_top  A_TOP(5, nterms): per term 5 int32, (l, -, ...) for SYS_TYPE 1, (l, nju, -,
- *          ...) for SYS_TYPE 4, (l1, nju1, l2, l, -) for SYS_TYPE 7 and 8, (l1, nju1, l2,
+ *          ...) for SYS_TYPE 4, (l1, l2, l, -, -) for SYS_TYPE 5, (l1, nju1, l2, l, -) for SYS_TYPE 7 and 8, (l1, nju1, l2,
  *          nju2, l) for SYS_TYPE 0 (:6276-6338);
  *   terms  expansion_terms(n_r_coll, nterms): terms[t * nR + iR], R fastest, in the
  *          energy unit of the PES_EXPAN_TERMS.DAT file;

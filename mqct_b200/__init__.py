@@ -46,6 +46,8 @@ class CollisionSystem:
     """Collision system after the $BASIS block and INI_ARRAYS.
 
     sys_type 1: channels (j,), energy BE j(j+1) - DE (j(j+1))^2 (MQCT_SOURCE_CODES/iotest.f:5454);
+    sys_type 5: channels (j1, j2) of two diatoms, energy BE j1(j1+1) - DE (j1(j1+1))^2 +
+    BE2 j2(j2+1) - DE2 (j2(j2+1))^2 (BE1/DE1/BE2/DE2 of $BASIS; BE2, DE2 default to BE, DE);
     sys_type 4: channels (j, ka, kc), energy EIGEN_VAL(A,B,C) (MQCT_SOURCE_CODES/iotest.f:6611-6618);
     sys_type 7: channels (j1, k, eps, j2), A j1(j1+1) - (A-C) k^2 + BE j2(j2+1) - DE (j2(j2+1))^2
     (MQCT_SOURCE_CODES/iotest.f:8311-8312); k and eps are kept in ka1 and kc1, and vec1 holds
@@ -57,7 +59,7 @@ class CollisionSystem:
     """
 
     def __init__(self, sys_type, channels, A=0.0, B=0.0, C=0.0, BE=0.0, DE=0.0, A2=None,
-                 B2=None, C2=None, e_ch=None, identical=False):
+                 B2=None, C2=None, e_ch=None, identical=False, BE2=None, DE2=None):
         ch = np.asarray(channels, dtype=np.int32)
         if ch.ndim == 1:
             ch = ch[:, None]
@@ -68,7 +70,9 @@ class CollisionSystem:
         z = np.zeros(nch, np.int32)
         self.j1 = np.ascontiguousarray(ch[:, 0])
         self.ka1 = self.kc1 = self.j2 = self.ka2 = self.kc2 = z
-        jmax = int(ch[:, 0].max()) if sys_type in (1, 4) else int(max(ch[:, 0].max(), ch[:, 3].max()))
+        j2col = 1 if sys_type == 5 else 3
+        jmax = (int(ch[:, 0].max()) if sys_type in (1, 4)
+                else int(max(ch[:, 0].max(), ch[:, j2col].max())))
         self.ldv = 2 * jmax + 1
         self.vec1 = np.zeros((nch, self.ldv))
         self.vec2 = np.zeros((nch, self.ldv))
@@ -77,6 +81,14 @@ class CollisionSystem:
             jj = self.j1 * (self.j1 + 1.0)
             E = BE * jj - DE * jj ** 2
             self.vec1[:, 0] = 1.0
+        elif sys_type == 5:
+            self.j2 = np.ascontiguousarray(ch[:, 1])
+            BE2 = BE if BE2 is None else BE2
+            DE2 = DE if DE2 is None else DE2
+            jj1 = self.j1 * (self.j1 + 1.0)
+            jj2 = self.j2 * (self.j2 + 1.0)
+            E = BE * jj1 - DE * jj1 ** 2 + BE2 * jj2 - DE2 * jj2 ** 2
+            self.vec1[np.arange(nch), self.j1] = 1.0
         elif sys_type in (4, 8):
             self.ka1 = np.ascontiguousarray(ch[:, 1])
             self.kc1 = np.ascontiguousarray(ch[:, 2])
@@ -139,7 +151,7 @@ class CollisionSystem:
             ind = np.zeros(2 * P, np.int32)
             check(L.mqct_fill_ind_mat_identical(n, self.m12, self.parity, ind))
         else:
-            j2p = ptr(self.j2) if sys_type in (7, 8, 0) else None
+            j2p = ptr(self.j2) if sys_type in (5, 7, 8, 0) else None
             n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
             self.indx_chann = np.zeros(n, np.int32)
             self.j12 = np.zeros(n, np.int32)
@@ -171,6 +183,8 @@ class CollisionSystem:
             cols += [self.j1[ic - 1]]
         elif self.sys_type == 4:
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1]]
+        elif self.sys_type == 5:
+            cols += [self.j1[ic - 1], self.j2[ic - 1]]    # matrix_ini.f:4760-4767
         elif self.sys_type in (7, 8):
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1], self.j2[ic - 1]]
         else:
@@ -330,10 +344,11 @@ def write_expansion_terms_list(path, labels):
 
 def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",
                            mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
-    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 1, 4, 7, 8 and 0).
+    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 1, 4, 5, 7, 8 and 0).
 
     labels: the TERMS list, one row per term: (l,) for SYS_TYPE 1, (l, nju) for SYS_TYPE
-    4, (l1, nju1, l2, l) for SYS_TYPE 7 and 8, (l1, nju1, l2, nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
+    4, (l1, l2, l) for SYS_TYPE 5, (l1, nju1, l2, l) for SYS_TYPE 7 and 8, (l1, nju1, l2,
+    nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
     PES_EXPAN_TERMS.DAT, in the unit e_unit (a key of E_UNIT or the Hartree value of
     one unit).  Returns (Mat_el, y2, skipped) as build_matrix."""
     R = np.ascontiguousarray(R, np.float64)

@@ -1786,13 +1786,29 @@ struct ExpansionPlan {
     const int64_t P = P_;
     const int32_t nR = nR_, n_terms = n_terms_;
     MQCT_ARG_CHECK(sys && ind_mat && R && a_top, "null argument");
-    const int type = sys->sys_type;
-    MQCT_ARG_CHECK(type == 1 || type == 4 || type == 7 || type == 8 || type == 0,
-                   "the expansion path supports SYS_TYPE 1, 4, 7, 8 and 0 (got %d)", type);
-    if (type == 1 || type == 4)
+    const int type_in = sys->sys_type;
+    MQCT_ARG_CHECK(type_in == 1 || type_in == 4 || type_in == 5 || type_in == 7 || type_in == 8 ||
+                       type_in == 0,
+                   "the expansion path supports SYS_TYPE 1, 4, 5, 7, 8 and 0 (got %d)", type_in);
+    if (type_in == 1 || type_in == 4)
       return init_atom(sys, ind_mat, P_, R, nR_, n_terms_, a_top, mij_cutoff_cm, r_cut1, r_cut2);
+    // SYS_TYPE 5 (two diatoms, case 5 at pot_comp.f:7076-7386 for distinguishable partners)
+    // is case 8 with the first rotor a diatom: its K-sum is <j1'' 0 l1 0|j1' 0>, every
+    // other factor the same; A_TOP (l1, l2, l) becomes (l1, 0, l2, l)
+    const bool diat1 = type_in == 5;
+    const int type = diat1 ? 8 : type_in;
+    std::vector<int32_t> a_top5;
+    if (diat1) {
+      a_top5.assign(5 * (size_t)n_terms_, 0);
+      for (int t = 0; t < n_terms_; ++t) {
+        a_top5[5 * t] = a_top[5 * t];
+        a_top5[5 * t + 2] = a_top[5 * t + 1];
+        a_top5[5 * t + 3] = a_top[5 * t + 2];
+      }
+      a_top = a_top5.data();
+    }
     MQCT_ARG_CHECK(sys->j1 && sys->j2 && sys->indx_chann && sys->j12 && sys->m12 &&
-                       sys->n_states > 0 && (type == 7 || (sys->vec1 && sys->ldv > 0)) &&
+                       sys->n_states > 0 && (type == 7 || diat1 || (sys->vec1 && sys->ldv > 0)) &&
                        (type != 0 || sys->vec2) && (type != 7 || (sys->ka1 && sys->kc1)),
                    "system arrays missing");
     MQCT_ARG_CHECK(P > 0 && P < ((int64_t)1 << 31) && n_terms > 0 && n_terms <= 4096 && nR >= 2 &&
@@ -1833,7 +1849,7 @@ struct ExpansionPlan {
     int j1max = 0, j2max = 0;
     for (int c = 0; c < n_ch; ++c) {
       MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 && sys->j2[c] >= 0 && sys->j2[c] <= 30 &&
-                         (type == 7 || 2 * sys->j1[c] + 1 <= sys->ldv) &&
+                         (type == 7 || diat1 || 2 * sys->j1[c] + 1 <= sys->ldv) &&
                          (type != 0 || 2 * sys->j2[c] + 1 <= sys->ldv),
                      "bad channel %d (j1, j2 <= 30, 2j + 1 <= ldv)", c + 1);
       if (type == 7)
@@ -1871,6 +1887,11 @@ struct ExpansionPlan {
     // the K-sum S1 is the four-term bracket of the reference (:7680-7707 with coef4)
     int ldv1 = sys->ldv;
     std::vector<double> vec1_sym;
+    if (diat1) {  // the first diatom: one component, K = 0
+      ldv1 = 2 * j1max + 1;
+      vec1_sym.assign((size_t)n_ch * ldv1, 0.0);
+      for (int c = 0; c < n_ch; ++c) vec1_sym[(size_t)c * ldv1 + sys->j1[c]] = 1.0;
+    }
     if (type == 7) {
       ldv1 = 2 * j1max + 1;
       vec1_sym.assign((size_t)n_ch * ldv1, 0.0);
@@ -1925,7 +1946,7 @@ struct ExpansionPlan {
     MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
     MQCT_CUDA_TRY(d_j1.upload(ch_j1, st));
     MQCT_CUDA_TRY(d_j2.upload(ch_j2, st));
-    if (type == 7) MQCT_CUDA_TRY(d_vec1.upload(vec1_sym, st));
+    if (type == 7 || diat1) MQCT_CUDA_TRY(d_vec1.upload(vec1_sym, st));
     else MQCT_CUDA_TRY(d_vec1.upload(sys->vec1, (size_t)n_ch * ldv1, st));
     if (type != 0) MQCT_CUDA_TRY(d_vec2.upload(vec2_diatom, st));
     else MQCT_CUDA_TRY(d_vec2.upload(sys->vec2, (size_t)n_ch * ldv2, st));

@@ -87,3 +87,14 @@ def test_atom_projection_to_matrix_pipeline(mq, oracle, gpu_available, sys_type)
     direct, _, _ = mq.build_matrix(s, R, grid, pes, precision=mq.PREC_FP64, mij_cutoff=0.0)
     expan, _, _ = mq.build_matrix_expansion(s, R, case["labels"], T, mij_cutoff=0.0)
     assert np.max(np.abs(direct - expan)) <= 1e-10 * np.abs(direct).max()
+
+
+def test_type5_expansion_matches_oracle(mq, oracle, gpu_available):
+    from test_oracle_type5 import LABS, type5_oracle
+    s, o8, _ = type5_oracle(mq, oracle)
+    R = mq.r_grid(30, 4.0, 15.0)
+    T = np.random.default_rng(5).normal(size=(len(R), len(LABS))) * np.exp(-R)[:, None] * 1e4
+    m, _, _ = mq.build_matrix_expansion(s, R, LABS, T, mij_cutoff=0.0)
+    mo = oracle.expansion_matrix_type8(o8, o8.states(), s.ind_mat,
+                                       [(a, 0, b, c) for a, b, c in LABS], T)
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
