@@ -77,7 +77,7 @@ struct PropDev {
   const int* perm;             // internal -> reference state index
   const int* inv_perm;         // reference -> internal state index
   const void* knots;           // nR x S of (M, y2) in T precision
-  double mass;
+  double mass, inv_mass;
   int mode;                    // MQCT_MODE_STD or MQCT_MODE_AT
   int cs;                      // coupled-states approximation: no Coriolis terms
   int mp_cap;                  // packed slots that fit in shared memory
@@ -122,11 +122,17 @@ __device__ inline void save_record(const TrajOut& o, int tr, int64_t& n, double 
 constexpr int kClsSlots = 11;
 
 // Shared-memory layout of one CTA (dynamic).
+struct SplineAt;
+
 template <class T>
 struct Smem {
   Cls* c;                      // kClsSlots classical slots (see above)
-  double* red;                 // reduction scratch, 3 per warp
-  int* flag;                   // [0] next trajectory, [1] keep running, [2] CS m-block or -1
+  double* red;                 // reduction scratch, 3 per warp, then the 3 block sums
+  SplineAt* spl;               // spline interval of the current R (one per right-hand side)
+  double* scal;                // [0] sin(theta), [1] dphi/dt, [2] 1/R, [3] 1/sin^2(theta),
+                               // [4..6] the last theta with its sine and 1/sin^2
+  int* flag;                   // [0] next trajectory, [1] keep running, [2] CS m-block or -1,
+                               // [3] the spline interval found last
   double* Rg;                  // nR grid
   double2* a_in;               // N (RHS input amplitudes)
   typename V2<T>::t* bt;       // N
@@ -154,17 +160,25 @@ __device__ inline void block_sum3(double& a, double& b, double& c, double* red) 
     red[3 * w + 2] = c;
   }
   __syncthreads();
-  double sa = 0.0, sb = 0.0, sc = 0.0;
+  // one thread adds the warp sums in warp order and publishes them (the next call's
+  // partial writes go to other slots, its totals only after its first barrier)
+  constexpr int W = PT / 32;
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sb = 0.0, sc = 0.0;
 #pragma unroll
-  for (int i = 0; i < PT / 32; ++i) {
-    sa += red[3 * i];
-    sb += red[3 * i + 1];
-    sc += red[3 * i + 2];
+    for (int i = 0; i < W; ++i) {
+      sa += red[3 * i];
+      sb += red[3 * i + 1];
+      sc += red[3 * i + 2];
+    }
+    red[3 * W] = sa;
+    red[3 * W + 1] = sb;
+    red[3 * W + 2] = sc;
   }
-  a = sa;
-  b = sb;
-  c = sc;
   __syncthreads();
+  a = red[3 * W];
+  b = red[3 * W + 1];
+  c = red[3 * W + 2];
 }
 
 // Spline coefficients at R (splint_bk, MQCT_SOURCE_CODES/mqct_eqtns.f:555-611;
@@ -175,26 +189,35 @@ struct SplineAt {
   bool zero;
   double aa, bb, cc1, cc2, cc3, cc4, cc5, cc6, h;
 };
-__device__ inline SplineAt spline_at(const double* R, int nR, double x) {
+// *hint: the interval found last (klo); when x is still inside it the bisection, whose
+// result it is, is skipped.
+__device__ inline SplineAt spline_at(const double* R, int nR, double x, int* hint) {
   SplineAt s;
   s.zero = x > R[nR - 1];
   int klo = 1, khi = nR;
+  const int hk = *hint;
+  if (hk >= 1 && hk < nR && R[hk - 1] <= x && x < R[hk]) {
+    klo = hk;
+    khi = hk + 1;
+  }
   while (khi - klo > 1) {
     int k = (khi + klo) >> 1;
     if (R[k - 1] > x) khi = k;
     else klo = k;
   }
+  *hint = klo;
   s.klo = klo - 1;
   double h = R[khi - 1] - R[klo - 1];
+  const double inv_h = 1.0 / h;
   s.h = h;
-  s.aa = (R[khi - 1] - x) / h;
-  s.bb = (x - R[klo - 1]) / h;
+  s.aa = (R[khi - 1] - x) * inv_h;
+  s.bb = (x - R[klo - 1]) * inv_h;
   s.cc1 = s.aa * s.aa * s.aa - s.aa;
   s.cc2 = s.bb * s.bb * s.bb - s.bb;
   s.cc3 = 3 * s.aa * s.aa - 1.0;
   s.cc4 = 3 * s.bb * s.bb - 1.0;
   s.cc5 = (h * h) / 6.0;
-  s.cc6 = s.cc5 / h;
+  s.cc6 = s.cc5 * inv_h;
   return s;
 }
 
@@ -229,9 +252,27 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
   const int tid = threadIdx.x;
   const int N = d.N;
   const Cls c = *cin;
-  const double sin_t = sin(c.th);
-  const double dphidt = c.Pphi / c.R / c.R / d.mass / (sin_t * sin_t);
-  const SplineAt sp = spline_at(sm.Rg, d.nR, c.R);
+  // the point's scalars, formed once and read by every thread after the first barrier
+  // (reciprocals of R, m and sin^2: two divisions per point on the serial path of
+  // thread 0 in place of the reference's chained ones; the same values to rounding)
+  if (tid == 0) {
+    // theta stays at pi/2 in planar motion: sin(theta) and 1/sin^2 are kept while it is
+    // unchanged
+    if (!(c.th == sm.scal[4])) {
+      const double st0 = sin(c.th);
+      sm.scal[4] = c.th;
+      sm.scal[5] = st0;
+      sm.scal[6] = 1.0 / (st0 * st0);
+    }
+    const double st = sm.scal[5];
+    const double inv_r = 1.0 / c.R;
+    const double inv_s2 = sm.scal[6];
+    sm.scal[0] = st;
+    sm.scal[1] = c.Pphi * inv_r * inv_r * d.inv_mass * inv_s2;
+    sm.scal[2] = inv_r;
+    sm.scal[3] = inv_s2;
+    *sm.spl = spline_at(sm.Rg, d.nR, c.R, sm.flag + 3);
+  }
   // coupled states: only the m-block of the initial state carries amplitude, so only
   // its slots are read and only its rows formed; bt, u and y of the other rows were
   // zeroed when the trajectory started and stay zero
@@ -246,6 +287,8 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     sm.ph[e].y = (T)(-s);
   }
   __syncthreads();
+  const double sin_t = sm.scal[0], dphidt = sm.scal[1];
+  const SplineAt sp = *sm.spl;
   for (int i = cs_r0 + tid; i < cs_r1; i += PT) {
     const double2 a = sm.a_in[i];
     const T2 p = sm.ph[__ldg(d.st_e + i)];
@@ -357,6 +400,39 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
       // phase B: rows of the pass, y_i = sum_j M_ij bt_j
       const int r0 = cs_blk >= 0 ? cs_r0 : d.pass_row0[p];
       const int r1 = cs_blk >= 0 ? cs_r1 : d.pass_row0[p + 1];
+      const int rows = r1 - r0;
+      // few rows (one m-block in CS mode): tpr threads per row, each a strided part of
+      // the row, joined by shuffles within the lane group; otherwise one thread per row
+      const int tpr = rows * 2 > PT ? 1 : (rows * 4 > PT ? 2 : (rows * 8 > PT ? 4 : 8));
+      if (tpr > 1) {
+        const int sub = tid % tpr, grp = tid / tpr, ng = PT / tpr;
+        for (int rb = r0; rb < r1; rb += ng) {  // the same trip count in every lane
+          const int r = rb + grp;
+          T yr = (T)0, yi = (T)0;
+          if (r < r1) {
+            const int b = __ldg(d.st_blk + r);
+            const int n = __ldg(d.blk_n + b), sb = __ldg(d.blk_s0 + b);
+            const int i = r - sb;
+            const T2* z = sm.bt + sb;
+            const T* Mb = sm.Mp + __ldg(d.blk_mp + b);
+            for (int j = sub; j < n; j += tpr) {
+              const int addr = j <= i ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
+              const T m = Mb[addr];
+              const T2 zz = z[j];
+              yr += m * zz.x;
+              yi += m * zz.y;
+            }
+          }
+          for (int o = tpr / 2; o > 0; o >>= 1) {
+            yr += __shfl_xor_sync(0xffffffffu, yr, o);
+            yi += __shfl_xor_sync(0xffffffffu, yi, o);
+          }
+          if (r < r1 && sub == 0) {
+            sm.y[r].x = yr;
+            sm.y[r].y = yi;
+          }
+        }
+      } else
       for (int r = r0 + tid; r < r1; r += PT) {
         const int b = __ldg(d.st_blk + r);
         const int n = __ldg(d.blk_n + b), sb = __ldg(d.blk_s0 + b);
@@ -413,12 +489,13 @@ __device__ void rhs(const PropDev& d, const Smem<T>& sm, double t, const Cls* ci
     da[q] = make_double2(ci, -cr);  // -i (cr + i ci)
   }
   if (tid == 0 && d.mode == MQCT_MODE_STD) {
-    const double R = c.R, m = d.mass;
-    dc->R = c.PR / m;
-    dc->PR = -f + c.Pth / R / R / m * c.Pth / R + c.Pphi / R / R / m * c.Pphi / R / (sin_t * sin_t);
+    const double ir = sm.scal[2], is2 = sm.scal[3], im = d.inv_mass;
+    const double ir3m = ir * ir * ir * im;
+    dc->R = c.PR * im;
+    dc->PR = -f + c.Pth * c.Pth * ir3m + c.Pphi * c.Pphi * ir3m * is2;
     dc->th = 0.0;
     dc->Pth = 0.0;
-    dc->phi = c.Pphi / R / R / m / (sin_t * sin_t);
+    dc->phi = dphidt;
     dc->Pphi = sin_t * g;
   }
 }
@@ -515,7 +592,9 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
     };
     sm.c = reinterpret_cast<Cls*>(take(sizeof(Cls) * kClsSlots));
     bk = reinterpret_cast<Book*>(take(sizeof(Book)));
-    sm.red = reinterpret_cast<double*>(take(sizeof(double) * 3 * (PT / 32)));
+    sm.red = reinterpret_cast<double*>(take(sizeof(double) * 3 * (PT / 32 + 1)));
+    sm.spl = reinterpret_cast<SplineAt*>(take(sizeof(SplineAt)));
+    sm.scal = reinterpret_cast<double*>(take(64));
     sm.flag = reinterpret_cast<int*>(take(16));
     sm.Rg = reinterpret_cast<double*>(take(sizeof(double) * d.nR));
     sm.a_in = reinterpret_cast<double2*>(take(sizeof(double2) * N));
@@ -526,6 +605,10 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
     sm.Mp = reinterpret_cast<T*>(take(sizeof(T) * (size_t)d.mp_cap));
   }
   for (int i = tid; i < d.nR; i += PT) sm.Rg[i] = d.R[i];
+  if (tid == 0) {
+    sm.scal[4] = __longlong_as_double(0x7ff8000000000000ULL);  // no theta yet
+    sm.flag[3] = 0;                                            // no interval yet
+  }
   Cls* const C = sm.c;       // current state
   Cls* const CT = sm.c + 1;  // classical point of the stage
   Cls* const KC = sm.c + 2;  // classical derivative of the stage
@@ -974,7 +1057,8 @@ struct PropPlan {
   size_t smem_fixed() const {
     const size_t t2 = 2 * tsize();
     auto a = [](size_t x) { return (x + 15) & ~size_t(15); };
-    return a(sizeof(Cls) * kClsSlots) + a(sizeof(Book)) + a(sizeof(double) * 3 * (PT / 32)) + a(16) +
+    return a(sizeof(Cls) * kClsSlots) + a(sizeof(Book)) + a(sizeof(double) * 3 * (PT / 32 + 1)) +
+           a(sizeof(SplineAt)) + a(64) + a(16) +
            a(8 * (size_t)nR) +
            a(16 * (size_t)N) + 3 * a(t2 * N) + a(t2 * n_e);
   }
@@ -1171,6 +1255,7 @@ struct PropPlan {
     d.perm = d_perm.p; d.inv_perm = d_inv.p;
     d.knots = arith == MQCT_PROP_FP32 ? (const void*)d_knots32.p : (const void*)d_knots64.p;
     d.mass = mass;
+    d.inv_mass = 1.0 / mass;
     d.mode = mode & MQCT_MODE_AT;
     d.cs = ((mode & MQCT_MODE_CS) != 0) || cs;
     d.mp_cap = mp_cap;
