@@ -73,10 +73,10 @@ int mqct_device_count(void);
 typedef struct mqct_sys_t {
   int32_t sys_type;          /* MQCT_SYS_*                                       */
   int32_t n_channels;
-  const int32_t* j1;         /* per channel: j (types 1, 4) or j1 (types 8, 0)   */
+  const int32_t* j1;         /* per channel: j (types 1, 3, 4) or j1 (5, 7, 8, 0) */
   const int32_t* ka1;
   const int32_t* kc1;
-  const int32_t* j2;         /* types 8, 0                                       */
+  const int32_t* j2;         /* types 5, 7, 8, 0                                 */
   const int32_t* ka2;        /* type 0                                           */
   const int32_t* kc2;
   const double* vec1;        /* rotor-1 eigenvectors, channel-major, stride ldv,
@@ -160,14 +160,16 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
 
 /* Matrix build from PES expansion terms (the READ_EXPANSION path: READ_EXPANSION_TERMS
  * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749), for
- * SYS_TYPE 1 (diatom + atom, case 1 at :6551-6622), SYS_TYPE 4 (asymmetric top + atom,
- * case 4 at :6955-7075), SYS_TYPE 5 (two diatoms, distinguishable partners, case 5 at
+ * SYS_TYPE 1 (diatom + atom, case 1 at :6551-6622), SYS_TYPE 3 (symmetric top + atom,
+ * case 3 at :6846-6954; the channel's k in sys->ka1, its parity eps in sys->kc1, vec1
+ * unused; its -nju branch carries -(-1)^nju as written there, type 4's carries 1),
+ * SYS_TYPE 4 (asymmetric top + atom, case 4 at :6955-7075), SYS_TYPE 5 (two diatoms, distinguishable partners, case 5 at
  * :7076-7386; j2 per channel in sys->j2, vec1 unused), SYS_TYPE 7 (symmetric top + diatom, case 7 at :7593-7824; the channel's k in
  * sys->ka1, its parity eps in sys->kc1, vec1 unused), SYS_TYPE 8 (asymmetric top +
  * diatom, case 8 at :7826-8058) and SYS_TYPE 0 (two asymmetric tops, distinguishable
  * partners, case 0 at :8257-8672).  The arrays are the reference's own:
  *   a_top  A_TOP(5, nterms): per term 5 int32, (l, -, ...) for SYS_TYPE 1, (l, nju, -,
- *          ...) for SYS_TYPE 4, (l1, l2, l, -, -) for SYS_TYPE 5, (l1, nju1, l2, l, -) for SYS_TYPE 7 and 8, (l1, nju1, l2,
+ *          ...) for SYS_TYPE 3 and 4, (l1, l2, l, -, -) for SYS_TYPE 5, (l1, nju1, l2, l, -) for SYS_TYPE 7 and 8, (l1, nju1, l2,
  *          nju2, l) for SYS_TYPE 0 (:6276-6338);
  *   terms  expansion_terms(n_r_coll, nterms): terms[t * nR + iR], R fastest, in the
  *          energy unit of the PES_EXPAN_TERMS.DAT file;
@@ -445,7 +447,7 @@ int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_re
 
 /* Formatted MTRX.DAT (SAVE_MTRX / READ_MTRX with UNFORMAT = NO): PRINT_MIJ and READ_MIJ,
  * MQCT_SOURCE_CODES/matrix_ini.f:4692-4877 and 5794-6630.  Five header counts, the
- * state table (the columns of state_rec, SYS_TYPE 1, 4, 7, 8 or 0 for the writer), the
+ * state table (the columns of state_rec, SYS_TYPE 1, 3, 4, 5, 7, 8 or 0 for the writer), the
  * pairs, the R grid (e19.12) and one line (k, iR, Mij) per element (e19.12).  The
  * header reader returns the counts and the number of state columns. */
 int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
@@ -500,7 +502,7 @@ int mqct_write_cross_sections(const char* path, double U_cm, int32_t chann_ini, 
 int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
 
 /* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
- * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 7, 8 and 0: the
+ * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 1, 3, 4, 7, 8 and 0: the
  * quadrature projection of the PES tabulated on the angular grid onto the expansion
  * terms,
  *   terms[t * nR + iR]    = sum_g V Re(EXPANSION_TERM_t) w(g)    (intgrlr)
@@ -511,8 +513,11 @@ int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
  * midpoint-equidistant when eq_gamma, else Gauss-Legendre); grid->n_alpha unused.
  * V in the reference's V_3_2 / V_TRANSFER order, V[iR][alpha2][beta1][beta2][gamma1]
  * (SYS_TYPE 7, 8) or V[iR][alpha2][beta1][beta2][gamma1][gamma2] (SYS_TYPE 0), in the
- * unit the terms are wanted in.  a_top: A_TOP(5, nterms), (l1, nju1, l2, l, -) for 7
- * and 8, (l1, nju1, l2, nju2, l) for 0, checked as the reference checks a term list
+ * unit the terms are wanted in.  For a rotor and an atom (cases 1, 3 and 4, :4973-5104;
+ * case 3 is case 4) V is V_2_1, V[iR][beta] (SYS_TYPE 1, grid->n_beta), or V_3_1,
+ * V[iR][beta][gamma] (SYS_TYPE 3 and 4, grid->n_beta and grid->n_gamma), and a_top
+ * holds (l, -, ...) or (l, nju, -, ...), nju >= 0.  a_top: A_TOP(5, nterms), (l1, nju1,
+ * l2, l, -) for 7 and 8, (l1, nju1, l2, nju2, l) for 0, checked as the reference checks a term list
  * (triangle rule, nju1 >= 0, nju2 >= 0 when nju1 = 0, no term twice up to the sign of
  * the nju's; with identical != 0, SYS_TYPE 0 only, also l1 >= l2, |nju1| >= |nju2|
  * when l1 = l2 and no term twice up to the exchange of the partners): MQCT_E_ARG

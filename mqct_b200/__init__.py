@@ -48,6 +48,8 @@ class CollisionSystem:
     sys_type 1: channels (j,), energy BE j(j+1) - DE (j(j+1))^2 (MQCT_SOURCE_CODES/iotest.f:5454);
     sys_type 5: channels (j1, j2) of two diatoms, energy BE j1(j1+1) - DE (j1(j1+1))^2 +
     BE2 j2(j2+1) - DE2 (j2(j2+1))^2 (BE1/DE1/BE2/DE2 of $BASIS; BE2, DE2 default to BE, DE);
+    sys_type 3: channels (j, k, eps) of a symmetric top, energy A j(j+1) - (A-C) k^2
+    (MQCT_SOURCE_CODES/iotest.f:6250, 6355); k and eps are kept in ka1 and kc1, vec1 as for 7;
     sys_type 4: channels (j, ka, kc), energy EIGEN_VAL(A,B,C) (MQCT_SOURCE_CODES/iotest.f:6611-6618);
     sys_type 7: channels (j1, k, eps, j2), A j1(j1+1) - (A-C) k^2 + BE j2(j2+1) - DE (j2(j2+1))^2
     (MQCT_SOURCE_CODES/iotest.f:8311-8312); k and eps are kept in ka1 and kc1, and vec1 holds
@@ -71,7 +73,7 @@ class CollisionSystem:
         self.j1 = np.ascontiguousarray(ch[:, 0])
         self.ka1 = self.kc1 = self.j2 = self.ka2 = self.kc2 = z
         j2col = 1 if sys_type == 5 else 3
-        jmax = (int(ch[:, 0].max()) if sys_type in (1, 4)
+        jmax = (int(ch[:, 0].max()) if sys_type in (1, 3, 4)
                 else int(max(ch[:, 0].max(), ch[:, j2col].max())))
         self.ldv = 2 * jmax + 1
         self.vec1 = np.zeros((nch, self.ldv))
@@ -100,13 +102,15 @@ class CollisionSystem:
                 self.j2 = np.ascontiguousarray(ch[:, 3])
                 jj = self.j2 * (self.j2 + 1.0)
                 E = E + BE * jj - DE * jj ** 2
-        elif sys_type == 7:
+        elif sys_type in (3, 7):
             self.ka1 = np.ascontiguousarray(ch[:, 1])
             self.kc1 = np.ascontiguousarray(ch[:, 2])
-            self.j2 = np.ascontiguousarray(ch[:, 3])
             j1 = self.j1.astype(np.float64)
-            jj = self.j2 * (self.j2 + 1.0)
-            E = A * j1 * (j1 + 1.0) - (A - C) * self.ka1 ** 2.0 + BE * jj - DE * jj ** 2
+            E = A * j1 * (j1 + 1.0) - (A - C) * self.ka1 ** 2.0
+            if sys_type == 7:
+                self.j2 = np.ascontiguousarray(ch[:, 3])
+                jj = self.j2 * (self.j2 + 1.0)
+                E = E + BE * jj - DE * jj ** 2
             for i in range(nch):
                 j, k, eps = int(ch[i, 0]), int(ch[i, 1]), int(ch[i, 2])
                 if not (0 <= k <= j and eps in (0, 1) and not (k == 0 and eps == 1)):
@@ -181,7 +185,7 @@ class CollisionSystem:
         cols = [st, ic, self.j12, self.m12]
         if self.sys_type == 1:
             cols += [self.j1[ic - 1]]
-        elif self.sys_type == 4:
+        elif self.sys_type in (3, 4):                      # matrix_ini.f:4744-4759
             cols += [self.j1[ic - 1], self.ka1[ic - 1], self.kc1[ic - 1]]
         elif self.sys_type == 5:
             cols += [self.j1[ic - 1], self.j2[ic - 1]]    # matrix_ini.f:4760-4767
@@ -344,10 +348,10 @@ def write_expansion_terms_list(path, labels):
 
 def build_matrix_expansion(system: CollisionSystem, R, labels, terms, e_unit="CM-1",
                            mij_cutoff=1e-12, r_cut1=6.0, r_cut2=8.0):
-    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 1, 4, 5, 7, 8 and 0).
+    """Matrix from PES expansion terms (READ_EXPANSION path; SYS_TYPE 1, 3, 4, 5, 7, 8, 0).
 
     labels: the TERMS list, one row per term: (l,) for SYS_TYPE 1, (l, nju) for SYS_TYPE
-    4, (l1, l2, l) for SYS_TYPE 5, (l1, nju1, l2, l) for SYS_TYPE 7 and 8, (l1, nju1, l2,
+    3 and 4, (l1, l2, l) for SYS_TYPE 5, (l1, nju1, l2, l) for SYS_TYPE 7 and 8, (l1, nju1, l2,
     nju2, l) for SYS_TYPE 0.  terms: nR x n_terms as the rows of
     PES_EXPAN_TERMS.DAT, in the unit e_unit (a key of E_UNIT or the Hartree value of
     one unit).  Returns (Mat_el, y2, skipped) as build_matrix."""
@@ -849,10 +853,10 @@ def _a_top(labels):
 
 
 def _projection_grid(V, sys_type, eq_gamma):
-    if sys_type in (1, 4):
+    if sys_type in (1, 3, 4):
         if V.ndim != (2 if sys_type == 1 else 3):
             raise ValueError("V must be (nR, n_beta) for SYS_TYPE 1, (nR, n_beta, n_gamma) for 4")
-        return _abi.Grid(V.shape[1], V.shape[2] if sys_type == 4 else 0, 0, 0, 0, 0,
+        return _abi.Grid(V.shape[1], V.shape[2] if sys_type != 1 else 0, 0, 0, 0, 0,
                          1 if eq_gamma else 0)
     nR, n2, n3, n4, n5 = V.shape[:5]
     n6 = V.shape[5] if sys_type == 0 else 0
@@ -885,13 +889,13 @@ class ProjectionPlan:
     ExpansionPlan.execute takes)."""
 
     def __init__(self, sys_type, labels, grid_shape, eq_gamma=True, identical=False):
-        """grid_shape: (n_beta,) for SYS_TYPE 1, (n_beta, n_gamma) for 4, (n_alpha2,
+        """grid_shape: (n_beta,) for SYS_TYPE 1, (n_beta, n_gamma) for 3 and 4, (n_alpha2,
         n_beta1, n_beta2, n_gamma1[, n_gamma2]) for 7, 8 and 0."""
         a_top = _a_top(labels)
         self.n_terms = len(a_top)
-        if sys_type in (1, 4):
+        if sys_type in (1, 3, 4):
             gs = tuple(grid_shape) + (0,)
-            self.grid = _abi.Grid(gs[0], gs[1] if sys_type == 4 else 0, 0, 0, 0, 0,
+            self.grid = _abi.Grid(gs[0], gs[1] if sys_type != 1 else 0, 0, 0, 0, 0,
                                   1 if eq_gamma else 0)
         else:
             gs = tuple(grid_shape) + ((0,) if len(grid_shape) == 4 else ())

@@ -175,13 +175,13 @@ int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int
 }
 
 // States per channel: m = -j..j (types 1, 4) or j12 = |j1-j2|..j1+j2 with its m
-// (types 5, 7, 8, 0), channel-major (MQCT_SOURCE_CODES/matrix_ini.f:148-173, 261-544).
+// (types 5, 7, 8, 0), channel-major; type 3 like 1 and 4 (MQCT_SOURCE_CODES/matrix_ini.f:148-173, 261-544).
 int mqct_count_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
                       const int32_t* j2) {
   if (n_channels <= 0 || !j1) return MQCT_E_ARG;
   int st = 0;
   for (int i = 0; i < n_channels; ++i) {
-    if (sys_type == 1 || sys_type == 4) st += 2 * j1[i] + 1;
+    if (sys_type == 1 || sys_type == 3 || sys_type == 4) st += 2 * j1[i] + 1;
     else if (sys_type == 5 || sys_type == 7 || sys_type == 8 || sys_type == 0) {
       if (!j2) return MQCT_E_ARG;
       for (int js = abs(j1[i] - j2[i]); js <= j1[i] + j2[i]; ++js) st += 2 * js + 1;
@@ -199,8 +199,9 @@ int mqct_enumerate_states(int32_t sys_type, int32_t n_channels, const int32_t* j
   if (n < 0) return n;
   int st = 0;
   for (int i = 0; i < n_channels; ++i) {
-    int lo = (sys_type == 1 || sys_type == 4) ? j1[i] : abs(j1[i] - j2[i]);
-    int hi = (sys_type == 1 || sys_type == 4) ? j1[i] : j1[i] + j2[i];
+    const bool one = sys_type == 1 || sys_type == 3 || sys_type == 4;
+    int lo = one ? j1[i] : abs(j1[i] - j2[i]);
+    int hi = one ? j1[i] : j1[i] + j2[i];
     for (int js = lo; js <= hi; ++js)
       for (int m = -js; m <= js; ++m) {
         indx_chann[st] = i + 1;
@@ -503,6 +504,7 @@ static bool parse_fortran_real(const char*& p, double* out) {
 
 static const char* const* mtrx_dat_columns(int coll_type, int* n) {
   static const char* c1[] = {"#STATE", "#CHANNEL", "J12", "M12", "J"};
+  static const char* c3[] = {"#STATE", "#CHANNEL", "J12", "M12", "J", "K", "EPS"};
   static const char* c4[] = {"#STATE", "#CHANNEL", "J12", "M12", "J", "KA", "KC"};
   static const char* c5[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "J2"};
   static const char* c7[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K", "EPS", "J2"};
@@ -511,6 +513,7 @@ static const char* const* mtrx_dat_columns(int coll_type, int* n) {
                              "J2", "KA2", "KC2", "P"};
   switch (coll_type) {
     case 1: *n = 5; return c1;
+    case 3: *n = 7; return c3;
     case 4: *n = 7; return c4;
     case 5: *n = 6; return c5;
     case 7: *n = 8; return c7;
@@ -526,7 +529,7 @@ int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
                         const double* mat) {
   int ncol = 0;
   const char* const* cols = mtrx_dat_columns(coll_type, &ncol);
-  MQCT_ARG_CHECK(cols, "mqct_write_mtrx_dat: SYS_TYPE %d not supported (1, 4, 5, 7, 8, 0)",
+  MQCT_ARG_CHECK(cols, "mqct_write_mtrx_dat: SYS_TYPE %d not supported (1, 3, 4, 5, 7, 8, 0)",
                  coll_type);
   MQCT_ARG_CHECK(path && state_rec && ind_mat && R && mat && P > 0 && nR > 1 && n_states > 0,
                  "mqct_write_mtrx_dat: bad arguments");

@@ -1486,12 +1486,16 @@ __global__ void expansion_identical_kernel(int64_t P, int n_terms, const int* __
 //       sum_K <j' K l nju|j'' K+nju> c'_K c''_{K+nju},
 // with c the rotor vector over K (the unit vector at K = 0 for the diatom of type 1,
 // where S = <j' 0 l 0|j'' 0>).  lab5 holds (l, nju) per term.
+// SYS_TYPE 3 (symmetric top + atom, :6846-6954) uses the same sum over the parity-adapted
+// top vectors (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)); its -nju branch carries
+// (-1)**(-1)**nju = -1 in place of 1 as written there (minus_branch2).
 __global__ void expansion_atom_kernel(int64_t P, int n_terms, const int* __restrict__ ind_mat,
                                       const int* __restrict__ st_chan,
                                       const int* __restrict__ st_m,
                                       const int* __restrict__ ch_j,
                                       const double* __restrict__ vec, int ldv,
-                                      const int* __restrict__ lab5, double* __restrict__ A) {
+                                      const int* __restrict__ lab5, int minus_branch2,
+                                      double* __restrict__ A) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= P * n_terms) return;
   const int64_t k = idx / n_terms;
@@ -1507,7 +1511,8 @@ __global__ void expansion_atom_kernel(int64_t P, int n_terms, const int* __restr
     double S = 0.0;
     for (int planar = 0; planar < (nju0 == 0 ? 1 : 2); ++planar) {
       const int nju = planar ? -nju0 : nju0;
-      const double f = (planar == 0 && (nju0 & 1)) ? -1.0 : 1.0;
+      double f = (planar == 0 && (nju0 & 1)) ? -1.0 : 1.0;
+      if (planar == 1 && minus_branch2) f = (nju0 & 1) ? 1.0 : -1.0;
       double b = 0.0;
       for (int kp = -jp; kp <= jp; ++kp) {
         const int kpp = kp + nju;
@@ -1713,7 +1718,8 @@ struct ExpansionPlan {
                 double r_cut1, double r_cut2) {
     const int type = sys->sys_type;
     MQCT_ARG_CHECK(sys->j1 && sys->indx_chann && sys->j12 && sys->m12 && sys->n_states > 0 &&
-                       (type == 1 || (sys->vec1 && sys->ldv > 0)),
+                       (type == 1 || type == 3 || (sys->vec1 && sys->ldv > 0)) &&
+                       (type != 3 || (sys->ka1 && sys->kc1)),
                    "system arrays missing");
     MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31) && n_terms_ > 0 && n_terms_ <= 4096 &&
                        nR_ >= 2 && nR_ <= 3072,
@@ -1722,7 +1728,7 @@ struct ExpansionPlan {
     MQCT_ARG_CHECK(sys->parity == nullptr, "identical partners are SYS_TYPE 0");
     std::vector<int> lab5(5 * (size_t)n_terms_, 0);
     for (int t = 0; t < n_terms_; ++t) {
-      const int l = a_top[5 * t], nju = type == 4 ? a_top[5 * t + 1] : 0;
+      const int l = a_top[5 * t], nju = type != 1 ? a_top[5 * t + 1] : 0;
       // the reference's check of nju (pot_comp.f:6985-6998); l bounded by the log factorials
       MQCT_ARG_CHECK(l >= 0 && l <= 60 && nju >= 0 && nju <= l,
                      "bad expansion term %d (l=%d nju=%d): 0 <= nju <= l <= 60", t + 1, l, nju);
@@ -1733,8 +1739,14 @@ struct ExpansionPlan {
     int jmax = 0;
     for (int c = 0; c < n_ch; ++c) {
       MQCT_ARG_CHECK(sys->j1[c] >= 0 && sys->j1[c] <= 30 &&
-                         (type == 1 || 2 * sys->j1[c] + 1 <= sys->ldv),
+                         (type == 1 || type == 3 || 2 * sys->j1[c] + 1 <= sys->ldv),
                      "bad channel %d (j <= 30, 2j + 1 <= ldv)", c + 1);
+      if (type == 3)
+        MQCT_ARG_CHECK(sys->ka1[c] >= 0 && sys->ka1[c] <= sys->j1[c] &&
+                           (sys->kc1[c] == 0 || sys->kc1[c] == 1) &&
+                           !(sys->ka1[c] == 0 && sys->kc1[c] == 1),
+                       "bad symmetric-top channel %d (j=%d k=%d eps=%d)", c + 1, sys->j1[c],
+                       sys->ka1[c], sys->kc1[c]);
       jmax = std::max(jmax, sys->j1[c]);
     }
     std::vector<int> st_chan(n_states);
@@ -1757,6 +1769,16 @@ struct ExpansionPlan {
       unit.assign((size_t)n_ch * ldv, 0.0);
       for (int c = 0; c < n_ch; ++c) unit[(size_t)c * ldv + sys->j1[c]] = 1.0;
     }
+    if (type == 3) {  // the parity-adapted symmetric top over K
+      ldv = 2 * jmax + 1;
+      unit.assign((size_t)n_ch * ldv, 0.0);
+      for (int c = 0; c < n_ch; ++c) {
+        const int j = sys->j1[c], kk = sys->ka1[c];
+        const double a = 1.0 / sqrt(2.0 * (1.0 + (kk == 0 ? 1.0 : 0.0)));
+        unit[(size_t)c * ldv + j + kk] += a;
+        unit[(size_t)c * ldv + j - kk] += (sys->kc1[c] & 1) ? -a : a;
+      }
+    }
     int rc = init_common(ind_mat, P_, R, nR_, n_terms_, mij_cutoff_cm, r_cut1, r_cut2);
     if (rc) return rc;
     this->n_ch = n_ch;
@@ -1765,7 +1787,7 @@ struct ExpansionPlan {
     MQCT_CUDA_TRY(d_chan.upload(st_chan, st));
     MQCT_CUDA_TRY(d_m.upload(sys->m12, n_states, st));
     MQCT_CUDA_TRY(d_j1.upload(sys->j1, n_ch, st));
-    if (type == 1) MQCT_CUDA_TRY(d_vec.upload(unit, st));
+    if (type == 1 || type == 3) MQCT_CUDA_TRY(d_vec.upload(unit, st));
     else MQCT_CUDA_TRY(d_vec.upload(sys->vec1, (size_t)n_ch * ldv, st));
     MQCT_CUDA_TRY(d_lab.upload(lab5, st));
     MQCT_CUDA_TRY(d_A.alloc((size_t)P * n_terms));
@@ -1773,7 +1795,8 @@ struct ExpansionPlan {
     const int64_t n_at = P * n_terms;
     MQCT_CUDA_TRY(cudaEventRecord(ev[0], st));
     expansion_atom_kernel<<<(unsigned)((n_at + 127) / 128), 128, 0, st>>>(
-        P, n_terms, d_ind.p, d_chan.p, d_m.p, d_j1.p, d_vec.p, ldv, d_lab.p, d_A.p);
+        P, n_terms, d_ind.p, d_chan.p, d_m.p, d_j1.p, d_vec.p, ldv, d_lab.p, type == 3 ? 1 : 0,
+        d_A.p);
     MQCT_CUDA_TRY(cudaGetLastError());
     MQCT_CUDA_TRY(cudaEventRecord(ev[1], st));
     MQCT_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1787,10 +1810,10 @@ struct ExpansionPlan {
     const int32_t nR = nR_, n_terms = n_terms_;
     MQCT_ARG_CHECK(sys && ind_mat && R && a_top, "null argument");
     const int type_in = sys->sys_type;
-    MQCT_ARG_CHECK(type_in == 1 || type_in == 4 || type_in == 5 || type_in == 7 || type_in == 8 ||
-                       type_in == 0,
-                   "the expansion path supports SYS_TYPE 1, 4, 5, 7, 8 and 0 (got %d)", type_in);
-    if (type_in == 1 || type_in == 4)
+    MQCT_ARG_CHECK(type_in == 1 || type_in == 3 || type_in == 4 || type_in == 5 || type_in == 7 ||
+                       type_in == 8 || type_in == 0,
+                   "the expansion path supports SYS_TYPE 1, 3, 4, 5, 7, 8 and 0 (got %d)", type_in);
+    if (type_in == 1 || type_in == 3 || type_in == 4)
       return init_atom(sys, ind_mat, P_, R, nR_, n_terms_, a_top, mij_cutoff_cm, r_cut1, r_cut2);
     // SYS_TYPE 5 (two diatoms, case 5 at pot_comp.f:7076-7386 for distinguishable partners)
     // is case 8 with the first rotor a diatom: its K-sum is <j1'' 0 l1 0|j1' 0>, every

@@ -236,9 +236,9 @@ __global__ void proj_terms_kernel(const double2* __restrict__ K, int nR, int r0,
 // when l1 = l2, and the exchange (l1, nju1) <-> (l2, nju2) counting as the same.  Beyond
 // the reference: |nju| <= l (the D function is undefined otherwise) and l <= kMaxL.
 int check_terms(int sys_type, int n_terms, const int32_t* a_top, int identical) {
-  if (sys_type == 1 || sys_type == 4) {  // (l) or (l, nju): nju >= 0 (pot_comp.f:5061-5066)
-    for (int t = 0; t < n_terms; ++t) {
-      const int l = a_top[5 * t], nju = sys_type == 4 ? a_top[5 * t + 1] : 0;
+  if (sys_type == 1 || sys_type == 3 || sys_type == 4) {  // (l) or (l, nju): nju >= 0
+    for (int t = 0; t < n_terms; ++t) {                    // (pot_comp.f:5005-5010, 5061-5066)
+      const int l = a_top[5 * t], nju = sys_type != 1 ? a_top[5 * t + 1] : 0;
       MQCT_ARG_CHECK(l >= 0 && l <= kMaxL, "term %d: l must be in 0..%d", t + 1, kMaxL);
       MQCT_ARG_CHECK(nju >= 0, "term %d: the values of M1 should be always positive", t + 1);
       MQCT_ARG_CHECK(nju <= l, "term %d: |nju| exceeds its l", t + 1);
@@ -334,7 +334,8 @@ struct mqct_projection_plan {
   }
 
   // SYS_TYPE 1 (diatom + atom, V_2_1(n_beta, n_r)) and 4 (top + atom, V_3_1(n_gamma,
-  // n_beta, n_r)), CALC_EXPANSION_TERMS cases 1 and 4 (pot_comp.f:4973-4999, 5054-5104):
+  // n_beta, n_r)), CALC_EXPANSION_TERMS cases 1 and 4 (pot_comp.f:4973-4999, 5054-5104;
+  // case 3, the symmetric top, :5000-5053, is case 4):
   //   type 1: terms = sum_beta WF_DIAT_TOP(l, 0; beta) V wb sin(beta) xbl 2 pi
   //   type 4: terms = sum_{beta,gamma} Re((-1)^nju WF_DIAT_TOP(l, nju; beta, gamma)) V wb wg
   //           sin(beta) xbl xgl
@@ -401,13 +402,13 @@ struct mqct_projection_plan {
   }
 
   int init(int sys, int nt, const int32_t* a_top, const mqct_grid_t& g, int identical) {
-    MQCT_ARG_CHECK(sys == 1 || sys == 4 || sys == 7 || sys == 8 || sys == 0,
-                   "the projection is built for SYS_TYPE 1, 4, 7, 8 and 0 (got %d)", sys);
+    MQCT_ARG_CHECK(sys == 1 || sys == 3 || sys == 4 || sys == 7 || sys == 8 || sys == 0,
+                   "the projection is built for SYS_TYPE 1, 3, 4, 7, 8 and 0 (got %d)", sys);
     MQCT_ARG_CHECK(nt > 0 && a_top, "no terms");
     MQCT_ARG_CHECK(!identical || sys == 0, "identical partners are SYS_TYPE 0");
     sys_type = sys;
     n_terms = nt;
-    if (sys == 1 || sys == 4) return init_atom(sys, nt, a_top, g);
+    if (sys == 1 || sys == 3 || sys == 4) return init_atom(sys == 3 ? 4 : sys, nt, a_top, g);
     sys_type = sys;
     n_terms = nt;
     n_a2 = g.n_alpha2;

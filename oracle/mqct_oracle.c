@@ -367,13 +367,13 @@ int orc_asym_top(double A, double B, double C, int j, int ka, int kc, double* en
 
 /* ---------------------------------------------------------------------- */
 /* States: SRC/matrix_ini.f:60-209 (count) and 261-544 (fill), distinguishable
- * particles.  Types 1/4: m=-j..j per channel; types 8/0: j12=|j1-j2|..j1+j2, m12. */
+ * particles.  Types 1/3/4: m=-j..j per channel; types 5/7/8/0: j12=|j1-j2|..j1+j2, m12. */
 int orc_count_states(const orc_system* sys) {
   int st = 0;
   for (int i = 0; i < sys->n_channels; ++i) {
     switch (sys->sys_type) {
-      case 1: case 4: st += 2 * sys->j1[i] + 1; break;
-      case 7: case 8: case 0: {
+      case 1: case 3: case 4: st += 2 * sys->j1[i] + 1; break;
+      case 5: case 7: case 8: case 0: {
         int a = sys->j1[i], b = sys->j2[i];
         for (int js = abs(a - b); js <= a + b; ++js) st += 2 * js + 1;
         break;
@@ -388,12 +388,13 @@ int orc_enumerate_states(const orc_system* sys, int32_t* indx_chann, int32_t* j1
                          double* ej) {
   int st = 0;
   for (int i = 0; i < sys->n_channels; ++i) {
-    if (sys->sys_type == 1 || sys->sys_type == 4) {
+    if (sys->sys_type == 1 || sys->sys_type == 3 || sys->sys_type == 4) {
       int j = sys->j1[i];
       for (int m = -j; m <= j; ++m) {
         indx_chann[st] = i + 1; j12[st] = j; m12[st] = m; ej[st] = sys->e_ch[i]; ++st;
       }
-    } else if (sys->sys_type == 7 || sys->sys_type == 8 || sys->sys_type == 0) {
+    } else if (sys->sys_type == 5 || sys->sys_type == 7 || sys->sys_type == 8 ||
+               sys->sys_type == 0) {
       int a = sys->j1[i], b = sys->j2[i];
       for (int js = abs(a - b); js <= a + b; ++js)
         for (int m = -js; m <= js; ++m) {
@@ -2019,12 +2020,13 @@ int orc_project_terms(int sys_type, int n_terms, const int32_t* a_top, int n_alp
 }
 
 /* CALC_EXPANSION_TERMS for a rotor and an atom (SRC/pot_comp.f:4973-4999 SYS_TYPE 1,
- * 5054-5104 SYS_TYPE 4; EXPANSION_TERM :3756-3768): V[iR][beta] (V_2_1) or
- * V[iR][beta][gamma] (V_3_1), terms[t * nR + iR] the real part as the reference sums it,
- * terms_im the imaginary part. */
+ * 5054-5104 SYS_TYPE 4, 5000-5053 SYS_TYPE 3 = the loop of 4; EXPANSION_TERM :3756-3780):
+ * V[iR][beta] (V_2_1) or V[iR][beta][gamma] (V_3_1), terms[t * nR + iR] the real part as
+ * the reference sums it, terms_im the imaginary part. */
 int orc_project_terms_atom(int sys_type, int n_terms, const int32_t* a_top, int n_beta,
                            int n_gamma, int eq_gamma, int nR, const double* V, double* terms,
                            double* terms_im) {
+  if (sys_type == 3) sys_type = 4;
   if (sys_type != 1 && sys_type != 4) return -1;
   if (sys_type == 1) n_gamma = 1;
   double* xb = (double*)malloc(sizeof(double) * n_beta);

@@ -492,7 +492,7 @@ def expansion_term(sys_type, l, l1, l2, nju1, nju2, beta1, gamma1, alpha2, beta2
 
 
 def project_terms_atom(sys_type, labels, V, eq_gamma=True):
-    """CALC_EXPANSION_TERMS for SYS_TYPE 1 (V: nR x n_beta) and 4 (V: nR x n_beta x
+    """CALC_EXPANSION_TERMS for SYS_TYPE 1 (V: nR x n_beta), 3 and 4 (V: nR x n_beta x
     n_gamma); labels (l,) or (l, nju).  Returns (terms, terms_im), n_terms x nR."""
     lab = np.asarray(labels, np.int32).reshape(len(labels), -1)
     a_top = np.zeros((len(lab), 5), np.int32)

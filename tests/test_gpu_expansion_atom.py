@@ -98,3 +98,27 @@ def test_type5_expansion_matches_oracle(mq, oracle, gpu_available):
     mo = oracle.expansion_matrix_type8(o8, o8.states(), s.ind_mat,
                                        [(a, 0, b, c) for a, b, c in LABS], T)
     assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+
+
+def test_type3_expansion_matches_oracle(mq, oracle, gpu_available):
+    """SYS_TYPE 3 (symmetric top + atom): the GPU build against the oracle's case-3
+    formula, with the -nju branch factor the reference writes for it."""
+    from test_oracle_type3 import LABELS, systems
+
+    s, o3, _ = systems(mq, oracle)
+    R = mq.r_grid(30, 3.0, 20.0)
+    T = np.random.default_rng(12).normal(size=(len(R), len(LABELS))) * np.exp(-R)[:, None] * 1e4
+    m, _, sk = mq.build_matrix_expansion(s, R, LABELS, T, mij_cutoff=0.0)
+    mo = oracle.expansion_matrix_atom(o3, o3.states(), s.ind_mat, LABELS, T, CM)
+    assert np.max(np.abs(m - mo)) <= 1e-12 * np.abs(mo).max()
+    assert not sk.any()
+
+
+def test_type3_projection_matches_oracle(mq, oracle, gpu_available):
+    from test_oracle_type3 import LABELS
+
+    V = np.random.default_rng(13).normal(size=(3, 16, 12)) * 1e3 + 20.0
+    T, Ti = mq.project_terms(3, LABELS, V)
+    To, Tio = oracle.project_terms_atom(3, LABELS, V)
+    bound = 1e-12 * np.abs(V).max() * 4 * np.pi
+    assert np.max(np.abs(T - To.T)) <= bound and np.max(np.abs(Ti - Tio.T)) <= bound
