@@ -145,7 +145,8 @@ typedef struct mqct_err_report_t {
   double rms_rel_err;        /* out                                            */
 } mqct_err_report_t;
 
-/* Matrix build (SYS_TYPE 1, 4 and 0): M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
+/* Matrix build (SYS_TYPE 1, 3, 4 and 0; SYS_TYPE 3 reads k from sys->ka1 and eps from
+ * sys->kc1 and forms the symmetric-top vectors itself): M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
  * (MQCT_SOURCE_CODES/pot_comp.f:1947-1952, 2535-2557, 3709-3721), converted to
  * Hartree, MIJ_CUTOFF truncation at R~r_cut1/r_cut2
  * (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997, columns whose max |M| there is

@@ -645,8 +645,38 @@ int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, 
                      int32_t nR_, const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec,
                      double mij_cut, double rc1, double rc2) {
   MQCT_ARG_CHECK(sys && ind_mat && R && grid && pes, "null argument");
-  MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 4 || sys->sys_type == 0,
-                 "matrix build supports SYS_TYPE 1, 4 and 0 (got %d)", sys->sys_type);
+  MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 3 || sys->sys_type == 4 ||
+                     sys->sys_type == 0,
+                 "matrix build supports SYS_TYPE 1, 3, 4 and 0 (got %d)", sys->sys_type);
+  if (sys->sys_type == 3) {
+    // WF_SYM_TOP (MQCT_SOURCE_CODES/basis_wave_functions.f:118-151) is WF_ASYM_TOP with the
+    // vector (|j k> + (1 - 2 eps) |j -k>) / sqrt(2 (1 + delta_k0)) over K, and case 3 of
+    // INTEGRATOR_TEMP (pot_comp.f:2259-2303) integrates as case 4 without an alpha grid.
+    MQCT_ARG_CHECK(sys->ka1 && sys->kc1 && sys->j1 && sys->n_channels > 0,
+                   "SYS_TYPE 3 needs j, k (ka1) and eps (kc1) per channel");
+    MQCT_ARG_CHECK(grid->n_alpha == 0, "SYS_TYPE 3 has no alpha grid");
+    int jmax = 0;
+    for (int c = 0; c < sys->n_channels; ++c) {
+      const int j = sys->j1[c], kk = sys->ka1[c], e = sys->kc1[c];
+      MQCT_ARG_CHECK(j >= 0 && j <= 40 && kk >= 0 && kk <= j && (e == 0 || e == 1) &&
+                         !(kk == 0 && e == 1),
+                     "bad symmetric-top channel %d (j=%d k=%d eps=%d)", c + 1, j, kk, e);
+      jmax = std::max(jmax, j);
+    }
+    const int ld = 2 * jmax + 1;
+    sym_top_vec.assign((size_t)sys->n_channels * ld, 0.0);
+    for (int c = 0; c < sys->n_channels; ++c) {
+      const int j = sys->j1[c], kk = sys->ka1[c];
+      const double a = 1.0 / sqrt(2.0 * (kk == 0 ? 2.0 : 1.0));
+      sym_top_vec[(size_t)c * ld + j + kk] += a;
+      sym_top_vec[(size_t)c * ld + j - kk] += (sys->kc1[c] & 1) ? -a : a;
+    }
+    sym_top_sys = *sys;
+    sym_top_sys.sys_type = 4;
+    sym_top_sys.vec1 = sym_top_vec.data();
+    sym_top_sys.ldv = ld;
+    sys = &sym_top_sys;
+  }
   MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31), "P out of range");
   MQCT_ARG_CHECK(nR_ >= 2, "nR must be >= 2");
   MQCT_ARG_CHECK(nR_ <= 3072, "nR=%d beyond the finalize limit of 3072 points", nR_);

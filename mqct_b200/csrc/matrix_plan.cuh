@@ -36,6 +36,9 @@ struct MatrixPlan {
   double cut = 0.0;
   int pes_kind = 0, pes_n_terms = 0, pes_n_sites1 = 0, pes_n_sites2 = 0;
   std::vector<double> Rh, h_beta, h_gamma, h_wt, h_alpha, h_walpha;
+  // SYS_TYPE 3 runs as SYS_TYPE 4 on the parity-adapted top vectors held here
+  std::vector<double> sym_top_vec;
+  mqct_sys_t sym_top_sys{};
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 

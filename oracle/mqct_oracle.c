@@ -269,6 +269,24 @@ void orc_wf_asym(int j, const double* coeff, int m, double alpha, double beta, d
   *im = wi;
 }
 
+/* Symmetric-top wavefunction of the level (j, k, eps):
+ * (D^j_{k m} + (1 - 2 eps) D^j_{-k m}) sqrt((2j+1)/8pi^2), divided by 2 for k = 0 and by
+ * sqrt(2) otherwise: SRC/basis_wave_functions.f:118-151 (WF_SYM_TOP). */
+void orc_wf_sym(int j, int k, int eps, int m, double alpha, double beta, double gamma,
+                double* re, double* im) {
+  double dwr, dwi, wr, wi;
+  orc_djkm(j, k, m, alpha, beta, gamma, &dwr, &dwi);
+  wr = dwr;
+  wi = dwi;
+  orc_djkm(j, -k, m, alpha, beta, gamma, &dwr, &dwi);
+  wr += dwr * (1.0 - 2 * eps);
+  wi += dwi * (1.0 - 2 * eps);
+  const double nrm = sqrt((2.0 * j + 1.0) / 8.0 / (ORC_PI * ORC_PI));
+  const double f = (k == 0) ? 0.5 : 1.0 / sqrt(2.0);
+  *re = wr * f * nrm;
+  *im = wi * f * nrm;
+}
+
 /* Rigid-rotor Hamiltonian element in the symmetric-top basis, z = c axis:
  * SRC/asym_top.f:103-137 (hamilt_kyro). */
 static double orc_hamilt(int j, int k1, int k2, double A, double B, double C) {
@@ -559,7 +577,7 @@ static void orc_make_agrid(int sys_type, const orc_grid* g, orc_agrid* a) {
   memset(a, 0, sizeof(*a));
   a->nb = g->n_beta;
   orc_axis_gl(g->n_beta, 0.0, ORC_PI, &a->bx, &a->bw, &a->xbl);
-  if (sys_type == 4 || sys_type == 0) {
+  if (sys_type == 3 || sys_type == 4 || sys_type == 0) {
     a->ng = g->n_gamma;
     if (g->eq_gamma) orc_axis_mid(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
     else orc_axis_gl(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
@@ -588,13 +606,14 @@ static void orc_free_agrid(orc_agrid* a) {
 }
 static int64_t orc_agrid_size(int sys_type, const orc_agrid* a) {
   if (sys_type == 1) return a->nb;
-  if (sys_type == 4) return (int64_t)a->nb * a->ng * (a->na > 0 ? a->na : 1);
+  if (sys_type == 3 || sys_type == 4) return (int64_t)a->nb * a->ng * (a->na > 0 ? a->na : 1);
   if (sys_type == 0) return (int64_t)a->naa * a->nb * a->nbb * a->ng * a->ngg;
   return -1;
 }
 
 /* Wavefunction of state st (0-based) at a grid point, dispatching on type:
  * type 1 WF_DIAT_TOP(j,m,beta,0); type 4 WF_ASYM_TOP(...,alpha,beta,gamma);
+ * type 3 WF_SYM_TOP(j,k,eps,m,...,0,beta,gamma) (SRC/pot_comp.f:2296-2302);
  * type 0 WF_ASYM_TOP_ASYM_TOP (SRC/basis_wave_functions.f:1-41). */
 static void orc_wf_state(const orc_system* sys, int ch, int j12, int m12, double al, double be,
                          double ga, double aal, double bbe, double gga, double* re, double* im) {
@@ -602,6 +621,8 @@ static void orc_wf_state(const orc_system* sys, int ch, int j12, int m12, double
     orc_wf_diat(sys->j1[ch], m12, be, 0.0, re, im);
   } else if (sys->sys_type == 4) {
     orc_wf_asym(sys->j1[ch], sys->vec1 + (size_t)ch * sys->ldv, m12, al, be, ga, re, im);
+  } else if (sys->sys_type == 3) {
+    orc_wf_sym(sys->j1[ch], sys->ka1[ch], sys->kc1[ch], m12, 0.0, be, ga, re, im);
   } else { /* type 0 */
     int j1 = sys->j1[ch], j2 = sys->j2[ch];
     double wr = 0.0, wi = 0.0;
@@ -629,7 +650,7 @@ static orc_gpt orc_grid_point(int sys_type, const orc_agrid* a, int64_t g) {
   if (sys_type == 1) {
     p.be = a->bx[g];
     p.wt = a->bw[g] * sin(p.be) * a->xbl * 2.0 * ORC_PI;
-  } else if (sys_type == 4) {
+  } else if (sys_type == 3 || sys_type == 4) {  /* type 3: beta, gamma (:2259-2303) */
     int na = a->na > 0 ? a->na : 1;
     int ia = (int)(g % na);
     int64_t r = g / na;
@@ -663,7 +684,8 @@ static double orc_pes_at(int sys_type, const orc_pes* pes, double R, const orc_g
                          int iR, int64_t g, int64_t ng) {
   if (pes->kind == ORC_PES_TABLE) return pes->table[(size_t)iR * ng + g];
   if (sys_type == 1) return orc_pes_eval(pes, R, 0.0, p->be, 0.0, 0.0, 0.0, 0.0);
-  if (sys_type == 4) return orc_pes_eval(pes, R, 0.0, -p->be, -p->ga, 0.0, 0.0, 0.0);
+  if (sys_type == 3 || sys_type == 4)  /* V_POT_TOP_ATOM, SYS_TYPE 3 and 4 */
+    return orc_pes_eval(pes, R, 0.0, -p->be, -p->ga, 0.0, 0.0, 0.0);
   return orc_pes_eval(pes, R, 0.0, p->be, p->ga, p->aal, p->bbe, p->gga);
 }
 
@@ -676,6 +698,7 @@ int orc_integrate_elements(const orc_system* sys, int n_states, const int32_t* i
                            int64_t k_begin, int64_t k_end, int iR_begin, int iR_end,
                            int n_threads, double* mat) {
   (void)P;
+  if (sys->sys_type == 3 && (!sys->ka1 || !sys->kc1)) return -1;
   orc_agrid a;
   orc_make_agrid(sys->sys_type, grid, &a);
   int64_t ng = orc_agrid_size(sys->sys_type, &a);

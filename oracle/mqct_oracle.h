@@ -39,6 +39,8 @@ void orc_wf_diat(int j, int m, double theta, double phi, double* re, double* im)
  * (2j+1) symmetric-top coefficients ordered K=-j..j.  Returns 0 or <0. */
 int  orc_asym_top(double A, double B, double C, int j, int ka, int kc,
                   double* energy, double* vec);
+void orc_wf_sym(int j, int k, int eps, int m, double alpha, double beta, double gamma,
+                double* re, double* im);
 void orc_wf_asym(int j, const double* coeff, int m, double alpha, double beta,
                  double gamma, double* re, double* im);
 

@@ -122,3 +122,21 @@ def test_type3_projection_matches_oracle(mq, oracle, gpu_available):
     To, Tio = oracle.project_terms_atom(3, LABELS, V)
     bound = 1e-12 * np.abs(V).max() * 4 * np.pi
     assert np.max(np.abs(T - To.T)) <= bound and np.max(np.abs(Ti - Tio.T)) <= bound
+
+
+@pytest.mark.parametrize("prec,tol", [("PREC_FP64", 1e-12), ("PREC_BF16X3", 1e-4)])
+def test_type3_direct_build_matches_oracle(mq, oracle, gpu_available, prec, tol):
+    """INTEGRATOR_TEMP case 3 on the GPU (run as case 4 on the parity-adapted vectors)
+    against the oracle's WF_SYM_TOP quadrature, on a seeded table PES."""
+    from test_oracle_type3 import systems
+
+    s, o3, _ = systems(mq, oracle)
+    R = mq.r_grid(6, 4.0, 12.0)
+    grid = (16, 14)
+    V = np.random.default_rng(14).normal(size=(len(R),) + grid) * 300.0 + 50.0
+    g = grid + (0, 0, 0, 0, 1)
+    pes = dict(kind=mq._abi.PES_TABLE, n_terms=0, params=np.zeros(1), table=V.reshape(-1))
+    m, _, _ = mq.build_matrix(s, R, g, pes, precision=getattr(mq, prec), mij_cutoff=0.0)
+    opes = oracle.OraclePes(0, 0, np.zeros(1), table=V.reshape(-1))
+    mo, _, _ = oracle.build_matrix(o3, o3.states(), s.ind_mat, R, g, opes, mij_cut=0.0)
+    assert np.max(np.abs(m - mo)) <= tol * np.abs(mo).max()

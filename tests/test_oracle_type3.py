@@ -81,3 +81,64 @@ def test_type3_formula_against_type4_of_the_same_vectors(mq, oracle):
         else:
             assert np.max(np.abs(m3 * m4)) <= 1e-13 * scale ** 2, (l, nu)
             assert np.abs(m3).max() > 0 and np.abs(m4).max() > 0, (l, nu)
+
+
+def _pes_from_terms(mq, oracle, labels, grid, R, seed):
+    """V = sum_t v_t (Y_{l nju} + Y*_{l nju}) on the (beta, gamma) grid (Y for nju = 0)."""
+    from test_oracle_expansion_atom import term_table
+
+    W = term_table(oracle, labels, grid, 4)
+    v = np.random.default_rng(seed).normal(size=(len(labels), len(R))) * 100
+    return v, np.einsum("tr,t...->r...", v, W)
+
+
+def test_type3_direct_quadrature_agrees_with_type4_of_the_same_vectors(mq, oracle):
+    """INTEGRATOR_TEMP case 3 (WF_SYM_TOP, pot_comp.f:2259-2303) equals case 4 with the
+    parity-adapted vectors, for a PES with all nju."""
+    s, o3, o4 = systems(mq, oracle)
+    R = np.array([5.0, 7.0])
+    grid = (16, 14)
+    _, V = _pes_from_terms(mq, oracle, LABELS, grid, R, 7)
+    pes = oracle.OraclePes(0, 0, np.zeros(1), table=V.reshape(-1))
+    g = grid + (0, 0, 0, 0, 1)
+    m3, _, _ = oracle.build_matrix(o3, o3.states(), s.ind_mat, R, g, pes, mij_cut=0.0)
+    m4, _, _ = oracle.build_matrix(o4, o4.states(), s.ind_mat, R, g, pes, mij_cut=0.0)
+    assert np.max(np.abs(m3 - m4)) <= 1e-13 * np.abs(m4).max()
+
+
+def test_type3_direct_and_expansion_paths(mq, oracle):
+    """The direct quadrature of V = sum_t v_t (Y + Y*) equals the case-3 expansion formula
+    for terms with nju = 0 or odd nju, and the case-4 formula of the same vectors for all
+    terms: the -nju factor of case 3 breaks the direct/expansion agreement at even nju > 0,
+    as written in the reference."""
+    s, o3, o4 = systems(mq, oracle)
+    R = np.array([5.0, 7.0])
+    grid = (20, 24)
+    g = grid + (0, 0, 0, 0, 1)
+    for labels, ok3 in (([lab for lab in LABELS if lab[1] == 0 or lab[1] % 2], True),
+                        (LABELS, False)):
+        v, V = _pes_from_terms(mq, oracle, labels, grid, R, 8)
+        pes = oracle.OraclePes(0, 0, np.zeros(1), table=V.reshape(-1))
+        direct, _, _ = oracle.build_matrix(o3, o3.states(), s.ind_mat, R, g, pes, mij_cut=0.0)
+        e4 = oracle.expansion_matrix_atom(o4, o4.states(), s.ind_mat, labels,
+                                          np.ascontiguousarray(v.T), CM)
+        e3 = oracle.expansion_matrix_atom(o3, o3.states(), s.ind_mat, labels,
+                                          np.ascontiguousarray(v.T), CM)
+        tol = 1e-10 * np.abs(direct).max()
+        assert np.max(np.abs(direct - e4)) <= tol
+        assert (np.max(np.abs(direct - e3)) <= tol) == ok3
+
+
+def test_type3_orthonormal_functions(mq, oracle):
+    """V = 1: the direct quadrature gives the unit matrix in Hartree per cm^-1 (Gauss-Legendre
+    in beta itself integrates the trigonometric integrand to 1e-12 from 30 points)."""
+    s, o3, _ = systems(mq, oracle)
+    R = np.array([5.0, 6.0])
+    grid = (30, 14)
+    V = np.ones((len(R),) + grid)
+    pes = oracle.OraclePes(0, 0, np.zeros(1), table=V.reshape(-1))
+    m, _, _ = oracle.build_matrix(o3, o3.states(), s.ind_mat, R, grid + (0, 0, 0, 0, 1), pes,
+                                  mij_cut=0.0)
+    diag = s.ind_mat[:, 0] == s.ind_mat[:, 1]
+    assert np.allclose(m[diag], CM, rtol=1e-12, atol=0)
+    assert np.max(np.abs(m[~diag])) <= 1e-13 * CM
