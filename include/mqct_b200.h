@@ -145,8 +145,9 @@ typedef struct mqct_err_report_t {
   double rms_rel_err;        /* out                                            */
 } mqct_err_report_t;
 
-/* Matrix build (SYS_TYPE 1, 3, 4 and 0; SYS_TYPE 3 reads k from sys->ka1 and eps from
- * sys->kc1 and forms the symmetric-top vectors itself): M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
+/* Matrix build (SYS_TYPE 1, 3, 4, 9 and 0; SYS_TYPE 3 reads k from sys->ka1 and eps
+ * from sys->kc1, SYS_TYPE 9 its second rotor's k from sys->ka2 and eps from sys->kc2,
+ * and both form the symmetric-top vectors themselves): M_k(R_i) = C sum_g w_g V(R_i,g) Re(psi_st1(g)* psi_st2(g))
  * (MQCT_SOURCE_CODES/pot_comp.f:1947-1952, 2535-2557, 3709-3721), converted to
  * Hartree, MIJ_CUTOFF truncation at R~r_cut1/r_cut2
  * (MQCT_SOURCE_CODES/matrix_ini.f:1969-1997, columns whose max |M| there is
@@ -167,11 +168,12 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
  * SYS_TYPE 4 (asymmetric top + atom, case 4 at :6955-7075), SYS_TYPE 5 (two diatoms, distinguishable partners, case 5 at
  * :7076-7386; j2 per channel in sys->j2, vec1 unused), SYS_TYPE 7 (symmetric top + diatom, case 7 at :7593-7824; the channel's k in
  * sys->ka1, its parity eps in sys->kc1, vec1 unused), SYS_TYPE 8 (asymmetric top +
- * diatom, case 8 at :7826-8058) and SYS_TYPE 0 (two asymmetric tops, distinguishable
- * partners, case 0 at :8257-8672).  The arrays are the reference's own:
+ * diatom, case 8 at :7826-8058), SYS_TYPE 9 (asymmetric top + symmetric top, case 9 at
+ * :8059-8256; the second rotor's k in sys->ka2, its eps in sys->kc2, vec2 unused) and
+ * SYS_TYPE 0 (two asymmetric tops, distinguishable partners, case 0 at :8257-8672).  The arrays are the reference's own:
  *   a_top  A_TOP(5, nterms): per term 5 int32, (l, -, ...) for SYS_TYPE 1, (l, nju, -,
  *          ...) for SYS_TYPE 3 and 4, (l1, l2, l, -, -) for SYS_TYPE 5, (l1, nju1, l2, l, -) for SYS_TYPE 7 and 8, (l1, nju1, l2,
- *          nju2, l) for SYS_TYPE 0 (:6276-6338);
+ *          nju2, l) for SYS_TYPE 9 and 0 (:6276-6338);
  *   terms  expansion_terms(n_r_coll, nterms): terms[t * nR + iR], R fastest, in the
  *          energy unit of the PES_EXPAN_TERMS.DAT file;
  *   e_unit conv_unit_e, the Hartree value of that unit (MQCT_SOURCE_CODES/matrix_ini.f:918-921:
@@ -448,7 +450,7 @@ int mqct_read_mtrx_uf(const char* path, int32_t state_rec_len, int32_t* state_re
 
 /* Formatted MTRX.DAT (SAVE_MTRX / READ_MTRX with UNFORMAT = NO): PRINT_MIJ and READ_MIJ,
  * MQCT_SOURCE_CODES/matrix_ini.f:4692-4877 and 5794-6630.  Five header counts, the
- * state table (the columns of state_rec, SYS_TYPE 1, 3, 4, 5, 7, 8 or 0 for the writer), the
+ * state table (the columns of state_rec, SYS_TYPE 1, 3, 4, 5, 7, 8, 9 or 0 for the writer), the
  * pairs, the R grid (e19.12) and one line (k, iR, Mij) per element (e19.12).  The
  * header reader returns the counts and the number of state columns. */
 int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
@@ -503,7 +505,7 @@ int mqct_write_cross_sections(const char* path, double U_cm, int32_t chann_ini, 
 int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
 
 /* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
- * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 1, 3, 4, 7, 8 and 0: the
+ * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 1, 3, 4, 7, 8, 9 and 0: the
  * quadrature projection of the PES tabulated on the angular grid onto the expansion
  * terms,
  *   terms[t * nR + iR]    = sum_g V Re(EXPANSION_TERM_t) w(g)    (intgrlr)
@@ -513,7 +515,7 @@ int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
  * grid->n_gamma = gamma1 and, for SYS_TYPE 0, grid->n_gamma2 = gamma2 (on [0, 2 pi],
  * midpoint-equidistant when eq_gamma, else Gauss-Legendre); grid->n_alpha unused.
  * V in the reference's V_3_2 / V_TRANSFER order, V[iR][alpha2][beta1][beta2][gamma1]
- * (SYS_TYPE 7, 8) or V[iR][alpha2][beta1][beta2][gamma1][gamma2] (SYS_TYPE 0), in the
+ * (SYS_TYPE 7, 8) or V[iR][alpha2][beta1][beta2][gamma1][gamma2] (SYS_TYPE 9 and 0), in the
  * unit the terms are wanted in.  For a rotor and an atom (cases 1, 3 and 4, :4973-5104;
  * case 3 is case 4) V is V_2_1, V[iR][beta] (SYS_TYPE 1, grid->n_beta), or V_3_1,
  * V[iR][beta][gamma] (SYS_TYPE 3 and 4, grid->n_beta and grid->n_gamma), and a_top

@@ -55,6 +55,9 @@ class CollisionSystem:
     (MQCT_SOURCE_CODES/iotest.f:8311-8312); k and eps are kept in ka1 and kc1, and vec1 holds
     the parity-adapted top (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) over K;
     sys_type 8: channels (j1, ka1, kc1, j2), EIGEN_VAL + BE j2(j2+1) (MQCT_SOURCE_CODES/iotest.f:9069-9079);
+    sys_type 9: channels (j1, ka1, kc1, j2, k2, eps2), EIGEN_VAL(A,B,C) + A2 j2(j2+1) -
+    (A2-C2) k2^2 (MQCT_SOURCE_CODES/iotest.f:9445-9498); k2 and eps2 are kept in ka2 and
+    kc2, vec2 holds the second rotor's parity-adapted vector;
     sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..);
     identical=True (IDENTICAL = YES): parity-adapted states with their exchange parity
     (self.parity), pairs only between equal parities (MQCT_SOURCE_CODES/matrix_ini.f:482-627).
@@ -118,6 +121,23 @@ class CollisionSystem:
                 a = 1.0 / np.sqrt(2.0 * (1.0 + (k == 0)))
                 self.vec1[i, j + k] += a
                 self.vec1[i, j - k] += -a if eps else a
+        elif sys_type == 9:
+            self.ka1, self.kc1 = np.ascontiguousarray(ch[:, 1]), np.ascontiguousarray(ch[:, 2])
+            self.j2, self.ka2, self.kc2 = (np.ascontiguousarray(ch[:, 3]),
+                                           np.ascontiguousarray(ch[:, 4]),
+                                           np.ascontiguousarray(ch[:, 5]))
+            A2 = A if A2 is None else A2
+            C2 = C if C2 is None else C2
+            for i in range(nch):
+                e1, v1 = asym_top_level(A, B, C, *map(int, ch[i, 0:3]))
+                j, k, eps = map(int, ch[i, 3:6])
+                if not (0 <= k <= j and eps in (0, 1) and not (k == 0 and eps == 1)):
+                    raise ValueError(f"bad symmetric-top level {tuple(ch[i, 3:6])}")
+                E[i] = e1 + A2 * j * (j + 1.0) - (A2 - C2) * k ** 2
+                self.vec1[i, :len(v1)] = v1
+                a = 1.0 / np.sqrt(2.0 * (1.0 + (k == 0)))
+                self.vec2[i, j + k] += a
+                self.vec2[i, j - k] += -a if eps else a
         elif sys_type == 0:
             self.ka1, self.kc1 = np.ascontiguousarray(ch[:, 1]), np.ascontiguousarray(ch[:, 2])
             self.j2, self.ka2, self.kc2 = (np.ascontiguousarray(ch[:, 3]),
@@ -155,7 +175,7 @@ class CollisionSystem:
             ind = np.zeros(2 * P, np.int32)
             check(L.mqct_fill_ind_mat_identical(n, self.m12, self.parity, ind))
         else:
-            j2p = ptr(self.j2) if sys_type in (5, 7, 8, 0) else None
+            j2p = ptr(self.j2) if sys_type in (5, 7, 8, 9, 0) else None
             n = check(L.mqct_count_states(self.sys_type, nch, self.j1, j2p))
             self.indx_chann = np.zeros(n, np.int32)
             self.j12 = np.zeros(n, np.int32)
@@ -859,8 +879,8 @@ def _projection_grid(V, sys_type, eq_gamma):
         return _abi.Grid(V.shape[1], V.shape[2] if sys_type != 1 else 0, 0, 0, 0, 0,
                          1 if eq_gamma else 0)
     nR, n2, n3, n4, n5 = V.shape[:5]
-    n6 = V.shape[5] if sys_type == 0 else 0
-    if sys_type == 0 and V.ndim != 6 or sys_type != 0 and V.ndim != 5:
+    n6 = V.shape[5] if sys_type in (0, 9) else 0
+    if sys_type in (0, 9) and V.ndim != 6 or sys_type not in (0, 9) and V.ndim != 5:
         raise ValueError("V must be (nR, n_alpha2, n_beta1, n_beta2, n_gamma1[, n_gamma2])")
     return _abi.Grid(n3, n5, 0, n4, n2, n6, 1 if eq_gamma else 0)
 

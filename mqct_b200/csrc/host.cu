@@ -175,14 +175,14 @@ int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int
 }
 
 // States per channel: m = -j..j (types 1, 4) or j12 = |j1-j2|..j1+j2 with its m
-// (types 5, 7, 8, 0), channel-major; type 3 like 1 and 4 (MQCT_SOURCE_CODES/matrix_ini.f:148-173, 261-544).
+// (types 5, 7, 8, 9, 0), channel-major; type 3 like 1 and 4 (MQCT_SOURCE_CODES/matrix_ini.f:148-173, 261-544).
 int mqct_count_states(int32_t sys_type, int32_t n_channels, const int32_t* j1,
                       const int32_t* j2) {
   if (n_channels <= 0 || !j1) return MQCT_E_ARG;
   int st = 0;
   for (int i = 0; i < n_channels; ++i) {
     if (sys_type == 1 || sys_type == 3 || sys_type == 4) st += 2 * j1[i] + 1;
-    else if (sys_type == 5 || sys_type == 7 || sys_type == 8 || sys_type == 0) {
+    else if (sys_type == 5 || sys_type == 7 || sys_type == 8 || sys_type == 9 || sys_type == 0) {
       if (!j2) return MQCT_E_ARG;
       for (int js = abs(j1[i] - j2[i]); js <= j1[i] + j2[i]; ++js) st += 2 * js + 1;
     } else {
@@ -509,6 +509,8 @@ static const char* const* mtrx_dat_columns(int coll_type, int* n) {
   static const char* c5[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "J2"};
   static const char* c7[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K", "EPS", "J2"};
   static const char* c8[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K1A", "K1C", "J2"};
+  static const char* c9[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "K1A", "K1C",
+                             "J2", "K2", "EPS"};
   static const char* c0[] = {"#STATE", "#CHANNEL", "J12", "M12", "J1", "KA1", "KC1",
                              "J2", "KA2", "KC2", "P"};
   switch (coll_type) {
@@ -518,6 +520,7 @@ static const char* const* mtrx_dat_columns(int coll_type, int* n) {
     case 5: *n = 6; return c5;
     case 7: *n = 8; return c7;
     case 8: *n = 8; return c8;
+    case 9: *n = 10; return c9;
     case 0: *n = 10; return c0;  // 11 with the exchange parity of identical partners
     default: *n = 0; return nullptr;
   }
@@ -529,7 +532,7 @@ int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
                         const double* mat) {
   int ncol = 0;
   const char* const* cols = mtrx_dat_columns(coll_type, &ncol);
-  MQCT_ARG_CHECK(cols, "mqct_write_mtrx_dat: SYS_TYPE %d not supported (1, 3, 4, 5, 7, 8, 0)",
+  MQCT_ARG_CHECK(cols, "mqct_write_mtrx_dat: SYS_TYPE %d not supported (1, 3, 4, 5, 7, 8, 9, 0)",
                  coll_type);
   MQCT_ARG_CHECK(path && state_rec && ind_mat && R && mat && P > 0 && nR > 1 && n_states > 0,
                  "mqct_write_mtrx_dat: bad arguments");
@@ -546,12 +549,14 @@ int mqct_write_mtrx_dat(const char* path, int32_t coll_type, int32_t n_channels,
   fprintf(f, "NUMBER_OF_STATES= %6d\n", n_states);
   fprintf(f, "MATRIX_SIZE= %9lld\n", (long long)P);
   fprintf(f, "R_GRID_SIZE= %4d\n", nR);
-  // the P column of identical partners is a2 / i2 (matrix_ini.f:4846-4857)
-  for (int c = 0; c < ncol; ++c) fprintf(f, c == 0 ? "%8s" : (c == 10 ? " %2s" : " %8s"), cols[c]);
+  // the P column of identical partners is a2 / i2 (matrix_ini.f:4846-4857); SYS_TYPE 9
+  // writes the columns after #CHANNEL as a3 / i3 (:4821-4832)
+  auto width = [&](int c) { return c == 0 || c == 1 ? 8 : (c == 10 ? 2 : (coll_type == 9 ? 3 : 8)); };
+  for (int c = 0; c < ncol; ++c) fprintf(f, c == 0 ? "%*s" : " %*s", width(c), cols[c]);
   fputc('\n', f);
   for (int st = 0; st < n_states; ++st) {
     for (int c = 0; c < ncol; ++c)
-      fprintf(f, c == 0 ? "%8d" : (c == 10 ? " %2d" : " %8d"), state_rec[(size_t)st * ncol + c]);
+      fprintf(f, c == 0 ? "%*d" : " %*d", width(c), state_rec[(size_t)st * ncol + c]);
     fputc('\n', f);
   }
   fprintf(f, "%16s %8s %8s\n", "MIJ_INDEX", "ST_1", "ST_2");
@@ -734,14 +739,14 @@ int mqct_read_expansion_terms(const char* path, int32_t nR, int32_t n_terms, dou
 
 // The writer of CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:5918-6270): appends
 // to the file; the header line ("R_Bohr" then one a19 label v_l1_nju1_l2_l, or
-// v_l1_nju1_l2_nju2_l for SYS_TYPE 0, per term, 3 blanks after each) only when the file
+// v_l1_nju1_l2_nju2_l for SYS_TYPE 0 and 9, per term, 3 blanks after each) only when the file
 // holds at most one line, then per R point f6.2, 1x and e19.12 with 3 blanks per term.
 int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_terms,
                                const int32_t* a_top, int32_t nR, const double* R,
                                const double* terms) {
   MQCT_ARG_CHECK(path && a_top && R && terms && nR > 0 && n_terms > 0, "bad arguments");
-  MQCT_ARG_CHECK(sys_type == 7 || sys_type == 8 || sys_type == 0,
-                 "PES_EXPAN_TERMS.DAT is written here for SYS_TYPE 7, 8 and 0");
+  MQCT_ARG_CHECK(sys_type == 7 || sys_type == 8 || sys_type == 9 || sys_type == 0,
+                 "PES_EXPAN_TERMS.DAT is written here for SYS_TYPE 7, 8, 9 and 0");
   int lines = 0;
   if (FILE* in = fopen(path, "r")) {
     std::string line;
@@ -757,7 +762,8 @@ int mqct_write_expansion_terms(const char* path, int32_t sys_type, int32_t n_ter
     for (int t = 0; t < n_terms; ++t) {
       const int32_t* q = a_top + 5 * t;
       char lab[96];
-      if (sys_type == 0) snprintf(lab, sizeof lab, "v_%d_%d_%d_%d_%d", q[0], q[1], q[2], q[3], q[4]);
+      if (sys_type == 0 || sys_type == 9)  // :6191-6214 as case 0
+        snprintf(lab, sizeof lab, "v_%d_%d_%d_%d_%d", q[0], q[1], q[2], q[3], q[4]);
       else snprintf(lab, sizeof lab, "v_%d_%d_%d_%d", q[0], q[1], q[2], q[3]);
       lab[19] = 0;  // a19 keeps the leftmost 19 characters
       if (t == 0) fprintf(f, "%-6s ", "R_Bohr");

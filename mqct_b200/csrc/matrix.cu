@@ -641,40 +641,60 @@ static int nearest_index(const std::vector<double>& R, double r) {
   return best;
 }
 
+// The parity-adapted symmetric-top vectors over K = -j..j of the levels (j, k, eps),
+// (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)): WF_SYM_TOP
+// (MQCT_SOURCE_CODES/basis_wave_functions.f:118-151) as a WF_ASYM_TOP vector.  out holds
+// n_ch rows of ld values.
+static int sym_top_vectors(int n_ch, const int32_t* j, const int32_t* k, const int32_t* eps,
+                           int ld, std::vector<double>& out) {
+  MQCT_ARG_CHECK(j && k && eps && n_ch > 0 && ld > 0, "symmetric-top levels missing");
+  out.assign((size_t)n_ch * ld, 0.0);
+  for (int c = 0; c < n_ch; ++c) {
+    const int jj = j[c], kk = k[c], e = eps[c];
+    MQCT_ARG_CHECK(jj >= 0 && jj <= 40 && 2 * jj + 1 <= ld && kk >= 0 && kk <= jj &&
+                       (e == 0 || e == 1) && !(kk == 0 && e == 1),
+                   "bad symmetric-top level at channel %d (j=%d k=%d eps=%d, ld=%d)", c + 1, jj,
+                   kk, e, ld);
+    const double a = 1.0 / sqrt(2.0 * (kk == 0 ? 2.0 : 1.0));
+    out[(size_t)c * ld + jj + kk] += a;
+    out[(size_t)c * ld + jj - kk] += e ? -a : a;
+  }
+  return MQCT_OK;
+}
+
 int MatrixPlan::init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P_, const double* R,
                      int32_t nR_, const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec,
                      double mij_cut, double rc1, double rc2) {
   MQCT_ARG_CHECK(sys && ind_mat && R && grid && pes, "null argument");
   MQCT_ARG_CHECK(sys->sys_type == 1 || sys->sys_type == 3 || sys->sys_type == 4 ||
-                     sys->sys_type == 0,
-                 "matrix build supports SYS_TYPE 1, 3, 4 and 0 (got %d)", sys->sys_type);
+                     sys->sys_type == 9 || sys->sys_type == 0,
+                 "matrix build supports SYS_TYPE 1, 3, 4, 9 and 0 (got %d)", sys->sys_type);
   if (sys->sys_type == 3) {
-    // WF_SYM_TOP (MQCT_SOURCE_CODES/basis_wave_functions.f:118-151) is WF_ASYM_TOP with the
-    // vector (|j k> + (1 - 2 eps) |j -k>) / sqrt(2 (1 + delta_k0)) over K, and case 3 of
+    // WF_SYM_TOP is WF_ASYM_TOP with the parity-adapted vector, and case 3 of
     // INTEGRATOR_TEMP (pot_comp.f:2259-2303) integrates as case 4 without an alpha grid.
-    MQCT_ARG_CHECK(sys->ka1 && sys->kc1 && sys->j1 && sys->n_channels > 0,
-                   "SYS_TYPE 3 needs j, k (ka1) and eps (kc1) per channel");
+    MQCT_ARG_CHECK(sys->n_channels > 0 && sys->j1, "SYS_TYPE 3 needs j, k (ka1), eps (kc1)");
     MQCT_ARG_CHECK(grid->n_alpha == 0, "SYS_TYPE 3 has no alpha grid");
     int jmax = 0;
-    for (int c = 0; c < sys->n_channels; ++c) {
-      const int j = sys->j1[c], kk = sys->ka1[c], e = sys->kc1[c];
-      MQCT_ARG_CHECK(j >= 0 && j <= 40 && kk >= 0 && kk <= j && (e == 0 || e == 1) &&
-                         !(kk == 0 && e == 1),
-                     "bad symmetric-top channel %d (j=%d k=%d eps=%d)", c + 1, j, kk, e);
-      jmax = std::max(jmax, j);
-    }
+    for (int c = 0; c < sys->n_channels; ++c) jmax = std::max(jmax, sys->j1[c]);
     const int ld = 2 * jmax + 1;
-    sym_top_vec.assign((size_t)sys->n_channels * ld, 0.0);
-    for (int c = 0; c < sys->n_channels; ++c) {
-      const int j = sys->j1[c], kk = sys->ka1[c];
-      const double a = 1.0 / sqrt(2.0 * (kk == 0 ? 2.0 : 1.0));
-      sym_top_vec[(size_t)c * ld + j + kk] += a;
-      sym_top_vec[(size_t)c * ld + j - kk] += (sys->kc1[c] & 1) ? -a : a;
-    }
+    int rc = sym_top_vectors(sys->n_channels, sys->j1, sys->ka1, sys->kc1, ld, sym_top_vec);
+    if (rc != MQCT_OK) return rc;
     sym_top_sys = *sys;
     sym_top_sys.sys_type = 4;
     sym_top_sys.vec1 = sym_top_vec.data();
     sym_top_sys.ldv = ld;
+    sys = &sym_top_sys;
+  } else if (sys->sys_type == 9) {
+    // asymmetric top + symmetric top: WF_ASYM_TOP_SYM_TOP (basis_wave_functions.f:42-82)
+    // is WF_ASYM_TOP_ASYM_TOP with the second rotor's parity-adapted vector (k in ka2,
+    // eps in kc2), and case 9 of INTEGRATOR_TEMP (pot_comp.f:3350-3538) integrates as case 0.
+    MQCT_ARG_CHECK(sys->n_channels > 0 && sys->j2 && sys->ldv > 0 && !sys->parity,
+                   "SYS_TYPE 9 needs j2, k (ka2), eps (kc2), ldv, distinguishable partners");
+    int rc = sym_top_vectors(sys->n_channels, sys->j2, sys->ka2, sys->kc2, sys->ldv, sym_top_vec);
+    if (rc != MQCT_OK) return rc;
+    sym_top_sys = *sys;
+    sym_top_sys.sys_type = 0;
+    sym_top_sys.vec2 = sym_top_vec.data();
     sys = &sym_top_sys;
   }
   MQCT_ARG_CHECK(P_ > 0 && P_ < ((int64_t)1 << 31), "P out of range");
@@ -1704,6 +1724,8 @@ struct ExpansionPlan {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int n_ch = 0, n_u = 0;
   bool a_stored = false;  // coefficients stored whole in d_A (identical partners, types 1 and 4)
+  std::vector<double> sym_top_vec;  // SYS_TYPE 9: the second rotor's vectors
+  mqct_sys_t sys_map{};
   DevBuf<int> d_k2r, d_ind, d_chan, d_j1, d_j2, d_term_u;
   DevBuf<double> d_K, d_M3, d_fac, d_M, d_gc, d_A;
 
@@ -1839,10 +1861,25 @@ struct ExpansionPlan {
     const int64_t P = P_;
     const int32_t nR = nR_, n_terms = n_terms_;
     MQCT_ARG_CHECK(sys && ind_mat && R && a_top, "null argument");
+    if (sys->sys_type == 9) {
+      // asymmetric top + symmetric top, case 9 (pot_comp.f:8059-8256): case 0 with the
+      // second rotor's K-sum over its parity-adapted vector, the four Clebsch-Gordan terms
+      // CG_1a..CG_4a with coef_parity; IDENTICAL_PES is not built there either
+      MQCT_ARG_CHECK(sys->n_channels > 0 && sys->j2 && sys->ldv > 0 && !sys->parity,
+                     "SYS_TYPE 9 needs j2, k (ka2), eps (kc2), ldv, distinguishable partners");
+      int rc = sym_top_vectors(sys->n_channels, sys->j2, sys->ka2, sys->kc2, sys->ldv,
+                               sym_top_vec);
+      if (rc != MQCT_OK) return rc;
+      sys_map = *sys;
+      sys_map.sys_type = 0;
+      sys_map.vec2 = sym_top_vec.data();
+      sys = &sys_map;
+    }
     const int type_in = sys->sys_type;
     MQCT_ARG_CHECK(type_in == 1 || type_in == 3 || type_in == 4 || type_in == 5 || type_in == 7 ||
                        type_in == 8 || type_in == 0,
-                   "the expansion path supports SYS_TYPE 1, 3, 4, 5, 7, 8 and 0 (got %d)", type_in);
+                   "the expansion path supports SYS_TYPE 1, 3, 4, 5, 7, 8, 9 and 0 (got %d)",
+                   type_in);
     if (type_in == 1 || type_in == 3 || type_in == 4)
       return init_atom(sys, ind_mat, P_, R, nR_, n_terms_, a_top, mij_cutoff_cm, r_cut1, r_cut2);
     // SYS_TYPE 5 (two diatoms, case 5 at pot_comp.f:7076-7386 for distinguishable partners)

@@ -402,8 +402,11 @@ struct mqct_projection_plan {
   }
 
   int init(int sys, int nt, const int32_t* a_top, const mqct_grid_t& g, int identical) {
-    MQCT_ARG_CHECK(sys == 1 || sys == 3 || sys == 4 || sys == 7 || sys == 8 || sys == 0,
-                   "the projection is built for SYS_TYPE 1, 3, 4, 7, 8 and 0 (got %d)", sys);
+    MQCT_ARG_CHECK(sys == 1 || sys == 3 || sys == 4 || sys == 7 || sys == 8 || sys == 9 ||
+                       sys == 0,
+                   "the projection is built for SYS_TYPE 1, 3, 4, 7, 8, 9 and 0 (got %d)", sys);
+    MQCT_ARG_CHECK(!identical || sys == 0, "identical partners are SYS_TYPE 0");
+    if (sys == 9) sys = 0;  // case 9 (pot_comp.f:5418-5765) is case 0; EXPANSION_TERM :3859
     MQCT_ARG_CHECK(nt > 0 && a_top, "no terms");
     MQCT_ARG_CHECK(!identical || sys == 0, "identical partners are SYS_TYPE 0");
     sys_type = sys;

@@ -391,7 +391,7 @@ int orc_count_states(const orc_system* sys) {
   for (int i = 0; i < sys->n_channels; ++i) {
     switch (sys->sys_type) {
       case 1: case 3: case 4: st += 2 * sys->j1[i] + 1; break;
-      case 5: case 7: case 8: case 0: {
+      case 5: case 7: case 8: case 9: case 0: {
         int a = sys->j1[i], b = sys->j2[i];
         for (int js = abs(a - b); js <= a + b; ++js) st += 2 * js + 1;
         break;
@@ -412,7 +412,7 @@ int orc_enumerate_states(const orc_system* sys, int32_t* indx_chann, int32_t* j1
         indx_chann[st] = i + 1; j12[st] = j; m12[st] = m; ej[st] = sys->e_ch[i]; ++st;
       }
     } else if (sys->sys_type == 5 || sys->sys_type == 7 || sys->sys_type == 8 ||
-               sys->sys_type == 0) {
+               sys->sys_type == 9 || sys->sys_type == 0) {
       int a = sys->j1[i], b = sys->j2[i];
       for (int js = abs(a - b); js <= a + b; ++js)
         for (int m = -js; m <= js; ++m) {
@@ -577,7 +577,7 @@ static void orc_make_agrid(int sys_type, const orc_grid* g, orc_agrid* a) {
   memset(a, 0, sizeof(*a));
   a->nb = g->n_beta;
   orc_axis_gl(g->n_beta, 0.0, ORC_PI, &a->bx, &a->bw, &a->xbl);
-  if (sys_type == 3 || sys_type == 4 || sys_type == 0) {
+  if (sys_type == 3 || sys_type == 4 || sys_type == 9 || sys_type == 0) {
     a->ng = g->n_gamma;
     if (g->eq_gamma) orc_axis_mid(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
     else orc_axis_gl(g->n_gamma, 0.0, 2 * ORC_PI, &a->gx, &a->gw, &a->xgl);
@@ -586,7 +586,7 @@ static void orc_make_agrid(int sys_type, const orc_grid* g, orc_agrid* a) {
     a->na = g->n_alpha;
     orc_axis_mid(g->n_alpha, 0.0, 2 * ORC_PI, &a->ax, &a->aw, &a->xal);
   }
-  if (sys_type == 0) {
+  if (sys_type == 0 || sys_type == 9) {
     a->nbb = g->n_beta2;
     orc_axis_gl(g->n_beta2, 0.0, ORC_PI, &a->bbx, &a->bbw, &a->xbbl);
     a->naa = g->n_alpha2;
@@ -607,7 +607,8 @@ static void orc_free_agrid(orc_agrid* a) {
 static int64_t orc_agrid_size(int sys_type, const orc_agrid* a) {
   if (sys_type == 1) return a->nb;
   if (sys_type == 3 || sys_type == 4) return (int64_t)a->nb * a->ng * (a->na > 0 ? a->na : 1);
-  if (sys_type == 0) return (int64_t)a->naa * a->nb * a->nbb * a->ng * a->ngg;
+  if (sys_type == 0 || sys_type == 9)
+    return (int64_t)a->naa * a->nb * a->nbb * a->ng * a->ngg;
   return -1;
 }
 
@@ -623,7 +624,7 @@ static void orc_wf_state(const orc_system* sys, int ch, int j12, int m12, double
     orc_wf_asym(sys->j1[ch], sys->vec1 + (size_t)ch * sys->ldv, m12, al, be, ga, re, im);
   } else if (sys->sys_type == 3) {
     orc_wf_sym(sys->j1[ch], sys->ka1[ch], sys->kc1[ch], m12, 0.0, be, ga, re, im);
-  } else { /* type 0 */
+  } else { /* type 0; type 9 WF_ASYM_TOP_SYM_TOP (SRC/basis_wave_functions.f:42-82) */
     int j1 = sys->j1[ch], j2 = sys->j2[ch];
     double wr = 0.0, wi = 0.0;
     for (int m1 = -j1; m1 <= j1; ++m1) {
@@ -631,7 +632,10 @@ static void orc_wf_state(const orc_system* sys, int ch, int j12, int m12, double
       if (abs(m2) > j2) continue;
       double dr1, di1, dr2, di2;
       orc_wf_asym(j1, sys->vec1 + (size_t)ch * sys->ldv, m1, al, be, ga, &dr1, &di1);
-      orc_wf_asym(j2, sys->vec2 + (size_t)ch * sys->ldv, m2, aal, bbe, gga, &dr2, &di2);
+      if (sys->sys_type == 9)
+        orc_wf_sym(j2, sys->ka2[ch], sys->kc2[ch], m2, aal, bbe, gga, &dr2, &di2);
+      else
+        orc_wf_asym(j2, sys->vec2 + (size_t)ch * sys->ldv, m2, aal, bbe, gga, &dr2, &di2);
       double cg = orc_cg(j1, j2, j12, m1, m2, m12);
       wr += cg * (dr1 * dr2 - di1 * di2);
       wi += cg * (dr1 * di2 + di1 * dr2);
@@ -699,6 +703,7 @@ int orc_integrate_elements(const orc_system* sys, int n_states, const int32_t* i
                            int n_threads, double* mat) {
   (void)P;
   if (sys->sys_type == 3 && (!sys->ka1 || !sys->kc1)) return -1;
+  if (sys->sys_type == 9 && (!sys->ka2 || !sys->kc2 || !sys->vec1)) return -1;
   orc_agrid a;
   orc_make_agrid(sys->sys_type, grid, &a);
   int64_t ng = orc_agrid_size(sys->sys_type, &a);
@@ -1637,19 +1642,25 @@ int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
                                const int32_t* j12, const int32_t* m12, int64_t P,
                                const int32_t* ind_mat, int n_terms, const int32_t* labels,
                                int nR, const double* terms, double e_unit, double* mat) {
-  if (sys->sys_type != 0 || !sys->j2 || !sys->vec1 || !sys->vec2) return -1;
+  const int t9 = sys->sys_type == 9;
+  if ((sys->sys_type != 0 && !t9) || !sys->j2 || !sys->vec1) return -1;
+  if (t9 ? (!sys->ka2 || !sys->kc2) : !sys->vec2) return -1;
 #pragma omp parallel for schedule(dynamic)
   for (int64_t k = 0; k < P; ++k) {
     const int sp = ind_mat[2 * k] - 1, spp = ind_mat[2 * k + 1] - 1;
     const int cp = indx_chann[sp] - 1, cpp = indx_chann[spp] - 1;
     const int j1p = sys->j1[cp], j2p = sys->j2[cp], j1pp = sys->j1[cpp], j2pp = sys->j2[cpp];
     const int j12p = j12[sp], j12pp = j12[spp], m = m12[sp];
+    /* SYS_TYPE 9: the second rotor is the symmetric top (j2, k2, eps2) of ka2, kc2 */
+    const int k2p_ = t9 ? sys->ka2[cp] : 0, k2pp_ = t9 ? sys->ka2[cpp] : 0;
+    const int e2p = t9 ? sys->kc2[cp] : 0, e2pp = t9 ? sys->kc2[cpp] : 0;
+    const double coef_parity = 1.0 / sqrt(2.0 * (1.0 + (k2p_ == 0)) * 2.0 * (1.0 + (k2pp_ == 0)));
     const double* v1p = sys->vec1 + (size_t)cp * sys->ldv;
     const double* v1pp = sys->vec1 + (size_t)cpp * sys->ldv;
-    const double* v2p = sys->vec2 + (size_t)cp * sys->ldv;
-    const double* v2pp = sys->vec2 + (size_t)cpp * sys->ldv;
+    const double* v2p = t9 ? NULL : sys->vec2 + (size_t)cp * sys->ldv;
+    const double* v2pp = t9 ? NULL : sys->vec2 + (size_t)cpp * sys->ldv;
     const double coef12 = sqrt((2.0 * j1pp + 1.0) / (2.0 * j1p + 1.0)) *
-                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0));
+                          sqrt((2.0 * j2pp + 1.0) / (2.0 * j2p + 1.0)) * (t9 ? coef_parity : 1.0);
     double* out = mat + (size_t)k * nR;
     for (int i = 0; i < nR; ++i) out[i] = 0.0;
     for (int t = 0; t < n_terms; ++t) {
@@ -1669,10 +1680,18 @@ int orc_expansion_matrix_type0(const orc_system* sys, const int32_t* indx_chann,
           if (abs(k1pp) > j1pp) continue;
           s1 += orc_cg(j1pp, l1, j1p, k1pp, n1, k1p) * v1p[j1p + k1p] * v1pp[j1pp + k1pp];
         }
-        for (int k2p = -j2p; k2p <= j2p; ++k2p) {
-          const int k2pp = k2p - n2;
-          if (abs(k2pp) > j2pp) continue;
-          s2 += orc_cg(j2pp, l2, j2p, k2pp, n2, k2p) * v2p[j2p + k2p] * v2pp[j2pp + k2pp];
+        if (t9) {  /* CG_in_all of case 9, SRC/pot_comp.f:8161-8172 */
+          const double sgp = (e2p & 1) ? -1.0 : 1.0, sgpp = (e2pp & 1) ? -1.0 : 1.0;
+          s2 = orc_cg(j2pp, l2, j2p, k2pp_, n2, k2p_) +
+               orc_cg(j2pp, l2, j2p, k2pp_, n2, -k2p_) * sgp +
+               orc_cg(j2pp, l2, j2p, -k2pp_, n2, k2p_) * sgpp +
+               orc_cg(j2pp, l2, j2p, -k2pp_, n2, -k2p_) * sgp * sgpp;
+        } else {
+          for (int k2p = -j2p; k2p <= j2p; ++k2p) {
+            const int k2pp = k2p - n2;
+            if (abs(k2pp) > j2pp) continue;
+            s2 += orc_cg(j2pp, l2, j2p, k2pp, n2, k2p) * v2p[j2p + k2p] * v2pp[j2pp + k2pp];
+          }
         }
         kt += phase * s1 * s2;
       }
