@@ -1172,18 +1172,17 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, 
   }
   rc = p->execute(dm.p, dy.p, ds.p);
   if (!rc && err && err->n_sampled > 0 && precision != MQCT_PREC_FP64) rc = p->error_report(dm.p, err);
+  if (!rc) rc = copy_d2h_host(Mat_el, dm.p, sizeof(double) * P * nR, p->stream);
+  if (!rc && Mat_el_y2) rc = copy_d2h_host(Mat_el_y2, dy.p, sizeof(double) * P * nR, p->stream);
+  if (!rc && skipped) rc = copy_d2h_host(skipped, ds.p, sizeof(int) * P, p->stream);
   if (!rc) {
-    cudaMemcpyAsync(Mat_el, dm.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, p->stream);
-    if (Mat_el_y2)
-      cudaMemcpyAsync(Mat_el_y2, dy.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost, p->stream);
-    if (skipped) cudaMemcpyAsync(skipped, ds.p, sizeof(int) * P, cudaMemcpyDeviceToHost, p->stream);
     e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) {
       set_error("matrix build failed: %s", cudaGetErrorString(e));
       rc = MQCT_E_CUDA;
     }
-    if (!rc) rc = p->tc_check_status();
   }
+  if (!rc) rc = p->tc_check_status();
   mqct_matrix_plan_destroy(h);
   return rc;
 }
@@ -2221,14 +2220,10 @@ int mqct_build_matrix_expansion(const mqct_sys_t* sys, const int32_t* ind_mat, i
   MQCT_CUDA_TRY(d_sk.alloc((size_t)P));
   rc = p.execute(d_T.p, e_unit, d_mat.p, Mat_el_y2 ? d_y2.p : nullptr, d_sk.p);
   if (rc) return rc;
-  MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el, d_mat.p, sizeof(double) * P * nR, cudaMemcpyDeviceToHost,
-                                p.st));
-  if (Mat_el_y2)
-    MQCT_CUDA_TRY(cudaMemcpyAsync(Mat_el_y2, d_y2.p, sizeof(double) * P * nR,
-                                  cudaMemcpyDeviceToHost, p.st));
-  if (skipped)
-    MQCT_CUDA_TRY(cudaMemcpyAsync(skipped, d_sk.p, sizeof(int32_t) * P, cudaMemcpyDeviceToHost,
-                                  p.st));
+  rc = copy_d2h_host(Mat_el, d_mat.p, sizeof(double) * P * nR, p.st);
+  if (!rc && Mat_el_y2) rc = copy_d2h_host(Mat_el_y2, d_y2.p, sizeof(double) * P * nR, p.st);
+  if (!rc && skipped) rc = copy_d2h_host(skipped, d_sk.p, sizeof(int32_t) * P, p.st);
+  if (rc) return rc;
   MQCT_CUDA_TRY(cudaStreamSynchronize(p.st));
   return MQCT_OK;
 }
