@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = json.load(open(os.path.join(ROOT, "BASELINE.json")))["metric"]
+WORKLOAD = ("asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), grid 48 GL beta x "
+            "48 gamma x 48 alpha, 300 R 3-25 bohr")
+L2_NOTE = "GPU arm: L2 flushed (256 MB write) between timed steps"
 
 
 def _args():
@@ -275,7 +278,7 @@ def run_gpu(a):
         return
     expansion = None if a.no_expansion else run_expansion(mq, syn)
     projection = None if a.no_expansion else run_projection(mq, peaks)
-    cpu = cpu_baseline_matrix(s, R, c2, a.cpu_seconds)
+    cpu = cpu_baseline_matrix(oracle_c2_system(), a.cpu_seconds)
     tc = prec in (mq.PREC_BF16X3, mq.PREC_F16X3)
     tc_name = "F16x3" if prec == mq.PREC_F16X3 else "BF16x3"
     peak = peaks.get("bf16_tflops", 1590.0)
@@ -292,12 +295,10 @@ def run_gpu(a):
         "vs_baseline": None,
         "dtype": (tc_name.lower() + "-fp32acc") if tc else "f64",
         "data": "synthetic (seeded site-site PES; no dataset)",
-        "config": {"workload": "asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), "
-                               "grid 48 GL beta x 48 gamma x 48 alpha, 300 R 3-25 bohr",
-                   "precision": (tc_name + " tcgen05") if tc else "FP64 CUDA cores",
-                   "elements_per_step": n_el, "grid_points": 48 * 48 * 48,
-                   "l2": "flushed (256 MB write) between timed steps",
-                   "parallelism": f"replicas x{world}"},
+        "config": {"workload": WORKLOAD, "l2": L2_NOTE},
+        "build": {"precision": (tc_name + " tcgen05") if tc else "FP64 CUDA cores",
+                  "elements_per_step": n_el, "grid_points": 48 * 48 * 48,
+                  "parallelism": f"replicas x{world}"},
         "segments_ms": {"basis_pes": float(seg[:, 0].mean()), "contraction": contract_ms,
                         "finalize": float(seg[:, 2].mean())},
         "roofline": {"bound": "tensor" if tc else "fp64", "achieved": achieved_tf,
@@ -417,33 +418,74 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
 
 
 # ---------------------------------------------------------------- CPU / reference arm
-def cpu_baseline_matrix(s, R, c2, seconds, n_threads=0):
-    """The reference algorithm (INTEGRATOR_TEMP restated, wavefunctions re-evaluated
-    at every grid point) on a bounded sample of elements at one R point."""
+def _synthetic():
+    """mqct_b200/synthetic.py loaded on its own (numpy only): the seeded inputs of the
+    workloads, without importing the CUDA library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "mqct_synthetic_inputs", os.path.join(ROOT, "mqct_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_c2_system():
+    """The c2 build's inputs from the oracle alone: levels and eigenvectors
+    (orc_asym_top), states, pairs (orc_ind_mat), R grid (orc_rgrid) and the seeded PES;
+    nothing of the CUDA library is loaded."""
     from oracle import pyoracle as po
     po.build()
-    ch = s.channels
-    osys = po.OracleSystem(4, ch[:, 0], ch[:, 1], ch[:, 2], e_ch=s.e_ch,
-                           vec1=s.vec1.reshape(-1), ldv=s.ldv)
+    syn = _synthetic()
+    c2 = syn.config_c2(alpha_grid=True)
+    ch = np.asarray(c2["channels"], np.int32)
+    ldv = 2 * int(ch[:, 0].max()) + 1
+    e_ch = np.zeros(len(ch))
+    vec = np.zeros((len(ch), ldv))
+    for i, (j, ka, kc) in enumerate(ch):
+        e, v = po.asym_top(c2["A"], c2["B"], c2["C"], int(j), int(ka), int(kc))
+        e_ch[i] = e
+        vec[i, :len(v)] = v
+    osys = po.OracleSystem(4, ch[:, 0], ch[:, 1], ch[:, 2], e_ch=e_ch, vec1=vec.reshape(-1),
+                           ldv=ldv)
     states = osys.states()
+    ind = po.ind_mat(states[2])
+    R = po.rgrid(c2["nR"], c2["rmin"], c2["rmax"])
     pd = c2["pes"]
     pes = po.OraclePes(pd["kind"], pd["n_terms"], pd["params"], sites1=pd["sites1"])
+    return dict(c2=c2, osys=osys, states=states, ind=ind, R=R, pes=pes)
+
+
+def cpu_baseline_matrix(sysd, seconds, n_threads=0, seed=0):
+    """The reference algorithm (INTEGRATOR_TEMP restated, wavefunctions re-evaluated
+    at every grid point for every element and R, as the reference does) on a bounded
+    sample of the build: seeded elements spread over the whole pair list (every
+    m-block and j), each at three R points spread over the grid (small, middle and
+    large R).  A short probe sizes the sample to about `seconds` of work."""
+    from oracle import pyoracle as po
+    ind, R = sysd["ind"], sysd["R"]
+    P = len(ind)
     cores = n_threads or os.cpu_count()
-    n_el = cores
-    k0 = s.P // 2
-    t0 = time.perf_counter()
-    po.integrate_elements(osys, states, s.ind_mat, R, c2["grid"], pes, literal=True,
-                          k_range=(k0, k0 + n_el), r_range=(150, 151), n_threads=n_threads)
-    t1 = time.perf_counter() - t0
-    n2 = int(max(cores, min(s.P - k0, n_el * max(1.0, (seconds - t1) / max(t1, 1e-3)))))
-    n2 = (n2 // cores) * cores or cores
-    t0 = time.perf_counter()
-    po.integrate_elements(osys, states, s.ind_mat, R, c2["grid"], pes, literal=True,
-                          k_range=(k0, k0 + n2), r_range=(150, 151), n_threads=n_threads)
-    t2 = time.perf_counter() - t0
-    return {"value": n2 / t2, "unit": "matrix elements/s", "cores": cores, "kind": "port",
-            "sample": f"{n2} elements x 1 R point of the same build (literal INTEGRATOR_TEMP "
-                      f"restatement, {cores} OpenMP threads), {t2:.1f} s"}
+    r_sel = np.array([R[len(R) // 10], R[len(R) // 2], R[(9 * len(R)) // 10]])
+    rng = np.random.default_rng(seed)
+
+    def run(n_el):
+        sel = np.sort(rng.choice(P, n_el, replace=False))
+        sub = np.ascontiguousarray(ind[sel])
+        t0 = time.perf_counter()
+        po.integrate_elements(sysd["osys"], sysd["states"], sub, r_sel, sysd["c2"]["grid"],
+                              sysd["pes"], literal=True, n_threads=n_threads)
+        return time.perf_counter() - t0
+
+    t1 = run(cores)
+    n2 = int(max(cores, min(P, cores * max(1.0, seconds / max(t1, 1e-3)))))
+    n2 = max(cores, (n2 // cores) * cores)
+    t2 = run(n2)
+    n_work = n2 * len(r_sel)
+    return {"value": n_work / t2, "unit": "matrix elements/s", "cores": cores, "kind": "port",
+            "sample": f"{n2} seeded elements spread over the {P} pairs x 3 R points "
+                      f"({', '.join(f'{r:.2f}' for r in r_sel)} bohr) of the same build "
+                      f"(literal INTEGRATOR_TEMP restatement of the oracle, {cores} OpenMP "
+                      f"threads), {t2:.1f} s"}
 
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
@@ -613,27 +655,30 @@ def run_projection(mq, peaks, nR=86):
 
 
 def run_reference(a):
+    """--impl reference: the oracle's restatement of the reference's INTEGRATOR_TEMP on
+    the host cores, inputs built by the oracle alone (the CUDA library is not loaded);
+    every step a bounded sample of the c2 build, the line's value the median over the
+    timed steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    c2, s, R = workload()
-    vals = []
-    for _ in range(a.warmup):
-        cpu_baseline_matrix(s, R, c2, 2.0)
+    sysd = oracle_c2_system()
+    for i in range(a.warmup):
+        cpu_baseline_matrix(sysd, 0.5, seed=1000 + i)
     t0 = time.perf_counter()
-    last = None
-    for _ in range(a.steps):
-        last = cpu_baseline_matrix(s, R, c2, a.cpu_seconds / 2)
+    vals, last = [], None
+    for i in range(a.steps):
+        last = cpu_baseline_matrix(sysd, a.cpu_seconds / 3, seed=i)
         vals.append(last["value"])
-    v = float(np.mean(vals))
+    v = float(np.median(vals))
     line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "matrix elements/s",
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": (time.perf_counter() - t0) / a.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded site-site PES; no dataset)",
-            "config": {"workload": "asym-top+atom matrix build: j<=8 (969 states, 31977 pairs), "
-                                   "grid 48 GL beta x 48 gamma x 48 alpha, 300 R 3-25 bohr"},
-            "cpu_baseline": dict(last, value=v),
+            "config": {"workload": WORKLOAD, "l2": L2_NOTE},
+            "cpu_baseline": dict(last, value=v,
+                                 sample=f"median of {a.steps} steps, each: " + last["sample"]),
             "e2e": {"value": v, "unit": "matrix elements/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

@@ -271,9 +271,12 @@ int mqct_matrix_plan_surrogate_stats(mqct_matrix_plan* plan, int32_t* n_exact_r,
  * output; all device pointers; stream: a cudaStream_t or NULL.  The grid-only
  * coefficients live in a fixed device array of the library, so nR is limited
  * to 399 (MQCT_E_RANGE beyond).  The first call on each device (with that
- * device current) looks up the array's address; make that first call before
- * any stream capture.  Calls that may overlap in time (other streams or host
- * threads) share the array and race: the caller serialises them. */
+ * device current) looks up the array's address and keeps it for the life of
+ * the process; make that first call before any stream capture.  After a
+ * cudaDeviceReset the library's device arrays are reloaded at new addresses, so
+ * a process that resets a device must not call this entry point again.  Calls
+ * that may overlap in time (other streams or host threads) share the array and
+ * race: the caller serialises them. */
 int mqct_spline_y2_noalloc(const double* d_R, int32_t nR, const double* d_mat,
                            const int32_t* d_skipped, int64_t P, double* d_y2, void* stream);
 

@@ -56,8 +56,9 @@ class CollisionSystem:
     the parity-adapted top (|j k> + (-1)^eps |j -k>) / sqrt(2 (1 + delta_k0)) over K;
     sys_type 8: channels (j1, ka1, kc1, j2), EIGEN_VAL + BE j2(j2+1) (MQCT_SOURCE_CODES/iotest.f:9069-9079);
     sys_type 9: channels (j1, ka1, kc1, j2, k2, eps2), EIGEN_VAL(A,B,C) + A2 j2(j2+1) -
-    (A2-C2) k2^2 (MQCT_SOURCE_CODES/iotest.f:9445-9498); k2 and eps2 are kept in ka2 and
-    kc2, vec2 holds the second rotor's parity-adapted vector;
+    (A2-C2) k2^2 (MQCT_SOURCE_CODES/iotest.f:9445-9498, 9670-9677); A2 = B2 of the symmetric
+    top, taken from B2 when A2 is not given, C2 required (iotest.f:9414-9416); k2 and eps2
+    are kept in ka2 and kc2, vec2 holds the second rotor's parity-adapted vector;
     sys_type 0: channels (j1, ka1, kc1, j2, ka2, kc2), EIGEN_VAL(A1..) + EIGEN_VAL(A2..);
     identical=True (IDENTICAL = YES): parity-adapted states with their exchange parity
     (self.parity), pairs only between equal parities (MQCT_SOURCE_CODES/matrix_ini.f:482-627).
@@ -126,8 +127,15 @@ class CollisionSystem:
             self.j2, self.ka2, self.kc2 = (np.ascontiguousarray(ch[:, 3]),
                                            np.ascontiguousarray(ch[:, 4]),
                                            np.ascontiguousarray(ch[:, 5]))
-            A2 = A if A2 is None else A2
-            C2 = C if C2 is None else C2
+            # the second (symmetric) top: A2 = B2, taken from B2 when A2 is not given, and
+            # C2 required (MQCT_SOURCE_CODES/iotest.f:1675-1677, 9414-9416)
+            a2 = 0.0 if A2 is None else float(A2)
+            b2 = 0.0 if B2 is None else float(B2)
+            if a2 + b2 == 0.0:
+                raise ValueError("SYS_TYPE 9: supply A2 or B2 of the symmetric top")
+            A2 = a2 if a2 != 0.0 else b2
+            if C2 is None or float(C2) == 0.0:
+                raise ValueError("SYS_TYPE 9: supply C2 of the symmetric top")
             for i in range(nch):
                 e1, v1 = asym_top_level(A, B, C, *map(int, ch[i, 0:3]))
                 j, k, eps = map(int, ch[i, 3:6])

@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -38,16 +39,23 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objs = []
     flags = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", _host_cxx(),
              "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")] + ARCH
+    cmds = []
     for src in srcs:
         obj = os.path.join(OUT, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= newest_hdr):
             continue
-        cmd = [_nvcc(), "-c", src, "-o", obj] + flags
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append([_nvcc(), "-c", src, "-o", obj] + flags)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [_nvcc(), "-shared", "-o", LIB] + objs + ARCH + ["-ccbin", _host_cxx(), "-lcudart"]
         if verbose:

@@ -21,10 +21,9 @@ constexpr double kAmuToAu = 1822.8885;
 constexpr double kCmToHartree = 1.0 / kEvToWn / kAuToEv;
 
 void set_error(const char* fmt, ...);
-// Device -> pageable host copy of a large result after the work queued on `after`,
-// through pinned staging slots and host threads (hostcopy.cu), complete on return; a
-// small copy is only queued on `after`, so the caller synchronises `after` before it
-// reads any destination.  Returns an MQCT_ code.
+// Device -> pageable host copy of a result after the work queued on `after`: large ones
+// through pinned staging slots and host threads (hostcopy.cu), small ones as one copy on
+// `after`; complete on return either way.  Returns an MQCT_ code.
 int copy_d2h_host(void* dst, const void* src, size_t bytes, cudaStream_t after);
 
 #define MQCT_CUDA_TRY(expr)                                                        \

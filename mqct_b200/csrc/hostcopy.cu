@@ -6,8 +6,8 @@
 // chunks from the device into its slot, waits for that copy and copies the slot into the
 // destination on the CPU, so the device copies of one thread overlap the host copies and
 // page faults of the others.  The slots are pinned once per process; concurrent calls take
-// turns on them.  A copy below two chunks is only queued on the caller's stream, which the
-// caller synchronises before it reads the destination.
+// turns on them.  A copy below two chunks goes through one cudaMemcpyAsync on the caller's
+// stream, which is then synchronised: either way the copy is complete on return.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -44,9 +44,10 @@ bool slots_ready() {  // with g_mu held
 int copy_d2h_host(void* dst, const void* src, size_t bytes, cudaStream_t after) {
   if (bytes == 0) return MQCT_OK;
   std::unique_lock<std::mutex> lk(g_mu);
-  if (bytes < 2 * kChunk || !slots_ready()) {  // queued on `after`; the caller synchronises
+  if (bytes < 2 * kChunk || !slots_ready()) {  // one copy on `after`, complete on return
     lk.unlock();
     MQCT_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, after));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(after));
     return MQCT_OK;
   }
   int dev = 0;

@@ -1243,20 +1243,21 @@ extern "C" int mqct_spline_y2_noalloc(const double* d_R, int32_t nR, const doubl
   double* coef = nullptr;
   {
     // set-up, once per device (with that device current): the address of the
-    // fixed coefficient array
+    // fixed coefficient array, and the kernel's dynamic shared-memory limit raised
+    // once to what the largest accepted grid needs (nothing else launches
+    // spline_kernel, so no later call changes it)
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (!g_noalloc_coef_ptr[dev]) {
       void* p = nullptr;
       MQCT_CUDA_TRY(cudaGetSymbolAddress(&p, g_spline_noalloc_coef));
+      MQCT_CUDA_TRY(cudaFuncSetAttribute(
+          spline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int)(sizeof(double) * 2 * SPL_EL * (size_t)(kNoAllocMaxR + 1))));
       g_noalloc_coef_ptr[dev] = static_cast<double*>(p);
     }
     coef = g_noalloc_coef_ptr[dev];
   }
   const size_t smem = sizeof(double) * 2 * SPL_EL * (size_t)(nR + 1);
-  // the launch limit is a property of the kernel that an allocating plan may
-  // have set lower for its own grid: raise it for this call's nR
-  MQCT_CUDA_TRY(cudaFuncSetAttribute(spline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   spline_coef_kernel<<<1, 1, 0, s>>>(nR, d_R, coef);
   MQCT_CUDA_TRY(cudaGetLastError());

@@ -10,7 +10,10 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import _abi
+# PES kinds of the C ABI (MQCT_PES_* in include/mqct_b200.h).  Kept here as plain
+# numbers so that this module also loads on its own, without the CUDA library (the
+# CPU baseline builds its inputs from it).
+PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3
 
 AMU_TO_AU = 1822.8885          # MQCT_SOURCE_CODES/iotest.f:24
 EV_TO_WN = 8065.5448
@@ -26,7 +29,7 @@ def legendre_pes(n_lambda=7, seed=1):
     A = rng.uniform(1e3, 1e5, n_lambda)
     b = rng.uniform(1.5, 2.5, n_lambda)
     Cc = rng.uniform(1e4, 1e5, n_lambda)
-    return dict(kind=_abi.PES_LEGENDRE, n_terms=n_lambda, params=np.concatenate([A, b, Cc]),
+    return dict(kind=PES_LEGENDRE, n_terms=n_lambda, params=np.concatenate([A, b, Cc]),
                 sites1=None, sites2=None)
 
 
@@ -50,7 +53,7 @@ def site_pes(n_terms=12, seed=2, sites=TRIATOMIC_SITES):
     p[:, 3] = rng.uniform(5.0, 7.0, n_terms)
     p[:, 4] = rng.uniform(1e4, 1e5, n_terms)
     p[:, 5] = p[:, 3]
-    return dict(kind=_abi.PES_SITES1, n_terms=n_terms, params=p.reshape(-1),
+    return dict(kind=PES_SITES1, n_terms=n_terms, params=p.reshape(-1),
                 sites1=np.ascontiguousarray(sites, dtype=np.float64).reshape(-1), sites2=None)
 
 
@@ -81,7 +84,7 @@ def site_pes2(seed=4, sites1=None, sites2=None):
     p[:, 4] = rng.uniform(5.0, 7.0, n)
     p[:, 5] = rng.uniform(1e4, 1e5, n) / 9.0
     p[:, 6] = p[:, 4]
-    return dict(kind=_abi.PES_SITES2, n_terms=n, params=p.reshape(-1),
+    return dict(kind=PES_SITES2, n_terms=n, params=p.reshape(-1),
                 sites1=np.ascontiguousarray(s1).reshape(-1),
                 sites2=np.ascontiguousarray(s2).reshape(-1))
 

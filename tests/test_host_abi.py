@@ -134,3 +134,11 @@ def test_compute_entry_points_validate_arguments(mq):
     h = _abi.vp()
     rc = L.mqct_prop_plan_create(None, 1, C.byref(h))
     assert rc < 0
+
+
+def test_synthetic_pes_kinds_match_the_abi(mq):
+    """The synthetic module keeps the PES kinds as plain numbers (it loads without the
+    CUDA library); they are the C ABI's MQCT_PES_* values."""
+    from mqct_b200 import _abi, synthetic as syn
+    assert (syn.PES_TABLE, syn.PES_LEGENDRE, syn.PES_SITES1, syn.PES_SITES2) == (
+        _abi.PES_TABLE, _abi.PES_LEGENDRE, _abi.PES_SITES1, _abi.PES_SITES2)

@@ -93,3 +93,22 @@ def test_type9_direct_quadrature_and_expansion(mq, oracle):
     e9 = oracle.expansion_matrix_type0(o9, o9.states(), s.ind_mat, LABELS[:10],
                                        np.ascontiguousarray(v.T), CM)
     assert np.max(np.abs(d9 - e9)) <= 1e-10 * np.abs(d9).max()
+
+
+def test_type9_second_top_constants_follow_the_reference(mq):
+    """A2 = B2 of the symmetric top: given as B2 alone (the reference's input form) it
+    gives the same levels as A2; neither, or no C2, is an error (iotest.f:9414-9416)."""
+    base = dict(A=27.9, B=14.5, C=9.3)
+    s_a = mq.CollisionSystem(9, CHANS, A2=9.94, C2=6.23, **base)
+    s_b = mq.CollisionSystem(9, CHANS, B2=9.94, C2=6.23, **base)
+    assert np.array_equal(s_a.e_ch, s_b.e_ch)
+    # distinct constants for the two molecules change the symmetric-top part only
+    s_c = mq.CollisionSystem(9, CHANS, B2=5.0, C2=3.0, **base)
+    for i, c in enumerate(CHANS):
+        e1, _ = mq.asym_top_level(27.9, 14.5, 9.3, *c[:3])
+        j, k = c[3], c[4]
+        assert abs(s_c.e_ch[i] - (e1 + 5.0 * j * (j + 1) - (5.0 - 3.0) * k * k)) < 1e-12
+    with pytest.raises(ValueError):
+        mq.CollisionSystem(9, CHANS, C2=6.23, **base)
+    with pytest.raises(ValueError):
+        mq.CollisionSystem(9, CHANS, A2=9.94, **base)
