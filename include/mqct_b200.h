@@ -159,6 +159,13 @@ int mqct_build_matrix(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P,
                       const mqct_pes_t* pes, int32_t precision, double mij_cutoff_cm,
                       double r_cut1, double r_cut2, double* Mat_el, double* Mat_el_y2,
                       int32_t* skipped, mqct_err_report_t* err);
+/* mqct_build_matrix keeps the plan and device buffers of its last call (one entry,
+ * guarded by a lock): a call whose inputs all equal the last call's (compared by two
+ * 64-bit digests of every array and scalar) copies the inputs to the device again and
+ * runs the kept plan, skipping the set-up and the device allocations.  This releases
+ * that entry (the plan and its device memory); the next call builds anew.  No
+ * counterpart in the reference. */
+void mqct_release_cached_build(void);
 
 /* Matrix build from PES expansion terms (the READ_EXPANSION path: READ_EXPANSION_TERMS
  * + EXPANSION_MATRIX_ELEMENT, MQCT_SOURCE_CODES/pot_comp.f:6276-6395, 6465-8749), for

@@ -27,7 +27,7 @@ __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables",
            "PropagationPlan", "propagate_record", "trajectory_set", "cross_sections",
            "cross_sections_device", "write_mtrx_uf",
            "read_mtrx_uf", "write_mtrx_dat", "read_mtrx_dat", "read_expansion_terms",
-           "spline_y2", "Surrogate", "build_matrix_expansion", "ExpansionPlan", "E_UNIT",
+           "spline_y2", "Surrogate", "release_cached_build", "build_matrix_expansion", "ExpansionPlan", "E_UNIT",
            "expansion_terms_list", "write_expansion_terms_list",
            "MqctError",
            "PREC_FP64", "PREC_BF16X3", "PREC_F16X3", "PROP_FP32", "PROP_FP64", "MODE_STD",
@@ -320,22 +320,36 @@ def _grid_struct(grid):
 
 
 def build_matrix(system: CollisionSystem, R, grid, pes, precision=PREC_FP64, mij_cutoff=1e-12,
-                 r_cut1=6.0, r_cut2=8.0):
+                 r_cut1=6.0, r_cut2=8.0, out=None):
     """MATRIX_MAKE direct integration on the GPU: returns Mat_el (P x nR, Hartree),
-    its spline second derivatives and the MIJ_CUTOFF flags."""
+    its spline second derivatives and the MIJ_CUTOFF flags.  out: optional (mat, y2,
+    skipped) arrays of shapes (P, nR), (P, nR), (P,) to fill (a host loop that reuses
+    its buffers, as the reference's host keeps Mat_el allocated)."""
     R = np.ascontiguousarray(R, np.float64)
     pes = pes if isinstance(pes, PesSpec) else PesSpec.from_dict(pes)
     P, nR = system.P, len(R)
-    mat = np.zeros(P * nR)
-    y2 = np.zeros(P * nR)
-    sk = np.zeros(P, np.int32)
+    if out is not None:
+        mat, y2, sk = out
+        if (mat.shape != (P, nR) or y2.shape != (P, nR) or sk.shape != (P,)
+                or mat.dtype != np.float64 or y2.dtype != np.float64 or sk.dtype != np.int32
+                or not (mat.flags.c_contiguous and y2.flags.c_contiguous and sk.flags.c_contiguous)):
+            raise ValueError("out arrays must be C-contiguous float64 (P, nR) x 2 and int32 (P,)")
+    else:
+        mat = np.zeros((P, nR))
+        y2 = np.zeros((P, nR))
+        sk = np.zeros(P, np.int32)
     s = system.c_struct()
     g = _grid_struct(grid)
     ps = pes.c_struct()
     check(lib().mqct_build_matrix(C.byref(s), np.ascontiguousarray(system.ind_mat.reshape(-1)), P,
                                   R, nR, C.byref(g), C.byref(ps), precision, mij_cutoff, r_cut1,
-                                  r_cut2, mat, ptr(y2), ptr(sk), None))
-    return mat.reshape(P, nR), y2.reshape(P, nR), sk
+                                  r_cut2, mat.reshape(-1), ptr(y2), ptr(sk), None))
+    return mat, y2, sk
+
+
+def release_cached_build():
+    """Free the plan and device buffers that build_matrix keeps from its last call."""
+    lib().mqct_release_cached_build()
 
 
 # Hartree value of the PES_EXPAN_TERMS.DAT energy units (E_UNITS, conv_unit_e of

@@ -14,12 +14,15 @@ void surrogate_feature_map(const void* sur, int* sys_type, double* r_c, double* 
 
 // Per-plan state of the tcgen05 path (contract_tc.cu).
 struct TcInfo {
-  int n_chunks = 0, chunks_per_split = 1, npad = 0, n0 = 0, n1 = 0, nbmax = 0, stages = 3;
-  int tmem_cols = 512, n_blocks = 0, n_sm = 148;
+  int n_chunks = 0, chunks_per_split = 1, npad = 0, nbmax = 0;
+  int n_parts = 1, part_c0[8] = {}, part_nc[8] = {};  // column parts of the radial axis
+  int nbuf = 2;                                        // B / basis-slice buffers
+  uint32_t b_stage = 0, psi_stage = 0;                 // bytes of one such buffer
+  int n_blocks = 0, n_sm = 148;
   size_t smem = 0;
   DevBuf<int> blk_row0, blk_n, blk_m;
   DevBuf<int64_t> blk_img_off;
-  DevBuf<float> alpha, walpha;
+  DevBuf<double> walpha;
   DevBuf<int> wexp;  // F16x3: power-of-two exponent of each W column
 };
 
@@ -76,7 +79,7 @@ struct MatrixPlan {
 
   // tcgen05 split-precision paths (contract_tc.cu)
   int tc_splits = 1, tc_ldp = 0, tc_npad = 0, tc_nchunk = 0;
-  DevBuf<float> d_part;                 // tc_splits x n_rows x tc_ldp
+  DevBuf<double> d_part;                // tc_splits x n_rows x tc_ldp FP64 sums
   DevBuf<unsigned short> d_bimg;        // pre-swizzled B (W) images, hi/lo planes
   DevBuf<float2> d_psi32;               // basis in FP32, chunk-major per row
   DevBuf<int> d_status;
@@ -89,6 +92,7 @@ struct MatrixPlan {
   int init(const mqct_sys_t* sys, const int32_t* ind_mat, int64_t P, const double* R, int32_t nR,
            const mqct_grid_t* grid, const mqct_pes_t* pes, int32_t prec, double mij_cut,
            double rc1, double rc2);
+  int refresh_inputs(const mqct_sys_t* sys, const double* R, const mqct_pes_t* pes);
   int run_basis_and_pes();
   int run_surrogate_pes(const struct PesDev& pd, const struct Type0Dev& t0);
   int execute(double* d_mat, double* d_y2, int32_t* d_skipped);
