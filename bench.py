@@ -49,7 +49,7 @@ def _args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="mqct", choices=["mqct", "reference"])
     p.add_argument("--precision", default="auto", choices=["auto", "f16x3", "bf16x3", "fp64"])
-    p.add_argument("--c3-traj", type=int, default=1024,
+    p.add_argument("--c3-traj", type=int, default=4096,
                    help="trajectories of the propagation workload timed (4096 = full set)")
     p.add_argument("--no-propagation", action="store_true")
     p.add_argument("--no-fp64-form", action="store_true")
@@ -374,9 +374,10 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
     trajs = [mq.Trajectory(float(E[i]), float(l[i]), 1, c3["dt"], c3["r_fin"], c3["r_fin"],
                            max_steps=400000) for i in range(n)]
     res = {}
-    for name, arith, nt in (("fp32", mq.PROP_FP32, n), ("fp64", mq.PROP_FP64, min(n, 256))):
+    for name, arith, nt in (("fp32", mq.PROP_FP32, n), ("fp64", mq.PROP_FP64, n)):
         plan = mq.PropagationPlan(tab, arith)
         plan.run(trajs[:min(8, nt)])  # warm-up
+        plan.tune(trajs[:nt])         # launch shape for these tables (capped probe runs)
         t0 = time.perf_counter()
         amp, cls, diag = plan.run(trajs[:nt])
         wall = time.perf_counter() - t0
@@ -387,7 +388,9 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
                      "table_bytes_per_step": plan.bytes_per_step,
                      "achieved_table_GBs": steps * plan.bytes_per_step / (ms / 1e3) / 1e9,
                      "frac_of_hbm_peak": steps * plan.bytes_per_step / (ms / 1e3) / 1e9 / _peaks()[0]["hbm_gbs"],
-                     "max_status": float(diag[:, 4].max())}
+                     "max_status": float(diag[:, 4].max()),
+                     "launch_shape": dict(zip(("threads_per_cta", "ctas_per_sm", "probe_ms"),
+                                              plan.shape()))}
         if name == "fp32":
             res["prob_fp32"] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
         else:

@@ -417,6 +417,18 @@ int mqct_prop_plan_set_integrator(mqct_prop_plan* plan, const mqct_integrator_t*
 /* CS_APPROX for the following runs of the plan (cs != 0), as MQCT_MODE_CS does for
  * one batch call. */
 int mqct_prop_plan_set_coupled_states(mqct_prop_plan* plan, int32_t cs);
+/* Launch-shape autotuning of the RK4 kernel (no counterpart in the reference, which
+ * runs one trajectory per MPI rank): the shapes 512 threads x 1 CTA per SM and 256
+ * threads x 2 CTAs per SM (each with its own split of the m-blocks into shared-memory
+ * passes) are timed on the first min(n_traj, 4 x SMs) of these trajectories, each capped
+ * at 32 steps, results discarded, and the faster shape is kept for the plan's runs.
+ * mqct_prop_plan_run tunes by itself on its first batch of at least 2 x SMs
+ * trajectories.  mqct_prop_plan_shape reports the shape (threads per CTA, CTAs per SM)
+ * and, after tuning, the probe times in ms (probe_ms[2], may be NULL). */
+int mqct_prop_plan_tune(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,
+                        int32_t mode);
+int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* ctas_per_sm,
+                         float* probe_ms);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
 int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,

@@ -735,6 +735,18 @@ class PropagationPlan:
         """CS_APPROX for the following runs."""
         check(lib().mqct_prop_plan_set_coupled_states(self.h, 1 if cs else 0))
 
+    def tune(self, trajs, mode=MODE_STD):
+        """Time the launch shapes on these trajectories (capped) and keep the faster."""
+        arr = _traj_array(trajs)
+        check(lib().mqct_prop_plan_tune(self.h, C.cast(arr, C.c_void_p), len(arr), mode))
+
+    def shape(self):
+        """(threads per CTA, CTAs per SM, probe ms of the 512x1 and 256x2 shapes)."""
+        t, c = C.c_int32(), C.c_int32()
+        ms = (C.c_float * 2)()
+        check(lib().mqct_prop_plan_shape(self.h, C.byref(t), C.byref(c), ms))
+        return int(t.value), int(c.value), (float(ms[0]), float(ms[1]))
+
     def sync(self):
         check(lib().mqct_prop_plan_sync(self.h))
 

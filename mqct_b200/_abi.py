@@ -94,7 +94,8 @@ EXPORTS = [
     "mqct_surrogate_destroy", "mqct_matrix_plan_set_surrogate", "mqct_matrix_plan_surrogate_stats",
     "mqct_prop_plan_create", "mqct_prop_plan_run", "mqct_prop_plan_run_device",
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
-    "mqct_prop_plan_destroy", "mqct_prop_plan_set_coupled_states",
+    "mqct_prop_plan_destroy", "mqct_prop_plan_set_coupled_states", "mqct_prop_plan_tune",
+    "mqct_prop_plan_shape",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
     "mqct_fill_ind_mat", "mqct_count_states_identical", "mqct_enumerate_states_identical",
     "mqct_count_pairs_identical", "mqct_fill_ind_mat_identical", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
@@ -164,6 +165,9 @@ def lib():
                                              C.c_int32, C.POINTER(AtPaths), C.c_int32,
                                              C.POINTER(Integrator), f64p, f64p, f64p]
     L.mqct_prop_plan_set_coupled_states.argtypes = [vp, C.c_int32]
+    L.mqct_prop_plan_tune.argtypes = [vp, vp, C.c_int64, C.c_int32]
+    L.mqct_prop_plan_shape.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_float)]
     L.mqct_prop_plan_set_integrator.argtypes = [vp, C.POINTER(Integrator)]
     L.mqct_expansion_plan_create.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
                                              C.c_int32, i32p, C.c_double, C.c_double, C.c_double,
