@@ -371,6 +371,11 @@ int mqct_propagate_batch_rec(const mqct_tables_t* tab, const mqct_traj_init_t* i
  * reaches hmin it stays there; a small positive hmin bounds the cost. */
 #define MQCT_INTEG_RK4 0
 #define MQCT_INTEG_ODEINT 1
+/* AT_ADAPT_STP = YES (MQCT_SOURCE_CODES/propagator.f:3034-3049, 3821-3860): RK4 whose
+ * steps in AT mode follow the coupling energy along the saved path; eps carries
+ * AT_ADAPTOL (reference default 0.5), hmin the unscaled TIME_STEP (the smallest step).
+ * Standard-mode runs keep their fixed dt. */
+#define MQCT_INTEG_AT_ADAPT 2
 typedef struct mqct_integrator_t {
   int32_t method;   /* MQCT_INTEG_* */
   double eps;       /* ODEINT accuracy (> 0) */

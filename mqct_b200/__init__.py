@@ -640,13 +640,16 @@ def _traj_array(trajs):
 
 def _integrator(integrator):
     """None or "RK4": RK4 with the trajectories' dt; ("ODEINT", eps, hmin): the adaptive
-    Cash-Karp scheme (PROPAGATOR = ODEINT) with accuracy eps and minimum step hmin."""
+    Cash-Karp scheme (PROPAGATOR = ODEINT) with accuracy eps and minimum step hmin;
+    ("AT_ADAPT", tol, time_step): RK4 whose AT-mode steps follow AT_ADAPT_STP with
+    AT_ADAPTOL = tol and the unscaled TIME_STEP as the smallest step."""
     if integrator is None or (isinstance(integrator, str) and integrator.upper() == "RK4"):
         return None
     name, eps, hmin = integrator
-    if name.upper() != "ODEINT":
+    kind = {"ODEINT": _abi.INTEG_ODEINT, "AT_ADAPT": _abi.INTEG_AT_ADAPT}.get(name.upper())
+    if kind is None:
         raise ValueError(f"unknown integrator {name!r}")
-    return _abi.Integrator(_abi.INTEG_ODEINT, float(eps), float(hmin))
+    return _abi.Integrator(kind, float(eps), float(hmin))
 
 
 def propagate(tables: PropagationTables, trajs, arith=PROP_FP64, mode=MODE_STD, at_paths=None,

@@ -89,7 +89,9 @@ struct PropDev {
   const int64_t* at_off;
   const int* at_n;
   const double* at_rec;        // records of 8
-  const double* at_y2;         // per record 4 second derivatives (R, theta, P_theta, P_phi)
+  const double* at_y2;         // per record 5 second derivatives (R, theta, P_theta, P_phi, pot)
+  int at_adapt;                // AT_ADAPT_STP: RK4 steps from the path's coupling energy
+  double at_tol, at_mintm;     // AT_ADAPTOL and TIME_STEP (the smallest step)
 };
 
 // Classical variables (R, P_R, theta, P_theta, phi, P_phi).
@@ -238,7 +240,7 @@ __device__ inline double at_splint(const double* rec, const double* y2, int n, i
   double xlo = rec[8 * (klo - 1)], xhi = rec[8 * (khi - 1)];
   double h = xhi - xlo, a = (xhi - t) / h, b = (t - xlo) / h;
   return a * rec[8 * (klo - 1) + col] + b * rec[8 * (khi - 1) + col] +
-         ((a * a * a - a) * y2[4 * (klo - 1) + ycol] + (b * b * b - b) * y2[4 * (khi - 1) + ycol]) *
+         ((a * a * a - a) * y2[5 * (klo - 1) + ycol] + (b * b * b - b) * y2[5 * (khi - 1) + ycol]) *
              (h * h) / 6.0;
 }
 
@@ -560,7 +562,7 @@ __device__ inline double kinetic(const Cls& c, double mass) {
 // Classical point of an AT trajectory at time t (thread 0).
 __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc) {
   const double* rec = d.at_rec + 8 * d.at_off[tr];
-  const double* y2 = d.at_y2 + 4 * d.at_off[tr];
+  const double* y2 = d.at_y2 + 5 * d.at_off[tr];
   const int n = d.at_n[tr];
   cc->R = at_splint(rec, y2, n, 1, 0, t);
   cc->th = at_splint(rec, y2, n, 3, 1, t);
@@ -570,9 +572,50 @@ __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc)
   cc->phi = 0.0;
 }
 
+// AT_ADAPT_STP (MQCT_SOURCE_CODES/propagator.f:3034-3049, 3821-3860): the next RK4 step of
+// an AT trajectory from the coupling energy along its path (record column 8).  From tcur,
+// probe points tmchk + tau (i + 1/2) accumulate |pot|; the step ends where
+// (tau i)^4 sum|pot| / i reaches `magic`, at the first sign change of pot (after t = 0), or
+// at the end of the path (then last = true).  Steps below mintm become mintm.  fa carries
+// the last probed value from step to step as in the reference.  Thread 0 only.
+__device__ inline double at_adapt_step(const PropDev& d, int tr, double tcur, double t_end,
+                                       double magic, double& fa, bool& last) {
+  const double* rec = d.at_rec + 8 * d.at_off[tr];
+  const double* y2 = d.at_y2 + 5 * d.at_off[tr];
+  const int n = d.at_n[tr];
+  const double tau = 10.0, tmchk = tcur;
+  double potbox = 0.0, dt = d.at_mintm;
+  for (int stps = 0; stps < (1 << 26);) {  // bounded: the path ends within t_end / tau probes
+    const double tmstp = tmchk + tau * (stps + 0.50);
+    stps += 1;
+    const double fb = at_splint(rec, y2, n, 7, 4, tmstp);
+    potbox += fabs(fb);
+    const double i_max = pow(tau * stps, 4.0) * potbox / stps;
+    bool done = false;
+    if (i_max >= magic) {
+      dt = fmax(tau * (stps - 1), d.at_mintm);
+      done = true;
+    } else if (tmstp > t_end) {
+      dt = t_end - tmchk;
+      last = true;
+      done = true;
+    } else if (tcur > 0.0) {
+      const double r = fa / fb;
+      if (r < 0.0 && r == r) {
+        dt = fmax(tau * (stps - 1), d.at_mintm);
+        done = true;
+      }
+    }
+    fa = fb;
+    if (done) break;
+  }
+  return dt;
+}
+
 // Per-trajectory bookkeeping of thread 0 (shared memory).
 struct Book {
   double tmpR1, tmpR2, eki, eqi;
+  double at_magic, at_fa, at_dt;  // AT_ADAPT_STP state (thread 0)
   int64_t n_rec;
   int status, vib, period, run;
 };
@@ -643,7 +686,16 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
     if (tid == 0) {
       const double k_vec = sqrt(d.mass * 2.0 * ti->e_coll);
       const double l_orb = sqrt(ti->l_real * (ti->l_real + 1.0));
-      *bk = Book{0.0, 0.0, 0.0, 0.0, 0, 0, 0, 0, 1};
+      *bk = Book{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0, 0, 0, 0, 1};
+      if (at && d.at_adapt) {
+        // the step-size scale of AT_ADAPT_STP, once per trajectory
+        const double u_cm = ti->e_coll / kCmToHartree;
+        double tmp3 = -exp(2.0 * kPi * (u_cm - 202.0) / 20.0);
+        if (fabs(tmp3) > 1e16) tmp3 = -1e16;
+        const double tmp4 = 0.30 + 0.80 * tmp3 / (1.0 - tmp3) - 4.250 * tmp3 / pow(1.0 - tmp3, 2.0);
+        const double tol = d.at_tol * pow(u_cm / 300.0, tmp4);
+        bk->at_magic = ti->e_coll * pow(t_end * tol, 4.0);
+      }
       *C = Cls{};
       sm.flag[2] = d.cs ? d.st_blk[s_int] : -1;
       if (!at && l_orb / k_vec > ti->r_start) {
@@ -857,7 +909,17 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
           dt = x2 - tcur;
         }
       } else {
-      if (at && tcur + dt >= t_end) {
+      if (at && d.at_adapt) {
+        if (tid == 0) {
+          bool lst = false;
+          bk->at_dt = at_adapt_step(d, tr, tcur, t_end, bk->at_magic, bk->at_fa, lst);
+          bk->run = lst ? 0 : 1;
+        }
+        __syncthreads();
+        dt = bk->at_dt;
+        last = bk->run == 0;
+        __syncthreads();
+      } else if (at && tcur + dt >= t_end) {
         dt = t_end - tcur;
         last = true;
       }
@@ -1027,6 +1089,8 @@ struct PropPlan {
   int method = MQCT_INTEG_RK4;
   double ode_eps = 1e-6, ode_hmin = 0.0;
   bool cs = false;  // CS_APPROX for every run of the plan
+  int at_adapt = 0;                     // AT_ADAPT_STP (RK4 steps of AT runs)
+  double at_tol = 0.5, at_mintm = 0.0;  // AT_ADAPTOL, TIME_STEP
 
   template <class T, bool A, int TB>
   static const void* pick_tb(int ns) {
@@ -1057,8 +1121,22 @@ struct PropPlan {
 
   int set_integrator(const mqct_integrator_t* in) {
     MQCT_ARG_CHECK(in, "null integrator");
-    MQCT_ARG_CHECK(in->method == MQCT_INTEG_RK4 || in->method == MQCT_INTEG_ODEINT,
+    MQCT_ARG_CHECK(in->method == MQCT_INTEG_RK4 || in->method == MQCT_INTEG_ODEINT ||
+                       in->method == MQCT_INTEG_AT_ADAPT,
                    "unknown integrator %d", in->method);
+    at_adapt = 0;
+    if (in->method == MQCT_INTEG_AT_ADAPT) {
+      // RK4 whose AT steps follow AT_ADAPT_STP; eps = AT_ADAPTOL, hmin = TIME_STEP
+      MQCT_ARG_CHECK(in->eps > 0.0 && in->hmin > 0.0,
+                     "AT_ADAPT_STP needs AT_ADAPTOL (eps) > 0 and TIME_STEP (hmin) > 0");
+      at_adapt = 1;
+      at_tol = in->eps;
+      at_mintm = in->hmin;
+      method = MQCT_INTEG_RK4;
+      MQCT_CUDA_TRY(cudaFuncSetAttribute(kernel_ptr(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes()));
+      return MQCT_OK;
+    }
     if (in->method == MQCT_INTEG_ODEINT) {
       MQCT_ARG_CHECK(in->eps > 0.0 && in->hmin >= 0.0, "ODEINT needs eps > 0 and hmin >= 0");
       // the error control resolves every component to relative eps of |y| + |h dy/dt|;
@@ -1348,6 +1426,9 @@ struct PropPlan {
     d.ode_eps = ode_eps;
     d.ode_hmin = ode_hmin;
     d.at_off = d_at_off.p; d.at_n = d_at_n.p; d.at_rec = d_at_rec.p; d.at_y2 = d_at_y2.p;
+    d.at_adapt = at_adapt;
+    d.at_tol = at_tol;
+    d.at_mintm = at_mintm;
     return d;
   }
 
@@ -1384,16 +1465,16 @@ struct PropPlan {
     }
     // spline second derivatives of R, theta, P_theta, P_phi over t with
     // finite-difference end slopes (MQCT_SOURCE_CODES/propagator.f:3116-3125)
-    std::vector<double> y2((size_t)total * 4, 0.0), u;
-    const int cols[4] = {1, 3, 4, 6};
+    std::vector<double> y2((size_t)total * 5, 0.0), u;
+    const int cols[5] = {1, 3, 4, 6, 7};
     for (int64_t t = 0; t < n_traj; ++t) {
       const double* r = at->rec + 8 * at->rec_off[t];
       const int n = at->n_rec[t];
       for (int i = 0; i + 1 < n; ++i)
         MQCT_ARG_CHECK(r[8 * (i + 1)] > r[8 * i], "AT path %lld: time not increasing", (long long)t);
       u.assign(n, 0.0);
-      for (int a = 0; a < 4; ++a) {
-        double* yy = y2.data() + 4 * at->rec_off[t];
+      for (int a = 0; a < 5; ++a) {
+        double* yy = y2.data() + 5 * at->rec_off[t];
         auto X = [&](int i) { return r[8 * i]; };
         auto Y = [&](int i) { return r[8 * i + cols[a]]; };
         const double yp1 = (Y(1) - Y(0)) / (X(1) - X(0));
@@ -1402,8 +1483,8 @@ struct PropPlan {
         u[0] = (3.0 / (X(1) - X(0))) * ((Y(1) - Y(0)) / (X(1) - X(0)) - yp1);
         for (int i = 1; i < n - 1; ++i) {
           const double sig = (X(i) - X(i - 1)) / (X(i + 1) - X(i - 1));
-          const double p = sig * yy[4 * (i - 1) + a] + 2.0;
-          yy[4 * i + a] = (sig - 1.0) / p;
+          const double p = sig * yy[5 * (i - 1) + a] + 2.0;
+          yy[5 * i + a] = (sig - 1.0) / p;
           u[i] = (6.0 * ((Y(i + 1) - Y(i)) / (X(i + 1) - X(i)) - (Y(i) - Y(i - 1)) / (X(i) - X(i - 1))) /
                       (X(i + 1) - X(i - 1)) -
                   sig * u[i - 1]) /
@@ -1411,8 +1492,8 @@ struct PropPlan {
         }
         const double un =
             (3.0 / (X(n - 1) - X(n - 2))) * (ypn - (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2)));
-        yy[4 * (n - 1) + a] = (un - 0.5 * u[n - 2]) / (0.5 * yy[4 * (n - 2) + a] + 1.0);
-        for (int i = n - 2; i >= 0; --i) yy[4 * i + a] = yy[4 * i + a] * yy[4 * (i + 1) + a] + u[i];
+        yy[5 * (n - 1) + a] = (un - 0.5 * u[n - 2]) / (0.5 * yy[5 * (n - 2) + a] + 1.0);
+        for (int i = n - 2; i >= 0; --i) yy[5 * i + a] = yy[5 * i + a] * yy[5 * (i + 1) + a] + u[i];
       }
     }
     MQCT_CUDA_TRY(d_at_off.upload(at->rec_off, n_traj, stream));

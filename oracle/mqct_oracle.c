@@ -1421,6 +1421,27 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   double t_end = t[n_at - 1];
   int64_t counter = 0;
   int run = 1;
+  /* AT_ADAPT_STP (method 2): the step of every RK4 step from the coupling energy along
+   * the path (column 8 of the records), SRC/propagator.f:3034-3049 and 3821-3860;
+   * eps = AT_ADAPTOL, hmin = TIME_STEP (the smallest step). */
+  double* pot = NULL;
+  double* pot2 = NULL;
+  double magic = 0.0, fa = 0.0;
+  if (tr->method == 2) {
+    pot = (double*)malloc(sizeof(double) * n_at);
+    pot2 = (double*)malloc(sizeof(double) * n_at);
+    for (int i = 0; i < n_at; ++i) pot[i] = rec[8 * i + 7];
+    double yp1 = (pot[1] - pot[0]) / (t[1] - t[0]);
+    double ypn = (pot[n_at - 1] - pot[n_at - 2]) / (t[n_at - 1] - t[n_at - 2]);
+    orc_spline(t, pot, n_at, yp1, ypn, pot2);
+    const double u_cm = tr->e_coll * ORC_EVTOWN * ORC_AUTOEV;
+    const double tmp1 = -0.80, tmp2 = 4.250, damp = 20.0;
+    double tmp3 = -exp(2.0 * ORC_PI * (u_cm - 202.0) / damp);
+    if (fabs(tmp3) > 1e16) tmp3 = -1e16;
+    const double tmp4 = 0.30 - tmp1 * tmp3 / (1.0 - tmp3) - tmp2 * tmp3 / pow(1.0 - tmp3, 2.0);
+    const double tol = tr->eps * pow(u_cm / 300.0, tmp4);
+    magic = tr->e_coll * pow(t_end * tol, 4.0);
+  }
   if (tr->method == 1) {  /* ODEINT: one adaptive call over the whole path (:3888-3905) */
     double hn;
     orc_odeint(n, q, tcur, t_end, tr->eps, dt, tr->hmin, orc_rhs_at, &c, &hn);
@@ -1430,7 +1451,37 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   }
   while (run) {
     ++counter;
-    if ((tcur + dt) >= t_end) {
+    if (tr->method == 2) {
+      const double tau = 10.0, mintm = tr->hmin, tmchk = tcur;
+      double potbox = 0.0;
+      for (int stps = 0;;) {
+        const double tmstp = tmchk + tau * (stps + 0.50);
+        stps += 1;
+        double fb, yp;
+        orc_splint(t, pot, pot2, n_at, tmstp, &fb, &yp);
+        potbox += fabs(fb);
+        const double i_max = pow(tau * stps, 4.0) * potbox / stps;
+        int done = 0;
+        if (i_max >= magic) {
+          dt = tau * (stps - 1);
+          if (dt < mintm) dt = mintm;
+          done = 1;
+        } else if (tmstp > t_end) {
+          dt = t_end - tmchk;
+          run = 0;
+          done = 1;
+        } else if (tcur > 0.0) {
+          const double r = fa / fb;
+          if (r < 0.0 && r == r) {
+            dt = tau * (stps - 1);
+            if (dt < mintm) dt = mintm;
+            done = 1;
+          }
+        }
+        fa = fb;
+        if (done) break;
+      }
+    } else if ((tcur + dt) >= t_end) {
       dt = t_end - tcur;
       run = 0;
     }
@@ -1445,6 +1496,7 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   diag[0] = tcur; diag[1] = (double)counter; diag[2] = fabs(1.0 - Pt); diag[3] = 0.0;
   diag[4] = 0; diag[5] = 0; diag[6] = 0; diag[7] = 0;
   for (int a = 0; a < 4; ++a) { free(c.col[a]); free(c.col2[a]); }
+  free(pot); free(pot2);
   free(t); free(q); free(dq); free(yt); free(dyt); free(dym);
   orc_ws_free(&w);
   return 0;

@@ -149,9 +149,10 @@ typedef struct orc_traj {
   int32_t numb_oscl_prds;  /* stop after this many R oscillations (default 1) */
   double time_lim;         /* <=0: none */
   int64_t max_steps;
-  int32_t method;          /* 0: RK4 (PROPAGATOR = RK4), 1: adaptive Cash-Karp (ODEINT) */
-  double eps;              /* ODEINT accuracy (eps_odeint) */
-  double hmin;             /* ODEINT minimum step (min_t_stp) */
+  int32_t method;          /* 0: RK4 (PROPAGATOR = RK4), 1: adaptive Cash-Karp (ODEINT),
+                              2: AT mode RK4 with AT_ADAPT_STP steps */
+  double eps;              /* ODEINT accuracy (eps_odeint); method 2: AT_ADAPTOL */
+  double hmin;             /* ODEINT minimum step (min_t_stp); method 2: TIME_STEP */
   int32_t cs;              /* CS_APPROX = YES: coupled-states approximation */
 } orc_traj;
 

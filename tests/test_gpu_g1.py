@@ -107,3 +107,30 @@ def test_cross_sections_on_the_device(mq, g1):
     assert partial.shape == ref.shape
     assert np.max(np.abs(partial.cpu().numpy() - ref) / ref) < 2e-7
     assert np.allclose(sigma.cpu().numpy(), g["sigma2_mproj"], rtol=1e-8)
+
+
+def test_at_adaptive_step_matches_oracle(mq, oracle, g1):
+    """AT_ADAPT_STP on the GPU (RK4 steps from the coupling energy along each saved
+    path, AT_ADAPTOL = 5e-4, TIME_STEP the smallest step) against the oracle's
+    restatement on the same paths: the same number of steps and the same end time,
+    probabilities within 1e-8 (FP64)."""
+    g = g1["g"]
+    tab = g1["tab9"]
+    trajs = g1["trajs2"][:6]
+    paths = g1["paths"][:6]
+    amp, _, diag = mq.propagate(tab, trajs, arith=mq.PROP_FP64, mode=mq.MODE_AT,
+                                at_paths=paths,
+                                integrator=("AT_ADAPT", 5e-4, float(g["time_step2"])))
+    otab = oracle.OracleTables(tab.j12, tab.m12, tab.ej, tab.ind_mat, tab.R, tab.mat, tab.y2,
+                               tab.mass_au)
+    N = len(tab.j12)
+    for i, t in enumerate(trajs):
+        tr = oracle.make_traj(t.e_coll, t.l_real, t.s_st, t.dt, t.r_start, t.r_fin,
+                              time_lim=t.time_lim, method=2, eps=5e-4,
+                              hmin=float(g["time_step2"]))
+        oamp, odiag = oracle.dotraject_at(otab, tr, paths[i])
+        assert diag[i, 1] == odiag[1]
+        assert diag[i, 0] == pytest.approx(odiag[0], rel=1e-12)
+        p = amp[i, :N] ** 2 + amp[i, N:] ** 2
+        po = oamp[:N] ** 2 + oamp[N:] ** 2
+        assert np.max(np.abs(p - po)) < 1e-8

@@ -149,3 +149,33 @@ def test_partial_cross_sections_per_j(g1_run):
     mine = (2 * J + 1.0)[:, None] / k ** 2 * np.pi * prob[J // int(g["dl"])] * ABOHR ** 2
     r = ref[:, 1:]
     assert np.max(np.abs(mine - r) / r) < 2e-7   # 8 printed digits
+
+
+def test_at_adaptive_step(oracle, g1_run):
+    """AT_ADAPT_STP (propagator.f:3034-3049, 3821-3860) on the example's second run:
+    steps from the coupling energy along each path, TIME_STEP as the smallest step.
+    No reference example runs it.  With the default AT_ADAPTOL = 0.5 the rule takes
+    steps of thousands of a.u. on these paths and RK4 diverges, as the restated rule
+    does; with AT_ADAPTOL = 5e-4 the run takes about a fifth of the fixed steps and
+    stays within 2e-3 of the fixed-step probabilities."""
+    g = g1_run["g"]
+    mass = float(g["mass_red"]) * AMU
+    U = float(g["U"])
+    E = U / EVTOWN / AUTOEV
+    rmax = float(g["rmax"])
+    s9 = g1_run["s9"]
+    tab9 = _tables(oracle, s9, g1_run["m9"], g["R"], mass)
+    dt2 = float(g["time_step2"]) / np.sqrt(U / 300.0)
+    N = s9.n_states
+    for i, l in enumerate(g["l"][:4]):
+        tr = oracle.make_traj(E, float(l), 1, dt2, rmax, rmax, 1, 1, float(g["time_lim"]),
+                              method=2, eps=5e-4, hmin=float(g["time_step2"]))
+        amp, diag = oracle.dotraject_at(tab9, tr, g1_run["paths"][i])
+        tf = oracle.make_traj(E, float(l), 1, dt2, rmax, rmax, 1, 1, float(g["time_lim"]))
+        amp_f, diag_f = oracle.dotraject_at(tab9, tf, g1_run["paths"][i])
+        assert diag[1] < 0.5 * diag_f[1]
+        assert diag[0] == pytest.approx(diag_f[0], rel=1e-12)   # both end at the path's end
+        assert diag[2] < 1e-3
+        p = amp[:N] ** 2 + amp[N:] ** 2
+        pf = amp_f[:N] ** 2 + amp_f[N:] ** 2
+        assert np.max(np.abs(p - pf)) < 2e-3
