@@ -226,6 +226,15 @@ int mqct_matrix_plan_sync(mqct_matrix_plan* plan);
 /* Flops of the contraction actually executed per build (2*P*nR*K times the
  * number of split-precision products). */
 double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
+/* Split-precision plans (no counterpart in the reference): the tensor-core accumulators
+ * are added to FP64 sums after every group of slices_per_drain alpha points of a
+ * 64-point grid chunk (1..64; more than 1 needs equal alpha weights; the plan's choice is
+ * 2 on an equal-weight alpha grid, else 1).  mqct_matrix_plan_layout reports that choice,
+ * the number of grid-chunk ranges whose FP64 sums the finalize adds, and the number of
+ * radial column parts (0 for the FP64 form). */
+int mqct_matrix_plan_set_drain(mqct_matrix_plan* plan, int32_t slices_per_drain);
+int mqct_matrix_plan_layout(const mqct_matrix_plan* plan, int32_t* slices_per_drain,
+                            int32_t* k_ranges, int32_t* column_parts);
 /* CUDA-event timings (ms) of the last execute, recorded on the plan's stream:
  * t3[0] basis + PES tables, t3[1] contraction, t3[2] finalize (units, cutoff,
  * spline).  Waits for the execute to finish. */

@@ -499,6 +499,16 @@ class MatrixPlan:
                                                    rel_bound, abs_bound_cm, n_check))
         self._sur = sur
 
+    def set_drain(self, slices_per_drain):
+        """Alpha points accumulated on the tensor cores between two FP64 drains."""
+        check(lib().mqct_matrix_plan_set_drain(self.h, int(slices_per_drain)))
+
+    def layout(self):
+        """(alpha points per drain, grid-chunk ranges, radial column parts)."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().mqct_matrix_plan_layout(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return int(a.value), int(b.value), int(c.value)
+
     def surrogate_stats(self):
         """(radial points re-evaluated exactly, largest checked residual ratio) of the
         last execute."""

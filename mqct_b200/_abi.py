@@ -82,7 +82,7 @@ class Integrator(C.Structure):
 # Every symbol declared in include/mqct_b200.h (checked by the ABI test).
 EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
-    "mqct_release_cached_build",
+    "mqct_release_cached_build", "mqct_matrix_plan_set_drain", "mqct_matrix_plan_layout",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
@@ -125,6 +125,9 @@ def lib():
     L.mqct_build_matrix.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
                                     C.POINTER(Grid), C.POINTER(Pes), C.c_int32, C.c_double,
                                     C.c_double, C.c_double, f64p, vp, vp, vp]
+    L.mqct_matrix_plan_set_drain.argtypes = [vp, C.c_int32]
+    L.mqct_matrix_plan_layout.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32)]
     L.mqct_release_cached_build.argtypes = []
     L.mqct_release_cached_build.restype = None
     L.mqct_matrix_plan_create.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,

@@ -256,6 +256,7 @@ __global__ void tc_psiimage_kernel(const double2* __restrict__ psi, int G2, int 
 // ---------------------------------------------------------------- main kernel
 struct TcArgs {
   int n_units, n_parts, n_ks, n_chunks, chunks_per_ks, n_alpha_it, nbmax;
+  int slices_per_drain;           // alpha points accumulated in FP32 between two drains
   int nbuf;                       // B / basis-slice buffers (1 or 2)
   uint32_t b_stage, psi_stage;    // bytes of one B / basis-slice buffer
   TcParts parts;
@@ -397,18 +398,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
               tc_fence_after();
             }
             const uint32_t td = tmem + sc * TC_NC_MAX;
+            // The small products first: (A_hi, B_lo) and (A_lo, B_hi) of every slice of the
+            // group, then (A_hi, B_hi), so that the small terms are added while the
+            // accumulator is still small (the MMA rounds relative to its largest addend).
+            const int ns_grp = min(a.slices_per_drain, a.n_alpha_it - al);
+            bool first = true;
+            for (int pr = 1; pr <= 3; ++pr) {
+              const int prod = pr % 3;  // 1, 2, then 0
+              const uint32_t ap = (prod == 2) ? 1 : 0, bp = (prod == 1) ? 1 : 0;
+              for (int sl = 0; sl < ns_grp; ++sl) {
 #pragma unroll
-            for (int kk = 0; kk < TC_KC / 16; ++kk) {
-              // products: (A_hi, B_hi), (A_hi, B_lo), (A_lo, B_hi)
-#pragma unroll
-              for (int pr = 0; pr < 3; ++pr) {
-                const uint32_t ap = (pr == 2) ? 1 : 0, bp = (pr == 1) ? 1 : 0;
-                const uint64_t ad = smem_desc(aoff + ap * TC_A_PLANE + kk * 2 * lbo_a, lbo_a, 128);
-                const uint64_t bd = smem_desc(boff0 + bp * bplane + kk * 2 * lbo_b, lbo_b, 128);
-                mma_f16(td, ad, bd, idesc, (kk | pr) ? 1u : 0u);
+                for (int kk = 0; kk < TC_KC / 16; ++kk) {
+                  const uint64_t ad = smem_desc(aoff + ap * TC_A_PLANE + kk * 2 * lbo_a, lbo_a, 128);
+                  const uint64_t bd = smem_desc(boff0 + bp * bplane + kk * 2 * lbo_b, lbo_b, 128);
+                  mma_f16(td, ad, bd, idesc, first ? 0u : 1u);
+                  first = false;
+                }
               }
             }
             mma_commit(&ACC_full[sc]);  // the epilogue may read once these MMAs complete
+            al += ns_grp - 1;
           }
           mma_commit(&A_empty[sa]);  // A and B may be overwritten once the chunk's MMAs complete
           mma_commit(&B_empty[sb]);
@@ -484,13 +493,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           ok = false;
           break;
         }
-        for (int al = 0; al < a.n_alpha_it; ++al, ++kacc) {
+        for (int al = 0; al < a.n_alpha_it; al += a.slices_per_drain, ++kacc) {
           const uint32_t sc = kacc & 1u;
           if (!mbar_wait(&ACC_full[sc], full_parity(kacc, 2), abort_flag, a.status, 33)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          // a group of several alpha points shares one (uniform) weight
           const double wa = a.walpha ? a.walpha[al] : 1.0;
           const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + sc * TC_NC_MAX + (uint32_t)(h * nch);
 #pragma unroll
@@ -580,6 +590,12 @@ int MatrixPlan::tc_init() {
   MQCT_CUDA_TRY(t.blk_m.upload(bm, stream));
   MQCT_CUDA_TRY(t.blk_img_off.upload(off, stream));
   if (n_alpha > 0) MQCT_CUDA_TRY(t.walpha.upload(h_walpha, stream));
+  // alpha points per drain: a group shares one weight, so groups of more than one point
+  // need equal weights (the midpoint alpha grid); 2 keeps the drains under the MMA time
+  t.alpha_uniform = true;
+  for (int i = 1; i < n_alpha; ++i)
+    if (h_walpha[i] != h_walpha[0]) t.alpha_uniform = false;
+  t.slices_per_drain = (n_alpha > 1 && t.alpha_uniform) ? 2 : 1;
   // K ranges: split the chunks only to fill the last wave of units (the FP64 sums of
   // every range are written once and added by the finalize)
   cudaDeviceGetAttribute(&t.n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -651,6 +667,7 @@ int MatrixPlan::tc_execute() {
   a.n_chunks = t.n_chunks;
   a.chunks_per_ks = t.chunks_per_split;
   a.n_alpha_it = n_alpha > 0 ? n_alpha : 1;
+  a.slices_per_drain = std::max(1, std::min(t.slices_per_drain, a.n_alpha_it));
   a.nbmax = t.nbmax;
   a.nbuf = t.nbuf;
   a.b_stage = t.b_stage;

@@ -1175,6 +1175,28 @@ int mqct_matrix_plan_timing(mqct_matrix_plan* plan, float* t3) {
   return MQCT_OK;
 }
 
+int mqct_matrix_plan_set_drain(mqct_matrix_plan* plan, int32_t slices_per_drain) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  MQCT_ARG_CHECK(p->tc, "the FP64 form has no tensor-core accumulators to drain");
+  MQCT_ARG_CHECK(slices_per_drain >= 1 && slices_per_drain <= 64, "slices_per_drain %d out of 1..64",
+                 slices_per_drain);
+  MQCT_ARG_CHECK(slices_per_drain == 1 || p->tc->alpha_uniform,
+                 "grouping alpha points needs equal alpha weights");
+  p->tc->slices_per_drain = slices_per_drain;
+  return MQCT_OK;
+}
+
+int mqct_matrix_plan_layout(const mqct_matrix_plan* plan, int32_t* slices_per_drain,
+                            int32_t* k_ranges, int32_t* column_parts) {
+  MQCT_ARG_CHECK(plan && slices_per_drain && k_ranges && column_parts, "null argument");
+  const MatrixPlan* p = reinterpret_cast<const MatrixPlan*>(plan);
+  *slices_per_drain = p->tc ? p->tc->slices_per_drain : 0;
+  *k_ranges = p->tc ? p->tc_splits : 0;
+  *column_parts = p->tc ? p->tc->n_parts : 0;
+  return MQCT_OK;
+}
+
 double mqct_matrix_plan_flops(const mqct_matrix_plan* plan) {
   return plan ? reinterpret_cast<const MatrixPlan*>(plan)->flops() : 0.0;
 }

@@ -17,6 +17,8 @@ struct TcInfo {
   int n_chunks = 0, chunks_per_split = 1, npad = 0, nbmax = 0;
   int n_parts = 1, part_c0[8] = {}, part_nc[8] = {};  // column parts of the radial axis
   int nbuf = 2;                                        // B / basis-slice buffers
+  int slices_per_drain = 1;                            // alpha points per FP64 drain
+  bool alpha_uniform = true;                           // all alpha weights equal
   uint32_t b_stage = 0, psi_stage = 0;                 // bytes of one such buffer
   int n_blocks = 0, n_sm = 148;
   size_t smem = 0;

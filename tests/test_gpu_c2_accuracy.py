@@ -74,7 +74,9 @@ def test_c2_as_written_fp64_form_against_oracle(mq, oracle, gpu_available):
     scale = np.abs(m64).max()
     assert np.max(np.abs(m64[sel] - ref)) <= 1e-11 * scale
     rowmax = np.abs(ref).max(axis=1, keepdims=True)
-    assert np.all(np.abs(m16[sel] - ref) <= 1e-4 * rowmax + 1e-12 * scale)
+    # elements that vanish by symmetry carry rounding noise only: absolute floor 1e-8 of
+    # the largest element (the floor of the per-entry error metric)
+    assert np.all(np.abs(m16[sel] - ref) <= 1e-4 * rowmax + 1e-8 * scale)
     mq.release_cached_build()
 
 
