@@ -171,6 +171,11 @@ def _matrix_bench(mq, s, R, c2, precision, steps, warmup, torch, flush):
     return plan, d_mat, d_sk, np.array(seg)
 
 
+def _layout(plan):
+    q, ks, parts = plan.layout()
+    return {"alpha_points_per_fp64_drain": q, "grid_chunk_ranges": ks, "radial_column_parts": parts}
+
+
 def run_gpu(a):
     import torch
     import mqct_b200 as mq
@@ -218,6 +223,7 @@ def run_gpu(a):
     n_el = s.P * len(R)
     value = world * n_el / (ms / 1e3)
     flops = plan.flops
+    layout = _layout(plan) if prec != mq.PREC_FP64 else None
     contract_ms = float(np.mean(seg[:, 1]))
     achieved_tf = flops / (contract_ms / 1e3) / 1e12
     out = {}
@@ -225,13 +231,19 @@ def run_gpu(a):
     # plain FP64 GPU form of the same build, and the accuracy of the split path
     fp64 = None
     acc = None
+    mat64_host = None
     if not a.no_fp64_form and prec != mq.PREC_FP64:
         plan64, d_mat64, d_sk64, seg64 = _matrix_bench(mq, s, R, c2, mq.PREC_FP64, 1, 1, torch, flush)
         ms64 = float(seg64.sum(axis=1).mean())
-        fp64 = {"ms_per_step": ms64, "speedup": ms64 / ms}
+        c64 = float(seg64[:, 1].mean())
+        fp64 = {"ms_per_step": ms64, "speedup": ms64 / ms,
+                "form": "FP64 tensor cores (mma.sync m8n8k4 f64), the same grid and alpha points",
+                "contraction_ms": c64,
+                "contraction_fp64_tflops": plan64.flops / (c64 / 1e3) / 1e12}
         m1 = d_mat.view(s.P, len(R)).double()
         m0 = d_mat64.view(s.P, len(R)).double()
         acc = matrix_accuracy(m1, m0, d_sk, d_sk64, torch)
+        mat64_host = m0.cpu().numpy()
         plan64.close()
     plan.close()
     del d_mat
@@ -275,7 +287,7 @@ def run_gpu(a):
     # propagation (secondary)
     prop = None
     if not a.no_propagation:
-        prop = run_propagation(mq, syn, s, R, mat, a, torch, world, dist)
+        prop = run_propagation(mq, syn, s, R, mat, a, torch, world, dist, mat64=mat64_host)
 
     if rank != 0:
         if dist is not None:
@@ -301,7 +313,8 @@ def run_gpu(a):
         "dtype": (tc_name.lower() + "-fp32acc") if tc else "f64",
         "data": "synthetic (seeded site-site PES; no dataset)",
         "config": {"workload": WORKLOAD, "l2": L2_NOTE},
-        "build": {"precision": (tc_name + " tcgen05") if tc else "FP64 CUDA cores",
+        "build": {"precision": (tc_name + " tcgen05") if tc else "FP64 tensor cores (mma.sync f64)",
+                  "layout": layout,
                   "elements_per_step": n_el, "grid_points": 48 * 48 * 48,
                   "parallelism": f"replicas x{world}"},
         "segments_ms": {"basis_pes": float(seg[:, 0].mean()), "contraction": contract_ms,
@@ -317,7 +330,10 @@ def run_gpu(a):
         "cpu_baseline": cpu,
         "e2e": {"value": n_el / (float(np.median(e2e_ms)) / 1e3), "unit": "matrix elements/s",
                 "ms": float(np.median(e2e_ms)), "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h),
+                "note": "mqct_build_matrix on host arrays: inputs copied up and Mat_el, y2, "
+                        "flags copied down every call; the plan of the first (untimed) call "
+                        "on the same inputs is reused; host output arrays reused"},
         "clocks": clk.summary(),
         # per build: rotor tables, basis, PES weights, [W column scaling (F16x3)], W image,
         # basis image, contraction, finalize; the FP64 form: tables, basis, PES, contraction,
@@ -356,13 +372,14 @@ def matrix_accuracy(m1, m0, sk1, sk0, torch):
                                      "p99": float(torch.quantile(e_k, 0.99)),
                                      "max": float(e_k.max())},
             "entry_rel_err_above_1e-3_rowmax": {"median": float(samp.median()),
-                                                "p99": float(torch.quantile(samp, 0.99))},
+                                                "p99": float(torch.quantile(samp, 0.99)),
+                                                "max": float(rel.max())},
             "max_abs_err_hartree": float(d.max()),
             "cutoff_flags_differing": int(flag_diff.sum()),
             "max_fp64_element_of_differing_flags": float(rowmax[flag_diff].max()) if bool(flag_diff.any()) else 0.0}
 
 
-def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
+def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
     from mqct_b200 import replicas
     c3 = syn.config_c3()
     tab = mq.PropagationTables.from_system(s, R, mat, syn.config_c2()["mass_amu"])
@@ -419,6 +436,23 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None):
                       "traj_steps": float(diag[:, 1].sum()),
                       "max_status": float(diag[:, 4].max())}
     plan.close()
+    # cross sections from the split-precision matrix against those from the FP64 form's
+    # matrix: the same 256 trajectories propagated in FP64 on each
+    if mat64 is not None:
+        tab64 = mq.PropagationTables.from_system(s, R, mat64, syn.config_c2()["mass_amu"])
+        ns_ = min(256, n)
+        sig = []
+        for tb in (tab, tab64):
+            pl = mq.PropagationPlan(tb, mq.PROP_FP64)
+            amp_, _, _ = pl.run(trajs[:ns_])
+            pl.close()
+            p_ = mq.channel_probabilities(amp_, s.indx_chann, s.n_channels)
+            sig.append(((2 * l[:ns_] + 1)[:, None] * p_).sum(0))
+        keep = sig[1] > 1e-4 * sig[1][1:].max()
+        keep[0] = False
+        res["sigma_rel_diff_matrix_split_vs_fp64"] = {
+            "trajectories": ns_, "channels": int(keep.sum()),
+            "max": float(np.max(np.abs(sig[0][keep] - sig[1][keep]) / sig[1][keep]))}
     res["workload"] = (f"{n} of the 4096 trajectories (b~U(0,15), E log-uniform 50-2000 cm^-1, "
                        "dt=5 a.u., R>25 stop), c2 matrix, retained pairs "
                        f"{tab.P} of {s.P}")

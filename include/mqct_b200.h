@@ -385,6 +385,13 @@ int mqct_propagate_batch_rec(const mqct_tables_t* tab, const mqct_traj_init_t* i
  * AT_ADAPTOL (reference default 0.5), hmin the unscaled TIME_STEP (the smallest step).
  * Standard-mode runs keep their fixed dt. */
 #define MQCT_INTEG_AT_ADAPT 2
+/* PROPAGATOR = ODEINT with bikram_int (bk_int / bk_int_adia,
+ * MQCT_SOURCE_CODES/suppl_routines.f:1468-1856, called at propagator.f:3889-3900,
+ * 3925-3931): one adaptive Cash-Karp call over [0, TIME_LIM] (standard mode; dt is
+ * its first step) or over the whole saved path (AT mode) that stops after any step at
+ * which R > R_fin or the oscillation or orbit caps are reached (in AT mode R and phi
+ * from the path's splines); eps and hmin as for ODEINT; FP64 arithmetic. */
+#define MQCT_INTEG_BK_INT 3
 typedef struct mqct_integrator_t {
   int32_t method;   /* MQCT_INTEG_* */
   double eps;       /* ODEINT accuracy (> 0) */

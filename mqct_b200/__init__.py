@@ -652,11 +652,13 @@ def _integrator(integrator):
     """None or "RK4": RK4 with the trajectories' dt; ("ODEINT", eps, hmin): the adaptive
     Cash-Karp scheme (PROPAGATOR = ODEINT) with accuracy eps and minimum step hmin;
     ("AT_ADAPT", tol, time_step): RK4 whose AT-mode steps follow AT_ADAPT_STP with
-    AT_ADAPTOL = tol and the unscaled TIME_STEP as the smallest step."""
+    AT_ADAPTOL = tol and the unscaled TIME_STEP as the smallest step; ("BK_INT", eps,
+    hmin): ODEINT with bikram_int (one adaptive call with per-step stop rules)."""
     if integrator is None or (isinstance(integrator, str) and integrator.upper() == "RK4"):
         return None
     name, eps, hmin = integrator
-    kind = {"ODEINT": _abi.INTEG_ODEINT, "AT_ADAPT": _abi.INTEG_AT_ADAPT}.get(name.upper())
+    kind = {"ODEINT": _abi.INTEG_ODEINT, "AT_ADAPT": _abi.INTEG_AT_ADAPT,
+            "BK_INT": _abi.INTEG_BK_INT}.get(name.upper())
     if kind is None:
         raise ValueError(f"unknown integrator {name!r}")
     return _abi.Integrator(kind, float(eps), float(hmin))

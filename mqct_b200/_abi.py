@@ -20,7 +20,7 @@ ERRORS = {-1: "MQCT_E_ARG", -2: "MQCT_E_CUDA", -3: "MQCT_E_NODEV", -4: "MQCT_E_I
 PREC_FP64, PREC_BF16X3, PREC_F16X3 = 0, 1, 2
 PROP_FP64, PROP_FP32 = 0, 1
 MODE_STD, MODE_AT, MODE_CS = 0, 1, 2
-INTEG_RK4, INTEG_ODEINT, INTEG_AT_ADAPT = 0, 1, 2
+INTEG_RK4, INTEG_ODEINT, INTEG_AT_ADAPT, INTEG_BK_INT = 0, 1, 2, 3
 PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3
 
 i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")

@@ -62,8 +62,10 @@ constexpr int TC_PSI_LD = 66;    // float2 per staged basis row (64 + pad)
 constexpr int TC_THREADS = 320;
 constexpr int TC_PRODUCERS = TC_THREADS - 64;  // X-producer / epilogue threads
 constexpr int TC_A_PLANE = TC_M * TC_KC * 2;    // bytes of one 16-bit plane of an A stage
-constexpr int TC_NC_MAX = 128;                  // columns of one part (TMEM buffer width)
+constexpr int TC_NC_MAX = 112;                  // columns of one part (TMEM buffer width)
 constexpr int TC_NCH_MAX = TC_NC_MAX / 2;       // columns drained by one epilogue thread
+constexpr int TC_TMEM_COLS = 256;               // allocation (a power of two >= 2 buffers)
+static_assert(2 * TC_NC_MAX <= TC_TMEM_COLS, "two accumulator buffers must fit the allocation");
 constexpr int TC_MAX_PARTS = 8;
 constexpr uint32_t TC_SPIN_LIMIT = kSpinLimit;  // bounded mbarrier waits
 
@@ -98,17 +100,17 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
           smem_u32(bar))
       : "memory");
 }
-// 8 consecutive TMEM columns of this warp's lane quarter (one 32-bit value per lane each).
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8]) {
-  uint32_t r[8];
+// 8 consecutive TMEM columns of this warp's lane quarter (one 32-bit value per lane each);
+// the values are valid after tmem_wait().
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(2 * TC_NC_MAX));
+                 "r"(TC_TMEM_COLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -503,13 +505,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           // a group of several alpha points shares one (uniform) weight
           const double wa = a.walpha ? a.walpha[al] : 1.0;
           const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + sc * TC_NC_MAX + (uint32_t)(h * nch);
+          // batches of up to 16 columns: two loads in flight, one wait per batch
 #pragma unroll
-          for (int i8 = 0; i8 < TC_NCH_MAX / 8; ++i8) {
-            if (8 * i8 < nch) {  // the same for the whole warp
-              float v[8];
-              tmem_ld8(taddr + 8 * i8, v);
+          for (int b16 = 0; b16 < (TC_NCH_MAX + 15) / 16; ++b16) {
+            if (16 * b16 < nch) {  // the same for the whole warp
+              uint32_t r[2][8];
 #pragma unroll
-              for (int e = 0; e < 8; ++e) S[8 * i8 + e] = fma((double)v[e], wa, S[8 * i8 + e]);
+              for (int i = 0; i < 2; ++i)
+                if (16 * b16 + 8 * i < nch) tmem_ld8(taddr + 16 * b16 + 8 * i, r[i]);
+              tmem_wait();
+#pragma unroll
+              for (int i = 0; i < 2; ++i)
+                if (16 * b16 + 8 * i < nch) {
+#pragma unroll
+                  for (int e = 0; e < 8; ++e) {
+                    double& acc = S[16 * b16 + 8 * i + e];
+                    acc = fma((double)__uint_as_float(r[i][e]), wa, acc);
+                  }
+                }
             }
           }
           tc_fence_before();
@@ -530,7 +543,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(2 * TC_NC_MAX));
+                 "r"(TC_TMEM_COLS));
   }
 }
 

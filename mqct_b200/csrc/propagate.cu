@@ -89,7 +89,9 @@ struct PropDev {
   const int64_t* at_off;
   const int* at_n;
   const double* at_rec;        // records of 8
-  const double* at_y2;         // per record 5 second derivatives (R, theta, P_theta, P_phi, pot)
+  const double* at_y2;         // per record kAtCols second derivatives (R, theta, P_theta,
+                               // P_phi, pot, phi)
+  int bk_int;                  // bikram_int: one adaptive call with per-step stop rules
   int at_adapt;                // AT_ADAPT_STP: RK4 steps from the path's coupling energy
   double at_tol, at_mintm;     // AT_ADAPTOL and TIME_STEP (the smallest step)
 };
@@ -227,6 +229,8 @@ __device__ inline SplineAt spline_at(const double* R, int nR, double x, int* hin
   return s;
 }
 
+constexpr int kAtCols = 6;  // splined columns of an AT path record
+
 // Cubic-spline value of an AT path column at time t (splint,
 // MQCT_SOURCE_CODES/suppl_routines.f:968-1002).
 __device__ inline double at_splint(const double* rec, const double* y2, int n, int col, int ycol,
@@ -240,7 +244,7 @@ __device__ inline double at_splint(const double* rec, const double* y2, int n, i
   double xlo = rec[8 * (klo - 1)], xhi = rec[8 * (khi - 1)];
   double h = xhi - xlo, a = (xhi - t) / h, b = (t - xlo) / h;
   return a * rec[8 * (klo - 1) + col] + b * rec[8 * (khi - 1) + col] +
-         ((a * a * a - a) * y2[5 * (klo - 1) + ycol] + (b * b * b - b) * y2[5 * (khi - 1) + ycol]) *
+         ((a * a * a - a) * y2[kAtCols * (klo - 1) + ycol] + (b * b * b - b) * y2[kAtCols * (khi - 1) + ycol]) *
              (h * h) / 6.0;
 }
 
@@ -562,7 +566,7 @@ __device__ inline double kinetic(const Cls& c, double mass) {
 // Classical point of an AT trajectory at time t (thread 0).
 __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc) {
   const double* rec = d.at_rec + 8 * d.at_off[tr];
-  const double* y2 = d.at_y2 + 5 * d.at_off[tr];
+  const double* y2 = d.at_y2 + kAtCols * d.at_off[tr];
   const int n = d.at_n[tr];
   cc->R = at_splint(rec, y2, n, 1, 0, t);
   cc->th = at_splint(rec, y2, n, 3, 1, t);
@@ -581,7 +585,7 @@ __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc)
 __device__ inline double at_adapt_step(const PropDev& d, int tr, double tcur, double t_end,
                                        double magic, double& fa, bool& last) {
   const double* rec = d.at_rec + 8 * d.at_off[tr];
-  const double* y2 = d.at_y2 + 5 * d.at_off[tr];
+  const double* y2 = d.at_y2 + kAtCols * d.at_off[tr];
   const int n = d.at_n[tr];
   const double tau = 10.0, tmchk = tcur;
   double potbox = 0.0, dt = d.at_mintm;
@@ -747,8 +751,13 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
         // ---- ODEINT (MQCT_SOURCE_CODES/suppl_routines.f:1229-1435; called per step dt at
         // propagator.f:3933, over the whole AT path at :3900).  All threads take the same
         // control decisions from block-wide values.
-        const double x1 = tcur, x2 = at ? t_end : tcur + dt;
+        // bikram_int (bk_int / bk_int_adia, MQCT_SOURCE_CODES/suppl_routines.f:1468-1856):
+        // one call over [t, TIME_LIM] (standard) or the whole path (AT) that stops after
+        // any step at which R > R_fin, the R oscillations or the orbits reach their caps
+        const double x1 = tcur, x2 = at ? t_end : (d.bk_int ? ti->time_lim : tcur + dt);
         double x = x1, h = dt_step, hnext = dt_step;
+        double bk_r1 = 0.0, bk_r2 = 0.0;
+        int bk_vib = 0;
         double2 k2[NS], k3[NS], k4[NS], k5[NS], yo[NS], ye[NS];
         // stage input: amplitudes y + h * (combination) into a_in, classical into CT
         auto set_stage = [&](double ts, auto comb, auto ccomb) {
@@ -898,15 +907,39 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
           for (int q = 0; q < NS; ++q)
             if (q < ns) y[q] = yo[q];
           if (tid == 0 && !at) *C = *CO;
+          if (d.bk_int) {
+            if (tid == 0) {
+              // R and phi of the step's end: the classical state, or the AT path's splines
+              const double* rec = at ? d.at_rec + 8 * d.at_off[tr] : nullptr;
+              const double* y2p = at ? d.at_y2 + kAtCols * d.at_off[tr] : nullptr;
+              const double rr = at ? at_splint(rec, y2p, d.at_n[tr], 1, 0, x) : C->R;
+              const double ph = at ? at_splint(rec, y2p, d.at_n[tr], 5, 5, x) : C->phi;
+              bool stop = rr > ti->r_fin;
+              if (!stop) {
+                if (nstp > 2 && (bk_r2 - bk_r1) < 0.0 && (bk_r1 - rr) > 0.0) ++bk_vib;
+                bk_r2 = bk_r1;
+                bk_r1 = rr;
+                stop = bk_vib >= ti->numb_oscl_prds;
+                if (!stop) {
+                  bk->period = (int)(fabs(ph) / 2.0 / kPi);
+                  stop = ti->numb_orb_prds <= bk->period;
+                }
+              }
+              bk->vib = bk_vib;
+              sm.flag[1] = stop ? 1 : 0;
+            }
+            __syncthreads();
+            if (sm.flag[1]) break;
+          }
           __syncthreads();
           if ((x - x2) * (x2 - x1) >= 0.0) break;
           if (fabs(hnext) < d.ode_hmin) hnext = d.ode_hmin;
           h = hnext;
         }
         dt_step = hnext;
-        if (at) {
+        if (at || d.bk_int) {
           last = true;
-          dt = x2 - tcur;
+          dt = x - tcur;  // the path's end, or where bk_int stopped
         }
       } else {
       if (at && d.at_adapt) {
@@ -963,7 +996,7 @@ propagate_kernel(PropDev d, const mqct_traj_init_t* __restrict__ init, int n_tra
           y[q] = make_double2(y[q].x + h6 * (k1[q].x + k[q].x + 2.0 * k23[q].x),
                               y[q].y + h6 * (k1[q].y + k[q].y + 2.0 * k23[q].y));
       }
-      if (kAdaptive && at) tcur = t_end;
+      if (kAdaptive && at && !d.bk_int) tcur = t_end;
       else tcur += dt;
       if (tid == 0) {
         bool run = !last;
@@ -1089,6 +1122,7 @@ struct PropPlan {
   int method = MQCT_INTEG_RK4;
   double ode_eps = 1e-6, ode_hmin = 0.0;
   bool cs = false;  // CS_APPROX for every run of the plan
+  int bk_int = 0;                       // bikram_int (ODEINT with per-step stop rules)
   int at_adapt = 0;                     // AT_ADAPT_STP (RK4 steps of AT runs)
   double at_tol = 0.5, at_mintm = 0.0;  // AT_ADAPTOL, TIME_STEP
 
@@ -1122,9 +1156,10 @@ struct PropPlan {
   int set_integrator(const mqct_integrator_t* in) {
     MQCT_ARG_CHECK(in, "null integrator");
     MQCT_ARG_CHECK(in->method == MQCT_INTEG_RK4 || in->method == MQCT_INTEG_ODEINT ||
-                       in->method == MQCT_INTEG_AT_ADAPT,
+                       in->method == MQCT_INTEG_AT_ADAPT || in->method == MQCT_INTEG_BK_INT,
                    "unknown integrator %d", in->method);
     at_adapt = 0;
+    bk_int = in->method == MQCT_INTEG_BK_INT ? 1 : 0;
     if (in->method == MQCT_INTEG_AT_ADAPT) {
       // RK4 whose AT steps follow AT_ADAPT_STP; eps = AT_ADAPTOL, hmin = TIME_STEP
       MQCT_ARG_CHECK(in->eps > 0.0 && in->hmin > 0.0,
@@ -1137,7 +1172,7 @@ struct PropPlan {
                                          (int)smem_bytes()));
       return MQCT_OK;
     }
-    if (in->method == MQCT_INTEG_ODEINT) {
+    if (in->method == MQCT_INTEG_ODEINT || in->method == MQCT_INTEG_BK_INT) {
       MQCT_ARG_CHECK(in->eps > 0.0 && in->hmin >= 0.0, "ODEINT needs eps > 0 and hmin >= 0");
       // the error control resolves every component to relative eps of |y| + |h dy/dt|;
       // FP32 rounding of the right-hand side (matrix, phases) leaves an error estimate
@@ -1146,7 +1181,7 @@ struct PropPlan {
                      "ODEINT needs FP64 arithmetic (FP32 rounding of the right-hand side "
                      "defeats its error control on small amplitudes)");
     }
-    method = in->method;
+    method = in->method == MQCT_INTEG_BK_INT ? MQCT_INTEG_ODEINT : in->method;
     ode_eps = in->eps;
     ode_hmin = in->hmin;
     if (method == MQCT_INTEG_ODEINT && tpb != PT) return set_shape(PT, 1);
@@ -1427,6 +1462,7 @@ struct PropPlan {
     d.ode_hmin = ode_hmin;
     d.at_off = d_at_off.p; d.at_n = d_at_n.p; d.at_rec = d_at_rec.p; d.at_y2 = d_at_y2.p;
     d.at_adapt = at_adapt;
+    d.bk_int = bk_int;
     d.at_tol = at_tol;
     d.at_mintm = at_mintm;
     return d;
@@ -1465,16 +1501,16 @@ struct PropPlan {
     }
     // spline second derivatives of R, theta, P_theta, P_phi over t with
     // finite-difference end slopes (MQCT_SOURCE_CODES/propagator.f:3116-3125)
-    std::vector<double> y2((size_t)total * 5, 0.0), u;
-    const int cols[5] = {1, 3, 4, 6, 7};
+    std::vector<double> y2((size_t)total * kAtCols, 0.0), u;
+    const int cols[kAtCols] = {1, 3, 4, 6, 7, 5};
     for (int64_t t = 0; t < n_traj; ++t) {
       const double* r = at->rec + 8 * at->rec_off[t];
       const int n = at->n_rec[t];
       for (int i = 0; i + 1 < n; ++i)
         MQCT_ARG_CHECK(r[8 * (i + 1)] > r[8 * i], "AT path %lld: time not increasing", (long long)t);
       u.assign(n, 0.0);
-      for (int a = 0; a < 5; ++a) {
-        double* yy = y2.data() + 5 * at->rec_off[t];
+      for (int a = 0; a < kAtCols; ++a) {
+        double* yy = y2.data() + kAtCols * at->rec_off[t];
         auto X = [&](int i) { return r[8 * i]; };
         auto Y = [&](int i) { return r[8 * i + cols[a]]; };
         const double yp1 = (Y(1) - Y(0)) / (X(1) - X(0));
@@ -1483,8 +1519,8 @@ struct PropPlan {
         u[0] = (3.0 / (X(1) - X(0))) * ((Y(1) - Y(0)) / (X(1) - X(0)) - yp1);
         for (int i = 1; i < n - 1; ++i) {
           const double sig = (X(i) - X(i - 1)) / (X(i + 1) - X(i - 1));
-          const double p = sig * yy[5 * (i - 1) + a] + 2.0;
-          yy[5 * i + a] = (sig - 1.0) / p;
+          const double p = sig * yy[kAtCols * (i - 1) + a] + 2.0;
+          yy[kAtCols * i + a] = (sig - 1.0) / p;
           u[i] = (6.0 * ((Y(i + 1) - Y(i)) / (X(i + 1) - X(i)) - (Y(i) - Y(i - 1)) / (X(i) - X(i - 1))) /
                       (X(i + 1) - X(i - 1)) -
                   sig * u[i - 1]) /
@@ -1492,8 +1528,8 @@ struct PropPlan {
         }
         const double un =
             (3.0 / (X(n - 1) - X(n - 2))) * (ypn - (Y(n - 1) - Y(n - 2)) / (X(n - 1) - X(n - 2)));
-        yy[5 * (n - 1) + a] = (un - 0.5 * u[n - 2]) / (0.5 * yy[5 * (n - 2) + a] + 1.0);
-        for (int i = n - 2; i >= 0; --i) yy[5 * i + a] = yy[5 * i + a] * yy[5 * (i + 1) + a] + u[i];
+        yy[kAtCols * (n - 1) + a] = (un - 0.5 * u[n - 2]) / (0.5 * yy[kAtCols * (n - 2) + a] + 1.0);
+        for (int i = n - 2; i >= 0; --i) yy[kAtCols * i + a] = yy[kAtCols * i + a] * yy[kAtCols * (i + 1) + a] + u[i];
       }
     }
     MQCT_CUDA_TRY(d_at_off.upload(at->rec_off, n_traj, stream));
@@ -1511,7 +1547,8 @@ struct PropPlan {
   }
 };
 
-static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mode) {
+static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mode,
+                         bool bk_int = false) {
   mode &= MQCT_MODE_AT;
   for (int64_t t = 0; t < n; ++t) {
     const mqct_traj_init_t& a = init[t];
@@ -1522,6 +1559,9 @@ static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mod
                      (long long)t);
       MQCT_ARG_CHECK(a.max_steps > 0 || a.time_lim > 0,
                      "trajectory %lld: needs a step cap or a time limit", (long long)t);
+      MQCT_ARG_CHECK(!bk_int || a.time_lim > 0,
+                     "trajectory %lld: bk_int integrates up to TIME_LIM, which must be > 0",
+                     (long long)t);
     }
   }
   return MQCT_OK;
@@ -1536,7 +1576,7 @@ static int validate_init(const mqct_traj_init_t* init, int64_t n, int N, int mod
 static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, int mode,
                     double* amp_out, double* cls_out, double* diag_out,
                     double* rec_out = nullptr, int64_t rec_cap = 0, int64_t* n_rec_out = nullptr) {
-  int rc = validate_init(init, n_traj, p->N, mode);
+  int rc = validate_init(init, n_traj, p->N, mode, p->bk_int != 0);
   if (rc) return rc;
   std::vector<int64_t> order(n_traj);
   for (int64_t t = 0; t < n_traj; ++t) order[t] = t;

@@ -1178,8 +1178,66 @@ static int orc_odeint(int n, double* ystart, double x1, double x2, double eps, d
   return nstp;
 }
 
+/* bk_int (SRC/suppl_routines.f:1468-1653): odeint over [x1, x2] (the whole trajectory)
+ * that stops after any step at which R > cut_r, the R oscillation count reaches
+ * numb_oscl or the orbit count int(|phi| / 2 pi) reaches numb_orb; R and phi are
+ * y[ir], y[iphi].  Returns the steps taken; *f_time is the time reached. */
+typedef void (*orc_probe_fn)(void* pctx, double x, const double* y, double* R, double* phi);
+static int orc_bk_int(int n, double* ystart, double x1, double x2, double eps, double h1,
+                      double hmin, orc_rhs_fn f, void* ctx, double* hnext_io, double* f_time,
+                      double cut_r, orc_probe_fn probe, void* pctx, int numb_oscl, int numb_orb,
+                      int* vib_out, int* period_out) {
+  const int MAXSTP = 10000;
+  double* w = (double*)calloc((size_t)n * 11, sizeof(double));
+  double *y = w, *dydx = w + n, *yscal = w + 2 * n, *ytemp = w + 3 * n, *yerr = w + 4 * n,
+         *yt = w + 5 * n, *ak = w + 6 * n;
+  double x = x1, h = copysign(h1, x2 - x1), hnext = h;
+  double tmp_R1 = 0.0, tmp_R2 = 0.0;
+  int vib = 0, period = 0, nstp;
+  int stopped = 0;
+  for (int i = 0; i < n; ++i) y[i] = ystart[i];
+  for (nstp = 1; nstp <= MAXSTP; ++nstp) {
+    f(ctx, x, y, dydx);
+    if (nstp < MAXSTP) {
+      for (int i = 0; i < n; ++i) yscal[i] = fabs(y[i]) + fabs(h * dydx[i]) + 1e-30;
+      if ((x + h - x2) * (x + h - x1) > 0.0) h = x2 - x;
+      orc_rkqs(n, y, dydx, &x, h, eps, yscal, &hnext, hmin, f, ctx, ytemp, yerr, ak, yt);
+      double rr, ph;
+      probe(pctx, x, y, &rr, &ph);
+      if (rr > cut_r) { stopped = 1; break; }
+      if (nstp > 2 && (tmp_R2 - tmp_R1) < 0.0 && (tmp_R1 - rr) > 0.0) vib += 1;
+      tmp_R2 = tmp_R1;
+      tmp_R1 = rr;
+      if (vib >= numb_oscl) { stopped = 1; break; }
+      period = (int)(fabs(ph) / 2.0 / ORC_PI);
+      if (numb_orb <= period) { stopped = 1; break; }
+    } else {  /* the last allowed step: RK4 over what remains */
+      orc_rk4(n, y, dydx, x, x2 - x, f, ctx, yt, ytemp, yerr);
+      x = x2 + copysign(1e-30, x2 - x1);
+    }
+    if ((x - x2) * (x2 - x1) >= 0.0) break;
+    if (fabs(hnext) < hmin) hnext = copysign(hmin, x2 - x1);
+    h = hnext;
+  }
+  (void)stopped;
+  for (int i = 0; i < n; ++i) ystart[i] = y[i];
+  *hnext_io = hnext;
+  *f_time = x;
+  *vib_out = vib;
+  *period_out = period;
+  free(w);
+  return nstp;
+}
+
 static void orc_rhs_std(void* ctx, double t, const double* y, double* dy) {
   orc_derivs_ws((orc_rhs_ws*)ctx, t, y, dy);
+}
+/* bk_int's R and phi in standard mode: the classical variables of the state. */
+static void orc_probe_std(void* pctx, double x, const double* y, double* R, double* phi) {
+  (void)x;
+  const int N = *(const int*)pctx;
+  *R = y[2 * N];
+  *phi = y[2 * N + 4];
 }
 
 /* Coupling energy sum_k d_f M_k Re(a_i* a_j e^{-i dE t}) (SRC/propagator.f:2725-2788). */
@@ -1263,6 +1321,14 @@ static int orc_dotraject_impl(const orc_tables* tab, const orc_traj* tr, double*
         }
         ++nr;
       }
+      if (tr->method == 3) {  /* ODEINT with bikram_int: one bk_int call (:3925-3931) */
+        double hn, ft;
+        orc_bk_int(n, q, tcur, tr->time_lim, tr->eps, tr->dt, tr->hmin, orc_rhs_std, &w, &hn, &ft,
+                   tr->r_fin, orc_probe_std, &N, tr->numb_oscl_prds, tr->numb_orb_prds, &vib,
+                   &period);
+        tcur = ft;  /* :4172 */
+        break;
+      }
       if (tr->method == 1) {  /* PROPAGATOR = ODEINT: adaptive steps over [t, t + dt] */
         double hn;
         orc_odeint(n, q, tcur, tcur + tr->dt, tr->eps, dt_step, tr->hmin, orc_rhs_std, &w, &hn);
@@ -1345,7 +1411,17 @@ typedef struct {
   const double* t;
   double* col[4];   /* R, theta, P_theta, P_phi */
   double* col2[4];
+  double* phi;      /* phi and its spline (bk_int_adia's orbit count) */
+  double* phi2;
 } orc_at_ctx;
+/* bk_int_adia's R and phi: the saved path's splines at x (SRC/suppl_routines.f:1760-1761). */
+static void orc_probe_at(void* pctx, double x, const double* y, double* R, double* phi) {
+  (void)y;
+  orc_at_ctx* c = (orc_at_ctx*)pctx;
+  double yp;
+  orc_splint(c->t, c->col[0], c->col2[0], c->n_at, x, R, &yp);
+  orc_splint(c->t, c->phi, c->phi2, c->n_at, x, phi, &yp);
+}
 static void orc_rhs_at(void* vctx, double t, const double* q, double* dq) {
   orc_at_ctx* c = (orc_at_ctx*)vctx;
   orc_rhs_ws* w = c->w;
@@ -1411,6 +1487,14 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
     double ypn = (c.col[a][n_at - 1] - c.col[a][n_at - 2]) / (t[n_at - 1] - t[n_at - 2]);
     orc_spline(t, c.col[a], n_at, yp1, ypn, c.col2[a]);
   }
+  c.phi = (double*)malloc(sizeof(double) * n_at);
+  c.phi2 = (double*)malloc(sizeof(double) * n_at);
+  for (int i = 0; i < n_at; ++i) c.phi[i] = rec[8 * i + 5];
+  {
+    double yp1 = (c.phi[1] - c.phi[0]) / (t[1] - t[0]);
+    double ypn = (c.phi[n_at - 1] - c.phi[n_at - 2]) / (t[n_at - 1] - t[n_at - 2]);
+    orc_spline(t, c.phi, n_at, yp1, ypn, c.phi2);
+  }
   double* q = (double*)calloc((size_t)n, sizeof(double));
   double* dq = (double*)calloc((size_t)n, sizeof(double));
   double* yt = (double*)calloc((size_t)n, sizeof(double));
@@ -1441,6 +1525,15 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
     const double tmp4 = 0.30 - tmp1 * tmp3 / (1.0 - tmp3) - tmp2 * tmp3 / pow(1.0 - tmp3, 2.0);
     const double tol = tr->eps * pow(u_cm / 300.0, tmp4);
     magic = tr->e_coll * pow(t_end * tol, 4.0);
+  }
+  if (tr->method == 3) {  /* ODEINT with bikram_int: bk_int_adia over the path (:3889-3896) */
+    double hn, ft;
+    int vib = 0, period = 0;
+    orc_bk_int(n, q, tcur, t_end, tr->eps, dt, tr->hmin, orc_rhs_at, &c, &hn, &ft, tr->r_fin,
+               orc_probe_at, &c, tr->numb_oscl_prds, tr->numb_orb_prds, &vib, &period);
+    tcur = ft;
+    counter = 1;
+    run = 0;
   }
   if (tr->method == 1) {  /* ODEINT: one adaptive call over the whole path (:3888-3905) */
     double hn;
@@ -1496,7 +1589,7 @@ int orc_dotraject_at(const orc_tables* tab, const orc_traj* tr, int n_at, const 
   diag[0] = tcur; diag[1] = (double)counter; diag[2] = fabs(1.0 - Pt); diag[3] = 0.0;
   diag[4] = 0; diag[5] = 0; diag[6] = 0; diag[7] = 0;
   for (int a = 0; a < 4; ++a) { free(c.col[a]); free(c.col2[a]); }
-  free(pot); free(pot2);
+  free(pot); free(pot2); free(c.phi); free(c.phi2);
   free(t); free(q); free(dq); free(yt); free(dyt); free(dym);
   orc_ws_free(&w);
   return 0;

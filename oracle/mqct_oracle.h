@@ -150,7 +150,10 @@ typedef struct orc_traj {
   double time_lim;         /* <=0: none */
   int64_t max_steps;
   int32_t method;          /* 0: RK4 (PROPAGATOR = RK4), 1: adaptive Cash-Karp (ODEINT),
-                              2: AT mode RK4 with AT_ADAPT_STP steps */
+                              2: AT mode RK4 with AT_ADAPT_STP steps, 3: standard mode
+                              ODEINT with bikram_int: one bk_int call over [0, time_lim]
+                              with the stop rules after every adaptive step, dt the
+                              first step (int_1st_stp) */
   double eps;              /* ODEINT accuracy (eps_odeint); method 2: AT_ADAPTOL */
   double hmin;             /* ODEINT minimum step (min_t_stp); method 2: TIME_STEP */
   int32_t cs;              /* CS_APPROX = YES: coupled-states approximation */

@@ -119,3 +119,22 @@ def test_at_mode_matches_oracle(mq, oracle, gpu_available):
     prob = mq.channel_probabilities(amp, s9.indx_chann, 9)
     ref = g["opacity2"][idx, 2:]
     assert np.max(np.abs(prob[1:] - ref[1:])) < 1e-6     # l = 85, 199
+
+
+def test_bk_int_matches_oracle(mq, oracle, g3):
+    """ODEINT with bikram_int on the GPU (one adaptive call over [0, TIME_LIM] with the
+    stop rules after every step) against the oracle's bk_int restatement: the same finish
+    times, probabilities within 1e-8, and the reference's RK4 probabilities within 1e-6."""
+    integ = ("BK_INT", 1e-4, 10.0)
+    amp, cls, diag = mq.propagate(g3["tab"], g3["trajs"], arith=mq.PROP_FP64, integrator=integ)
+    ot = [oracle.make_traj(t.e_coll, t.l_real, t.s_st, t.dt, t.r_start, t.r_fin,
+                           t.numb_orb_prds, t.numb_oscl_prds, t.time_lim, t.max_steps,
+                           method=3, eps=1e-4, hmin=10.0) for t in g3["trajs"]]
+    oamp, ocls, odiag = oracle.propagate_batch(g3["otab"], ot)
+    pg = mq.channel_probabilities(amp, g3["s"].indx_chann, 10)
+    po_ = mq.channel_probabilities(oamp, g3["s"].indx_chann, 10)
+    assert np.max(np.abs(pg - po_)) < 1e-8
+    assert np.allclose(diag[:, 0], odiag[:, 0], rtol=1e-12)
+    assert np.all(cls[:, 0] > float(g3["g"]["rmax"]))
+    ref = g3["g"]["opacity"][[40, 80, 110], 2:]
+    assert np.max(np.abs(pg - ref)) < 1e-6

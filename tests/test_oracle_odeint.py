@@ -64,3 +64,34 @@ def test_odeint_at_mode_matches_reference_rk4(mq, oracle):
         i = list(g["l"]).index(l)
         assert np.max(np.abs(prob - g["opacity2"][i, 2:])) < 1e-6
         assert diag[0] == path[-1, 0] and diag[2] < 1e-10
+
+
+def test_bk_int_standard_mode(oracle):
+    """ODEINT with bikram_int (bk_int, suppl_routines.f:1468-1653): one adaptive call
+    over [0, TIME_LIM] that stops after the step at which R first exceeds R_fin.  On the
+    G3 trajectories it reproduces the reference's RK4 probabilities like the per-dt
+    ODEINT does, and it stops at the first adaptive step beyond R_fin, within one
+    minimum step of the RK4 run's finish time.  The call is capped at 10 000 adaptive
+    steps (MAXSTP), after which the reference takes one RK4 step to TIME_LIM; with
+    amplitudes at rounding level a small minimum step reaches that cap, so hmin is
+    10 a.u. here."""
+    g = _g3()
+    tab, _, _ = _g3_tables(oracle, g)
+    U = float(g["U"])
+    E = U / EVTOWN / AUTOEV
+    dt = float(g["time_step"]) / np.sqrt(U / 300.0)
+    rmax = float(g["rmax"])
+    st = g["states"]
+    N = len(st)
+    ls = [40, 80, 110]
+    trajs = [oracle.make_traj(E, float(l), 1, dt, rmax, rmax, 1, 1, float(g["time_lim"]), 0,
+                              method=3, eps=1e-4, hmin=10.0) for l in ls]
+    amp, cls, diag = oracle.propagate_batch(tab, trajs)
+    p = amp[:, :N] ** 2 + amp[:, N:] ** 2
+    prob = np.zeros((len(ls), 10))
+    for s in range(N):
+        prob[:, st[s, 1] - 1] += p[:, s]
+    assert np.max(np.abs(prob - g["opacity"][ls, 2:])) < 1e-6
+    assert np.all(cls[:, 0] > rmax)                       # stopped just beyond R_fin
+    assert np.all(np.abs(diag[:, 0] - g["deflection"][ls, 4]) <= 10.0)
+    assert np.all(diag[:, 2] < 1e-8)
