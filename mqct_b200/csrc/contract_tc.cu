@@ -505,24 +505,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           // a group of several alpha points shares one (uniform) weight
           const double wa = a.walpha ? a.walpha[al] : 1.0;
           const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + sc * TC_NC_MAX + (uint32_t)(h * nch);
-          // batches of up to 16 columns: two loads in flight, one wait per batch
+          // batches of 8 columns, software-pipelined: the next batch's TMEM load is in
+          // flight while this batch is added to the FP64 sums
+          constexpr int NB8 = TC_NCH_MAX / 8;
+          uint32_t r[2][8];
+          tmem_ld8(taddr, r[0]);
+          tmem_wait();
 #pragma unroll
-          for (int b16 = 0; b16 < (TC_NCH_MAX + 15) / 16; ++b16) {
-            if (16 * b16 < nch) {  // the same for the whole warp
-              uint32_t r[2][8];
+          for (int b8 = 0; b8 < NB8; ++b8) {
+            if (8 * b8 < nch) {  // the same for the whole warp
+              const bool more = 8 * (b8 + 1) < nch;
+              if (more) tmem_ld8(taddr + 8 * (b8 + 1), r[(b8 + 1) & 1]);
 #pragma unroll
-              for (int i = 0; i < 2; ++i)
-                if (16 * b16 + 8 * i < nch) tmem_ld8(taddr + 16 * b16 + 8 * i, r[i]);
-              tmem_wait();
-#pragma unroll
-              for (int i = 0; i < 2; ++i)
-                if (16 * b16 + 8 * i < nch) {
-#pragma unroll
-                  for (int e = 0; e < 8; ++e) {
-                    double& acc = S[16 * b16 + 8 * i + e];
-                    acc = fma((double)__uint_as_float(r[i][e]), wa, acc);
-                  }
-                }
+              for (int e = 0; e < 8; ++e) {
+                double& acc = S[8 * b8 + e];
+                acc = fma((double)__uint_as_float(r[b8 & 1][e]), wa, acc);
+              }
+              if (more) tmem_wait();
             }
           }
           tc_fence_before();
