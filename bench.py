@@ -391,39 +391,66 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
     trajs = [mq.Trajectory(float(E[i]), float(l[i]), 1, c3["dt"], c3["r_fin"], c3["r_fin"],
                            max_steps=400000) for i in range(n)]
     res = {}
-    for name, arith, nt in (("fp32", mq.PROP_FP32, n), ("fp64", mq.PROP_FP64, n)):
+    # right-hand-side work of the lockstep engine: the four knot products per m-block,
+    # 2 (re, im) x 2 flops per matrix entry, 4 right-hand sides per RK4 step
+    _, blk = np.unique(tab.m12, return_counts=True)
+    flops_per_step = 4.0 * 16.0 * float((blk.astype(np.float64) ** 2).sum())
+    props = torch.cuda.get_device_properties(0)
+    fp32_peak = props.multi_processor_count * 128 * 2 * _peaks()[0].get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    probs = {}
+    runs = (("fp32", mq.PROP_FP32, mq.ENGINE_LOCKSTEP),
+            ("fp32_per_trajectory", mq.PROP_FP32, mq.ENGINE_PER_TRAJECTORY),
+            ("fp64", mq.PROP_FP64, mq.ENGINE_PER_TRAJECTORY),
+            ("fp64_lockstep", mq.PROP_FP64, mq.ENGINE_LOCKSTEP))
+    for name, arith, engine in runs:
+        nt = n
         plan = mq.PropagationPlan(tab, arith)
+        plan.set_engine(engine)
         plan.run(trajs[:min(8, nt)])  # warm-up
-        plan.tune(trajs[:nt])         # launch shape for these tables (capped probe runs)
+        if engine == mq.ENGINE_PER_TRAJECTORY:
+            plan.tune(trajs[:nt])     # launch shape for these tables (capped probe runs)
         t0 = time.perf_counter()
         amp, cls, diag = plan.run(trajs[:nt])
         wall = time.perf_counter() - t0
         ms = replicas.max_over_ranks(plan.timing(), dist, device="cuda")
         steps = float(diag[:, 1].sum())
-        res[name] = {"n_traj": nt, "kernel_ms": ms, "wall_s": wall,
-                     "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
-                     "table_bytes_per_step": plan.bytes_per_step,
-                     "achieved_table_GBs": steps * plan.bytes_per_step / (ms / 1e3) / 1e9,
-                     "frac_of_hbm_peak": steps * plan.bytes_per_step / (ms / 1e3) / 1e9 / _peaks()[0]["hbm_gbs"],
-                     "max_status": float(diag[:, 4].max()),
-                     "launch_shape": dict(zip(("threads_per_cta", "ctas_per_sm", "probe_ms"),
-                                              plan.shape()))}
-        if name == "fp32":
-            res["prob_fp32"] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
+        eng, rounds = plan.engine()
+        r = {"n_traj": nt, "kernel_ms": ms, "wall_s": wall,
+             "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
+             "engine": {mq.ENGINE_LOCKSTEP: "lockstep", mq.ENGINE_PER_TRAJECTORY: "per-trajectory"}[eng],
+             "max_status": float(diag[:, 4].max())}
+        if eng == mq.ENGINE_LOCKSTEP:
+            r["rounds"] = rounds
+            r["rhs_flops_per_step"] = flops_per_step
+            r["achieved_tflops"] = steps * flops_per_step / (ms / 1e3) / 1e12
+            if arith == mq.PROP_FP32:
+                r["fp32_peak_tflops_nominal"] = fp32_peak
+                r["frac_of_fp32_peak"] = r["achieved_tflops"] / fp32_peak
         else:
-            p64 = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
-            p32 = res.pop("prob_fp32")[:nt]
-            res["max_abs_prob_diff_fp32_vs_fp64"] = float(np.abs(p32 - p64).max())
-            # opacity-weighted sums sum_traj (2l+1) P_f (cross sections up to a common
-            # factor) of the FP32 and FP64 runs over the same trajectories
-            w = 2 * l[:nt] + 1
-            s32, s64 = (w[:, None] * p32).sum(0), (w[:, None] * p64).sum(0)
-            keep = s64 > 1e-4 * s64[1:].max()
-            keep[0] = False  # elastic channel
-            res["sigma_rel_diff_fp32_vs_fp64"] = {
-                "channels": int(keep.sum()),
-                "max": float(np.max(np.abs(s32[keep] - s64[keep]) / s64[keep]))}
+            r["table_bytes_per_step"] = plan.bytes_per_step
+            r["achieved_table_GBs"] = steps * plan.bytes_per_step / (ms / 1e3) / 1e9
+            r["frac_of_hbm_peak"] = r["achieved_table_GBs"] / _peaks()[0]["hbm_gbs"]
+            r["launch_shape"] = dict(zip(("threads_per_cta", "ctas_per_sm", "probe_ms"), plan.shape()))
+        res[name] = r
+        probs[name] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
         plan.close()
+    p32, p64 = probs["fp32"], probs["fp64"]
+    res["max_abs_prob_diff_fp32_vs_fp64"] = float(np.abs(p32 - p64).max())
+    res["max_abs_prob_diff_engines_fp32"] = float(np.abs(p32 - probs["fp32_per_trajectory"]).max())
+    res["max_abs_prob_diff_engines_fp64"] = float(np.abs(p64 - probs["fp64_lockstep"]).max())
+    # opacity-weighted sums sum_traj (2l+1) P_f (cross sections up to a common factor) of
+    # the FP32 lockstep run and the FP64 form over the same trajectories
+    w = 2 * l[:n] + 1
+    s32, s64 = (w[:, None] * p32).sum(0), (w[:, None] * p64).sum(0)
+    keep = s64 > 1e-4 * s64[1:].max()
+    keep[0] = False  # elastic channel
+    res["sigma_rel_diff_fp32_vs_fp64"] = {
+        "channels": int(keep.sum()),
+        "max": float(np.max(np.abs(s32[keep] - s64[keep]) / s64[keep]))}
+    res["speedup_fp32_lockstep_vs_fp32_per_trajectory"] = (res["fp32"]["traj_per_s"] /
+                                                           res["fp32_per_trajectory"]["traj_per_s"])
+    res["speedup_fp64_lockstep_vs_fp64_form"] = (res["fp64_lockstep"]["traj_per_s"] /
+                                                 res["fp64"]["traj_per_s"])
     res["speedup_fp32_vs_fp64_form"] = res["fp32"]["traj_per_s"] / res["fp64"]["traj_per_s"]
     # the coupled-states approximation (CS_APPROX) on the same trajectories: only the
     # m-block of the initial state is streamed and propagated

@@ -450,6 +450,25 @@ int mqct_prop_plan_tune(mqct_prop_plan* plan, const mqct_traj_init_t* init, int6
                         int32_t mode);
 int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* ctas_per_sm,
                          float* probe_ms);
+/* Propagation engines (no counterpart in the reference, which integrates one trajectory
+ * per MPI rank).  MQCT_ENGINE_PER_TRAJECTORY: the persistent kernel that holds one
+ * trajectory per CTA (every mode and integrator).  MQCT_ENGINE_LOCKSTEP: all trajectories
+ * of the batch advance one RK4 stage per round, grouped by the spline interval of their
+ * stage point, so that a group shares one load of the interval's knot rows; standard
+ * mode, RK4, no CS approximation, no SAVE_TRAJECT records, m-blocks of at most 128
+ * states (other runs take the per-trajectory kernel).  Its right-hand side applies the
+ * spline as four knot products (M_lo, M_hi - M_lo, M''_lo, M''_hi) per interval instead of
+ * interpolating slot by slot: the same arithmetic type, other rounding.  Its device-buffer
+ * runs (mqct_prop_plan_run_device) read the initial conditions back for the bound on the
+ * rounds and return when the batch is done.  MQCT_ENGINE_AUTO (default): the lockstep
+ * engine for eligible batches of at least 1024 trajectories.  mqct_prop_plan_engine
+ * reports the engine of the last run and, for the lockstep engine, the rounds it ran
+ * (rounds may be NULL). */
+#define MQCT_ENGINE_AUTO 0
+#define MQCT_ENGINE_PER_TRAJECTORY 1
+#define MQCT_ENGINE_LOCKSTEP 2
+int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine);
+int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* rounds);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
 int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,

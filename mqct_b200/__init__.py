@@ -19,8 +19,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (MODE_AT, MODE_CS, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError,
-                   check, lib, ptr)
+from ._abi import (ENGINE_AUTO, ENGINE_LOCKSTEP, ENGINE_PER_TRAJECTORY, MODE_AT, MODE_CS, MODE_STD,
+                   PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64, MqctError, check, lib,
+                   ptr)
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
 __all__ = ["CollisionSystem", "build_matrix", "MatrixPlan", "PropagationTables", "propagate",
@@ -749,6 +750,17 @@ class PropagationPlan:
     def set_coupled_states(self, cs=True):
         """CS_APPROX for the following runs."""
         check(lib().mqct_prop_plan_set_coupled_states(self.h, 1 if cs else 0))
+
+    def set_engine(self, engine=ENGINE_AUTO):
+        """ENGINE_AUTO, ENGINE_PER_TRAJECTORY or ENGINE_LOCKSTEP for the following runs
+        (mqct_prop_plan_set_engine)."""
+        check(lib().mqct_prop_plan_set_engine(self.h, int(engine)))
+
+    def engine(self):
+        """(engine of the last run, lockstep rounds of the last run or 0)."""
+        e, r = C.c_int32(), C.c_int64()
+        check(lib().mqct_prop_plan_engine(self.h, C.byref(e), C.byref(r)))
+        return int(e.value), int(r.value)
 
     def tune(self, trajs, mode=MODE_STD):
         """Time the launch shapes on these trajectories (capped) and keep the faster."""

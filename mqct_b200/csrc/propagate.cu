@@ -42,6 +42,7 @@
 #include <map>
 
 #include "common.cuh"
+#include "propagate.cuh"
 
 using namespace mqct;
 
@@ -53,53 +54,6 @@ constexpr int UNROLL = 4;      // slots per thread in flight in phase A
 // Launch shapes: TPB threads per CTA; TPB == 256 runs two CTAs (two trajectories) per SM
 // so that one trajectory's load latency overlaps the other's work.  The plan picks the
 // faster shape for its tables by timing both (PropPlan::tune).
-
-template <class T> struct V2;
-template <> struct V2<float> { using t = float2; };
-template <> struct V2<double> { using t = double2; };
-
-struct PropDev {
-  int N, nR, n_e, n_pass;
-  int64_t S;                   // slots per knot row (all blocks, padded)
-  const double* R;             // nR
-  const int* pass_row0;        // first internal state of each pass (n_pass + 1)
-  const int64_t* pass_slot0;   // first slot of each pass (n_pass + 1)
-  const int* st_blk;           // block of each internal state
-  const int* blk_n;            // states per block
-  const int* blk_s0;           // first internal state of the block
-  const int* blk_mp;           // offset of the block's triangle inside its pass
-  const int64_t* blk_slot0;    // first slot of each block (n_blocks + 1)
-  const int* blk_pass;         // pass holding each block
-  const uint32_t* loc;         // per slot: internal (row | column << 16)
-  const int* st_e;             // energy class per internal state
-  const double* e_val;         // energy per class, Hartree
-  const int* nb_plus;          // internal index of the reference-order successor, or -1
-  const int* nb_minus;         // internal index of the reference-order predecessor, or -1
-  const double* cplus;         // coefficient of the successor's amplitude
-  const double* cminus;        // coefficient of the predecessor's amplitude
-  const int* perm;             // internal -> reference state index
-  const int* inv_perm;         // reference -> internal state index
-  const void* knots;           // nR x S of (M, y2) in T precision
-  double mass, inv_mass;
-  int mode;                    // MQCT_MODE_STD or MQCT_MODE_AT
-  int cs;                      // coupled-states approximation: no Coriolis terms
-  int mp_cap;                  // packed slots that fit in shared memory
-  double ode_eps, ode_hmin;    // ODEINT accuracy and minimum step (adaptive kernel)
-  // AT paths
-  const int64_t* at_off;
-  const int* at_n;
-  const double* at_rec;        // records of 8
-  const double* at_y2;         // per record kAtCols second derivatives (R, theta, P_theta,
-                               // P_phi, pot, phi)
-  int bk_int;                  // bikram_int: one adaptive call with per-step stop rules
-  int at_adapt;                // AT_ADAPT_STP: RK4 steps from the path's coupling energy
-  double at_tol, at_mintm;     // AT_ADAPTOL and TIME_STEP (the smallest step)
-};
-
-// Classical variables (R, P_R, theta, P_theta, phi, P_phi).
-struct Cls {
-  double R, PR, th, Pth, phi, Pphi;
-};
 
 struct TrajOut {
   double* amp;
@@ -129,8 +83,6 @@ __device__ inline void save_record(const TrajOut& o, int tr, int64_t& n, double 
 constexpr int kClsSlots = 11;
 
 // Shared-memory layout of one CTA (dynamic).
-struct SplineAt;
-
 template <class T>
 struct Smem {
   Cls* c;                      // kClsSlots classical slots (see above)
@@ -189,45 +141,6 @@ __device__ inline void block_sum3(double& a, double& b, double& c, double* red) 
   c = red[3 * W + 2];
 }
 
-// Spline coefficients at R (splint_bk, MQCT_SOURCE_CODES/mqct_eqtns.f:555-611;
-// above R_n the matrix is zero, MQCT_SOURCE_CODES/mqct_eqtns.f:545-549; below
-// R_1 the first interval's cubic, the net effect of :534-551).
-struct SplineAt {
-  int klo;
-  bool zero;
-  double aa, bb, cc1, cc2, cc3, cc4, cc5, cc6, h;
-};
-// *hint: the interval found last (klo); when x is still inside it the bisection, whose
-// result it is, is skipped.
-__device__ inline SplineAt spline_at(const double* R, int nR, double x, int* hint) {
-  SplineAt s;
-  s.zero = x > R[nR - 1];
-  int klo = 1, khi = nR;
-  const int hk = *hint;
-  if (hk >= 1 && hk < nR && R[hk - 1] <= x && x < R[hk]) {
-    klo = hk;
-    khi = hk + 1;
-  }
-  while (khi - klo > 1) {
-    int k = (khi + klo) >> 1;
-    if (R[k - 1] > x) khi = k;
-    else klo = k;
-  }
-  *hint = klo;
-  s.klo = klo - 1;
-  double h = R[khi - 1] - R[klo - 1];
-  const double inv_h = 1.0 / h;
-  s.h = h;
-  s.aa = (R[khi - 1] - x) * inv_h;
-  s.bb = (x - R[klo - 1]) * inv_h;
-  s.cc1 = s.aa * s.aa * s.aa - s.aa;
-  s.cc2 = s.bb * s.bb * s.bb - s.bb;
-  s.cc3 = 3 * s.aa * s.aa - 1.0;
-  s.cc4 = 3 * s.bb * s.bb - 1.0;
-  s.cc5 = (h * h) / 6.0;
-  s.cc6 = s.cc5 * inv_h;
-  return s;
-}
 
 constexpr int kAtCols = 6;  // splined columns of an AT path record
 
@@ -558,10 +471,6 @@ constexpr double kCkB21 = .2, kCkB31 = 3.0 / 40.0, kCkB32 = 9.0 / 40.0, kCkB41 =
 constexpr double kCkA4 = (double)0.6f;
 constexpr int kOdeMaxSteps = 10000;  // MAXSTP of odeint
 
-__device__ inline double kinetic(const Cls& c, double mass) {
-  return c.PR * c.PR / 2.0 / mass + c.Pth * c.Pth / 2.0 / mass / (c.R * c.R) +
-         c.Pphi * c.Pphi / 2.0 / mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
-}
 
 // Classical point of an AT trajectory at time t (thread 0).
 __device__ inline void classical_at(const PropDev& d, int tr, double t, Cls* cc) {
@@ -1121,6 +1030,10 @@ struct PropPlan {
 
   int method = MQCT_INTEG_RK4;
   double ode_eps = 1e-6, ode_hmin = 0.0;
+  // engine choice (MQCT_ENGINE_*), the engine of the last run and the lockstep engine
+  int engine = MQCT_ENGINE_AUTO;
+  int last_engine = 0;
+  LsEngine* ls = nullptr;
   bool cs = false;  // CS_APPROX for every run of the plan
   int bk_int = 0;                       // bikram_int (ODEINT with per-step stop rules)
   int at_adapt = 0;                     // AT_ADAPT_STP (RK4 steps of AT runs)
@@ -1476,6 +1389,7 @@ struct PropPlan {
              double* cls, double* diag, double* rec = nullptr, int64_t rec_cap = 0,
              int64_t* n_rec = nullptr) {
     MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 30), "n_traj out of range");
+    last_engine = MQCT_ENGINE_PER_TRAJECTORY;
     MQCT_CUDA_TRY(cudaMemsetAsync(d_queue.p, 0, sizeof(int), stream));
     PropDev d = dev_view(mode);
     TrajOut o{amp, cls, diag, rec, rec_cap, n_rec};
@@ -1540,7 +1454,28 @@ struct PropPlan {
     return MQCT_OK;
   }
 
+  // The lockstep engine takes standard-mode RK4 runs without CS or SAVE_TRAJECT records
+  // when every m-block has at most 128 states: always with MQCT_ENGINE_LOCKSTEP, from
+  // kLockstepMinBatch trajectories with MQCT_ENGINE_AUTO (smaller batches share few knot
+  // rows, and the per-trajectory kernel then has less work per right-hand side).
+  static constexpr int64_t kLockstepMinBatch = 1024;
+  bool use_lockstep(int mode, int64_t n_traj, bool records) const {
+    if (engine == MQCT_ENGINE_PER_TRAJECTORY || records || mode != MQCT_MODE_STD || cs ||
+        method != MQCT_INTEG_RK4 || !ls_eligible(h_blk_n))
+      return false;
+    return engine == MQCT_ENGINE_LOCKSTEP || n_traj >= kLockstepMinBatch;
+  }
+  int run_lockstep(const mqct_traj_init_t* d_init_p, const mqct_traj_init_t* h_init,
+                   int64_t n_traj, double* amp, double* cls, double* diag) {
+    MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 24), "n_traj out of range for the lockstep engine");
+    if (!ls) ls = ls_create();
+    last_engine = MQCT_ENGINE_LOCKSTEP;
+    return ls_run(ls, dev_view(MQCT_MODE_STD), arith == MQCT_PROP_FP32, h_blk_n, n_sm, stream, ev0,
+                  ev1, d_init_p, h_init, (int)n_traj, amp, cls, diag);
+  }
+
   ~PropPlan() {
+    if (ls) ls_destroy(ls);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1593,7 +1528,8 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
   }
   std::vector<mqct_traj_init_t> sorted(n_traj);
   for (int64_t t = 0; t < n_traj; ++t) sorted[t] = init[order[t]];
-  if (!p->tuned && p->method == MQCT_INTEG_RK4 && n_traj >= 2LL * p->n_sm) {
+  const bool lockstep = p->use_lockstep(mode, n_traj, rec_out != nullptr);
+  if (!lockstep && !p->tuned && p->method == MQCT_INTEG_RK4 && n_traj >= 2LL * p->n_sm) {
     rc = p->tune(sorted.data(), n_traj, mode);
     if (rc) return rc;
   }
@@ -1601,15 +1537,21 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
   MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
   MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
   MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
+  if (lockstep) {
+    rc = p->run_lockstep(p->d_init.p, sorted.data(), n_traj, p->d_amp.p, p->d_cls.p, p->d_diag.p);
+    if (rc) return rc;
+  }
   DevBuf<double> d_rec;
   DevBuf<int64_t> d_nrec;
   if (rec_out) {
     MQCT_CUDA_TRY(d_rec.alloc((size_t)n_traj * rec_cap * 8));
     MQCT_CUDA_TRY(d_nrec.alloc((size_t)n_traj));
   }
-  rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p, d_rec.p,
-                 rec_cap, d_nrec.p);
-  if (rc) return rc;
+  if (!lockstep) {
+    rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p, d_rec.p,
+                   rec_cap, d_nrec.p);
+    if (rc) return rc;
+  }
   const size_t na = (size_t)2 * p->N;
   std::vector<double> amp(reorder ? (size_t)n_traj * na : 0), cls(reorder ? n_traj * 6 : 0),
       diag(reorder ? n_traj * 8 : 0), rec(reorder && rec_out ? (size_t)n_traj * rec_cap * 8 : 0);
@@ -1672,8 +1614,19 @@ int mqct_prop_plan_create(const mqct_tables_t* tab, int32_t arith, mqct_prop_pla
 int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_init,
                               int64_t n_traj, double* d_amp, double* d_cls, double* d_diag) {
   MQCT_ARG_CHECK(plan && d_init && d_amp && d_cls && d_diag, "null argument");
-  return reinterpret_cast<PropPlan*>(plan)->launch(d_init, n_traj, MQCT_MODE_STD, d_amp, d_cls,
-                                                   d_diag);
+  PropPlan* p = reinterpret_cast<PropPlan*>(plan);
+  if (p->use_lockstep(MQCT_MODE_STD, n_traj, false)) {
+    // the lockstep engine bounds its rounds by the trajectories' step caps and time limits
+    MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 24), "n_traj out of range for the lockstep engine");
+    std::vector<mqct_traj_init_t> h((size_t)n_traj);
+    MQCT_CUDA_TRY(cudaMemcpyAsync(h.data(), d_init, sizeof(mqct_traj_init_t) * n_traj,
+                                  cudaMemcpyDeviceToHost, p->stream));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    const int rc = validate_init(h.data(), n_traj, p->N, MQCT_MODE_STD);
+    if (rc) return rc;
+    return p->run_lockstep(d_init, h.data(), n_traj, d_amp, d_cls, d_diag);
+  }
+  return p->launch(d_init, n_traj, MQCT_MODE_STD, d_amp, d_cls, d_diag);
 }
 
 int mqct_prop_plan_run(mqct_prop_plan* plan, const mqct_traj_init_t* init, int64_t n_traj,
@@ -1723,6 +1676,23 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
     probe_ms[0] = p->tuned ? p->tune_ms[0] : 0.f;
     probe_ms[1] = p->tuned ? p->tune_ms[1] : 0.f;
   }
+  return MQCT_OK;
+}
+
+int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MQCT_ARG_CHECK(engine == MQCT_ENGINE_AUTO || engine == MQCT_ENGINE_PER_TRAJECTORY ||
+                     engine == MQCT_ENGINE_LOCKSTEP,
+                 "unknown engine %d", engine);
+  reinterpret_cast<PropPlan*>(plan)->engine = engine;
+  return MQCT_OK;
+}
+
+int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* rounds) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  const PropPlan* p = reinterpret_cast<const PropPlan*>(plan);
+  if (engine) *engine = p->last_engine;
+  if (rounds) *rounds = p->last_engine == MQCT_ENGINE_LOCKSTEP ? ls_rounds(p->ls) : 0;
   return MQCT_OK;
 }
 
