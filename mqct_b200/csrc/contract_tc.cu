@@ -100,6 +100,39 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
           smem_u32(bar))
       : "memory");
 }
+// One accumulation group: Q slices x three split products x four K-steps, in the order
+// small products first ((A_hi, B_lo), (A_lo, B_hi), then (A_hi, B_hi)).  The descriptors are
+// the chunk's base descriptors plus compile-time or per-chunk offsets (a descriptor holds the
+// shared-memory address >> 4 in its low bits), so that the issuing thread does little more
+// than issue: the tensor cores consume a group as fast as one thread issues it.
+template <int Q>
+__device__ __forceinline__ void mma_group(uint32_t td, uint64_t ad0, uint64_t bd0, uint32_t bpl16,
+                                          uint32_t bkk16, uint32_t idesc, int nsl) {
+  constexpr uint32_t akk16 = (uint32_t)(2 * (TC_M / 8) * 128) >> 4;
+  constexpr uint32_t apl16 = (uint32_t)TC_A_PLANE >> 4;
+  uint32_t acc = 0u;
+#pragma unroll
+  for (int pr = 1; pr <= 3; ++pr) {
+    const int prod = pr % 3;
+    const uint32_t ap = (prod == 2) ? 1u : 0u, bp = (prod == 1) ? 1u : 0u;
+    const uint64_t adp = ad0 + ap * apl16, bdp = bd0 + bp * bpl16;
+#pragma unroll
+    for (int sl = 0; sl < (Q > 0 ? Q : 1); ++sl) {
+      if (Q == 0 && sl >= nsl) break;
+#pragma unroll
+      for (int kk = 0; kk < TC_KC / 16; ++kk) {
+        mma_f16(td, adp + kk * akk16, bdp + (uint64_t)(kk * bkk16), idesc, acc);
+        acc = 1u;
+      }
+    }
+    if (Q == 0) {  // a group whose size is not a compile-time case: the remaining slices
+      for (int sl = 1; sl < nsl; ++sl)
+#pragma unroll
+        for (int kk = 0; kk < TC_KC / 16; ++kk)
+          mma_f16(td, adp + kk * akk16, bdp + (uint64_t)(kk * bkk16), idesc, 1u);
+    }
+  }
+}
 // 8 consecutive TMEM columns of this warp's lane quarter (one 32-bit value per lane each);
 // the values are valid after tmem_wait().
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
@@ -390,6 +423,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           tc_fence_after();
           const uint32_t aoff = sA0 + sa * (2 * TC_A_PLANE);
           const uint32_t boff0 = sB0 + sb * a.b_stage;
+          const uint64_t ad0 = smem_desc(aoff, lbo_a, 128), bd0 = smem_desc(boff0, lbo_b, 128);
+          const uint32_t bpl16 = bplane >> 4, bkk16 = (2 * lbo_b) >> 4;
           for (int al = 0; al < a.n_alpha_it; ++al, ++kacc) {
             const uint32_t sc = kacc & 1u;
             if (kacc >= 2) {  // the epilogue must have drained this accumulator
@@ -400,23 +435,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
               tc_fence_after();
             }
             const uint32_t td = tmem + sc * TC_NC_MAX;
-            // The small products first: (A_hi, B_lo) and (A_lo, B_hi) of every slice of the
-            // group, then (A_hi, B_hi), so that the small terms are added while the
-            // accumulator is still small (the MMA rounds relative to its largest addend).
             const int ns_grp = min(a.slices_per_drain, a.n_alpha_it - al);
-            bool first = true;
-            for (int pr = 1; pr <= 3; ++pr) {
-              const int prod = pr % 3;  // 1, 2, then 0
-              const uint32_t ap = (prod == 2) ? 1 : 0, bp = (prod == 1) ? 1 : 0;
-              for (int sl = 0; sl < ns_grp; ++sl) {
-#pragma unroll
-                for (int kk = 0; kk < TC_KC / 16; ++kk) {
-                  const uint64_t ad = smem_desc(aoff + ap * TC_A_PLANE + kk * 2 * lbo_a, lbo_a, 128);
-                  const uint64_t bd = smem_desc(boff0 + bp * bplane + kk * 2 * lbo_b, lbo_b, 128);
-                  mma_f16(td, ad, bd, idesc, first ? 0u : 1u);
-                  first = false;
-                }
-              }
+            switch (ns_grp) {
+              case 1: mma_group<1>(td, ad0, bd0, bpl16, bkk16, idesc, 1); break;
+              case 2: mma_group<2>(td, ad0, bd0, bpl16, bkk16, idesc, 2); break;
+              case 4: mma_group<4>(td, ad0, bd0, bpl16, bkk16, idesc, 4); break;
+              case 8: mma_group<8>(td, ad0, bd0, bpl16, bkk16, idesc, 8); break;
+              default: mma_group<0>(td, ad0, bd0, bpl16, bkk16, idesc, ns_grp); break;
             }
             mma_commit(&ACC_full[sc]);  // the epilogue may read once these MMAs complete
             al += ns_grp - 1;
