@@ -461,7 +461,7 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
  * interpolating slot by slot: the same arithmetic type, other rounding.  Its device-buffer
  * runs (mqct_prop_plan_run_device) read the initial conditions back for the bound on the
  * rounds and return when the batch is done.  MQCT_ENGINE_AUTO (default): the lockstep
- * engine for eligible batches of at least 1024 trajectories.  mqct_prop_plan_engine
+ * engine for eligible batches of at least 4096 trajectories.  mqct_prop_plan_engine
  * reports the engine of the last run and, for the lockstep engine, the rounds it ran
  * (rounds may be NULL). */
 #define MQCT_ENGINE_AUTO 0

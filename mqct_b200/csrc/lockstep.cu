@@ -101,7 +101,9 @@ struct LsDev {
   int* kcnt;                       // per key: trajectories of this round
   int* gstart;                     // per key: its first group of this round
   int* gkey;                       // per group of this round: its key
-  int* bucket;                     // per key: its trajectories (n_traj places each)
+  int* bucket[2];                  // per key: its trajectories (n_traj places each), for the
+                                   // rounds of even and odd parity
+  int* tdone;                      // per trajectory: its block items finished this round
   int* n_groups;                   // groups of up to G trajectories of this round
   int* n_items;                    // groups x blocks
   int* queue;                      // ls_rhs work queue
@@ -112,6 +114,15 @@ struct LsDev {
   double* cls;
   double* diag;
 };
+
+template <class T>
+__device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane, bool init, int rpar);
+template <int G, int NT>
+__device__ void ls_group(const PropDev& d, const LsDev& L);
+
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 // ---------------------------------------------------------------- ls_rhs
 template <class T>
@@ -128,6 +139,7 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
   __shared__ T s_cf[G][7];
   __shared__ double s_dt[G], s_dphi[G];
   __shared__ double s_red[LS_MAX_UNITS][TB][3];
+  __shared__ int s_fin[G];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N = d.N;
   const T2* __restrict__ AIN = reinterpret_cast<const T2*>(L.AIN[par]);
@@ -139,37 +151,45 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
   T2* bt = reinterpret_cast<T2*>(ls_smem + ((sizeof(E) * (size_t)L.tri_cap + 15) & ~size_t(15)));
   for (;;) {
     __syncthreads();  // the previous item's shared data is no longer read
-    if (tid == 0) {
+    if (warp == 0) {
       // item = (block of the blk_order rank, group of up to G trajectories of one key);
-      // the groups of the largest block come first
-      const int it = atomicAdd(L.queue, 1);
+      // the groups of the largest block come first.  Warp 0 fetches it and the group's
+      // parameters (lane t: trajectory t).
+      int it = 0;
+      if (lane == 0) it = atomicAdd(L.queue, 1);
+      it = __shfl_sync(0xffffffffu, it, 0);
       const int n_it = *L.n_items;
-      s_item[0] = it < n_it ? 1 : 0;
+      int key = 0, b = 0, g = 0, off = 0;
       if (it < n_it) {
         const int tg = *L.n_groups;
         const int bo = it / tg, gi = it - bo * tg;
-        const int key = L.gkey[gi];
-        const int off = (gi - L.gstart[key]) * G;
+        key = L.gkey[gi];
+        off = (gi - L.gstart[key]) * G;
+        b = L.blk_order[bo];
+        g = min(G, L.kcnt[key] - off);
+        if (lane < g) {
+          const int tr = L.bucket[par][(size_t)key * L.n_traj + off + lane];
+          const LsTraj& S = L.tr[tr];
+          s_tr[lane] = tr;
+          s_stage[lane] = S.stage;
+          s_dt[lane] = S.dt;
+          s_dphi[lane] = S.dphidt;
+#pragma unroll
+          for (int q = 0; q < 7; ++q) s_cf[lane][q] = (T)S.sp[q];
+        }
+      }
+      if (lane == 0) {
+        s_item[0] = it < n_it ? 1 : 0;
         s_item[1] = key;
-        s_item[2] = L.blk_order[bo];
-        s_item[3] = min(G, L.kcnt[key] - off) | (off << 6);
+        s_item[2] = b;
+        s_item[3] = g | (off << 6);
       }
     }
     __syncthreads();
     if (!s_item[0]) break;
-    const int key = s_item[1], b = s_item[2], g = s_item[3] & 63, off = s_item[3] >> 6;
+    const int key = s_item[1], b = s_item[2], g = s_item[3] & 63;
     const int nb = __ldg(d.blk_n + b), r0 = __ldg(d.blk_s0 + b);
     const bool zero = key == d.nR - 1;  // above the grid: the matrix is zero
-    if (tid < g) {
-      const int tr = L.bucket[(size_t)key * L.n_traj + off + tid];
-      const LsTraj& S = L.tr[tr];
-      s_tr[tid] = tr;
-      s_stage[tid] = S.stage;
-      s_dt[tid] = S.dt;
-      s_dphi[tid] = S.dphidt;
-#pragma unroll
-      for (int q = 0; q < 7; ++q) s_cf[tid][q] = (T)S.sp[q];
-    }
     // the block's triangle at knot rows key and key + 1: (lo, hi - lo, lo'', hi'')
     if (!zero) {
       const int64_t q0 = __ldg(d.blk_slot0 + b);
@@ -188,7 +208,6 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
         K4[q] = e;
       }
     }
-    __syncthreads();  // trajectory parameters ready
     // bt = D^* a of the block's states: row j holds the G trajectories (unused ones zero)
     for (int idx = tid; idx < G * nb; idx += Cfg::THREADS) {
       const int j = idx / G, t = idx - j * G;
@@ -215,6 +234,23 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
       for (int tt = 0; tt < TB; ++tt)
 #pragma unroll
         for (int q = 0; q < 4; ++q) zr[tt][q] = zi[tt][q] = (T)0;
+      // the row updates' operands into L1 while the products run
+      if (i < nb) {
+        const int gi = r0 + i;
+#pragma unroll
+        for (int tt = 0; tt < TB; ++tt) {
+          const int t = set * TB + tt;
+          if (t < g) {
+            const size_t base = (size_t)s_tr[t] * N;
+            prefetch_l1(L.Y + base + gi);
+            prefetch_l1(ACC + base + gi);
+            prefetch_l1(PH + (size_t)s_tr[t] * d.n_e + __ldg(d.st_e + gi));
+            const int np_ = __ldg(d.nb_plus + gi), nm = __ldg(d.nb_minus + gi);
+            if (np_ >= 0) prefetch_l1(AIN + base + np_);
+            if (nm >= 0) prefetch_l1(AIN + base + nm);
+          }
+        }
+      }
       if (!zero) {
         const int Ti = ic * (ic + 1) / 2;
         int Tj = 0;
@@ -352,7 +388,28 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
       pp[0] = a0;
       pp[1] = a1;
       pp[2] = a2;
+      // the item that completes a trajectory's blocks takes its classical step
+      __threadfence();
+      s_fin[tid] = atomicAdd(L.tdone + s_tr[tid], 1) == L.n_blocks - 1;
     }
+    __syncthreads();
+    for (int t = warp; t < g; t += NW) {
+      if (s_fin[t]) {
+        __threadfence();
+        if (lane == 0) L.tdone[s_tr[t]] = 0;
+        ls_traj_step<T>(d, L, s_tr[t], lane, false, par ^ 1);
+      }
+    }
+  }
+  // the last CTA of the round forms the next round's groups
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(L.done, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    ls_group<G, Cfg::THREADS>(d, L);
   }
 }
 
@@ -360,7 +417,7 @@ ls_rhs_kernel(PropDev d, LsDev L, int par) {
 // Classical part of a trajectory between two rounds (lane 0 of its warp) and the set-up
 // of its next stage point; init: the trajectory's start instead.
 template <class T>
-__device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane, bool init) {
+__device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane, bool init, int rpar) {
   using T2 = typename V2<T>::t;
   LsTraj& S = L.tr[tr];
   int act = 0;
@@ -402,9 +459,9 @@ __device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane,
       double F = 0.0, g = 0.0, pot = 0.0;
       const double* pp = L.part + (size_t)tr * L.n_blocks * 3;
       for (int b = 0; b < L.n_blocks; ++b) {
-        F += pp[3 * b];
-        g += pp[3 * b + 1];
-        pot += pp[3 * b + 2];
+        F += __ldcg(pp + 3 * b);
+        g += __ldcg(pp + 3 * b + 1);
+        pot += __ldcg(pp + 3 * b + 2);
       }
       act = 1;
       if (s == 4) {  // closing evaluation done: F = quantum energy, g = norm
@@ -523,7 +580,7 @@ __device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane,
       S.sp[6] = sp.cc4 * sp.cc6;
       const int key = sp.zero ? d.nR - 1 : sp.klo;
       S.key = key;
-      L.bucket[(size_t)key * L.n_traj + atomicAdd(L.cnt + key, 1)] = tr;
+      L.bucket[rpar][(size_t)key * L.n_traj + atomicAdd(L.cnt + key, 1)] = tr;
     }
   }
   act = __shfl_sync(0xffffffffu, act, 0);
@@ -545,12 +602,12 @@ __device__ void ls_traj_step(const PropDev& d, const LsDev& L, int tr, int lane,
 
 // The last CTA of a round: the next round's groups of up to G trajectories per key (their
 // trajectories are in the key's bucket), registration counters reset.
-template <int G>
+template <int G, int NT>
 __device__ void ls_group(const PropDev& d, const LsDev& L) {
-  __shared__ int s_sum[LS_CLS_THREADS], s_gsum[LS_CLS_THREADS];
+  __shared__ int s_sum[NT], s_gsum[NT];
   const int tid = threadIdx.x;
   const int nk = d.nR;
-  const int per = (nk + LS_CLS_THREADS - 1) / LS_CLS_THREADS;
+  const int per = (nk + NT - 1) / NT;
   const int k0 = min(nk, tid * per), k1 = min(nk, k0 + per);
   int sc = 0, sg = 0;
   for (int k = k0; k < k1; ++k) {
@@ -562,14 +619,14 @@ __device__ void ls_group(const PropDev& d, const LsDev& L) {
   s_gsum[tid] = sg;
   __syncthreads();
   // inclusive scans over the threads' chunks of keys (Hillis-Steele)
-  for (int o = 1; o < LS_CLS_THREADS; o <<= 1) {
+  for (int o = 1; o < NT; o <<= 1) {
     const int a = tid >= o ? s_sum[tid - o] : 0, ag = tid >= o ? s_gsum[tid - o] : 0;
     __syncthreads();
     s_sum[tid] += a;
     s_gsum[tid] += ag;
     __syncthreads();
   }
-  const int total = s_sum[LS_CLS_THREADS - 1], tgroups = s_gsum[LS_CLS_THREADS - 1];
+  const int total = s_sum[NT - 1], tgroups = s_gsum[NT - 1];
   int grun = tid > 0 ? s_gsum[tid - 1] : 0;
   for (int k = k0; k < k1; ++k) {
     const int c = __ldcg(L.cnt + k);
@@ -589,11 +646,13 @@ __device__ void ls_group(const PropDev& d, const LsDev& L) {
   }
 }
 
+// The start of a run: every trajectory's initial state and first stage point, registered
+// for round 0; the last CTA forms round 0's groups.
 template <class T>
-__global__ void __launch_bounds__(LS_CLS_THREADS) ls_cls_kernel(PropDev d, LsDev L, int init) {
+__global__ void __launch_bounds__(LS_CLS_THREADS) ls_init_kernel(PropDev d, LsDev L) {
   const int lane = threadIdx.x & 31;
   const int tr = blockIdx.x * (LS_CLS_THREADS / 32) + (threadIdx.x >> 5);
-  if (tr < L.n_traj && (init || L.tr[tr].active)) ls_traj_step<T>(d, L, tr, lane, init != 0);
+  if (tr < L.n_traj) ls_traj_step<T>(d, L, tr, lane, true, 0);
   __shared__ int s_last;
   __threadfence();
   __syncthreads();
@@ -601,7 +660,7 @@ __global__ void __launch_bounds__(LS_CLS_THREADS) ls_cls_kernel(PropDev d, LsDev
   __syncthreads();
   if (s_last) {
     __threadfence();
-    ls_group<LsCfg<T>::G>(d, L);
+    ls_group<LsCfg<T>::G, LS_CLS_THREADS>(d, L);
   }
 }
 
@@ -635,7 +694,7 @@ struct LsEngine {
   DevBuf<double2> Y;
   DevBuf<double2> acc, ain0, ain1, ph;  // T2 arrays, sized in double2 units
   DevBuf<double> part;
-  DevBuf<int> cnt, kcnt, gstart, gkey, bucket, ctr, blk_order;  // ctr: n_items, queue, done,
+  DevBuf<int> cnt, kcnt, gstart, gkey, bucket, tdone, ctr, blk_order;  // ctr: n_items, queue, done,
                                                                  // n_active, n_groups
   int cap_traj = -1, cap_arith = -1;
   int* h_active = nullptr;  // pinned, two slots
@@ -693,7 +752,8 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     MQCT_CUDA_TRY(e->ph.alloc((size_t)n_traj * d.n_e * sizeof(T2) / sizeof(double2) + 1));
     MQCT_CUDA_TRY(e->part.alloc((size_t)n_traj * nb * 3));
     MQCT_CUDA_TRY(e->gkey.alloc(max_groups));
-    MQCT_CUDA_TRY(e->bucket.alloc((size_t)nk * n_traj));
+    MQCT_CUDA_TRY(e->bucket.alloc((size_t)2 * nk * n_traj));
+    MQCT_CUDA_TRY(e->tdone.alloc(n_traj));
     e->cap_traj = n_traj;
     e->cap_arith = arith;
   }
@@ -701,7 +761,8 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     MQCT_CUDA_TRY(e->cnt.alloc(nk));
     MQCT_CUDA_TRY(e->kcnt.alloc(nk));
     MQCT_CUDA_TRY(e->gstart.alloc(nk));
-    if (e->bucket.n != (size_t)nk * e->cap_traj) MQCT_CUDA_TRY(e->bucket.alloc((size_t)nk * e->cap_traj));
+    if (e->bucket.n != (size_t)2 * nk * e->cap_traj)
+      MQCT_CUDA_TRY(e->bucket.alloc((size_t)2 * nk * e->cap_traj));
   }
   if (!e->ctr.p) MQCT_CUDA_TRY(e->ctr.alloc(5));
   {
@@ -732,7 +793,9 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
   L.kcnt = e->kcnt.p;
   L.gstart = e->gstart.p;
   L.gkey = e->gkey.p;
-  L.bucket = e->bucket.p;
+  L.bucket[0] = e->bucket.p;
+  L.bucket[1] = e->bucket.p + (size_t)nk * n_traj;
+  L.tdone = e->tdone.p;
   L.n_groups = e->ctr.p + 4;
   L.n_items = e->ctr.p;
   L.queue = e->ctr.p + 1;
@@ -762,6 +825,7 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
   const int grid_rhs = n_sm * per_sm;
   const int grid_cls = (n_traj + LS_CLS_THREADS / 32 - 1) / (LS_CLS_THREADS / 32);
   MQCT_CUDA_TRY(cudaMemsetAsync(e->cnt.p, 0, sizeof(int) * nk, st));
+  MQCT_CUDA_TRY(cudaMemsetAsync(e->tdone.p, 0, sizeof(int) * n_traj, st));
   MQCT_CUDA_TRY(cudaMemsetAsync(e->ctr.p, 0, sizeof(int) * 5, st));
   // the graph of kLsRoundsPerGraph rounds (rebuilt when the buffers or the type change)
   const bool same = e->graph && e->graph_arith == arith &&
@@ -776,7 +840,6 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     MQCT_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int r = 0; r < kLsRoundsPerGraph; ++r) {
       ls_rhs_kernel<T><<<grid_rhs, Cfg::THREADS, smem, st>>>(d, L, r & 1);
-      ls_cls_kernel<T><<<grid_cls, LS_CLS_THREADS, 0, st>>>(d, L, 0);
     }
     cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (ce != cudaSuccess) {
@@ -797,7 +860,7 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     ls_start_kernel<T><<<blocks, 256, 0, st>>>(d, L);
     MQCT_CUDA_TRY(cudaGetLastError());
   }
-  ls_cls_kernel<T><<<grid_cls, LS_CLS_THREADS, 0, st>>>(d, L, 1);
+  ls_init_kernel<T><<<grid_cls, LS_CLS_THREADS, 0, st>>>(d, L);
   MQCT_CUDA_TRY(cudaGetLastError());
   // graph launches until no trajectory runs; the count of one launch is read while the
   // next one runs (a launch after the last trajectory finished finds no work items)
