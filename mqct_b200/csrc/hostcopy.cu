@@ -6,7 +6,8 @@
 // chunks from the device into its slot, waits for that copy and copies the slot into the
 // destination on the CPU, so the device copies of one thread overlap the host copies and
 // page faults of the others.  The slots are pinned once per process; concurrent calls take
-// turns on them.  A copy below two chunks goes through one cudaMemcpyAsync on the caller's
+// turns on them.  A copy below two chunks, or into a destination that is itself pinned
+// (cudaHostAlloc'd or registered), goes through one cudaMemcpyAsync on the caller's
 // stream, which is then synchronised: either way the copy is complete on return.
 #include <cuda_runtime.h>
 
@@ -43,6 +44,16 @@ bool slots_ready() {  // with g_mu held
 
 int copy_d2h_host(void* dst, const void* src, size_t bytes, cudaStream_t after) {
   if (bytes == 0) return MQCT_OK;
+  {
+    // a pinned (page-locked or registered) destination takes the copy engine directly
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost) {
+      MQCT_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, after));
+      MQCT_CUDA_TRY(cudaStreamSynchronize(after));
+      return MQCT_OK;
+    }
+    cudaGetLastError();  // an unregistered pointer may leave an error code on older drivers
+  }
   std::unique_lock<std::mutex> lk(g_mu);
   if (bytes < 2 * kChunk || !slots_ready()) {  // one copy on `after`, complete on return
     lk.unlock();
