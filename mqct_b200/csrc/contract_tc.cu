@@ -28,17 +28,17 @@
 // most 128 radial points) x one range of K-chunks.  Column parts keep two FP32
 // accumulators of a part in TMEM (double buffering: the tensor cores fill one
 // while the epilogue drains the other) and the FP64 sums of a part in registers.
-// Warp roles (320 threads):
+// Warp roles (576 threads):
 //   warp 0      bulk-copy (TMA) producer: per K-chunk the pre-arranged W image of
 //               the part (hi and lo planes, K-major core-matrix layout) and the
 //               block's rotor-basis slice, one cp.async.bulk each, mbarrier
 //               complete_tx, double-buffered where shared memory allows;
 //   warp 1      TMEM allocator + single-thread MMA issuer;
-//   warps 2..9  X producers and epilogue: per K-chunk X = Re(psi_a^* psi_b) in FP32
+//   warps 2..17 X producers and epilogue: per K-chunk X = Re(psi_a^* psi_b) in FP32
 //               from the staged basis, split to 16-bit hi/lo parts in the
-//               core-matrix layout (two threads per tile row); then, for every
+//               core-matrix layout (four threads per tile row); then, for every
 //               alpha point of the chunk, tcgen05.ld of the accumulator and the FP64
-//               update of the sums (two warps per TMEM lane quarter, each half of the
+//               update of the sums (four warps per TMEM lane quarter, each a quarter of the
 //               part's columns); at the end of a unit the FP64 sums go to global
 //               memory, one array per K range.
 // The operand tiles use the K-major SWIZZLE_NONE canonical layout: 8 rows x
@@ -59,14 +59,16 @@ namespace mqct {
 constexpr int TC_M = 128;        // rows per tile
 constexpr int TC_KC = 64;        // K elements per chunk (8 core-matrix columns of 8 x 16 bit)
 constexpr int TC_PSI_LD = 66;    // float2 per staged basis row (64 + pad)
-constexpr int TC_THREADS = 320;
+constexpr int TC_THREADS = 576;
 constexpr int TC_PRODUCERS = TC_THREADS - 64;  // X-producer / epilogue threads
 constexpr int TC_A_PLANE = TC_M * TC_KC * 2;    // bytes of one 16-bit plane of an A stage
 constexpr int TC_NC_MAX = 112;                  // columns of one part (TMEM buffer width)
-constexpr int TC_NCH_MAX = TC_NC_MAX / 2;       // columns drained by one epilogue thread
+constexpr int TC_KSPLIT = TC_PRODUCERS / TC_M;   // threads per tile row in X production
+constexpr int TC_NCH_MAX = 32;                  // columns drained by one epilogue thread
 constexpr int TC_TMEM_COLS = 256;               // allocation (a power of two >= 2 buffers)
 static_assert(2 * TC_NC_MAX <= TC_TMEM_COLS, "two accumulator buffers must fit the allocation");
 constexpr int TC_MAX_PARTS = 8;
+constexpr int TC_SMEM_ALPHA = 64;                // alpha weights kept in shared memory
 constexpr uint32_t TC_SPIN_LIMIT = kSpinLimit;  // bounded mbarrier waits
 
 // Shared-memory matrix descriptor: K-major, SWIZZLE_NONE, version 1.
@@ -321,6 +323,8 @@ __device__ __forceinline__ uint32_t empty_parity(uint32_t k, uint32_t nb) {
 
 template <bool kF16>
 __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
+  static_assert(TC_PRODUCERS % TC_M == 0 && (TC_KC / 8) % TC_KSPLIT == 0, "X production split");
+  static_assert((TC_NC_MAX / 8 + 3) / 4 <= TC_NCH_MAX / 8, "drain split");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   unsigned char* sB = reinterpret_cast<unsigned char*>(base);           // nbuf x b_stage
@@ -340,6 +344,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 18);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(bars + 19);
 
+  // the alpha weights in shared memory: the epilogue reads one per drain, and a global
+  // load there would sit on the drain's critical path
+  __shared__ double s_walpha[TC_SMEM_ALPHA];
+  for (int i = threadIdx.x; i < TC_SMEM_ALPHA; i += TC_THREADS)
+    s_walpha[i] = (a.walpha && i < a.n_alpha_it) ? a.walpha[i] : 1.0;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < 2; ++s) {
@@ -455,12 +464,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       for (uint32_t it = 0; it < TC_SPIN_LIMIT && !mbar_try_wait(DONE, 0); ++it) {}
     }
   } else {
-    // ---------------- X producers (warps 2..9) and epilogue
+    // ---------------- X producers (warps 2..17) and epilogue
     const int t = threadIdx.x - 64;
     const int p = t & (TC_M - 1);  // tile row generated by this thread
-    const int kh = t / TC_M;       // half of the chunk's K groups
+    const int kh = t / TC_M;       // quarter of the chunk's K groups
     const int q = warp & 3;        // TMEM lane quarter accessible to this warp
-    const int h = (warp - 2) >> 2; // half of the part's columns drained by this warp
+    const int h = (warp - 2) >> 2; // quarter of the part's columns drained by this warp
     uint32_t kc = 0, ka = 0, kacc = 0;
     double S[TC_NCH_MAX];
     for (int u = blockIdx.x; u < a.n_units && !*abort_flag; u += gridDim.x) {
@@ -468,7 +477,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       const int blk = a.tile_block[tile];
       const int row = tile * TC_M + p;
       const int la = a.rowa[row] - a.blk_row0[blk], lb = a.rowb[row] - a.blk_row0[blk];
-      const int nch = a.parts.nc[pt] / 2, col0 = a.parts.c0[pt] + h * nch;
+      // the part's batches of 8 columns split over the four warps of a lane quarter (the
+      // drain is latency-bound: sixteen epilogue warps keep more of it in flight)
+      const int nb8 = a.parts.nc[pt] / 8;
+      const int b8lo = h * nb8 / 4, b8hi = (h + 1) * nb8 / 4;
+      const int nch = 8 * (b8hi - b8lo), coff = 8 * b8lo, col0 = a.parts.c0[pt] + coff;
       const int c0 = ks * a.chunks_per_ks, c1 = min(a.n_chunks, c0 + a.chunks_per_ks);
 #pragma unroll
       for (int i = 0; i < TC_NCH_MAX; ++i) S[i] = 0.0;
@@ -485,8 +498,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
         unsigned char* hi = sA + sa * (2 * TC_A_PLANE);
         unsigned char* lo = hi + TC_A_PLANE;
 #pragma unroll
-        for (int kq = 0; kq < TC_KC / 16; ++kq) {
-          const int kg = kh * (TC_KC / 16) + kq;
+        for (int kq = 0; kq < TC_KC / 8 / TC_KSPLIT; ++kq) {
+          const int kg = kh * (TC_KC / 8 / TC_KSPLIT) + kq;
           float x[8];
 #pragma unroll
           for (int e = 0; e < 8; e += 2) {
@@ -528,8 +541,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
           }
           tc_fence_after();
           // a group of several alpha points shares one (uniform) weight
-          const double wa = a.walpha ? a.walpha[al] : 1.0;
-          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + sc * TC_NC_MAX + (uint32_t)(h * nch);
+          const double wa = al < TC_SMEM_ALPHA ? s_walpha[al] : (a.walpha ? a.walpha[al] : 1.0);
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + sc * TC_NC_MAX + (uint32_t)coff;
           // batches of 8 columns, software-pipelined: the next batch's TMEM load is in
           // flight while this batch is added to the FP64 sums
           constexpr int NB8 = TC_NCH_MAX / 8;
@@ -614,6 +627,12 @@ int MatrixPlan::tc_init() {
   t.psi_stage = (uint32_t)up((size_t)t.nbmax * TC_PSI_LD * 8);
   int dev_smem = 0;
   cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  {
+    // the kernel's static shared memory (the alpha weights) comes out of the same budget
+    cudaFuncAttributes fa{};
+    MQCT_CUDA_TRY(cudaFuncGetAttributes(&fa, tc_contract_kernel<true>));
+    dev_smem -= (int)fa.sharedSizeBytes;
+  }
   for (t.nbuf = 2; t.nbuf >= 1; --t.nbuf) {
     t.smem = 1024 + (size_t)t.nbuf * (t.b_stage + t.psi_stage) + 2ull * 2 * TC_A_PLANE + 256;
     if (t.smem <= (size_t)dev_smem) break;
