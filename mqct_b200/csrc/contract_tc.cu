@@ -59,12 +59,18 @@ namespace mqct {
 constexpr int TC_M = 128;        // rows per tile
 constexpr int TC_KC = 64;        // K elements per chunk (8 core-matrix columns of 8 x 16 bit)
 constexpr int TC_PSI_LD = 66;    // float2 per staged basis row (64 + pad)
-constexpr int TC_THREADS = 576;
-constexpr int TC_PRODUCERS = TC_THREADS - 64;  // X-producer / epilogue threads
+// Epilogue warps: a template parameter of the kernel, 8 (two per TMEM lane quarter) or 16
+// (four per lane quarter, for builds with several accumulation groups per K-chunk, where
+// the drain is latency-bound and more warps keep more of it in flight).
+template <int PE>
+struct TcShape {
+  static constexpr int THREADS = 64 + 32 * PE;
+  static constexpr int PRODUCERS = 32 * PE;         // X-producer / epilogue threads
+  static constexpr int WPQ = PE / 4;                // epilogue warps per TMEM lane quarter
+  static constexpr int NCH_MAX = PE == 8 ? 56 : 32;  // columns drained by one epilogue thread
+};
 constexpr int TC_A_PLANE = TC_M * TC_KC * 2;    // bytes of one 16-bit plane of an A stage
 constexpr int TC_NC_MAX = 112;                  // columns of one part (TMEM buffer width)
-constexpr int TC_KSPLIT = TC_PRODUCERS / TC_M;   // threads per tile row in X production
-constexpr int TC_NCH_MAX = 32;                  // columns drained by one epilogue thread
 constexpr int TC_TMEM_COLS = 256;               // allocation (a power of two >= 2 buffers)
 static_assert(2 * TC_NC_MAX <= TC_TMEM_COLS, "two accumulator buffers must fit the allocation");
 constexpr int TC_MAX_PARTS = 8;
@@ -321,10 +327,13 @@ __device__ __forceinline__ uint32_t empty_parity(uint32_t k, uint32_t nb) {
   return ((k / nb) + 1u) & 1u;
 }
 
-template <bool kF16>
-__global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
+template <bool kF16, int PE>
+__global__ void __launch_bounds__(TcShape<PE>::THREADS, 1) tc_contract_kernel(TcArgs a) {
+  constexpr int TC_THREADS = TcShape<PE>::THREADS, TC_PRODUCERS = TcShape<PE>::PRODUCERS;
+  constexpr int TC_KSPLIT = TC_PRODUCERS / TC_M;  // threads per tile row in X production
+  constexpr int TC_WPQ = TcShape<PE>::WPQ, TC_NCH_MAX = TcShape<PE>::NCH_MAX;
   static_assert(TC_PRODUCERS % TC_M == 0 && (TC_KC / 8) % TC_KSPLIT == 0, "X production split");
-  static_assert((TC_NC_MAX / 8 + 3) / 4 <= TC_NCH_MAX / 8, "drain split");
+  static_assert((TC_NC_MAX / 8 + TC_WPQ - 1) / TC_WPQ <= TC_NCH_MAX / 8, "drain split");
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uintptr_t base = (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023);
   unsigned char* sB = reinterpret_cast<unsigned char*>(base);           // nbuf x b_stage
@@ -467,9 +476,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
     // ---------------- X producers (warps 2..17) and epilogue
     const int t = threadIdx.x - 64;
     const int p = t & (TC_M - 1);  // tile row generated by this thread
-    const int kh = t / TC_M;       // quarter of the chunk's K groups
+    const int kh = t / TC_M;       // share of the chunk's K groups formed by this thread
     const int q = warp & 3;        // TMEM lane quarter accessible to this warp
-    const int h = (warp - 2) >> 2; // quarter of the part's columns drained by this warp
+    const int h = (warp - 2) >> 2; // share of the part's columns drained by this warp
     uint32_t kc = 0, ka = 0, kacc = 0;
     double S[TC_NCH_MAX];
     for (int u = blockIdx.x; u < a.n_units && !*abort_flag; u += gridDim.x) {
@@ -477,10 +486,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) tc_contract_kernel(TcArgs a) {
       const int blk = a.tile_block[tile];
       const int row = tile * TC_M + p;
       const int la = a.rowa[row] - a.blk_row0[blk], lb = a.rowb[row] - a.blk_row0[blk];
-      // the part's batches of 8 columns split over the four warps of a lane quarter (the
-      // drain is latency-bound: sixteen epilogue warps keep more of it in flight)
+      // the part's batches of 8 columns split over the warps of a lane quarter
       const int nb8 = a.parts.nc[pt] / 8;
-      const int b8lo = h * nb8 / 4, b8hi = (h + 1) * nb8 / 4;
+      const int b8lo = h * nb8 / TC_WPQ, b8hi = (h + 1) * nb8 / TC_WPQ;
       const int nch = 8 * (b8hi - b8lo), coff = 8 * b8lo, col0 = a.parts.c0[pt] + coff;
       const int c0 = ks * a.chunks_per_ks, c1 = min(a.n_chunks, c0 + a.chunks_per_ks);
 #pragma unroll
@@ -630,7 +638,7 @@ int MatrixPlan::tc_init() {
   {
     // the kernel's static shared memory (the alpha weights) comes out of the same budget
     cudaFuncAttributes fa{};
-    MQCT_CUDA_TRY(cudaFuncGetAttributes(&fa, tc_contract_kernel<true>));
+    MQCT_CUDA_TRY(cudaFuncGetAttributes(&fa, tc_contract_kernel<true, 16>));
     dev_smem -= (int)fa.sharedSizeBytes;
   }
   for (t.nbuf = 2; t.nbuf >= 1; --t.nbuf) {
@@ -678,12 +686,16 @@ int MatrixPlan::tc_init() {
   if (precision == MQCT_PREC_F16X3) {
     MQCT_CUDA_TRY(t.wexp.alloc((size_t)nR));
     MQCT_CUDA_TRY(cudaMemsetAsync(d_col_scale.p, 0, sizeof(double) * t.npad, stream));
-    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<true>,
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<true, 8>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<true, 16>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   } else {
     std::vector<double> ones(t.npad, 1.0);
     MQCT_CUDA_TRY(d_col_scale.upload(ones, stream));
-    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<false>,
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<false, 8>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
+    MQCT_CUDA_TRY(cudaFuncSetAttribute(tc_contract_kernel<false, 16>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.smem));
   }
   return MQCT_OK;
@@ -744,8 +756,18 @@ int MatrixPlan::tc_execute() {
   a.ldp = tc_ldp;
   a.status = d_status.p;
   int grid = std::min(a.n_units, t.n_sm);
-  if (f16) tc_contract_kernel<true><<<grid, TC_THREADS, t.smem, stream>>>(a);
-  else tc_contract_kernel<false><<<grid, TC_THREADS, t.smem, stream>>>(a);
+  // sixteen epilogue warps when a K-chunk has several accumulation groups (the drains then
+  // dominate: the as-written alpha grid), eight when it has one (the drain of a chunk then
+  // alternates with its X production, and eight warps with more registers are faster)
+  const bool many = (a.n_alpha_it + a.slices_per_drain - 1) / a.slices_per_drain >= 2;
+  t.pe_warps = many ? 16 : 8;
+  if (f16) {
+    if (many) tc_contract_kernel<true, 16><<<grid, TcShape<16>::THREADS, t.smem, stream>>>(a);
+    else tc_contract_kernel<true, 8><<<grid, TcShape<8>::THREADS, t.smem, stream>>>(a);
+  } else {
+    if (many) tc_contract_kernel<false, 16><<<grid, TcShape<16>::THREADS, t.smem, stream>>>(a);
+    else tc_contract_kernel<false, 8><<<grid, TcShape<8>::THREADS, t.smem, stream>>>(a);
+  }
   MQCT_CUDA_TRY(cudaGetLastError());
   return MQCT_OK;
 }

@@ -19,6 +19,7 @@ struct TcInfo {
   int nbuf = 2;                                        // B / basis-slice buffers
   int slices_per_drain = 1;                            // alpha points per FP64 drain
   bool alpha_uniform = true;                           // all alpha weights equal
+  int pe_warps = 8;                                    // epilogue warps of the last launch
   uint32_t b_stage = 0, psi_stage = 0;                 // bytes of one such buffer
   int n_blocks = 0, n_sm = 148;
   size_t smem = 0;

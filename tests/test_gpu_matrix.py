@@ -120,3 +120,22 @@ def test_plan_reuse_is_deterministic(mq, gpu_available):
     plan.sync()
     assert torch.equal(out[0], out[1])
     plan.close()
+
+
+def test_pinned_output_arrays_match_pageable(mq, gpu_available):
+    """mqct_build_matrix into pinned host arrays (the copy engine writes them directly) gives
+    the results it writes into pageable arrays (staged through the library's pinned slots);
+    the c2 system at j <= 6 is large enough for the staged path (Mat_el above 16 MB)."""
+    import torch
+    s = _c2_small(mq, jmax=6)
+    R = mq.r_grid(300, 3.0, 25.0)
+    assert s.P * len(R) * 8 > 16 << 20
+    args = (s, R, (12, 12, 0, 0, 0, 0, 1), syn.site_pes(12, seed=2))
+    ref = mq.build_matrix(*args, precision=mq.PREC_FP64)
+    pinned = (torch.empty((s.P, len(R)), dtype=torch.float64, pin_memory=True),
+              torch.empty((s.P, len(R)), dtype=torch.float64, pin_memory=True),
+              torch.empty(s.P, dtype=torch.int32, pin_memory=True))
+    got = mq.build_matrix(*args, precision=mq.PREC_FP64, out=tuple(t.numpy() for t in pinned))
+    mq.release_cached_build()
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
