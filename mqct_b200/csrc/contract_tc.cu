@@ -28,17 +28,18 @@
 // most 128 radial points) x one range of K-chunks.  Column parts keep two FP32
 // accumulators of a part in TMEM (double buffering: the tensor cores fill one
 // while the epilogue drains the other) and the FP64 sums of a part in registers.
-// Warp roles (576 threads):
+// Warp roles (64 + 32 PE threads; PE = 16 epilogue warps when a K-chunk has several
+// accumulation groups, 8 when it has one):
 //   warp 0      bulk-copy (TMA) producer: per K-chunk the pre-arranged W image of
 //               the part (hi and lo planes, K-major core-matrix layout) and the
 //               block's rotor-basis slice, one cp.async.bulk each, mbarrier
 //               complete_tx, double-buffered where shared memory allows;
 //   warp 1      TMEM allocator + single-thread MMA issuer;
-//   warps 2..17 X producers and epilogue: per K-chunk X = Re(psi_a^* psi_b) in FP32
+//   warps 2..   X producers and epilogue: per K-chunk X = Re(psi_a^* psi_b) in FP32
 //               from the staged basis, split to 16-bit hi/lo parts in the
-//               core-matrix layout (four threads per tile row); then, for every
+//               core-matrix layout (PE / 4 threads per tile row); then, for every
 //               alpha point of the chunk, tcgen05.ld of the accumulator and the FP64
-//               update of the sums (four warps per TMEM lane quarter, each a quarter of the
+//               update of the sums (PE / 4 warps per TMEM lane quarter, each a share of the
 //               part's columns); at the end of a unit the FP64 sums go to global
 //               memory, one array per K range.
 // The operand tiles use the K-major SWIZZLE_NONE canonical layout: 8 rows x
@@ -473,7 +474,7 @@ __global__ void __launch_bounds__(TcShape<PE>::THREADS, 1) tc_contract_kernel(Tc
       for (uint32_t it = 0; it < TC_SPIN_LIMIT && !mbar_try_wait(DONE, 0); ++it) {}
     }
   } else {
-    // ---------------- X producers (warps 2..17) and epilogue
+    // ---------------- X producers (warps 2 to PE + 1) and epilogue
     const int t = threadIdx.x - 64;
     const int p = t & (TC_M - 1);  // tile row generated by this thread
     const int kh = t / TC_M;       // share of the chunk's K groups formed by this thread

@@ -11,7 +11,8 @@
 // groups them by the spline interval of their stage point, so that one load of the
 // interval's knots serves the whole group:
 //
-//   ls_rhs  (persistent, one work item at a time from a device queue): item = (interval,
+//   ls_rhs  (one launch per round; persistent CTAs take one work item at a time from a
+//           device queue): item = (interval,
 //           m-block, group of up to G trajectories of that interval).  The block's knot
 //           triangle at the two rows of the interval is staged in shared memory as
 //           (M_lo, M_hi - M_lo, M''_lo, M''_hi) per slot, bt = D^* a of the group's
@@ -27,12 +28,15 @@
 //           and the block's share of F = Re(bt^+ M' bt), g = Im((D^* u)^+ y) and
 //           pot = Re(bt^+ y), written per (trajectory, block) -- no atomics, so every
 //           sum has a fixed order and the results do not depend on the grouping.
-//   ls_cls  (one warp per trajectory): sums the block shares in block order, forms the
-//           classical derivative, takes the RK4 stage of the classical variables, at the
-//           end of a step the stop rules (MQCT_SOURCE_CODES/propagator.f:4011-4050); sets
-//           up the next stage point (spline interval, factors, phases e^{-iEt} per
-//           energy class) and registers the trajectory in the bucket of its interval; the
-//           last CTA to finish forms the next round's groups of up to G trajectories.
+//           The item that completes a trajectory's blocks (a per-trajectory counter)
+//           takes its classical step with one warp (ls_traj_step): the block shares
+//           summed in block order, the classical derivative, the RK4 stage of the
+//           classical variables, at the end of a step the stop rules
+//           (MQCT_SOURCE_CODES/propagator.f:4011-4050); the next stage point (spline
+//           interval, factors, phases e^{-iEt} per energy class); the trajectory is
+//           registered in its interval's bucket for the next round.  The last CTA to
+//           finish the round forms the next round's groups of up to G trajectories
+//           (ls_group).  ls_init_kernel does the same for the start of a run.
 //
 // A finished trajectory takes one closing evaluation at its final state (the energy
 // bookkeeping of MQCT_SOURCE_CODES/propagator.f:4182-4343) and retires.  The arithmetic
