@@ -235,6 +235,20 @@ double mqct_matrix_plan_flops(const mqct_matrix_plan* plan);
 int mqct_matrix_plan_set_drain(mqct_matrix_plan* plan, int32_t slices_per_drain);
 int mqct_matrix_plan_layout(const mqct_matrix_plan* plan, int32_t* slices_per_drain,
                             int32_t* k_ranges, int32_t* column_parts);
+/* Epilogue layout of the tensor-core contraction (no reference counterpart): 8 warps (two
+ * per TMEM lane quarter, more registers each) or 16 (four per lane quarter, more of the
+ * latency-bound drain in flight).  By default the launch takes 16 when a K-chunk has several
+ * accumulation groups and 8 otherwise; mqct_matrix_plan_tune times one execute with each
+ * (into the caller's device outputs, which receive the build) and keeps the faster.  The two
+ * layouts give bitwise identical results (every column's sum has the same order).
+ * mqct_matrix_plan_epilogue reports the layout the next execute uses and, after tuning,
+ * the contraction times of the two (tune_ms[2], may be NULL).  The FP64 form has no such
+ * layout (tune returns at once, epilogue reports 0). */
+int mqct_matrix_plan_tune(mqct_matrix_plan* plan, double* d_mat, double* d_y2,
+                          int32_t* d_skipped);
+int mqct_matrix_plan_epilogue(const mqct_matrix_plan* plan, int32_t* warps, float* tune_ms);
+/* Force the layout (8 or 16 warps) for the following executes, or 0 for the default rule. */
+int mqct_matrix_plan_set_epilogue(mqct_matrix_plan* plan, int32_t warps);
 /* CUDA-event timings (ms) of the last execute, recorded on the plan's stream:
  * t3[0] basis + PES tables, t3[1] contraction, t3[2] finalize (units, cutoff,
  * spline).  Waits for the execute to finish. */

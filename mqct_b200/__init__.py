@@ -510,6 +510,23 @@ class MatrixPlan:
         check(lib().mqct_matrix_plan_layout(self.h, C.byref(a), C.byref(b), C.byref(c)))
         return int(a.value), int(b.value), int(c.value)
 
+    def tune(self, d_mat: int, d_y2: int = 0, d_skipped: int = 0):
+        """Time the two epilogue layouts of the tensor-core contraction (one execute each into
+        these device outputs) and keep the faster (mqct_matrix_plan_tune)."""
+        check(lib().mqct_matrix_plan_tune(self.h, d_mat, d_y2 or None, d_skipped or None))
+
+    def set_epilogue(self, warps=0):
+        """Force 8 or 16 epilogue warps for the following executes (0: the default rule)."""
+        check(lib().mqct_matrix_plan_set_epilogue(self.h, int(warps)))
+
+    def epilogue(self):
+        """(epilogue warps of the next execute, contraction ms of the 8- and 16-warp layouts
+        after tuning)."""
+        w = C.c_int32()
+        ms = (C.c_float * 2)()
+        check(lib().mqct_matrix_plan_epilogue(self.h, C.byref(w), ms))
+        return int(w.value), (float(ms[0]), float(ms[1]))
+
     def surrogate_stats(self):
         """(radial points re-evaluated exactly, largest checked residual ratio) of the
         last execute."""

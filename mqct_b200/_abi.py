@@ -84,6 +84,7 @@ class Integrator(C.Structure):
 EXPORTS = [
     "mqct_last_error", "mqct_version", "mqct_device_count", "mqct_build_matrix",
     "mqct_release_cached_build", "mqct_matrix_plan_set_drain", "mqct_matrix_plan_layout",
+    "mqct_matrix_plan_tune", "mqct_matrix_plan_epilogue", "mqct_matrix_plan_set_epilogue",
     "mqct_matrix_plan_create", "mqct_matrix_plan_execute", "mqct_matrix_plan_sync",
     "mqct_matrix_plan_flops", "mqct_matrix_plan_timing", "mqct_matrix_plan_destroy",
     "mqct_spline_y2_noalloc", "mqct_build_matrix_expansion", "mqct_propagate_batch",
@@ -127,6 +128,9 @@ def lib():
                                     C.POINTER(Grid), C.POINTER(Pes), C.c_int32, C.c_double,
                                     C.c_double, C.c_double, f64p, vp, vp, vp]
     L.mqct_matrix_plan_set_drain.argtypes = [vp, C.c_int32]
+    L.mqct_matrix_plan_tune.argtypes = [vp, vp, vp, vp]
+    L.mqct_matrix_plan_set_epilogue.argtypes = [vp, C.c_int32]
+    L.mqct_matrix_plan_epilogue.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float)]
     L.mqct_matrix_plan_layout.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_int32)]
     L.mqct_release_cached_build.argtypes = []

@@ -760,7 +760,8 @@ int MatrixPlan::tc_execute() {
   // sixteen epilogue warps when a K-chunk has several accumulation groups (the drains then
   // dominate: the as-written alpha grid), eight when it has one (the drain of a chunk then
   // alternates with its X production, and eight warps with more registers are faster)
-  const bool many = (a.n_alpha_it + a.slices_per_drain - 1) / a.slices_per_drain >= 2;
+  const bool many = t.pe_force ? t.pe_force == 16
+                               : (a.n_alpha_it + a.slices_per_drain - 1) / a.slices_per_drain >= 2;
   t.pe_warps = many ? 16 : 8;
   if (f16) {
     if (many) tc_contract_kernel<true, 16><<<grid, TcShape<16>::THREADS, t.smem, stream>>>(a);

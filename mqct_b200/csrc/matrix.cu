@@ -1197,6 +1197,51 @@ int mqct_matrix_plan_layout(const mqct_matrix_plan* plan, int32_t* slices_per_dr
   return MQCT_OK;
 }
 
+int mqct_matrix_plan_tune(mqct_matrix_plan* plan, double* d_mat, double* d_y2,
+                          int32_t* d_skipped) {
+  MQCT_ARG_CHECK(plan && d_mat, "null argument");
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  if (!p->tc) return MQCT_OK;  // the FP64 form has one layout
+  const int cand[2] = {8, 16};
+  int best = 0;
+  for (int k = 0; k < 2; ++k) {
+    p->tc->pe_force = cand[k];
+    float t3[3] = {0.f, 0.f, 0.f};
+    for (int rep = 0; rep < 2; ++rep) {  // the first launch of a layout loads its code
+      int rc = p->execute(d_mat, d_y2, d_skipped);
+      if (rc) return rc;
+      MQCT_CUDA_TRY(cudaEventSynchronize(p->ev[3]));
+      rc = p->tc_check_status();
+      if (rc) return rc;
+      MQCT_CUDA_TRY(cudaEventElapsedTime(&t3[1], p->ev[1], p->ev[2]));
+    }
+    p->tc->pe_tune_ms[k] = t3[1];
+    if (t3[1] < p->tc->pe_tune_ms[best]) best = k;
+  }
+  p->tc->pe_force = cand[best];
+  return MQCT_OK;
+}
+
+int mqct_matrix_plan_set_epilogue(mqct_matrix_plan* plan, int32_t warps) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MQCT_ARG_CHECK(warps == 0 || warps == 8 || warps == 16, "epilogue warps %d not 0, 8 or 16",
+                 warps);
+  MatrixPlan* p = reinterpret_cast<MatrixPlan*>(plan);
+  if (p->tc) p->tc->pe_force = warps;
+  return MQCT_OK;
+}
+
+int mqct_matrix_plan_epilogue(const mqct_matrix_plan* plan, int32_t* warps, float* tune_ms) {
+  MQCT_ARG_CHECK(plan && warps, "null argument");
+  const MatrixPlan* p = reinterpret_cast<const MatrixPlan*>(plan);
+  *warps = p->tc ? (p->tc->pe_force ? p->tc->pe_force : p->tc->pe_warps) : 0;
+  if (tune_ms) {
+    tune_ms[0] = p->tc ? p->tc->pe_tune_ms[0] : 0.f;
+    tune_ms[1] = p->tc ? p->tc->pe_tune_ms[1] : 0.f;
+  }
+  return MQCT_OK;
+}
+
 double mqct_matrix_plan_flops(const mqct_matrix_plan* plan) {
   return plan ? reinterpret_cast<const MatrixPlan*>(plan)->flops() : 0.0;
 }

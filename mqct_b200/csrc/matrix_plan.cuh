@@ -20,6 +20,8 @@ struct TcInfo {
   int slices_per_drain = 1;                            // alpha points per FP64 drain
   bool alpha_uniform = true;                           // all alpha weights equal
   int pe_warps = 8;                                    // epilogue warps of the last launch
+  int pe_force = 0;                                    // 8 or 16 (tuned or set), 0: by rule
+  float pe_tune_ms[2] = {0.f, 0.f};                    // contraction ms with 8 and 16
   uint32_t b_stage = 0, psi_stage = 0;                 // bytes of one such buffer
   int n_blocks = 0, n_sm = 148;
   size_t smem = 0;

@@ -109,3 +109,37 @@ def test_tc_plan_reports_flops_and_timing(mq, gpu_available):
     t = plan.timing()
     assert all(x > 0 for x in t)
     plan.close()
+
+
+@pytest.mark.parametrize("grid", [(12, 12, 8, 0, 0, 0, 1), (16, 16, 0, 0, 0, 0, 1)])
+def test_epilogue_layouts_agree_and_tune(mq, gpu_available, grid):
+    """The 8- and 16-warp epilogue layouts of the contraction give bitwise identical
+    matrices (every column's sum has the same order); mqct_matrix_plan_tune times both,
+    keeps one of them and its build equals them."""
+    import torch
+    s = _c2_small(mq)
+    R = mq.r_grid(300, 3.0, 25.0)
+    plan = mq.MatrixPlan(s, R, grid, syn.site_pes(12, seed=2), precision=mq.PREC_F16X3)
+    n = s.P * len(R)
+    out = {}
+    for w in (8, 16, 0):
+        plan.set_epilogue(w)
+        m = torch.empty(n, dtype=torch.float64, device="cuda")
+        y = torch.empty_like(m)
+        sk = torch.empty(s.P, dtype=torch.int32, device="cuda")
+        plan.execute(m.data_ptr(), y.data_ptr(), sk.data_ptr())
+        plan.sync()
+        out[w] = (m.cpu(), y.cpu(), sk.cpu())
+    # the default rule: 16 warps with several accumulation groups per chunk, else 8
+    assert plan.epilogue()[0] == (16 if grid[2] > 2 else 8)
+    m = torch.empty(n, dtype=torch.float64, device="cuda")
+    plan.tune(m.data_ptr())
+    plan.sync()
+    w, ms = plan.epilogue()
+    assert w in (8, 16) and ms[0] > 0 and ms[1] > 0
+    for k in range(3):
+        assert torch.equal(out[8][k], out[16][k]) and torch.equal(out[0][k], out[8][k])
+    assert torch.equal(m.cpu(), out[8][0])
+    with pytest.raises(mq.MqctError):
+        plan.set_epilogue(12)
+    plan.close()
