@@ -238,8 +238,9 @@ int mqct_matrix_plan_layout(const mqct_matrix_plan* plan, int32_t* slices_per_dr
 /* Epilogue layout of the tensor-core contraction (no reference counterpart): 8 warps (two
  * per TMEM lane quarter, more registers each) or 16 (four per lane quarter, more of the
  * latency-bound drain in flight).  By default the launch takes 16 when a K-chunk has several
- * accumulation groups and 8 otherwise; mqct_matrix_plan_tune times one execute with each
- * (into the caller's device outputs, which receive the build) and keeps the faster.  The two
+ * accumulation groups and 8 otherwise; mqct_matrix_plan_tune runs four executes with each
+ * (into the caller's device outputs, which receive the build), takes the minimum contraction
+ * time of the last three and keeps the faster layout.  The two
  * layouts give bitwise identical results (every column's sum has the same order).
  * mqct_matrix_plan_epilogue reports the layout the next execute uses and, after tuning,
  * the contraction times of the two (tune_ms[2], may be NULL).  The FP64 form has no such

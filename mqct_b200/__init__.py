@@ -511,8 +511,9 @@ class MatrixPlan:
         return int(a.value), int(b.value), int(c.value)
 
     def tune(self, d_mat: int, d_y2: int = 0, d_skipped: int = 0):
-        """Time the two epilogue layouts of the tensor-core contraction (one execute each into
-        these device outputs) and keep the faster (mqct_matrix_plan_tune)."""
+        """Time the two epilogue layouts of the tensor-core contraction (four executes each
+        into these device outputs, the minimum of the last three) and keep the faster
+        (mqct_matrix_plan_tune)."""
         check(lib().mqct_matrix_plan_tune(self.h, d_mat, d_y2 or None, d_skipped or None))
 
     def set_epilogue(self, warps=0):
