@@ -476,14 +476,34 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
  * interpolating slot by slot: the same arithmetic type, other rounding.  Its device-buffer
  * runs (mqct_prop_plan_run_device) read the initial conditions back for the bound on the
  * rounds and return when the batch is done.  MQCT_ENGINE_AUTO (default): the lockstep
- * engine for eligible batches of at least 4096 trajectories.  mqct_prop_plan_engine
- * reports the engine of the last run and, for the lockstep engine, the rounds it ran
- * (rounds may be NULL). */
+ * engine for eligible batches of at least 4096 trajectories, the resident engine (below)
+ * for eligible FP32 batches of at most 1024.  MQCT_ENGINE_RESIDENT: one
+ * thread-block cluster per trajectory, the m-blocks split between its CTAs, each holding
+ * the two knot rows of its blocks in shared memory (reloaded when the stage point leaves
+ * the spline interval); the CTAs exchange their parts of the quadratic forms and the
+ * neighbour amplitudes of the Coriolis vector through distributed shared memory once per
+ * right-hand side.  FP32 plans, standard mode, RK4, no CS, no records, m-blocks of at
+ * most 255 states, and the tables must fit the shared memory of a cluster of at most 8
+ * CTAs (other runs take the engine the AUTO rule picks).  Its arithmetic is that of the
+ * per-trajectory kernel (slot-by-slot interpolation), with other summation orders.
+ * MQCT_ENGINE_AUTO takes it for eligible FP32 batches of at most 1024 trajectories (fewer
+ * trajectories at once, each faster: the faster engine for such batches).
+ * mqct_prop_plan_engine reports the engine of the last run and, for the lockstep engine,
+ * the rounds it ran (rounds may be NULL). */
 #define MQCT_ENGINE_AUTO 0
 #define MQCT_ENGINE_PER_TRAJECTORY 1
 #define MQCT_ENGINE_LOCKSTEP 2
+#define MQCT_ENGINE_RESIDENT 3
 int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine);
 int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* rounds);
+/* Cluster size of the resident engine: 0 (default) eight CTAs for a batch that the
+ * clusters of eight hold at once, else the smallest of 2..8 CTAs whose shared memory holds
+ * the tables; or a size in 2..8 (used when the tables fit it).  mqct_prop_plan_cluster
+ * reports the cluster size and the clusters resident on the device: those of the last run
+ * when it took the resident engine, else those of the setting (0 meaning the smallest
+ * size) for the plan's tables; both 0 when the engine does not apply to the plan. */
+int mqct_prop_plan_set_cluster(mqct_prop_plan* plan, int32_t ctas);
+int mqct_prop_plan_cluster(mqct_prop_plan* plan, int32_t* ctas, int32_t* clusters);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */
 int mqct_asym_top_level(double A, double B, double C, int32_t j, int32_t ka, int32_t kc,

@@ -1034,6 +1034,8 @@ struct PropPlan {
   int engine = MQCT_ENGINE_AUTO;
   int last_engine = 0;
   LsEngine* ls = nullptr;
+  RsEngine* rs = nullptr;
+  int rs_cl = 0;  // cluster size asked for the resident engine (0: the smallest that fits)
   bool cs = false;  // CS_APPROX for every run of the plan
   int bk_int = 0;                       // bikram_int (ODEINT with per-step stop rules)
   int at_adapt = 0;                     // AT_ADAPT_STP (RK4 steps of AT runs)
@@ -1468,6 +1470,45 @@ struct PropPlan {
       return false;
     return engine == MQCT_ENGINE_LOCKSTEP || n_traj >= kLockstepMinBatch;
   }
+  // The resident engine takes the runs the lockstep engine could take (FP32 only) when the
+  // tables fit a cluster: always with MQCT_ENGINE_RESIDENT, up to kResidentMaxBatch
+  // trajectories with MQCT_ENGINE_AUTO.  It gives each trajectory a cluster of CTAs, so a
+  // trajectory's steps take less time than on the per-trajectory kernel, but fewer run at
+  // once: on the 969-state asymmetric-top tables it is faster for 33 trajectories (0.64 s
+  // against 1.97 s), 512 (4.55 s against 6.04 s) and 1024 (8.9 s against 10.7 s), slower
+  // for 4096 (35.9 s against 24.2 s).  With the cluster size left to the plan, a batch that
+  // fits the clusters of eight CTAs runs on them (shorter steps), a larger one on the
+  // smallest cluster that holds the tables (more clusters).
+  static constexpr int64_t kResidentMaxBatch = 1024;
+  int rs_clusters8 = -1;  // clusters of eight CTAs resident on the device (-1: not asked yet)
+  int last_rs[2] = {0, 0};  // cluster size and clusters of the last resident run
+  bool use_resident(int mode, int64_t n_traj, bool records) {
+    if (engine == MQCT_ENGINE_PER_TRAJECTORY || engine == MQCT_ENGINE_LOCKSTEP || records ||
+        mode != MQCT_MODE_STD || cs || method != MQCT_INTEG_RK4 || arith != MQCT_PROP_FP32)
+      return false;
+    if (engine == MQCT_ENGINE_AUTO && n_traj > kResidentMaxBatch) return false;
+    if (!rs) rs = rs_create();
+    const PropDev d = dev_view(MQCT_MODE_STD);
+    int cl = rs_cl;
+    if (!cl) {
+      if (rs_clusters8 < 0) {
+        rs_set_cluster(rs, 8);
+        rs_clusters8 = rs_usable(rs, d, h_blk_n, h_blk_s0, stream) ? rs_clusters(rs) : 0;
+      }
+      cl = n_traj <= rs_clusters8 ? 8 : 0;
+    }
+    rs_set_cluster(rs, cl);
+    return rs_usable(rs, d, h_blk_n, h_blk_s0, stream);
+  }
+  int run_resident(const mqct_traj_init_t* d_init_p, int64_t n_traj, double* amp, double* cls,
+                   double* diag) {
+    MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1LL << 31), "n_traj out of range");
+    last_engine = MQCT_ENGINE_RESIDENT;
+    last_rs[0] = rs_cluster(rs);
+    last_rs[1] = rs_clusters(rs);
+    return rs_run(rs, dev_view(MQCT_MODE_STD), h_blk_n, h_blk_s0, stream, ev0, ev1, d_init_p,
+                  (int)n_traj, amp, cls, diag);
+  }
   int run_lockstep(const mqct_traj_init_t* d_init_p, const mqct_traj_init_t* h_init,
                    int64_t n_traj, double* amp, double* cls, double* diag) {
     MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 24), "n_traj out of range for the lockstep engine");
@@ -1479,6 +1520,7 @@ struct PropPlan {
 
   ~PropPlan() {
     if (ls) ls_destroy(ls);
+    if (rs) rs_destroy(rs);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -1531,8 +1573,9 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
   }
   std::vector<mqct_traj_init_t> sorted(n_traj);
   for (int64_t t = 0; t < n_traj; ++t) sorted[t] = init[order[t]];
-  const bool lockstep = p->use_lockstep(mode, n_traj, rec_out != nullptr);
-  if (!lockstep && !p->tuned && p->method == MQCT_INTEG_RK4 && n_traj >= 2LL * p->n_sm) {
+  const bool resident = p->use_resident(mode, n_traj, rec_out != nullptr);
+  const bool lockstep = !resident && p->use_lockstep(mode, n_traj, rec_out != nullptr);
+  if (!lockstep && !resident && !p->tuned && p->method == MQCT_INTEG_RK4 && n_traj >= 2LL * p->n_sm) {
     rc = p->tune(sorted.data(), n_traj, mode);
     if (rc) return rc;
   }
@@ -1540,7 +1583,10 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
   MQCT_CUDA_TRY(p->d_amp.alloc((size_t)n_traj * 2 * p->N));
   MQCT_CUDA_TRY(p->d_cls.alloc((size_t)n_traj * 6));
   MQCT_CUDA_TRY(p->d_diag.alloc((size_t)n_traj * 8));
-  if (lockstep) {
+  if (resident) {
+    rc = p->run_resident(p->d_init.p, n_traj, p->d_amp.p, p->d_cls.p, p->d_diag.p);
+    if (rc) return rc;
+  } else if (lockstep) {
     rc = p->run_lockstep(p->d_init.p, sorted.data(), n_traj, p->d_amp.p, p->d_cls.p, p->d_diag.p);
     if (rc) return rc;
   }
@@ -1550,7 +1596,7 @@ static int run_host(PropPlan* p, const mqct_traj_init_t* init, int64_t n_traj, i
     MQCT_CUDA_TRY(d_rec.alloc((size_t)n_traj * rec_cap * 8));
     MQCT_CUDA_TRY(d_nrec.alloc((size_t)n_traj));
   }
-  if (!lockstep) {
+  if (!lockstep && !resident) {
     rc = p->launch(p->d_init.p, n_traj, mode, p->d_amp.p, p->d_cls.p, p->d_diag.p, d_rec.p,
                    rec_cap, d_nrec.p);
     if (rc) return rc;
@@ -1618,6 +1664,15 @@ int mqct_prop_plan_run_device(mqct_prop_plan* plan, const mqct_traj_init_t* d_in
                               int64_t n_traj, double* d_amp, double* d_cls, double* d_diag) {
   MQCT_ARG_CHECK(plan && d_init && d_amp && d_cls && d_diag, "null argument");
   PropPlan* p = reinterpret_cast<PropPlan*>(plan);
+  if (p->use_resident(MQCT_MODE_STD, n_traj, false)) {
+    std::vector<mqct_traj_init_t> h((size_t)n_traj);
+    MQCT_CUDA_TRY(cudaMemcpyAsync(h.data(), d_init, sizeof(mqct_traj_init_t) * n_traj,
+                                  cudaMemcpyDeviceToHost, p->stream));
+    MQCT_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    const int rc = validate_init(h.data(), n_traj, p->N, MQCT_MODE_STD);
+    if (rc) return rc;
+    return p->run_resident(d_init, n_traj, d_amp, d_cls, d_diag);
+  }
   if (p->use_lockstep(MQCT_MODE_STD, n_traj, false)) {
     // the lockstep engine bounds its rounds by the trajectories' step caps and time limits
     MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 24), "n_traj out of range for the lockstep engine");
@@ -1685,9 +1740,36 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
 int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine) {
   MQCT_ARG_CHECK(plan, "null plan");
   MQCT_ARG_CHECK(engine == MQCT_ENGINE_AUTO || engine == MQCT_ENGINE_PER_TRAJECTORY ||
-                     engine == MQCT_ENGINE_LOCKSTEP,
+                     engine == MQCT_ENGINE_LOCKSTEP || engine == MQCT_ENGINE_RESIDENT,
                  "unknown engine %d", engine);
   reinterpret_cast<PropPlan*>(plan)->engine = engine;
+  return MQCT_OK;
+}
+
+int mqct_prop_plan_set_cluster(mqct_prop_plan* plan, int32_t ctas) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  MQCT_ARG_CHECK(ctas == 0 || (ctas >= 2 && ctas <= 8), "cluster size %d not 0 or 2..8", ctas);
+  reinterpret_cast<PropPlan*>(plan)->rs_cl = ctas;
+  return MQCT_OK;
+}
+
+int mqct_prop_plan_cluster(mqct_prop_plan* plan, int32_t* ctas, int32_t* clusters) {
+  MQCT_ARG_CHECK(plan, "null plan");
+  PropPlan* p = reinterpret_cast<PropPlan*>(plan);
+  if (ctas) *ctas = 0;
+  if (clusters) *clusters = 0;
+  if (p->arith != MQCT_PROP_FP32) return MQCT_OK;
+  if (p->last_engine == MQCT_ENGINE_RESIDENT) {
+    if (ctas) *ctas = p->last_rs[0];
+    if (clusters) *clusters = p->last_rs[1];
+    return MQCT_OK;
+  }
+  if (!p->rs) p->rs = rs_create();
+  rs_set_cluster(p->rs, p->rs_cl);
+  if (!rs_usable(p->rs, p->dev_view(MQCT_MODE_STD), p->h_blk_n, p->h_blk_s0, p->stream))
+    return MQCT_OK;
+  if (ctas) *ctas = rs_cluster(p->rs);
+  if (clusters) *clusters = rs_clusters(p->rs);
   return MQCT_OK;
 }
 

@@ -116,4 +116,20 @@ int ls_run(LsEngine* e, const PropDev& d, bool fp32, const std::vector<int>& blk
            cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const mqct_traj_init_t* d_init,
            const mqct_traj_init_t* h_init, int n_traj, double* amp, double* cls, double* diag);
 
+// Cluster-resident engine (resident.cu): standard mode, RK4, no CS, FP32; one thread-block
+// cluster per trajectory holds the knot rows of its spline interval in shared memory.
+// rs_usable lays the engine out for the tables (once per table) and reports whether they
+// fit; rs_run launches it on stream st, ev0 / ev1 bracketing the kernel.
+struct RsEngine;
+RsEngine* rs_create();
+void rs_destroy(RsEngine* e);
+void rs_set_cluster(RsEngine* e, int cl);
+int rs_cluster(const RsEngine* e);
+int rs_clusters(const RsEngine* e);
+bool rs_usable(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+               const std::vector<int>& blk_s0, cudaStream_t st);
+int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+           const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+           const mqct_traj_init_t* d_init, int n_traj, double* amp, double* cls, double* diag);
+
 }  // namespace mqct
