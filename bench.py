@@ -478,6 +478,31 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
                       "traj_steps": float(diag[:, 1].sum()),
                       "max_status": float(diag[:, 4].max())}
     plan.close()
+    # a batch that cannot fill the GPU (132 trajectories, every 31st of the set): the
+    # cluster-resident engine (the plan's choice for FP32 batches up to 1024) against the
+    # per-trajectory kernel in FP32 and in FP64 (the FP64 form)
+    small = trajs[::31][:132]
+    sb = {"n_traj": len(small)}
+    sp = {}
+    for name, arith, engine in (("fp32_resident", mq.PROP_FP32, mq.ENGINE_RESIDENT),
+                                ("fp32_per_trajectory", mq.PROP_FP32, mq.ENGINE_PER_TRAJECTORY),
+                                ("fp64", mq.PROP_FP64, mq.ENGINE_PER_TRAJECTORY)):
+        plan = mq.PropagationPlan(tab, arith)
+        plan.set_engine(engine)
+        plan.run(small[:8])
+        amp, cls, diag = plan.run(small)
+        ms = replicas.max_over_ranks(plan.timing(), dist, device="cuda")
+        sb[name] = {"kernel_ms": ms, "traj_per_s": world * len(small) / (ms / 1e3),
+                    "max_status": float(diag[:, 4].max())}
+        if engine == mq.ENGINE_RESIDENT:
+            sb[name]["cluster_ctas"], sb[name]["clusters"] = plan.cluster()
+        sp[name] = mq.channel_probabilities(amp, s.indx_chann, s.n_channels)
+        plan.close()
+    sb["speedup_resident_vs_fp32_per_trajectory"] = (sb["fp32_per_trajectory"]["kernel_ms"] /
+                                                     sb["fp32_resident"]["kernel_ms"])
+    sb["speedup_resident_vs_fp64_form"] = sb["fp64"]["kernel_ms"] / sb["fp32_resident"]["kernel_ms"]
+    sb["max_abs_prob_diff_resident_vs_fp64"] = float(np.abs(sp["fp32_resident"] - sp["fp64"]).max())
+    res["small_batch"] = sb
     # cross sections from the split-precision matrix against those from the FP64 form's
     # matrix: the same 256 trajectories propagated in FP64 on each
     if mat64 is not None:
