@@ -758,8 +758,9 @@ static int rs_prepare(RsEngine* e, const PropDev& d, const std::vector<int>& blk
     }
   }
   if (!CL) return MQCT_OK;
+  // the largest request any layout may make (plans of other tables share the function)
   MQCT_CUDA_TRY(cudaFuncSetAttribute((const void*)rs_kernel,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)room));
   cudaLaunchConfig_t cfg{};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -778,13 +779,16 @@ static int rs_prepare(RsEngine* e, const PropDev& d, const std::vector<int>& blk
   const int N = d.N;
   std::vector<int> st_e(N), nbp(N), nbm(N), perm(N);
   std::vector<double> cp(N), cm(N), Rh(d.nR);
-  MQCT_CUDA_TRY(cudaMemcpy(st_e.data(), d.st_e, sizeof(int) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(nbp.data(), d.nb_plus, sizeof(int) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(nbm.data(), d.nb_minus, sizeof(int) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(perm.data(), d.perm, sizeof(int) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(cp.data(), d.cplus, sizeof(double) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(cm.data(), d.cminus, sizeof(double) * N, cudaMemcpyDeviceToHost));
-  MQCT_CUDA_TRY(cudaMemcpy(Rh.data(), d.R, sizeof(double) * d.nR, cudaMemcpyDeviceToHost));
+  // the plan's tables, read back on its stream (they were uploaded on it)
+  const cudaMemcpyKind D2H = cudaMemcpyDeviceToHost;
+  MQCT_CUDA_TRY(cudaMemcpyAsync(st_e.data(), d.st_e, sizeof(int) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(nbp.data(), d.nb_plus, sizeof(int) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(nbm.data(), d.nb_minus, sizeof(int) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(perm.data(), d.perm, sizeof(int) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(cp.data(), d.cplus, sizeof(double) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(cm.data(), d.cminus, sizeof(double) * N, D2H, st));
+  MQCT_CUDA_TRY(cudaMemcpyAsync(Rh.data(), d.R, sizeof(double) * d.nR, D2H, st));
+  MQCT_CUDA_TRY(cudaStreamSynchronize(st));
   std::vector<double> ih(d.nR, 0.0);
   for (int k = 0; k + 1 < d.nR; ++k) ih[k] = 1.0 / (Rh[k + 1] - Rh[k]);
   std::vector<int> b0(CL + 1, 0), blk, ls0, lr0, rows(CL, 0), nslots(CL, 0), owner(N, 0);
