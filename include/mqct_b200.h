@@ -600,6 +600,24 @@ int mqct_write_cross_sections(const char* path, double U_cm, int32_t chann_ini, 
                               const int32_t* exists, const double* sigma_f, const double* E_bill,
                               double p_err_pct, int32_t with_e_err, double e_err_pct);
 int mqct_write_cross_sections_footer(const char* path, int32_t n_traj_total);
+/* The elastic-scattering files of ELAST_CALC (MQCT_SOURCE_CODES/propagator.f:5897-5943):
+ *   mqct_write_deflection: one block of DEFLECTION_FUNCTION.out, per trajectory l, l / k,
+ *     the deflection angle and the scattering phase (rad), the finish time (a.u.), the
+ *     energy and norm errors (percent), the orbiting periods and the oscillations of R;
+ *   mqct_write_diff_cross: one block of DIFF_CROSS.out, the angles (given in rad, written
+ *     in degrees) and the elastic differential cross section (Angstrom^2).
+ * The deflection angles, phases and cross sections themselves are host arithmetic on the
+ * propagation's outputs (mqct_b200.deflection_angles, scattering_phases,
+ * elastic_cross_section, differential_cross_section). */
+int mqct_write_deflection(const char* path, int32_t s_st, int32_t j12, int32_t m12,
+                          int32_t i_ener, double U_cm, int32_t n_traj, const int32_t* l,
+                          double k_vec, const double* deflection, const double* phase,
+                          const double* finish_time, const double* e_err_pct,
+                          const double* p_err_pct, const int32_t* periods,
+                          const int32_t* oscillations);
+int mqct_write_diff_cross(const char* path, int32_t i_ener, int32_t s_st, int32_t j12,
+                          int32_t m12, int32_t n_angles, const double* theta_rad,
+                          const double* dcs);
 
 /* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
  * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 1, 3, 4, 7, 8, 9 and 0: the

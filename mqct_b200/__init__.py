@@ -859,6 +859,103 @@ def cross_sections(prob, j_ini, J_down, J_up, L_min, k_vec, U_cm=None, e_ch=None
     return sig_U, sig_U * U_cm / e_bill, e_bill
 
 
+def deflection_angles(cls, trajs, mass_au):
+    """Deflection angle of each trajectory (rad), the DEFLCT_ANGLE column of
+    DEFLECTION_FUNCTION.out (MQCT_SOURCE_CODES/propagator.f:3260-3294, 4485): the angle
+    from the final to the initial velocity, signed by the z component of
+    v_final x v_initial, its windings past -pi counted (the reference's loop count); pi for
+    l = 0 (head-on).  cls: the final classical variables (R, P_R, theta, P_theta, phi, P_phi)
+    as the propagation returns them; trajs: the initial conditions (e_coll, l_real,
+    r_start).  The motion stays in the plane theta = pi/2, so the velocity's direction
+    angle is phi + atan2(v_phi, v_R) with v_phi = P_phi / (m R sin theta) > 0, a continuous
+    function of time: its change over the trajectory is the reference's step-by-step
+    angle with its loops.  The reference evaluates it at the start of its last loop pass
+    (one step before the final state); the difference is below its printed digits."""
+    cls = np.asarray(cls, dtype=np.float64)
+    out = np.empty(len(trajs))
+    for i, t in enumerate(trajs):
+        if t.l_real == 0.0:
+            out[i] = np.pi
+            continue
+        k = np.sqrt(2.0 * mass_au * t.e_coll)
+        lo = np.sqrt(t.l_real * (t.l_real + 1.0))
+        pr0 = -np.sqrt(k * k - lo * lo / (t.r_start * t.r_start))
+        psi0 = np.arctan2(lo / (mass_au * t.r_start), pr0 / mass_au)
+        R, PR, th, _, phi, Pphi = cls[i]
+        psi = phi + np.arctan2(Pphi / (mass_au * R * np.sin(th)), PR / mass_au)
+        out[i] = psi0 - psi
+    return out
+
+
+def scattering_phases(l, deflection):
+    """Scattering phase of each trajectory (rad), the SCAT_PHASE column of
+    DEFLECTION_FUNCTION.out (ELAST_CALC, MQCT_SOURCE_CODES/propagator.f:5694-5715): zero for
+    the last trajectory, then backwards phase_i = phase_{i+1} - (chi_i + chi_{i+1}) / 2
+    |l_{i+1} - l_i| (trapezoid over the deflection function)."""
+    l = np.asarray(l, dtype=np.float64)
+    chi = np.asarray(deflection, dtype=np.float64)
+    ph = np.zeros(len(chi))
+    for i in range(len(chi) - 2, -1, -1):
+        ph[i] = ph[i + 1] - (chi[i] + chi[i + 1]) / 2.0 * abs(l[i + 1] - l[i])
+    return ph
+
+
+def elastic_cross_section(l, p_elastic, phase, k_vec, weight=None):
+    """Elastic cross section (Angstrom^2), the elastic row of CROSS_SECTIONS.out without
+    DIFF_CROSS (ELAST_CALC, MQCT_SOURCE_CODES/propagator.f:5717-5749):
+    sigma_el = pi / k^2 sum_i w_i |1 - sqrt(P_el,i) e^{i phase_i}|^2 (2 l_i + 1) |l_{i+1} - l_i|
+    over all trajectories but the last; weight: the identical-particle parity weights w_i
+    (1 when None)."""
+    l = np.asarray(l, dtype=np.float64)
+    p = np.asarray(p_elastic, dtype=np.float64)
+    ph = np.asarray(phase, dtype=np.float64)
+    w = np.ones(len(l)) if weight is None else np.asarray(weight, dtype=np.float64)
+    s = 0.0
+    for i in range(len(l) - 1):
+        amp = 1.0 - np.sqrt(p[i]) * np.exp(1j * ph[i])
+        s += w[i] * abs(amp) ** 2 / k_vec ** 2 * np.pi * (2.0 * l[i] + 1.0) * abs(l[i + 1] - l[i])
+    return s * A_BOHR ** 2
+
+
+def differential_cross_section(p_elastic, phase, j_ini, J_down, J_up, L_min, k_vec, n_angles,
+                               dl=1):
+    """Elastic differential cross section (DIFF_CROSS = YES; ELAST_CALC,
+    MQCT_SOURCE_CODES/propagator.f:5755-5830): on the angles theta_k = (k - 1) pi /
+    (n_angles - 1),
+    f(theta) = i / (2 k (2j + 1)) sum_J (2J + 1) sum_{l=|J-j|}^{J+j} P_l(cos theta)
+               (1 - sqrt(P_el(traj(l))) e^{i phase(traj(l))}),
+    dsigma/dOmega = |f|^2 (Angstrom^2, the DIFF_CROSS.out column), and the elastic cross
+    section 2 pi int dsigma/dOmega sin theta dtheta by the trapezoid rule over the angles,
+    which replaces the one above in CROSS_SECTIONS.out.  traj(l) = (l - L_min) / dl as in
+    INELAST_CALC.  Returns (theta in rad, dsigma/dOmega, sigma_el).  The reference's
+    trapezoid sum starts at k = 1 and so reads the elements before its arrays; it starts at
+    the second angle here."""
+    p = np.asarray(p_elastic, dtype=np.float64)
+    ph = np.asarray(phase, dtype=np.float64)
+    n_traj = len(p)
+    theta = np.arange(n_angles) * np.pi / (n_angles - 1)
+    x = np.cos(theta)
+    lmax = J_up + j_ini
+    # Legendre polynomials P_l(x) by the three-term recurrence
+    P = np.zeros((lmax + 1, n_angles))
+    P[0] = 1.0
+    if lmax >= 1:
+        P[1] = x
+    for n in range(2, lmax + 1):
+        P[n] = ((2 * n - 1) * x * P[n - 1] - (n - 1) * P[n - 2]) / n
+    f = np.zeros(n_angles, dtype=np.complex128)
+    for J in range(J_down, J_up + 1):
+        for lv in range(abs(J - j_ini), J + j_ini + 1):
+            i = (lv - L_min) // dl
+            if 0 <= i < n_traj:
+                f += (P[lv] * (1.0 - np.sqrt(p[i]) * np.exp(1j * ph[i])) * (2.0 * J + 1.0)
+                      * 1j / k_vec / 2.0 / (2.0 * j_ini + 1.0))
+    dcs = np.abs(f) ** 2
+    sig = float(np.sum((dcs[:-1] * np.sin(theta[:-1]) + dcs[1:] * np.sin(theta[1:]))
+                       * np.pi * np.diff(theta)))
+    return theta, dcs * A_BOHR ** 2, sig * A_BOHR ** 2
+
+
 def cross_sections_device(d_amp, system: CollisionSystem, j_ini, J_down, J_up, L_min, k_vec,
                           dl=1):
     """INELAST_CALC on the GPU from device amplitudes (a CUDA float64 torch tensor, n_traj x
@@ -1052,6 +1149,28 @@ def write_opacity(path, s_st, j12, m12, i_ener, U_cm, l, k_vec, prob, path_total
                                    int(s_st), int(j12), int(m12), int(i_ener), float(U_cm),
                                    len(li), li, float(k_vec), prob.shape[1], prob.reshape(-1),
                                    int(chann_ini)))
+
+
+def write_deflection(path, s_st, j12, m12, i_ener, U_cm, l, k_vec, deflection, phase,
+                     finish_time, e_err_pct, p_err_pct, periods, oscillations):
+    """Append one block to DEFLECTION_FUNCTION.out (per trajectory: l, l / k, deflection
+    angle and scattering phase in rad, finish time in a.u., energy and norm errors in
+    percent, orbiting periods, oscillations of R)."""
+    f64 = lambda a: np.ascontiguousarray(a, np.float64)  # noqa: E731
+    li = np.ascontiguousarray(l, np.int32)
+    check(lib().mqct_write_deflection(path.encode(), int(s_st), int(j12), int(m12), int(i_ener),
+                                      float(U_cm), len(li), li, float(k_vec), f64(deflection),
+                                      f64(phase), f64(finish_time), f64(e_err_pct),
+                                      f64(p_err_pct), np.ascontiguousarray(periods, np.int32),
+                                      np.ascontiguousarray(oscillations, np.int32)))
+
+
+def write_diff_cross(path, i_ener, s_st, j12, m12, theta, dcs):
+    """Append one block to DIFF_CROSS.out (theta in rad, written in degrees; dsigma/dOmega
+    in Angstrom^2)."""
+    th = np.ascontiguousarray(theta, np.float64)
+    check(lib().mqct_write_diff_cross(path.encode(), int(i_ener), int(s_st), int(j12), int(m12),
+                                      len(th), th, np.ascontiguousarray(dcs, np.float64)))
 
 
 def write_partial_j(path, s_st, j12, m12, i_ener, U_cm, J, partial):

@@ -854,6 +854,53 @@ int mqct_write_opacity(const char* path, const char* path_total, int32_t s_st, i
   return close_checked(f, path_total);
 }
 
+// DEFLECTION_FUNCTION.out (ELAST_CALC, propagator.f:5897-5928): per trajectory l, l / k,
+// the deflection angle and scattering phase (rad), the finish time (a.u.), the energy and
+// norm errors (percent), the orbiting periods and the oscillations of R.
+int mqct_write_deflection(const char* path, int32_t s_st, int32_t j12, int32_t m12,
+                          int32_t i_ener, double U_cm, int32_t n_traj, const int32_t* l,
+                          double k_vec, const double* deflection, const double* phase,
+                          const double* finish_time, const double* e_err_pct,
+                          const double* p_err_pct, const int32_t* periods,
+                          const int32_t* oscillations) {
+  MQCT_ARG_CHECK(path && l && deflection && phase && finish_time && e_err_pct && p_err_pct &&
+                     periods && oscillations && n_traj > 0 && k_vec > 0.0,
+                 "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  fprintf(f, "energy#%d, (U= %s cm^-1)\nstate= %d\nj12= %d\nm12= %d\n", i_ener,
+          fortran_f0_3(U_cm).c_str(), s_st, j12, m12);
+  fprintf(f, "%5s  %14s     %17s    %15s       %17s    %15s      %13s    %5s   %5s\n", "L_ORB",
+          "B_IMPACT(a.u.)", "DEFLCT_ANGLE(rad)", "SCAT_PHASE(rad)", "FINISH_TIME(a.u.)",
+          "ENERGY_ERROR(%)", "NORM_ERROR(%)", "LOOPS", "OSCIL");
+  for (int t = 0; t < n_traj; ++t)
+    fprintf(f, "%4d  %s %s  %s   %s %s %s   %5d   %5d\n", l[t],
+            fortran_e(l[t] / k_vec, 15, 8).c_str(), fortran_e(deflection[t], 19, 8).c_str(),
+            fortran_e(phase[t], 19, 8).c_str(), fortran_e(finish_time[t], 19, 8).c_str(),
+            fortran_e(e_err_pct[t], 19, 8).c_str(), fortran_e(p_err_pct[t], 19, 8).c_str(),
+            periods[t], oscillations[t]);
+  fprintf(f, " \n");
+  return close_checked(f, path);
+}
+
+// DIFF_CROSS.out (ELAST_CALC with DIFF_CROSS = YES, propagator.f:5931-5943): the angle
+// in degrees and the elastic differential cross section in Angstrom^2 (list-directed
+// header records as gfortran writes them).
+int mqct_write_diff_cross(const char* path, int32_t i_ener, int32_t s_st, int32_t j12,
+                          int32_t m12, int32_t n_angles, const double* theta_rad,
+                          const double* dcs) {
+  MQCT_ARG_CHECK(path && theta_rad && dcs && n_angles > 0, "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  fprintf(f, " energy %11d\n state =  %11d\n j12= %11d\n m12= %11d\n", i_ener, s_st, j12, m12);
+  fprintf(f, "%19s %19s\n", "ANGLE,deg", "DIFF. CROSS.,angs^2");
+  for (int k = 0; k < n_angles; ++k)
+    fprintf(f, "%s %s\n", fortran_e(theta_rad[k] * 180.0 / kPi, 19, 7).c_str(),
+            fortran_e(dcs[k], 19, 7).c_str());
+  fprintf(f, " \n");
+  return close_checked(f, path);
+}
+
 // PARTIAL_CROSS_SECTIONS_J.out (propagator.f:4845-4868): per total J the J-resolved
 // cross sections of every channel, Angstrom^2.
 int mqct_write_partial_j(const char* path, int32_t s_st, int32_t j12, int32_t m12,

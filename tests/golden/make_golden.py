@@ -179,10 +179,31 @@ def main(ref_root):
                             open(os.path.join(d, name)).read())
                            for name in ("OPACITY_FUNCTIONS_L.out", "TOTAL_PROBABILITIES_L.out",
                                         "PARTIAL_CROSS_SECTIONS_J.out", "M_PROJ_CROSSECTIONS.out",
-                                        "CROSS_SECTIONS.out")},
+                                        "CROSS_SECTIONS.out", "DEFLECTION_FUNCTION.out")},
                         # $SYSTEM of MF_He_CS_MQCT.inp (R_COM in bohr whatever R_UNITS)
                         mass_red=3.7523705333, rmax=42.40, U=50.0, b_impct=20.0,
                         time_step=10.0, time_lim=3.5e6)
+
+    # G8: elastic scattering with DIFF_CROSS = YES (ND3 + D2, SYS_TYPE 7, U = 800 cm^-1,
+    # 101 trajectories l = 0..100, j_ini = 0, 2000 angles): the printed deflection function
+    # and phases, the elastic channel's probabilities, the differential cross section and
+    # the elastic cross section of CROSS_SECTIONS.out (ELAST_CALC, propagator.f:5581-6137).
+    d = os.path.join(ex, "SYS_TYPE_7", "NH3_H2_DIFF_CROSS")
+    defl8 = _read_table(os.path.join(d, "DEFLECTION_FUNCTION.out"), 9, first_int=False)
+    opac8 = _read_table(os.path.join(d, "OPACITY_FUNCTIONS_L.out"), 16)
+    sig8 = []
+    for line in open(os.path.join(d, "CROSS_SECTIONS.out")):
+        t = line.split()
+        if len(t) == 5 and t[0].isdigit():
+            sig8.append(float(t[2]))
+    np.savez_compressed(os.path.join(out, "g8_diff_cross.npz"), deflection=defl8,
+                        p_elastic=opac8[:, 2], sigma_U=np.array(sig8),
+                        text_diff_cross=np.array(open(os.path.join(d, "DIFF_CROSS.out")).read()),
+                        text_deflection_function=np.array(
+                            open(os.path.join(d, "DEFLECTION_FUNCTION.out")).read()),
+                        # $SYSTEM of NH3H2.inp
+                        mass_red=3.354120939, U=800.0, n_angles=2000, j_ini=0, J_down=0,
+                        J_up=100, L_min=0, dl=1)
 
     # G1 AT trajectory record layout: Fortran unformatted, 8 float64 per record.
     d = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_AT_Approximation", "AT_MQCT_2nd_Step",

@@ -2,7 +2,9 @@
 CS example (fixture tests/golden/g4_type4_layout.npz, see tests/test_oracle_cs.py) run
 through mqct_propagate_batch against the oracle and the reference's printed results,
 in FP64 (probabilities within 1e-8 of the oracle, 2e-7 of the 8 printed digits) and
-FP32 (2e-4), the plan switch, and AT-MQCT with CS against the oracle (1e-9)."""
+FP32 (2e-4), the plan switch, AT-MQCT with CS against the oracle (1e-9), and the elastic
+scattering of ELAST_CALC (deflection function, phases, elastic cross section) from the
+final classical states against the printed ones."""
 import os
 
 import numpy as np
@@ -76,3 +78,21 @@ def test_cs_at_mode_matches_oracle(mq, oracle, gpu_available, g4):
         oamp, odiag = oracle.dotraject_at(g4["otab"], g4["otr"][i], paths[n])
         assert np.max(np.abs(amp[n] - oamp)) < 1e-9
         assert diag[n, 1] == odiag[1]
+
+
+def test_elastic_scattering_matches_reference(mq, gpu_available, g4):
+    """ELAST_CALC from the propagation's final classical states: the deflection function
+    (DEFLECTION_FUNCTION.out, 8 printed digits) within 1e-6 rad, the scattering phases
+    within 1e-5 rad, and the elastic cross section of CROSS_SECTIONS.out within 1e-6
+    relative."""
+    amp, cls, diag = mq.propagate(g4["tab"], g4["trajs"], arith=mq.PROP_FP64,
+                                  coupled_states=True)
+    d = g4["g"]["deflection"]
+    chi = mq.deflection_angles(cls, g4["trajs"], g4["tab"].mass_au)
+    assert np.max(np.abs(chi - d[:, 2])) < 1e-6
+    l = np.array([t.l_real for t in g4["trajs"]])
+    ph = mq.scattering_phases(l, chi)
+    assert np.max(np.abs(ph - d[:, 3])) < 1e-5
+    pg = channel_prob(amp, g4["g"]["states"])
+    sig = mq.elastic_cross_section(l, pg[:, 0], ph, g4["k"])
+    assert abs(sig / g4["g"]["sigma_U"][0] - 1) < 1e-6
