@@ -618,6 +618,11 @@ int mqct_write_deflection(const char* path, int32_t s_st, int32_t j12, int32_t m
 int mqct_write_diff_cross(const char* path, int32_t i_ener, int32_t s_st, int32_t j12,
                           int32_t m12, int32_t n_angles, const double* theta_rad,
                           const double* dcs);
+/* SPLINED_DEFLECTION_OPACITY_L.out of PROB_SPLINE runs (MQCT_SOURCE_CODES/propagator.f:
+ * 6063-6110): per integer l (l[i], i < n_l) l / k, l, the splined deflection function and
+ * the splined channel probabilities prob[i * n_ch + c] (mqct_b200.splined_opacity). */
+int mqct_write_splined_opacity(const char* path, int32_t n_l, const int32_t* l, double k_vec,
+                               const double* deflection, int32_t n_ch, const double* prob);
 
 /* CALC_EXPANSION_TERMS (MQCT_SOURCE_CODES/pot_comp.f:4695-6274; replaces the R-grid
  * loop of :5174-5765 and EXPANSION_TERM, :3739-3896), SYS_TYPE 1, 3, 4, 7, 8, 9 and 0: the

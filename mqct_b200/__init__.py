@@ -956,6 +956,107 @@ def differential_cross_section(p_elastic, phase, j_ini, J_down, J_up, L_min, k_v
     return theta, dcs * A_BOHR ** 2, sig * A_BOHR ** 2
 
 
+def _clamped_spline(x, y):
+    """Second derivatives of the cubic spline through (x, y) with the end slopes of the
+    first and last chords (the tridiagonal recurrence of Numerical Recipes' `spline`, as
+    the reference calls it with finite-difference end slopes)."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    n = len(x)
+    yp1 = (y[1] - y[0]) / (x[1] - x[0])
+    ypn = (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2])
+    y2, u = np.zeros(n), np.zeros(n)
+    y2[0] = -0.5
+    u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1)
+    for i in range(1, n - 1):
+        sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1])
+        p = sig * y2[i - 1] + 2.0
+        y2[i] = (sig - 1.0) / p
+        u[i] = (6.0 * ((y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]))
+                / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p
+    un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]))
+    y2[n - 1] = (un - 0.5 * u[n - 2]) / (0.5 * y2[n - 2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[k] = y2[k] * y2[k + 1] + u[k]
+    return y2
+
+
+def _splint(x, y, y2, v):
+    """The spline at v (bisection for the interval; outside the knots the end interval's
+    cubic)."""
+    klo, khi = 0, len(x) - 1
+    while khi - klo > 1:
+        k = (khi + klo) // 2
+        if x[k] > v:
+            khi = k
+        else:
+            klo = k
+    h = x[khi] - x[klo]
+    a, b = (x[khi] - v) / h, (v - x[klo]) / h
+    return a * y[klo] + b * y[khi] + ((a ** 3 - a) * y2[klo] + (b ** 3 - b) * y2[khi]) * h * h / 6.0
+
+
+def cross_sections_spline(prob, l_traj, j_ini, J_down, J_up, k_vec):
+    """INELAST_CALC with PROB_SPLINE = YES (MQCT_SOURCE_CODES/propagator.f:4889-4975): the
+    channel probabilities of the trajectories (run at l_traj, e.g. every DL-th l) are
+    splined over l (clamped, chord end slopes) and the J sums take the spline at every
+    integer l: sigma_f = pi/k^2 sum_J sum_{l=|J-j|}^{J+j} (2J+1)/(2j+1) P_f(l), Angstrom^2."""
+    prob = np.asarray(prob, dtype=np.float64)
+    lt = np.asarray(l_traj, dtype=np.float64)
+    sig = np.zeros(prob.shape[1])
+    for c in range(prob.shape[1]):
+        y2 = _clamped_spline(lt, prob[:, c])
+        for J in range(J_down, J_up + 1):
+            for lv in range(abs(J - j_ini), J + j_ini + 1):
+                sig[c] += (_splint(lt, prob[:, c], y2, float(lv)) * (2.0 * J + 1.0) / k_vec ** 2
+                           / (2.0 * j_ini + 1) * np.pi)
+    return sig * A_BOHR ** 2
+
+
+def elastic_cross_section_spline(l_traj, p_elastic, deflection, L_min, L_max, k_vec):
+    """ELAST_CALC with PROB_SPLINE = YES (MQCT_SOURCE_CODES/propagator.f:5960-6060): the
+    deflection function and log10 of the elastic probability (floored at 1e-30) of the
+    trajectories at l_traj are splined over l; the phases run backwards on the integer
+    grid, phase(L_max) = 0, phase(l) = phase(l + 1) - (chi(l) + chi(l + 1)) / 2, and
+    sigma_el = pi/k^2 sum_{l=L_min}^{L_max-1} |1 - sqrt(P_el(l)) e^{i phase(l)}|^2 (2l + 1).
+    Returns (sigma_el in Angstrom^2, phases at l = L_min..L_max)."""
+    lt = np.asarray(l_traj, dtype=np.float64)
+    chi = np.asarray(deflection, dtype=np.float64)
+    lp = np.log10(np.maximum(np.asarray(p_elastic, dtype=np.float64), 1e-30))
+    y2c, y2p = _clamped_spline(lt, chi), _clamped_spline(lt, lp)
+    ph = np.zeros(L_max - L_min + 1)
+    s = 0.0
+    for lv in range(L_max - 1, L_min - 1, -1):
+        c1 = _splint(lt, chi, y2c, float(lv))
+        c2 = _splint(lt, chi, y2c, float(lv + 1))
+        i = lv - L_min
+        ph[i] = ph[i + 1] - (c1 + c2) / 2.0
+        p = 10.0 ** _splint(lt, lp, y2p, float(lv))
+        s += abs(1.0 - np.sqrt(p) * np.exp(1j * ph[i])) ** 2 / k_vec ** 2 * np.pi * (2.0 * lv + 1)
+    return s * A_BOHR ** 2, ph
+
+
+def splined_opacity(l_traj, prob, deflection, L_min, L_max, log_space=True):
+    """The deflection function and channel probabilities splined to every integer l from
+    L_min to L_max, as SPLINED_DEFLECTION_OPACITY_L.out lists them
+    (MQCT_SOURCE_CODES/propagator.f:6080-6110): probabilities splined in log10 space
+    (floored at 1e-30) as the reference does now, or linearly (log_space=False) as its
+    earlier INTERPOLATED_PROBS_DEFLECTION_L.out did.  Returns (l, chi, prob [n_l, n_ch])."""
+    lt = np.asarray(l_traj, dtype=np.float64)
+    prob = np.asarray(prob, dtype=np.float64)
+    chi = np.asarray(deflection, dtype=np.float64)
+    ls = np.arange(L_min, L_max + 1)
+    y2c = _clamped_spline(lt, chi)
+    out_chi = np.array([_splint(lt, chi, y2c, float(v)) for v in ls])
+    out_p = np.zeros((len(ls), prob.shape[1]))
+    for c in range(prob.shape[1]):
+        y = np.log10(np.maximum(prob[:, c], 1e-30)) if log_space else prob[:, c]
+        y2 = _clamped_spline(lt, y)
+        v = np.array([_splint(lt, y, y2, float(q)) for q in ls])
+        out_p[:, c] = 10.0 ** v if log_space else v
+    return ls, out_chi, out_p
+
+
 def cross_sections_device(d_amp, system: CollisionSystem, j_ini, J_down, J_up, L_min, k_vec,
                           dl=1):
     """INELAST_CALC on the GPU from device amplitudes (a CUDA float64 torch tensor, n_traj x
@@ -1171,6 +1272,16 @@ def write_diff_cross(path, i_ener, s_st, j12, m12, theta, dcs):
     th = np.ascontiguousarray(theta, np.float64)
     check(lib().mqct_write_diff_cross(path.encode(), int(i_ener), int(s_st), int(j12), int(m12),
                                       len(th), th, np.ascontiguousarray(dcs, np.float64)))
+
+
+def write_splined_opacity(path, l, k_vec, deflection, prob):
+    """Append the SPLINED_DEFLECTION_OPACITY_L.out table (per integer l: l / k, l, the splined
+    deflection function, the splined channel probabilities prob [n_l, n_channels])."""
+    li = np.ascontiguousarray(l, np.int32)
+    prob = np.ascontiguousarray(prob, np.float64)
+    check(lib().mqct_write_splined_opacity(path.encode(), len(li), li, float(k_vec),
+                                           np.ascontiguousarray(deflection, np.float64),
+                                           prob.shape[1], prob.reshape(-1)))
 
 
 def write_partial_j(path, s_st, j12, m12, i_ener, U_cm, J, partial):

@@ -107,7 +107,7 @@ EXPORTS = [
     "mqct_projection_plan_create", "mqct_projection_plan_execute", "mqct_projection_plan_sync",
     "mqct_projection_plan_timing", "mqct_projection_plan_destroy", "mqct_project_terms",
     "mqct_write_opacity", "mqct_write_partial_j", "mqct_write_m_proj",
-    "mqct_write_deflection", "mqct_write_diff_cross",
+    "mqct_write_deflection", "mqct_write_diff_cross", "mqct_write_splined_opacity",
     "mqct_write_cross_sections", "mqct_write_cross_sections_footer",
 ]
 
@@ -243,6 +243,8 @@ def lib():
     L.mqct_write_deflection.argtypes = [C.c_char_p] + [C.c_int32] * 4 + [
         C.c_double, C.c_int32, i32p, C.c_double] + [f64p] * 5 + [i32p, i32p]
     L.mqct_write_diff_cross.argtypes = [C.c_char_p] + [C.c_int32] * 5 + [f64p, f64p]
+    L.mqct_write_splined_opacity.argtypes = [C.c_char_p, C.c_int32, i32p, C.c_double, f64p,
+                                             C.c_int32, f64p]
     L.mqct_write_cross_sections.argtypes = [C.c_char_p, C.c_double, C.c_int32, C.c_int32, vp,
                                             f64p, f64p, C.c_double, C.c_int32, C.c_double]
     L.mqct_write_cross_sections_footer.argtypes = [C.c_char_p, C.c_int32]

@@ -901,6 +901,30 @@ int mqct_write_diff_cross(const char* path, int32_t i_ener, int32_t s_st, int32_
   return close_checked(f, path);
 }
 
+// SPLINED_DEFLECTION_OPACITY_L.out (ELAST_CALC with PROB_SPLINE, propagator.f:6063-6110):
+// per integer l the impact parameter l / k, l, the splined deflection function and the
+// splined channel probabilities.
+int mqct_write_splined_opacity(const char* path, int32_t n_l, const int32_t* l, double k_vec,
+                               const double* deflection, int32_t n_ch, const double* prob) {
+  MQCT_ARG_CHECK(path && l && deflection && prob && n_l > 0 && n_ch > 0 && k_vec > 0.0,
+                 "bad arguments");
+  FILE* f = open_append(path);
+  if (!f) return MQCT_E_IO;
+  for (int c = 1; c <= n_ch; ++c) {
+    if (c == 1) fprintf(f, "%-8s       %-7s     %-12s  ", "B_IMPACT", "     L ", "DEF_FUNCTION");
+    fprintf(f, "CHANNEL=%6d  ", c);
+  }
+  fprintf(f, "\n");
+  for (int i = 0; i < n_l; ++i) {
+    fprintf(f, "%s %6d %12.4f     ", fortran_e(l[i] / k_vec, 15, 8).c_str(), l[i], deflection[i]);
+    for (int c = 0; c < n_ch; ++c)
+      fprintf(f, "%s ", fortran_e(prob[(size_t)i * n_ch + c], 15, 8).c_str());
+    fprintf(f, "\n");
+  }
+  fprintf(f, " \n");
+  return close_checked(f, path);
+}
+
 // PARTIAL_CROSS_SECTIONS_J.out (propagator.f:4845-4868): per total J the J-resolved
 // cross sections of every channel, Angstrom^2.
 int mqct_write_partial_j(const char* path, int32_t s_st, int32_t j12, int32_t m12,

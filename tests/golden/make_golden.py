@@ -205,6 +205,24 @@ def main(ref_root):
                         mass_red=3.354120939, U=800.0, n_angles=2000, j_ini=0, J_down=0,
                         J_up=100, L_min=0, dl=1)
 
+    # G9: PROB_SPLINE = YES with DL = 3 (CO + H2, SYS_TYPE 6, U = 1000 cm^-1, 47
+    # trajectories at l = 1, 4, ..., 139, j_ini = 0): probabilities and deflection function
+    # splined over l in INELAST_CALC and ELAST_CALC (propagator.f:4889-4975, 5960-6110).
+    d = os.path.join(ex, "SYS_TYPE_6", "CO_H2_Prob_spline")
+    opac9 = _read_table(os.path.join(d, "OPACITY_FUNCTIONS_L.out"), 6)
+    defl9 = _read_table(os.path.join(d, "DEFLECTION_FUNCTION.out"), 9, first_int=False)
+    sig9 = []
+    for line in open(os.path.join(d, "CROSS_SECTIONS.out")):
+        t = line.split()
+        if len(t) == 5 and t[0].isdigit():
+            sig9.append(float(t[2]))
+    np.savez_compressed(os.path.join(out, "g9_prob_spline.npz"), opacity=opac9, deflection=defl9,
+                        sigma_U=np.array(sig9),
+                        text_interpolated=np.array(open(os.path.join(
+                            d, "INTERPOLATED_PROBS_DEFLECTION_L.out")).read()),
+                        # $SYSTEM of CO_H2_Prob_spline.inp; l = 0 .. int(B_IMPCT k)
+                        mass_red=1.88027, U=1000.0, dl=3, L_min=0, L_max=139)
+
     # G1 AT trajectory record layout: Fortran unformatted, 8 float64 per record.
     d = os.path.join(ex, "SYS_TYPE_0", "H2O_H2O_AT_Approximation", "AT_MQCT_2nd_Step",
                      "AT_APPROX_TRAJS", "500.00000", "0", "0")

@@ -97,3 +97,45 @@ def test_deflection_angles_from_final_states(mq, oracle):
                           float(g["rmax"]), max_steps=1) for l in range(len(trajs))]
     chi = mq.deflection_angles(cls, init, float(g["mass_red"]) * 1822.8885)
     assert np.max(np.abs(chi - g["deflection"][:, 2])) < 2e-7
+
+
+def test_probability_spline_cross_sections_co_h2(mq, tmp_path):
+    """PROB_SPLINE = YES with DL = 3 (CO + H2, fixture g9_prob_spline.npz, EXAMPLES_IO/
+    SYS_TYPE_6/CO_H2_Prob_spline): inelastic cross sections from the probabilities splined
+    over l (1e-7 relative of the printed ones), the elastic cross section from the splined
+    deflection function and elastic probability (1e-7), and the splined table of
+    INTERPOLATED_PROBS_DEFLECTION_L.out (the reference's earlier name of
+    SPLINED_DEFLECTION_OPACITY_L.out, probabilities splined linearly there) byte for byte."""
+    g = np.load(os.path.join(GOLD, "g9_prob_spline.npz"))
+    op, d = g["opacity"], g["deflection"]
+    lt = op[:, 1]
+    assert np.array_equal(lt, np.arange(1, 140, 3)) and np.array_equal(lt, d[:, 0])
+    k = _k(float(g["U"]), float(g["mass_red"]))
+    L_min, L_max = int(g["L_min"]), int(g["L_max"])
+    sig = mq.cross_sections_spline(op[:, 2:], lt, 0, L_min, L_max, k)
+    assert np.allclose(sig[1:], g["sigma_U"][1:], rtol=1e-7, atol=0)
+    sig_el, ph = mq.elastic_cross_section_spline(lt, op[:, 2], d[:, 2], L_min, L_max, k)
+    assert ph[-1] == 0.0 and len(ph) == L_max - L_min + 1
+    assert abs(sig_el / g["sigma_U"][0] - 1) < 1e-7        # 0.3243445614E+03 A^2
+    ls, chi, p = mq.splined_opacity(lt, op[:, 2:], d[:, 2], L_min, L_max, log_space=False)
+    ref = str(g["text_interpolated"])
+    rows = np.array([[float(x) for x in ln.split()] for ln in ref.split("\n")[1:]
+                     if len(ln.split()) == 7])
+    assert np.array_equal(rows[:, 1], ls)
+    assert np.max(np.abs(chi - rows[:, 2])) < 5.01e-5        # printed with 4 decimals
+    # the elastic column to the inputs' 8 digits; the inelastic ones fall by decades between
+    # knots, and a value splined between two of them keeps fewer of the inputs' digits
+    assert np.max(np.abs(p[:, 0] - rows[:, 3]) / rows[:, 3]) < 2e-8
+    assert np.max(np.abs(p - rows[:, 3:]) / rows[:, 3:]) < 5e-6
+    path = tmp_path / "SPLINED_DEFLECTION_OPACITY_L.out"
+    mq.write_splined_opacity(str(path), ls, k, rows[:, 2], rows[:, 3:])
+    got_l, ref_l = path.read_text().split("\n"), ref.split("\n")
+    assert len(got_l) == len(ref_l) and got_l[0] == ref_l[0]
+    for a, b in zip(got_l[1:], ref_l[1:]):       # l / k recomputed: within its last digit
+        if a != b:
+            assert a[15:] == b[15:]
+            assert abs(float(a[:15]) - float(b[:15])) <= 1.01e-8 * max(1.0, abs(float(b[:15])))
+    # log-space splines (the reference's present ELAST_CALC) give the same probabilities
+    # to the printed digits where they are not tiny
+    _, _, plog = mq.splined_opacity(lt, op[:, 2:], d[:, 2], L_min, L_max)
+    assert np.max(np.abs(plog[:, 0] - rows[:, 3])) < 1e-7
