@@ -141,3 +141,24 @@ def test_asym_top_system_matches_per_trajectory_kernel(mq, gpu_available, c2_tab
     assert e8 == mq.ENGINE_RESIDENT and sh8[0] == 8
     p8 = mq.channel_probabilities(a8, s.indx_chann, s.n_channels)
     assert np.max(np.abs(p8 - p_rs)) < 5e-5
+
+
+def test_start_beyond_the_grid(mq, oracle, gpu_available, g3):
+    """Trajectories that start outside the R grid (the matrix is zero above R_max: no knot
+    rows, y = 0) enter it and leave again: the resident engine against the oracle (FP64)
+    and the FP32 per-trajectory kernel."""
+    R = g3["tab"].R
+    r0 = float(R[-1]) + 4.0
+    base = g3["trajs"][::9][:12]
+    trajs = [mq.Trajectory(t.e_coll, t.l_real, t.s_st, t.dt, r0, r0, time_lim=t.time_lim)
+             for t in base]
+    amp, cls, diag, eng, _ = _run(mq, g3["tab"], trajs, mq.PROP_FP32, mq.ENGINE_RESIDENT)
+    assert eng == mq.ENGINE_RESIDENT
+    a2, c2, d2, _, _ = _run(mq, g3["tab"], trajs, mq.PROP_FP32, mq.ENGINE_PER_TRAJECTORY)
+    oamp, ocls, odiag = _oracle_run(oracle, g3["otab"], trajs)
+    idx = g3["s"].indx_chann
+    p = mq.channel_probabilities(amp, idx, 10)
+    assert np.max(np.abs(p - mq.channel_probabilities(oamp, idx, 10))) < 2e-4
+    assert np.max(np.abs(p - mq.channel_probabilities(a2, idx, 10))) < 5e-5
+    assert np.array_equal(diag[:, 4], odiag[:, 4])
+    assert np.allclose(diag[:, 1], odiag[:, 1], rtol=1e-3)
