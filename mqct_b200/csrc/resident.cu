@@ -77,7 +77,9 @@ struct RsRow {
   int ri;        // reference state index (output order)
   int nbp, nbm;  // J_+ / J_- neighbour as rank << 16 | local row, or -1
   int ent_i;     // block entry of the CTA << 8 | row inside the block
-  double cp, cm; // their coefficients
+  int to_p, to_m;  // the row whose J_+ / J_- neighbour this row is (rank << 16 | local row),
+                   // or -1: where this row's stage inputs are pushed
+  double cp, cm; // the coefficients of nbp and nbm
 };
 
 struct RsDev {
@@ -100,7 +102,8 @@ struct RsDev {
 
 // Dynamic shared memory of one CTA (offsets in bytes, 16-byte aligned).
 struct RsSmem {
-  size_t kn0, kn1, mp, loc, y64, acc, ain0, ain1, bt, u, ph0, ph1, rows, rg, ih, ev, total;
+  size_t kn0, kn1, mp, loc, y64, acc, ain0, ain1, halo0, halo1, bt, u, ph0, ph1, rows, rg, ih,
+      ev, total;
 };
 __host__ __device__ inline RsSmem rs_layout(int ns_cap, int nr_cap, int n_e, int nR) {
   RsSmem s{};
@@ -118,6 +121,8 @@ __host__ __device__ inline RsSmem rs_layout(int ns_cap, int nr_cap, int n_e, int
   s.acc = take((size_t)nr_cap * 8);
   s.ain0 = take((size_t)nr_cap * 8);
   s.ain1 = take((size_t)nr_cap * 8);
+  s.halo0 = take((size_t)nr_cap * 16);
+  s.halo1 = take((size_t)nr_cap * 16);
   s.bt = take((size_t)nr_cap * 8);
   s.u = take((size_t)nr_cap * 8);
   s.ph0 = take((size_t)n_e * 8);
@@ -130,8 +135,8 @@ __host__ __device__ inline RsSmem rs_layout(int ns_cap, int nr_cap, int n_e, int
   return s;
 }
 
-// Block-wide sums of three doubles (fixed order), broadcast to all threads.
-__device__ inline void rs_sum3(double& a, double& b, double& c, double* red) {
+// Warp sums of three doubles (fixed tree) into red[3 w + q]; the block's barrier follows.
+__device__ inline void rs_warp_parts(double a, double b, double c, double* red) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -145,21 +150,6 @@ __device__ inline void rs_sum3(double& a, double& b, double& c, double* red) {
     red[3 * w + 2] = c;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double sa = 0.0, sb = 0.0, sc = 0.0;
-    for (int i = 0; i < RS_WARPS; ++i) {
-      sa += red[3 * i];
-      sb += red[3 * i + 1];
-      sc += red[3 * i + 2];
-    }
-    red[3 * RS_WARPS] = sa;
-    red[3 * RS_WARPS + 1] = sb;
-    red[3 * RS_WARPS + 2] = sc;
-  }
-  __syncthreads();
-  a = red[3 * RS_WARPS];
-  b = red[3 * RS_WARPS + 1];
-  c = red[3 * RS_WARPS + 2];
 }
 
 // Start of a trajectory (thread 0): MQCT_SOURCE_CODES/propagator.f:2531-2566.  Returns
@@ -416,6 +406,7 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
   double2* Y = reinterpret_cast<double2*>(rs_sm + L.y64);
   float2* ACC = reinterpret_cast<float2*>(rs_sm + L.acc);
   float2* AIN[2] = {reinterpret_cast<float2*>(rs_sm + L.ain0), reinterpret_cast<float2*>(rs_sm + L.ain1)};
+  float4* HALO[2] = {reinterpret_cast<float4*>(rs_sm + L.halo0), reinterpret_cast<float4*>(rs_sm + L.halo1)};
   float2* bt = reinterpret_cast<float2*>(rs_sm + L.bt);
   float2* uv = reinterpret_cast<float2*>(rs_sm + L.u);
   float2* PH[2] = {reinterpret_cast<float2*>(rs_sm + L.ph0), reinterpret_cast<float2*>(rs_sm + L.ph1)};
@@ -429,6 +420,21 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
   __shared__ double part[2][RS_MAX_CL][3];
   __shared__ int s_tr, s_ec;
   __shared__ int s_n[RS_MAX_BLK], s_ls0[RS_MAX_BLK], s_lr0[RS_MAX_BLK], s_q0[RS_MAX_BLK];
+  // a row's new stage input into the Coriolis neighbour slots (J_+ in .xy, J_- in .zw of
+  // halo) of the rows that need it, in whichever CTA holds them: remote stores before the
+  // cluster barrier, so that the next evaluation reads its neighbours locally
+  auto push = [&](const RsRow& w, float2 v, float4* halo) {
+    if (w.to_p >= 0) {
+      const int r = w.to_p >> 16, l = w.to_p & 0xffff;
+      float4* h = r == rank ? halo : clu.map_shared_rank(halo, r);
+      reinterpret_cast<float2*>(h + l)[0] = v;
+    }
+    if (w.to_m >= 0) {
+      const int r = w.to_m >> 16, l = w.to_m & 0xffff;
+      float4* h = r == rank ? halo : clu.map_shared_rank(halo, r);
+      reinterpret_cast<float2*>(h + l)[1] = v;
+    }
+  };
   const int e0 = D.rk_b0[rank], nbk = D.rk_b0[rank + 1] - e0;
   const int nr = D.rk_rows[rank], nsl_r = D.rk_slots[rank];
   for (int e = tid; e < nbk; e += RS_THREADS) {
@@ -479,6 +485,7 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
         const double one = w.gi == S.s_int ? 1.0 : 0.0;
         Y[lr] = make_double2(one, 0.0);
         a0[lr] = make_float2((float)one, 0.f);
+        push(w, a0[lr], HALO[rc & 1]);
         if (!go) {  // not propagated: the initial unit vector is the result
           amp[w.ri] = one;
           amp[d.N + w.ri] = 0.0;
@@ -506,26 +513,24 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
         }
       }
       // bt = D^* a and u = (J_+ + J_-) a of this CTA's rows (MQCT_SOURCE_CODES/
-      // mqct_eqtns.f:447-464); a neighbour held by another CTA is read from its memory
+      // mqct_eqtns.f:447-464); the neighbours' stage inputs were pushed into halo
       const float2* ph = PH[par];
-      float2* ain = AIN[par];
+      const float2* ain = AIN[par];
+      const float4* halo = HALO[par];
       for (int lr = tid; lr < nr; lr += RS_THREADS) {
         const RsRow w = row[lr];
         const float2 a = ain[lr];
         const float2 p = ph[w.ec];
         bt[lr] = make_float2(p.x * a.x - p.y * a.y, p.x * a.y + p.y * a.x);
+        const float4 hv = halo[lr];
         double ur = 0.0, ui = 0.0;
         if (w.nbp >= 0) {
-          const int r = w.nbp >> 16, l = w.nbp & 0xffff;
-          const float2 an = r == rank ? ain[l] : clu.map_shared_rank(ain, r)[l];
-          ur += w.cp * (double)an.x;
-          ui += w.cp * (double)an.y;
+          ur += w.cp * (double)hv.x;
+          ui += w.cp * (double)hv.y;
         }
         if (w.nbm >= 0) {
-          const int r = w.nbm >> 16, l = w.nbm & 0xffff;
-          const float2 an = r == rank ? ain[l] : clu.map_shared_rank(ain, r)[l];
-          ur += w.cm * (double)an.x;
-          ui += w.cm * (double)an.y;
+          ur += w.cm * (double)hv.z;
+          ui += w.cm * (double)hv.w;
         }
         uv[lr] = make_float2((float)ur, (float)ui);
       }
@@ -616,38 +621,41 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
           const double ci = zi + 0.5 * dphidt * (double)uu.y;
           const double dar = ci, dai = -cr;
           const double2 yo = Y[lr];
+          float2 nx;
           if (s == 0) {
             ACC[lr] = make_float2((float)dar, (float)dai);
-            aout[lr] = make_float2((float)(yo.x + 0.5 * dt * dar), (float)(yo.y + 0.5 * dt * dai));
+            nx = make_float2((float)(yo.x + 0.5 * dt * dar), (float)(yo.y + 0.5 * dt * dai));
           } else if (s < 3) {
             const float2 a0 = ACC[lr];
             ACC[lr] = make_float2((float)((double)a0.x + 2.0 * dar), (float)((double)a0.y + 2.0 * dai));
             const double c = s == 1 ? 0.5 * dt : dt;
-            aout[lr] = make_float2((float)(yo.x + c * dar), (float)(yo.y + c * dai));
+            nx = make_float2((float)(yo.x + c * dar), (float)(yo.y + c * dai));
           } else {
             const float2 a0 = ACC[lr];
             const double h6 = dt / 6.0;
             const double2 yn = make_double2(yo.x + h6 * ((double)a0.x + dar),
                                             yo.y + h6 * ((double)a0.y + dai));
             Y[lr] = yn;
-            aout[lr] = make_float2((float)yn.x, (float)yn.y);
+            nx = make_float2((float)yn.x, (float)yn.y);
           }
+          aout[lr] = nx;
+          push(w, nx, HALO[par ^ 1]);
         }
         if (s == 4) {
           f = fe;
           g = nn;
         }
       }
-      rs_sum3(f, g, pt, red);
-      // this CTA's parts into every CTA of the cluster; the cluster barrier (release /
-      // acquire: the parts and the stage-input amplitudes written above are visible after
-      // it) is split so that the next right-hand side's phases, whose time is known before
-      // the classical step, are formed while the other CTAs arrive
-      if (tid < D.CL) {
-        double* dst = clu.map_shared_rank(&part[par][rank][0], tid);
-        dst[0] = f;
-        dst[1] = g;
-        dst[2] = pt;
+      // this CTA's parts (warp sums, then the warps in order by one thread per quantity) into
+      // every CTA of the cluster; the cluster barrier (release / acquire: the parts and the
+      // stage inputs pushed above are visible after it) is split so that the next right-hand
+      // side's phases, whose time is known before the classical step, are formed while the
+      // other CTAs arrive
+      rs_warp_parts(f, g, pt, red);
+      if (tid < 3) {
+        double v = 0.0;
+        for (int i = 0; i < RS_WARPS; ++i) v += red[3 * i + tid];
+        for (int r = 0; r < D.CL; ++r) *clu.map_shared_rank(&part[par][rank][tid], r) = v;
       }
       rs_arrive();
       if (s != 4) rs_phases(PH[par ^ 1], ev, D.n_e, s < 2 ? S.tcur + 0.5 * S.dt : S.tcur + S.dt);
@@ -818,6 +826,19 @@ static int rs_prepare(RsEngine* e, const PropDev& d, const std::vector<int>& blk
     nslots[r] = so;
     b0[r + 1] = (int)blk.size();
   }
+  // per state: the row whose J_+ (J_-) neighbour it is, where its stage inputs are pushed
+  // (each state is the J_+ and the J_- neighbour of at most one state)
+  std::vector<int> to_p(N, -1), to_m(N, -1);
+  for (int gi = 0; gi < N; ++gi) {
+    if (nbp[gi] >= 0) {
+      if (to_p[nbp[gi]] >= 0) return MQCT_OK;  // a second consumer: the engine does not apply
+      to_p[nbp[gi]] = owner[gi];
+    }
+    if (nbm[gi] >= 0) {
+      if (to_m[nbm[gi]] >= 0) return MQCT_OK;
+      to_m[nbm[gi]] = owner[gi];
+    }
+  }
   for (int r = 0; r < CL; ++r)
     for (int lr = 0; lr < rows[r]; ++lr) {
       RsRow& w = rtab[(size_t)r * sp.nr_cap + lr];
@@ -826,6 +847,8 @@ static int rs_prepare(RsEngine* e, const PropDev& d, const std::vector<int>& blk
       w.ri = perm[gi];
       w.nbp = nbp[gi] >= 0 ? owner[nbp[gi]] : -1;
       w.nbm = nbm[gi] >= 0 ? owner[nbm[gi]] : -1;
+      w.to_p = to_p[gi];
+      w.to_m = to_m[gi];
       w.cp = cp[gi];
       w.cm = cm[gi];
     }
