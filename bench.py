@@ -413,10 +413,15 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
     props = torch.cuda.get_device_properties(0)
     fp32_peak = props.multi_processor_count * 128 * 2 * _peaks()[0].get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     probs = {}
-    runs = (("fp32", mq.PROP_FP32, mq.ENGINE_LOCKSTEP),
+    # fp32: the plan's own choice (for 4 096 trajectories the lockstep engine with its last
+    # trajectories handed to the resident engine); the engines alone beside it
+    runs = (("fp32", mq.PROP_FP32, mq.ENGINE_AUTO),
+            ("fp32_lockstep", mq.PROP_FP32, mq.ENGINE_LOCKSTEP),
             ("fp32_per_trajectory", mq.PROP_FP32, mq.ENGINE_PER_TRAJECTORY),
-            ("fp64", mq.PROP_FP64, mq.ENGINE_PER_TRAJECTORY),
-            ("fp64_lockstep", mq.PROP_FP64, mq.ENGINE_LOCKSTEP))
+            ("fp64", mq.PROP_FP64, mq.ENGINE_PER_TRAJECTORY))
+    names = {mq.ENGINE_LOCKSTEP: "lockstep", mq.ENGINE_PER_TRAJECTORY: "per-trajectory",
+             mq.ENGINE_RESIDENT: "resident",
+             mq.ENGINE_LOCKSTEP_TAIL: "lockstep, last trajectories on the resident engine"}
     for name, arith, engine in runs:
         nt = n
         plan = mq.PropagationPlan(tab, arith)
@@ -432,9 +437,11 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
         eng, rounds = plan.engine()
         r = {"n_traj": nt, "kernel_ms": ms, "wall_s": wall,
              "traj_per_s": world * nt / (ms / 1e3), "traj_steps": steps,
-             "engine": {mq.ENGINE_LOCKSTEP: "lockstep", mq.ENGINE_PER_TRAJECTORY: "per-trajectory"}[eng],
+             "engine": names[eng],
              "max_status": float(diag[:, 4].max())}
-        if eng == mq.ENGINE_LOCKSTEP:
+        if eng == mq.ENGINE_LOCKSTEP_TAIL:
+            r["handed_to_resident"] = plan.handed()
+        if eng in (mq.ENGINE_LOCKSTEP, mq.ENGINE_LOCKSTEP_TAIL):
             r["rounds"] = rounds
             r["rhs_flops_per_step"] = flops_per_step
             r["achieved_tflops"] = steps * flops_per_step / (ms / 1e3) / 1e12
@@ -452,9 +459,9 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
     p32, p64 = probs["fp32"], probs["fp64"]
     res["max_abs_prob_diff_fp32_vs_fp64"] = float(np.abs(p32 - p64).max())
     res["max_abs_prob_diff_engines_fp32"] = float(np.abs(p32 - probs["fp32_per_trajectory"]).max())
-    res["max_abs_prob_diff_engines_fp64"] = float(np.abs(p64 - probs["fp64_lockstep"]).max())
+    res["max_abs_prob_diff_fp32_vs_fp32_lockstep"] = float(np.abs(p32 - probs["fp32_lockstep"]).max())
     # opacity-weighted sums sum_traj (2l+1) P_f (cross sections up to a common factor) of
-    # the FP32 lockstep run and the FP64 form over the same trajectories
+    # the FP32 run (the plan's choice) and the FP64 form over the same trajectories
     w = 2 * l[:n] + 1
     s32, s64 = (w[:, None] * p32).sum(0), (w[:, None] * p64).sum(0)
     keep = s64 > 1e-4 * s64[1:].max()
@@ -462,10 +469,10 @@ def run_propagation(mq, syn, s, R, mat, a, torch, world, dist=None, mat64=None):
     res["sigma_rel_diff_fp32_vs_fp64"] = {
         "channels": int(keep.sum()),
         "max": float(np.max(np.abs(s32[keep] - s64[keep]) / s64[keep]))}
-    res["speedup_fp32_lockstep_vs_fp32_per_trajectory"] = (res["fp32"]["traj_per_s"] /
-                                                           res["fp32_per_trajectory"]["traj_per_s"])
-    res["speedup_fp64_lockstep_vs_fp64_form"] = (res["fp64_lockstep"]["traj_per_s"] /
-                                                 res["fp64"]["traj_per_s"])
+    res["speedup_fp32_vs_fp32_per_trajectory"] = (res["fp32"]["traj_per_s"] /
+                                                  res["fp32_per_trajectory"]["traj_per_s"])
+    res["speedup_fp32_vs_fp32_lockstep"] = (res["fp32"]["traj_per_s"] /
+                                            res["fp32_lockstep"]["traj_per_s"])
     res["speedup_fp32_vs_fp64_form"] = res["fp32"]["traj_per_s"] / res["fp64"]["traj_per_s"]
     # the coupled-states approximation (CS_APPROX) on the same trajectories: only the
     # m-block of the initial state is streamed and propagated

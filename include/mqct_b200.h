@@ -477,7 +477,12 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
  * runs (mqct_prop_plan_run_device) read the initial conditions back for the bound on the
  * rounds and return when the batch is done.  MQCT_ENGINE_AUTO (default): the lockstep
  * engine for eligible batches of at least 4096 trajectories, the resident engine (below)
- * for eligible FP32 batches of at most 1024.  MQCT_ENGINE_RESIDENT: one
+ * for eligible FP32 batches of at most 1024, and for eligible FP32 batches of at least 4096
+ * MQCT_ENGINE_LOCKSTEP_TAIL: the lockstep engine until at most six trajectories per
+ * resident cluster still run, then the resident engine, which continues each of them from
+ * the start of its RK4 step (mqct_prop_plan_handed reports how many the last run handed
+ * over; FP64 plans and tables the resident engine does not take run the plain lockstep
+ * engine).  MQCT_ENGINE_RESIDENT: one
  * thread-block cluster per trajectory, the m-blocks split between its CTAs, each holding
  * the two knot rows of its blocks in shared memory (reloaded when the stage point leaves
  * the spline interval); the CTAs exchange their parts of the quadratic forms and the
@@ -494,6 +499,7 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
 #define MQCT_ENGINE_PER_TRAJECTORY 1
 #define MQCT_ENGINE_LOCKSTEP 2
 #define MQCT_ENGINE_RESIDENT 3
+#define MQCT_ENGINE_LOCKSTEP_TAIL 4
 int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine);
 int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* rounds);
 /* Cluster size of the resident engine: 0 (default) eight CTAs for a batch that the
@@ -503,6 +509,7 @@ int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* 
  * when it took the resident engine, else those of the setting (0 meaning the smallest
  * size) for the plan's tables; both 0 when the engine does not apply to the plan. */
 int mqct_prop_plan_set_cluster(mqct_prop_plan* plan, int32_t ctas);
+int mqct_prop_plan_handed(const mqct_prop_plan* plan, int32_t* n);
 int mqct_prop_plan_cluster(mqct_prop_plan* plan, int32_t* ctas, int32_t* clusters);
 
 /* Host-side helpers mirroring INI_ARRAYS / EIGEN_VEC / the R grid. */

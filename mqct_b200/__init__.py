@@ -19,8 +19,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (ENGINE_AUTO, ENGINE_LOCKSTEP, ENGINE_PER_TRAJECTORY, ENGINE_RESIDENT, MODE_AT,
-                   MODE_CS, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64,
+from ._abi import (ENGINE_AUTO, ENGINE_LOCKSTEP, ENGINE_LOCKSTEP_TAIL, ENGINE_PER_TRAJECTORY,
+                   ENGINE_RESIDENT, MODE_AT, MODE_CS, MODE_STD, PREC_BF16X3, PREC_F16X3, PREC_FP64, PROP_FP32, PROP_FP64,
                    MqctError, check, lib, ptr)
 from .synthetic import A_BOHR, AMU_TO_AU, AU_TO_EV, CM_TO_HARTREE, EV_TO_WN
 
@@ -770,8 +770,8 @@ class PropagationPlan:
         check(lib().mqct_prop_plan_set_coupled_states(self.h, 1 if cs else 0))
 
     def set_engine(self, engine=ENGINE_AUTO):
-        """ENGINE_AUTO, ENGINE_PER_TRAJECTORY, ENGINE_LOCKSTEP or ENGINE_RESIDENT for the
-        following runs (mqct_prop_plan_set_engine)."""
+        """ENGINE_AUTO, ENGINE_PER_TRAJECTORY, ENGINE_LOCKSTEP, ENGINE_RESIDENT or
+        ENGINE_LOCKSTEP_TAIL for the following runs (mqct_prop_plan_set_engine)."""
         check(lib().mqct_prop_plan_set_engine(self.h, int(engine)))
 
     def set_cluster(self, ctas=0):
@@ -785,6 +785,13 @@ class PropagationPlan:
         a, b = C.c_int32(), C.c_int32()
         check(lib().mqct_prop_plan_cluster(self.h, C.byref(a), C.byref(b)))
         return int(a.value), int(b.value)
+
+    def handed(self):
+        """Trajectories the last lockstep run handed to the resident engine
+        (mqct_prop_plan_handed)."""
+        n = C.c_int32()
+        check(lib().mqct_prop_plan_handed(self.h, C.byref(n)))
+        return int(n.value)
 
     def engine(self):
         """(engine of the last run, lockstep rounds of the last run or 0)."""

@@ -21,7 +21,8 @@ PREC_FP64, PREC_BF16X3, PREC_F16X3 = 0, 1, 2
 PROP_FP64, PROP_FP32 = 0, 1
 MODE_STD, MODE_AT, MODE_CS = 0, 1, 2
 INTEG_RK4, INTEG_ODEINT, INTEG_AT_ADAPT, INTEG_BK_INT = 0, 1, 2, 3
-ENGINE_AUTO, ENGINE_PER_TRAJECTORY, ENGINE_LOCKSTEP, ENGINE_RESIDENT = 0, 1, 2, 3
+(ENGINE_AUTO, ENGINE_PER_TRAJECTORY, ENGINE_LOCKSTEP, ENGINE_RESIDENT,
+ ENGINE_LOCKSTEP_TAIL) = 0, 1, 2, 3, 4
 PES_TABLE, PES_LEGENDRE, PES_SITES1, PES_SITES2 = 0, 1, 2, 3
 
 i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -98,7 +99,7 @@ EXPORTS = [
     "mqct_prop_plan_sync", "mqct_prop_plan_bytes_per_step", "mqct_prop_plan_timing",
     "mqct_prop_plan_destroy", "mqct_prop_plan_set_coupled_states", "mqct_prop_plan_tune",
     "mqct_prop_plan_shape", "mqct_prop_plan_set_engine", "mqct_prop_plan_engine",
-    "mqct_prop_plan_set_cluster", "mqct_prop_plan_cluster",
+    "mqct_prop_plan_set_cluster", "mqct_prop_plan_cluster", "mqct_prop_plan_handed",
     "mqct_asym_top_level", "mqct_count_states", "mqct_enumerate_states", "mqct_count_pairs",
     "mqct_fill_ind_mat", "mqct_count_states_identical", "mqct_enumerate_states_identical",
     "mqct_count_pairs_identical", "mqct_fill_ind_mat_identical", "mqct_r_grid", "mqct_write_mtrx_uf", "mqct_read_mtrx_uf_header",
@@ -182,6 +183,7 @@ def lib():
     L.mqct_prop_plan_set_engine.argtypes = [vp, C.c_int32]
     L.mqct_prop_plan_engine.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int64)]
     L.mqct_prop_plan_set_cluster.argtypes = [vp, C.c_int32]
+    L.mqct_prop_plan_handed.argtypes = [vp, C.POINTER(C.c_int32)]
     L.mqct_prop_plan_cluster.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     L.mqct_expansion_plan_create.argtypes = [C.POINTER(Sys), i32p, C.c_int64, f64p, C.c_int32,
                                              C.c_int32, i32p, C.c_double, C.c_double, C.c_double,

@@ -692,6 +692,30 @@ __global__ void ls_start_kernel(PropDev d, LsDev L) {
 }
 
 
+// The trajectories still running at a graph boundary (every one at the start of an RK4
+// step, or before its closing evaluation): their state into the hand-over records.
+__global__ void ls_export_kernel(LsDev L, RsResume* out, int* count) {
+  const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tr >= L.n_traj) return;
+  const LsTraj& S = L.tr[tr];
+  if (!S.active) return;
+  RsResume r;
+  r.C = S.C;
+  r.tcur = S.tcur;
+  r.eki = S.eki;
+  r.eqi = S.eqi;
+  r.tmpR1 = S.tmpR1;
+  r.tmpR2 = S.tmpR2;
+  r.counter = S.counter;
+  r.status = S.status;
+  r.vib = S.vib;
+  r.period = S.period;
+  r.stage = S.stage;
+  r.hint = S.hint;
+  r.tr = tr;
+  out[atomicAdd(count, 1)] = r;
+}
+
 // ---------------------------------------------------------------- host
 struct LsEngine {
   DevBuf<LsTraj> tr;
@@ -732,7 +756,8 @@ template <class T>
 static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n, int n_sm,
                     cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
                     const mqct_traj_init_t* d_init, const mqct_traj_init_t* h_init, int n_traj,
-                    double* amp, double* cls, double* diag) {
+                    double* amp, double* cls, double* diag, int hand_below, RsResume* hand_out,
+                    int* hand_n, const double2** hand_amp) {
   using T2 = typename V2<T>::t;
   using Cfg = LsCfg<T>;
   const int N = d.N, nb = (int)blk_n.size(), arith = sizeof(T) == 4 ? 1 : 2;
@@ -768,7 +793,7 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     if (e->bucket.n != (size_t)2 * nk * e->cap_traj)
       MQCT_CUDA_TRY(e->bucket.alloc((size_t)2 * nk * e->cap_traj));
   }
-  if (!e->ctr.p) MQCT_CUDA_TRY(e->ctr.alloc(5));
+  if (!e->ctr.p) MQCT_CUDA_TRY(e->ctr.alloc(6));  // [5]: trajectories handed over
   {
     // blocks by size, largest first: the work queue hands out the longest items first
     std::vector<int> order(nb);
@@ -875,6 +900,7 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
   MQCT_CUDA_TRY(cudaMemcpyAsync(e->h_active + k, L.n_active, sizeof(int), cudaMemcpyDeviceToHost, st));
   MQCT_CUDA_TRY(cudaEventRecord(e->ev_copy[k], st));
   MQCT_CUDA_TRY(cudaEventRecord(ev1, st));
+  if (hand_n) *hand_n = 0;
   for (;;) {
     MQCT_CUDA_TRY(cudaGraphLaunch(e->graph, st));
     MQCT_CUDA_TRY(cudaMemcpyAsync(e->h_active + (k ^ 1), L.n_active, sizeof(int),
@@ -882,6 +908,21 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
     MQCT_CUDA_TRY(cudaEventRecord(e->ev_copy[k ^ 1], st));
     MQCT_CUDA_TRY(cudaEventSynchronize(e->ev_copy[k]));
     if (e->h_active[k] == 0) break;
+    if (hand_below > 0 && e->h_active[k] <= hand_below) {
+      // few trajectories left: after the graph in flight, the running ones (each at a step
+      // start or before its closing evaluation: the rounds so far are a multiple of 4) go
+      // to the caller
+      rounds += kLsRoundsPerGraph;
+      MQCT_CUDA_TRY(cudaMemsetAsync(e->ctr.p + 5, 0, sizeof(int), st));
+      ls_export_kernel<<<(n_traj + 255) / 256, 256, 0, st>>>(L, hand_out, e->ctr.p + 5);
+      MQCT_CUDA_TRY(cudaGetLastError());
+      int n = 0;
+      MQCT_CUDA_TRY(cudaMemcpyAsync(&n, e->ctr.p + 5, sizeof(int), cudaMemcpyDeviceToHost, st));
+      MQCT_CUDA_TRY(cudaStreamSynchronize(st));
+      *hand_n = n;
+      *hand_amp = e->Y.p;
+      break;
+    }
     rounds += kLsRoundsPerGraph;
     MQCT_CUDA_TRY(cudaEventRecord(ev1, st));
     k ^= 1;
@@ -898,9 +939,13 @@ static int ls_run_t(LsEngine* e, const PropDev& d, const std::vector<int>& blk_n
 
 int ls_run(LsEngine* e, const PropDev& d, bool fp32, const std::vector<int>& blk_n, int n_sm,
            cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const mqct_traj_init_t* d_init,
-           const mqct_traj_init_t* h_init, int n_traj, double* amp, double* cls, double* diag) {
-  return fp32 ? ls_run_t<float>(e, d, blk_n, n_sm, st, ev0, ev1, d_init, h_init, n_traj, amp, cls, diag)
-              : ls_run_t<double>(e, d, blk_n, n_sm, st, ev0, ev1, d_init, h_init, n_traj, amp, cls, diag);
+           const mqct_traj_init_t* h_init, int n_traj, double* amp, double* cls, double* diag,
+           int hand_below, RsResume* hand_out, int* hand_n, const double2** hand_amp) {
+  MQCT_ARG_CHECK(hand_below <= 0 || (hand_out && hand_n && hand_amp), "hand-over buffers missing");
+  return fp32 ? ls_run_t<float>(e, d, blk_n, n_sm, st, ev0, ev1, d_init, h_init, n_traj, amp,
+                                cls, diag, hand_below, hand_out, hand_n, hand_amp)
+              : ls_run_t<double>(e, d, blk_n, n_sm, st, ev0, ev1, d_init, h_init, n_traj, amp,
+                                 cls, diag, hand_below, hand_out, hand_n, hand_amp);
 }
 
 }  // namespace mqct

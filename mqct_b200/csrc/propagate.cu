@@ -1468,7 +1468,8 @@ struct PropPlan {
     if (engine == MQCT_ENGINE_PER_TRAJECTORY || records || mode != MQCT_MODE_STD || cs ||
         method != MQCT_INTEG_RK4 || !ls_eligible(h_blk_n))
       return false;
-    return engine == MQCT_ENGINE_LOCKSTEP || n_traj >= kLockstepMinBatch;
+    return engine == MQCT_ENGINE_LOCKSTEP || engine == MQCT_ENGINE_LOCKSTEP_TAIL ||
+           n_traj >= kLockstepMinBatch;
   }
   // The resident engine takes the runs the lockstep engine could take (FP32 only) when the
   // tables fit a cluster: always with MQCT_ENGINE_RESIDENT, up to kResidentMaxBatch
@@ -1483,7 +1484,8 @@ struct PropPlan {
   int rs_clusters8 = -1;  // clusters of eight CTAs resident on the device (-1: not asked yet)
   int last_rs[2] = {0, 0};  // cluster size and clusters of the last resident run
   bool use_resident(int mode, int64_t n_traj, bool records) {
-    if (engine == MQCT_ENGINE_PER_TRAJECTORY || engine == MQCT_ENGINE_LOCKSTEP || records ||
+    if (engine == MQCT_ENGINE_PER_TRAJECTORY || engine == MQCT_ENGINE_LOCKSTEP ||
+        engine == MQCT_ENGINE_LOCKSTEP_TAIL || records ||
         mode != MQCT_MODE_STD || cs || method != MQCT_INTEG_RK4 || arith != MQCT_PROP_FP32)
       return false;
     if (engine == MQCT_ENGINE_AUTO && n_traj > kResidentMaxBatch) return false;
@@ -1509,13 +1511,44 @@ struct PropPlan {
     return rs_run(rs, dev_view(MQCT_MODE_STD), h_blk_n, h_blk_s0, stream, ev0, ev1, d_init_p,
                   (int)n_traj, amp, cls, diag);
   }
+  // With MQCT_ENGINE_AUTO an FP32 lockstep run hands its last trajectories to the resident
+  // engine: once at most kHandPerCluster per resident cluster still run, the lockstep
+  // rounds, whose fixed cost no longer has trajectories to share it, stop, and each of the
+  // remaining ones continues on a cluster of its own from the start of its RK4 step (the
+  // long tail of the slowest trajectories: 58 k steps for the longest of the 4 096
+  // benchmark trajectories against 9.6 k for the median).
+  static constexpr int kHandPerCluster = 6;
+  DevBuf<RsResume> d_hand;
+  int last_handed = 0;  // trajectories the last lockstep run handed to the resident engine
   int run_lockstep(const mqct_traj_init_t* d_init_p, const mqct_traj_init_t* h_init,
                    int64_t n_traj, double* amp, double* cls, double* diag) {
     MQCT_ARG_CHECK(n_traj > 0 && n_traj < (1 << 24), "n_traj out of range for the lockstep engine");
     if (!ls) ls = ls_create();
     last_engine = MQCT_ENGINE_LOCKSTEP;
-    return ls_run(ls, dev_view(MQCT_MODE_STD), arith == MQCT_PROP_FP32, h_blk_n, n_sm, stream, ev0,
-                  ev1, d_init_p, h_init, (int)n_traj, amp, cls, diag);
+    last_handed = 0;
+    const PropDev d = dev_view(MQCT_MODE_STD);
+    int hand_below = 0;
+    if ((engine == MQCT_ENGINE_AUTO || engine == MQCT_ENGINE_LOCKSTEP_TAIL) &&
+        arith == MQCT_PROP_FP32) {
+      if (!rs) rs = rs_create();
+      rs_set_cluster(rs, rs_cl);
+      if (rs_usable(rs, d, h_blk_n, h_blk_s0, stream)) {
+        hand_below = kHandPerCluster * rs_clusters(rs);
+        if (d_hand.n < (size_t)n_traj) MQCT_CUDA_TRY(d_hand.alloc((size_t)n_traj));
+      }
+    }
+    int handed = 0;
+    const double2* hand_amp = nullptr;
+    int rc = ls_run(ls, d, arith == MQCT_PROP_FP32, h_blk_n, n_sm, stream, ev0, ev1, d_init_p,
+                    h_init, (int)n_traj, amp, cls, diag, hand_below, d_hand.p, &handed,
+                    &hand_amp);
+    if (hand_below > 0) last_engine = MQCT_ENGINE_LOCKSTEP_TAIL;
+    if (rc || handed == 0) return rc;
+    last_handed = handed;
+    last_rs[0] = rs_cluster(rs);
+    last_rs[1] = rs_clusters(rs);
+    return rs_run_resume(rs, d, h_blk_n, h_blk_s0, stream, ev1, d_init_p, d_hand.p, handed,
+                         hand_amp, amp, cls, diag);
   }
 
   ~PropPlan() {
@@ -1740,9 +1773,17 @@ int mqct_prop_plan_shape(const mqct_prop_plan* plan, int32_t* threads, int32_t* 
 int mqct_prop_plan_set_engine(mqct_prop_plan* plan, int32_t engine) {
   MQCT_ARG_CHECK(plan, "null plan");
   MQCT_ARG_CHECK(engine == MQCT_ENGINE_AUTO || engine == MQCT_ENGINE_PER_TRAJECTORY ||
-                     engine == MQCT_ENGINE_LOCKSTEP || engine == MQCT_ENGINE_RESIDENT,
+                     engine == MQCT_ENGINE_LOCKSTEP || engine == MQCT_ENGINE_RESIDENT ||
+                     engine == MQCT_ENGINE_LOCKSTEP_TAIL,
                  "unknown engine %d", engine);
   reinterpret_cast<PropPlan*>(plan)->engine = engine;
+  return MQCT_OK;
+}
+
+int mqct_prop_plan_handed(const mqct_prop_plan* plan, int32_t* n) {
+  MQCT_ARG_CHECK(plan && n, "null argument");
+  const PropPlan* p = reinterpret_cast<const PropPlan*>(plan);
+  *n = p->last_engine == MQCT_ENGINE_LOCKSTEP_TAIL ? p->last_handed : 0;
   return MQCT_OK;
 }
 
@@ -1777,7 +1818,10 @@ int mqct_prop_plan_engine(const mqct_prop_plan* plan, int32_t* engine, int64_t* 
   MQCT_ARG_CHECK(plan, "null plan");
   const PropPlan* p = reinterpret_cast<const PropPlan*>(plan);
   if (engine) *engine = p->last_engine;
-  if (rounds) *rounds = p->last_engine == MQCT_ENGINE_LOCKSTEP ? ls_rounds(p->ls) : 0;
+  if (rounds)
+    *rounds = (p->last_engine == MQCT_ENGINE_LOCKSTEP || p->last_engine == MQCT_ENGINE_LOCKSTEP_TAIL)
+                  ? ls_rounds(p->ls)
+                  : 0;
   return MQCT_OK;
 }
 

@@ -103,10 +103,23 @@ __device__ inline double kinetic(const Cls& c, double mass) {
          c.Pphi * c.Pphi / 2.0 / mass / (c.R * c.R) / (sin(c.th) * sin(c.th));
 }
 
+// A running trajectory handed from the lockstep engine to the resident engine at the
+// start of an RK4 step (stage 0) or before its closing evaluation (stage 4): its classical
+// state, bookkeeping and index; its FP64 amplitudes stay in the lockstep engine's array.
+struct RsResume {
+  Cls C;
+  double tcur, eki, eqi, tmpR1, tmpR2;
+  int counter, status, vib, period, stage, hint, tr;
+};
+
 // Lockstep engine (lockstep.cu): standard mode, RK4, no CS; every m-block of at most 128
 // states.  ls_run propagates n_traj trajectories whose initial conditions are on the
 // device (d_init) and on the host (h_init, for the bound on the rounds), writing the
 // outputs of the per-trajectory kernel; ev0 / ev1 bracket the device work on stream st.
+// With hand_below > 0 it stops at the first graph boundary after the running trajectories
+// fell to hand_below or fewer and writes those that still run into hand_out (device, n_traj
+// places), their count into *hand_n (host; 0 when the run ended in the engine) and the
+// engine's FP64 amplitude array (n_traj x N, internal order) into *hand_amp.
 struct LsEngine;
 LsEngine* ls_create();
 void ls_destroy(LsEngine* e);
@@ -114,7 +127,9 @@ bool ls_eligible(const std::vector<int>& blk_n);
 int64_t ls_rounds(const LsEngine* e);
 int ls_run(LsEngine* e, const PropDev& d, bool fp32, const std::vector<int>& blk_n, int n_sm,
            cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1, const mqct_traj_init_t* d_init,
-           const mqct_traj_init_t* h_init, int n_traj, double* amp, double* cls, double* diag);
+           const mqct_traj_init_t* h_init, int n_traj, double* amp, double* cls, double* diag,
+           int hand_below = 0, RsResume* hand_out = nullptr, int* hand_n = nullptr,
+           const double2** hand_amp = nullptr);
 
 // Cluster-resident engine (resident.cu): standard mode, RK4, no CS, FP32; one thread-block
 // cluster per trajectory holds the knot rows of its spline interval in shared memory.
@@ -131,5 +146,13 @@ bool rs_usable(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
 int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
            const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
            const mqct_traj_init_t* d_init, int n_traj, double* amp, double* cls, double* diag);
+// The n trajectories a lockstep run handed over (resume, device; their amplitudes in
+// resume_amp, n_traj x N internal order, indexed by the trajectories' own indices):
+// continued to their end, outputs at their own indices; only ev1 is recorded (after the
+// kernel).
+int rs_run_resume(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+                  const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev1,
+                  const mqct_traj_init_t* d_init, const RsResume* resume, int n,
+                  const double2* resume_amp, double* amp, double* cls, double* diag);
 
 }  // namespace mqct

@@ -94,6 +94,8 @@ struct RsDev {
   const RsRow* rows;      // per rank x nr_cap
   const uint16_t* loc;    // per rank x ns_cap: local row | local column << 8 of each slot
   const double* ih;       // per interval: 1 / (R_{k+1} - R_k)
+  const RsResume* resume;    // trajectories handed over by the lockstep engine, or null:
+  const double2* resume_amp; // then queue entry i is resume[i] with these amplitudes
   int* queue;
   double* amp;
   double* cls;
@@ -223,6 +225,33 @@ __device__ inline SplineAt rs_spline(const double* Rg, const double* ih, int nR,
   s.cc5 = (h * h) / 6.0;
   s.cc6 = s.cc5 * inv_h;
   return s;
+}
+
+// A trajectory handed over by the lockstep engine (thread 0): its state at the start of an
+// RK4 step or before its closing evaluation.
+__device__ inline void rs_resume(RsCls& S, const PropDev& d, const RsResume& r,
+                                 const mqct_traj_init_t& ti) {
+  const int t0 = S.tag[0], t1 = S.tag[1];
+  RsCls z{};
+  z.tag[0] = t0;
+  z.tag[1] = t1;
+  z.s_int = d.inv_perm[ti.s_st - 1];
+  z.dt = ti.dt;
+  z.C = r.C;
+  z.CT = r.C;
+  z.tcur = r.tcur;
+  z.eki = r.eki;
+  z.eqi = r.eqi;
+  z.tmpR1 = r.tmpR1;
+  z.tmpR2 = r.tmpR2;
+  z.counter = r.counter;
+  z.status = r.status;
+  z.vib = r.vib;
+  z.period = r.period;
+  z.stage = r.stage;
+  z.hint = r.hint;
+  z.th_c = __longlong_as_double(0x7ff8000000000000ULL);
+  S = z;
 }
 
 // The stage point's scalars, spline interval and factors, and the knot rows to load
@@ -468,11 +497,17 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
       for (int r = 0; r < D.CL; ++r) *clu.map_shared_rank(&s_tr, r) = t;
     }
     clu.sync();
-    const int tr = s_tr;
-    if (tr >= D.n_traj) break;
+    const int qi = s_tr;
+    if (qi >= D.n_traj) break;
+    const int tr = D.resume ? D.resume[qi].tr : qi;
     if (tid == 0) {
       s_ti = D.init[tr];
-      if (rs_start(S, d, D, s_ti, tr, rank == 0)) rs_point(S, d, Rg, ih);
+      if (D.resume) {
+        rs_resume(S, d, D.resume[qi], s_ti);
+        rs_point(S, d, Rg, ih);
+      } else if (rs_start(S, d, D, s_ti, tr, rank == 0)) {
+        rs_point(S, d, Rg, ih);
+      }
       s_ec = d.st_e[S.s_int];
     }
     __syncthreads();
@@ -483,8 +518,11 @@ __global__ void __launch_bounds__(RS_THREADS, 1) rs_kernel(PropDev d, RsDev D) {
       for (int lr = tid; lr < nr; lr += RS_THREADS) {
         const RsRow w = row[lr];
         const double one = w.gi == S.s_int ? 1.0 : 0.0;
-        Y[lr] = make_double2(one, 0.0);
-        a0[lr] = make_float2((float)one, 0.f);
+        // a handed-over trajectory's amplitudes, its stage input their FP32 rounding (as
+        // the lockstep engine forms it at the end of a step); else the initial unit vector
+        const double2 y0 = D.resume ? D.resume_amp[(size_t)tr * d.N + w.gi] : make_double2(one, 0.0);
+        Y[lr] = y0;
+        a0[lr] = make_float2((float)y0.x, (float)y0.y);
         push(w, a0[lr], HALO[rc & 1]);
         if (!go) {  // not propagated: the initial unit vector is the result
           amp[w.ri] = one;
@@ -879,17 +917,21 @@ bool rs_usable(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
   return rs_prepare(e, d, blk_n, blk_s0, st, &ok) == MQCT_OK && ok;
 }
 
-int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
-           const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
-           const mqct_traj_init_t* d_init, int n_traj, double* amp, double* cls, double* diag) {
+// One launch over n queue entries (trajectories, or hand-over records when resume is set);
+// ev0 recorded before it unless null, ev1 after it.
+static int rs_launch(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+                     const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev0,
+                     cudaEvent_t ev1, const mqct_traj_init_t* d_init, int n,
+                     const RsResume* resume, const double2* resume_amp, double* amp,
+                     double* cls, double* diag) {
   bool ok = false;
   int rc = rs_prepare(e, d, blk_n, blk_s0, st, &ok);
   if (rc) return rc;
   MQCT_ARG_CHECK(ok, "resident engine: the tables do not fit a cluster's shared memory");
-  MQCT_ARG_CHECK(n_traj > 0, "n_traj must be positive");
+  MQCT_ARG_CHECK(n > 0, "no trajectories");
   RsDev D{};
   D.init = d_init;
-  D.n_traj = n_traj;
+  D.n_traj = n;
   D.CL = e->CL;
   D.ns_cap = e->ns_cap;
   D.nr_cap = e->nr_cap;
@@ -903,11 +945,13 @@ int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
   D.rows = e->rows.p;
   D.loc = e->loc.p;
   D.ih = e->ih.p;
+  D.resume = resume;
+  D.resume_amp = resume_amp;
   D.queue = e->queue.p;
   D.amp = amp;
   D.cls = cls;
   D.diag = diag;
-  const int ncl = std::min(e->n_clusters, n_traj);
+  const int ncl = std::min(e->n_clusters, n);
   cudaLaunchConfig_t cfg{};
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -921,11 +965,27 @@ int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
   cfg.attrs = at;
   cfg.numAttrs = 1;
   MQCT_CUDA_TRY(cudaMemsetAsync(e->queue.p, 0, sizeof(int), st));
-  MQCT_CUDA_TRY(cudaEventRecord(ev0, st));
+  if (ev0) MQCT_CUDA_TRY(cudaEventRecord(ev0, st));
   MQCT_CUDA_TRY(cudaLaunchKernelEx(&cfg, rs_kernel, d, D));
   MQCT_CUDA_TRY(cudaGetLastError());
   MQCT_CUDA_TRY(cudaEventRecord(ev1, st));
   return MQCT_OK;
+}
+
+int rs_run(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+           const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev0, cudaEvent_t ev1,
+           const mqct_traj_init_t* d_init, int n_traj, double* amp, double* cls, double* diag) {
+  return rs_launch(e, d, blk_n, blk_s0, st, ev0, ev1, d_init, n_traj, nullptr, nullptr, amp,
+                   cls, diag);
+}
+
+int rs_run_resume(RsEngine* e, const PropDev& d, const std::vector<int>& blk_n,
+                  const std::vector<int>& blk_s0, cudaStream_t st, cudaEvent_t ev1,
+                  const mqct_traj_init_t* d_init, const RsResume* resume, int n,
+                  const double2* resume_amp, double* amp, double* cls, double* diag) {
+  MQCT_ARG_CHECK(resume && resume_amp, "hand-over records missing");
+  return rs_launch(e, d, blk_n, blk_s0, st, nullptr, ev1, d_init, n, resume, resume_amp, amp,
+                   cls, diag);
 }
 
 }  // namespace mqct

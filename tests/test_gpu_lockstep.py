@@ -156,3 +156,27 @@ def test_asym_top_system_matches_per_trajectory_kernel(mq, gpu_available, c2_tab
     p32 = mq.channel_probabilities(a32, s.indx_chann, s.n_channels)
     assert np.max(np.abs(p32 - p_pt)) < 2e-4
     assert np.all(d32[:, 4] == 0)
+
+
+def test_lockstep_tail_on_resident_engine(mq, gpu_available, c2_tables):
+    """MQCT_ENGINE_LOCKSTEP_TAIL (the plan's choice for large FP32 batches): the lockstep
+    engine hands the trajectories still running to the resident engine at a graph boundary
+    (here after the first graph: the batch is below the hand-over count), which continues
+    each from the start of its RK4 step; the results are those of the FP32 per-trajectory
+    kernel to FP32 rounding."""
+    s, trajs, tab = c2_tables["s"], c2_tables["trajs"], c2_tables["tab"]
+    plan = mq.PropagationPlan(tab, mq.PROP_FP32)
+    plan.set_engine(mq.ENGINE_LOCKSTEP_TAIL)
+    a_t, _, d_t = plan.run(trajs)
+    eng, rounds = plan.engine()
+    assert eng == mq.ENGINE_LOCKSTEP_TAIL and rounds > 0 and 0 < plan.handed() <= len(trajs)
+    plan.close()
+    a_p, _, d_p, _ = _run(mq, tab, trajs, mq.PROP_FP32, mq.ENGINE_PER_TRAJECTORY)
+    p_t = mq.channel_probabilities(a_t, s.indx_chann, s.n_channels)
+    p_p = mq.channel_probabilities(a_p, s.indx_chann, s.n_channels)
+    assert np.max(np.abs(p_t - p_p)) < 5e-5
+    assert np.all(d_t[:, 4] == 0)
+    assert np.allclose(d_t[:, 1], d_p[:, 1], rtol=1e-3)
+    # the norm errors are the RK4 discretisation's (long FP32 trajectories drift), the same
+    # for both engines to rounding
+    assert np.allclose(d_t[:, 2], d_p[:, 2], rtol=0.05, atol=1e-6)
