@@ -139,3 +139,19 @@ def test_probability_spline_cross_sections_co_h2(mq, tmp_path):
     # to the printed digits where they are not tiny
     _, _, plog = mq.splined_opacity(lt, op[:, 2:], d[:, 2], L_min, L_max)
     assert np.max(np.abs(plog[:, 0] - rows[:, 3])) < 1e-7
+
+
+def test_clamped_spline_matches_scipy(mq):
+    """The host spline of the PROB_SPLINE branch (Numerical Recipes' clamped spline with
+    chord end slopes, as the reference calls it) against scipy's clamped cubic spline on
+    a non-uniform grid, inside and outside the knots."""
+    from scipy.interpolate import CubicSpline
+    rng = np.random.default_rng(5)
+    x = np.cumsum(rng.uniform(0.5, 3.0, 25))
+    y = np.exp(-0.1 * x) * np.cos(0.7 * x) + 0.01 * rng.standard_normal(25)
+    yp1, ypn = (y[1] - y[0]) / (x[1] - x[0]), (y[-1] - y[-2]) / (x[-1] - x[-2])
+    ref = CubicSpline(x, y, bc_type=((1, yp1), (1, ypn)))
+    y2 = mq._clamped_spline(x, y)
+    assert np.allclose(y2, ref(x, 2), rtol=1e-10, atol=1e-12)
+    for v in np.concatenate([np.linspace(x[0], x[-1], 101), [x[0] - 1.0, x[-1] + 1.0]]):
+        assert abs(mq._splint(x, y, y2, v) - ref(v)) < 1e-12
