@@ -155,3 +155,33 @@ def test_clamped_spline_matches_scipy(mq):
     assert np.allclose(y2, ref(x, 2), rtol=1e-10, atol=1e-12)
     for v in np.concatenate([np.linspace(x[0], x[-1], 101), [x[0] - 1.0, x[-1] + 1.0]]):
         assert abs(mq._splint(x, y, y2, v) - ref(v)) < 1e-12
+
+
+def test_deflection_and_elastic_standard_mode_h2o_h2(mq, oracle):
+    """Standard MQCT (Coriolis coupling on) on the reference's H2O + H2 example (fixture
+    g3_h2o_h2_type8.npz, 123 trajectories): the deflection function from the oracle's
+    final classical states against the printed one (8 digits), the phases from it, and the
+    elastic cross section of CROSS_SECTIONS.out (the probabilities agree with the printed
+    ones to ~2e-7, so 1e-6 relative)."""
+    g = np.load(os.path.join(GOLD, "g3_h2o_h2_type8.npz"))
+    s = mq.CollisionSystem(8, g["channels"], A=float(g["A"]), B=float(g["B"]), C=float(g["C"]),
+                           BE=float(g["BE"]))
+    tab = mq.PropagationTables.from_system(s, g["R"], g["mat"], float(g["mass_red"]))
+    otab = oracle.OracleTables(tab.j12, tab.m12, tab.ej, tab.ind_mat, tab.R, tab.mat, tab.y2,
+                               tab.mass_au)
+    trajs, meta = mq.trajectory_set(float(g["U"]), float(g["b_impct"]), float(g["mass_red"]), 1,
+                                    float(g["time_step"]), float(g["rmax"]),
+                                    time_lim=float(g["time_lim"]))
+    ot = [oracle.make_traj(t.e_coll, t.l_real, t.s_st, t.dt, t.r_start, t.r_fin,
+                           t.numb_orb_prds, t.numb_oscl_prds, t.time_lim, t.max_steps)
+          for t in trajs]
+    amp, cls, _ = oracle.propagate_batch(otab, ot)
+    d = g["deflection"]
+    chi = mq.deflection_angles(cls, trajs, tab.mass_au)
+    assert np.max(np.abs(chi - d[:, 2])) < 2e-7
+    l = np.array([t.l_real for t in trajs])
+    ph = mq.scattering_phases(l, chi)
+    assert np.max(np.abs(ph - d[:, 3])) < 2e-6
+    p = mq.channel_probabilities(amp, s.indx_chann, 10)
+    sig = mq.elastic_cross_section(l, p[:, 0], ph, meta["k"])
+    assert abs(sig / g["sigma_U"][0] - 1) < 1e-6                # 0.9913967495E+02 A^2
